@@ -1,0 +1,126 @@
+/* qz_oracle.h -- CPU restatement of the QUARZ hot path, used ONLY as a test checker.
+ *
+ * TEST INFRASTRUCTURE. Nothing in the product (quarz_b200/) links, loads or calls this
+ * library. Only tests/, __graft_entry__.smoke() and bench.py's cpu_baseline / --impl
+ * reference leg may use it, and only to check or to time the reference algorithm on the
+ * host cores.
+ *
+ * What it restates (QUARZ v2.0.0, file:line within the reference project):
+ *   radial grid          src/RadialGrid.cpp:139-196 (generators), :231-273 (volumes)
+ *   field operators      src/FieldSolver.cpp:90-103 (fv_rows), :113-179 (L0/L1D/L1F/L2D, stencils)
+ *   solve / gradients    src/FieldSolver.cpp:242-289
+ *   tridiagonal          src/Tridiag.cpp:362-496 (Thomas, PCR, partition)
+ *   plasma species      src/PlasmaSpecies.cpp:14-48 (AB), :57-89 (geometry/gather), :202-295 (load),
+ *                        :409-478 (deposit), :480-506 (deposit_rho), :508-559 (deposit_S), :561-668 (push)
+ *   sweep                src/Simulation.cpp:394-457 (zero/combine), :477-633 (W+, Bz, B+, store),
+ *                        :636-795 (step_fields), :797-819 (solve_slice_fields), :1370-1448 (run)
+ *   beam                 src/Beam.cpp:483-570 (gaussian sampler), :725-785 (deposit), :900-905 (push),
+ *                        :948-1131 (advance, Vay only), :1133-1192 (sums / from_sums)
+ *   pushers              src/Pushers.hpp:144-176 (gamma2_root, solve_implicit, vay)
+ *   mode sums            src/SliceData.hpp:70-83
+ *
+ * Parity is pinned against the reference's own unit tests (tests/test_solvers.cpp,
+ * tests/test_pushers.cpp, tests/test_ab.cpp) and its stored validation numbers
+ * (validation/reference_full.txt, reference_quick.txt); see tests/test_oracle_*.py.
+ *
+ * Arithmetic: FP64 throughout, single-threaded, particles in index order (the reference's
+ * serial summation order); build with -ffp-contract=off so every expression rounds as written.
+ */
+#ifndef QZ_ORACLE_H
+#define QZ_ORACLE_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- random numbers used by the reference's beam generator (inputs only) ---- */
+typedef struct { uint64_t mt[312]; int idx; int have_saved; double saved; } qzo_rng;
+void     qzo_rng_seed(qzo_rng* g, uint64_t seed);
+uint64_t qzo_rng_u64(qzo_rng* g);
+double   qzo_rng_canonical(qzo_rng* g);      /* uniform [0,1) with 53 bits */
+double   qzo_rng_normal(qzo_rng* g);         /* N(0,1), polar method with one cached variate */
+
+/* ---- grid generators ---- */
+int qzo_make_uniform(double R, double dr, double* out, int cap);
+int qzo_make_regions(double R, const double* ends, const double* hs, int nreg, double max_ratio,
+                     double* out, int cap);
+
+/* ---- stand-alone pieces for unit tests ---- */
+enum { QZO_THOMAS = 0, QZO_PCR = 1, QZO_PARTITION = 2 };
+int qzo_tridiag(int method, int M, const double* a, const double* b, const double* c, const double* d,
+                double* x);
+/* (L_op - chi) f = scale*rhs on the grid given by nodes; op: 0 L0, 1 L1D, 2 L1F, 3 L2D.
+   chi/wall may be NULL. */
+int qzo_field_solve(const double* nodes, int M, int op, int method, const double* rhs, const double* chi,
+                    const double* wall, double scale, double* f);
+/* operator rows (a,b,c of length M each) and gradient stencils (gm,g0,gp,ir of length M) */
+int qzo_operator_rows(const double* nodes, int M, int op, double* a, double* b, double* c, double* flux_coef);
+int qzo_stencils(const double* nodes, int M, double* gm, double* g0, double* gp, double* ir);
+int qzo_grid_volumes(const double* nodes, int M, double* V);
+void qzo_vay(const double u[3], const double E[3], const double B[3], double eps, double out[3]);
+int qzo_ab_coeffs(int order, double* c);
+int qzo_ab_variable(int order, const double* t, double h, double* c);
+
+/* ---- whole-deck simulation ---- */
+typedef struct {
+    int modes;            /* 0 or 1 */
+    int picard;           /* B+ Picard iterations (1 for m = 0) */
+    int ab_order;         /* 1..5 */
+    double delta_min, max_qsa;
+    double xi_min, dxi;   /* internal xi of slice 0, slice spacing */
+    int K;                /* slices */
+    int ngp;              /* beams.xi_shape = ngp */
+    int tridiag;          /* QZO_THOMAS / PCR / PARTITION */
+    int neutralize;
+} qzo_params;
+
+typedef struct {
+    double q, m;
+    int ppc, ntheta;
+    int mobile;
+    double density;       /* <name>.density factor */
+    double rmax;          /* plasma.rmax (1e300: none) */
+    double channel_depth, channel_radius;   /* radial = channel when channel_radius > 0 */
+} qzo_species_params;
+
+typedef struct qzo_sim qzo_sim;
+
+qzo_sim* qzo_sim_create(const qzo_params* p, const double* nodes, int M);
+void     qzo_sim_destroy(qzo_sim* s);
+int      qzo_sim_add_species(qzo_sim* s, const qzo_species_params* sp);
+/* particles: n x 7 (x y px py pz xi w), internal xi; gref/xiref as computed by the generator */
+int      qzo_sim_add_beam(qzo_sim* s, const double* p7, long n, double q, double m, int rigid,
+                          double gref, double xiref);
+/* sample the reference's gaussian beam; writes the 7-column particles (internal xi) to out
+   (capacity n*7) and gref/xiref; returns the number of particles */
+long     qzo_sample_gaussian(double n0, double sr, double xi0_int, double sxi, double gamma0, double espread,
+                             double emit, double cut, double cx0, double cy0, double cxs, double cys,
+                             double xp0, double yp0, long np, int nrot, int mirror, uint64_t seed, double xcut,
+                             double* out, double* gref, double* xiref);
+/* one quasi-static sweep (beam deposit + plasma load + sweep), as Simulation::step_fields */
+int      qzo_sim_step_fields(qzo_sim* s, double t);
+/* beam push of every non-rigid beam */
+int      qzo_sim_push_beams(qzo_sim* s, double dt_kick, double dt_drift);
+/* 17 moment sums of beam b (Beam::sums) */
+int      qzo_sim_beam_sums(const qzo_sim* s, int b, double out[17]);
+int      qzo_sim_beam_get(const qzo_sim* s, int b, double* p7);   /* n x 7 copy out */
+long     qzo_sim_beam_count(const qzo_sim* s, int b);
+/* field store (K, M, F_NC), beam sources (K, M, B_NC), diagnostics (K, M, D_NC): read-only views */
+const double* qzo_sim_fld(const qzo_sim* s);
+const double* qzo_sim_bsrc(const qzo_sim* s);
+const double* qzo_sim_diag(const qzo_sim* s);
+long     qzo_sim_lost(const qzo_sim* s);
+/* plasma state of species sp after the last sweep (x y px py dl w, n values each) */
+int      qzo_sim_plasma_get(const qzo_sim* s, int sp, double* out6, int cap);
+/* run the reference time loop: nsteps+1 sweeps and nsteps pushes with constant dt;
+   moments (17 per beam per step, step-major) go to mom if non-NULL */
+int      qzo_sim_run(qzo_sim* s, int nsteps, double dt, double* mom);
+/* beam deposit only (into the sim's bsrc, which is zeroed first) */
+int      qzo_sim_deposit_beams(qzo_sim* s);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
