@@ -1,0 +1,172 @@
+/* qz_b200.h -- C ABI of libqz_b200.so: the B200 hot path of QUARZ (quasi-static xi sweep,
+ * beam deposit, field gather + Vay push, beam moments).
+ *
+ * Conventions
+ *   - Every entry point returns qz_status: 0 = ok, > 0 = error (qz_last_error() has the text).
+ *     No C++ exception crosses this boundary.
+ *   - "dev" pointers are CUDA device pointers on the current device; "host" pointers are host
+ *     memory. All arrays are FP64, LayoutRight (last index fastest), exactly the layouts of the
+ *     reference's Kokkos Views:
+ *        fld  (K, M, F_NC)  F_NC = 6 (m = 0) / 18 (m = 1)   src/FieldStore.hpp:9-13
+ *        bsrc (K, M, B_NC)  B_NC = 5 / 15                   src/FieldStore.hpp:16-20
+ *        diag (K, M, D_NC)  D_NC = 3 / 9                    src/Simulation.hpp:44
+ *     k = slice (head first; internal xi = xi_min + k dxi, xi_internal = -xi_user), j = node.
+ *   - `stream` is a cudaStream_t passed as void* (NULL: the legacy default stream).
+ *   - Handles are not thread-safe: one handle per host thread / stream.
+ */
+#ifndef QZ_B200_H
+#define QZ_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int qz_status;
+enum {
+    QZ_OK = 0,
+    QZ_ERR_ARG = 1,          /* invalid argument (null pointer, size, option) */
+    QZ_ERR_CUDA = 2,         /* a CUDA call failed */
+    QZ_ERR_UNSUPPORTED = 3,  /* option not on this path (e.g. laser, ionization) */
+    QZ_ERR_NOMEM = 4,        /* device or host allocation failed */
+    QZ_ERR_SIZE = 5          /* problem too large for this kernel configuration */
+};
+
+/* text of the last error of the calling thread ("" if none) */
+const char* qz_last_error(void);
+/* library version string */
+const char* qz_version(void);
+
+/* ------------------------------------------------------------------ radial grid + operators
+ * Replaces RadialGrid::RadialGrid(nodes) + RadialGrid::finalize (src/RadialGrid.cpp:229-273) and
+ * FieldSolver::FieldSolver (src/FieldSolver.cpp:113-179): hat-function volumes, the tridiagonal
+ * rows of L0 / L1D / L1F / L2D and the gradient stencils, uploaded to the device.
+ * nodes: host, M values, 0 = r_0 < r_1 < ... < r_{M-1} = R. */
+typedef struct qz_grid qz_grid;
+qz_status qz_grid_create(const double* nodes_host, int M, qz_grid** out);
+qz_status qz_grid_destroy(qz_grid* g);
+/* host copies of V_j (M) and, for op = 0..3 (L0, L1D, L1F, L2D), the rows a, b, c (M each) */
+qz_status qz_grid_volumes(const qz_grid* g, double* V_host);
+qz_status qz_grid_operator(const qz_grid* g, int op, double* a_host, double* b_host, double* c_host,
+                           double* flux_coef);
+
+/* ------------------------------------------------------------------ the xi sweep
+ * Replaces Simulation::step_fields' per-slice chain (src/Simulation.cpp:636-795) with the plasma of
+ * PlasmaSpecies (load src/PlasmaSpecies.cpp:202-295, deposit :409-478, deposit_rho :480-506,
+ * deposit_S :508-559, push :561-668) and the field solves of Simulation::solve_slice_fields
+ * (src/Simulation.cpp:797-819). Single rank, constant dxi (no sub-slicing), no laser / ionization /
+ * smoothing filter. */
+typedef struct {
+    double q, m;             /* <name>.charge, <name>.mass */
+    int ppc, ntheta;         /* <name>.ppc, <name>.ntheta */
+    int mobile;              /* <name>.mobile */
+    double density;          /* <name>.density factor */
+    double rmax;             /* plasma.rmax (use 1e300 for none) */
+    double channel_depth, channel_radius;   /* plasma.radial = channel when channel_radius > 0 */
+} qz_species;
+
+typedef struct {
+    int modes;               /* 0: m = 0 only; 1: m = 0 and 1 */
+    int picard;              /* solver.picard */
+    int ab_order;            /* pusher.ab_order, 1..5 */
+    double delta_min;        /* pusher.delta_min */
+    double max_qsa;          /* pusher.max_qsa_factor */
+    double xi_min;           /* internal xi of slice 0 (= -xi.max) */
+    double dxi;              /* xi.step */
+    int K;                   /* slices */
+    int ngp;                 /* beams.xi_shape = ngp */
+    int neutralize;          /* plasma.neutralize */
+    int nspecies;
+    qz_species species[4];
+} qz_sweep_params;
+
+typedef struct {
+    unsigned long long lost;     /* plasma particles removed (trapped / beyond the wall) */
+    unsigned long long reserved[3];
+} qz_counters;
+
+typedef struct qz_sweep qz_sweep;
+qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p, qz_sweep** out);
+qz_status qz_sweep_destroy(qz_sweep* s);
+/* One sweep. bsrc (dev, read), fld / diag (dev, written), counters (host, optional, accumulated). */
+qz_status qz_sweep_run(qz_sweep* s, const double* bsrc_dev, double* fld_dev, double* diag_dev,
+                       qz_counters* counters_host, void* stream);
+/* plasma state after the last sweep: out_host (6, n) = x y px py Delta w; returns n in *n */
+qz_status qz_sweep_plasma(qz_sweep* s, double* out_host, int cap, int* n);
+/* per-phase clock cycles of the last run (6 values: prologue, deposit, psi/E_z/B_z, S, B+, store+push);
+   enable = 1 turns the counters on for later runs */
+qz_status qz_sweep_timing(qz_sweep* s, int enable, unsigned long long* cycles6_host);
+
+/* ------------------------------------------------------------------ beams
+ * A beam is a view of 7 device columns (x y px py pz xi w), internal xi.
+ * Replaces Beam::deposit (src/Beam.cpp:725-785), Beam::push / advance with the Vay pusher
+ * (src/Beam.cpp:900-905, :948-1131) and Beam::sums (src/Beam.cpp:1133-1155). */
+typedef struct {
+    double *x, *y, *px, *py, *pz, *xi, *w;
+    int64_t n;
+    double q, m;
+} qz_beam_view;
+
+typedef struct {
+    double xi_min, dxi;
+    int K;
+    int ngp;
+    int modes;
+} qz_box;
+
+/* adds the beam's sources to bsrc (dev, (K, M, B_NC)); bsrc is NOT cleared */
+qz_status qz_beam_deposit(const qz_grid* g, const qz_beam_view* b, const qz_box* box, double* bsrc_dev,
+                          void* stream);
+/* advance by dt (move = 1) or the explicit start-up kick (move = 0) with the fields fld (dev) */
+qz_status qz_beam_advance(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld_dev,
+                          double dt_kick, double dt_drift, int move, void* stream);
+/* Beam::push: start-up half kick when *started == 0 (then *started = 1), then a full step. */
+qz_status qz_beam_push(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld_dev,
+                       double dt_kick, double dt_drift, int* started, void* stream);
+/* Beam::push followed by Beam::deposit of the moved particle into bsrc_next (dev, not cleared):
+   the two passes of consecutive time steps in one pass over the particles */
+qz_status qz_beam_push_deposit(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld_dev,
+                               double dt_kick, double dt_drift, int* started, double* bsrc_next_dev,
+                               void* stream);
+/* the 17 moment sums of Beam::sums into out17 (dev); deterministic order */
+qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
+
+/* The reference's gaussian generator (Beam::init_gaussian, src/Beam.cpp:483-570) on the host, with
+   the same std::mt19937_64 / std::normal_distribution stream. out_host: n x 7 (internal xi).
+   sxi <= 0 selects the flattop profile of length -sxi. Returns the particle count in *n. */
+qz_status qz_sample_gaussian(double n0, double sigma_r, double xi0_internal, double sigma_xi, double gamma0,
+                             double espread, double emit_n, double cut, double x0, double y0, double xs_internal,
+                             double ys_internal, double xp0, double yp0, int64_t nparticles, int nsym,
+                             int mirror_y, uint64_t seed, double xi_cut_internal, double* out_host,
+                             double* gref, double* xiref, int64_t* n);
+
+/* ------------------------------------------------------------------ whole time steps
+ * Simulation::run's loop (src/Simulation.cpp:1370-1448) for constant dt: per step one sweep and
+ * (except after the last sweep) one push of every non-rigid beam, with the next step's beam
+ * deposit fused into the push. Beams are given as HOST arrays (n x 7) and copied in; results
+ * (fields, moments, final particles) are copied back. */
+typedef struct qz_sim qz_sim;
+qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, qz_sim** out);
+qz_status qz_sim_destroy(qz_sim* s);
+qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q, double m, int rigid,
+                          double gref, double xiref);
+/* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL */
+qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, void* stream);
+/* copy out the field store / diagnostics of the last sweep (host, K*M*F_NC / K*M*D_NC) */
+qz_status qz_sim_fields(qz_sim* s, double* fld_host, double* diag_host);
+/* copy out beam b's particles (host, n x 7) */
+qz_status qz_sim_beam(qz_sim* s, int b, double* p7_host);
+qz_status qz_sim_counters(qz_sim* s, qz_counters* out);
+/* One time step with HOST beam buffers, the per-step call of an adapter whose beams live in host
+   memory (Simulation::step_fields + Beam::push on host Views, src/Simulation.cpp:1396-1442): copies
+   every beam in (cols_host[b]: 7 x n SoA, x y px py pz xi w), deposits all beams, sweeps, computes
+   the moments (moments_host: nbeams x 17, or NULL), pushes the non-rigid beams when push != 0, and
+   copies the particles back into cols_host. Pinned host memory makes the copies asynchronous. */
+qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, double dt_drift, int push,
+                           double* moments_host, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

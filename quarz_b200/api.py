@@ -1,0 +1,253 @@
+"""Python objects over the C ABI of libqz_b200 (names follow the reference's classes).
+
+Device memory is handled with torch tensors (float64, cuda) purely as plumbing: the kernels receive
+raw device pointers through the C ABI.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from . import deck as _deck
+from ._lib import BeamView, Box, Counters, QZError, Species, SweepParams, check, lib
+
+_dp = C.POINTER(C.c_double)
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp)
+
+
+def _stream_ptr(stream) -> Optional[int]:
+    if stream is None:
+        return None
+    return int(getattr(stream, "cuda_stream", stream))
+
+
+def _dev(t) -> int:
+    import torch
+
+    if not (isinstance(t, torch.Tensor) and t.is_cuda and t.dtype == torch.float64 and t.is_contiguous()):
+        raise QZError(1, "expected a contiguous float64 CUDA tensor")
+    return t.data_ptr()
+
+
+# ---------------------------------------------------------------- grid
+class RadialGrid:
+    """Radial grid, node volumes, operator rows and stencils on the device (qz_grid)."""
+
+    def __init__(self, nodes: Sequence[float]):
+        self.nodes = np.ascontiguousarray(nodes, dtype=np.float64)
+        h = C.c_void_p()
+        check(lib().qz_grid_create(_p(self.nodes), len(self.nodes), C.byref(h)))
+        self.h = h
+
+    @property
+    def M(self) -> int:
+        return len(self.nodes)
+
+    def volumes(self) -> np.ndarray:
+        V = np.zeros(self.M)
+        check(lib().qz_grid_volumes(self.h, _p(V)))
+        return V
+
+    def operator(self, op: str):
+        k = {"L0": 0, "L1D": 1, "L1F": 2, "L2D": 3}[op]
+        a, b, c, fc = np.zeros(self.M), np.zeros(self.M), np.zeros(self.M), np.zeros(1)
+        check(lib().qz_grid_operator(self.h, k, _p(a), _p(b), _p(c), _p(fc)))
+        return a, b, c, float(fc[0])
+
+    def __del__(self):
+        if getattr(self, "h", None) and lib is not None:
+            try:
+                lib().qz_grid_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+
+def sweep_params(spec: "_deck.RunSpec") -> SweepParams:
+    """qz_sweep_params from a RunSpec (quarz_b200.deck)."""
+    p = SweepParams()
+    p.modes = spec.modes
+    p.picard = spec.picard
+    p.ab_order = spec.ab_order
+    p.delta_min = spec.delta_min
+    p.max_qsa = spec.max_qsa
+    p.xi_min = spec.xi_min
+    p.dxi = spec.dxi
+    p.K = spec.K
+    p.ngp = 1 if spec.ngp else 0
+    p.neutralize = 1 if spec.neutralize else 0
+    if len(spec.species) > 4:
+        raise QZError(1, "at most 4 plasma species")
+    p.nspecies = len(spec.species)
+    for i, sp in enumerate(spec.species):
+        p.species[i] = Species(q=sp.q, m=sp.m, ppc=sp.ppc, ntheta=sp.ntheta, mobile=1 if sp.mobile else 0,
+                               density=sp.density, rmax=sp.rmax, channel_depth=sp.channel_depth,
+                               channel_radius=sp.channel_radius)
+    return p
+
+
+# ---------------------------------------------------------------- sweep
+class Sweep:
+    """One quasi-static sweep per call (qz_sweep)."""
+
+    def __init__(self, grid: RadialGrid, params: SweepParams):
+        self.grid = grid
+        self.params = params
+        h = C.c_void_p()
+        check(lib().qz_sweep_create(grid.h, C.byref(params), C.byref(h)))
+        self.h = h
+
+    def run(self, bsrc, fld, diag, stream=None) -> int:
+        cnt = Counters()
+        check(lib().qz_sweep_run(self.h, _dev(bsrc), _dev(fld), _dev(diag), C.byref(cnt), _stream_ptr(stream)))
+        return int(cnt.lost)
+
+    def run_async(self, bsrc, fld, diag, stream=None) -> None:
+        check(lib().qz_sweep_run(self.h, _dev(bsrc), _dev(fld), _dev(diag), None, _stream_ptr(stream)))
+
+    def plasma(self) -> np.ndarray:
+        cap = 1 << 22
+        out = np.zeros(6 * cap)
+        n = C.c_int()
+        check(lib().qz_sweep_plasma(self.h, _p(out), cap, C.byref(n)))
+        return out[: 6 * n.value].reshape(6, n.value)
+
+    def timing(self, enable: bool = True) -> np.ndarray:
+        cyc = (C.c_ulonglong * 6)()
+        check(lib().qz_sweep_timing(self.h, 1 if enable else 0, cyc))
+        return np.array(list(cyc), dtype=np.float64)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().qz_sweep_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+
+# ---------------------------------------------------------------- beams
+class BeamOps:
+    """Beam deposit / push / sums on 7 device columns (tensor (7, n): x y px py pz xi w)."""
+
+    @staticmethod
+    def view(cols, q: float, m: float) -> BeamView:
+        base = _dev(cols)
+        n = cols.shape[1]
+        v = BeamView()
+        for c, name in enumerate(("x", "y", "px", "py", "pz", "xi", "w")):
+            setattr(v, name, base + 8 * n * c)
+        v.n, v.q, v.m = n, q, m
+        return v
+
+    @staticmethod
+    def box(xi_min: float, dxi: float, K: int, ngp: bool = False, modes: int = 0) -> Box:
+        return Box(xi_min=xi_min, dxi=dxi, K=K, ngp=1 if ngp else 0, modes=modes)
+
+    @staticmethod
+    def deposit(grid: RadialGrid, cols, q, m, box: Box, bsrc, stream=None):
+        v = BeamOps.view(cols, q, m)
+        check(lib().qz_beam_deposit(grid.h, C.byref(v), C.byref(box), _dev(bsrc), _stream_ptr(stream)))
+
+    @staticmethod
+    def advance(grid, cols, q, m, box, fld, dt_kick, dt_drift, move, stream=None):
+        v = BeamOps.view(cols, q, m)
+        check(lib().qz_beam_advance(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift, int(move),
+                                    _stream_ptr(stream)))
+
+    @staticmethod
+    def push(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, stream=None) -> int:
+        v = BeamOps.view(cols, q, m)
+        st = C.c_int(started)
+        check(lib().qz_beam_push(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift, C.byref(st),
+                                 _stream_ptr(stream)))
+        return st.value
+
+    @staticmethod
+    def push_deposit(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, bsrc_next, stream=None) -> int:
+        v = BeamOps.view(cols, q, m)
+        st = C.c_int(started)
+        check(lib().qz_beam_push_deposit(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift,
+                                         C.byref(st), _dev(bsrc_next), _stream_ptr(stream)))
+        return st.value
+
+    @staticmethod
+    def sums(cols, gref, xiref, out17, stream=None):
+        v = BeamOps.view(cols, -1.0, 1.0)
+        check(lib().qz_beam_sums(C.byref(v), gref, xiref, _dev(out17), _stream_ptr(stream)))
+
+
+def sample_gaussian(n0, sr, xi0, sxi, gamma0, espread, emit, cut, cx0, cy0, cxs, cys, xp0, yp0, np_, nrot, mirror,
+                    seed, xcut) -> Tuple[np.ndarray, float, float]:
+    """The reference's gaussian beam generator (std::mt19937_64 + std::normal_distribution), on the host."""
+    out = np.zeros((int(np_), 7))
+    gref, xiref = np.zeros(1), np.zeros(1)
+    n = C.c_int64()
+    check(lib().qz_sample_gaussian(n0, sr, xi0, sxi, gamma0, espread, emit, cut, cx0, cy0, cxs, cys, xp0, yp0,
+                                   int(np_), int(nrot), int(mirror), C.c_uint64(int(seed)), xcut, _p(out), _p(gref),
+                                   _p(xiref), C.byref(n)))
+    return out[: n.value], float(gref[0]), float(xiref[0])
+
+
+def sample_beam(b: "_deck.BeamSpec"):
+    a = _deck.sampler_args(b)
+    a["np_"] = a.pop("np")
+    return sample_gaussian(**a)
+
+
+# ---------------------------------------------------------------- whole time steps
+class Simulation:
+    """Simulation::run for constant dt on one GPU (qz_sim): sweeps, moments, fused push + deposit."""
+
+    def __init__(self, spec: "_deck.RunSpec", beams: Optional[List[Tuple[np.ndarray, float, float]]] = None):
+        self.spec = spec
+        self.grid = RadialGrid(spec.nodes)
+        self.params = sweep_params(spec)
+        h = C.c_void_p()
+        check(lib().qz_sim_create(self.grid.h, C.byref(self.params), C.byref(h)))
+        self.h = h
+        self.beam_data = []
+        for i, b in enumerate(spec.beams):
+            parts, gref, xiref = beams[i] if beams is not None else sample_beam(b)
+            parts = np.ascontiguousarray(parts, dtype=np.float64)
+            self.beam_data.append((parts, gref, xiref))
+            check(lib().qz_sim_add_beam(self.h, _p(parts), len(parts), b.q, b.m, 1 if b.rigid else 0, gref, xiref))
+        self.fnc = 18 if spec.modes else 6
+        self.dnc = 9 if spec.modes else 3
+
+    def run(self, nsteps: int, dt: float, stream=None) -> np.ndarray:
+        nb = len(self.spec.beams)
+        mom = np.zeros((nsteps + 1, max(nb, 1), 17))
+        check(lib().qz_sim_run(self.h, int(nsteps), float(dt), _p(mom) if nb else None, _stream_ptr(stream)))
+        return mom[:, :nb, :]
+
+    def fields(self):
+        K, M = self.spec.K, self.spec.M
+        fld = np.zeros(K * M * self.fnc)
+        diag = np.zeros(K * M * self.dnc)
+        check(lib().qz_sim_fields(self.h, _p(fld), _p(diag)))
+        return fld.reshape(K, M, self.fnc), diag.reshape(K, M, self.dnc)
+
+    def beam(self, b: int) -> np.ndarray:
+        n = len(self.beam_data[b][0])
+        out = np.zeros((n, 7))
+        check(lib().qz_sim_beam(self.h, b, _p(out)))
+        return out
+
+    def lost(self) -> int:
+        c = Counters()
+        check(lib().qz_sim_counters(self.h, C.byref(c)))
+        return int(c.lost)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().qz_sim_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None

@@ -1,0 +1,803 @@
+// qz_abi.cu -- the extern "C" boundary of libqz_b200.so (declared in include/qz_b200.h) and the
+// host-side set-up it needs: grid volumes and operator rows (computed on the host in FP64 exactly
+// as the reference does, then uploaded), the fresh plasma of the box head, the gaussian beam
+// generator, and the time-step runner.
+#include "qz_b200.h"
+#include "qz_internal.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <random>
+#include <string>
+#include <vector>
+
+namespace {
+
+thread_local std::string g_err;
+
+qz_status fail(qz_status code, const std::string& msg) {
+    g_err = msg;
+    return code;
+}
+
+#define QZ_CUDA(call)                                                                          \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(QZ_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));      \
+    } while (0)
+
+constexpr double PI = 3.14159265358979323846;
+
+template <class T>
+qz_status dev_upload(T** dst, const std::vector<T>& src) {
+    *dst = nullptr;
+    if (src.empty()) return QZ_OK;
+    QZ_CUDA(cudaMalloc((void**)dst, sizeof(T) * src.size()));
+    QZ_CUDA(cudaMemcpy(*dst, src.data(), sizeof(T) * src.size(), cudaMemcpyHostToDevice));
+    return QZ_OK;
+}
+
+}  // namespace
+
+// ===================================================================== grid
+struct qz_grid {
+    int M = 0, N = 0, C = 0;
+    double R = 0;
+    std::vector<double> r, h, rmid, V, inv_h, inv_V;
+    std::vector<double> opa[4], opb[4], opc[4];
+    double flux_coef = 0;
+    std::vector<double> gm, g0, gp, ir;
+    // device
+    double *d_r = nullptr, *d_inv_h = nullptr, *d_inv_V = nullptr;
+    double *d_gm = nullptr, *d_g0 = nullptr, *d_gp = nullptr, *d_ir = nullptr;
+    double* d_opT = nullptr;     // L0, L1D, L1F, L2D rows chunk-transposed, [4][3][32*C]
+    ~qz_grid() {
+        for (double* p : {d_r, d_inv_h, d_inv_V, d_gm, d_g0, d_gp, d_ir, d_opT})
+            if (p) cudaFree(p);
+    }
+};
+
+namespace {
+
+// rows of the finite-volume operator L_n, n >= 1 (src/FieldSolver.cpp:90-103)
+void fv_rows(const qz_grid& g, int n, std::vector<double>& a, std::vector<double>& b, std::vector<double>& c) {
+    const int N = g.N, M = N + 1;
+    a.assign(M, 0.0); b.assign(M, 0.0); c.assign(M, 0.0);
+    b[0] = 1.0;
+    b[N] = 1.0;
+    auto kp = [&](int j) { return 1.0 / (g.h[j] * std::pow(g.rmid[j], 2 * n - 1)); };
+    for (int j = 1; j < N; ++j) {
+        const double dV = 0.5 * (g.h[j] + g.h[j - 1]);
+        const double pre = std::pow(g.r[j], n - 1) / dV;
+        c[j] = pre * std::pow(g.r[j + 1], n) * kp(j);
+        a[j] = pre * std::pow(g.r[j - 1], n) * kp(j - 1);
+        b[j] = -pre * std::pow(g.r[j], n) * (kp(j) + kp(j - 1));
+    }
+}
+
+int chunk_rows(int M) {
+    int C = (M + 31) / 32;
+    if (C < 2) C = 2;
+    if ((C & 1) == 0) ++C;    // odd stride: lanes of a warp hit distinct shared-memory banks
+    return C;
+}
+
+}  // namespace
+
+extern "C" const char* qz_last_error(void) { return g_err.c_str(); }
+extern "C" const char* qz_version(void) { return "qz_b200 0.1 (sm_100a, FP64)"; }
+
+extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
+    if (!nodes || !out) return fail(QZ_ERR_ARG, "qz_grid_create: null pointer");
+    *out = nullptr;
+    if (M < 3) return fail(QZ_ERR_ARG, "grid: need at least 2 cells");
+    if (std::abs(nodes[0]) > 0) return fail(QZ_ERR_ARG, "grid: first node must be r=0");
+    for (int j = 1; j < M; ++j)
+        if (!(nodes[j] > nodes[j - 1])) return fail(QZ_ERR_ARG, "grid: nodes must be strictly increasing");
+    qz_grid* g = new (std::nothrow) qz_grid;
+    if (!g) return fail(QZ_ERR_NOMEM, "qz_grid_create: out of host memory");
+    // src/RadialGrid.cpp:231-273
+    g->M = M;
+    g->N = M - 1;
+    const int N = g->N;
+    g->r.assign(nodes, nodes + M);
+    g->R = g->r[N];
+    g->h.resize(N);
+    g->rmid.resize(N);
+    for (int j = 0; j < N; ++j) {
+        g->h[j] = g->r[j + 1] - g->r[j];
+        g->rmid[j] = 0.5 * (g->r[j + 1] + g->r[j]);
+    }
+    g->V.assign(M, 0.0);
+    for (int j = 0; j <= N; ++j) {
+        double v = 0;
+        if (j > 0) v += g->r[j - 1] * g->h[j - 1] / 2 + g->h[j - 1] * g->h[j - 1] / 3;
+        if (j < N) v += g->r[j] * g->h[j] / 2 + g->h[j] * g->h[j] / 6;
+        g->V[j] = 2 * PI * v;
+    }
+    g->inv_V.resize(M);
+    g->inv_h.resize(N);
+    for (int j = 0; j <= N; ++j) g->inv_V[j] = 1.0 / g->V[j];
+    for (int j = 0; j < N; ++j) g->inv_h[j] = 1.0 / g->h[j];
+    // operators (src/FieldSolver.cpp:117-156)
+    {
+        std::vector<double>&a = g->opa[0], &b = g->opb[0], &c = g->opc[0];
+        a.assign(M, 0.0); b.assign(M, 0.0); c.assign(M, 0.0);
+        for (int j = 0; j < N; ++j) {
+            const double invV = 2 * PI / g->V[j];
+            a[j] = (j > 0) ? g->rmid[j - 1] / g->h[j - 1] * invV : 0.0;
+            c[j] = g->rmid[j] / g->h[j] * invV;
+            b[j] = -(a[j] + c[j]);
+        }
+        b[N] = 1.0;
+    }
+    fv_rows(*g, 1, g->opa[1], g->opb[1], g->opc[1]);
+    fv_rows(*g, 1, g->opa[2], g->opb[2], g->opc[2]);
+    {
+        const double dV = 0.5 * g->h[N - 1];
+        const double kp = 1.0 / (g->h[N - 1] * std::pow(g->rmid[N - 1], 2 * 1 - 1));
+        const double k = kp / dV;
+        g->opa[2][N] = g->r[N - 1] * k;
+        g->opb[2][N] = -g->r[N] * k;
+        g->flux_coef = 1.0 / dV;
+    }
+    fv_rows(*g, 2, g->opa[3], g->opb[3], g->opc[3]);
+    // gradient stencils and 1/r (src/FieldSolver.cpp:157-176)
+    g->gm.assign(M, 0.0); g->g0.assign(M, 0.0); g->gp.assign(M, 0.0); g->ir.assign(M, 0.0);
+    for (int j = 1; j < N; ++j) {
+        const double hm = g->h[j - 1], hp = g->h[j];
+        const double den = hm * hp * (hm + hp);
+        g->gp[j] = hm * hm / den;
+        g->gm[j] = -hp * hp / den;
+        g->g0[j] = (hp * hp - hm * hm) / den;
+    }
+    {
+        const double h1 = g->h[N - 1], h2 = (N >= 2) ? g->h[N - 2] : g->h[N - 1];
+        const double s = h1 + h2;
+        g->g0[N] = (2 * h1 + h2) / (h1 * s);
+        g->gm[N] = -s / (h1 * h2);
+        g->gp[N] = h1 / (h2 * s);
+    }
+    for (int j = 1; j <= N; ++j) g->ir[j] = 1.0 / g->r[j];
+    g->ir[0] = 1.0 / g->r[1];
+    // chunk-transposed operator rows for the warp solver: row i = lane*C + ii at [ii*32 + lane];
+    // rows beyond M are identity rows
+    g->C = chunk_rows(M);
+    const int C = g->C;
+    std::vector<double> opT((size_t)4 * 3 * 32 * C, 0.0);
+    for (int op = 0; op < 4; ++op)
+        for (int lane = 0; lane < 32; ++lane)
+            for (int ii = 0; ii < C; ++ii) {
+                const int i = lane * C + ii;
+                const size_t t = (size_t)ii * 32 + lane;
+                double* base = opT.data() + (size_t)op * 3 * 32 * C;
+                base[t] = i < M ? g->opa[op][i] : 0.0;
+                base[32 * C + t] = i < M ? g->opb[op][i] : 1.0;
+                base[64 * C + t] = i < M ? g->opc[op][i] : 0.0;
+            }
+    qz_status st;
+    if ((st = dev_upload(&g->d_r, g->r)) || (st = dev_upload(&g->d_inv_h, g->inv_h)) ||
+        (st = dev_upload(&g->d_inv_V, g->inv_V)) || (st = dev_upload(&g->d_gm, g->gm)) ||
+        (st = dev_upload(&g->d_g0, g->g0)) || (st = dev_upload(&g->d_gp, g->gp)) ||
+        (st = dev_upload(&g->d_ir, g->ir)) || (st = dev_upload(&g->d_opT, opT))) {
+        delete g;
+        return st;
+    }
+    *out = g;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_grid_destroy(qz_grid* g) {
+    delete g;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_grid_volumes(const qz_grid* g, double* V) {
+    if (!g || !V) return fail(QZ_ERR_ARG, "qz_grid_volumes: null pointer");
+    std::memcpy(V, g->V.data(), sizeof(double) * g->M);
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_grid_operator(const qz_grid* g, int op, double* a, double* b, double* c, double* fc) {
+    if (!g || !a || !b || !c || op < 0 || op > 3) return fail(QZ_ERR_ARG, "qz_grid_operator: bad argument");
+    std::memcpy(a, g->opa[op].data(), sizeof(double) * g->M);
+    std::memcpy(b, g->opb[op].data(), sizeof(double) * g->M);
+    std::memcpy(c, g->opc[op].data(), sizeof(double) * g->M);
+    if (fc) *fc = g->flux_coef;
+    return QZ_OK;
+}
+
+// ===================================================================== sweep
+struct qz_sweep {
+    const qz_grid* g = nullptr;
+    qz_sweep_params p{};
+    int np = 0, npad = 0, nbg = 0;
+    double* d_pinit = nullptr;
+    double* d_bg = nullptr;
+    double* d_ps = nullptr;
+    double* d_q = nullptr;
+    unsigned long long* d_cnt = nullptr;
+    unsigned long long* d_tim = nullptr;
+    bool timing = false;
+    qzb::SweepArgs base{};
+    ~qz_sweep() {
+        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_q, (void*)d_cnt, (void*)d_tim})
+            if (q) cudaFree(q);
+    }
+};
+
+namespace {
+
+double prof_radial(const qz_species& s, double r) {
+    if (r > s.rmax) return 0.0;
+    if (s.channel_radius > 0) return 1.0 + s.channel_depth * (r / s.channel_radius) * (r / s.channel_radius);
+    return 1.0;
+}
+
+// fresh cold plasma rings of one species at the box head (src/PlasmaSpecies.cpp:202-295):
+// appends x y px py Delta w per particle
+void load_species(const qz_grid& g, const qz_species& sp, std::vector<double> cols[6]) {
+    const double fz = 1.0 * sp.density;
+    const int ppc = sp.ppc, nth = sp.ntheta;
+    for (int j = 0; j < g.N; ++j) {
+        const double h = g.h[j];
+        for (int m = 0; m < ppc; ++m) {
+            const double ra = g.r[j] + m * h / ppc, rb = g.r[j] + (m + 1) * h / ppc;
+            const double r = (2.0 / 3.0) * (rb * rb * rb - ra * ra * ra) / (rb * rb - ra * ra);
+            const double vring = fz * PI * (rb * rb - ra * ra);
+            const double wring = prof_radial(sp, r) * vring;
+            const double off = ((j * ppc + m) % 2) * 0.5;
+            for (int l = 0; l < nth; ++l) {
+                const double th = 2 * PI * (l + off) / nth;
+                const double X = (nth == 1) ? r : r * std::cos(th), Y = (nth == 1) ? 0.0 : r * std::sin(th);
+                const double W = wring / nth;
+                if (W == 0) continue;
+                cols[0].push_back(X); cols[1].push_back(Y); cols[2].push_back(0.0); cols[3].push_back(0.0);
+                cols[4].push_back(1.0); cols[5].push_back(W);
+            }
+        }
+    }
+}
+
+}  // namespace
+
+extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p, qz_sweep** out) {
+    if (!g || !p || !out) return fail(QZ_ERR_ARG, "qz_sweep_create: null pointer");
+    *out = nullptr;
+    if (p->modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_create: modes = 1 is not built yet");
+    if (p->ab_order < 1 || p->ab_order > 5) return fail(QZ_ERR_ARG, "pusher.ab_order must be 1..5");
+    if (p->K < 1 || !(p->dxi > 0)) return fail(QZ_ERR_ARG, "xi: need K >= 1 and dxi > 0");
+    if (p->nspecies < 0 || p->nspecies > 4) return fail(QZ_ERR_ARG, "nspecies must be 0..4");
+    const int M = g->M;
+    int dev = 0, optin = 0;
+    QZ_CUDA(cudaGetDevice(&dev));
+    QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    // shared-memory layout: the fastest that fits (double-buffered sources, operator rows, solver
+    // scratch in shared memory), else move the solver scratch and the operator rows to global memory
+    static const bool kLayouts[5][3] = {{true, true, true}, {false, true, true}, {false, true, false},
+                                        {false, false, true}, {false, false, false}};
+    int lay = -1;
+    for (int i = 0; i < 5 && lay < 0; ++i) {
+        if (qzb::sweep_m0_smem_bytes(M, g->C, kLayouts[i][0], kLayouts[i][1], kLayouts[i][2]) <= (size_t)optin)
+            lay = i;
+    }
+    const bool q_in_smem = lay >= 0 && kLayouts[lay][2];
+    const size_t smem = lay >= 0 ? qzb::sweep_m0_smem_bytes(M, g->C, kLayouts[lay][0], kLayouts[lay][1],
+                                                             kLayouts[lay][2])
+                                 : qzb::sweep_m0_smem_bytes(M, g->C, false, false, false);
+    if (lay < 0)
+        return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " needs " + std::to_string(smem) +
+                                     " B of shared memory, the device allows " + std::to_string(optin));
+    qz_sweep* s = new (std::nothrow) qz_sweep;
+    if (!s) return fail(QZ_ERR_NOMEM, "qz_sweep_create: out of host memory");
+    s->g = g;
+    s->p = *p;
+    // plasma: mobile species -> particle state, immobile -> background particles
+    std::vector<double> mob[6], bg[3];
+    qzb::SweepArgs& A = s->base;
+    A.nsp = 0;
+    A.sp_off[0] = 0;
+    for (int i = 0; i < p->nspecies; ++i) {
+        const qz_species& sp = p->species[i];
+        if (sp.ppc < 1 || sp.ntheta < 1 || !(sp.m > 0)) {
+            delete s;
+            return fail(QZ_ERR_ARG, "species: ppc, ntheta >= 1 and m > 0 required");
+        }
+        std::vector<double> cols[6];
+        load_species(*g, sp, cols);
+        if (sp.mobile) {
+            for (int v = 0; v < 6; ++v) mob[v].insert(mob[v].end(), cols[v].begin(), cols[v].end());
+            A.sp_q[A.nsp] = sp.q;
+            A.sp_qm[A.nsp] = sp.q / sp.m;
+            ++A.nsp;
+            A.sp_off[A.nsp] = (int)mob[0].size();
+        } else {
+            bg[0].insert(bg[0].end(), cols[0].begin(), cols[0].end());
+            bg[1].insert(bg[1].end(), cols[1].begin(), cols[1].end());
+            for (double w : cols[5]) bg[2].push_back(w * sp.q);
+        }
+    }
+    s->np = (int)mob[0].size();
+    s->npad = ((s->np + 31) / 32) * 32;
+    if (s->npad == 0) s->npad = 32;
+    s->nbg = (int)bg[0].size();
+    std::vector<double> pinit((size_t)6 * s->npad, 0.0);
+    for (int v = 0; v < 6; ++v) std::copy(mob[v].begin(), mob[v].end(), pinit.begin() + (size_t)v * s->npad);
+    std::vector<double> bgp;
+    for (int v = 0; v < 3; ++v) bgp.insert(bgp.end(), bg[v].begin(), bg[v].end());
+    qz_status st;
+    if ((st = dev_upload(&s->d_pinit, pinit)) || (st = dev_upload(&s->d_bg, bgp))) {
+        delete s;
+        return st;
+    }
+    const size_t nps = (size_t)(6 + 5 * p->ab_order) * s->npad;
+    if (cudaMalloc((void**)&s->d_ps, sizeof(double) * nps) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_cnt, sizeof(unsigned long long) * 4) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_tim, sizeof(unsigned long long) * 8) != cudaSuccess ||
+        (!q_in_smem && cudaMalloc((void**)&s->d_q, sizeof(double) * 9 * 32 * (size_t)g->C) != cudaSuccess)) {
+        delete s;
+        return fail(QZ_ERR_NOMEM, "qz_sweep_create: device allocation failed");
+    }
+    // AB coefficients (src/PlasmaSpecies.cpp:14-28)
+    static const double AB[5][5] = {{1, 0, 0, 0, 0},
+                                    {1.5, -0.5, 0, 0, 0},
+                                    {23. / 12, -16. / 12, 5. / 12, 0, 0},
+                                    {55. / 24, -59. / 24, 37. / 24, -9. / 24, 0},
+                                    {1901. / 720, -2774. / 720, 2616. / 720, -1274. / 720, 251. / 720}};
+    A.M = M;
+    A.N = g->N;
+    A.K = p->K;
+    A.C = g->C;
+    A.R = g->R;
+    A.dxi = p->dxi;
+    A.idxi = 1.0 / p->dxi;
+    A.r = g->d_r; A.inv_h = g->d_inv_h; A.inv_V = g->d_inv_V;
+    A.gm = g->d_gm; A.g0 = g->d_g0; A.gp = g->d_gp; A.ir = g->d_ir;
+    A.opT = g->d_opT;
+    A.flux_coef = g->flux_coef;
+    A.np = s->np;
+    A.npad = s->npad;
+    A.ord = p->ab_order;
+    for (int m = 0; m < 5; ++m) A.ab[m] = AB[p->ab_order - 1][m];
+    A.delta_min = p->delta_min;
+    A.max_qsa = p->max_qsa;
+    A.p_init = s->d_pinit;
+    A.nbg = s->nbg;
+    A.bg_p = s->d_bg;
+    A.neutralize = p->neutralize;
+    A.ps = s->d_ps;
+    A.ngp = p->ngp;
+    A.counters = s->d_cnt;
+    A.timing = nullptr;
+    A.q_global = s->d_q;
+    A.dbuf = kLayouts[lay][0];
+    A.opT_smem = kLayouts[lay][1];
+    A.q_smem = kLayouts[lay][2];
+    *out = s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_destroy(qz_sweep* s) {
+    delete s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
+                                  void* stream) {
+    if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    qzb::SweepArgs A = s->base;
+    A.bsrc = bsrc;
+    A.fld = fld;
+    A.diag = diag;
+    QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
+    if (s->timing) {
+        QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 8, st));
+        A.timing = s->d_tim;
+    }
+    QZ_CUDA(qzb::launch_sweep_m0(A, st));
+    if (cnt) {
+        unsigned long long h[4];
+        QZ_CUDA(cudaMemcpyAsync(h, s->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+        QZ_CUDA(cudaStreamSynchronize(st));
+        cnt->lost += h[0];
+    }
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_plasma(qz_sweep* s, double* out, int cap, int* n) {
+    if (!s || !out || !n) return fail(QZ_ERR_ARG, "qz_sweep_plasma: null pointer");
+    *n = s->np;
+    if (cap < s->np) return fail(QZ_ERR_SIZE, "qz_sweep_plasma: capacity too small");
+    for (int v = 0; v < 6; ++v)
+        QZ_CUDA(cudaMemcpy(out + (size_t)v * s->np, s->d_ps + (size_t)v * s->npad, sizeof(double) * s->np,
+                           cudaMemcpyDeviceToHost));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_timing(qz_sweep* s, int enable, unsigned long long* cycles6) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sweep_timing: null pointer");
+    if (cycles6) QZ_CUDA(cudaMemcpy(cycles6, s->d_tim, sizeof(unsigned long long) * 6, cudaMemcpyDeviceToHost));
+    s->timing = enable != 0;
+    return QZ_OK;
+}
+
+// ===================================================================== beams
+namespace {
+
+qzb::BeamArgs beam_args(const qz_grid* g, const qz_beam_view* b, const qz_box* box) {
+    qzb::BeamArgs B{};
+    B.x = b->x; B.y = b->y; B.px = b->px; B.py = b->py; B.pz = b->pz; B.xi = b->xi; B.w = b->w;
+    B.n = (long)b->n;
+    B.q = b->q;
+    B.m = b->m;
+    B.M = g->M;
+    B.N = g->N;
+    B.R = g->R;
+    B.r = g->d_r;
+    B.inv_h = g->d_inv_h;
+    B.inv_V = g->d_inv_V;
+    B.xi_min = box->xi_min;
+    B.dxi = box->dxi;
+    B.idxi = 1.0 / box->dxi;
+    B.K = box->K;
+    B.ngp = box->ngp;
+    B.modes = box->modes;
+    return B;
+}
+
+qz_status check_beam(const qz_grid* g, const qz_beam_view* b, const qz_box* box) {
+    if (!g || !b || !box) return fail(QZ_ERR_ARG, "beam: null pointer");
+    if (b->n > 0 && (!b->x || !b->y || !b->px || !b->py || !b->pz || !b->xi || !b->w))
+        return fail(QZ_ERR_ARG, "beam: null column");
+    if (box->K < 2 || !(box->dxi > 0)) return fail(QZ_ERR_ARG, "beam: box needs K >= 2 and dxi > 0");
+    if (box->modes != 0 && box->modes != 1) return fail(QZ_ERR_ARG, "beam: modes must be 0 or 1");
+    return QZ_OK;
+}
+
+}  // namespace
+
+extern "C" qz_status qz_beam_deposit(const qz_grid* g, const qz_beam_view* b, const qz_box* box, double* bsrc,
+                                     void* stream) {
+    if (qz_status st = check_beam(g, b, box)) return st;
+    if (!bsrc) return fail(QZ_ERR_ARG, "qz_beam_deposit: null bsrc");
+    QZ_CUDA(qzb::launch_beam_deposit(beam_args(g, b, box), bsrc, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_beam_advance(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld,
+                                     double dt_kick, double dt_drift, int move, void* stream) {
+    if (qz_status st = check_beam(g, b, box)) return st;
+    if (!fld) return fail(QZ_ERR_ARG, "qz_beam_advance: null fld");
+    QZ_CUDA(qzb::launch_beam_push(beam_args(g, b, box), fld, dt_kick, dt_drift, move, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_beam_push(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld,
+                                  double dt_kick, double dt_drift, int* started, void* stream) {
+    if (qz_status st = check_beam(g, b, box)) return st;
+    if (!fld || !started) return fail(QZ_ERR_ARG, "qz_beam_push: null pointer");
+    const qzb::BeamArgs B = beam_args(g, b, box);
+    if (!*started) {
+        QZ_CUDA(qzb::launch_beam_push(B, fld, -0.5 * dt_kick, -0.5 * dt_kick, 0, (cudaStream_t)stream));
+        *started = 1;
+    }
+    QZ_CUDA(qzb::launch_beam_push(B, fld, dt_kick, dt_drift, 1, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_beam_push_deposit(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld,
+                                          double dt_kick, double dt_drift, int* started, double* bsrc_next,
+                                          void* stream) {
+    if (qz_status st = check_beam(g, b, box)) return st;
+    if (!fld || !started || !bsrc_next) return fail(QZ_ERR_ARG, "qz_beam_push_deposit: null pointer");
+    const qzb::BeamArgs B = beam_args(g, b, box);
+    if (!*started) {
+        QZ_CUDA(qzb::launch_beam_push(B, fld, -0.5 * dt_kick, -0.5 * dt_kick, 0, (cudaStream_t)stream));
+        *started = 1;
+    }
+    QZ_CUDA(qzb::launch_beam_push_deposit(B, fld, dt_kick, dt_drift, bsrc_next, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+namespace {
+// partial-sum scratch of qz_beam_sums, per device, grown on demand
+double* g_sum_scratch = nullptr;
+int g_sum_blocks = 0;
+}  // namespace
+
+extern "C" qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17, void* stream) {
+    if (!b || !out17) return fail(QZ_ERR_ARG, "qz_beam_sums: null pointer");
+    qzb::BeamArgs B{};
+    B.x = b->x; B.y = b->y; B.px = b->px; B.py = b->py; B.pz = b->pz; B.xi = b->xi; B.w = b->w;
+    B.n = (long)b->n;
+    const int nb = qzb::beam_sums_blocks(B.n);
+    if (nb > g_sum_blocks) {
+        if (g_sum_scratch) cudaFree(g_sum_scratch);
+        g_sum_scratch = nullptr;
+        g_sum_blocks = 0;
+        QZ_CUDA(cudaMalloc((void**)&g_sum_scratch, sizeof(double) * 17 * nb));
+        g_sum_blocks = nb;
+    }
+    QZ_CUDA(qzb::launch_beam_sums(B, gref, xiref, g_sum_scratch, nb, out17, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sample_gaussian(double n0, double sr, double xi0, double sxi, double gamma0, double espread,
+                                        double emit, double cut, double cx0, double cy0, double cxs, double cys,
+                                        double xp0, double yp0, int64_t np, int nrot, int mirror, uint64_t seed,
+                                        double xcut, double* out, double* gref, double* xiref, int64_t* n) {
+    // src/Beam.cpp:483-570, with the same standard-library generators
+    if (!out || !gref || !xiref || !n) return fail(QZ_ERR_ARG, "qz_sample_gaussian: null pointer");
+    const bool flat = !(sxi > 0);
+    const double len = flat ? -sxi : 0.0;
+    const int nsym = nrot * (mirror ? 2 : 1);
+    if (nrot < 1 || np % nsym != 0) return fail(QZ_ERR_ARG, "nparticles must be a multiple of nsym (x2 with mirror_y)");
+    const double Pr = 1.0 - std::exp(-0.5 * cut * cut);
+    auto Phi = [](double x) { return 0.5 * (1.0 + std::erf(x / std::sqrt(2.0))); };
+    double wtot;
+    if (!flat) {
+        const double lo = std::max(-cut, (xcut - xi0) / sxi);
+        if (lo >= cut) return fail(QZ_ERR_ARG, "xi_cut_head removes the whole beam");
+        wtot = n0 * std::pow(2 * PI, 1.5) * sr * sr * sxi * Pr * (Phi(cut) - Phi(lo));
+    } else {
+        const double lo = std::max(xi0 - 0.5 * len, xcut), hi = xi0 + 0.5 * len;
+        if (lo >= hi) return fail(QZ_ERR_ARG, "xi_cut_head removes the whole beam");
+        wtot = n0 * 2 * PI * sr * sr * Pr * (hi - lo);
+    }
+    const double wmac = wtot / np;
+    std::mt19937_64 rng(seed);
+    std::normal_distribution<double> N01(0.0, 1.0);
+    std::uniform_real_distribution<double> U01(0.0, 1.0);
+    const double spx = (sr > 0) ? emit / sr : 0.0;
+    double aw = 0, awg = 0, awxi = 0;
+    int64_t cnt = 0;
+    for (int64_t i0 = 0; i0 < np; i0 += nsym) {
+        double x, y;
+        do { x = sr * N01(rng); y = sr * N01(rng); } while (x * x + y * y > cut * cut * sr * sr);
+        double xi;
+        do {
+            if (!flat) { do { xi = N01(rng); } while (std::abs(xi) > cut); xi = xi0 + sxi * xi; }
+            else xi = xi0 + len * (U01(rng) - 0.5);
+        } while (xi < xcut);
+        double px = spx * N01(rng), py = spx * N01(rng);
+        const double gam = gamma0 * (1.0 + espread * N01(rng));
+        px += gam * xp0;
+        py += gam * yp0;
+        const double pz2 = gam * gam - 1.0 - px * px - py * py;
+        if (pz2 <= 0) return fail(QZ_ERR_ARG, "gamma too small for the transverse momentum spread");
+        const double tpx = px - gam * xp0, tpy = py - gam * yp0;
+        for (int l = 0; l < nsym; ++l) {
+            const int lr = l % nrot;
+            const double sgn = (l >= nrot) ? -1.0 : 1.0;
+            const double ph = 2 * PI * lr / nrot, cp = std::cos(ph), sp = std::sin(ph);
+            double* q = out + 7 * cnt;
+            q[0] = cp * x - sp * y + cx0 + cxs * (xi - xi0);
+            q[1] = sgn * (sp * x + cp * y) + cy0 + cys * (xi - xi0);
+            q[2] = cp * tpx - sp * tpy + gam * xp0;
+            q[3] = sgn * (sp * tpx + cp * tpy) + gam * yp0;
+            q[4] = std::sqrt(pz2);
+            q[5] = xi;
+            q[6] = wmac;
+            if (q[6] != 0) {
+                const double g = std::sqrt(1 + q[2] * q[2] + q[3] * q[3] + q[4] * q[4]);
+                aw += q[6];
+                awg += q[6] * g;
+                awxi += q[6] * q[5];
+            }
+            ++cnt;
+        }
+    }
+    *gref = 0;
+    *xiref = 0;
+    if (aw > 0) { *gref = awg / aw; *xiref = awxi / aw; }
+    *n = cnt;
+    return QZ_OK;
+}
+
+// ===================================================================== time steps
+struct qz_sim {
+    const qz_grid* g = nullptr;
+    qz_sweep* sw = nullptr;
+    qz_sweep_params p{};
+    int fnc = 6, bnc = 5, dnc = 3;
+    double *d_fld = nullptr, *d_diag = nullptr, *d_bsrc[2] = {nullptr, nullptr}, *d_mom = nullptr;
+    int cur = 0;
+    bool bsrc_valid = false;
+    struct Beam {
+        double* d = nullptr;     // 7 columns of n
+        int64_t n = 0;
+        double q = -1, m = 1, gref = 0, xiref = 0;
+        int rigid = 0, started = 0;
+        qz_beam_view view() const {
+            qz_beam_view v;
+            v.x = d; v.y = d + n; v.px = d + 2 * n; v.py = d + 3 * n; v.pz = d + 4 * n; v.xi = d + 5 * n; v.w = d + 6 * n;
+            v.n = n; v.q = q; v.m = m;
+            return v;
+        }
+    };
+    std::vector<Beam> beams;
+    qz_counters cnt{};
+    ~qz_sim() {
+        for (auto& b : beams)
+            if (b.d) cudaFree(b.d);
+        for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom})
+            if (q) cudaFree(q);
+        qz_sweep_destroy(sw);
+    }
+};
+
+extern "C" qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, qz_sim** out) {
+    if (!g || !p || !out) return fail(QZ_ERR_ARG, "qz_sim_create: null pointer");
+    *out = nullptr;
+    qz_sim* s = new (std::nothrow) qz_sim;
+    if (!s) return fail(QZ_ERR_NOMEM, "qz_sim_create: out of host memory");
+    s->g = g;
+    s->p = *p;
+    if (qz_status st = qz_sweep_create(g, p, &s->sw)) { delete s; return st; }
+    s->fnc = p->modes ? 18 : 6;
+    s->bnc = p->modes ? 15 : 5;
+    s->dnc = p->modes ? 9 : 3;
+    const size_t KM = (size_t)p->K * g->M;
+    if (cudaMalloc((void**)&s->d_fld, sizeof(double) * KM * s->fnc) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_diag, sizeof(double) * KM * s->dnc) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_bsrc[0], sizeof(double) * KM * s->bnc) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_bsrc[1], sizeof(double) * KM * s->bnc) != cudaSuccess) {
+        delete s;
+        return fail(QZ_ERR_NOMEM, "qz_sim_create: device allocation failed");
+    }
+    *out = s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_destroy(qz_sim* s) {
+    delete s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_add_beam(qz_sim* s, const double* p7, int64_t n, double q, double m, int rigid,
+                                     double gref, double xiref) {
+    if (!s || (n > 0 && !p7) || n < 0) return fail(QZ_ERR_ARG, "qz_sim_add_beam: bad argument");
+    qz_sim::Beam b;
+    b.n = n; b.q = q; b.m = m; b.rigid = rigid; b.gref = gref; b.xiref = xiref;
+    std::vector<double> cols((size_t)7 * (n > 0 ? n : 1), 0.0);
+    for (int64_t i = 0; i < n; ++i)
+        for (int c = 0; c < 7; ++c) cols[(size_t)c * n + i] = p7[7 * i + c];
+    if (qz_status st = dev_upload(&b.d, cols)) return st;
+    s->beams.push_back(b);
+    const int nb = (int)s->beams.size();
+    if (s->d_mom) cudaFree(s->d_mom);
+    s->d_mom = nullptr;
+    QZ_CUDA(cudaMalloc((void**)&s->d_mom, sizeof(double) * 17 * nb));
+    s->bsrc_valid = false;
+    return QZ_OK;
+}
+
+namespace {
+qz_box sim_box(const qz_sim* s) {
+    qz_box box;
+    box.xi_min = s->p.xi_min;
+    box.dxi = s->p.dxi;
+    box.K = s->p.K;
+    box.ngp = s->p.ngp;
+    box.modes = s->p.modes;
+    return box;
+}
+}  // namespace
+
+extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_host, void* stream) {
+    if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t KMb = (size_t)s->p.K * s->g->M * s->bnc;
+    const qz_box box = sim_box(s);
+    const int nb = (int)s->beams.size();
+    if (!s->bsrc_valid) {
+        QZ_CUDA(cudaMemsetAsync(s->d_bsrc[s->cur], 0, sizeof(double) * KMb, st));
+        for (auto& b : s->beams) {
+            const qz_beam_view v = b.view();
+            if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[s->cur], stream)) return e;
+        }
+        s->bsrc_valid = true;
+    }
+    double dt_prev = dt;
+    for (int n = 0; n <= nsteps; ++n) {
+        if (qz_status e = qz_sweep_run(s->sw, s->d_bsrc[s->cur], s->d_fld, s->d_diag, nullptr, stream)) return e;
+        if (mom_host) {
+            for (int b = 0; b < nb; ++b) {
+                const qz_beam_view v = s->beams[b].view();
+                if (qz_status e = qz_beam_sums(&v, s->beams[b].gref, s->beams[b].xiref, s->d_mom + 17 * b, stream))
+                    return e;
+            }
+            QZ_CUDA(cudaMemcpyAsync(mom_host + (size_t)n * nb * 17, s->d_mom, sizeof(double) * 17 * nb,
+                                    cudaMemcpyDeviceToHost, st));
+        }
+        if (n < nsteps) {
+            const double dkick = 0.5 * (dt_prev + dt), ddrift = dt;
+            const int nxt = 1 - s->cur;
+            QZ_CUDA(cudaMemsetAsync(s->d_bsrc[nxt], 0, sizeof(double) * KMb, st));
+            for (auto& b : s->beams) {
+                qz_beam_view v = b.view();
+                if (b.rigid) {
+                    if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[nxt], stream)) return e;
+                } else {
+                    if (qz_status e = qz_beam_push_deposit(s->g, &v, &box, s->d_fld, dkick, ddrift, &b.started,
+                                                           s->d_bsrc[nxt], stream))
+                        return e;
+                }
+            }
+            s->cur = nxt;
+            dt_prev = dt;
+        }
+    }
+    unsigned long long h[4];
+    QZ_CUDA(cudaMemcpyAsync(h, s->sw->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+    QZ_CUDA(cudaStreamSynchronize(st));
+    s->cnt.lost += h[0];
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_fields(qz_sim* s, double* fld, double* diag) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sim_fields: null pointer");
+    const size_t KM = (size_t)s->p.K * s->g->M;
+    if (fld) QZ_CUDA(cudaMemcpy(fld, s->d_fld, sizeof(double) * KM * s->fnc, cudaMemcpyDeviceToHost));
+    if (diag) QZ_CUDA(cudaMemcpy(diag, s->d_diag, sizeof(double) * KM * s->dnc, cudaMemcpyDeviceToHost));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_beam(qz_sim* s, int b, double* p7) {
+    if (!s || !p7 || b < 0 || b >= (int)s->beams.size()) return fail(QZ_ERR_ARG, "qz_sim_beam: bad argument");
+    const auto& B = s->beams[b];
+    std::vector<double> cols((size_t)7 * B.n);
+    if (B.n > 0) QZ_CUDA(cudaMemcpy(cols.data(), B.d, sizeof(double) * cols.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < B.n; ++i)
+        for (int c = 0; c < 7; ++c) p7[7 * i + c] = cols[(size_t)c * B.n + i];
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_counters(qz_sim* s, qz_counters* out) {
+    if (!s || !out) return fail(QZ_ERR_ARG, "qz_sim_counters: null pointer");
+    *out = s->cnt;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_kick, double dt_drift, int push,
+                                      double* mom_host, void* stream) {
+    if (!s || (!s->beams.empty() && !cols)) return fail(QZ_ERR_ARG, "qz_sim_step_host: null pointer");
+    cudaStream_t st = (cudaStream_t)stream;
+    const size_t KMb = (size_t)s->p.K * s->g->M * s->bnc;
+    const qz_box box = sim_box(s);
+    const int nb = (int)s->beams.size();
+    for (int b = 0; b < nb; ++b) {
+        if (!cols[b]) return fail(QZ_ERR_ARG, "qz_sim_step_host: null beam buffer");
+        QZ_CUDA(cudaMemcpyAsync(s->beams[b].d, cols[b], sizeof(double) * 7 * s->beams[b].n, cudaMemcpyHostToDevice,
+                                st));
+    }
+    QZ_CUDA(cudaMemsetAsync(s->d_bsrc[s->cur], 0, sizeof(double) * KMb, st));
+    for (auto& b : s->beams) {
+        const qz_beam_view v = b.view();
+        if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[s->cur], stream)) return e;
+    }
+    if (qz_status e = qz_sweep_run(s->sw, s->d_bsrc[s->cur], s->d_fld, s->d_diag, nullptr, stream)) return e;
+    for (int b = 0; b < nb; ++b) {
+        const qz_beam_view v = s->beams[b].view();
+        if (qz_status e = qz_beam_sums(&v, s->beams[b].gref, s->beams[b].xiref, s->d_mom + 17 * b, stream)) return e;
+    }
+    if (push)
+        for (auto& b : s->beams) {
+            if (b.rigid) continue;
+            qz_beam_view v = b.view();
+            if (qz_status e = qz_beam_push(s->g, &v, &box, s->d_fld, dt_kick, dt_drift, &b.started, stream)) return e;
+        }
+    for (int b = 0; b < nb; ++b)
+        QZ_CUDA(cudaMemcpyAsync(cols[b], s->beams[b].d, sizeof(double) * 7 * s->beams[b].n, cudaMemcpyDeviceToHost,
+                                st));
+    if (mom_host && nb > 0)
+        QZ_CUDA(cudaMemcpyAsync(mom_host, s->d_mom, sizeof(double) * 17 * nb, cudaMemcpyDeviceToHost, st));
+    QZ_CUDA(cudaStreamSynchronize(st));
+    s->bsrc_valid = false;
+    return QZ_OK;
+}

@@ -1,0 +1,40 @@
+"""Generates the validation fixtures of tests/golden from the reference checkout (run once, in the
+container that has it):  python tests/golden/make_validation_fixtures.py /root/reference
+
+  validation_numbers.json  printed results of validation/reference_full.txt and reference_quick.txt
+                           for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain)
+  decks/*.in               the validation decks those numbers come from (blowout, gain, betatron, linear)
+"""
+import json
+import os
+import re
+import shutil
+import sys
+
+ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+here = os.path.dirname(os.path.abspath(__file__))
+out = {}
+for tag, fn in (("full", "reference_full.txt"), ("quick", "reference_quick.txt")):
+    for line in open(os.path.join(ref, "validation", fn)):
+        m = re.match(r"(uniform_dr0\.01_dxi0\.01|stretched_dxi0\.005|stretched_dxi0\.005_PCR)\s+Ez\(-5\)=(\S+) "
+                     r"Ez\(-7\)=(\S+) Ez\(-8\)=(\S+) Ezmin=(\S+) @xi=(\S+)\s+Wr/r\(r=\.5,xi=-6\)=(\S+)", line)
+        if m:
+            out["blowout_" + m.group(1)] = dict(zip(["Ez(-5)", "Ez(-7)", "Ez(-8)", "Ezmin", "xi_min", "Wr/r"],
+                                                    m.groups()[1:]))
+        m = re.match(r"max \|r_rms - r0 \|cos\(w_b t\)\|\| / r0 = (\S+)", line)
+        if m:
+            out["betatron_" + tag] = m.group(1)
+        m = re.match(r"d<gamma>/dt = (\S+)", line)
+        if m:
+            out["gain_" + tag] = m.group(1)
+        m = re.match(r"(uniform dr=0\.01|stretched 0\.002 -> 0\.05)\s*: max\|Ez\|=(\S+)\s+rel\.err Ez\(r=0\)=(\S+)\s+"
+                     r"psi\(0\)=(\S+)\s+\(Er-Bth\)\(r=0\.5\)=(\S+)", line)
+        if m:
+            out["linear_" + m.group(1).split()[0] + "_" + tag] = dict(
+                zip(["max|Ez|", "rel.err Ez(r=0)", "psi(0)", "(Er-Bth)(r=0.5)"], m.groups()[1:]))
+with open(os.path.join(here, "validation_numbers.json"), "w") as f:
+    json.dump(out, f, indent=1, sort_keys=True)
+os.makedirs(os.path.join(here, "decks"), exist_ok=True)
+for d in ("blowout.in", "gain.in", "betatron.in", "linear.in"):
+    shutil.copy(os.path.join(ref, "validation", d), os.path.join(here, "decks", d))
+print(json.dumps(out, indent=1, sort_keys=True))
