@@ -94,9 +94,10 @@ qz_status qz_sweep_run(qz_sweep* s, const double* bsrc_dev, double* fld_dev, dou
                        qz_counters* counters_host, void* stream);
 /* plasma state after the last sweep: out_host (6, n) = x y px py Delta w; returns n in *n */
 qz_status qz_sweep_plasma(qz_sweep* s, double* out_host, int cap, int* n);
-/* per-phase clock cycles of the last run (6 values: prologue, deposit, psi/E_z/B_z, S, B+, store+push);
-   enable = 1 turns the counters on for later runs */
-qz_status qz_sweep_timing(qz_sweep* s, int enable, unsigned long long* cycles6_host);
+/* per-phase clock cycles of the last run, 16 counters: [0] prologue, [1] psi/E_z/B_z phase, [2] S+ deposit,
+   [3] B+ phase, [4] store + push + deposit, [5..8] parts of phase 1; enable = 1 turns the counters on for
+   later runs */
+qz_status qz_sweep_timing(qz_sweep* s, int enable, unsigned long long* cycles16_host);
 
 /* ------------------------------------------------------------------ beams
  * A beam is a view of 7 device columns (x y px py pz xi w), internal xi.

@@ -118,7 +118,7 @@ class Sweep:
         return out[: 6 * n.value].reshape(6, n.value)
 
     def timing(self, enable: bool = True) -> np.ndarray:
-        cyc = (C.c_ulonglong * 6)()
+        cyc = (C.c_ulonglong * 16)()
         check(lib().qz_sweep_timing(self.h, 1 if enable else 0, cyc))
         return np.array(list(cyc), dtype=np.float64)
 

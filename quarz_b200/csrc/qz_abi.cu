@@ -45,18 +45,17 @@ qz_status dev_upload(T** dst, const std::vector<T>& src) {
 
 // ===================================================================== grid
 struct qz_grid {
-    int M = 0, N = 0, C = 0;
+    int M = 0, N = 0;
     double R = 0;
     std::vector<double> r, h, rmid, V, inv_h, inv_V;
     std::vector<double> opa[4], opb[4], opc[4];
     double flux_coef = 0;
     std::vector<double> gm, g0, gp, ir;
+    std::vector<double> consts;  // per-node constants of the sweep (13 x M)
     // device
-    double *d_r = nullptr, *d_inv_h = nullptr, *d_inv_V = nullptr;
-    double *d_gm = nullptr, *d_g0 = nullptr, *d_gp = nullptr, *d_ir = nullptr;
-    double* d_opT = nullptr;     // L0, L1D, L1F, L2D rows chunk-transposed, [4][3][32*C]
+    double *d_r = nullptr, *d_inv_h = nullptr, *d_inv_V = nullptr, *d_consts = nullptr;
     ~qz_grid() {
-        for (double* p : {d_r, d_inv_h, d_inv_V, d_gm, d_g0, d_gp, d_ir, d_opT})
+        for (double* p : {d_r, d_inv_h, d_inv_V, d_consts})
             if (p) cudaFree(p);
     }
 };
@@ -79,12 +78,6 @@ void fv_rows(const qz_grid& g, int n, std::vector<double>& a, std::vector<double
     }
 }
 
-int chunk_rows(int M) {
-    int C = (M + 31) / 32;
-    if (C < 2) C = 2;
-    if ((C & 1) == 0) ++C;    // odd stride: lanes of a warp hit distinct shared-memory banks
-    return C;
-}
 
 }  // namespace
 
@@ -164,26 +157,28 @@ extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
     }
     for (int j = 1; j <= N; ++j) g->ir[j] = 1.0 / g->r[j];
     g->ir[0] = 1.0 / g->r[1];
-    // chunk-transposed operator rows for the warp solver: row i = lane*C + ii at [ii*32 + lane];
-    // rows beyond M are identity rows
-    g->C = chunk_rows(M);
-    const int C = g->C;
-    std::vector<double> opT((size_t)4 * 3 * 32 * C, 0.0);
-    for (int op = 0; op < 4; ++op)
-        for (int lane = 0; lane < 32; ++lane)
-            for (int ii = 0; ii < C; ++ii) {
-                const int i = lane * C + ii;
-                const size_t t = (size_t)ii * 32 + lane;
-                double* base = opT.data() + (size_t)op * 3 * 32 * C;
-                base[t] = i < M ? g->opa[op][i] : 0.0;
-                base[32 * C + t] = i < M ? g->opb[op][i] : 1.0;
-                base[64 * C + t] = i < M ? g->opc[op][i] : 0.0;
-            }
+    // per-node constants of the sweep: stencils, 1/r, L0 Thomas factors, L1D and L1F rows
+    {
+        std::vector<double> cs((size_t)13 * M, 0.0);
+        auto put = [&](int k, const std::vector<double>& v) { std::copy(v.begin(), v.end(), cs.begin() + (size_t)k * M); };
+        put(0, g->gm); put(1, g->g0); put(2, g->gp); put(3, g->ir);
+        // Thomas on L0 with its Dirichlet row N (src/Tridiag.cpp:445-459): u_i = b_i - a_i c_{i-1}/u_{i-1}
+        const std::vector<double>&a0 = g->opa[0], &b0 = g->opb[0], &c0 = g->opc[0];
+        double cp = 0.0;
+        for (int i = 0; i < M; ++i) {
+            const double rr = 1.0 / (b0[i] - (i > 0 ? a0[i] * cp : 0.0));
+            cp = c0[i] * rr;
+            cs[(size_t)4 * M + i] = rr;
+            cs[(size_t)5 * M + i] = -rr * a0[i];
+            cs[(size_t)6 * M + i] = -cp;
+        }
+        put(7, g->opa[1]); put(8, g->opb[1]); put(9, g->opc[1]);
+        put(10, g->opa[2]); put(11, g->opb[2]); put(12, g->opc[2]);
+        g->consts = cs;
+    }
     qz_status st;
     if ((st = dev_upload(&g->d_r, g->r)) || (st = dev_upload(&g->d_inv_h, g->inv_h)) ||
-        (st = dev_upload(&g->d_inv_V, g->inv_V)) || (st = dev_upload(&g->d_gm, g->gm)) ||
-        (st = dev_upload(&g->d_g0, g->g0)) || (st = dev_upload(&g->d_gp, g->gp)) ||
-        (st = dev_upload(&g->d_ir, g->ir)) || (st = dev_upload(&g->d_opT, opT))) {
+        (st = dev_upload(&g->d_inv_V, g->inv_V)) || (st = dev_upload(&g->d_consts, g->consts))) {
         delete g;
         return st;
     }
@@ -219,13 +214,12 @@ struct qz_sweep {
     double* d_pinit = nullptr;
     double* d_bg = nullptr;
     double* d_ps = nullptr;
-    double* d_q = nullptr;
     unsigned long long* d_cnt = nullptr;
     unsigned long long* d_tim = nullptr;
     bool timing = false;
     qzb::SweepArgs base{};
     ~qz_sweep() {
-        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_q, (void*)d_cnt, (void*)d_tim})
+        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_cnt, (void*)d_tim})
             if (q) cudaFree(q);
     }
 };
@@ -276,22 +270,17 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     int dev = 0, optin = 0;
     QZ_CUDA(cudaGetDevice(&dev));
     QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-    // shared-memory layout: the fastest that fits (double-buffered sources, operator rows, solver
-    // scratch in shared memory), else move the solver scratch and the operator rows to global memory
-    static const bool kLayouts[5][3] = {{true, true, true}, {false, true, true}, {false, true, false},
-                                        {false, false, true}, {false, false, false}};
+    // shared-memory layout: the fastest that fits (double-buffered sources, constants in shared
+    // memory), else single-buffered sources and/or constants read from global memory
+    static const bool kLayouts[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
     int lay = -1;
-    for (int i = 0; i < 5 && lay < 0; ++i) {
-        if (qzb::sweep_m0_smem_bytes(M, g->C, kLayouts[i][0], kLayouts[i][1], kLayouts[i][2]) <= (size_t)optin)
-            lay = i;
-    }
-    const bool q_in_smem = lay >= 0 && kLayouts[lay][2];
-    const size_t smem = lay >= 0 ? qzb::sweep_m0_smem_bytes(M, g->C, kLayouts[lay][0], kLayouts[lay][1],
-                                                             kLayouts[lay][2])
-                                 : qzb::sweep_m0_smem_bytes(M, g->C, false, false, false);
-    if (lay < 0)
-        return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " needs " + std::to_string(smem) +
-                                     " B of shared memory, the device allows " + std::to_string(optin));
+    for (int i = 0; i < 4 && lay < 0; ++i)
+        if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1]) <= (size_t)optin) lay = i;
+    const int rpt = (M + qzb::kSweepThreads - 1) / qzb::kSweepThreads;
+    if (lay < 0 || rpt > 4)
+        return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " is too large for one CTA (" +
+                                     std::to_string(qzb::sweep_m0_smem_bytes(M, false, false)) + " B of shared memory, "
+                                     "the device allows " + std::to_string(optin) + ")");
     qz_sweep* s = new (std::nothrow) qz_sweep;
     if (!s) return fail(QZ_ERR_NOMEM, "qz_sweep_create: out of host memory");
     s->g = g;
@@ -337,8 +326,7 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     const size_t nps = (size_t)(6 + 5 * p->ab_order) * s->npad;
     if (cudaMalloc((void**)&s->d_ps, sizeof(double) * nps) != cudaSuccess ||
         cudaMalloc((void**)&s->d_cnt, sizeof(unsigned long long) * 4) != cudaSuccess ||
-        cudaMalloc((void**)&s->d_tim, sizeof(unsigned long long) * 8) != cudaSuccess ||
-        (!q_in_smem && cudaMalloc((void**)&s->d_q, sizeof(double) * 9 * 32 * (size_t)g->C) != cudaSuccess)) {
+        cudaMalloc((void**)&s->d_tim, sizeof(unsigned long long) * 16) != cudaSuccess) {
         delete s;
         return fail(QZ_ERR_NOMEM, "qz_sweep_create: device allocation failed");
     }
@@ -351,13 +339,12 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     A.M = M;
     A.N = g->N;
     A.K = p->K;
-    A.C = g->C;
+    A.rows_per_thread = rpt;
     A.R = g->R;
     A.dxi = p->dxi;
     A.idxi = 1.0 / p->dxi;
     A.r = g->d_r; A.inv_h = g->d_inv_h; A.inv_V = g->d_inv_V;
-    A.gm = g->d_gm; A.g0 = g->d_g0; A.gp = g->d_gp; A.ir = g->d_ir;
-    A.opT = g->d_opT;
+    A.consts = g->d_consts;
     A.flux_coef = g->flux_coef;
     A.np = s->np;
     A.npad = s->npad;
@@ -373,10 +360,8 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     A.ngp = p->ngp;
     A.counters = s->d_cnt;
     A.timing = nullptr;
-    A.q_global = s->d_q;
     A.dbuf = kLayouts[lay][0];
-    A.opT_smem = kLayouts[lay][1];
-    A.q_smem = kLayouts[lay][2];
+    A.const_smem = kLayouts[lay][1];
     *out = s;
     return QZ_OK;
 }
@@ -396,7 +381,7 @@ extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, 
     A.diag = diag;
     QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
     if (s->timing) {
-        QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 8, st));
+        QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 16, st));
         A.timing = s->d_tim;
     }
     QZ_CUDA(qzb::launch_sweep_m0(A, st));
@@ -421,7 +406,7 @@ extern "C" qz_status qz_sweep_plasma(qz_sweep* s, double* out, int cap, int* n) 
 
 extern "C" qz_status qz_sweep_timing(qz_sweep* s, int enable, unsigned long long* cycles6) {
     if (!s) return fail(QZ_ERR_ARG, "qz_sweep_timing: null pointer");
-    if (cycles6) QZ_CUDA(cudaMemcpy(cycles6, s->d_tim, sizeof(unsigned long long) * 6, cudaMemcpyDeviceToHost));
+    if (cycles6) QZ_CUDA(cudaMemcpy(cycles6, s->d_tim, sizeof(unsigned long long) * 16, cudaMemcpyDeviceToHost));
     s->timing = enable != 0;
     return QZ_OK;
 }

@@ -11,16 +11,15 @@ constexpr int kMaxSpecies = 4;
 
 // Everything the m = 0 sweep kernel reads or writes. Pointers are device pointers.
 struct SweepArgs {
-    int M, N, K, C;                 // nodes, cells, slices, solver rows per lane (odd)
+    int M, N, K;                    // nodes, cells, slices
+    int rows_per_thread;            // tridiagonal rows owned by one thread: ceil(M / kSweepThreads)
     double R, dxi, idxi;
     const double* r;                // nodes [M]
     const double* inv_h;            // 1/h [N]
     const double* inv_V;            // 1/V [M]
-    const double* gm;               // gradient stencils [M] (src/FieldSolver.cpp:157-176)
-    const double* g0;
-    const double* gp;
-    const double* ir;               // 1/r, axis 1/r_1
-    const double* opT;              // L0, L1D, L1F rows, chunk-transposed: [op][a|b|c][ii*32+lane]
+    // per-node constants, 13 arrays of M: gradient stencils gm g0 gp, 1/r (src/FieldSolver.cpp:157-176);
+    // L0 Thomas factors 1/u, -a/u, -c/u; rows a b c of L1D and of L1F (src/FieldSolver.cpp:117-156)
+    const double* consts;
     double flux_coef;               // coefficient of g in the flux row of L1F
     // mobile plasma species: particles [sp_off[s], sp_off[s+1])
     int nsp;
@@ -34,20 +33,18 @@ struct SweepArgs {
     int nbg;                        // immobile particles (background)
     const double* bg_p;             // (3, nbg): x, y, w*q
     int neutralize;
-    double* ps;                     // working state (6 + 5*ord, npad)
+    double* ps;                     // working state (6 + 5*ord, npad), used when np > kSweepThreads
     const double* bsrc;             // beam sources (K, M, 5)
     int ngp;
     double* fld;                    // (K, M, 6)
     double* diag;                   // (K, M, 3)
     unsigned long long* counters;   // [0] plasma particles removed
     unsigned long long* timing;     // optional: clock cycles per phase [6]
-    double* q_global;               // solver scratch in global memory (9*32*C) when shared memory is short
     int dbuf;                       // double-buffered slice sources (push fused with the next deposit)
-    int opT_smem;                   // operator rows copied into shared memory
-    int q_smem;                     // solver scratch in shared memory
+    int const_smem;                 // per-node constants copied into shared memory
 };
 
-size_t sweep_m0_smem_bytes(int M, int C, bool dbuf, bool opT_smem, bool q_smem);
+size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem);
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
 
 // Beam particles (SoA, device) and the box they live in.

@@ -5,18 +5,24 @@
 //   (psi, E_z, W+, B_z, deposit_S, B+) -> store_slice -> PlasmaSpecies::push
 // for azimuthal mode m = 0.
 //
-// Layout. All radial arrays of a slice (sources, fields, grid, stencils, operator rows) live in
-// shared memory. With at most kThreads plasma particles, thread p owns particle p and keeps its
-// state -- position, momentum, Delta, weight and the Adams-Bashforth history -- in registers for
-// the whole sweep; larger plasmas keep the state in a global scratch buffer instead.
+// Layout. The radial arrays of a slice (sources, fields, grid, stencils, operator rows) live in shared
+// memory (the constant ones fall back to global memory for very large grids). With at most 512
+// plasma particles, thread p owns particle p and keeps its state -- position, momentum, Delta,
+// weight and the Adams-Bashforth history -- in registers for the whole sweep; larger plasmas keep
+// the state in a global scratch buffer.
 //
-// Slice schedule (4 block barriers per slice when the sources are double-buffered):
-//   P2  warps 0-2: psi (+W+), E_z, B_z solves          | warps 3-15: sources of slice k+1 = beam + background
-//   P3  all: S+ deposit
-//   P4  warps 0-1: B_r, B_theta solves
-//   P5  all: store slice k; push k -> k+1 and deposit into the sources of slice k+1
-// Every tridiagonal system is solved by ONE warp (partition method: each lane eliminates a chunk of
-// C rows; the chunk couplings form a 32-unknown system solved by warp-shuffle cyclic reduction).
+// Tridiagonal solves. Every system is solved by all 512 threads at once: thread t owns rows
+// [t*R, t*R + R), and the three Thomas recurrences -- pivots u_i = b_i - a_i c_{i-1} / u_{i-1},
+// forward y_i = (d_i - a_i y_{i-1}) / u_i, backward x_i = y_i - (c_i / u_i) x_{i+1} -- are evaluated
+// as block-wide scans: pivots as normalised prefix products of 2x2 matrices, the substitutions as
+// scans of affine maps. Each scan costs five warp-shuffle levels and one block barrier. The psi,
+// E_z and B_z systems share the constant operator L0, whose pivots are computed once on the host.
+//
+// Slice schedule (4 phase barriers + 7 scan barriers per slice):
+//   P2  psi, E_z, B_z (two scans, three right-hand sides); sources of slice k+1 = beam + background
+//   P3  S+ deposit by the particles
+//   P4  B_r, B_theta (pivot scan + forward and backward scans of the two systems)
+//   P5  store slice k; push k -> k+1 and deposit into the sources of slice k+1
 #include "qz_device.cuh"
 #include "qz_internal.h"
 
@@ -25,83 +31,208 @@ namespace qzb {
 namespace {
 
 constexpr int kThreads = kSweepThreads;
+constexpr int kW = kThreads / 32;
+constexpr unsigned FULL = 0xffffffffu;
 
-// ---------------------------------------------------------------- warp-level tridiagonal solve
-// Rows come from `rows(ii, i, a, b, c, d)` for row i = lane*C + ii of the lane's chunk (rows i >= M
-// are identity rows). q: 3*32*C doubles of scratch, transposed [ii][lane]. x: result, by row.
-template <class Rows>
-__device__ __forceinline__ void warp_solve(const Rows& rows, const int C, const int M, double* __restrict__ q,
-                                           double* __restrict__ x) {
-    const int l = threadIdx.x & 31;
-    double* qa = q;
-    double* qc = q + 32 * C;
-    double* qd = q + 64 * C;
-    const int s = l * C;
-    double a0, b0, c0, d0;
-    rows(0, s, a0, b0, c0, d0);
-    double a, b, c, d;
-    rows(1, s + 1, a, b, c, d);
-    double rr = 1.0 / b;
-    double pa = a * rr, pc = c * rr, pd = d * rr;
-    qa[32 + l] = pa; qc[32 + l] = pc; qd[32 + l] = pd;
-    for (int ii = 2; ii < C; ++ii) {
-        rows(ii, s + ii, a, b, c, d);
-        rr = 1.0 / (b - a * pc);
-        pd = rr * (d - a * pd);
-        pa = -rr * a * pa;
-        pc = rr * c;
-        qa[ii * 32 + l] = pa; qc[ii * 32 + l] = pc; qd[ii * 32 + l] = pd;
-    }
-    const double Ba = pa, Bc = pc, Bd = pd;     // chunk-end row: x_e + Ba x_s + Bc x_{next s} = Bd
-    if (C >= 4) {
-        double na = qa[(C - 2) * 32 + l], nc = qc[(C - 2) * 32 + l], nd = qd[(C - 2) * 32 + l];
-        for (int ii = C - 3; ii >= 1; --ii) {
-            const double cn = qc[ii * 32 + l];
-            nd = qd[ii * 32 + l] - cn * nd;
-            na = qa[ii * 32 + l] - cn * na;
-            nc = -cn * nc;
-            qa[ii * 32 + l] = na; qc[ii * 32 + l] = nc; qd[ii * 32 + l] = nd;
+// ---------------------------------------------------------------- block scans
+// Shared scratch for the warp totals of one scan: 8 x kW doubles; two of them alternate.
+
+// exact power-of-two rescaling of a 2x2 matrix (its largest entry into [1, 2))
+__device__ __forceinline__ void renorm(double& m00, double& m01, double& m10, double& m11) {
+    const double mx = fmax(fmax(fabs(m00), fabs(m01)), fmax(fabs(m10), fabs(m11)));
+    if (!(mx > 0.0) || !(mx < 1e300)) return;
+    const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
+    const double s = __hiloint2double((1023 - e) << 20, 0);
+    m00 *= s; m01 *= s; m10 *= s; m11 *= s;
+}
+
+// Exclusive forward scan of the affine maps y -> a y + b (thread order = row order), applied to
+// y_{-1} = 0: yb[r] is y just before this thread's rows.
+template <int NR>
+__device__ __forceinline__ void scan_fwd(double a, const double (&b)[NR], double (&yb)[NR], double* tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double A = a, B[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) B[r] = b[r];
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+        const double Ap = __shfl_up_sync(FULL, A, st);
+        double Bp[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) Bp[r] = __shfl_up_sync(FULL, B[r], st);
+        if (lane >= st) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) B[r] = fma(A, Bp[r], B[r]);
+            A *= Ap;
         }
     }
-    double r1a, r1c, r1d;                        // row s+1 in terms of x_s and x_e
-    if (C >= 3) { r1a = qa[32 + l]; r1c = qc[32 + l]; r1d = qd[32 + l]; }
-    else { r1a = Ba; r1c = Bc; r1d = Bd; }
-    // chunk-start row: aA x_{prev e} + bA x_s + cA x_e = dA
-    const double aA = (l == 0) ? 0.0 : a0;
-    const double bA = b0 - c0 * r1a, cA = -c0 * r1c, dA = d0 - c0 * r1d;
-    // eliminate x_s of this lane and of the next lane from the chunk-end row: a system in x_e only
-    const unsigned FULL = 0xffffffffu;
-    const double aAn = __shfl_down_sync(FULL, aA, 1), bAn = __shfl_down_sync(FULL, bA, 1);
-    const double cAn = __shfl_down_sync(FULL, cA, 1), dAn = __shfl_down_sync(FULL, dA, 1);
-    const double u = Ba / bA;
-    const double v = (l < 31) ? Bc / bAn : 0.0;
-    double ea = -u * aA;
-    double eb = 1.0 - u * cA - (l < 31 ? v * aAn : 0.0);
-    double ec = (l < 31) ? -v * cAn : 0.0;
-    double ed = Bd - u * dA - (l < 31 ? v * dAn : 0.0);
+    if (lane == 31) {
+        tot[warp] = A;
 #pragma unroll
-    for (int st = 1; st < 32; st *= 2) {
-        const double al = __shfl_up_sync(FULL, ea, st), bl = __shfl_up_sync(FULL, eb, st);
-        const double cl = __shfl_up_sync(FULL, ec, st), dl = __shfl_up_sync(FULL, ed, st);
-        const double ah = __shfl_down_sync(FULL, ea, st), bh = __shfl_down_sync(FULL, eb, st);
-        const double ch = __shfl_down_sync(FULL, ec, st), dh = __shfl_down_sync(FULL, ed, st);
-        const bool lo = l - st >= 0, hi = l + st < 32;
-        const double alpha = lo ? -ea / bl : 0.0;
-        const double gamma = hi ? -ec / bh : 0.0;
-        const double na = lo ? alpha * al : 0.0;
-        const double nc = hi ? gamma * ch : 0.0;
-        const double nb = eb + (lo ? alpha * cl : 0.0) + (hi ? gamma * ah : 0.0);
-        const double nd = ed + (lo ? alpha * dl : 0.0) + (hi ? gamma * dh : 0.0);
-        ea = na; eb = nb; ec = nc; ed = nd;
+        for (int r = 0; r < NR; ++r) tot[kW * (1 + r) + warp] = B[r];
     }
-    const double xe = ed / eb;
-    const double xep = __shfl_up_sync(FULL, xe, 1);
-    const double xs = (dA - (l > 0 ? aA * xep : 0.0) - cA * xe) / bA;
-    if (s < M) x[s] = xs;
-    if (s + C - 1 < M) x[s + C - 1] = xe;
-    for (int ii = 1; ii < C - 1; ++ii) {
-        const int i = s + ii;
-        if (i < M) x[i] = qd[ii * 32 + l] - qa[ii * 32 + l] * xs - qc[ii * 32 + l] * xe;
+    double eA = __shfl_up_sync(FULL, A, 1), eB[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) eB[r] = __shfl_up_sync(FULL, B[r], 1);
+    if (lane == 0) {
+        eA = 1.0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) eB[r] = 0.0;
+    }
+    __syncthreads();
+    double ta = lane < kW ? tot[lane] : 1.0, tb[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) tb[r] = lane < kW ? tot[kW * (1 + r) + lane] : 0.0;
+#pragma unroll
+    for (int st = 1; st < kW; st <<= 1) {
+        const double ap = __shfl_up_sync(FULL, ta, st);
+        double bp[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) bp[r] = __shfl_up_sync(FULL, tb[r], st);
+        if (lane >= st) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) tb[r] = fma(ta, bp[r], tb[r]);
+            ta *= ap;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const double cw = __shfl_sync(FULL, tb[r], (warp + 31) & 31);
+        yb[r] = fma(eA, warp > 0 ? cw : 0.0, eB[r]);
+    }
+}
+
+// Exclusive backward scan of x -> a x + b applied to x_{end} = 0: xa[r] is x just after this
+// thread's rows.
+template <int NR>
+__device__ __forceinline__ void scan_bwd(double a, const double (&b)[NR], double (&xa)[NR], double* tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double A = a, B[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) B[r] = b[r];
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+        const double An = __shfl_down_sync(FULL, A, st);
+        double Bn[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) Bn[r] = __shfl_down_sync(FULL, B[r], st);
+        if (lane + st < 32) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) B[r] = fma(A, Bn[r], B[r]);
+            A *= An;
+        }
+    }
+    if (lane == 0) {
+        tot[warp] = A;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) tot[kW * (1 + r) + warp] = B[r];
+    }
+    double eA = __shfl_down_sync(FULL, A, 1), eB[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) eB[r] = __shfl_down_sync(FULL, B[r], 1);
+    if (lane == 31) {
+        eA = 1.0;
+#pragma unroll
+        for (int r = 0; r < NR; ++r) eB[r] = 0.0;
+    }
+    __syncthreads();
+    double ta = lane < kW ? tot[lane] : 1.0, tb[NR];
+#pragma unroll
+    for (int r = 0; r < NR; ++r) tb[r] = lane < kW ? tot[kW * (1 + r) + lane] : 0.0;
+#pragma unroll
+    for (int st = 1; st < kW; st <<= 1) {
+        const double an = __shfl_down_sync(FULL, ta, st);
+        double bn[NR];
+#pragma unroll
+        for (int r = 0; r < NR; ++r) bn[r] = __shfl_down_sync(FULL, tb[r], st);
+        if (lane + st < kW) {
+#pragma unroll
+            for (int r = 0; r < NR; ++r) tb[r] = fma(ta, bn[r], tb[r]);
+            ta *= an;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < NR; ++r) {
+        const double cw = __shfl_sync(FULL, tb[r], (warp + 1) & 31);
+        xa[r] = fma(eA, warp < kW - 1 ? cw : 0.0, eB[r]);
+    }
+}
+
+// Exclusive scan of 2x2 matrix products (later rows on the left) for NS systems: on return
+// (p[s], q[s]) = first column of the product of all matrices before this thread's rows.
+template <int NS>
+__device__ __forceinline__ void scan_pivots(double (&m)[NS][4], double (&p)[NS], double (&q)[NS], double* tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+#pragma unroll
+        for (int s = 0; s < NS; ++s) {
+            const double p00 = __shfl_up_sync(FULL, m[s][0], st), p01 = __shfl_up_sync(FULL, m[s][1], st);
+            const double p10 = __shfl_up_sync(FULL, m[s][2], st), p11 = __shfl_up_sync(FULL, m[s][3], st);
+            if (lane >= st) {
+                const double n00 = m[s][0] * p00 + m[s][1] * p10, n01 = m[s][0] * p01 + m[s][1] * p11;
+                const double n10 = m[s][2] * p00 + m[s][3] * p10, n11 = m[s][2] * p01 + m[s][3] * p11;
+                m[s][0] = n00; m[s][1] = n01; m[s][2] = n10; m[s][3] = n11;
+                renorm(m[s][0], m[s][1], m[s][2], m[s][3]);
+            }
+        }
+    }
+    if (lane == 31)
+#pragma unroll
+        for (int s = 0; s < NS; ++s)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) tot[kW * (4 * s + e) + warp] = m[s][e];
+    double ex[NS][4];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+#pragma unroll
+        for (int e = 0; e < 4; ++e) ex[s][e] = __shfl_up_sync(FULL, m[s][e], 1);
+    if (lane == 0)
+#pragma unroll
+        for (int s = 0; s < NS; ++s) { ex[s][0] = 1.0; ex[s][1] = 0.0; ex[s][2] = 0.0; ex[s][3] = 1.0; }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+        double t00 = lane < kW ? tot[kW * (4 * s) + lane] : 1.0, t01 = lane < kW ? tot[kW * (4 * s + 1) + lane] : 0.0;
+        double t10 = lane < kW ? tot[kW * (4 * s + 2) + lane] : 0.0, t11 = lane < kW ? tot[kW * (4 * s + 3) + lane] : 1.0;
+#pragma unroll
+        for (int st = 1; st < kW; st <<= 1) {
+            const double p00 = __shfl_up_sync(FULL, t00, st), p01 = __shfl_up_sync(FULL, t01, st);
+            const double p10 = __shfl_up_sync(FULL, t10, st), p11 = __shfl_up_sync(FULL, t11, st);
+            if (lane >= st) {
+                const double n00 = t00 * p00 + t01 * p10, n01 = t00 * p01 + t01 * p11;
+                const double n10 = t10 * p00 + t11 * p10, n11 = t10 * p01 + t11 * p11;
+                t00 = n00; t01 = n01; t10 = n10; t11 = n11;
+                renorm(t00, t01, t10, t11);
+            }
+        }
+        const int src = (warp + 31) & 31;
+        double c00 = __shfl_sync(FULL, t00, src), c10 = __shfl_sync(FULL, t10, src);
+        if (warp == 0) { c00 = 1.0; c10 = 0.0; }
+        // column 0 of (within-warp exclusive product) x (carry of the earlier warps)
+        p[s] = ex[s][0] * c00 + ex[s][1] * c10;
+        q[s] = ex[s][2] * c00 + ex[s][3] * c10;
+    }
+}
+
+// ---------------------------------------------------------------- batched shared-memory adds
+// All NA updates of one thread are issued together (independent compare-and-swap rounds) instead
+// of one serialised atomic loop per address. Lock-free: every round at least one contender of
+// each address succeeds, so the loop ends after at most one round per contender.
+template <int NA>
+__device__ __forceinline__ void add_multi(double* const (&p)[NA], const double (&v)[NA]) {
+    unsigned long long old[NA];
+#pragma unroll
+    for (int i = 0; i < NA; ++i) old[i] = __double_as_longlong(*reinterpret_cast<volatile double*>(p[i]));
+    unsigned pend = (1u << NA) - 1u;
+    for (int round = 0; pend && round < 4 * kThreads; ++round) {
+#pragma unroll
+        for (int i = 0; i < NA; ++i)
+            if (pend & (1u << i)) {
+                const unsigned long long nv = __double_as_longlong(__longlong_as_double(old[i]) + v[i]);
+                const unsigned long long got = atomicCAS(reinterpret_cast<unsigned long long*>(p[i]), old[i], nv);
+                if (got == old[i]) pend &= ~(1u << i); else old[i] = got;
+            }
     }
 }
 
@@ -112,29 +243,42 @@ struct Src {                                              // plasma + beam sourc
 
 struct Smem {
     double *r, *iv, *ih;                                  // grid
-    double *gm, *g0, *gp, *ir;                            // gradient stencils, 1/r
+    const double *gm, *g0, *gp, *ir;                      // gradient stencils, 1/r
+    const double *l0r, *l0f, *l0b;                        // L0 Thomas: 1/u, -a/u, -c/u
+    const double *l1a, *l1b, *l1c, *lfa, *lfb, *lfc;      // L1D and L1F rows
     double* src0;                                         // sources: 9 arrays, twice when A.dbuf
     double *bgt, *bgr;                                    // neutralising background
-    double *psi, *ez, *bz, *wr1, *bpr, *bpi;              // fields of the slice
-    const double* opT;                                    // operator rows (shared or global)
-    double* q;                                            // solver scratch (shared or global)
+    double *psi, *ez, *bz, *bpr, *bpi;                    // fields of the slice
+    double* tot;                                          // scan scratch, 2 x 8 x kW
     int* lost;
 };
 
 __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
-    const int M = A.M, C = A.C;
+    const int M = A.M;
     Smem S;
     double* p = base;
     S.r = p; p += M; S.iv = p; p += M; S.ih = p; p += M;
-    S.gm = p; p += M; S.g0 = p; p += M; S.gp = p; p += M; S.ir = p; p += M;
+    const double* q = A.const_smem ? p : A.consts;
+    S.gm = q; S.g0 = q + M; S.gp = q + 2 * M; S.ir = q + 3 * M;
+    S.l0r = q + 4 * M; S.l0f = q + 5 * M; S.l0b = q + 6 * M;
+    S.l1a = q + 7 * M; S.l1b = q + 8 * M; S.l1c = q + 9 * M;
+    S.lfa = q + 10 * M; S.lfb = q + 11 * M; S.lfc = q + 12 * M;
+    if (A.const_smem) p += 13 * (size_t)M;
     S.src0 = p;
     p += (A.dbuf ? 18 : 9) * (size_t)M;
     S.bgt = p; p += M; S.bgr = p; p += M;
-    S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.wr1 = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
-    if (A.opT_smem) { S.opT = p; p += 9 * 32 * C; } else { S.opT = A.opT; }
-    if (A.q_smem) { S.q = p; p += 9 * 32 * C; } else { S.q = A.q_global; }
+    S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
+    S.tot = p; p += 2 * 8 * kW;
     S.lost = reinterpret_cast<int*>(p);
     return S;
+}
+
+__device__ __forceinline__ Src src_of(const Smem& S, int M, int b) {
+    double* p = S.src0 + (size_t)b * 9 * M;
+    Src s;
+    s.rhot = p; s.drho = p + M; s.jz = p + 2 * M; s.chi = p + 3 * M; s.ne = p + 4 * M;
+    s.ni = p + 5 * M; s.jpi1 = p + 6 * M; s.S1r = p + 7 * M; s.S1i = p + 8 * M;
+    return s;
 }
 
 // beam source values of slice k at node j needed by the m = 0 sweep (src/Simulation.cpp:420-441):
@@ -164,15 +308,6 @@ __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, int k, int j) {
     return r;
 }
 
-// the 9 source arrays of buffer b
-__device__ __forceinline__ Src src_of(const Smem& S, int M, int b) {
-    double* p = S.src0 + (size_t)b * 9 * M;
-    Src s;
-    s.rhot = p; s.drho = p + M; s.jz = p + 2 * M; s.chi = p + 3 * M; s.ne = p + 4 * M;
-    s.ni = p + 5 * M; s.jpi1 = p + 6 * M; s.S1r = p + 7 * M; s.S1i = p + 8 * M;
-    return s;
-}
-
 // initial source values of a slice: background + beam; the plasma deposit is added on top
 __device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j, const BeamRow& br) {
     s.rhot[j] = S.bgt[j] + br.rt;
@@ -191,6 +326,22 @@ __device__ __forceinline__ double grad_at(const Smem& S, int N, const double* f,
     if (i == 0) return odd ? f[1] * S.ir[0] : 0.0;
     if (i == N) return S.g0[N] * f[N] + S.gm[N] * f[N - 1] + S.gp[N] * f[N - 2];
     return S.gm[i] * f[i - 1] + S.g0[i] * f[i] + S.gp[i] * f[i + 1];
+}
+
+// cell of x starting from a guess (the previous cell): walks for small moves, bisects otherwise;
+// the same cell as locate() (src/RadialGrid.hpp:73-82) for every x
+__device__ __forceinline__ int locate_from(const double* __restrict__ r, int N, double R, double x, int j) {
+    if (x <= 0.0) return 0;
+    if (x >= R) return N - 1;
+    j = j < 0 ? 0 : (j > N - 1 ? N - 1 : j);
+#pragma unroll 1
+    for (int step = 0; step < 3; ++step) {
+        if (r[j] > x) { if (j == 0) break; --j; continue; }
+        if (r[j + 1] <= x) { if (j == N - 1) break; ++j; continue; }
+        return j;
+    }
+    if (r[j] <= x && x < r[j + 1]) return j;
+    return locate(r, N, R, x);
 }
 
 // ---------------------------------------------------------------- one plasma particle
@@ -230,6 +381,11 @@ __device__ __forceinline__ void species_params(const SweepArgs& A, int p, double
     qm = A.sp_qm[s];
 }
 
+// W+ mode 1 at the particle: lin(w1) with w1 = -psi' (src/Simulation.cpp:477-498)
+__device__ __forceinline__ double w1_at(const Smem& S, int N, const PGeo& g) {
+    return g.W0 * (-grad_at(S, N, S.psi, g.j, false)) + g.W1 * (-grad_at(S, N, S.psi, g.j + 1, false));
+}
+
 // src/PlasmaSpecies.cpp:409-478, m = 0 (plasma rho and J_r feed nothing on this path: not deposited)
 template <int ORD>
 __device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGeo& g, const Src& s, const Smem& S) {
@@ -241,6 +397,8 @@ __device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGe
     const double ur = g.c * ux + g.s * uy, uth = g.c * uy - g.s * ux;
     const double wq = w * P.q;
     double* dens = (P.q < 0.0) ? s.ne : s.ni;
+    double* adr[12];
+    double val[12];
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         const int jj = g.j + cc;
@@ -251,21 +409,23 @@ __device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGe
         const double dr = wq * ur * dWc * iv;
         const double vjz = a * pz * invd, vchi = a * P.qm * invd;
         const double vn = w * Wc * iv * gam * invd;
-        atomicAdd(&s.rhot[jj], a);
-        atomicAdd(&s.drho[jj], dr);
-        atomicAdd(&s.jz[jj], vjz);
-        atomicAdd(&s.chi[jj], vchi);
-        atomicAdd(&dens[jj], vn);
-        atomicAdd(&s.jpi1[jj], a * uth);
+        adr[6 * cc + 0] = s.rhot + jj; val[6 * cc + 0] = a;
+        adr[6 * cc + 1] = s.drho + jj; val[6 * cc + 1] = dr;
+        adr[6 * cc + 2] = s.jz + jj;   val[6 * cc + 2] = vjz;
+        adr[6 * cc + 3] = s.chi + jj;  val[6 * cc + 3] = vchi;
+        adr[6 * cc + 4] = dens + jj;   val[6 * cc + 4] = vn;
+        adr[6 * cc + 5] = s.jpi1 + jj; val[6 * cc + 5] = a * uth;
     }
+    add_multi<12>(adr, val);
 }
 
 // src/PlasmaSpecies.cpp:508-559, m = 0
 template <int ORD>
-__device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PGeo& g, const Src& s, const Smem& S) {
+__device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PGeo& g, const Src& s, const Smem& S,
+                                                  int N) {
     const double qm = P.qm;
     const double PX = P.px, PY = P.py, D = P.dl;
-    const double r1 = lin(S.wr1, g);
+    const double r1 = w1_at(S, N, g);
     const double Wx = r1 * g.c - 0.0 * g.s, Wy = r1 * g.s + 0.0 * g.c;
     const double Ez = lin(S.ez, g), Bz = lin(S.bz, g);
     const double gam = (1.0 + PX * PX + PY * PY + D * D) / (2.0 * D);
@@ -276,6 +436,8 @@ __device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PG
     const double ax = (qm * (gam * Wx + PY * Bz) * invd) * invd - PX * dD * invd * invd;
     const double ay = (qm * (gam * Wy - PX * Bz) * invd) * invd - PY * dD * invd * invd;
     const double wq = P.w * P.q;
+    double* adr[4];
+    double val[4];
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         const int jj = g.j + cc;
@@ -288,9 +450,10 @@ __device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PG
         const double f2 = uth * Worc;
         Ar += f2 * uy;
         Ai -= f2 * ux;
-        atomicAdd(&s.S1r[jj], iv * (Ar * g.c + Ai * g.s));
-        atomicAdd(&s.S1i[jj], iv * (Ai * g.c - Ar * g.s));
+        adr[2 * cc] = s.S1r + jj;     val[2 * cc] = iv * (Ar * g.c + Ai * g.s);
+        adr[2 * cc + 1] = s.S1i + jj; val[2 * cc + 1] = iv * (Ai * g.c - Ar * g.s);
     }
+    add_multi<4>(adr, val);
 }
 
 // src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns false
@@ -300,7 +463,7 @@ __device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, con
                                               bool first) {
     const double qm = P.qm;
     const double X = P.x, Y = P.y, PX = P.px, PY = P.py, D = P.dl;
-    const double r1 = lin(S.wr1, g);
+    const double r1 = w1_at(S, A.N, g);
     const double Wx = r1 * g.c - 0.0 * g.s, Wy = r1 * g.s + 0.0 * g.c;
     const double Ez = lin(S.ez, g), Bz = lin(S.bz, g);
     const double br = lin(S.bpr, g), bi = lin(S.bpi, g);
@@ -363,18 +526,51 @@ __device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, con
     return true;
 }
 
+// right-hand sides of the psi, E_z, B_z systems at row i (src/Simulation.cpp:798-799, :517-527)
+__device__ __forceinline__ void rhs_l0(const Smem& S, const Src& s, int N, int i, double& d0, double& d1,
+                                       double& d2) {
+    d0 = d1 = d2 = 0.0;
+    if (i < N) {
+        d0 = -1.0 * s.rhot[i];
+        d1 = -1.0 * s.drho[i];
+        const double t1 = grad_at(S, N, s.jpi1, i, true);
+        const double t2 = (i == 0 ? s.jpi1[1] : s.jpi1[i]) * S.ir[i];
+        d2 = 1.0 * (-(t1 + t2));
+    }
+}
+
+// row i of (L1D - chi) (sys 0) and (L1F - chi) (sys 1) with its right-hand side
+// (src/FieldSolver.cpp:242-261, src/Simulation.cpp:535-591)
+__device__ __forceinline__ void row_b(const Smem& S, const Src& s, int N, double fc, int sys, int i, double& a,
+                                      double& b, double& cm, double& d) {
+    if (sys == 0) {
+        a = S.l1a[i]; b = S.l1b[i]; cm = i > 0 ? S.l1c[i - 1] : 0.0;
+        if (i >= 1 && i < N) { b = b - s.chi[i]; d = 1.0 * (-s.S1i[i]); } else { d = 0.0; }
+    } else {
+        a = S.lfa[i]; b = S.lfb[i]; cm = i > 0 ? S.lfc[i - 1] : 0.0;
+        if (i >= 1) {
+            b = b - s.chi[i];
+            d = 1.0 * (grad_at(S, N, s.jz, i, false) + s.S1r[i]);
+            if (i == N) d -= fc * s.jz[N];
+        } else {
+            d = 0.0;
+        }
+    }
+}
+
 }  // namespace
 
-template <int ORD, bool REG>
+template <int ORD, bool REG, int kMaxR>
 __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A) {
     extern __shared__ double smem_raw[];
-    const int M = A.M, N = A.N, K = A.K, C = A.C;
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int M = A.M, N = A.N, K = A.K, Rw = kMaxR == 1 ? 1 : A.rows_per_thread;   // rows per thread
+    const int tid = threadIdx.x;
     const Smem S = carve(smem_raw, A);
     const int np = A.np, npad = A.npad;
     const double R = A.R;
+    const int row0 = tid * Rw;                                  // this thread's rows [row0, row0 + Rw)
     unsigned long long* tim = A.timing;
-    long long t_prev = 0;
+    long long t_prev = 0, t_sub = 0;
     if (tim && tid == 0) t_prev = clock64();
 #define PHASE_MARK(ph)                                                        \
     do {                                                                      \
@@ -384,21 +580,28 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             t_prev = tn;                                                      \
         }                                                                     \
     } while (0)
+#define SUB_MARK(slot)                                                        \
+    do {                                                                      \
+        if (tim && tid == 0) {                                                \
+            const long long tn = clock64();                                   \
+            tim[slot] += (unsigned long long)(tn - t_sub);                    \
+            t_sub = tn;                                                       \
+        }                                                                     \
+    } while (0)
 
     // ---------------- prologue: grid, operators, fresh plasma, background (src/Simulation.cpp:653-708)
     for (int j = tid; j < M; j += kThreads) {
         S.r[j] = A.r[j];
         S.iv[j] = A.inv_V[j];
         S.ih[j] = (j < N) ? A.inv_h[j] : 0.0;
-        S.gm[j] = A.gm[j]; S.g0[j] = A.g0[j]; S.gp[j] = A.gp[j]; S.ir[j] = A.ir[j];
         S.bgt[j] = 0.0;
         S.bgr[j] = 0.0;
         S.bpr[j] = 0.0;
         S.bpi[j] = 0.0;
         src_of(S, M, 0).ne[j] = 0.0;
     }
-    if (A.opT_smem)
-        for (int t = tid; t < 9 * 32 * C; t += kThreads) const_cast<double*>(S.opT)[t] = A.opT[t];
+    if (A.const_smem)
+        for (int t = tid; t < 13 * M; t += kThreads) const_cast<double*>(S.gm)[t] = A.consts[t];
     if (tid == 0) *S.lost = 0;
     PState<ORD> P;
     int J = 0;                                             // cell of the thread's particle
@@ -429,25 +632,28 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
         if (wq == 0.0) continue;
         const PGeo g = geometry(S.r, S.ih, N, R, x, y);
         const double a0 = wq * g.W0 * S.iv[g.j], a1 = wq * g.W1 * S.iv[g.j + 1];
-        atomicAdd(&S.bgt[g.j], a0); atomicAdd(&S.bgr[g.j], a0);
-        atomicAdd(&S.bgt[g.j + 1], a1); atomicAdd(&S.bgr[g.j + 1], a1);
+        double* adr[4] = {S.bgt + g.j, S.bgr + g.j, S.bgt + g.j + 1, S.bgr + g.j + 1};
+        const double val[4] = {a0, a0, a1, a1};
+        add_multi<4>(adr, val);
     }
     if (A.neutralize) {
+        double* ne0 = src_of(S, M, 0).ne;
         for (int p = tid; p < np; p += kThreads) {
             const double w = A.p_init[5 * (size_t)npad + p];
             if (w == 0.0) continue;
             double q, qm;
             species_params(A, p, q, qm);
             const PGeo g = geometry(S.r, S.ih, N, R, A.p_init[p], A.p_init[npad + p]);
-            const double a0 = w * q * g.W0 * S.iv[g.j], a1 = w * q * g.W1 * S.iv[g.j + 1];
-            atomicAdd(&src_of(S, M, 0).ne[g.j], a0);
-            atomicAdd(&src_of(S, M, 0).ne[g.j + 1], a1);
+            double* adr[2] = {ne0 + g.j, ne0 + g.j + 1};
+            const double val[2] = {w * q * g.W0 * S.iv[g.j], w * q * g.W1 * S.iv[g.j + 1]};
+            add_multi<2>(adr, val);
         }
     }
     __syncthreads();
     for (int j = tid; j < M; j += kThreads) {
-        if (A.neutralize) { S.bgt[j] -= src_of(S, M, 0).ne[j]; S.bgr[j] -= src_of(S, M, 0).ne[j]; }
-        init_sources(src_of(S, M, 0), S, j, beam_row(A, 0, j));
+        const Src s0 = src_of(S, M, 0);
+        if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
+        init_sources(s0, S, j, beam_row(A, 0, j));
     }
     __syncthreads();
     // deposit of slice 0
@@ -469,106 +675,193 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
     __syncthreads();
     PHASE_MARK(0);
 
-    // warps 3.. initialise the sources of the next slice while warps 0-2 solve (A.dbuf)
-    constexpr int kInitBase = 96;
-    constexpr int kInitThreads = kThreads - kInitBase;
-
+    int scan_par = 0;                                            // alternates the scan scratch
+    const double fc = A.flux_coef;
     for (int k = 0; k < K; ++k) {
         const Src s = src_of(S, M, A.dbuf ? (k & 1) : 0);
         const Src sn = src_of(S, M, A.dbuf ? ((k + 1) & 1) : 0);
-        // ---------------- P2: psi, E_z, B_z (src/Simulation.cpp:797-807, :477-532)
-        if (warp < 3) {
-            double* q = S.q + warp * 3 * 32 * C;
-            const double* aT = S.opT;                            // L0
-            const double* bT = aT + 32 * C;
-            const double* cT = bT + 32 * C;
-            if (warp == 0) {
-                auto rows = [&](int ii, int i, double& a, double& b, double& c, double& d) {
-                    const int t = ii * 32 + lane;
-                    a = aT[t]; b = bT[t]; c = cT[t];
-                    d = (i < N) ? -1.0 * s.rhot[i] : 0.0;    // L0: Dirichlet row N; padding rows identity
-                };
-                warp_solve(rows, C, M, q, S.psi);
-                __syncwarp();
-                for (int ii = 0; ii < C; ++ii) {               // W+ mode 1: w1 = -psi' (src/Simulation.cpp:477-498)
-                    const int i = lane * C + ii;
-                    if (i < M) S.wr1[i] = -grad_at(S, N, S.psi, i, false);
-                }
-            } else if (warp == 1) {
-                auto rows = [&](int ii, int i, double& a, double& b, double& c, double& d) {
-                    const int t = ii * 32 + lane;
-                    a = aT[t]; b = bT[t]; c = cT[t];
-                    d = (i < N) ? -1.0 * s.drho[i] : 0.0;
-                };
-                warp_solve(rows, C, M, q, S.ez);
-            } else {
-                auto rows = [&](int ii, int i, double& a, double& b, double& c, double& d) {
-                    const int t = ii * 32 + lane;
-                    a = aT[t]; b = bT[t]; c = cT[t];
-                    if (i < N) {                                // L B_z = -(J_theta' + J_theta/r)
-                        const double t1 = grad_at(S, N, s.jpi1, i, true);
-                        const double t2 = (i == 0 ? s.jpi1[1] : s.jpi1[i]) * S.ir[i];
-                        d = 1.0 * (-(t1 + t2));
-                    } else {
-                        d = 0.0;
-                    }
-                };
-                warp_solve(rows, C, M, q, S.bz);
+        if (tim && tid == 0) t_sub = clock64();
+        // beam rows of slice k+1 for this thread's nodes (consumed below, latency overlaps the solves)
+        BeamRow pre[kMaxR];
+        if (A.dbuf && k + 1 < K)
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u)
+                if (u < Rw && row0 + u < M) pre[u] = beam_row(A, k + 1, row0 + u);
+
+        // ---------------- P2: psi, E_z, B_z with L0 (src/Simulation.cpp:797-807, :501-532)
+        {
+            // forward: y_i = (-a_i/u_i) y_{i-1} + d_i/u_i
+            double cA = 1.0, cB[3] = {0.0, 0.0, 0.0};
+            double dv[kMaxR][3];
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+                dv[u][0] = dv[u][1] = dv[u][2] = 0.0;
+                if (u >= Rw || i >= M) continue;
+                rhs_l0(S, s, N, i, dv[u][0], dv[u][1], dv[u][2]);
+                const double rr = S.l0r[i], af = S.l0f[i];
+#pragma unroll
+                for (int e = 0; e < 3; ++e) cB[e] = fma(af, cB[e], rr * dv[u][e]);
+                cA *= af;
             }
-        } else if (A.dbuf && k + 1 < K) {
-            for (int j = tid - kInitBase; j < M; j += kInitThreads) init_sources(sn, S, j, beam_row(A, k + 1, j));
+            SUB_MARK(5);
+            double yb[3];
+            scan_fwd<3>(cA, cB, yb, S.tot + (scan_par++ & 1) * 8 * kW);
+            SUB_MARK(6);
+            double y[kMaxR][3];
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+                y[u][0] = y[u][1] = y[u][2] = 0.0;
+                if (u >= Rw || i >= M) continue;
+                const double rr = S.l0r[i], af = S.l0f[i];
+#pragma unroll
+                for (int e = 0; e < 3; ++e) { yb[e] = fma(af, yb[e], rr * dv[u][e]); y[u][e] = yb[e]; }
+            }
+            // backward: x_i = (-c_i/u_i) x_{i+1} + y_i
+            double bA = 1.0, bB[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+            for (int u = kMaxR - 1; u >= 0; --u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+                const double ab = S.l0b[i];
+#pragma unroll
+                for (int e = 0; e < 3; ++e) bB[e] = fma(ab, bB[e], y[u][e]);
+                bA *= ab;
+            }
+            double xa[3];
+            scan_bwd<3>(bA, bB, xa, S.tot + (scan_par++ & 1) * 8 * kW);
+            SUB_MARK(7);
+#pragma unroll
+            for (int u = kMaxR - 1; u >= 0; --u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+                const double ab = S.l0b[i];
+#pragma unroll
+                for (int e = 0; e < 3; ++e) xa[e] = fma(ab, xa[e], y[u][e]);
+                S.psi[i] = xa[0];
+                S.ez[i] = xa[1];
+                S.bz[i] = xa[2];
+            }
+            if (A.dbuf && k + 1 < K)
+#pragma unroll
+                for (int u = 0; u < kMaxR; ++u)
+                    if (u < Rw && row0 + u < M) init_sources(sn, S, row0 + u, pre[u]);
+            SUB_MARK(8);
         }
         __syncthreads();
         PHASE_MARK(1);
 
         // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559)
         if (REG) {
-            if (tid < np && P.w != 0.0) depositS_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), s, S);
+            if (tid < np && P.w != 0.0) depositS_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), s, S, N);
         } else {
             for (int p = tid; p < np; p += kThreads) {
                 PState<ORD> Q;
                 pload(Q, A.ps, npad, p);
                 if (Q.w == 0.0) continue;
                 species_params(A, p, Q.q, Q.qm);
-                depositS_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), s, S);
+                depositS_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), s, S, N);
             }
         }
         __syncthreads();
         PHASE_MARK(2);
 
-        // ---------------- P4: B+ (src/Simulation.cpp:535-591, m = 0: one pass); sources of k+1
-        if (warp == 0) {
-            const double* aT = S.opT + 1 * 3 * 32 * C;              // (L1D - chi) B_r0 = -S_i
-            const double* bT = aT + 32 * C;
-            const double* cT = bT + 32 * C;
-            auto rows = [&](int ii, int i, double& a, double& b, double& c, double& d) {
-                const int t = ii * 32 + lane;
-                a = aT[t]; b = bT[t]; c = cT[t];
-                if (i >= 1 && i < N) {
-                    b = b - s.chi[i];
-                    d = 1.0 * (-s.S1i[i]);
-                } else {
-                    d = 0.0;
+        // ---------------- P4: B+ (src/Simulation.cpp:535-591, m = 0: one pass)
+        //   (L1D - chi) B_r0 = -S_i (rows 0, N Dirichlet); (L1F - chi) B_theta0 = J_z' + S_r, flux wall J_z(R)
+        {
+            // pivots: product of T_i = [[b_i, -a_i c_{i-1}], [1, 0]] over the thread's rows
+            double m[2][4];
+#pragma unroll
+            for (int sy = 0; sy < 2; ++sy) { m[sy][0] = 1.0; m[sy][1] = 0.0; m[sy][2] = 0.0; m[sy][3] = 1.0; }
+            double ra[kMaxR][2], rb[kMaxR][2], rc[kMaxR][2], rd[kMaxR][2];
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+#pragma unroll
+                for (int sy = 0; sy < 2; ++sy) {
+                    ra[u][sy] = 0.0; rb[u][sy] = 1.0; rc[u][sy] = 0.0; rd[u][sy] = 0.0;
+                    if (u >= Rw || i >= M) continue;
+                    row_b(S, s, N, fc, sy, i, ra[u][sy], rb[u][sy], rc[u][sy], rd[u][sy]);
+                    const double t01 = -ra[u][sy] * rc[u][sy];
+                    const double n00 = rb[u][sy] * m[sy][0] + t01 * m[sy][2];
+                    const double n01 = rb[u][sy] * m[sy][1] + t01 * m[sy][3];
+                    m[sy][2] = m[sy][0]; m[sy][3] = m[sy][1];
+                    m[sy][0] = n00; m[sy][1] = n01;
+                    renorm(m[sy][0], m[sy][1], m[sy][2], m[sy][3]);
                 }
-            };
-            warp_solve(rows, C, M, S.q, S.bpr);
-        } else if (warp == 1) {
-            const double* aT = S.opT + 2 * 3 * 32 * C;              // (L1F - chi) B_theta0 = J_z' + S_r
-            const double* bT = aT + 32 * C;
-            const double* cT = bT + 32 * C;
-            const double fc = A.flux_coef;
-            auto rows = [&](int ii, int i, double& a, double& b, double& c, double& d) {
-                const int t = ii * 32 + lane;
-                a = aT[t]; b = bT[t]; c = cT[t];
-                if (i >= 1 && i <= N) {
-                    b = b - s.chi[i];
-                    d = 1.0 * (grad_at(S, N, s.jz, i, false) + s.S1r[i]);
-                    if (i == N) d -= fc * s.jz[N];             // flux wall g = J_z(R)
-                } else {
-                    d = 0.0;
+            }
+            double pp[2], qq[2];
+            scan_pivots<2>(m, pp, qq, S.tot + (scan_par++ & 1) * 8 * kW);
+            // this thread's pivots (rc holds c_{i-1}; rinv = 1/u_i = p_{i-1}/p_i), forward composites
+            double rinv[kMaxR][2];
+            double fA[2] = {1.0, 1.0}, fB[2] = {0.0, 0.0};
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+#pragma unroll
+                for (int sy = 0; sy < 2; ++sy) {
+                    rinv[u][sy] = 0.0;
+                    if (u >= Rw || i >= M) continue;
+                    const double pn = rb[u][sy] * pp[sy] - ra[u][sy] * rc[u][sy] * qq[sy];
+                    qq[sy] = pp[sy];
+                    pp[sy] = pn;
+                    const double rr = qq[sy] / pp[sy];
+                    const double sc = fabs(pp[sy]);
+                    if (sc > 1e100 || sc < 1e-100) { pp[sy] /= sc; qq[sy] /= sc; }
+                    rinv[u][sy] = rr;
+                    const double af = -rr * ra[u][sy];
+                    fB[sy] = fma(af, fB[sy], rr * rd[u][sy]);
+                    fA[sy] *= af;
                 }
-            };
-            warp_solve(rows, C, M, S.q + 3 * 32 * C, S.bpi);
+            }
+            // forward substitution of both systems
+            double fb2[2][1] = {{fB[0]}, {fB[1]}}, yb0[1], yb1[1];
+            scan_fwd<1>(fA[0], fb2[0], yb0, S.tot + (scan_par++ & 1) * 8 * kW);
+            scan_fwd<1>(fA[1], fb2[1], yb1, S.tot + (scan_par++ & 1) * 8 * kW);
+            double y[kMaxR][2];
+            double yy[2] = {yb0[0], yb1[0]};
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+#pragma unroll
+                for (int sy = 0; sy < 2; ++sy) {
+                    y[u][sy] = 0.0;
+                    if (u >= Rw || i >= M) continue;
+                    yy[sy] = fma(-rinv[u][sy] * ra[u][sy], yy[sy], rinv[u][sy] * rd[u][sy]);
+                    y[u][sy] = yy[sy];
+                }
+            }
+            // backward substitution: x_i = -(c_i / u_i) x_{i+1} + y_i
+            double bA[2] = {1.0, 1.0}, bB[2] = {0.0, 0.0};
+#pragma unroll
+            for (int u = kMaxR - 1; u >= 0; --u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+#pragma unroll
+                for (int sy = 0; sy < 2; ++sy) {
+                    const double c = sy ? S.lfc[i] : S.l1c[i];
+                    const double ab = -(c * rinv[u][sy]);
+                    bB[sy] = fma(ab, bB[sy], y[u][sy]);
+                    bA[sy] *= ab;
+                }
+            }
+            double bb2[2][1] = {{bB[0]}, {bB[1]}}, xa0[1], xa1[1];
+            scan_bwd<1>(bA[0], bb2[0], xa0, S.tot + (scan_par++ & 1) * 8 * kW);
+            scan_bwd<1>(bA[1], bb2[1], xa1, S.tot + (scan_par++ & 1) * 8 * kW);
+            double xx[2] = {xa0[0], xa1[0]};
+#pragma unroll
+            for (int u = kMaxR - 1; u >= 0; --u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+#pragma unroll
+                for (int sy = 0; sy < 2; ++sy) {
+                    const double c = sy ? S.lfc[i] : S.l1c[i];
+                    xx[sy] = fma(-(c * rinv[u][sy]), xx[sy], y[u][sy]);
+                }
+                S.bpr[i] = xx[0];
+                S.bpi[i] = xx[1];
+            }
         }
         __syncthreads();
         PHASE_MARK(3);
@@ -578,7 +871,8 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             const size_t fb = (size_t)k * M;
             for (int j = tid; j < M; j += kThreads) {
                 double* F = A.fld + (fb + j) * F_NC0;
-                F[F_EP1R] = S.wr1[j] + S.bpi[j];
+                const double w1 = -grad_at(S, N, S.psi, j, false);
+                F[F_EP1R] = w1 + S.bpi[j];
                 F[F_EP1I] = 0.0 - S.bpr[j];
                 F[F_BP1R] = S.bpr[j];
                 F[F_BP1I] = S.bpi[j];
@@ -592,7 +886,7 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
         }
         if (k + 1 < K) {
             if (!A.dbuf) {
-                __syncthreads();                                    // store read the sources
+                __syncthreads();                                    // the store read the sources
                 for (int j = tid; j < M; j += kThreads) init_sources(sn, S, j, beam_row(A, k + 1, j));
                 __syncthreads();
             }
@@ -600,9 +894,9 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             if (REG) {
                 if (tid < np && P.w != 0.0) {
                     if (push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first)) {
-                        const PGeo G = geometry(S.r, S.ih, N, R, P.x, P.y);
-                        J = G.j;
-                        deposit_particle(P, G, sn, S);
+                        const double rn = sqrt(P.x * P.x + P.y * P.y);
+                        J = locate_from(S.r, N, R, rn, J);
+                        deposit_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), sn, S);
                     } else {
                         atomicAdd(S.lost, 1);
                     }
@@ -629,33 +923,37 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
     if (REG && tid < np) pstore(P, A.ps, npad, tid);
     if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
 #undef PHASE_MARK
+#undef SUB_MARK
 }
 
-size_t sweep_m0_smem_bytes(int M, int C, bool dbuf, bool opT_smem, bool q_smem) {
-    size_t d = (size_t)(dbuf ? 33 : 24) * M;
-    if (opT_smem) d += 9 * 32 * (size_t)C;
-    if (q_smem) d += 9 * 32 * (size_t)C;
+size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem) {
+    size_t d = (size_t)(3 + 2 + 5 + (dbuf ? 18 : 9)) * M + 2 * 8 * kW;
+    if (const_smem) d += 13 * (size_t)M;
     return sizeof(double) * d + 16;
 }
 
 namespace {
-template <int ORD, bool REG>
+template <int ORD, bool REG, int RM>
 cudaError_t launch_t(const SweepArgs& A, size_t smem, cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(sweep_m0_kernel<ORD, REG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(sweep_m0_kernel<ORD, REG, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    sweep_m0_kernel<ORD, REG><<<1, kThreads, smem, stream>>>(A);
+    sweep_m0_kernel<ORD, REG, RM><<<1, kThreads, smem, stream>>>(A);
     return cudaGetLastError();
 }
 
 template <int ORD>
 cudaError_t launch_o(const SweepArgs& A, size_t smem, cudaStream_t stream) {
-    return A.np <= kThreads ? launch_t<ORD, true>(A, smem, stream) : launch_t<ORD, false>(A, smem, stream);
+    const bool reg = A.np <= kThreads;
+    if (A.rows_per_thread == 1)
+        return reg ? launch_t<ORD, true, 1>(A, smem, stream) : launch_t<ORD, false, 1>(A, smem, stream);
+    return reg ? launch_t<ORD, true, 4>(A, smem, stream) : launch_t<ORD, false, 4>(A, smem, stream);
 }
 }  // namespace
 
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream) {
-    const size_t smem = sweep_m0_smem_bytes(A.M, A.C, A.dbuf, A.opT_smem, A.q_smem);
+    if (A.rows_per_thread < 1 || A.rows_per_thread > 4) return cudaErrorInvalidValue;
+    const size_t smem = sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem);
     switch (A.ord) {
         case 1: return launch_o<1>(A, smem, stream);
         case 2: return launch_o<2>(A, smem, stream);

@@ -7,6 +7,7 @@ import numpy as np
 from quarz_b200 import deck
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+ROOT_DIR = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 from quarz_b200.workloads import PLAIN_BLOWOUT as CONFIG0  # noqa: E402
 from quarz_b200.workloads import pinched_witness_deck as config1_deck  # noqa: E402
