@@ -18,7 +18,7 @@
 // scans of affine maps. Each scan costs five warp-shuffle levels and one block barrier. The psi,
 // E_z and B_z systems share the constant operator L0, whose pivots are computed once on the host.
 //
-// Slice schedule (4 phase barriers + 7 scan barriers per slice):
+// Slice schedule (4 phase barriers + 5 scan barriers per slice):
 //   P2  psi, E_z, B_z (two scans, three right-hand sides); sources of slice k+1 = beam + background
 //   P3  S+ deposit by the particles
 //   P4  B_r, B_theta (pivot scan + forward and backward scans of the two systems)
@@ -158,6 +158,87 @@ __device__ __forceinline__ void scan_bwd(double a, const double (&b)[NR], double
     }
 }
 
+// The same two scans for NS independent systems, each with its own map y -> a[s] y + b[s].
+template <int NS>
+__device__ __forceinline__ void scan_fwd_n(const double (&a)[NS], const double (&b)[NS], double (&yb)[NS],
+                                           double* tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double A[NS], B[NS];
+#pragma unroll
+    for (int r = 0; r < NS; ++r) { A[r] = a[r]; B[r] = b[r]; }
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+        double Ap[NS], Bp[NS];
+#pragma unroll
+        for (int r = 0; r < NS; ++r) { Ap[r] = __shfl_up_sync(FULL, A[r], st); Bp[r] = __shfl_up_sync(FULL, B[r], st); }
+        if (lane >= st)
+#pragma unroll
+            for (int r = 0; r < NS; ++r) { B[r] = fma(A[r], Bp[r], B[r]); A[r] *= Ap[r]; }
+    }
+    if (lane == 31)
+#pragma unroll
+        for (int r = 0; r < NS; ++r) { tot[kW * (2 * r) + warp] = A[r]; tot[kW * (2 * r + 1) + warp] = B[r]; }
+    double eA[NS], eB[NS];
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+        eA[r] = __shfl_up_sync(FULL, A[r], 1);
+        eB[r] = __shfl_up_sync(FULL, B[r], 1);
+        if (lane == 0) { eA[r] = 1.0; eB[r] = 0.0; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+        double ta = lane < kW ? tot[kW * (2 * r) + lane] : 1.0, tb = lane < kW ? tot[kW * (2 * r + 1) + lane] : 0.0;
+#pragma unroll
+        for (int st = 1; st < kW; st <<= 1) {
+            const double ap = __shfl_up_sync(FULL, ta, st), bp = __shfl_up_sync(FULL, tb, st);
+            if (lane >= st) { tb = fma(ta, bp, tb); ta *= ap; }
+        }
+        const double cw = __shfl_sync(FULL, tb, (warp + 31) & 31);
+        yb[r] = fma(eA[r], warp > 0 ? cw : 0.0, eB[r]);
+    }
+}
+
+template <int NS>
+__device__ __forceinline__ void scan_bwd_n(const double (&a)[NS], const double (&b)[NS], double (&xa)[NS],
+                                           double* tot) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double A[NS], B[NS];
+#pragma unroll
+    for (int r = 0; r < NS; ++r) { A[r] = a[r]; B[r] = b[r]; }
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+        double An[NS], Bn[NS];
+#pragma unroll
+        for (int r = 0; r < NS; ++r) { An[r] = __shfl_down_sync(FULL, A[r], st); Bn[r] = __shfl_down_sync(FULL, B[r], st); }
+        if (lane + st < 32)
+#pragma unroll
+            for (int r = 0; r < NS; ++r) { B[r] = fma(A[r], Bn[r], B[r]); A[r] *= An[r]; }
+    }
+    if (lane == 0)
+#pragma unroll
+        for (int r = 0; r < NS; ++r) { tot[kW * (2 * r) + warp] = A[r]; tot[kW * (2 * r + 1) + warp] = B[r]; }
+    double eA[NS], eB[NS];
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+        eA[r] = __shfl_down_sync(FULL, A[r], 1);
+        eB[r] = __shfl_down_sync(FULL, B[r], 1);
+        if (lane == 31) { eA[r] = 1.0; eB[r] = 0.0; }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < NS; ++r) {
+        double ta = lane < kW ? tot[kW * (2 * r) + lane] : 1.0, tb = lane < kW ? tot[kW * (2 * r + 1) + lane] : 0.0;
+#pragma unroll
+        for (int st = 1; st < kW; st <<= 1) {
+            const double an = __shfl_down_sync(FULL, ta, st), bn = __shfl_down_sync(FULL, tb, st);
+            if (lane + st < kW) { tb = fma(ta, bn, tb); ta *= an; }
+        }
+        const double cw = __shfl_sync(FULL, tb, (warp + 1) & 31);
+        xa[r] = fma(eA[r], warp < kW - 1 ? cw : 0.0, eB[r]);
+    }
+}
+
 // Exclusive scan of 2x2 matrix products (later rows on the left) for NS systems: on return
 // (p[s], q[s]) = first column of the product of all matrices before this thread's rows.
 template <int NS>
@@ -236,6 +317,33 @@ __device__ __forceinline__ void add_multi(double* const (&p)[NA], const double (
     }
 }
 
+// Warp aggregation of deposits: lanes holding contributions to the same cell form runs of equal
+// keys in lane order (plasma particles stay close to their radial loading order); a segmented
+// warp-shuffle scan sums each run, and only the last lane of a run updates shared memory. Runs
+// split by reordering only cost extra updates, never correctness. Blowout piles tens of particles
+// into a few sheath or axis cells, where per-particle updates of the same word would serialise.
+template <int NV>
+__device__ __forceinline__ bool warp_runs_sum(int key, double (&v)[NV]) {
+    const int lane = threadIdx.x & 31;
+    const int kprev = __shfl_up_sync(FULL, key, 1);
+    const bool head = (lane == 0) || (kprev != key);
+    const unsigned heads = __ballot_sync(FULL, head);
+    if (heads == FULL) return true;                   // no shared cell in this warp
+    const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
+#pragma unroll
+    for (int st = 1; st < 32; st <<= 1) {
+        const int sp = __shfl_up_sync(FULL, seg, st);
+        double vp[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) vp[i] = __shfl_up_sync(FULL, v[i], st);
+        if (lane >= st && sp == seg)
+#pragma unroll
+            for (int i = 0; i < NV; ++i) v[i] += vp[i];
+    }
+    const int knext = __shfl_down_sync(FULL, key, 1);
+    return (lane == 31) || (knext != key);
+}
+
 // ---------------------------------------------------------------- shared-memory layout
 struct Src {                                              // plasma + beam sources of one slice
     double *rhot, *drho, *jz, *chi, *ne, *ni, *jpi1, *S1r, *S1i;
@@ -248,7 +356,7 @@ struct Smem {
     const double *l1a, *l1b, *l1c, *lfa, *lfb, *lfc;      // L1D and L1F rows
     double* src0;                                         // sources: 9 arrays, twice when A.dbuf
     double *bgt, *bgr;                                    // neutralising background
-    double *psi, *ez, *bz, *bpr, *bpi;                    // fields of the slice
+    double *psi, *ez, *bz, *wr1, *bpr, *bpi;              // fields of the slice (wr1 = -psi')
     double* tot;                                          // scan scratch, 2 x 8 x kW
     int* lost;
 };
@@ -267,7 +375,7 @@ __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
     S.src0 = p;
     p += (A.dbuf ? 18 : 9) * (size_t)M;
     S.bgt = p; p += M; S.bgr = p; p += M;
-    S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
+    S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.wr1 = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
     S.tot = p; p += 2 * 8 * kW;
     S.lost = reinterpret_cast<int*>(p);
     return S;
@@ -381,14 +489,14 @@ __device__ __forceinline__ void species_params(const SweepArgs& A, int p, double
     qm = A.sp_qm[s];
 }
 
-// W+ mode 1 at the particle: lin(w1) with w1 = -psi' (src/Simulation.cpp:477-498)
-__device__ __forceinline__ double w1_at(const Smem& S, int N, const PGeo& g) {
-    return g.W0 * (-grad_at(S, N, S.psi, g.j, false)) + g.W1 * (-grad_at(S, N, S.psi, g.j + 1, false));
-}
+// W+ mode 1 at the particle: lin(w1), w1 = -psi' (src/Simulation.cpp:477-498)
+__device__ __forceinline__ double w1_at(const Smem& S, int N, const PGeo& g) { return lin(S.wr1, g); }
 
-// src/PlasmaSpecies.cpp:409-478, m = 0 (plasma rho and J_r feed nothing on this path: not deposited)
+// src/PlasmaSpecies.cpp:409-478, m = 0 (plasma rho and J_r feed nothing on this path: not deposited).
+// Contributions of one particle to nodes j (v[0..5]) and j+1 (v[6..11]): rho - J_z, d/dxi, J_z, chi,
+// density, J_theta.
 template <int ORD>
-__device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGeo& g, const Src& s, const Smem& S) {
+__device__ __forceinline__ void deposit_values(const PState<ORD>& P, const PGeo& g, const Smem& S, double (&v)[12]) {
     const double PX = P.px, PY = P.py, D = P.dl, w = P.w;
     const double gam = (1.0 + PX * PX + PY * PY + D * D) / (2.0 * D);
     const double invd = 1.0 / D;
@@ -396,9 +504,6 @@ __device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGe
     const double ux = PX * invd, uy = PY * invd;
     const double ur = g.c * ux + g.s * uy, uth = g.c * uy - g.s * ux;
     const double wq = w * P.q;
-    double* dens = (P.q < 0.0) ? s.ne : s.ni;
-    double* adr[12];
-    double val[12];
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         const int jj = g.j + cc;
@@ -409,20 +514,43 @@ __device__ __forceinline__ void deposit_particle(const PState<ORD>& P, const PGe
         const double dr = wq * ur * dWc * iv;
         const double vjz = a * pz * invd, vchi = a * P.qm * invd;
         const double vn = w * Wc * iv * gam * invd;
-        adr[6 * cc + 0] = s.rhot + jj; val[6 * cc + 0] = a;
-        adr[6 * cc + 1] = s.drho + jj; val[6 * cc + 1] = dr;
-        adr[6 * cc + 2] = s.jz + jj;   val[6 * cc + 2] = vjz;
-        adr[6 * cc + 3] = s.chi + jj;  val[6 * cc + 3] = vchi;
-        adr[6 * cc + 4] = dens + jj;   val[6 * cc + 4] = vn;
-        adr[6 * cc + 5] = s.jpi1 + jj; val[6 * cc + 5] = a * uth;
+        v[6 * cc + 0] = a;
+        v[6 * cc + 1] = dr;
+        v[6 * cc + 2] = vjz;
+        v[6 * cc + 3] = vchi;
+        v[6 * cc + 4] = vn;
+        v[6 * cc + 5] = a * uth;
     }
-    add_multi<12>(adr, val);
 }
 
-// src/PlasmaSpecies.cpp:508-559, m = 0
+// warp-wide: every lane calls it (active = the lane has a particle); key = 2 j + (positive species)
+__device__ __forceinline__ void deposit_warp(bool active, int j, bool neg, double (&v)[12], const Src& s) {
+    const int lane = threadIdx.x & 31;
+    if (!active)
+#pragma unroll
+        for (int i = 0; i < 12; ++i) v[i] = 0.0;
+    const int key = active ? 2 * j + (neg ? 0 : 1) : -1 - lane;
+    if (warp_runs_sum<12>(key, v) && active) {
+        double* dens = neg ? s.ne : s.ni;
+        double* adr[12];
+#pragma unroll
+        for (int cc = 0; cc < 2; ++cc) {
+            const int jj = j + cc;
+            adr[6 * cc + 0] = s.rhot + jj;
+            adr[6 * cc + 1] = s.drho + jj;
+            adr[6 * cc + 2] = s.jz + jj;
+            adr[6 * cc + 3] = s.chi + jj;
+            adr[6 * cc + 4] = dens + jj;
+            adr[6 * cc + 5] = s.jpi1 + jj;
+        }
+        add_multi<12>(adr, v);
+    }
+}
+
+// src/PlasmaSpecies.cpp:508-559, m = 0: S+ contributions to nodes j (v[0..1]) and j+1 (v[2..3])
 template <int ORD>
-__device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PGeo& g, const Src& s, const Smem& S,
-                                                  int N) {
+__device__ __forceinline__ void depositS_values(const PState<ORD>& P, const PGeo& g, const Smem& S, int N,
+                                                double (&v)[4]) {
     const double qm = P.qm;
     const double PX = P.px, PY = P.py, D = P.dl;
     const double r1 = w1_at(S, N, g);
@@ -436,8 +564,6 @@ __device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PG
     const double ax = (qm * (gam * Wx + PY * Bz) * invd) * invd - PX * dD * invd * invd;
     const double ay = (qm * (gam * Wy - PX * Bz) * invd) * invd - PY * dD * invd * invd;
     const double wq = P.w * P.q;
-    double* adr[4];
-    double val[4];
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         const int jj = g.j + cc;
@@ -450,10 +576,21 @@ __device__ __forceinline__ void depositS_particle(const PState<ORD>& P, const PG
         const double f2 = uth * Worc;
         Ar += f2 * uy;
         Ai -= f2 * ux;
-        adr[2 * cc] = s.S1r + jj;     val[2 * cc] = iv * (Ar * g.c + Ai * g.s);
-        adr[2 * cc + 1] = s.S1i + jj; val[2 * cc + 1] = iv * (Ai * g.c - Ar * g.s);
+        v[2 * cc] = iv * (Ar * g.c + Ai * g.s);
+        v[2 * cc + 1] = iv * (Ai * g.c - Ar * g.s);
     }
-    add_multi<4>(adr, val);
+}
+
+__device__ __forceinline__ void depositS_warp(bool active, int j, double (&v)[4], const Src& s) {
+    const int lane = threadIdx.x & 31;
+    if (!active)
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i] = 0.0;
+    const int key = active ? j : -1 - lane;
+    if (warp_runs_sum<4>(key, v) && active) {
+        double* adr[4] = {s.S1r + j, s.S1i + j, s.S1r + j + 1, s.S1i + j + 1};
+        add_multi<4>(adr, v);
+    }
 }
 
 // src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns false
@@ -615,7 +752,14 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
                 for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
             species_params(A, tid, P.q, P.qm);
         } else {
+            P.x = P.y = P.px = P.py = 0.0;
+            P.dl = 1.0;
             P.w = 0.0;
+            P.q = P.qm = -1.0;
+#pragma unroll
+            for (int m = 0; m < ORD; ++m)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
         }
     } else {
         for (int p = tid; p < np; p += kThreads) {
@@ -657,19 +801,34 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
     }
     __syncthreads();
     // deposit of slice 0
+    const int lane = tid & 31;
     if (REG) {
-        if (tid < np && P.w != 0.0) {
+        const bool act = tid < np && P.w != 0.0;
+        double v[12];
+        if (act) {
             const PGeo G = geometry(S.r, S.ih, N, R, P.x, P.y);
             J = G.j;
-            deposit_particle(P, G, src_of(S, M, 0), S);
+            deposit_values(P, G, S, v);
         }
+        deposit_warp(act, J, P.q < 0.0, v, src_of(S, M, 0));
     } else {
-        for (int p = tid; p < np; p += kThreads) {
+        for (int base = tid - lane; base < np; base += kThreads) {
+            const int p = base + lane;
             PState<ORD> Q;
-            pload(Q, A.ps, npad, p);
-            if (Q.w == 0.0) continue;
-            species_params(A, p, Q.q, Q.qm);
-            deposit_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), src_of(S, M, 0), S);
+            bool act = false;
+            int j = 0;
+            double v[12];
+            if (p < np) {
+                pload(Q, A.ps, npad, p);
+                species_params(A, p, Q.q, Q.qm);
+                act = Q.w != 0.0;
+                if (act) {
+                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                    j = g.j;
+                    deposit_values(Q, g, S, v);
+                }
+            }
+            deposit_warp(act, j, act && Q.q < 0.0, v, src_of(S, M, 0));
         }
     }
     __syncthreads();
@@ -708,6 +867,7 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             double yb[3];
             scan_fwd<3>(cA, cB, yb, S.tot + (scan_par++ & 1) * 8 * kW);
             SUB_MARK(6);
+            const double ypsi_prev = yb[0];                         // y of psi just before this thread's rows
             double y[kMaxR][3];
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u) {
@@ -732,6 +892,18 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             double xa[3];
             scan_bwd<3>(bA, bB, xa, S.tot + (scan_par++ & 1) * 8 * kW);
             SUB_MARK(7);
+            // psi on the window [row0 - 1, row0 + Rw]: the rows of this thread, x after them (the
+            // backward carry) and x before them, x_{row0-1} = y_{row0-1} - (c/u)_{row0-1} x_{row0}
+            // with y_{row0-1} the forward carry -- so W+ = -psi' needs no further exchange
+            double pw[kMaxR + 2];
+            pw[kMaxR + 1] = 0.0;
+            {
+                double xr = xa[0];
+#pragma unroll
+                for (int u = kMaxR; u >= 1; --u) pw[u] = 0.0;
+                const int last = (row0 + Rw <= M ? Rw : M - row0);
+                if (last >= 0) pw[last + 1 > kMaxR + 1 ? kMaxR + 1 : last + 1] = xr;
+            }
 #pragma unroll
             for (int u = kMaxR - 1; u >= 0; --u) {
                 const int i = row0 + u;
@@ -742,6 +914,21 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
                 S.psi[i] = xa[0];
                 S.ez[i] = xa[1];
                 S.bz[i] = xa[2];
+                pw[u + 1] = xa[0];
+            }
+            pw[0] = (row0 >= 1 && row0 < M) ? fma(S.l0b[row0 - 1], pw[1], ypsi_prev) : 0.0;
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+                if (i == 0) {
+                    S.wr1[0] = -0.0;
+                } else if (i < N) {
+                    S.wr1[i] = -(S.gm[i] * pw[u] + S.g0[i] * pw[u + 1] + S.gp[i] * pw[u + 2]);
+                }
+                if (i == N - 1) {                                  // the one-sided wall stencil needs psi_{N-2..N}
+                    S.wr1[N] = -(S.g0[N] * pw[u + 2] + S.gm[N] * pw[u + 1] + S.gp[N] * pw[u]);
+                }
             }
             if (A.dbuf && k + 1 < K)
 #pragma unroll
@@ -754,14 +941,28 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
 
         // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559)
         if (REG) {
-            if (tid < np && P.w != 0.0) depositS_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), s, S, N);
+            const bool act = tid < np && P.w != 0.0;
+            double v[4];
+            if (act) depositS_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, N, v);
+            depositS_warp(act, J, v, s);
         } else {
-            for (int p = tid; p < np; p += kThreads) {
-                PState<ORD> Q;
-                pload(Q, A.ps, npad, p);
-                if (Q.w == 0.0) continue;
-                species_params(A, p, Q.q, Q.qm);
-                depositS_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), s, S, N);
+            for (int base = tid - lane; base < np; base += kThreads) {
+                const int p = base + lane;
+                bool act = false;
+                int j = 0;
+                double v[4];
+                if (p < np) {
+                    PState<ORD> Q;
+                    pload(Q, A.ps, npad, p);
+                    species_params(A, p, Q.q, Q.qm);
+                    act = Q.w != 0.0;
+                    if (act) {
+                        const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                        j = g.j;
+                        depositS_values(Q, g, S, N, v);
+                    }
+                }
+                depositS_warp(act, j, v, s);
             }
         }
         __syncthreads();
@@ -816,11 +1017,9 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
                 }
             }
             // forward substitution of both systems
-            double fb2[2][1] = {{fB[0]}, {fB[1]}}, yb0[1], yb1[1];
-            scan_fwd<1>(fA[0], fb2[0], yb0, S.tot + (scan_par++ & 1) * 8 * kW);
-            scan_fwd<1>(fA[1], fb2[1], yb1, S.tot + (scan_par++ & 1) * 8 * kW);
+            double yy[2];
+            scan_fwd_n<2>(fA, fB, yy, S.tot + (scan_par++ & 1) * 8 * kW);
             double y[kMaxR][2];
-            double yy[2] = {yb0[0], yb1[0]};
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u) {
                 const int i = row0 + u;
@@ -846,10 +1045,8 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
                     bA[sy] *= ab;
                 }
             }
-            double bb2[2][1] = {{bB[0]}, {bB[1]}}, xa0[1], xa1[1];
-            scan_bwd<1>(bA[0], bb2[0], xa0, S.tot + (scan_par++ & 1) * 8 * kW);
-            scan_bwd<1>(bA[1], bb2[1], xa1, S.tot + (scan_par++ & 1) * 8 * kW);
-            double xx[2] = {xa0[0], xa1[0]};
+            double xx[2];
+            scan_bwd_n<2>(bA, bB, xx, S.tot + (scan_par++ & 1) * 8 * kW);
 #pragma unroll
             for (int u = kMaxR - 1; u >= 0; --u) {
                 const int i = row0 + u;
@@ -871,8 +1068,7 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             const size_t fb = (size_t)k * M;
             for (int j = tid; j < M; j += kThreads) {
                 double* F = A.fld + (fb + j) * F_NC0;
-                const double w1 = -grad_at(S, N, S.psi, j, false);
-                F[F_EP1R] = w1 + S.bpi[j];
+                F[F_EP1R] = S.wr1[j] + S.bpi[j];
                 F[F_EP1I] = 0.0 - S.bpr[j];
                 F[F_BP1R] = S.bpr[j];
                 F[F_BP1I] = S.bpi[j];
@@ -892,28 +1088,43 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
             }
             const bool first = (k == 0);
             if (REG) {
-                if (tid < np && P.w != 0.0) {
+                bool act = tid < np && P.w != 0.0;
+                double v[12];
+                if (act) {
                     if (push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first)) {
                         const double rn = sqrt(P.x * P.x + P.y * P.y);
                         J = locate_from(S.r, N, R, rn, J);
-                        deposit_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), sn, S);
+                        deposit_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, v);
                     } else {
+                        act = false;
                         atomicAdd(S.lost, 1);
                     }
                 }
+                deposit_warp(act, J, P.q < 0.0, v, sn);
             } else {
-                for (int p = tid; p < np; p += kThreads) {
+                for (int base = tid - lane; base < np; base += kThreads) {
+                    const int p = base + lane;
+                    bool act = false;
+                    int j = 0;
+                    double v[12];
                     PState<ORD> Q;
-                    pload(Q, A.ps, npad, p);
-                    if (Q.w == 0.0) continue;
-                    species_params(A, p, Q.q, Q.qm);
-                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                    if (push_particle(Q, g, S, A, first)) {
-                        deposit_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), sn, S);
-                    } else {
-                        atomicAdd(S.lost, 1);
+                    if (p < np) {
+                        pload(Q, A.ps, npad, p);
+                        species_params(A, p, Q.q, Q.qm);
+                        if (Q.w != 0.0) {
+                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                            if (push_particle(Q, g, S, A, first)) {
+                                const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                j = g2.j;
+                                deposit_values(Q, g2, S, v);
+                                act = true;
+                            } else {
+                                atomicAdd(S.lost, 1);
+                            }
+                            pstore(Q, A.ps, npad, p);
+                        }
                     }
-                    pstore(Q, A.ps, npad, p);
+                    deposit_warp(act, j, act && Q.q < 0.0, v, sn);
                 }
             }
         }
@@ -927,7 +1138,7 @@ __global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A
 }
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem) {
-    size_t d = (size_t)(3 + 2 + 5 + (dbuf ? 18 : 9)) * M + 2 * 8 * kW;
+    size_t d = (size_t)(3 + 2 + 6 + (dbuf ? 18 : 9)) * M + 2 * 8 * kW;
     if (const_smem) d += 13 * (size_t)M;
     return sizeof(double) * d + 16;
 }
