@@ -1,1144 +1,18 @@
-// qz_sweep.cu -- the quasi-static xi sweep of one time step as ONE persistent CTA (sm_100a, FP64).
-//
-// Replaces the per-slice kernel chain of Simulation::step_fields (src/Simulation.cpp:636-795):
-//   zero_sources -> PlasmaSpecies::deposit -> combine_sources -> solve_slice_fields
-//   (psi, E_z, W+, B_z, deposit_S, B+) -> store_slice -> PlasmaSpecies::push
-// for azimuthal mode m = 0.
-//
-// Layout. The radial arrays of a slice (sources, fields, grid, stencils, operator rows) live in shared
-// memory (the constant ones fall back to global memory for very large grids). With at most 512
-// plasma particles, thread p owns particle p and keeps its state -- position, momentum, Delta,
-// weight and the Adams-Bashforth history -- in registers for the whole sweep; larger plasmas keep
-// the state in a global scratch buffer.
-//
-// Tridiagonal solves. Every system is solved by all 512 threads at once: thread t owns rows
-// [t*R, t*R + R), and the three Thomas recurrences -- pivots u_i = b_i - a_i c_{i-1} / u_{i-1},
-// forward y_i = (d_i - a_i y_{i-1}) / u_i, backward x_i = y_i - (c_i / u_i) x_{i+1} -- are evaluated
-// as block-wide scans: pivots as normalised prefix products of 2x2 matrices, the substitutions as
-// scans of affine maps. Each scan costs five warp-shuffle levels and one block barrier. The psi,
-// E_z and B_z systems share the constant operator L0, whose pivots are computed once on the host.
-//
-// Slice schedule (4 phase barriers + 5 scan barriers per slice):
-//   P2  psi, E_z, B_z (two scans, three right-hand sides); sources of slice k+1 = beam + background
-//   P3  S+ deposit by the particles
-//   P4  B_r, B_theta (pivot scan + forward and backward scans of the two systems)
-//   P5  store slice k; push k -> k+1 and deposit into the sources of slice k+1
-#include "qz_device.cuh"
-#include "qz_internal.h"
+// qz_sweep.cu -- stand-alone sweep launch: one CTA runs the whole xi sweep of one time step
+// (the sweep itself is in qz_sweep_body.cuh).
+#include "qz_sweep_body.cuh"
 
 namespace qzb {
 
-namespace {
-
-constexpr int kThreads = kSweepThreads;
-constexpr int kW = kThreads / 32;
-constexpr unsigned FULL = 0xffffffffu;
-
-// ---------------------------------------------------------------- block scans
-// Shared scratch for the warp totals of one scan: 8 x kW doubles; two of them alternate.
-
-// exact power-of-two rescaling of a 2x2 matrix (its largest entry into [1, 2))
-__device__ __forceinline__ void renorm(double& m00, double& m01, double& m10, double& m11) {
-    const double mx = fmax(fmax(fabs(m00), fabs(m01)), fmax(fabs(m10), fabs(m11)));
-    if (!(mx > 0.0) || !(mx < 1e300)) return;
-    const int e = ((__double2hiint(mx) >> 20) & 0x7ff) - 1023;
-    const double s = __hiloint2double((1023 - e) << 20, 0);
-    m00 *= s; m01 *= s; m10 *= s; m11 *= s;
-}
-
-// Exclusive forward scan of the affine maps y -> a y + b (thread order = row order), applied to
-// y_{-1} = 0: yb[r] is y just before this thread's rows.
-template <int NR>
-__device__ __forceinline__ void scan_fwd(double a, const double (&b)[NR], double (&yb)[NR], double* tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double A = a, B[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) B[r] = b[r];
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-        const double Ap = __shfl_up_sync(FULL, A, st);
-        double Bp[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) Bp[r] = __shfl_up_sync(FULL, B[r], st);
-        if (lane >= st) {
-#pragma unroll
-            for (int r = 0; r < NR; ++r) B[r] = fma(A, Bp[r], B[r]);
-            A *= Ap;
-        }
-    }
-    if (lane == 31) {
-        tot[warp] = A;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) tot[kW * (1 + r) + warp] = B[r];
-    }
-    double eA = __shfl_up_sync(FULL, A, 1), eB[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) eB[r] = __shfl_up_sync(FULL, B[r], 1);
-    if (lane == 0) {
-        eA = 1.0;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) eB[r] = 0.0;
-    }
-    __syncthreads();
-    double ta = lane < kW ? tot[lane] : 1.0, tb[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) tb[r] = lane < kW ? tot[kW * (1 + r) + lane] : 0.0;
-#pragma unroll
-    for (int st = 1; st < kW; st <<= 1) {
-        const double ap = __shfl_up_sync(FULL, ta, st);
-        double bp[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) bp[r] = __shfl_up_sync(FULL, tb[r], st);
-        if (lane >= st) {
-#pragma unroll
-            for (int r = 0; r < NR; ++r) tb[r] = fma(ta, bp[r], tb[r]);
-            ta *= ap;
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-        const double cw = __shfl_sync(FULL, tb[r], (warp + 31) & 31);
-        yb[r] = fma(eA, warp > 0 ? cw : 0.0, eB[r]);
-    }
-}
-
-// Exclusive backward scan of x -> a x + b applied to x_{end} = 0: xa[r] is x just after this
-// thread's rows.
-template <int NR>
-__device__ __forceinline__ void scan_bwd(double a, const double (&b)[NR], double (&xa)[NR], double* tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double A = a, B[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) B[r] = b[r];
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-        const double An = __shfl_down_sync(FULL, A, st);
-        double Bn[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) Bn[r] = __shfl_down_sync(FULL, B[r], st);
-        if (lane + st < 32) {
-#pragma unroll
-            for (int r = 0; r < NR; ++r) B[r] = fma(A, Bn[r], B[r]);
-            A *= An;
-        }
-    }
-    if (lane == 0) {
-        tot[warp] = A;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) tot[kW * (1 + r) + warp] = B[r];
-    }
-    double eA = __shfl_down_sync(FULL, A, 1), eB[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) eB[r] = __shfl_down_sync(FULL, B[r], 1);
-    if (lane == 31) {
-        eA = 1.0;
-#pragma unroll
-        for (int r = 0; r < NR; ++r) eB[r] = 0.0;
-    }
-    __syncthreads();
-    double ta = lane < kW ? tot[lane] : 1.0, tb[NR];
-#pragma unroll
-    for (int r = 0; r < NR; ++r) tb[r] = lane < kW ? tot[kW * (1 + r) + lane] : 0.0;
-#pragma unroll
-    for (int st = 1; st < kW; st <<= 1) {
-        const double an = __shfl_down_sync(FULL, ta, st);
-        double bn[NR];
-#pragma unroll
-        for (int r = 0; r < NR; ++r) bn[r] = __shfl_down_sync(FULL, tb[r], st);
-        if (lane + st < kW) {
-#pragma unroll
-            for (int r = 0; r < NR; ++r) tb[r] = fma(ta, bn[r], tb[r]);
-            ta *= an;
-        }
-    }
-#pragma unroll
-    for (int r = 0; r < NR; ++r) {
-        const double cw = __shfl_sync(FULL, tb[r], (warp + 1) & 31);
-        xa[r] = fma(eA, warp < kW - 1 ? cw : 0.0, eB[r]);
-    }
-}
-
-// The same two scans for NS independent systems, each with its own map y -> a[s] y + b[s].
-template <int NS>
-__device__ __forceinline__ void scan_fwd_n(const double (&a)[NS], const double (&b)[NS], double (&yb)[NS],
-                                           double* tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double A[NS], B[NS];
-#pragma unroll
-    for (int r = 0; r < NS; ++r) { A[r] = a[r]; B[r] = b[r]; }
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-        double Ap[NS], Bp[NS];
-#pragma unroll
-        for (int r = 0; r < NS; ++r) { Ap[r] = __shfl_up_sync(FULL, A[r], st); Bp[r] = __shfl_up_sync(FULL, B[r], st); }
-        if (lane >= st)
-#pragma unroll
-            for (int r = 0; r < NS; ++r) { B[r] = fma(A[r], Bp[r], B[r]); A[r] *= Ap[r]; }
-    }
-    if (lane == 31)
-#pragma unroll
-        for (int r = 0; r < NS; ++r) { tot[kW * (2 * r) + warp] = A[r]; tot[kW * (2 * r + 1) + warp] = B[r]; }
-    double eA[NS], eB[NS];
-#pragma unroll
-    for (int r = 0; r < NS; ++r) {
-        eA[r] = __shfl_up_sync(FULL, A[r], 1);
-        eB[r] = __shfl_up_sync(FULL, B[r], 1);
-        if (lane == 0) { eA[r] = 1.0; eB[r] = 0.0; }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < NS; ++r) {
-        double ta = lane < kW ? tot[kW * (2 * r) + lane] : 1.0, tb = lane < kW ? tot[kW * (2 * r + 1) + lane] : 0.0;
-#pragma unroll
-        for (int st = 1; st < kW; st <<= 1) {
-            const double ap = __shfl_up_sync(FULL, ta, st), bp = __shfl_up_sync(FULL, tb, st);
-            if (lane >= st) { tb = fma(ta, bp, tb); ta *= ap; }
-        }
-        const double cw = __shfl_sync(FULL, tb, (warp + 31) & 31);
-        yb[r] = fma(eA[r], warp > 0 ? cw : 0.0, eB[r]);
-    }
-}
-
-template <int NS>
-__device__ __forceinline__ void scan_bwd_n(const double (&a)[NS], const double (&b)[NS], double (&xa)[NS],
-                                           double* tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double A[NS], B[NS];
-#pragma unroll
-    for (int r = 0; r < NS; ++r) { A[r] = a[r]; B[r] = b[r]; }
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-        double An[NS], Bn[NS];
-#pragma unroll
-        for (int r = 0; r < NS; ++r) { An[r] = __shfl_down_sync(FULL, A[r], st); Bn[r] = __shfl_down_sync(FULL, B[r], st); }
-        if (lane + st < 32)
-#pragma unroll
-            for (int r = 0; r < NS; ++r) { B[r] = fma(A[r], Bn[r], B[r]); A[r] *= An[r]; }
-    }
-    if (lane == 0)
-#pragma unroll
-        for (int r = 0; r < NS; ++r) { tot[kW * (2 * r) + warp] = A[r]; tot[kW * (2 * r + 1) + warp] = B[r]; }
-    double eA[NS], eB[NS];
-#pragma unroll
-    for (int r = 0; r < NS; ++r) {
-        eA[r] = __shfl_down_sync(FULL, A[r], 1);
-        eB[r] = __shfl_down_sync(FULL, B[r], 1);
-        if (lane == 31) { eA[r] = 1.0; eB[r] = 0.0; }
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < NS; ++r) {
-        double ta = lane < kW ? tot[kW * (2 * r) + lane] : 1.0, tb = lane < kW ? tot[kW * (2 * r + 1) + lane] : 0.0;
-#pragma unroll
-        for (int st = 1; st < kW; st <<= 1) {
-            const double an = __shfl_down_sync(FULL, ta, st), bn = __shfl_down_sync(FULL, tb, st);
-            if (lane + st < kW) { tb = fma(ta, bn, tb); ta *= an; }
-        }
-        const double cw = __shfl_sync(FULL, tb, (warp + 1) & 31);
-        xa[r] = fma(eA[r], warp < kW - 1 ? cw : 0.0, eB[r]);
-    }
-}
-
-// Exclusive scan of 2x2 matrix products (later rows on the left) for NS systems: on return
-// (p[s], q[s]) = first column of the product of all matrices before this thread's rows.
-template <int NS>
-__device__ __forceinline__ void scan_pivots(double (&m)[NS][4], double (&p)[NS], double (&q)[NS], double* tot) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-#pragma unroll
-        for (int s = 0; s < NS; ++s) {
-            const double p00 = __shfl_up_sync(FULL, m[s][0], st), p01 = __shfl_up_sync(FULL, m[s][1], st);
-            const double p10 = __shfl_up_sync(FULL, m[s][2], st), p11 = __shfl_up_sync(FULL, m[s][3], st);
-            if (lane >= st) {
-                const double n00 = m[s][0] * p00 + m[s][1] * p10, n01 = m[s][0] * p01 + m[s][1] * p11;
-                const double n10 = m[s][2] * p00 + m[s][3] * p10, n11 = m[s][2] * p01 + m[s][3] * p11;
-                m[s][0] = n00; m[s][1] = n01; m[s][2] = n10; m[s][3] = n11;
-                renorm(m[s][0], m[s][1], m[s][2], m[s][3]);
-            }
-        }
-    }
-    if (lane == 31)
-#pragma unroll
-        for (int s = 0; s < NS; ++s)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) tot[kW * (4 * s + e) + warp] = m[s][e];
-    double ex[NS][4];
-#pragma unroll
-    for (int s = 0; s < NS; ++s)
-#pragma unroll
-        for (int e = 0; e < 4; ++e) ex[s][e] = __shfl_up_sync(FULL, m[s][e], 1);
-    if (lane == 0)
-#pragma unroll
-        for (int s = 0; s < NS; ++s) { ex[s][0] = 1.0; ex[s][1] = 0.0; ex[s][2] = 0.0; ex[s][3] = 1.0; }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < NS; ++s) {
-        double t00 = lane < kW ? tot[kW * (4 * s) + lane] : 1.0, t01 = lane < kW ? tot[kW * (4 * s + 1) + lane] : 0.0;
-        double t10 = lane < kW ? tot[kW * (4 * s + 2) + lane] : 0.0, t11 = lane < kW ? tot[kW * (4 * s + 3) + lane] : 1.0;
-#pragma unroll
-        for (int st = 1; st < kW; st <<= 1) {
-            const double p00 = __shfl_up_sync(FULL, t00, st), p01 = __shfl_up_sync(FULL, t01, st);
-            const double p10 = __shfl_up_sync(FULL, t10, st), p11 = __shfl_up_sync(FULL, t11, st);
-            if (lane >= st) {
-                const double n00 = t00 * p00 + t01 * p10, n01 = t00 * p01 + t01 * p11;
-                const double n10 = t10 * p00 + t11 * p10, n11 = t10 * p01 + t11 * p11;
-                t00 = n00; t01 = n01; t10 = n10; t11 = n11;
-                renorm(t00, t01, t10, t11);
-            }
-        }
-        const int src = (warp + 31) & 31;
-        double c00 = __shfl_sync(FULL, t00, src), c10 = __shfl_sync(FULL, t10, src);
-        if (warp == 0) { c00 = 1.0; c10 = 0.0; }
-        // column 0 of (within-warp exclusive product) x (carry of the earlier warps)
-        p[s] = ex[s][0] * c00 + ex[s][1] * c10;
-        q[s] = ex[s][2] * c00 + ex[s][3] * c10;
-    }
-}
-
-// ---------------------------------------------------------------- batched shared-memory adds
-// All NA updates of one thread are issued together (independent compare-and-swap rounds) instead
-// of one serialised atomic loop per address. Lock-free: every round at least one contender of
-// each address succeeds, so the loop ends after at most one round per contender.
-template <int NA>
-__device__ __forceinline__ void add_multi(double* const (&p)[NA], const double (&v)[NA]) {
-    unsigned long long old[NA];
-#pragma unroll
-    for (int i = 0; i < NA; ++i) old[i] = __double_as_longlong(*reinterpret_cast<volatile double*>(p[i]));
-    unsigned pend = (1u << NA) - 1u;
-    for (int round = 0; pend && round < 4 * kThreads; ++round) {
-#pragma unroll
-        for (int i = 0; i < NA; ++i)
-            if (pend & (1u << i)) {
-                const unsigned long long nv = __double_as_longlong(__longlong_as_double(old[i]) + v[i]);
-                const unsigned long long got = atomicCAS(reinterpret_cast<unsigned long long*>(p[i]), old[i], nv);
-                if (got == old[i]) pend &= ~(1u << i); else old[i] = got;
-            }
-    }
-}
-
-// Warp aggregation of deposits: lanes holding contributions to the same cell form runs of equal
-// keys in lane order (plasma particles stay close to their radial loading order); a segmented
-// warp-shuffle scan sums each run, and only the last lane of a run updates shared memory. Runs
-// split by reordering only cost extra updates, never correctness. Blowout piles tens of particles
-// into a few sheath or axis cells, where per-particle updates of the same word would serialise.
-template <int NV>
-__device__ __forceinline__ bool warp_runs_sum(int key, double (&v)[NV]) {
-    const int lane = threadIdx.x & 31;
-    const int kprev = __shfl_up_sync(FULL, key, 1);
-    const bool head = (lane == 0) || (kprev != key);
-    const unsigned heads = __ballot_sync(FULL, head);
-    if (heads == FULL) return true;                   // no shared cell in this warp
-    const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
-        const int sp = __shfl_up_sync(FULL, seg, st);
-        double vp[NV];
-#pragma unroll
-        for (int i = 0; i < NV; ++i) vp[i] = __shfl_up_sync(FULL, v[i], st);
-        if (lane >= st && sp == seg)
-#pragma unroll
-            for (int i = 0; i < NV; ++i) v[i] += vp[i];
-    }
-    const int knext = __shfl_down_sync(FULL, key, 1);
-    return (lane == 31) || (knext != key);
-}
-
-// ---------------------------------------------------------------- shared-memory layout
-struct Src {                                              // plasma + beam sources of one slice
-    double *rhot, *drho, *jz, *chi, *ne, *ni, *jpi1, *S1r, *S1i;
-};
-
-struct Smem {
-    double *r, *iv, *ih;                                  // grid
-    const double *gm, *g0, *gp, *ir;                      // gradient stencils, 1/r
-    const double *l0r, *l0f, *l0b;                        // L0 Thomas: 1/u, -a/u, -c/u
-    const double *l1a, *l1b, *l1c, *lfa, *lfb, *lfc;      // L1D and L1F rows
-    double* src0;                                         // sources: 9 arrays, twice when A.dbuf
-    double *bgt, *bgr;                                    // neutralising background
-    double *psi, *ez, *bz, *wr1, *bpr, *bpi;              // fields of the slice (wr1 = -psi')
-    double* tot;                                          // scan scratch, 2 x 8 x kW
-    int* lost;
-};
-
-__device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
-    const int M = A.M;
-    Smem S;
-    double* p = base;
-    S.r = p; p += M; S.iv = p; p += M; S.ih = p; p += M;
-    const double* q = A.const_smem ? p : A.consts;
-    S.gm = q; S.g0 = q + M; S.gp = q + 2 * M; S.ir = q + 3 * M;
-    S.l0r = q + 4 * M; S.l0f = q + 5 * M; S.l0b = q + 6 * M;
-    S.l1a = q + 7 * M; S.l1b = q + 8 * M; S.l1c = q + 9 * M;
-    S.lfa = q + 10 * M; S.lfb = q + 11 * M; S.lfc = q + 12 * M;
-    if (A.const_smem) p += 13 * (size_t)M;
-    S.src0 = p;
-    p += (A.dbuf ? 18 : 9) * (size_t)M;
-    S.bgt = p; p += M; S.bgr = p; p += M;
-    S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.wr1 = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
-    S.tot = p; p += 2 * 8 * kW;
-    S.lost = reinterpret_cast<int*>(p);
-    return S;
-}
-
-__device__ __forceinline__ Src src_of(const Smem& S, int M, int b) {
-    double* p = S.src0 + (size_t)b * 9 * M;
-    Src s;
-    s.rhot = p; s.drho = p + M; s.jz = p + 2 * M; s.chi = p + 3 * M; s.ne = p + 4 * M;
-    s.ni = p + 5 * M; s.jpi1 = p + 6 * M; s.S1r = p + 7 * M; s.S1i = p + 8 * M;
-    return s;
-}
-
-// beam source values of slice k at node j needed by the m = 0 sweep (src/Simulation.cpp:420-441):
-// rho - J_z, its xi-derivative (central / one-sided, or backward for ngp), J_z, J_theta
-struct BeamRow { double rt, drt, jz, jt; };
-
-__device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, int k, int j) {
-    const size_t st = (size_t)A.M * B_NC0;
-    const double* bk = A.bsrc + (size_t)k * st + (size_t)j * B_NC0;
-    BeamRow r;
-    r.rt = bk[B_RT0];
-    r.jz = bk[B_JZ0];
-    r.jt = bk[B_JP1I];
-    const int K = A.K;
-    if (A.ngp) {
-        const double prev = (k > 0) ? bk[B_RT0 - (ptrdiff_t)st] : 0.0;
-        r.drt = (r.rt - prev) * A.idxi;
-    } else if (K == 1) {
-        r.drt = 0.0;
-    } else if (k == 0) {
-        r.drt = (bk[st + B_RT0] - r.rt) * A.idxi;
-    } else if (k == K - 1) {
-        r.drt = (r.rt - bk[B_RT0 - (ptrdiff_t)st]) * A.idxi;
-    } else {
-        r.drt = 0.5 * (bk[st + B_RT0] - bk[B_RT0 - (ptrdiff_t)st]) * A.idxi;
-    }
-    return r;
-}
-
-// initial source values of a slice: background + beam; the plasma deposit is added on top
-__device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j, const BeamRow& br) {
-    s.rhot[j] = S.bgt[j] + br.rt;
-    s.drho[j] = br.drt;
-    s.jz[j] = br.jz;
-    s.jpi1[j] = br.jt;
-    s.chi[j] = 0.0;
-    s.ne[j] = 0.0;
-    s.ni[j] = S.bgr[j] > 0.0 ? S.bgr[j] : 0.0;
-    s.S1r[j] = 0.0;
-    s.S1i[j] = 0.0;
-}
-
-// 3-point non-uniform gradient at node i (src/FieldSolver.cpp:263-281); odd: axis value f1/r1
-__device__ __forceinline__ double grad_at(const Smem& S, int N, const double* f, int i, bool odd) {
-    if (i == 0) return odd ? f[1] * S.ir[0] : 0.0;
-    if (i == N) return S.g0[N] * f[N] + S.gm[N] * f[N - 1] + S.gp[N] * f[N - 2];
-    return S.gm[i] * f[i - 1] + S.g0[i] * f[i] + S.gp[i] * f[i + 1];
-}
-
-// cell of x starting from a guess (the previous cell): walks for small moves, bisects otherwise;
-// the same cell as locate() (src/RadialGrid.hpp:73-82) for every x
-__device__ __forceinline__ int locate_from(const double* __restrict__ r, int N, double R, double x, int j) {
-    if (x <= 0.0) return 0;
-    if (x >= R) return N - 1;
-    j = j < 0 ? 0 : (j > N - 1 ? N - 1 : j);
-#pragma unroll 1
-    for (int step = 0; step < 3; ++step) {
-        if (r[j] > x) { if (j == 0) break; --j; continue; }
-        if (r[j + 1] <= x) { if (j == N - 1) break; ++j; continue; }
-        return j;
-    }
-    if (r[j] <= x && x < r[j + 1]) return j;
-    return locate(r, N, R, x);
-}
-
-// ---------------------------------------------------------------- one plasma particle
-// history h[m] holds the force m pushes ago (h[0] newest): the reference's ring buffer
-// (src/PlasmaSpecies.cpp:621-632) with the slot rotation done by moving values.
-template <int ORD>
-struct PState {
-    double x, y, px, py, dl, w;
-    double h[ORD][5];
-    double q, qm;
-};
-
-template <int ORD>
-__device__ __forceinline__ void pload(PState<ORD>& P, const double* __restrict__ ps, int npad, int p) {
-    P.x = ps[p]; P.y = ps[npad + p]; P.px = ps[2 * (size_t)npad + p]; P.py = ps[3 * (size_t)npad + p];
-    P.dl = ps[4 * (size_t)npad + p]; P.w = ps[5 * (size_t)npad + p];
-#pragma unroll
-    for (int m = 0; m < ORD; ++m)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) P.h[m][v] = ps[(6 + (size_t)m * 5 + v) * npad + p];
-}
-
-template <int ORD>
-__device__ __forceinline__ void pstore(const PState<ORD>& P, double* __restrict__ ps, int npad, int p) {
-    ps[p] = P.x; ps[npad + p] = P.y; ps[2 * (size_t)npad + p] = P.px; ps[3 * (size_t)npad + p] = P.py;
-    ps[4 * (size_t)npad + p] = P.dl; ps[5 * (size_t)npad + p] = P.w;
-#pragma unroll
-    for (int m = 0; m < ORD; ++m)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) ps[(6 + (size_t)m * 5 + v) * npad + p] = P.h[m][v];
-}
-
-__device__ __forceinline__ void species_params(const SweepArgs& A, int p, double& q, double& qm) {
-    int s = 0;
-    while (s + 1 < A.nsp && p >= A.sp_off[s + 1]) ++s;
-    q = A.sp_q[s];
-    qm = A.sp_qm[s];
-}
-
-// W+ mode 1 at the particle: lin(w1), w1 = -psi' (src/Simulation.cpp:477-498)
-__device__ __forceinline__ double w1_at(const Smem& S, int N, const PGeo& g) { return lin(S.wr1, g); }
-
-// src/PlasmaSpecies.cpp:409-478, m = 0 (plasma rho and J_r feed nothing on this path: not deposited).
-// Contributions of one particle to nodes j (v[0..5]) and j+1 (v[6..11]): rho - J_z, d/dxi, J_z, chi,
-// density, J_theta.
-template <int ORD>
-__device__ __forceinline__ void deposit_values(const PState<ORD>& P, const PGeo& g, const Smem& S, double (&v)[12]) {
-    const double PX = P.px, PY = P.py, D = P.dl, w = P.w;
-    const double gam = (1.0 + PX * PX + PY * PY + D * D) / (2.0 * D);
-    const double invd = 1.0 / D;
-    const double pz = gam - D;
-    const double ux = PX * invd, uy = PY * invd;
-    const double ur = g.c * ux + g.s * uy, uth = g.c * uy - g.s * ux;
-    const double wq = w * P.q;
-#pragma unroll
-    for (int cc = 0; cc < 2; ++cc) {
-        const int jj = g.j + cc;
-        const double iv = S.iv[jj];
-        const double Wc = cc ? g.W1 : g.W0;
-        const double dWc = cc ? g.ih : -g.ih;
-        const double a = wq * Wc * iv;
-        const double dr = wq * ur * dWc * iv;
-        const double vjz = a * pz * invd, vchi = a * P.qm * invd;
-        const double vn = w * Wc * iv * gam * invd;
-        v[6 * cc + 0] = a;
-        v[6 * cc + 1] = dr;
-        v[6 * cc + 2] = vjz;
-        v[6 * cc + 3] = vchi;
-        v[6 * cc + 4] = vn;
-        v[6 * cc + 5] = a * uth;
-    }
-}
-
-// warp-wide: every lane calls it (active = the lane has a particle); key = 2 j + (positive species)
-__device__ __forceinline__ void deposit_warp(bool active, int j, bool neg, double (&v)[12], const Src& s) {
-    const int lane = threadIdx.x & 31;
-    if (!active)
-#pragma unroll
-        for (int i = 0; i < 12; ++i) v[i] = 0.0;
-    const int key = active ? 2 * j + (neg ? 0 : 1) : -1 - lane;
-    if (warp_runs_sum<12>(key, v) && active) {
-        double* dens = neg ? s.ne : s.ni;
-        double* adr[12];
-#pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-            const int jj = j + cc;
-            adr[6 * cc + 0] = s.rhot + jj;
-            adr[6 * cc + 1] = s.drho + jj;
-            adr[6 * cc + 2] = s.jz + jj;
-            adr[6 * cc + 3] = s.chi + jj;
-            adr[6 * cc + 4] = dens + jj;
-            adr[6 * cc + 5] = s.jpi1 + jj;
-        }
-        add_multi<12>(adr, v);
-    }
-}
-
-// src/PlasmaSpecies.cpp:508-559, m = 0: S+ contributions to nodes j (v[0..1]) and j+1 (v[2..3])
-template <int ORD>
-__device__ __forceinline__ void depositS_values(const PState<ORD>& P, const PGeo& g, const Smem& S, int N,
-                                                double (&v)[4]) {
-    const double qm = P.qm;
-    const double PX = P.px, PY = P.py, D = P.dl;
-    const double r1 = w1_at(S, N, g);
-    const double Wx = r1 * g.c - 0.0 * g.s, Wy = r1 * g.s + 0.0 * g.c;
-    const double Ez = lin(S.ez, g), Bz = lin(S.bz, g);
-    const double gam = (1.0 + PX * PX + PY * PY + D * D) / (2.0 * D);
-    const double invd = 1.0 / D;
-    const double ux = PX * invd, uy = PY * invd;
-    const double ur = g.c * ux + g.s * uy, uth = g.c * uy - g.s * ux;
-    const double dD = qm * ((PX * Wx + PY * Wy) * invd - Ez);
-    const double ax = (qm * (gam * Wx + PY * Bz) * invd) * invd - PX * dD * invd * invd;
-    const double ay = (qm * (gam * Wy - PX * Bz) * invd) * invd - PY * dD * invd * invd;
-    const double wq = P.w * P.q;
-#pragma unroll
-    for (int cc = 0; cc < 2; ++cc) {
-        const int jj = g.j + cc;
-        const double iv = S.iv[jj] * wq;
-        const double Wc = cc ? g.W1 : g.W0;
-        const double dWc = cc ? g.ih : -g.ih;
-        const double Worc = cc ? g.Wor1 : g.Wor0;
-        double Ar = ax * Wc + ux * ur * dWc;
-        double Ai = ay * Wc + uy * ur * dWc;
-        const double f2 = uth * Worc;
-        Ar += f2 * uy;
-        Ai -= f2 * ux;
-        v[2 * cc] = iv * (Ar * g.c + Ai * g.s);
-        v[2 * cc + 1] = iv * (Ai * g.c - Ar * g.s);
-    }
-}
-
-__device__ __forceinline__ void depositS_warp(bool active, int j, double (&v)[4], const Src& s) {
-    const int lane = threadIdx.x & 31;
-    if (!active)
-#pragma unroll
-        for (int i = 0; i < 4; ++i) v[i] = 0.0;
-    const int key = active ? j : -1 - lane;
-    if (warp_runs_sum<4>(key, v) && active) {
-        double* adr[4] = {s.S1r + j, s.S1i + j, s.S1r + j + 1, s.S1i + j + 1};
-        add_multi<4>(adr, v);
-    }
-}
-
-// src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns false
-// when the particle is removed (trapped or beyond the wall)
-template <int ORD>
-__device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, const Smem& S, const SweepArgs& A,
-                                              bool first) {
-    const double qm = P.qm;
-    const double X = P.x, Y = P.y, PX = P.px, PY = P.py, D = P.dl;
-    const double r1 = w1_at(S, A.N, g);
-    const double Wx = r1 * g.c - 0.0 * g.s, Wy = r1 * g.s + 0.0 * g.c;
-    const double Ez = lin(S.ez, g), Bz = lin(S.bz, g);
-    const double br = lin(S.bpr, g), bi = lin(S.bpi, g);
-    const double Bx = br * g.c - bi * g.s, By = br * g.s + bi * g.c;
-    const double gam = (1.0 + PX * PX + PY * PY + D * D) / (2.0 * D);
-    const double invd = 1.0 / D;
-    double fv[5];
-    fv[0] = PX * invd;
-    fv[1] = PY * invd;
-    fv[2] = qm * (gam * Wx * invd + By + PY * Bz * invd);
-    fv[3] = qm * (gam * Wy * invd - Bx - PX * Bz * invd);
-    fv[4] = qm * ((PX * Wx + PY * Wy) * invd - Ez);
-    if (first) {
-#pragma unroll
-        for (int m = 0; m < ORD; ++m)
-#pragma unroll
-            for (int v = 0; v < 5; ++v) P.h[m][v] = fv[v];
-    } else {
-#pragma unroll
-        for (int m = ORD - 1; m > 0; --m)
-#pragma unroll
-            for (int v = 0; v < 5; ++v) P.h[m][v] = P.h[m - 1][v];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) P.h[0][v] = fv[v];
-    }
-    double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int m = 0; m < ORD; ++m) {
-        const double cm = A.ab[m];
-#pragma unroll
-        for (int v = 0; v < 5; ++v) sum[v] += cm * P.h[m][v];
-    }
-    const double dxi = A.dxi;
-    double xn = X + dxi * sum[0], yn = Y + dxi * sum[1];
-    double pxn = PX + dxi * sum[2], pyn = PY + dxi * sum[3];
-    const double dn = D + dxi * sum[4];
-    const double gn = (1.0 + pxn * pxn + pyn * pyn + dn * dn) / (2.0 * dn);
-    if (!(dn > A.delta_min) || gn > A.max_qsa * dn) {
-        P.w = 0.0;
-        return false;
-    }
-    const double R = A.R;
-    const double rn = sqrt(xn * xn + yn * yn);
-    if (rn > R) {                    // specular reflection at the wall, incl. the history
-        const double nx = xn / rn, ny = yn / rn;
-        const double rr = 2.0 * R - rn;
-        if (rr < 0.0) { P.w = 0.0; return false; }
-        xn = nx * rr; yn = ny * rr;
-        const double pn = pxn * nx + pyn * ny;
-        pxn -= 2.0 * pn * nx; pyn -= 2.0 * pn * ny;
-#pragma unroll
-        for (int m = 0; m < ORD; ++m) {
-            const double a = P.h[m][0] * nx + P.h[m][1] * ny;
-            P.h[m][0] -= 2.0 * a * nx; P.h[m][1] -= 2.0 * a * ny;
-            const double b = P.h[m][2] * nx + P.h[m][3] * ny;
-            P.h[m][2] -= 2.0 * b * nx; P.h[m][3] -= 2.0 * b * ny;
-        }
-    }
-    P.x = xn; P.y = yn; P.px = pxn; P.py = pyn; P.dl = dn;
-    return true;
-}
-
-// right-hand sides of the psi, E_z, B_z systems at row i (src/Simulation.cpp:798-799, :517-527)
-__device__ __forceinline__ void rhs_l0(const Smem& S, const Src& s, int N, int i, double& d0, double& d1,
-                                       double& d2) {
-    d0 = d1 = d2 = 0.0;
-    if (i < N) {
-        d0 = -1.0 * s.rhot[i];
-        d1 = -1.0 * s.drho[i];
-        const double t1 = grad_at(S, N, s.jpi1, i, true);
-        const double t2 = (i == 0 ? s.jpi1[1] : s.jpi1[i]) * S.ir[i];
-        d2 = 1.0 * (-(t1 + t2));
-    }
-}
-
-// row i of (L1D - chi) (sys 0) and (L1F - chi) (sys 1) with its right-hand side
-// (src/FieldSolver.cpp:242-261, src/Simulation.cpp:535-591)
-__device__ __forceinline__ void row_b(const Smem& S, const Src& s, int N, double fc, int sys, int i, double& a,
-                                      double& b, double& cm, double& d) {
-    if (sys == 0) {
-        a = S.l1a[i]; b = S.l1b[i]; cm = i > 0 ? S.l1c[i - 1] : 0.0;
-        if (i >= 1 && i < N) { b = b - s.chi[i]; d = 1.0 * (-s.S1i[i]); } else { d = 0.0; }
-    } else {
-        a = S.lfa[i]; b = S.lfb[i]; cm = i > 0 ? S.lfc[i - 1] : 0.0;
-        if (i >= 1) {
-            b = b - s.chi[i];
-            d = 1.0 * (grad_at(S, N, s.jz, i, false) + s.S1r[i]);
-            if (i == N) d -= fc * s.jz[N];
-        } else {
-            d = 0.0;
-        }
-    }
-}
-
-}  // namespace
-
 template <int ORD, bool REG, int kMaxR>
-__global__ void __launch_bounds__(kThreads, 1) sweep_m0_kernel(const SweepArgs A) {
+__global__ void __launch_bounds__(kSweepThreads, 1) sweep_m0_kernel(const SweepArgs A) {
     extern __shared__ double smem_raw[];
-    const int M = A.M, N = A.N, K = A.K, Rw = kMaxR == 1 ? 1 : A.rows_per_thread;   // rows per thread
-    const int tid = threadIdx.x;
-    const Smem S = carve(smem_raw, A);
-    const int np = A.np, npad = A.npad;
-    const double R = A.R;
-    const int row0 = tid * Rw;                                  // this thread's rows [row0, row0 + Rw)
-    unsigned long long* tim = A.timing;
-    long long t_prev = 0, t_sub = 0;
-    if (tim && tid == 0) t_prev = clock64();
-#define PHASE_MARK(ph)                                                        \
-    do {                                                                      \
-        if (tim && tid == 0) {                                                \
-            const long long tn = clock64();                                   \
-            tim[ph] += (unsigned long long)(tn - t_prev);                     \
-            t_prev = tn;                                                      \
-        }                                                                     \
-    } while (0)
-#define SUB_MARK(slot)                                                        \
-    do {                                                                      \
-        if (tim && tid == 0) {                                                \
-            const long long tn = clock64();                                   \
-            tim[slot] += (unsigned long long)(tn - t_sub);                    \
-            t_sub = tn;                                                       \
-        }                                                                     \
-    } while (0)
-
-    // ---------------- prologue: grid, operators, fresh plasma, background (src/Simulation.cpp:653-708)
-    for (int j = tid; j < M; j += kThreads) {
-        S.r[j] = A.r[j];
-        S.iv[j] = A.inv_V[j];
-        S.ih[j] = (j < N) ? A.inv_h[j] : 0.0;
-        S.bgt[j] = 0.0;
-        S.bgr[j] = 0.0;
-        S.bpr[j] = 0.0;
-        S.bpi[j] = 0.0;
-        src_of(S, M, 0).ne[j] = 0.0;
-    }
-    if (A.const_smem)
-        for (int t = tid; t < 13 * M; t += kThreads) const_cast<double*>(S.gm)[t] = A.consts[t];
-    if (tid == 0) *S.lost = 0;
-    PState<ORD> P;
-    int J = 0;                                             // cell of the thread's particle
-    if (REG) {
-        if (tid < np) {
-            P.x = A.p_init[tid]; P.y = A.p_init[npad + tid]; P.px = A.p_init[2 * npad + tid];
-            P.py = A.p_init[3 * npad + tid]; P.dl = A.p_init[4 * npad + tid]; P.w = A.p_init[5 * npad + tid];
-#pragma unroll
-            for (int m = 0; m < ORD; ++m)
-#pragma unroll
-                for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
-            species_params(A, tid, P.q, P.qm);
-        } else {
-            P.x = P.y = P.px = P.py = 0.0;
-            P.dl = 1.0;
-            P.w = 0.0;
-            P.q = P.qm = -1.0;
-#pragma unroll
-            for (int m = 0; m < ORD; ++m)
-#pragma unroll
-                for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
-        }
-    } else {
-        for (int p = tid; p < np; p += kThreads) {
-#pragma unroll
-            for (int v = 0; v < 6; ++v) A.ps[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
-            for (int v = 0; v < 5 * ORD; ++v) A.ps[(size_t)(6 + v) * npad + p] = 0.0;
-        }
-    }
-    __syncthreads();
-    // immobile species deposit into the background; mobile ones are subtracted (neutralisation,
-    // src/Simulation.cpp:672-684); src[0].ne is the scratch of the mobile deposit
-    for (int p = tid; p < A.nbg; p += kThreads) {
-        const double x = A.bg_p[p], y = A.bg_p[A.nbg + p], wq = A.bg_p[2 * A.nbg + p];
-        if (wq == 0.0) continue;
-        const PGeo g = geometry(S.r, S.ih, N, R, x, y);
-        const double a0 = wq * g.W0 * S.iv[g.j], a1 = wq * g.W1 * S.iv[g.j + 1];
-        double* adr[4] = {S.bgt + g.j, S.bgr + g.j, S.bgt + g.j + 1, S.bgr + g.j + 1};
-        const double val[4] = {a0, a0, a1, a1};
-        add_multi<4>(adr, val);
-    }
-    if (A.neutralize) {
-        double* ne0 = src_of(S, M, 0).ne;
-        for (int p = tid; p < np; p += kThreads) {
-            const double w = A.p_init[5 * (size_t)npad + p];
-            if (w == 0.0) continue;
-            double q, qm;
-            species_params(A, p, q, qm);
-            const PGeo g = geometry(S.r, S.ih, N, R, A.p_init[p], A.p_init[npad + p]);
-            double* adr[2] = {ne0 + g.j, ne0 + g.j + 1};
-            const double val[2] = {w * q * g.W0 * S.iv[g.j], w * q * g.W1 * S.iv[g.j + 1]};
-            add_multi<2>(adr, val);
-        }
-    }
-    __syncthreads();
-    for (int j = tid; j < M; j += kThreads) {
-        const Src s0 = src_of(S, M, 0);
-        if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
-        init_sources(s0, S, j, beam_row(A, 0, j));
-    }
-    __syncthreads();
-    // deposit of slice 0
-    const int lane = tid & 31;
-    if (REG) {
-        const bool act = tid < np && P.w != 0.0;
-        double v[12];
-        if (act) {
-            const PGeo G = geometry(S.r, S.ih, N, R, P.x, P.y);
-            J = G.j;
-            deposit_values(P, G, S, v);
-        }
-        deposit_warp(act, J, P.q < 0.0, v, src_of(S, M, 0));
-    } else {
-        for (int base = tid - lane; base < np; base += kThreads) {
-            const int p = base + lane;
-            PState<ORD> Q;
-            bool act = false;
-            int j = 0;
-            double v[12];
-            if (p < np) {
-                pload(Q, A.ps, npad, p);
-                species_params(A, p, Q.q, Q.qm);
-                act = Q.w != 0.0;
-                if (act) {
-                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                    j = g.j;
-                    deposit_values(Q, g, S, v);
-                }
-            }
-            deposit_warp(act, j, act && Q.q < 0.0, v, src_of(S, M, 0));
-        }
-    }
-    __syncthreads();
-    PHASE_MARK(0);
-
-    int scan_par = 0;                                            // alternates the scan scratch
-    const double fc = A.flux_coef;
-    for (int k = 0; k < K; ++k) {
-        const Src s = src_of(S, M, A.dbuf ? (k & 1) : 0);
-        const Src sn = src_of(S, M, A.dbuf ? ((k + 1) & 1) : 0);
-        if (tim && tid == 0) t_sub = clock64();
-        // beam rows of slice k+1 for this thread's nodes (consumed below, latency overlaps the solves)
-        BeamRow pre[kMaxR];
-        if (A.dbuf && k + 1 < K)
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u)
-                if (u < Rw && row0 + u < M) pre[u] = beam_row(A, k + 1, row0 + u);
-
-        // ---------------- P2: psi, E_z, B_z with L0 (src/Simulation.cpp:797-807, :501-532)
-        {
-            // forward: y_i = (-a_i/u_i) y_{i-1} + d_i/u_i
-            double cA = 1.0, cB[3] = {0.0, 0.0, 0.0};
-            double dv[kMaxR][3];
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-                dv[u][0] = dv[u][1] = dv[u][2] = 0.0;
-                if (u >= Rw || i >= M) continue;
-                rhs_l0(S, s, N, i, dv[u][0], dv[u][1], dv[u][2]);
-                const double rr = S.l0r[i], af = S.l0f[i];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) cB[e] = fma(af, cB[e], rr * dv[u][e]);
-                cA *= af;
-            }
-            SUB_MARK(5);
-            double yb[3];
-            scan_fwd<3>(cA, cB, yb, S.tot + (scan_par++ & 1) * 8 * kW);
-            SUB_MARK(6);
-            const double ypsi_prev = yb[0];                         // y of psi just before this thread's rows
-            double y[kMaxR][3];
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-                y[u][0] = y[u][1] = y[u][2] = 0.0;
-                if (u >= Rw || i >= M) continue;
-                const double rr = S.l0r[i], af = S.l0f[i];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) { yb[e] = fma(af, yb[e], rr * dv[u][e]); y[u][e] = yb[e]; }
-            }
-            // backward: x_i = (-c_i/u_i) x_{i+1} + y_i
-            double bA = 1.0, bB[3] = {0.0, 0.0, 0.0};
-#pragma unroll
-            for (int u = kMaxR - 1; u >= 0; --u) {
-                const int i = row0 + u;
-                if (u >= Rw || i >= M) continue;
-                const double ab = S.l0b[i];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) bB[e] = fma(ab, bB[e], y[u][e]);
-                bA *= ab;
-            }
-            double xa[3];
-            scan_bwd<3>(bA, bB, xa, S.tot + (scan_par++ & 1) * 8 * kW);
-            SUB_MARK(7);
-            // psi on the window [row0 - 1, row0 + Rw]: the rows of this thread, x after them (the
-            // backward carry) and x before them, x_{row0-1} = y_{row0-1} - (c/u)_{row0-1} x_{row0}
-            // with y_{row0-1} the forward carry -- so W+ = -psi' needs no further exchange
-            double pw[kMaxR + 2];
-            pw[kMaxR + 1] = 0.0;
-            {
-                double xr = xa[0];
-#pragma unroll
-                for (int u = kMaxR; u >= 1; --u) pw[u] = 0.0;
-                const int last = (row0 + Rw <= M ? Rw : M - row0);
-                if (last >= 0) pw[last + 1 > kMaxR + 1 ? kMaxR + 1 : last + 1] = xr;
-            }
-#pragma unroll
-            for (int u = kMaxR - 1; u >= 0; --u) {
-                const int i = row0 + u;
-                if (u >= Rw || i >= M) continue;
-                const double ab = S.l0b[i];
-#pragma unroll
-                for (int e = 0; e < 3; ++e) xa[e] = fma(ab, xa[e], y[u][e]);
-                S.psi[i] = xa[0];
-                S.ez[i] = xa[1];
-                S.bz[i] = xa[2];
-                pw[u + 1] = xa[0];
-            }
-            pw[0] = (row0 >= 1 && row0 < M) ? fma(S.l0b[row0 - 1], pw[1], ypsi_prev) : 0.0;
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-                if (u >= Rw || i >= M) continue;
-                if (i == 0) {
-                    S.wr1[0] = -0.0;
-                } else if (i < N) {
-                    S.wr1[i] = -(S.gm[i] * pw[u] + S.g0[i] * pw[u + 1] + S.gp[i] * pw[u + 2]);
-                }
-                if (i == N - 1) {                                  // the one-sided wall stencil needs psi_{N-2..N}
-                    S.wr1[N] = -(S.g0[N] * pw[u + 2] + S.gm[N] * pw[u + 1] + S.gp[N] * pw[u]);
-                }
-            }
-            if (A.dbuf && k + 1 < K)
-#pragma unroll
-                for (int u = 0; u < kMaxR; ++u)
-                    if (u < Rw && row0 + u < M) init_sources(sn, S, row0 + u, pre[u]);
-            SUB_MARK(8);
-        }
-        __syncthreads();
-        PHASE_MARK(1);
-
-        // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559)
-        if (REG) {
-            const bool act = tid < np && P.w != 0.0;
-            double v[4];
-            if (act) depositS_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, N, v);
-            depositS_warp(act, J, v, s);
-        } else {
-            for (int base = tid - lane; base < np; base += kThreads) {
-                const int p = base + lane;
-                bool act = false;
-                int j = 0;
-                double v[4];
-                if (p < np) {
-                    PState<ORD> Q;
-                    pload(Q, A.ps, npad, p);
-                    species_params(A, p, Q.q, Q.qm);
-                    act = Q.w != 0.0;
-                    if (act) {
-                        const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                        j = g.j;
-                        depositS_values(Q, g, S, N, v);
-                    }
-                }
-                depositS_warp(act, j, v, s);
-            }
-        }
-        __syncthreads();
-        PHASE_MARK(2);
-
-        // ---------------- P4: B+ (src/Simulation.cpp:535-591, m = 0: one pass)
-        //   (L1D - chi) B_r0 = -S_i (rows 0, N Dirichlet); (L1F - chi) B_theta0 = J_z' + S_r, flux wall J_z(R)
-        {
-            // pivots: product of T_i = [[b_i, -a_i c_{i-1}], [1, 0]] over the thread's rows
-            double m[2][4];
-#pragma unroll
-            for (int sy = 0; sy < 2; ++sy) { m[sy][0] = 1.0; m[sy][1] = 0.0; m[sy][2] = 0.0; m[sy][3] = 1.0; }
-            double ra[kMaxR][2], rb[kMaxR][2], rc[kMaxR][2], rd[kMaxR][2];
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-#pragma unroll
-                for (int sy = 0; sy < 2; ++sy) {
-                    ra[u][sy] = 0.0; rb[u][sy] = 1.0; rc[u][sy] = 0.0; rd[u][sy] = 0.0;
-                    if (u >= Rw || i >= M) continue;
-                    row_b(S, s, N, fc, sy, i, ra[u][sy], rb[u][sy], rc[u][sy], rd[u][sy]);
-                    const double t01 = -ra[u][sy] * rc[u][sy];
-                    const double n00 = rb[u][sy] * m[sy][0] + t01 * m[sy][2];
-                    const double n01 = rb[u][sy] * m[sy][1] + t01 * m[sy][3];
-                    m[sy][2] = m[sy][0]; m[sy][3] = m[sy][1];
-                    m[sy][0] = n00; m[sy][1] = n01;
-                    renorm(m[sy][0], m[sy][1], m[sy][2], m[sy][3]);
-                }
-            }
-            double pp[2], qq[2];
-            scan_pivots<2>(m, pp, qq, S.tot + (scan_par++ & 1) * 8 * kW);
-            // this thread's pivots (rc holds c_{i-1}; rinv = 1/u_i = p_{i-1}/p_i), forward composites
-            double rinv[kMaxR][2];
-            double fA[2] = {1.0, 1.0}, fB[2] = {0.0, 0.0};
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-#pragma unroll
-                for (int sy = 0; sy < 2; ++sy) {
-                    rinv[u][sy] = 0.0;
-                    if (u >= Rw || i >= M) continue;
-                    const double pn = rb[u][sy] * pp[sy] - ra[u][sy] * rc[u][sy] * qq[sy];
-                    qq[sy] = pp[sy];
-                    pp[sy] = pn;
-                    const double rr = qq[sy] / pp[sy];
-                    const double sc = fabs(pp[sy]);
-                    if (sc > 1e100 || sc < 1e-100) { pp[sy] /= sc; qq[sy] /= sc; }
-                    rinv[u][sy] = rr;
-                    const double af = -rr * ra[u][sy];
-                    fB[sy] = fma(af, fB[sy], rr * rd[u][sy]);
-                    fA[sy] *= af;
-                }
-            }
-            // forward substitution of both systems
-            double yy[2];
-            scan_fwd_n<2>(fA, fB, yy, S.tot + (scan_par++ & 1) * 8 * kW);
-            double y[kMaxR][2];
-#pragma unroll
-            for (int u = 0; u < kMaxR; ++u) {
-                const int i = row0 + u;
-#pragma unroll
-                for (int sy = 0; sy < 2; ++sy) {
-                    y[u][sy] = 0.0;
-                    if (u >= Rw || i >= M) continue;
-                    yy[sy] = fma(-rinv[u][sy] * ra[u][sy], yy[sy], rinv[u][sy] * rd[u][sy]);
-                    y[u][sy] = yy[sy];
-                }
-            }
-            // backward substitution: x_i = -(c_i / u_i) x_{i+1} + y_i
-            double bA[2] = {1.0, 1.0}, bB[2] = {0.0, 0.0};
-#pragma unroll
-            for (int u = kMaxR - 1; u >= 0; --u) {
-                const int i = row0 + u;
-                if (u >= Rw || i >= M) continue;
-#pragma unroll
-                for (int sy = 0; sy < 2; ++sy) {
-                    const double c = sy ? S.lfc[i] : S.l1c[i];
-                    const double ab = -(c * rinv[u][sy]);
-                    bB[sy] = fma(ab, bB[sy], y[u][sy]);
-                    bA[sy] *= ab;
-                }
-            }
-            double xx[2];
-            scan_bwd_n<2>(bA, bB, xx, S.tot + (scan_par++ & 1) * 8 * kW);
-#pragma unroll
-            for (int u = kMaxR - 1; u >= 0; --u) {
-                const int i = row0 + u;
-                if (u >= Rw || i >= M) continue;
-#pragma unroll
-                for (int sy = 0; sy < 2; ++sy) {
-                    const double c = sy ? S.lfc[i] : S.l1c[i];
-                    xx[sy] = fma(-(c * rinv[u][sy]), xx[sy], y[u][sy]);
-                }
-                S.bpr[i] = xx[0];
-                S.bpi[i] = xx[1];
-            }
-        }
-        __syncthreads();
-        PHASE_MARK(3);
-
-        // ---------------- P5: store slice k; push k -> k+1 and deposit into slice k+1
-        {
-            const size_t fb = (size_t)k * M;
-            for (int j = tid; j < M; j += kThreads) {
-                double* F = A.fld + (fb + j) * F_NC0;
-                F[F_EP1R] = S.wr1[j] + S.bpi[j];
-                F[F_EP1I] = 0.0 - S.bpr[j];
-                F[F_BP1R] = S.bpr[j];
-                F[F_BP1I] = S.bpi[j];
-                F[F_EZ0] = S.ez[j];
-                F[F_BZ0] = S.bz[j];
-                double* D = A.diag + (fb + j) * D_NC0;
-                D[D_PSI0] = S.psi[j];
-                D[D_NE0] = s.ne[j];
-                D[D_NI0] = s.ni[j];
-            }
-        }
-        if (k + 1 < K) {
-            if (!A.dbuf) {
-                __syncthreads();                                    // the store read the sources
-                for (int j = tid; j < M; j += kThreads) init_sources(sn, S, j, beam_row(A, k + 1, j));
-                __syncthreads();
-            }
-            const bool first = (k == 0);
-            if (REG) {
-                bool act = tid < np && P.w != 0.0;
-                double v[12];
-                if (act) {
-                    if (push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first)) {
-                        const double rn = sqrt(P.x * P.x + P.y * P.y);
-                        J = locate_from(S.r, N, R, rn, J);
-                        deposit_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, v);
-                    } else {
-                        act = false;
-                        atomicAdd(S.lost, 1);
-                    }
-                }
-                deposit_warp(act, J, P.q < 0.0, v, sn);
-            } else {
-                for (int base = tid - lane; base < np; base += kThreads) {
-                    const int p = base + lane;
-                    bool act = false;
-                    int j = 0;
-                    double v[12];
-                    PState<ORD> Q;
-                    if (p < np) {
-                        pload(Q, A.ps, npad, p);
-                        species_params(A, p, Q.q, Q.qm);
-                        if (Q.w != 0.0) {
-                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                            if (push_particle(Q, g, S, A, first)) {
-                                const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                                j = g2.j;
-                                deposit_values(Q, g2, S, v);
-                                act = true;
-                            } else {
-                                atomicAdd(S.lost, 1);
-                            }
-                            pstore(Q, A.ps, npad, p);
-                        }
-                    }
-                    deposit_warp(act, j, act && Q.q < 0.0, v, sn);
-                }
-            }
-        }
-        __syncthreads();
-        PHASE_MARK(4);
-    }
-    if (REG && tid < np) pstore(P, A.ps, npad, tid);
-    if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
-#undef PHASE_MARK
-#undef SUB_MARK
+    NoGate g;
+    sweep_body<ORD, REG, kMaxR>(A, smem_raw, g);
 }
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem) {
-    size_t d = (size_t)(3 + 2 + 6 + (dbuf ? 18 : 9)) * M + 2 * 8 * kW;
+    size_t d = (size_t)(3 + 2 + 6 + (dbuf ? 18 : 9)) * M + 2 * 8 * (kSweepThreads / 32);
     if (const_smem) d += 13 * (size_t)M;
     return sizeof(double) * d + 16;
 }
@@ -1149,13 +23,13 @@ cudaError_t launch_t(const SweepArgs& A, size_t smem, cudaStream_t stream) {
     cudaError_t e = cudaFuncSetAttribute(sweep_m0_kernel<ORD, REG, RM>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)smem);
     if (e != cudaSuccess) return e;
-    sweep_m0_kernel<ORD, REG, RM><<<1, kThreads, smem, stream>>>(A);
+    sweep_m0_kernel<ORD, REG, RM><<<1, kSweepThreads, smem, stream>>>(A);
     return cudaGetLastError();
 }
 
 template <int ORD>
 cudaError_t launch_o(const SweepArgs& A, size_t smem, cudaStream_t stream) {
-    const bool reg = A.np <= kThreads;
+    const bool reg = A.np <= kSweepThreads;
     if (A.rows_per_thread == 1)
         return reg ? launch_t<ORD, true, 1>(A, smem, stream) : launch_t<ORD, false, 1>(A, smem, stream);
     return reg ? launch_t<ORD, true, 4>(A, smem, stream) : launch_t<ORD, false, 4>(A, smem, stream);
