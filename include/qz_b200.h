@@ -132,6 +132,16 @@ qz_status qz_beam_push_deposit(const qz_grid* g, qz_beam_view* b, const qz_box* 
                                void* stream);
 /* the 17 moment sums of Beam::sums into out17 (dev); deterministic order */
 qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
+/* qz_beam_sums without any device allocation, for callers that cannot allocate (a host whose
+   device memory all belongs to its own pool allocator; a step loop that cannot take the device-wide
+   synchronisation of cudaFree). No counterpart in the reference: it is an addition of this library.
+   The partial sums live in a static device array of 17 x 592 doubles (80,512 bytes per device),
+   enough for any n: the reduction uses at most 592 blocks. A request for more rows than that fails
+   with QZ_ERR_SIZE. The first call on each device does the set-up (looks up the array's address with
+   that device current) and should be made before any stream capture. Nothing has to be zeroed
+   beforehand. Calls in flight at the same time on one device share the array and race: order
+   them on one stream or serialise them on the host. Same result as qz_beam_sums. */
+qz_status qz_beam_sums_noalloc(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
 
 /* The reference's gaussian generator (Beam::init_gaussian, src/Beam.cpp:483-570) on the host, with
    the same std::mt19937_64 / std::normal_distribution stream. out_host: n x 7 (internal xi).

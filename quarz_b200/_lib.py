@@ -65,6 +65,7 @@ SIGNATURES = {
     "qz_beam_push_deposit": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,
                              C.POINTER(C.c_int), C.c_void_p, C.c_void_p],
     "qz_beam_sums": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
+    "qz_beam_sums_noalloc": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "qz_sample_gaussian": [C.c_double] * 14 + [C.c_int64, C.c_int, C.c_int, C.c_uint64, C.c_double, _dp, _dp, _dp,
                                                C.POINTER(C.c_int64)],
     "qz_sim_create": [C.c_void_p, C.POINTER(SweepParams), C.POINTER(C.c_void_p)],

@@ -181,6 +181,12 @@ class BeamOps:
         v = BeamOps.view(cols, -1.0, 1.0)
         check(lib().qz_beam_sums(C.byref(v), gref, xiref, _dev(out17), _stream_ptr(stream)))
 
+    @staticmethod
+    def sums_noalloc(cols, gref, xiref, out17, stream=None):
+        """qz_beam_sums_noalloc: the same sums with no device allocation (static scratch)."""
+        v = BeamOps.view(cols, -1.0, 1.0)
+        check(lib().qz_beam_sums_noalloc(C.byref(v), gref, xiref, _dev(out17), _stream_ptr(stream)))
+
 
 def sample_gaussian(n0, sr, xi0, sxi, gamma0, espread, emit, cut, cx0, cy0, cxs, cys, xp0, yp0, np_, nrot, mirror,
                     seed, xcut) -> Tuple[np.ndarray, float, float]:

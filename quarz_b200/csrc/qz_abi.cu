@@ -512,6 +512,28 @@ extern "C" qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xir
     return QZ_OK;
 }
 
+// The moment sums for callers that must not allocate device memory: a host whose device memory
+// is all owned by its own pool (every byte handed out by its arena, so a cudaMalloc behind its back
+// can fail or fragment what it reserved), and a step loop that cannot afford the implicit device-
+// wide synchronisation of cudaFree when qz_beam_sums grows its scratch. The partial sums live in a
+// static device array of 17 x 592 doubles; the first call on each device looks up its address.
+extern "C" qz_status qz_beam_sums_noalloc(const qz_beam_view* b, double gref, double xiref, double* out17,
+                                          void* stream) {
+    if (!b || !out17) return fail(QZ_ERR_ARG, "qz_beam_sums_noalloc: null pointer");
+    if (b->n < 0) return fail(QZ_ERR_ARG, "qz_beam_sums_noalloc: negative particle count");
+    qzb::BeamArgs B{};
+    B.x = b->x; B.y = b->y; B.px = b->px; B.py = b->py; B.pz = b->pz; B.xi = b->xi; B.w = b->w;
+    B.n = (long)b->n;
+    int need = 0;
+    const cudaError_t e = qzb::beam_sums_static(B, gref, xiref, out17, (cudaStream_t)stream, &need);
+    if (need > qzb::kSumsStaticBlocks)
+        return fail(QZ_ERR_SIZE, "qz_beam_sums_noalloc: needs " + std::to_string(need) +
+                                     " partial-sum rows, the static scratch holds " +
+                                     std::to_string(qzb::kSumsStaticBlocks));
+    if (e != cudaSuccess) return fail(QZ_ERR_CUDA, std::string("qz_beam_sums_noalloc: ") + cudaGetErrorString(e));
+    return QZ_OK;
+}
+
 extern "C" qz_status qz_sample_gaussian(double n0, double sr, double xi0, double sxi, double gamma0, double espread,
                                         double emit, double cut, double cx0, double cy0, double cxs, double cys,
                                         double xp0, double yp0, int64_t np, int nrot, int mirror, uint64_t seed,

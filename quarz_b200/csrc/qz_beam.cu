@@ -9,6 +9,8 @@
 #include "qz_device.cuh"
 #include "qz_internal.h"
 
+#include <mutex>
+
 namespace qzb {
 
 namespace {
@@ -273,6 +275,45 @@ cudaError_t launch_beam_sums(const BeamArgs& B, double gref, double xiref, doubl
     beam_sums_partial<<<nblocks, kSumThreads, 0, s>>>(B, gref, xiref, partial);
     beam_sums_final<<<1, 32, 0, s>>>(partial, nblocks, out17);
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------- moment sums without allocation
+// Partial-sum scratch of beam_sums_static in static device memory: one 17-double row per block of
+// beam_sums_partial, sized for the block cap of beam_sums_blocks (148 x 4 blocks, 80,512 bytes per
+// device). Every row the final reduction reads is written by the same call first, so nothing in it
+// has to start at zero; two calls in flight at once on one device (other streams, other host
+// threads) share it and race.
+static __device__ __align__(256) double g_sums_static[17 * kSumsStaticBlocks];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_static_mu;
+double* g_static_ptr[kMaxDevices] = {};
+}  // namespace
+
+cudaError_t beam_sums_static(const BeamArgs& B, double gref, double xiref, double* out17, cudaStream_t s,
+                             int* nblocks_needed) {
+    const int nb = beam_sums_blocks(B.n);
+    *nblocks_needed = nb;
+    if (nb > kSumsStaticBlocks) return cudaErrorInvalidValue;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    double* partial = nullptr;
+    {
+        // set-up, once per device, with that device current: the address of this device's copy
+        // of the static scratch (no allocation; the module's static memory already exists)
+        std::lock_guard<std::mutex> lock(g_static_mu);
+        if (!g_static_ptr[dev]) {
+            void* ptr = nullptr;
+            e = cudaGetSymbolAddress(&ptr, g_sums_static);
+            if (e != cudaSuccess) return e;
+            g_static_ptr[dev] = static_cast<double*>(ptr);
+        }
+        partial = g_static_ptr[dev];
+    }
+    return launch_beam_sums(B, gref, xiref, partial, nb, out17, s);
 }
 
 }  // namespace qzb

@@ -71,5 +71,12 @@ cudaError_t launch_beam_push_deposit(const BeamArgs& B, const double* fld, doubl
 cudaError_t launch_beam_sums(const BeamArgs& B, double gref, double xiref, double* partial, int nblocks,
                              double* out17, cudaStream_t s);
 int beam_sums_blocks(long n);
+// Block cap of beam_sums_blocks (148 x 4), the row count of the static scratch of beam_sums_static.
+constexpr int kSumsStaticBlocks = 148 * 4;
+// beam_sums with the partial sums in a static __device__ array instead of caller- or library-
+// allocated memory; the first call on a device looks up that device's address of the array.
+// *nblocks_needed: the rows the call needs (cudaErrorInvalidValue when above kSumsStaticBlocks).
+cudaError_t beam_sums_static(const BeamArgs& B, double gref, double xiref, double* out17, cudaStream_t s,
+                             int* nblocks_needed);
 
 }  // namespace qzb
