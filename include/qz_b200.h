@@ -162,8 +162,37 @@ qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, qz_sim** out
 qz_status qz_sim_destroy(qz_sim* s);
 qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q, double m, int rigid,
                           double gref, double xiref);
-/* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL */
+/* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
+   By default (m = 0, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
+   consecutive steps run concurrently on different SMs, each slice gated on the beam pushes of the
+   previous step that can deposit into it, and the pushes are gated on the fields they gather: the
+   same arithmetic as the step-by-step loop of Simulation::run (src/Simulation.cpp:1370-1448), with
+   the beam deposits summed in a different order. The beams are kept in xi-cell order on the device
+   (qz_sim_beam returns them in the caller's order). */
 qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, void* stream);
+/* Schedule of qz_sim_run: pipelined = 0 runs the steps one kernel after another (one sweep launch,
+   then one push launch per beam, per step); sweep_ctas = CTAs running sweeps (0: one per step, up to
+   the SMs left for at least max(8, SMs/5) push CTAs); a push task (bucket) holds at most `bucket`
+   particles (0: 1024) of at most `span` neighbouring xi cells (0: 2) -- the next step's sweep trails
+   the previous one by about span + 5 slices; timeout_s = limit of every wait inside the pipelined
+   launch (0: keep, default 20 s), after which the launch ends and qz_sim_run returns QZ_ERR_CUDA.
+   No counterpart in the reference (its own pipelining over time steps is across MPI ranks,
+   src/Simulation.cpp:851-870). */
+qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span, double timeout_s);
+/* the schedule of the last qz_sim_run: grid, sweep CTAs, push CTAs, ring slots, buckets, bucket size,
+   pipelined (1/0), cell span of a bucket */
+qz_status qz_sim_schedule(qz_sim* s, int* info8);
+/* Timeline of the last pipelined run, 22 values per step n: GPU clock (ns, %globaltimer) at the start
+   and the end of sweep n, when it had stored 1/16, 2/16, ... 16/16 of the slices, then its longest
+   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 3 totals of
+   the push workers: tasks, scans that found no ready task, claims lost to another worker.
+   Up to cap values; *n = 22 (nsteps+1) + 3. enable = 1 records it in later runs. */
+qz_status qz_sim_trace(qz_sim* s, int enable, unsigned long long* out, int cap, int* n);
+/* qz_sim_run with the beams in HOST memory: copies every beam in (cols_host[b]: 7 x n SoA in the
+   caller's order, x y px py pz xi w), runs nsteps, and copies the particles back into cols_host in
+   the same order. Pinned host memory makes the copies asynchronous. */
+qz_status qz_sim_run_host(qz_sim* s, int nsteps, double dt, double* const* cols_host, double* moments_host,
+                          void* stream);
 /* copy out the field store / diagnostics of the last sweep (host, K*M*F_NC / K*M*D_NC) */
 qz_status qz_sim_fields(qz_sim* s, double* fld_host, double* diag_host);
 /* copy out beam b's particles (host, n x 7) */

@@ -232,6 +232,40 @@ class Simulation:
         check(lib().qz_sim_run(self.h, int(nsteps), float(dt), _p(mom) if nb else None, _stream_ptr(stream)))
         return mom[:, :nb, :]
 
+    def set_schedule(self, pipelined: bool = True, sweep_ctas: int = 0, bucket: int = 0, span: int = 0,
+                     timeout_s: float = 0.0):
+        """qz_sim_set_schedule: pipelined (one launch for the whole run) or step by step."""
+        check(lib().qz_sim_set_schedule(self.h, 1 if pipelined else 0, int(sweep_ctas), int(bucket), int(span),
+                                        float(timeout_s)))
+
+    def schedule(self) -> dict:
+        """The schedule of the last run (qz_sim_schedule)."""
+        info = (C.c_int * 8)()
+        check(lib().qz_sim_schedule(self.h, info))
+        keys = ("grid", "sweep_ctas", "push_ctas", "ring", "buckets", "bucket", "pipelined", "span")
+        return dict(zip(keys, list(info)))
+
+    def trace(self, enable: bool = True) -> np.ndarray:
+        """Timeline of the last pipelined run (qz_sim_trace): per step (start, end, 16 progress marks) in ns
+        of GPU clock, and the push workers' (tasks, empty scans, lost claims); enable turns the recording
+        on for later runs."""
+        n = C.c_int()
+        check(lib().qz_sim_trace(self.h, 1 if enable else 0, None, 0, C.byref(n)))
+        out = (C.c_ulonglong * max(n.value, 1))()
+        check(lib().qz_sim_trace(self.h, 1 if enable else 0, out, n.value, C.byref(n)))
+        v = np.array(list(out)[: n.value], dtype=np.float64)
+        return v[:-3].reshape(-1, 22), v[-3:]
+
+    def run_host(self, nsteps: int, dt: float, cols_host, stream=None) -> np.ndarray:
+        """qz_sim_run_host: beams in host memory (list of (7, n) float64 arrays, updated in place)."""
+        nb = len(self.spec.beams)
+        ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) if isinstance(c, np.ndarray) else int(c.data_ptr())
+                                           for c in cols_host])
+        mom = np.zeros((nsteps + 1, max(nb, 1), 17))
+        check(lib().qz_sim_run_host(self.h, int(nsteps), float(dt), ptrs, _p(mom) if nb else None,
+                                    _stream_ptr(stream)))
+        return mom[:, :nb, :]
+
     def fields(self):
         K, M = self.spec.K, self.spec.M
         fld = np.zeros(K * M * self.fnc)

@@ -616,7 +616,11 @@ struct qz_sim {
     int cur = 0;
     bool bsrc_valid = false;
     struct Beam {
-        double* d = nullptr;     // 7 columns of n
+        double* d = nullptr;     // 7 columns of n (the library's order: sorted by xi cell after a pipelined run)
+        double* d2 = nullptr;    // second copy for reordering
+        int* orig = nullptr;     // caller's index of each particle of d
+        int* orig2 = nullptr;
+        bool orig_identity = true;
         int64_t n = 0;
         double q = -1, m = 1, gref = 0, xiref = 0;
         int rigid = 0, started = 0;
@@ -629,10 +633,41 @@ struct qz_sim {
     };
     std::vector<Beam> beams;
     qz_counters cnt{};
+    // time-step pipeline (qz_pipeline.cu): options, last schedule, buffers kept between runs
+    struct Pipe {
+        int enabled = 1, sweep_ctas = 0, bucket = 1024, span = 2;
+        double timeout_s = 20.0;
+        int info[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // grid, sweep CTAs, worker CTAs, ring, buckets, bucket size, pipelined
+        int trace = 0;                             // record sweep start / end times
+        unsigned long long* d_trace = nullptr;
+        size_t trace_n = 0;
+        std::vector<unsigned long long> h_trace;
+        double *fld = nullptr, *diag = nullptr, *bsrc = nullptr;
+        int ring = 0;
+        bool clean = false;                        // every beam-source slot is zero
+        double* ps = nullptr;
+        size_t ps_n = 0;
+        int* sync = nullptr;
+        size_t sync_n = 0;
+        int* bk = nullptr;                         // beam, start, end, cmax (4 x nbk), then cnt_le (K)
+        size_t bk_n = 0;
+        double *pmom = nullptr, *mom = nullptr;
+        size_t pmom_n = 0, mom_n = 0;
+        qzb::CellSortBuf sort{};
+        long sort_n = 0;
+        int* cmin = nullptr;                       // group starts of one beam
+        size_t cm_n = 0;
+    } pipe;
     ~qz_sim() {
         for (auto& b : beams)
-            if (b.d) cudaFree(b.d);
-        for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom})
+            for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
+                if (q) cudaFree(q);
+        for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom, pipe.fld, pipe.diag, pipe.bsrc, pipe.ps,
+                          pipe.pmom, pipe.mom})
+            if (q) cudaFree(q);
+        for (void* q : {(void*)pipe.sync, (void*)pipe.bk, (void*)pipe.sort.keys[0], (void*)pipe.sort.keys[1],
+                        (void*)pipe.sort.vals[0], (void*)pipe.sort.vals[1], pipe.sort.tmp, (void*)pipe.sort.nlive,
+                        (void*)pipe.cmin, (void*)pipe.d_trace})
             if (q) cudaFree(q);
         qz_sweep_destroy(sw);
     }
@@ -675,6 +710,16 @@ extern "C" qz_status qz_sim_add_beam(qz_sim* s, const double* p7, int64_t n, dou
     for (int64_t i = 0; i < n; ++i)
         for (int c = 0; c < 7; ++c) cols[(size_t)c * n + i] = p7[7 * i + c];
     if (qz_status st = dev_upload(&b.d, cols)) return st;
+    const size_t nn = (size_t)(n > 0 ? n : 1);
+    if (cudaMalloc((void**)&b.d2, sizeof(double) * 7 * nn) != cudaSuccess ||
+        cudaMalloc((void**)&b.orig, sizeof(int) * nn) != cudaSuccess ||
+        cudaMalloc((void**)&b.orig2, sizeof(int) * nn) != cudaSuccess) {
+        for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
+            if (q) cudaFree(q);
+        return fail(QZ_ERR_NOMEM, "qz_sim_add_beam: device allocation failed");
+    }
+    if (s->beams.size() >= (size_t)qzb::kMaxBeams && s->pipe.enabled)
+        s->pipe.enabled = 0;   // the pipeline handles up to kMaxBeams beams; more run step by step
     s->beams.push_back(b);
     const int nb = (int)s->beams.size();
     if (s->d_mom) cudaFree(s->d_mom);
@@ -696,9 +741,237 @@ qz_box sim_box(const qz_sim* s) {
 }
 }  // namespace
 
-extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_host, void* stream) {
-    if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
-    cudaStream_t st = (cudaStream_t)stream;
+namespace {
+
+template <class T>
+qz_status grow(T** p, size_t* have, size_t need, const char* what) {
+    if (*have >= need && *p) return QZ_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *have = 0;
+    if (cudaMalloc((void**)p, sizeof(T) * (need > 0 ? need : 1)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(QZ_ERR_NOMEM, std::string("qz_sim_run: device allocation failed (") + what + ")");
+    }
+    *have = need;
+    return QZ_OK;
+}
+
+// Simulation::run for constant dt as one pipelined launch (qz_pipeline.cu): the beams are put in
+// xi-cell order (their caller order is kept in orig), cut into buckets, the step-0 beam sources are
+// deposited into ring slot 0, then all sweeps and pushes run concurrently.
+qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cudaStream_t st) {
+    auto& P_ = s->pipe;
+    const int K = s->p.K, M = s->g->M, nb = (int)s->beams.size();
+    const qz_box box = sim_box(s);
+    // 1. order each beam by xi cell; buckets of P_.bucket live particles
+    long nmax = 1;
+    for (auto& b : s->beams) nmax = std::max<long>(nmax, (long)b.n);
+    if (P_.sort_n < nmax) {
+        for (void* q : {(void*)P_.sort.keys[0], (void*)P_.sort.keys[1], (void*)P_.sort.vals[0],
+                        (void*)P_.sort.vals[1], P_.sort.tmp, (void*)P_.sort.nlive})
+            if (q) cudaFree(q);
+        P_.sort = qzb::CellSortBuf{};
+        P_.sort_n = 0;
+        P_.sort.tmp_bytes = qzb::cell_sort_temp_bytes(nmax);
+        if (cudaMalloc((void**)&P_.sort.keys[0], sizeof(unsigned) * nmax) != cudaSuccess ||
+            cudaMalloc((void**)&P_.sort.keys[1], sizeof(unsigned) * nmax) != cudaSuccess ||
+            cudaMalloc((void**)&P_.sort.vals[0], sizeof(int) * nmax) != cudaSuccess ||
+            cudaMalloc((void**)&P_.sort.vals[1], sizeof(int) * nmax) != cudaSuccess ||
+            cudaMalloc(&P_.sort.tmp, P_.sort.tmp_bytes + 16) != cudaSuccess ||
+            cudaMalloc((void**)&P_.sort.nlive, sizeof(int)) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (sort buffers)");
+        }
+        P_.sort_n = nmax;
+    }
+    const int bk = P_.bucket > 0 ? P_.bucket : 1024;
+    struct Bucket { int cmin, beam, start, end, cmax; };
+    std::vector<Bucket> list;
+    for (int q = 0; q < nb; ++q) {
+        auto& b = s->beams[q];
+        if (b.n <= 0) continue;
+        if (b.orig_identity) {
+            QZ_CUDA(qzb::fill_iota(b.orig, b.n, st));
+            b.orig_identity = false;
+        }
+        const qz_beam_view v = b.view();
+        const qzb::BeamArgs B = beam_args(s->g, &v, &box);
+        QZ_CUDA(qzb::cell_sort(B, b.d, b.d2, b.orig, b.orig2, P_.sort, st));
+        std::swap(b.d, b.d2);
+        std::swap(b.orig, b.orig2);
+        int nlive = 0;
+        QZ_CUDA(cudaMemcpyAsync(&nlive, P_.sort.nlive, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QZ_CUDA(cudaStreamSynchronize(st));
+        // buckets: never across a group of span cells, at most bk particles (near-equal parts)
+        const int span = P_.span > 0 ? P_.span : 2;
+        const int ngroups = (K + 1 + span - 1) / span;
+        if (qz_status e = grow(&P_.cmin, &P_.cm_n, (size_t)ngroups + 1, "bucket groups")) return e;
+        QZ_CUDA(qzb::group_starts(P_.sort, nlive, span, ngroups, P_.cmin, st));
+        std::vector<int> gs(ngroups + 1);
+        QZ_CUDA(cudaMemcpyAsync(gs.data(), P_.cmin, sizeof(int) * gs.size(), cudaMemcpyDeviceToHost, st));
+        QZ_CUDA(cudaStreamSynchronize(st));
+        for (int g = 0; g < ngroups; ++g) {
+            const int a = gs[g], cnt = gs[g + 1] - gs[g];
+            if (cnt <= 0) continue;
+            const int parts = (cnt + bk - 1) / bk;
+            const int cmin = g * span - 1, cmax = std::min(g * span + span - 2, K - 1);
+            for (int i = 0; i < parts; ++i)
+                list.push_back({cmin, q, a + (int)((long)cnt * i / parts), a + (int)((long)cnt * (i + 1) / parts), cmax});
+        }
+    }
+    std::stable_sort(list.begin(), list.end(), [](const Bucket& a, const Bucket& b) { return a.cmin < b.cmin; });
+    const int nbk = (int)list.size();
+    std::vector<int> bkh((size_t)4 * nbk + K);
+    for (int i = 0; i < nbk; ++i) {
+        bkh[i] = list[i].beam;
+        bkh[nbk + i] = list[i].start;
+        bkh[2 * nbk + i] = list[i].end;
+        bkh[3 * nbk + i] = list[i].cmax;
+    }
+    for (int r = 0, c = 0; r < K; ++r) {
+        while (c < nbk && list[c].cmin <= r) ++c;
+        bkh[4 * nbk + r] = c;
+    }
+    if (qz_status e = grow(&P_.bk, &P_.bk_n, bkh.size(), "buckets")) return e;
+    QZ_CUDA(cudaMemcpyAsync(P_.bk, bkh.data(), sizeof(int) * bkh.size(), cudaMemcpyHostToDevice, st));
+
+    // 2. schedule: one CTA per SM; sweeps for every step up to the SMs left after the workers
+    qzb::PipeArgs A{};
+    A.sw = s->sw->base;
+    A.sw.counters = s->sw->d_cnt;
+    A.sw.timing = nullptr;
+    int sms = 0;
+    const int grid = qzb::pipeline_max_grid(A, &sms);
+    if (grid < 2) return fail(QZ_ERR_UNSUPPORTED, "qz_sim_run: the pipelined kernel cannot be resident here");
+    const int g1 = std::min(grid, sms);
+    const int wmin = std::max(8, g1 / 5);
+    int nsweep = P_.sweep_ctas > 0 ? P_.sweep_ctas : std::min(nsteps + 1, g1 - wmin);
+    nsweep = std::max(1, std::min({nsweep, nsteps + 1, g1 - 1}));
+    const int ring = std::max(2, std::min(nsteps + 1, nsweep + 2));
+    // 3. buffers
+    const size_t KM = (size_t)K * M;
+    if (P_.ring < ring) {
+        for (double* q : {P_.fld, P_.diag, P_.bsrc})
+            if (q) cudaFree(q);
+        P_.fld = P_.diag = P_.bsrc = nullptr;
+        P_.ring = 0;
+        if (cudaMalloc((void**)&P_.fld, sizeof(double) * KM * s->fnc * ring) != cudaSuccess ||
+            cudaMalloc((void**)&P_.diag, sizeof(double) * KM * s->dnc * ring) != cudaSuccess ||
+            cudaMalloc((void**)&P_.bsrc, sizeof(double) * KM * s->bnc * ring) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (field rings)");
+        }
+        P_.ring = ring;
+        P_.clean = false;
+    }
+    if (!P_.clean) QZ_CUDA(cudaMemsetAsync(P_.bsrc, 0, sizeof(double) * KM * s->bnc * P_.ring, st));
+    P_.clean = false;
+    const size_t ps_slot = (size_t)(6 + 5 * s->p.ab_order) * std::max(1, s->sw->npad);
+    if (qz_status e = grow(&P_.ps, &P_.ps_n, ps_slot * nsweep, "plasma scratch")) return e;
+    const size_t nsync = 4 * (size_t)(nsteps + 1) + nbk + 2;
+    if (qz_status e = grow(&P_.sync, &P_.sync_n, nsync, "sync words")) return e;
+    QZ_CUDA(cudaMemsetAsync(P_.sync, 0, sizeof(int) * nsync, st));
+    int* bdone = P_.sync + 4 * (size_t)(nsteps + 1);
+    if (nbk) QZ_CUDA(cudaMemsetAsync(bdone, 0xff, sizeof(int) * nbk, st));
+    const bool moms = mom_host != nullptr && nb > 0;
+    if (moms) {
+        if (qz_status e = grow(&P_.pmom, &P_.pmom_n, (size_t)(nsteps + 1) * std::max(nbk, 1) * 17, "moments"))
+            return e;
+        if (qz_status e = grow(&P_.mom, &P_.mom_n, (size_t)(nsteps + 1) * nb * 17, "moments")) return e;
+        QZ_CUDA(cudaMemsetAsync(P_.mom, 0, sizeof(double) * (nsteps + 1) * nb * 17, st));
+    }
+    QZ_CUDA(cudaMemsetAsync(s->sw->d_cnt, 0, sizeof(unsigned long long) * 4, st));
+    // 4. beam sources of step 0 into slot 0
+    for (auto& b : s->beams) {
+        const qz_beam_view v = b.view();
+        if (qz_status e = qz_beam_deposit(s->g, &v, &box, P_.bsrc, st)) return e;
+    }
+    // 5. launch
+    A.nsteps = nsteps;
+    A.nsweep = nsweep;
+    A.ring = ring;
+    A.fld_slot = KM * s->fnc;
+    A.diag_slot = KM * s->dnc;
+    A.bsrc_slot = KM * s->bnc;
+    A.ps_slot = ps_slot;
+    A.fld = P_.fld;
+    A.diag = P_.diag;
+    A.bsrc = P_.bsrc;
+    A.ps = P_.ps;
+    A.nbeams = nb;
+    for (int q = 0; q < nb; ++q) {
+        const auto& b = s->beams[q];
+        const qz_beam_view v = b.view();
+        A.beam[q] = beam_args(s->g, &v, &box);
+        A.rigid[q] = b.rigid;
+        A.startup[q] = b.started ? 0 : 1;
+        A.gref[q] = b.gref;
+        A.xiref[q] = b.xiref;
+    }
+    A.dt_kick = dt;
+    A.dt_drift = dt;
+    A.nbk = nbk;
+    A.bk_beam = P_.bk;
+    A.bk_start = P_.bk + nbk;
+    A.bk_end = P_.bk + 2 * nbk;
+    A.bk_cmax = P_.bk + 3 * nbk;
+    A.cnt_le = P_.bk + 4 * nbk;
+    A.pmom = moms ? P_.pmom : nullptr;
+    A.prog = P_.sync;
+    A.sdone = P_.sync + (nsteps + 1);
+    A.pdone = P_.sync + 2 * (size_t)(nsteps + 1);
+    A.next = P_.sync + 3 * (size_t)(nsteps + 1);
+    A.bdone = bdone;
+    A.err = bdone + nbk;
+    A.lo = bdone + nbk + 1;
+    A.timeout_ns = (unsigned long long)(P_.timeout_s * 1e9);
+    A.trace = nullptr;
+    if (P_.trace) {
+        const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + 3;
+        if (qz_status e = grow(&P_.d_trace, &P_.trace_n, ntr, "trace")) return e;
+        QZ_CUDA(cudaMemsetAsync(P_.d_trace, 0, sizeof(unsigned long long) * ntr, st));
+        A.trace = P_.d_trace;
+    }
+    QZ_CUDA(qzb::launch_pipeline(A, g1, st));
+    if (moms) QZ_CUDA(qzb::launch_moments_reduce(A, P_.mom, st));
+    int err = 0;
+    unsigned long long h[4];
+    QZ_CUDA(cudaMemcpyAsync(&err, A.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    QZ_CUDA(cudaMemcpyAsync(h, s->sw->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
+    if (moms)
+        QZ_CUDA(cudaMemcpyAsync(mom_host, P_.mom, sizeof(double) * (nsteps + 1) * nb * 17, cudaMemcpyDeviceToHost, st));
+    // the last sweep's fields are what qz_sim_fields returns
+    const int last = nsteps % ring;
+    QZ_CUDA(cudaMemcpyAsync(s->d_fld, P_.fld + (size_t)last * A.fld_slot, sizeof(double) * A.fld_slot,
+                            cudaMemcpyDeviceToDevice, st));
+    QZ_CUDA(cudaMemcpyAsync(s->d_diag, P_.diag + (size_t)last * A.diag_slot, sizeof(double) * A.diag_slot,
+                            cudaMemcpyDeviceToDevice, st));
+    if (P_.trace) {
+        P_.h_trace.assign((size_t)qzb::kTraceStride * (nsteps + 1) + 3, 0ull);
+        QZ_CUDA(cudaMemcpyAsync(P_.h_trace.data(), P_.d_trace, sizeof(unsigned long long) * P_.h_trace.size(),
+                                cudaMemcpyDeviceToHost, st));
+    }
+    QZ_CUDA(cudaStreamSynchronize(st));
+    s->cnt.lost += h[0];
+    s->bsrc_valid = false;
+    const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 2};
+    std::copy(info, info + 8, P_.info);
+    if (err) {
+        static const char* site[] = {"?", "field ring slot", "beam-source rows", "no push task ready"};
+        const int w = (err >> 8) & 0xff;
+        return fail(QZ_ERR_CUDA, std::string("qz_sim_run: pipeline wait timed out (") + site[w <= 3 ? w : 0] +
+                                     "); results of this call are invalid");
+    }
+    P_.clean = true;
+    if (nsteps > 0)
+        for (auto& b : s->beams)
+            if (!b.rigid) b.started = 1;
+    return QZ_OK;
+}
+
+qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cudaStream_t st) {
+    void* stream = (void*)st;
     const size_t KMb = (size_t)s->p.K * s->g->M * s->bnc;
     const qz_box box = sim_box(s);
     const int nb = (int)s->beams.size();
@@ -744,6 +1017,71 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     QZ_CUDA(cudaMemcpyAsync(h, s->sw->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
     QZ_CUDA(cudaStreamSynchronize(st));
     s->cnt.lost += h[0];
+    s->pipe.info[6] = 0;
+    return QZ_OK;
+}
+
+}  // namespace
+
+extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_host, void* stream) {
+    if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
+    if (!(dt > 0.0)) return fail(QZ_ERR_ARG, "qz_sim_run: dt must be positive");
+    cudaStream_t st = (cudaStream_t)stream;
+    if (s->pipe.enabled && s->p.modes == 0) return run_pipelined(s, nsteps, dt, mom_host, st);
+    return run_sequential(s, nsteps, dt, mom_host, st);
+}
+
+extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span,
+                                         double timeout_s) {
+    if (!s || sweep_ctas < 0 || bucket < 0 || span < 0 || timeout_s < 0)
+        return fail(QZ_ERR_ARG, "qz_sim_set_schedule: bad argument");
+    if (pipelined && s->beams.size() > (size_t)qzb::kMaxBeams)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_set_schedule: the pipelined run handles at most 4 beams");
+    s->pipe.enabled = pipelined ? 1 : 0;
+    s->pipe.sweep_ctas = sweep_ctas;
+    s->pipe.bucket = bucket > 0 ? bucket : 1024;
+    s->pipe.span = span > 0 ? span : 2;
+    if (timeout_s > 0) s->pipe.timeout_s = timeout_s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_schedule(qz_sim* s, int* info8) {
+    if (!s || !info8) return fail(QZ_ERR_ARG, "qz_sim_schedule: null pointer");
+    std::copy(s->pipe.info, s->pipe.info + 8, info8);
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_trace(qz_sim* s, int enable, unsigned long long* out, int cap, int* n) {
+    if (!s || cap < 0 || (cap > 0 && !out)) return fail(QZ_ERR_ARG, "qz_sim_trace: bad argument");
+    const int have = (int)s->pipe.h_trace.size();
+    if (n) *n = have;
+    for (int i = 0; i < std::min(cap, have); ++i) out[i] = s->pipe.h_trace[i];
+    s->pipe.trace = enable ? 1 : 0;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_run_host(qz_sim* s, int nsteps, double dt, double* const* cols, double* mom_host,
+                                     void* stream) {
+    if (!s || nsteps < 0 || (!s->beams.empty() && !cols)) return fail(QZ_ERR_ARG, "qz_sim_run_host: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    for (auto& b : s->beams) {
+        const size_t i = &b - s->beams.data();
+        if (!cols[i]) return fail(QZ_ERR_ARG, "qz_sim_run_host: null beam buffer");
+        QZ_CUDA(cudaMemcpyAsync(b.d, cols[i], sizeof(double) * 7 * b.n, cudaMemcpyHostToDevice, st));
+        b.orig_identity = true;
+    }
+    s->bsrc_valid = false;
+    if (qz_status e = qz_sim_run(s, nsteps, dt, mom_host, stream)) return e;
+    for (auto& b : s->beams) {
+        const size_t i = &b - s->beams.data();
+        if (!b.orig_identity) {
+            QZ_CUDA(qzb::unpermute7(b.d, b.d2, b.orig, b.n, st));
+            std::swap(b.d, b.d2);
+            b.orig_identity = true;
+        }
+        QZ_CUDA(cudaMemcpyAsync(cols[i], b.d, sizeof(double) * 7 * b.n, cudaMemcpyDeviceToHost, st));
+    }
+    QZ_CUDA(cudaStreamSynchronize(st));
     return QZ_OK;
 }
 
@@ -759,9 +1097,13 @@ extern "C" qz_status qz_sim_beam(qz_sim* s, int b, double* p7) {
     if (!s || !p7 || b < 0 || b >= (int)s->beams.size()) return fail(QZ_ERR_ARG, "qz_sim_beam: bad argument");
     const auto& B = s->beams[b];
     std::vector<double> cols((size_t)7 * B.n);
+    std::vector<int> orig(B.orig_identity ? 0 : (size_t)B.n);
     if (B.n > 0) QZ_CUDA(cudaMemcpy(cols.data(), B.d, sizeof(double) * cols.size(), cudaMemcpyDeviceToHost));
-    for (int64_t i = 0; i < B.n; ++i)
-        for (int c = 0; c < 7; ++c) p7[7 * i + c] = cols[(size_t)c * B.n + i];
+    if (!orig.empty()) QZ_CUDA(cudaMemcpy(orig.data(), B.orig, sizeof(int) * orig.size(), cudaMemcpyDeviceToHost));
+    for (int64_t i = 0; i < B.n; ++i) {
+        const int64_t o = orig.empty() ? i : orig[i];     // the caller's index of this particle
+        for (int c = 0; c < 7; ++c) p7[7 * o + c] = cols[(size_t)c * B.n + i];
+    }
     return QZ_OK;
 }
 
@@ -782,6 +1124,7 @@ extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_
         if (!cols[b]) return fail(QZ_ERR_ARG, "qz_sim_step_host: null beam buffer");
         QZ_CUDA(cudaMemcpyAsync(s->beams[b].d, cols[b], sizeof(double) * 7 * s->beams[b].n, cudaMemcpyHostToDevice,
                                 st));
+        s->beams[b].orig_identity = true;
     }
     QZ_CUDA(cudaMemsetAsync(s->d_bsrc[s->cur], 0, sizeof(double) * KMb, st));
     for (auto& b : s->beams) {

@@ -6,8 +6,7 @@
 // particle columns is coalesced. The field store is read through L2 (a bilinear gather of the
 // (xi, r) cell, 4 x 6 doubles for m = 0); deposits are FP64 reductions into L2. The push can be
 // fused with the deposit of the next time step (the particle is deposited right after it moved).
-#include "qz_device.cuh"
-#include "qz_internal.h"
+#include "qz_beam_body.cuh"
 
 #include <mutex>
 
@@ -15,61 +14,8 @@ namespace qzb {
 
 namespace {
 
+using namespace beam_detail;
 constexpr int kBeamThreads = 256;
-
-__device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restrict__ bsrc, double X, double Y,
-                                            double PX, double PY, double PZ, double XI, double wi) {
-    const double R = B.R;
-    const double r = sqrt(X * X + Y * Y);
-    if (r > R) return;
-    const double c = r > 0.0 ? X / r : 1.0, s = r > 0.0 ? Y / r : 0.0;
-    const double sx = (XI - B.xi_min) * B.idxi;
-    const int k = B.ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
-    const int nloc = B.K;
-    if (k < -1 || k >= nloc) return;
-    const double tk = B.ngp ? 0.0 : sx - k;
-    const double p2 = PX * PX + PY * PY;
-    const double gam = sqrt(1.0 + p2 + PZ * PZ);
-    const double omvz = (1.0 + p2) / (gam * (gam + PZ));
-    const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
-    const double vr = c * vx + s * vy, vt = c * vy - s * vx;
-    int j;
-    double t;
-    weights(B.r, B.inv_h, B.N, R, r, j, t);
-    const double Wr[2] = {1.0 - t, t};
-    const double Wk[2] = {1.0 - tk, tk};
-    const double q = B.q;
-    const int nc = B.modes ? B_NC1 : B_NC0;
-    const int na = B.ngp ? 1 : 2;
-    for (int a = 0; a < na; ++a) {
-        const int kk = k + a;
-        if (kk < 0 || kk >= nloc) continue;
-#pragma unroll
-        for (int b = 0; b < 2; ++b) {
-            const int jj = j + b;
-            double* o = bsrc + ((size_t)kk * B.M + jj) * nc;
-            const double d = wi * q * Wk[a] * Wr[b] * B.inv_V[jj] * B.idxi;
-            atomicAdd(o + B_RT0, d * omvz);
-            atomicAdd(o + B_JZ0, d * vz);
-            atomicAdd(o + B_JP1R, d * vr);
-            atomicAdd(o + B_JP1I, d * vt);
-            atomicAdd(o + B_RHO0, d);
-            if (B.modes) {
-                atomicAdd(o + B_RT1R, d * omvz * c);
-                atomicAdd(o + B_RT1I, -d * omvz * s);
-                atomicAdd(o + B_JZ1R, d * vz * c);
-                atomicAdd(o + B_JZ1I, -d * vz * s);
-                atomicAdd(o + B_RHO1R, d * c);
-                atomicAdd(o + B_RHO1I, -d * s);
-                atomicAdd(o + B_JP0R, d * vx);
-                atomicAdd(o + B_JP0I, d * vy);
-                const double c2 = c * c - s * s, s2 = 2.0 * c * s;
-                atomicAdd(o + B_JP2R, d * (vx * c2 + vy * s2));
-                atomicAdd(o + B_JP2I, d * (vy * c2 - vx * s2));
-            }
-        }
-    }
-}
 
 __global__ void __launch_bounds__(kBeamThreads) beam_deposit_kernel(const BeamArgs B, double* __restrict__ bsrc) {
     const long stride = (long)gridDim.x * blockDim.x;
@@ -77,70 +23,6 @@ __global__ void __launch_bounds__(kBeamThreads) beam_deposit_kernel(const BeamAr
         const double wi = B.w[i];
         if (wi == 0.0) continue;
         deposit_one(B, bsrc, B.x[i], B.y[i], B.px[i], B.py[i], B.pz[i], B.xi[i], wi);
-    }
-}
-
-// bilinear (xi, r) gather and mode sums at the particle (src/Beam.cpp:972-1008)
-__device__ __forceinline__ void gather(const BeamArgs& B, const double* __restrict__ fld, double X, double Y,
-                                       double XI, double& c, double& sn, V3& E, V3& Bf) {
-    const double r = sqrt(X * X + Y * Y);
-    c = r > 0.0 ? X / r : 1.0;
-    sn = r > 0.0 ? Y / r : 0.0;
-    double s = (XI - B.xi_min) * B.idxi;
-    const int nloc = B.K;
-    int k;
-    double tk;
-    if (B.ngp) {
-        k = (int)floor(s + 0.5);
-        k = k < 0 ? 0 : (k > nloc - 1 ? nloc - 1 : k);
-        tk = 0.0;
-    } else {
-        k = (int)floor(s);
-        if (k < 0) { k = 0; s = 0.0; }
-        if (k > nloc - 2) { k = nloc - 2; s = nloc - 1; }
-        tk = s - k;
-    }
-    const int k1 = B.ngp ? k : k + 1;
-    int j;
-    double t;
-    weights(B.r, B.inv_h, B.N, B.R, r, j, t);
-    const int nc = B.modes ? F_NC1 : F_NC0;
-    const double* f00 = fld + ((size_t)k * B.M + j) * nc;
-    const double* f01 = f00 + nc;
-    const double* f10 = fld + ((size_t)k1 * B.M + j) * nc;
-    const double* f11 = f10 + nc;
-    auto bil = [&](int comp) {
-        return (1.0 - tk) * ((1.0 - t) * f00[comp] + t * f01[comp]) + tk * ((1.0 - t) * f10[comp] + t * f11[comp]);
-    };
-    if (B.modes) {
-        // eval_vector / eval_scalar with m = 1 (src/SliceData.hpp:70-83)
-        const double c2 = c * c - sn * sn, s2 = 2.0 * c * sn;
-        {
-            const double r0 = bil(F_EP0R), i0 = bil(F_EP0I), r1 = bil(F_EP1R), i1 = bil(F_EP1I);
-            const double r2 = bil(F_EP2R), i2 = bil(F_EP2I);
-            E.x = r1 * c - i1 * sn;
-            E.y = r1 * sn + i1 * c;
-            E.x += r0 + r2 * c2 - i2 * s2;
-            E.y += i0 + r2 * s2 + i2 * c2;
-        }
-        {
-            const double r0 = bil(F_BP0R), i0 = bil(F_BP0I), r1 = bil(F_BP1R), i1 = bil(F_BP1I);
-            const double r2 = bil(F_BP2R), i2 = bil(F_BP2I);
-            Bf.x = r1 * c - i1 * sn;
-            Bf.y = r1 * sn + i1 * c;
-            Bf.x += r0 + r2 * c2 - i2 * s2;
-            Bf.y += i0 + r2 * s2 + i2 * c2;
-        }
-        E.z = bil(F_EZ0) + 2.0 * (bil(F_EZ1R) * c - bil(F_EZ1I) * sn);
-        Bf.z = bil(F_BZ0) + 2.0 * (bil(F_BZ1R) * c - bil(F_BZ1I) * sn);
-    } else {
-        const double er = bil(F_EP1R), ei = bil(F_EP1I), br = bil(F_BP1R), bi = bil(F_BP1I);
-        E.x = er * c - ei * sn;
-        E.y = er * sn + ei * c;
-        Bf.x = br * c - bi * sn;
-        Bf.y = br * sn + bi * c;
-        E.z = bil(F_EZ0);
-        Bf.z = bil(F_BZ0);
     }
 }
 
@@ -158,7 +40,7 @@ __global__ void __launch_bounds__(kBeamThreads) beam_push_kernel(const BeamArgs 
         const double X = B.x[i], Y = B.y[i], XI = B.xi[i];
         double c, sn;
         V3 E, Bf;
-        gather(B, fld, X, Y, XI, c, sn, E, Bf);
+        gather<false>(B, fld, X, Y, XI, c, sn, E, Bf);
         V3 u = {B.px[i], B.py[i], B.pz[i]};
         const double h = 0.5 * qm * dt_kick;
         if (!move) {                 // leapfrog start-up: explicit kick (src/Beam.cpp:1038-1044)

@@ -1,0 +1,196 @@
+// qz_beam_body.cuh -- device functions of the beam path (deposit, gather + Vay push, moment sums),
+// shared by the stand-alone beam kernels (qz_beam.cu) and the time-step pipeline (qz_pipeline.cu).
+//
+// Beam::deposit (src/Beam.cpp:725-785), Beam::advance with the Vay pusher (src/Beam.cpp:948-1131,
+// src/Pushers.hpp:171-176), Beam::sums (src/Beam.cpp:1133-1155).
+#pragma once
+#include "qz_device.cuh"
+#include "qz_internal.h"
+
+namespace qzb {
+namespace beam_detail {
+
+// kL2: the data was written by other SMs during the same launch, so it is read from L2 (ld.global.cg)
+template <bool kL2>
+__device__ __forceinline__ double fload(const double* p) { return kL2 ? __ldcg(p) : *p; }
+
+__device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restrict__ bsrc, double X, double Y,
+                                            double PX, double PY, double PZ, double XI, double wi) {
+    const double R = B.R;
+    const double r = sqrt(X * X + Y * Y);
+    if (r > R) return;
+    const double c = r > 0.0 ? X / r : 1.0, s = r > 0.0 ? Y / r : 0.0;
+    const double sx = (XI - B.xi_min) * B.idxi;
+    const int k = B.ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
+    const int nloc = B.K;
+    if (k < -1 || k >= nloc) return;
+    const double tk = B.ngp ? 0.0 : sx - k;
+    const double p2 = PX * PX + PY * PY;
+    const double gam = sqrt(1.0 + p2 + PZ * PZ);
+    const double omvz = (1.0 + p2) / (gam * (gam + PZ));
+    const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
+    const double vr = c * vx + s * vy, vt = c * vy - s * vx;
+    int j;
+    double t;
+    weights(B.r, B.inv_h, B.N, R, r, j, t);
+    const double Wr[2] = {1.0 - t, t};
+    const double Wk[2] = {1.0 - tk, tk};
+    const double q = B.q;
+    const int nc = B.modes ? B_NC1 : B_NC0;
+    const int na = B.ngp ? 1 : 2;
+    for (int a = 0; a < na; ++a) {
+        const int kk = k + a;
+        if (kk < 0 || kk >= nloc) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int jj = j + b;
+            double* o = bsrc + ((size_t)kk * B.M + jj) * nc;
+            const double d = wi * q * Wk[a] * Wr[b] * B.inv_V[jj] * B.idxi;
+            atomicAdd(o + B_RT0, d * omvz);
+            atomicAdd(o + B_JZ0, d * vz);
+            atomicAdd(o + B_JP1R, d * vr);
+            atomicAdd(o + B_JP1I, d * vt);
+            atomicAdd(o + B_RHO0, d);
+            if (B.modes) {
+                atomicAdd(o + B_RT1R, d * omvz * c);
+                atomicAdd(o + B_RT1I, -d * omvz * s);
+                atomicAdd(o + B_JZ1R, d * vz * c);
+                atomicAdd(o + B_JZ1I, -d * vz * s);
+                atomicAdd(o + B_RHO1R, d * c);
+                atomicAdd(o + B_RHO1I, -d * s);
+                atomicAdd(o + B_JP0R, d * vx);
+                atomicAdd(o + B_JP0I, d * vy);
+                const double c2 = c * c - s * s, s2 = 2.0 * c * s;
+                atomicAdd(o + B_JP2R, d * (vx * c2 + vy * s2));
+                atomicAdd(o + B_JP2I, d * (vy * c2 - vx * s2));
+            }
+        }
+    }
+}
+
+// bilinear (xi, r) gather and mode sums at the particle (src/Beam.cpp:972-1008)
+template <bool kL2>
+__device__ __forceinline__ void gather(const BeamArgs& B, const double* __restrict__ fld, double X, double Y,
+                                       double XI, double& c, double& sn, V3& E, V3& Bf) {
+    const double r = sqrt(X * X + Y * Y);
+    c = r > 0.0 ? X / r : 1.0;
+    sn = r > 0.0 ? Y / r : 0.0;
+    double s = (XI - B.xi_min) * B.idxi;
+    const int nloc = B.K;
+    int k;
+    double tk;
+    if (B.ngp) {
+        k = (int)floor(s + 0.5);
+        k = k < 0 ? 0 : (k > nloc - 1 ? nloc - 1 : k);
+        tk = 0.0;
+    } else {
+        k = (int)floor(s);
+        if (k < 0) { k = 0; s = 0.0; }
+        if (k > nloc - 2) { k = nloc - 2; s = nloc - 1; }
+        tk = s - k;
+    }
+    const int k1 = B.ngp ? k : k + 1;
+    int j;
+    double t;
+    weights(B.r, B.inv_h, B.N, B.R, r, j, t);
+    const int nc = B.modes ? F_NC1 : F_NC0;
+    const double* f00 = fld + ((size_t)k * B.M + j) * nc;
+    const double* f01 = f00 + nc;
+    const double* f10 = fld + ((size_t)k1 * B.M + j) * nc;
+    const double* f11 = f10 + nc;
+    auto bil = [&](int comp) {
+        return (1.0 - tk) * ((1.0 - t) * fload<kL2>(f00 + comp) + t * fload<kL2>(f01 + comp)) +
+               tk * ((1.0 - t) * fload<kL2>(f10 + comp) + t * fload<kL2>(f11 + comp));
+    };
+    if (B.modes) {
+        // eval_vector / eval_scalar with m = 1 (src/SliceData.hpp:70-83)
+        const double c2 = c * c - sn * sn, s2 = 2.0 * c * sn;
+        {
+            const double r0 = bil(F_EP0R), i0 = bil(F_EP0I), r1 = bil(F_EP1R), i1 = bil(F_EP1I);
+            const double r2 = bil(F_EP2R), i2 = bil(F_EP2I);
+            E.x = r1 * c - i1 * sn;
+            E.y = r1 * sn + i1 * c;
+            E.x += r0 + r2 * c2 - i2 * s2;
+            E.y += i0 + r2 * s2 + i2 * c2;
+        }
+        {
+            const double r0 = bil(F_BP0R), i0 = bil(F_BP0I), r1 = bil(F_BP1R), i1 = bil(F_BP1I);
+            const double r2 = bil(F_BP2R), i2 = bil(F_BP2I);
+            Bf.x = r1 * c - i1 * sn;
+            Bf.y = r1 * sn + i1 * c;
+            Bf.x += r0 + r2 * c2 - i2 * s2;
+            Bf.y += i0 + r2 * s2 + i2 * c2;
+        }
+        E.z = bil(F_EZ0) + 2.0 * (bil(F_EZ1R) * c - bil(F_EZ1I) * sn);
+        Bf.z = bil(F_BZ0) + 2.0 * (bil(F_BZ1R) * c - bil(F_BZ1I) * sn);
+    } else {
+        const double er = bil(F_EP1R), ei = bil(F_EP1I), br = bil(F_BP1R), bi = bil(F_BP1I);
+        E.x = er * c - ei * sn;
+        E.y = er * sn + ei * c;
+        Bf.x = br * c - bi * sn;
+        Bf.y = br * sn + bi * c;
+        E.z = bil(F_EZ0);
+        Bf.z = bil(F_BZ0);
+    }
+}
+
+
+// One particle of Beam::advance (src/Beam.cpp:948-1131): gather at the old position, optional explicit
+// start-up kick with the same fields (h_start != 0, src/Beam.cpp:1038-1044), Vay with h = q/m dt_kick/2,
+// drift, removal at the wall or outside the box. Returns false when the particle was removed.
+struct PState7 {
+    double x, y, px, py, pz, xi, w;
+};
+
+template <bool kL2>
+__device__ __forceinline__ bool push_one(const BeamArgs& B, const double* __restrict__ fld, PState7& p, double h,
+                                         double h_start, double dt) {
+    double c, sn;
+    V3 E, Bf;
+    gather<kL2>(B, fld, p.x, p.y, p.xi, c, sn, E, Bf);
+    V3 u = {p.px, p.py, p.pz};
+    if (h_start != 0.0) {
+        const double g0 = sqrt(1.0 + dot3(u, u));
+        const double ig = 1.0 / g0;
+        const V3 v = {ig * u.x, ig * u.y, ig * u.z};
+        const V3 vxb = cross3(v, Bf);
+        const double h2 = 2.0 * h_start;
+        u = {u.x + h2 * (E.x + vxb.x), u.y + h2 * (E.y + vxb.y), u.z + h2 * (E.z + vxb.z)};
+    }
+    u = vay(u, E, Bf, h);
+    const double p2 = u.x * u.x + u.y * u.y;
+    const double gam = sqrt(1.0 + p2 + u.z * u.z);
+    const double omvz = (1.0 + p2) / (gam * (gam + u.z));
+    const double xn = p.x + u.x / gam * dt, yn = p.y + u.y / gam * dt;
+    const double xin = p.xi + omvz * dt;
+    const double xmin = B.xi_min, xmax = B.xi_min + (B.K - 1) * B.dxi;
+    p.x = xn; p.y = yn; p.px = u.x; p.py = u.y; p.pz = u.z; p.xi = xin;
+    if (xn * xn + yn * yn >= B.R * B.R || xin < xmin || xin > xmax) {
+        p.w = 0.0;
+        return false;
+    }
+    return true;
+}
+
+// the weighted moments of Beam::sums (src/Beam.cpp:1133-1155) of one particle, added to acc[17]
+__device__ __forceinline__ void sums_add(double* acc, const PState7& p, double gref, double xiref) {
+    const double g = sqrt(1.0 + p.px * p.px + p.py * p.py + p.pz * p.pz);
+    const double G = g - gref, XI = p.xi - xiref;
+    const double v[15] = {G, G * G, XI, XI * XI, p.x * p.x + p.y * p.y, p.x, p.y, p.x * p.x, p.y * p.y,
+                          p.px, p.py, p.px * p.px, p.py * p.py, p.x * p.px, p.y * p.py};
+    acc[16] += 1.0;
+    acc[0] += p.w;
+#pragma unroll
+    for (int c = 0; c < 15; ++c) acc[c + 1] += p.w * v[c];
+}
+
+// the xi cell of a particle for bucketing: floor((xi - xi_min)/dxi) clamped to [-1, K-1]
+__device__ __forceinline__ int xi_cell(const BeamArgs& B, double xi) {
+    const double s = (xi - B.xi_min) * B.idxi;
+    if (!(s >= -1.0)) return -1;
+    if (s >= (double)(B.K - 1)) return B.K - 1;
+    return (int)floor(s);
+}
+
+}  // namespace beam_detail
+}  // namespace qzb

@@ -79,4 +79,75 @@ constexpr int kSumsStaticBlocks = 148 * 4;
 cudaError_t beam_sums_static(const BeamArgs& B, double gref, double xiref, double* out17, cudaStream_t s,
                              int* nblocks_needed);
 
+// ---------------------------------------------------------------- time-step pipeline
+// Consecutive time steps of Simulation::run in one cooperative launch: CTAs [0, nsweep) each run whole
+// sweeps (steps n = blockIdx.x, +nsweep, ...); the other CTAs push beam buckets (a bucket is a run of
+// particles of one beam, sorted by xi cell). Step n+1's sweep at slice k only needs the beam sources
+// of rows <= k+3, i.e. the push of step n of the buckets whose particles sit in those rows, which in
+// turn needs step n's fields a few slices further: consecutive steps run concurrently, staggered by
+// a few slices. Particles only move towards larger xi cells (1 - v_z > 0), so the lowest cell of a
+// bucket when it was formed is a lower bound for all later steps.
+constexpr int kMaxBeams = 4;
+
+struct PipeArgs {
+    SweepArgs sw;                   // bsrc / fld / diag / ps of sw are unused: rings below
+    int nsteps;                     // sweeps 0..nsteps, pushes 0..nsteps-1
+    int nsweep;                     // CTAs running sweeps
+    int ring;                       // slots of the field / diagnostics / beam-source rings
+    size_t fld_slot, diag_slot, bsrc_slot, ps_slot;   // doubles per slot (ps: per sweep CTA)
+    double *fld, *diag, *bsrc, *ps;
+    int nbeams;
+    BeamArgs beam[kMaxBeams];
+    int rigid[kMaxBeams], startup[kMaxBeams];
+    double gref[kMaxBeams], xiref[kMaxBeams];
+    double dt_kick, dt_drift;
+    int nbk;                        // buckets, ordered by their initial lowest xi cell
+    const int *bk_beam, *bk_start, *bk_end;
+    int* bk_cmax;                   // highest xi cell of the bucket's live particles (before the next push)
+    const int* cnt_le;              // [K]: number of buckets whose initial lowest cell is <= row
+    double* pmom;                   // (nsteps + 1, nbk, 17) partial moment sums, or null
+    // synchronisation words (device; set before the launch)
+    int* prog;                      // [nsteps + 1] slices stored by sweep n (0)
+    int* sdone;                     // [nsteps + 1] sweep n finished, its beam-source slot is zero again (0)
+    int* pdone;                     // [nsteps + 1] bucket tasks finished for step n (0)
+    int* bdone;                     // [nbk] last step whose push finished (-1)
+    int* next;                      // [nsteps + 1] next unclaimed bucket of step n (0)
+    int* err;                       // != 0: a wait gave up, (site << 8) | 1 (0)
+    int* lo;                        // steps below *lo have every task claimed (0)
+    unsigned long long timeout_ns;  // limit of every wait
+    unsigned long long* trace;      // optional, kTraceStride per step: %globaltimer at the start and end of
+                                    // sweep n, when it passed each 16th of the box, then its longest wait
+                                    // for beam rows (ns, bucket, row, bucket's cmax); after the steps:
+                                    // worker totals (tasks, empty scans, lost claims)
+};
+constexpr int kTraceStride = 22;
+
+size_t pipeline_smem_bytes(int M, bool dbuf, bool const_smem);
+// resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count
+int pipeline_max_grid(const PipeArgs& P, int* sms);
+// cooperative launch of grid CTAs (fails unless all of them can be resident at once)
+cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream);
+// mom (nsteps + 1, nbeams, 17) from the bucket partials, in bucket order
+cudaError_t launch_moments_reduce(const PipeArgs& P, double* mom, cudaStream_t s);
+
+// Ordering a beam by xi cell (stable radix sort of the cell keys; removed particles last) for the
+// pipeline's buckets. Buffers of n entries: keys[2], vals[2]; tmp of cell_sort_temp_bytes(n).
+struct CellSortBuf {
+    unsigned* keys[2];
+    int* vals[2];
+    void* tmp;
+    size_t tmp_bytes;
+    int* nlive;                 // device: live particles of the last sort
+};
+size_t cell_sort_temp_bytes(long n);
+// stage (7 x n) = cols sorted by cell, orig_stage = orig permuted the same way
+cudaError_t cell_sort(const BeamArgs& B, double* cols, double* stage, int* orig, int* orig_stage,
+                      const CellSortBuf& buf, cudaStream_t s);
+cudaError_t fill_iota(int* p, long n, cudaStream_t s);
+// dst (7 x n) = src in the caller's order: dst[c][orig[p]] = src[c][p]
+cudaError_t unpermute7(const double* src, double* dst, const int* orig, long n, cudaStream_t s);
+// start[g] = first live particle of the last sort in cells [g span - 1, g span + span - 2] (g < ngroups),
+// start[ngroups] = nlive
+cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngroups, int* start, cudaStream_t s);
+
 }  // namespace qzb

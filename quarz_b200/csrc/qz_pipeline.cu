@@ -1,0 +1,538 @@
+// qz_pipeline.cu -- consecutive time steps of Simulation::run (src/Simulation.cpp:1370-1448) in one
+// cooperative launch, so that the sequential xi sweeps of consecutive steps run concurrently on
+// different SMs instead of one after another on one SM.
+//
+// Roles. CTAs [0, nsweep) run whole sweeps (qz_sweep_body.cuh), step n on CTA n % nsweep. In the other
+// CTAs every warp is a worker: it claims (step, bucket) tasks that are ready and, per bucket, adds the
+// moment sums of Beam::sums for that step, pushes the particles with that step's fields (Beam::push)
+// and deposits them into the next step's beam sources (Beam::deposit), all in one pass.
+//
+// Ordering (every wait spins on an acquire load, bounded by %globaltimer; on time-out it records the
+// place in *err and returns, and every other wait gives up as soon as *err is set):
+//  - sweep n reads beam-source rows <= r only when every bucket whose initial lowest cell is <= r has
+//    finished its push of step n-1 (particles only move to larger xi cells, so no other particle can
+//    deposit into those rows);
+//  - the push of (n, b) gathers rows <= cmax_b + 1 of step n's fields: it waits for sweep n to have
+//    stored them, and for bucket b's push of step n-1 (the same particles);
+//  - rings: sweep n writes field slot n % ring once the push of step n - ring is done; the sweep zeroes
+//    each beam-source row when it no longer needs it, so that slot is clean for step n + ring, whose
+//    depositors wait for sweep n to finish.
+// A task is claimed only once it is ready, oldest step first, so workers never hold a task they
+// wait on; sweeps wait only for pushes of older steps, so with all CTAs resident (cooperative launch)
+// the waits cannot form a cycle. Data written by other SMs during the launch (fields, beam sources, particles, bucket bounds)
+// is read with ld.global.cg, so that no stale L1 line is used.
+#include "qz_beam_body.cuh"
+#include "qz_sweep_body.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+namespace qzb {
+
+namespace {
+
+using beam_detail::deposit_one;
+using beam_detail::PState7;
+using beam_detail::push_one;
+using beam_detail::sums_add;
+using beam_detail::xi_cell;
+
+constexpr int kT = kSweepThreads;
+
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// where a wait gave up: *err = (site << 8) | 1
+enum WaitSite { W_RING = 1, W_ROWS = 2, W_TASK = 3 };
+
+// Wait until *p >= v. Bounded: gives up after P.timeout_ns, or as soon as another CTA reported an error.
+__device__ bool wait_ge(const PipeArgs& P, const int* p, int v, int site) {
+    if (ld_acquire(p) >= v) return true;
+    const unsigned long long t0 = gtimer();
+    for (;;) {
+        __nanosleep(64);
+        if (ld_acquire(p) >= v) return true;
+        if (ld_acquire(P.err) != 0) return false;
+        if (gtimer() - t0 > P.timeout_ns) {
+            atomicCAS(P.err, 0, (site << 8) | 1);
+            return false;
+        }
+    }
+}
+
+// Per-sweep state of the gate, in shared memory so that it holds no registers across the slice loop.
+struct GateState {
+    const double* bsrc;   // this step's ring slots
+    double* fld;
+    double* diag;
+    double* ps;           // this CTA's plasma scratch
+    int n;                // time step of this sweep
+    int cursor;           // buckets [0, cursor) are known to have pushed step n-1
+};
+
+// The gate of a sweep inside the pipeline (the hooks sweep_body calls).
+struct PipeGate {
+    static constexpr bool kActive = true;
+    const PipeArgs* P;    // the kernel's __grid_constant__ parameter block
+    GateState* g;         // shared
+
+    __device__ const double* bsrc(const SweepArgs&) const { return g->bsrc; }
+    __device__ double* fld(const SweepArgs&) const { return g->fld; }
+    __device__ double* diag(const SweepArgs&) const { return g->diag; }
+    __device__ double* ps(const SweepArgs&) const { return g->ps; }
+
+    // thread 0: beam-source rows <= r are final
+    __device__ bool before_rows(int r) {
+        const int need = P->cnt_le[r];
+        int c = g->cursor;
+        const int n = g->n;
+        while (c < need) {
+            const unsigned long long t0 = P->trace ? gtimer() : 0ull;
+            if (!wait_ge(*P, P->bdone + c, n - 1, W_ROWS)) return false;
+            if (P->trace) {                           // the longest wait of this sweep: for which bucket
+                unsigned long long* tr = P->trace + (size_t)kTraceStride * n;
+                const unsigned long long dtw = gtimer() - t0;
+                if (dtw > tr[18]) {
+                    tr[18] = dtw;
+                    tr[19] = (unsigned long long)c;
+                    tr[20] = (unsigned long long)r;
+                    tr[21] = (unsigned long long)(long long)__ldcg(P->bk_cmax + c);
+                }
+            }
+            ++c;
+        }
+        g->cursor = c;
+        return true;
+    }
+    // every thread, after its stores of slice k: row k-1 of the beam sources is no longer needed
+    __device__ void slice_done_all(int k) {
+        if (k >= 1) {
+            const int nr = P->sw.M * B_NC0;
+            double* row = const_cast<double*>(g->bsrc) + (size_t)(k - 1) * nr;
+            for (int i = threadIdx.x; i < nr; i += kT) __stcg(row + i, 0.0);
+        }
+    }
+    // thread 0, after the barrier that ends slice k: publish it (the fence covers the stores of the
+    // whole CTA, which the barrier ordered before it)
+    __device__ bool slice_done(int k) {
+        __threadfence();
+        st_release(P->prog + g->n, k + 1);
+        if (P->trace) {                               // progress marks at every 16th of the box
+            const int K = P->sw.K;
+            const int j = (16 * (k + 1)) / K;
+            if (j > (16 * k) / K)
+                P->trace[(size_t)kTraceStride * g->n + 1 + j] = gtimer();
+        }
+        return ld_acquire(P->err) == 0;
+    }
+};
+
+template <int ORD, bool REG, int kMaxR>
+__device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
+    __shared__ int s_ok;
+    __shared__ GateState gs;
+    const int tid = threadIdx.x;
+    const int K = P.sw.K, M = P.sw.M;
+    for (int n = blockIdx.x; n <= P.nsteps; n += P.nsweep) {
+        const int slot = n % P.ring;
+        if (tid == 0) {
+            s_ok = (n < P.ring) ? 1 : (wait_ge(P, P.pdone + (n - P.ring), P.nbk, W_RING) ? 1 : 0);
+            gs.bsrc = P.bsrc + slot * P.bsrc_slot;
+            gs.fld = P.fld + slot * P.fld_slot;
+            gs.diag = P.diag + slot * P.diag_slot;
+            gs.ps = P.ps + blockIdx.x * P.ps_slot;
+            gs.n = n;
+            gs.cursor = 0;
+        }
+        __syncthreads();
+        if (!s_ok) return;
+        if (P.trace && tid == 0) P.trace[(size_t)kTraceStride * n] = gtimer();
+        PipeGate g{&P, &gs};
+        if (!sweep_body<ORD, REG, kMaxR>(P.sw, smem, g)) return;
+        // the last row (the others were zeroed slice by slice)
+        double* row = P.bsrc + slot * P.bsrc_slot + (size_t)(K - 1) * M * B_NC0;
+        for (int i = tid; i < M * B_NC0; i += kT) __stcg(row + i, 0.0);
+        __syncthreads();
+        if (tid == 0) {
+            __threadfence();
+            st_release(P.sdone + n, 1);
+            if (P.trace) P.trace[(size_t)kTraceStride * n + 1] = gtimer();
+        }
+    }
+}
+
+// Is task (m, b) ready: bucket b pushed step m-1, and (for a push) step m's fields stored up to the
+// bucket's cells and the next step's beam-source slot clean. Every condition only ever turns true.
+__device__ __forceinline__ bool task_ready(const PipeArgs& P, int m, int b) {
+    if (ld_acquire(P.bdone + b) < m - 1) return false;
+    if (m >= P.nsteps) return true;                       // moments of the final state only
+    const int cm = __ldcg(P.bk_cmax + b);
+    if (ld_acquire(P.prog + m) < min(max(cm, 0) + 2, P.sw.K)) return false;
+    if (m + 1 >= P.ring && ld_acquire(P.sdone + (m + 1 - P.ring)) < 1) return false;
+    return true;
+}
+
+// Warp-collective: claim the oldest ready task. Lane i looks at step lo + i (+32, ...), the lowest
+// ready step is claimed with a CAS on its next-bucket counter, so a claimed task never waits. Returns
+// false when every task is claimed, or on an error / time-out (recorded in *err).
+__device__ __forceinline__ bool claim_task(const PipeArgs& P, int last, int& n, int& b, unsigned long long* st) {
+    const int lane = threadIdx.x & 31;
+    const unsigned long long t0 = gtimer();
+    unsigned sleep_ns = 64;       // back off while nothing is ready: idle warps must not flood L2
+    for (;;) {
+        if (ld_acquire(P.err) != 0) return false;
+        const int lo = __shfl_sync(0xffffffffu, lane == 0 ? ld_acquire(P.lo) : 0, 0);
+        if (lo > last) return false;
+        for (int base = lo; base <= last; base += 32) {
+            const int m = base + lane;
+            int idx = P.nbk;
+            bool ready = false;
+            if (m <= last) {
+                idx = ld_acquire(P.next + m);
+                if (idx < P.nbk) ready = task_ready(P, m, idx);
+            }
+            const unsigned full = __ballot_sync(0xffffffffu, idx >= P.nbk);
+            if (base == lo && (full & 1u)) {              // steps lo, lo+1, ... fully claimed
+                const int c = (~full == 0u) ? 32 : __ffs(~full) - 1;
+                if (lane == 0) atomicMax(P.lo, base + c);
+            }
+            unsigned rm = __ballot_sync(0xffffffffu, ready);
+            // warps start at different ready steps (oldest first only for warp 0 of each rotation), so
+            // that they do not all race for one step's counter
+            const int rot = (int)((blockIdx.x * (kT / 32) + (threadIdx.x >> 5)) & 31);
+            while (rm) {
+                const unsigned hi = rm >> rot, low = rm & ((1u << rot) - 1u);
+                const int src = hi ? rot + __ffs(hi) - 1 : __ffs(low) - 1;
+                int got = 0;
+                if (lane == src) got = atomicCAS(P.next + m, idx, idx + 1) == idx ? 1 : 0;
+                if (__shfl_sync(0xffffffffu, got, src)) {
+                    ++st[0];
+                    n = base + src;
+                    b = __shfl_sync(0xffffffffu, idx, src);
+                    return true;
+                }
+                rm &= ~(1u << src);
+                ++st[2];
+            }
+        }
+        ++st[1];
+        __nanosleep(sleep_ns);
+        sleep_ns = min(2 * sleep_ns, 8192u);
+        if (gtimer() - t0 > P.timeout_ns) {
+            if (lane == 0) atomicCAS(P.err, 0, (W_TASK << 8) | 1);
+            return false;
+        }
+    }
+}
+
+// Worker CTAs: every warp is an independent worker that claims (step, bucket) tasks.
+__device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int M = P.sw.M, N = P.sw.N;
+    // grid arrays in shared memory: the binary search of every lookup stays on chip
+    double* r = smem;
+    double* ih = r + M;
+    double* iV = ih + M;
+    for (int j = tid; j < M; j += kT) {
+        r[j] = P.sw.r[j];
+        iV[j] = P.sw.inv_V[j];
+        if (j < N) ih[j] = P.sw.inv_h[j];
+    }
+    __syncthreads();
+    const int last = P.pmom ? P.nsteps : P.nsteps - 1;     // the last step with tasks
+    int n, b;
+    unsigned long long st[3] = {0, 0, 0};                  // tasks, scans that found nothing, lost claims
+    while (claim_task(P, last, n, b, st)) {
+        const bool push = n < P.nsteps;
+        const int bb = __ldg(P.bk_beam + b);
+        const long i0 = __ldg(P.bk_start + b), i1 = __ldg(P.bk_end + b);
+        BeamArgs Bb = P.beam[bb];
+        Bb.r = r;
+        Bb.inv_h = ih;
+        Bb.inv_V = iV;
+        const double* fld = P.fld + (size_t)(n % P.ring) * P.fld_slot;
+        double* bnext = P.bsrc + (size_t)((n + 1) % P.ring) * P.bsrc_slot;
+        const double qm = Bb.q / Bb.m;
+        const double h = 0.5 * qm * P.dt_kick;
+        const double hs = (n == 0 && P.startup[bb]) ? 0.5 * qm * (-0.5 * P.dt_kick) : 0.0;
+        const bool rigid = P.rigid[bb] != 0;
+        const double gref = P.gref[bb], xiref = P.xiref[bb];
+        double acc[17];
+#pragma unroll
+        for (int c = 0; c < 17; ++c) acc[c] = 0.0;
+        int cmax = -2;
+        for (long i = i0 + lane; i < i1; i += 32) {
+            PState7 p;
+            p.w = __ldcg(Bb.w + i);
+            if (p.w == 0.0) continue;
+            p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
+            p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
+            p.xi = __ldcg(Bb.xi + i);
+            if (P.pmom) sums_add(acc, p, gref, xiref);
+            if (!push) continue;
+            if (rigid) {
+                deposit_one(Bb, bnext, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
+                cmax = max(cmax, xi_cell(Bb, p.xi));
+                continue;
+            }
+            const bool alive = push_one<true>(Bb, fld, p, h, hs, P.dt_drift);
+            __stcg(Bb.x + i, p.x); __stcg(Bb.y + i, p.y);
+            __stcg(Bb.px + i, p.px); __stcg(Bb.py + i, p.py); __stcg(Bb.pz + i, p.pz);
+            __stcg(Bb.xi + i, p.xi);
+            if (!alive) {
+                __stcg(Bb.w + i, 0.0);
+                continue;
+            }
+            deposit_one(Bb, bnext, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
+            cmax = max(cmax, xi_cell(Bb, p.xi));
+        }
+        // bucket results: moments of step n (before the push) in lane order, highest live cell after it
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
+        if (P.pmom) {
+            double mine = 0.0;
+#pragma unroll
+            for (int c = 0; c < 17; ++c) {
+                double x = acc[c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == c) mine = x;
+            }
+            if (lane < 17) P.pmom[((size_t)n * P.nbk + b) * 17 + lane] = mine;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            // never below the previous bound: cells only grow, and a bucket may have no live particle
+            if (push) __stcg(P.bk_cmax + b, max(cmax, __ldcg(P.bk_cmax + b)));
+            __threadfence();
+            if (push) st_release(P.bdone + b, n);
+            atomicAdd(P.pdone + n, 1);
+        }
+        __syncwarp();
+    }
+    if (P.trace && lane == 0) {
+        unsigned long long* ws = P.trace + (size_t)kTraceStride * (P.nsteps + 1);
+        for (int c = 0; c < 3; ++c) atomicAdd(ws + c, st[c]);
+    }
+}
+
+template <int ORD, bool REG, int kMaxR>
+__global__ void __launch_bounds__(kSweepThreads, 1) pipeline_kernel(const __grid_constant__ PipeArgs P) {
+    extern __shared__ double smem_raw[];
+    if ((int)blockIdx.x < P.nsweep)
+        sweep_role<ORD, REG, kMaxR>(P, smem_raw);
+    else
+        worker_role(P, smem_raw);
+}
+
+// moments of step n, beam q: the bucket partials of that beam in bucket order (deterministic)
+__global__ void moments_reduce_kernel(const __grid_constant__ PipeArgs P, double* __restrict__ mom) {
+    const int n = blockIdx.x / P.nbeams, q = blockIdx.x % P.nbeams, c = threadIdx.x;
+    if (c >= 17) return;
+    double v = 0.0;
+    for (int b = 0; b < P.nbk; ++b)
+        if (P.bk_beam[b] == q) v += P.pmom[((size_t)n * P.nbk + b) * 17 + c];
+    mom[((size_t)n * P.nbeams + q) * 17 + c] = v;
+}
+
+template <int ORD, bool REG, int RM>
+cudaError_t launch_t(const PipeArgs& P, int grid, size_t smem, cudaStream_t stream) {
+    auto fn = pipeline_kernel<ORD, REG, RM>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {(void*)&P};
+    return cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(kSweepThreads), args, smem, stream);
+}
+
+template <int ORD, bool REG, int RM>
+int occupancy_t(size_t smem) {
+    auto fn = pipeline_kernel<ORD, REG, RM>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, smem) != cudaSuccess) return 0;
+    return nb;
+}
+
+template <int ORD>
+cudaError_t launch_o(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
+    const bool reg = P.sw.np <= kSweepThreads;
+    if (P.sw.rows_per_thread == 1)
+        return reg ? launch_t<ORD, true, 1>(P, grid, smem, s) : launch_t<ORD, false, 1>(P, grid, smem, s);
+    return reg ? launch_t<ORD, true, 4>(P, grid, smem, s) : launch_t<ORD, false, 4>(P, grid, smem, s);
+}
+
+template <int ORD>
+int occupancy_o(const PipeArgs& P, size_t smem) {
+    const bool reg = P.sw.np <= kSweepThreads;
+    if (P.sw.rows_per_thread == 1) return reg ? occupancy_t<ORD, true, 1>(smem) : occupancy_t<ORD, false, 1>(smem);
+    return reg ? occupancy_t<ORD, true, 4>(smem) : occupancy_t<ORD, false, 4>(smem);
+}
+
+// ---------------------------------------------------------------- ordering the beam by xi cell
+// sort key of a particle: its xi cell + 1 (0 .. K), removed particles last (K + 1)
+__global__ void cell_keys_kernel(const BeamArgs B, unsigned* __restrict__ keys, int* __restrict__ vals,
+                                 int* __restrict__ nlive) {
+    int cnt = 0;
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += stride) {
+        const bool live = B.w[i] != 0.0;
+        keys[i] = live ? (unsigned)(xi_cell(B, B.xi[i]) + 1) : (unsigned)(B.K + 1);
+        vals[i] = (int)i;
+        cnt += live ? 1 : 0;
+    }
+    cnt = __reduce_add_sync(0xffffffffu, cnt);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd(nlive, cnt);
+}
+
+// dst = src permuted by idx (7 columns of n), orig_out = orig_in permuted the same way
+__global__ void gather7_kernel(const double* __restrict__ src, double* __restrict__ dst, const int* __restrict__ idx,
+                               const int* __restrict__ orig_in, int* __restrict__ orig_out, long n) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const long j = idx[p];
+#pragma unroll
+        for (int c = 0; c < 7; ++c) dst[c * n + p] = src[c * n + j];
+        orig_out[p] = orig_in[j];
+    }
+}
+
+// first sorted live particle of each group of span cells: start[g] = first i with key >= g * span
+// (keys sorted: cell + 1), start[ngroups] = nlive
+__global__ void group_starts_kernel(const unsigned* __restrict__ keys, long nlive, int span, int ngroups,
+                                    int* __restrict__ start) {
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g > ngroups) return;
+    if (g == ngroups) {
+        start[g] = (int)nlive;
+        return;
+    }
+    const unsigned key = (unsigned)g * (unsigned)span;
+    long lo = 0, hi = nlive;                          // lower bound of key in keys[0, nlive)
+    while (lo < hi) {
+        const long mid = (lo + hi) >> 1;
+        if (keys[mid] < key) lo = mid + 1; else hi = mid;
+    }
+    start[g] = (int)lo;
+}
+
+__global__ void iota_kernel(int* __restrict__ p, long n) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) p[i] = (int)i;
+}
+
+// dst[orig[p]] = src[p] for the 7 columns: back to the caller's particle order
+__global__ void scatter7_kernel(const double* __restrict__ src, double* __restrict__ dst, const int* __restrict__ orig,
+                                long n) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    for (long p = (long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += stride) {
+        const long j = orig[p];
+#pragma unroll
+        for (int c = 0; c < 7; ++c) dst[c * n + j] = src[c * n + p];
+    }
+}
+
+int grid_of(long n, int threads) {
+    long b = (n + threads - 1) / threads;
+    if (b > 148L * 8) b = 148L * 8;
+    return (int)(b < 1 ? 1 : b);
+}
+
+}  // namespace
+
+size_t cell_sort_temp_bytes(long n) {
+    size_t bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, bytes, (const unsigned*)nullptr, (unsigned*)nullptr, (const int*)nullptr,
+                                    (int*)nullptr, (int)n, 0, 32);
+    return bytes;
+}
+
+cudaError_t cell_sort(const BeamArgs& B, double* cols, double* stage, int* orig, int* orig_stage,
+                      const CellSortBuf& buf, cudaStream_t s) {
+    if (B.n <= 0) return cudaSuccess;
+    const int n = (int)B.n;
+    cudaError_t e = cudaMemsetAsync(buf.nlive, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    cell_keys_kernel<<<grid_of(n, 256), 256, 0, s>>>(B, buf.keys[0], buf.vals[0], buf.nlive);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    int bits = 1;
+    while ((1u << bits) <= (unsigned)(B.K + 1)) ++bits;
+    size_t bytes = buf.tmp_bytes;
+    e = cub::DeviceRadixSort::SortPairs(buf.tmp, bytes, buf.keys[0], buf.keys[1], buf.vals[0], buf.vals[1], n, 0, bits,
+                                        s);
+    if (e != cudaSuccess) return e;
+    gather7_kernel<<<grid_of(n, 256), 256, 0, s>>>(cols, stage, buf.vals[1], orig, orig_stage, (long)n);
+    return cudaGetLastError();
+}
+
+cudaError_t fill_iota(int* p, long n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    iota_kernel<<<grid_of(n, 256), 256, 0, s>>>(p, n);
+    return cudaGetLastError();
+}
+
+cudaError_t unpermute7(const double* src, double* dst, const int* orig, long n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    scatter7_kernel<<<grid_of(n, 256), 256, 0, s>>>(src, dst, orig, n);
+    return cudaGetLastError();
+}
+
+cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngroups, int* start, cudaStream_t s) {
+    group_starts_kernel<<<(ngroups + 1 + 127) / 128, 128, 0, s>>>(buf.keys[1], nlive, span, ngroups, start);
+    return cudaGetLastError();
+}
+
+size_t pipeline_smem_bytes(int M, bool dbuf, bool const_smem) {
+    const size_t sweep = sweep_m0_smem_bytes(M, dbuf, const_smem);
+    const size_t worker = sizeof(double) * 3 * (size_t)M + 64;
+    return sweep > worker ? sweep : worker;
+}
+
+int pipeline_max_grid(const PipeArgs& P, int* sms) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    *sms = nsm;
+    const size_t smem = pipeline_smem_bytes(P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    int per = 0;
+    switch (P.sw.ord) {
+        case 1: per = occupancy_o<1>(P, smem); break;
+        case 2: per = occupancy_o<2>(P, smem); break;
+        case 3: per = occupancy_o<3>(P, smem); break;
+        case 4: per = occupancy_o<4>(P, smem); break;
+        case 5: per = occupancy_o<5>(P, smem); break;
+        default: return 0;
+    }
+    return per * nsm;
+}
+
+cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream) {
+    if (P.sw.rows_per_thread < 1 || P.sw.rows_per_thread > 4) return cudaErrorInvalidValue;
+    if (P.nsweep < 1 || grid <= P.nsweep || P.ring < 2 || P.nbeams > kMaxBeams) return cudaErrorInvalidValue;
+    const size_t smem = pipeline_smem_bytes(P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    switch (P.sw.ord) {
+        case 1: return launch_o<1>(P, grid, smem, stream);
+        case 2: return launch_o<2>(P, grid, smem, stream);
+        case 3: return launch_o<3>(P, grid, smem, stream);
+        case 4: return launch_o<4>(P, grid, smem, stream);
+        case 5: return launch_o<5>(P, grid, smem, stream);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_moments_reduce(const PipeArgs& P, double* mom, cudaStream_t s) {
+    if (!P.pmom || P.nbeams < 1) return cudaSuccess;
+    moments_reduce_kernel<<<(P.nsteps + 1) * P.nbeams, 32, 0, s>>>(P, mom);
+    return cudaGetLastError();
+}
+
+}  // namespace qzb

@@ -41,6 +41,11 @@ struct NoGate {
     __device__ bool before_rows(int) { return true; }       // thread 0: beam-source rows <= row are final
     __device__ void slice_done_all(int) {}                   // every thread, after its stores of slice k
     __device__ bool slice_done(int) { return true; }         // thread 0, after the barrier: publish slice k
+    // this sweep's buffers
+    __device__ const double* bsrc(const SweepArgs& A) const { return A.bsrc; }
+    __device__ double* fld(const SweepArgs& A) const { return A.fld; }
+    __device__ double* diag(const SweepArgs& A) const { return A.diag; }
+    __device__ double* ps(const SweepArgs& A) const { return A.ps; }
 };
 
 // ---------------------------------------------------------------- block scans
@@ -408,9 +413,9 @@ template <bool kL2>                       // kL2: the rows were written by other
 __device__ __forceinline__ double ldb(const double* p) { return kL2 ? __ldcg(p) : *p; }
 
 template <bool kL2>
-__device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, int k, int j) {
+__device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
-    const double* bk = A.bsrc + (size_t)k * st + (size_t)j * B_NC0;
+    const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC0;
     BeamRow r;
     r.rt = ldb<kL2>(bk + B_RT0);
     r.jz = ldb<kL2>(bk + B_JZ0);
@@ -718,7 +723,7 @@ using namespace sweep_detail;
 // several time steps run concurrently (NoGate: a stand-alone sweep). Returns false if a gate wait
 // gave up (the CTA then stops at the next slice boundary).
 template <int ORD, bool REG, int kMaxR, class Gate>
-__device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw, Gate& G) {
+__device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw, Gate& gate) {
     const int M = A.M, N = A.N, K = A.K, Rw = kMaxR == 1 ? 1 : A.rows_per_thread;   // rows per thread
     const int tid = threadIdx.x;
     const Smem S = carve(smem_raw, A);
@@ -783,8 +788,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     } else {
         for (int p = tid; p < np; p += kThreads) {
 #pragma unroll
-            for (int v = 0; v < 6; ++v) A.ps[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
-            for (int v = 0; v < 5 * ORD; ++v) A.ps[(size_t)(6 + v) * npad + p] = 0.0;
+            for (int v = 0; v < 6; ++v) gate.ps(A)[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
+            for (int v = 0; v < 5 * ORD; ++v) gate.ps(A)[(size_t)(6 + v) * npad + p] = 0.0;
         }
     }
     __syncthreads();
@@ -812,13 +817,13 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             add_multi<2>(adr, val);
         }
     }
-    if (Gate::kActive && tid == 0) *S.flag = G.before_rows(K - 1 < 2 ? K - 1 : 2) ? 1 : 0;
+    if (Gate::kActive && tid == 0) *S.flag = gate.before_rows(K - 1 < 2 ? K - 1 : 2) ? 1 : 0;
     __syncthreads();
     if (Gate::kActive && !*S.flag) return false;
     for (int j = tid; j < M; j += kThreads) {
         const Src s0 = src_of(S, M, 0);
         if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
-        init_sources(s0, S, j, beam_row<Gate::kActive>(A, 0, j));
+        init_sources(s0, S, j, beam_row<Gate::kActive>(A, gate.bsrc(A), 0, j));
     }
     __syncthreads();
     // deposit of slice 0
@@ -840,7 +845,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             int j = 0;
             double v[12];
             if (p < np) {
-                pload(Q, A.ps, npad, p);
+                pload(Q, gate.ps(A), npad, p);
                 species_params(A, p, Q.q, Q.qm);
                 act = Q.w != 0.0;
                 if (act) {
@@ -866,7 +871,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         if (A.dbuf && k + 1 < K)
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u)
-                if (u < Rw && row0 + u < M) pre[u] = beam_row<Gate::kActive>(A, k + 1, row0 + u);
+                if (u < Rw && row0 + u < M) pre[u] = beam_row<Gate::kActive>(A, gate.bsrc(A), k + 1, row0 + u);
 
         // ---------------- P2: psi, E_z, B_z with L0 (src/Simulation.cpp:797-807, :501-532)
         {
@@ -974,7 +979,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 double v[4];
                 if (p < np) {
                     PState<ORD> Q;
-                    pload(Q, A.ps, npad, p);
+                    pload(Q, gate.ps(A), npad, p);
                     species_params(A, p, Q.q, Q.qm);
                     act = Q.w != 0.0;
                     if (act) {
@@ -1088,14 +1093,14 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         {
             const size_t fb = (size_t)k * M;
             for (int j = tid; j < M; j += kThreads) {
-                double* F = A.fld + (fb + j) * F_NC0;
+                double* F = gate.fld(A) + (fb + j) * F_NC0;
                 F[F_EP1R] = S.wr1[j] + S.bpi[j];
                 F[F_EP1I] = 0.0 - S.bpr[j];
                 F[F_BP1R] = S.bpr[j];
                 F[F_BP1I] = S.bpi[j];
                 F[F_EZ0] = S.ez[j];
                 F[F_BZ0] = S.bz[j];
-                double* D = A.diag + (fb + j) * D_NC0;
+                double* D = gate.diag(A) + (fb + j) * D_NC0;
                 D[D_PSI0] = S.psi[j];
                 D[D_NE0] = s.ne[j];
                 D[D_NI0] = s.ni[j];
@@ -1104,7 +1109,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         if (k + 1 < K) {
             if (!A.dbuf) {
                 __syncthreads();                                    // the store read the sources
-                for (int j = tid; j < M; j += kThreads) init_sources(sn, S, j, beam_row<Gate::kActive>(A, k + 1, j));
+                for (int j = tid; j < M; j += kThreads) init_sources(sn, S, j, beam_row<Gate::kActive>(A, gate.bsrc(A), k + 1, j));
                 __syncthreads();
             }
             const bool first = (k == 0);
@@ -1130,7 +1135,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                     double v[12];
                     PState<ORD> Q;
                     if (p < np) {
-                        pload(Q, A.ps, npad, p);
+                        pload(Q, gate.ps(A), npad, p);
                         species_params(A, p, Q.q, Q.qm);
                         if (Q.w != 0.0) {
                             const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
@@ -1142,23 +1147,23 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                             } else {
                                 atomicAdd(S.lost, 1);
                             }
-                            pstore(Q, A.ps, npad, p);
+                            pstore(Q, gate.ps(A), npad, p);
                         }
                     }
                     deposit_warp(act, j, act && Q.q < 0.0, v, sn);
                 }
             }
         }
-        if (Gate::kActive) G.slice_done_all(k);                     // every thread, before the barrier
+        if (Gate::kActive) gate.slice_done_all(k);                     // every thread, before the barrier
         __syncthreads();
         PHASE_MARK(4);
         if (Gate::kActive) {
-            if (tid == 0) *S.flag = (G.slice_done(k) && (k + 1 >= K || G.before_rows(k + 3 < K ? k + 3 : K - 1))) ? 1 : 0;
+            if (tid == 0) *S.flag = (gate.slice_done(k) && (k + 1 >= K || gate.before_rows(k + 3 < K ? k + 3 : K - 1))) ? 1 : 0;
             __syncthreads();
             if (!*S.flag) return false;
         }
     }
-    if (REG && tid < np) pstore(P, A.ps, npad, tid);
+    if (REG && tid < np) pstore(P, gate.ps(A), npad, tid);
     if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
     return true;
 #undef PHASE_MARK
