@@ -1,14 +1,16 @@
 #!/usr/bin/env python
-"""Benchmark of the QUARZ hot path on B200: one time step of the pinched-witness workload.
+"""Benchmark of the QUARZ hot path on B200: the pinched-witness run.
 
 Workload (quarz_b200.workloads.pinched_witness): m = 0, 512 stretched radial nodes (5e-4 -> 0.05),
 2400 xi slices (dxi 0.005), ppc 1 cold plasma (511 rings per slice), driver 1e6 + witness 1e6 beam
-particles, dt 5. One step = one quasi-static sweep (2400 slice solves) + the Vay push of both beams
-with the next step's beam deposit fused in.
+particles, dt 5, 100 time steps. One bench step = the whole run as Simulation::run does it: 101
+quasi-static sweeps (2400 slice solves each), the moment sums of every step, and 100 Vay pushes of
+both beams with the next step's deposit, through the library's public call (qz_sim_run), starting
+every time from the same initial beams (resident in HBM).
 
-Metric: slice-solves/s = K * steps / time (whole job: summed over GPUs; each GPU runs an independent
-replica of the workload -- the sweep is sequential in xi, so there is no data-path collective).
-Also reported: beam pushes/s.
+Metric: slice-solves/s = K * (time steps + 1) / time (whole job: summed over GPUs; each GPU runs an
+independent replica -- the sweep is sequential in xi, so there is no data-path collective). Also
+reported: beam pushes/s.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 """
@@ -17,6 +19,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import sys
 import threading
 import time
@@ -27,6 +30,10 @@ sys.path.insert(0, ROOT)
 METRIC = "slice-solves/s"
 UNIT = "slice-solves/s"
 WORKLOAD = "pinched_witness"
+# our kernels per run, per beam: iota + cell keys + reorder + group starts + step-0 deposit; per run:
+# the pipelined kernel + the moment reduction (the radix sort's own kernels are library code)
+OWN_LAUNCHES_PER_BEAM = 5
+OWN_LAUNCHES_PER_RUN = 2
 
 
 def _peaks():
@@ -38,15 +45,39 @@ def _peaks():
         return 6650.0, "fallback"
 
 
-def _config(spec, nb_total, extra=None):
+def _traffic_ratio():
+    """DRAM bytes per algorithmic byte of the pipelined kernel, from the ncu capture of a shorter run of
+    the same workload summarised in profiles/ (traffic grows with the steps like the algorithmic bytes),
+    or None."""
+    path = os.path.join(ROOT, "profiles", "pipeline_kernel_pinched_witness.md")
+    try:
+        with open(path) as f:
+            m = re.search(r"dram_bytes_per_algorithmic_byte:\s*([0-9.eE+]+)", f.read())
+        return float(m.group(1)) if m else None
+    except OSError:
+        return None
+
+
+def _config(spec, nb_total, steps, extra=None):
     c = {"workload": WORKLOAD, "modes": spec.modes, "radial_nodes": spec.M, "xi_slices": spec.K,
          "dxi": spec.dxi, "plasma_ppc": spec.species[0].ppc, "plasma_particles_per_slice": spec.M - 1,
-         "beam_particles": nb_total, "ab_order": spec.ab_order, "dt": spec.dt,
-         "l2": "inputs larger than L2: beam 112 MB + field store 59 MB + beam sources 49 MB per step",
+         "beam_particles": nb_total, "ab_order": spec.ab_order, "dt": spec.dt, "time_steps_per_run": steps,
+         "l2": "inputs larger than L2: beams 112 MB + a field store of 59 MB and beam sources of 49 MB per step "
+               "in flight (rings of one slot per step)",
          "parallelism": "replicas"}
     if extra:
         c.update(extra)
     return c
+
+
+def algorithmic_bytes(spec, nb_total, steps):
+    """HBM bytes a run must move at least: per sweep the beam sources read (5 doubles per node and
+    slice) and the fields + diagnostics written (6 + 3); per push step every particle read and written
+    (7 doubles each way), the field store read once (6) and the next beam sources written once (5)."""
+    km = spec.K * spec.M
+    sweep = km * (5 + 6 + 3) * 8
+    push = nb_total * 7 * 8 * 2 + km * (6 + 5) * 8
+    return (steps + 1) * sweep + steps * push
 
 
 class ClockSampler:
@@ -99,129 +130,99 @@ class ClockSampler:
                 "samples": len(self.samples)}
 
 
+def _workload(args):
+    from quarz_b200 import workloads
+
+    spec = workloads.pinched_witness()
+    if args.time_steps:
+        spec.steps = args.time_steps
+    return spec
+
+
 def run_b200(args, rank, world, local_rank):
     import numpy as np
     import torch
 
     import quarz_b200 as Q
-    from quarz_b200 import workloads
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    spec = workloads.pinched_witness()
+    spec = _workload(args)
+    T = spec.steps
     beams = [Q.sample_beam(b) for b in spec.beams]
-    K, M = spec.K, spec.M
-    grid = Q.RadialGrid(spec.nodes)
-    sweep = Q.Sweep(grid, Q.sweep_params(spec))
-    f64 = dict(dtype=torch.float64, device=dev)
-    fld = torch.zeros(K * M * 6, **f64)
-    diag = torch.zeros(K * M * 3, **f64)
-    bsrc = [torch.zeros(K * M * 5, **f64), torch.zeros(K * M * 5, **f64)]
-    cols = [torch.from_numpy(np.ascontiguousarray(p.T)).to(dev).contiguous() for p, _, _ in beams]
     nb_total = sum(len(p) for p, _, _ in beams)
-    box = Q.BeamOps.box(spec.xi_min, spec.dxi, K, spec.ngp, spec.modes)
+    sim = Q.Simulation(spec, beams=beams)
+    init = [torch.from_numpy(np.ascontiguousarray(p.T)).to(dev).contiguous() for p, _, _ in beams]
     stream = torch.cuda.Stream(device=dev)
-    started = [0] * len(beams)
-    state = {"cur": 0}
-    dt = spec.dt
+    kernel_ms, moments = [], []
 
-    def step(ev=None):
-        cur, nxt = state["cur"], 1 - state["cur"]
-        if ev is not None:
-            ev[0].record(stream)
-        sweep.run_async(bsrc[cur], fld, diag, stream=stream)
-        if ev is not None:
-            ev[1].record(stream)
-        bsrc[nxt].zero_()
-        if ev is not None:
-            ev[2].record(stream)
-        for i, b in enumerate(spec.beams):
-            started[i] = Q.BeamOps.push_deposit(grid, cols[i], b.q, b.m, box, fld, dt, dt, started[i], bsrc[nxt],
-                                                stream=stream)
-        if ev is not None:
-            ev[3].record(stream)
-        state["cur"] = nxt
+    def one():
+        for b in range(len(init)):
+            sim.set_beam(b, init[b], stream=stream)
+        moments.append(sim.run(T, spec.dt, stream=stream))
+        kernel_ms.append(sim.times()["kernel_ms"])
 
-    with torch.cuda.stream(stream):
-        for i, b in enumerate(spec.beams):
-            Q.BeamOps.deposit(grid, cols[i], b.q, b.m, box, bsrc[0], stream=stream)
-        for _ in range(args.warmup):
-            step()
-    # the first push includes the leapfrog start-up kick; all timed steps are regular ones
+    for _ in range(args.warmup):
+        one()
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    evs = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    kernel_ms.clear()
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local_rank) as clk:
         torch.cuda.synchronize(dev)
-        with torch.cuda.stream(stream):
-            t0.record(stream)
-            for s in range(args.steps):
-                step(evs[s])
-            t1.record(stream)
+        t0.record(stream)
+        for _ in range(args.steps):
+            one()
+        t1.record(stream)
         torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
     ms = t0.elapsed_time(t1)
-    sweep_ms = [e[0].elapsed_time(e[1]) for e in evs]
-    push_ms = [e[2].elapsed_time(e[3]) for e in evs]
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
-    launches_per_step = 1 + len(spec.beams)   # sweep kernel + fused push/deposit per beam
-    # end-to-end through the host-buffer call of the C ABI (qz_sim_step_host)
-    e2e = run_e2e(args, spec, beams, dev) if args.e2e_steps > 0 else None
-    out = {
-        "ms": ms, "sweep_ms": sweep_ms, "push_ms": push_ms, "clocks": clk.result(), "spec": spec,
-        "nb_total": nb_total, "launches": launches_per_step * args.steps, "e2e": e2e,
-    }
-    return out
+    sched = sim.schedule()
+    e2e = run_e2e(args, spec, beams, sim, dev) if args.e2e_steps > 0 else None
+    launches = (OWN_LAUNCHES_PER_BEAM * len(beams) + OWN_LAUNCHES_PER_RUN) * args.steps
+    return {"ms": ms, "kernel_ms": kernel_ms, "clocks": clk.result(), "spec": spec, "nb_total": nb_total,
+            "launches": launches, "e2e": e2e, "schedule": sched}
 
 
-def run_e2e(args, spec, beams, dev):
-    import ctypes as C
-
+def run_e2e(args, spec, beams, sim, dev):
+    """The same run through the host-buffer call (qz_sim_run_host): the beams are copied in from pinned
+    host memory and back out every run, inside the timed region."""
     import numpy as np
     import torch
 
-    import quarz_b200 as Q
-    from quarz_b200._lib import check, lib
-
-    sim = Q.Simulation(spec, beams=beams)
     host = [torch.from_numpy(np.ascontiguousarray(p.T)).contiguous().pin_memory() for p, _, _ in beams]
-    ptrs = (C.c_void_p * len(host))(*[h.data_ptr() for h in host])
-    mom = np.zeros((len(beams), 17))
+    init = [h.clone() for h in host]
     stream = torch.cuda.Stream(device=dev)
-    sp = C.c_void_p(stream.cuda_stream)
-    dt = spec.dt
-
-    def one():
-        check(lib().qz_sim_step_host(sim.h, ptrs, dt, dt, 1, mom.ctypes.data_as(C.POINTER(C.c_double)), sp))
-
-    for _ in range(2):
-        one()
-    torch.cuda.synchronize(dev)
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(args.e2e_steps):
-        one()
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1) / args.e2e_steps
+    ms = []
+    for i in range(1 + args.e2e_steps):
+        for h, h0 in zip(host, init):
+            h.copy_(h0)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.run_host(spec.steps, spec.dt, host, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        if i > 0:                                   # the first call is a warm-up
+            ms.append(e0.elapsed_time(e1))
     nbytes = sum(7 * 8 * len(p) for p, _, _ in beams)
-    return {"ms_per_step": ms, "h2d_bytes_per_step": nbytes, "d2h_bytes_per_step": nbytes + 17 * 8 * len(beams)}
+    return {"ms_per_run": sum(ms) / len(ms), "h2d_bytes_per_step": nbytes,
+            "d2h_bytes_per_step": nbytes + 17 * 8 * len(beams) * (spec.steps + 1)}
 
 
-def oracle_step_rate(steps, warmup, spec=None):
-    """The CPU oracle (serial restatement of the reference path) on the same workload: slice-solves/s."""
+def oracle_rate(time_steps, warmup, spec):
+    """The CPU oracle (serial restatement of the reference path) on the same workload: slice-solves/s
+    over time_steps full time steps (sweep + moment sums + push), after warm-up steps."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
-    from quarz_b200 import workloads
 
     O.build()
-    spec = spec or workloads.pinched_witness()
     sim = O.OracleSim(spec)
     dt = spec.dt
     sim.step_fields(0.0)
@@ -230,22 +231,25 @@ def oracle_step_rate(steps, warmup, spec=None):
         sim.step_fields(0.0)
         sim.push_beams(dt, dt)
     t = time.perf_counter()
-    for _ in range(steps):
+    for _ in range(time_steps):
         sim.step_fields(0.0)
+        for b in range(len(spec.beams)):
+            sim.beam_sums(b)
         sim.push_beams(dt, dt)
     el = time.perf_counter() - t
-    return spec.K * steps / el, el, spec
+    return spec.K * time_steps / el, el
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=5, help="timed runs (each: the workload's time steps)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--e2e-steps", type=int, default=5)
-    ap.add_argument("--cpu-steps", type=int, default=10, help="oracle steps of the cpu_baseline sample")
+    ap.add_argument("--e2e-steps", type=int, default=3, help="timed runs through the host-buffer call")
+    ap.add_argument("--cpu-steps", type=int, default=10, help="oracle time steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's 100)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -254,62 +258,63 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        rate, el, spec = oracle_step_rate(args.steps, args.warmup)
+        spec = _workload(args)
+        # each bench step is one full time step of the oracle (a bounded sample of the run)
+        rate, el = oracle_rate(args.steps, args.warmup, spec)
         nb = sum(b.nparticles for b in spec.beams)
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": _config(spec, nb),
+                "data": "synthetic", "config": _config(spec, nb, spec.steps),
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                                 "sample": f"{args.steps} full time steps of the workload (sweep + beam push) "
-                                           f"after {args.warmup} warm-up steps, serial oracle"},
+                                 "sample": f"{args.steps} full time steps of the workload (sweep + moment sums + "
+                                           f"beam push) after {args.warmup} warm-up steps, serial oracle"},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
 
     if world > 1:
+        import datetime
+
         import torch
 
-        torch.distributed.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     r = run_b200(args, rank, world, local_rank)
     spec = r["spec"]
-    K = spec.K
-    ms_step = r["ms"] / args.steps
-    value = world * K * args.steps / (r["ms"] * 1e-3)
-    # roofline of the dominant kernel (the sweep): algorithmic HBM bytes per slice =
-    # beam-source row read (5 M doubles) + field row and diagnostics written ((6 + 3) M doubles)
-    sweep_ms = sorted(r["sweep_ms"])[len(r["sweep_ms"]) // 2]
-    bytes_sweep = K * spec.M * (5 + 6 + 3) * 8
-    hbm, peak_kind = _peaks()
-    achieved = bytes_sweep / (sweep_ms * 1e-3) / 1e9
-    push_ms = sorted(r["push_ms"])[len(r["push_ms"]) // 2]
+    K, T = spec.K, spec.steps
     nbt = r["nb_total"]
-    bytes_push = nbt * (7 * 8 + 7 * 8) + K * spec.M * (6 + 5) * 8   # particles read+written, fld read, bsrc write
-    push_gbs = bytes_push / (push_ms * 1e-3) / 1e9
+    ms_step = r["ms"] / args.steps
+    value = world * K * (T + 1) * args.steps / (r["ms"] * 1e-3)
+    # roofline of the dominant kernel (the pipelined run: one launch per bench step)
+    kms = sorted(r["kernel_ms"])[len(r["kernel_ms"]) // 2]
+    alg = algorithmic_bytes(spec, nbt, T)
+    hbm, peak_kind = _peaks()
+    achieved = alg / (kms * 1e-3) / 1e9
+    ratio = _traffic_ratio()
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": _config(spec, nbt),
-        "beam_pushes_per_s": world * nbt / (push_ms * 1e-3),
-        "sweep_ms": sweep_ms, "per_slice_us": 1e3 * sweep_ms / K, "push_deposit_ms": push_ms,
-        "roofline": {"bound": "hbm", "kernel": "sweep_m0_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                     "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": None,
-                     "note": "one CTA on one SM, latency-bound chain of 5 barrier phases per slice; "
-                             "algorithmic bytes = K*M*(5+6+3)*8 per sweep"},
-        "roofline_beam": {"bound": "hbm", "kernel": "beam_push_kernel<deposit>", "achieved": push_gbs, "peak": hbm,
-                          "unit": "GB/s", "frac": push_gbs / hbm, "peak_kind": peak_kind},
+        "data": "synthetic", "config": _config(spec, nbt, T, {"schedule": r["schedule"]}),
+        "beam_pushes_per_s": world * nbt * T * args.steps / (r["ms"] * 1e-3),
+        "kernel_ms_per_run": kms, "per_sweep_ms": kms / (T + 1),
+        "roofline": {"bound": "hbm", "kernel": "pipeline_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                     "frac": achieved / hbm, "peak_kind": peak_kind,
+                     "traffic": ratio * alg if ratio else None,
+                     "algorithmic_bytes": alg,
+                     "note": "one launch per run; its floor is one sweep's dependent chain (K slices, one SM) "
+                             "plus the step-to-step stagger, not HBM: see DESIGN.md"},
         "clocks": r["clocks"], "gpu_launches": r["launches"],
     }
     if r["e2e"]:
         e = r["e2e"]
-        line["e2e"] = {"value": world * K / (e["ms_per_step"] * 1e-3), "unit": UNIT,
+        line["e2e"] = {"value": world * K * (T + 1) / (e["ms_per_run"] * 1e-3), "unit": UNIT,
                        "h2d_bytes_per_step": e["h2d_bytes_per_step"], "d2h_bytes_per_step": e["d2h_bytes_per_step"],
-                       "ms_per_step": e["ms_per_step"]}
+                       "ms_per_step": e["ms_per_run"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        rate, el, _ = oracle_step_rate(args.cpu_steps, 1, spec)
+        rate, el = oracle_rate(args.cpu_steps, 1, spec)
         line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
-                                "sample": f"{args.cpu_steps} full time steps of the same workload (sweep + beam push), "
-                                          f"serial oracle, {el:.1f} s"}
+                                "sample": f"{args.cpu_steps} full time steps of the same workload (sweep + moment "
+                                          f"sums + beam push), serial oracle, {el:.1f} s"}
     if world > 1:
         import torch
 

@@ -182,6 +182,12 @@ qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int buck
 /* the schedule of the last qz_sim_run: grid, sweep CTAs, push CTAs, ring slots, buckets, bucket size,
    pipelined (1/0), cell span of a bucket */
 qz_status qz_sim_schedule(qz_sim* s, int* info8);
+/* GPU time (ms, CUDA events on the run's stream) of the parts of the last pipelined run: [0] set-up
+   (beam ordering, buckets, step-0 beam deposit), [1] the pipelined kernel, [2] moments and copies. */
+qz_status qz_sim_times(qz_sim* s, double* ms3);
+/* Replace beam b's particles (7 x n SoA in the caller's order, x y px py pz xi w) from device memory
+   (on_device = 1) or host memory; the started flag of the leapfrog is kept. */
+qz_status qz_sim_set_beam(qz_sim* s, int b, const double* cols7, int on_device, void* stream);
 /* Timeline of the last pipelined run, 22 values per step n: GPU clock (ns, %globaltimer) at the start
    and the end of sweep n, when it had stored 1/16, 2/16, ... 16/16 of the slices, then its longest
    wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 3 totals of

@@ -78,6 +78,8 @@ SIGNATURES = {
     "qz_sim_step_host": [C.c_void_p, C.POINTER(C.c_void_p), C.c_double, C.c_double, C.c_int, _dp, C.c_void_p],
     "qz_sim_set_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double],
     "qz_sim_schedule": [C.c_void_p, C.POINTER(C.c_int)],
+    "qz_sim_times": [C.c_void_p, _dp],
+    "qz_sim_set_beam": [C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_void_p],
     "qz_sim_trace": [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong), C.c_int, C.POINTER(C.c_int)],
     "qz_sim_run_host": [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_void_p), _dp, C.c_void_p],
 }

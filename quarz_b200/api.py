@@ -245,6 +245,20 @@ class Simulation:
         keys = ("grid", "sweep_ctas", "push_ctas", "ring", "buckets", "bucket", "pipelined", "span")
         return dict(zip(keys, list(info)))
 
+    def times(self) -> dict:
+        """GPU ms of the parts of the last pipelined run (qz_sim_times)."""
+        t = np.zeros(3)
+        check(lib().qz_sim_times(self.h, _p(t)))
+        return {"setup_ms": t[0], "kernel_ms": t[1], "finish_ms": t[2]}
+
+    def set_beam(self, b: int, cols, stream=None) -> None:
+        """qz_sim_set_beam: beam b's particles from a (7, n) float64 array, numpy (host) or torch (device)."""
+        if isinstance(cols, np.ndarray):
+            cols = np.ascontiguousarray(cols, dtype=np.float64)
+            check(lib().qz_sim_set_beam(self.h, int(b), cols.ctypes.data, 0, _stream_ptr(stream)))
+        else:
+            check(lib().qz_sim_set_beam(self.h, int(b), _dev(cols), 1, _stream_ptr(stream)))
+
     def trace(self, enable: bool = True) -> np.ndarray:
         """Timeline of the last pipelined run (qz_sim_trace): per step (start, end, 16 progress marks) in ns
         of GPU clock, and the push workers' (tasks, empty scans, lost claims); enable turns the recording

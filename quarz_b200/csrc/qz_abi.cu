@@ -642,6 +642,8 @@ struct qz_sim {
         unsigned long long* d_trace = nullptr;
         size_t trace_n = 0;
         std::vector<unsigned long long> h_trace;
+        cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};   // start, launch, kernel end, end
+        float times[3] = {0, 0, 0};
         double *fld = nullptr, *diag = nullptr, *bsrc = nullptr;
         int ring = 0;
         bool clean = false;                        // every beam-source slot is zero
@@ -669,6 +671,8 @@ struct qz_sim {
                         (void*)pipe.sort.vals[0], (void*)pipe.sort.vals[1], pipe.sort.tmp, (void*)pipe.sort.nlive,
                         (void*)pipe.cmin, (void*)pipe.d_trace})
             if (q) cudaFree(q);
+        for (cudaEvent_t e : pipe.ev)
+            if (e) cudaEventDestroy(e);
         qz_sweep_destroy(sw);
     }
 };
@@ -764,6 +768,9 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     auto& P_ = s->pipe;
     const int K = s->p.K, M = s->g->M, nb = (int)s->beams.size();
     const qz_box box = sim_box(s);
+    if (!P_.ev[0])
+        for (auto& e : P_.ev) QZ_CUDA(cudaEventCreate(&e));
+    QZ_CUDA(cudaEventRecord(P_.ev[0], st));
     // 1. order each beam by xi cell; buckets of P_.bucket live particles
     long nmax = 1;
     for (auto& b : s->beams) nmax = std::max<long>(nmax, (long)b.n);
@@ -933,7 +940,9 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         QZ_CUDA(cudaMemsetAsync(P_.d_trace, 0, sizeof(unsigned long long) * ntr, st));
         A.trace = P_.d_trace;
     }
+    QZ_CUDA(cudaEventRecord(P_.ev[1], st));
     QZ_CUDA(qzb::launch_pipeline(A, g1, st));
+    QZ_CUDA(cudaEventRecord(P_.ev[2], st));
     if (moms) QZ_CUDA(qzb::launch_moments_reduce(A, P_.mom, st));
     int err = 0;
     unsigned long long h[4];
@@ -952,7 +961,9 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         QZ_CUDA(cudaMemcpyAsync(P_.h_trace.data(), P_.d_trace, sizeof(unsigned long long) * P_.h_trace.size(),
                                 cudaMemcpyDeviceToHost, st));
     }
+    QZ_CUDA(cudaEventRecord(P_.ev[3], st));
     QZ_CUDA(cudaStreamSynchronize(st));
+    for (int i = 0; i < 3; ++i) QZ_CUDA(cudaEventElapsedTime(&P_.times[i], P_.ev[i], P_.ev[i + 1]));
     s->cnt.lost += h[0];
     s->bsrc_valid = false;
     const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 2};
@@ -1048,6 +1059,22 @@ extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_cta
 extern "C" qz_status qz_sim_schedule(qz_sim* s, int* info8) {
     if (!s || !info8) return fail(QZ_ERR_ARG, "qz_sim_schedule: null pointer");
     std::copy(s->pipe.info, s->pipe.info + 8, info8);
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_times(qz_sim* s, double* ms3) {
+    if (!s || !ms3) return fail(QZ_ERR_ARG, "qz_sim_times: null pointer");
+    for (int i = 0; i < 3; ++i) ms3[i] = s->pipe.times[i];
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_set_beam(qz_sim* s, int b, const double* cols7, int on_device, void* stream) {
+    if (!s || !cols7 || b < 0 || b >= (int)s->beams.size()) return fail(QZ_ERR_ARG, "qz_sim_set_beam: bad argument");
+    auto& B = s->beams[b];
+    QZ_CUDA(cudaMemcpyAsync(B.d, cols7, sizeof(double) * 7 * B.n,
+                            on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, (cudaStream_t)stream));
+    B.orig_identity = true;
+    s->bsrc_valid = false;
     return QZ_OK;
 }
 
