@@ -52,10 +52,11 @@ struct qz_grid {
     double flux_coef = 0;
     std::vector<double> gm, g0, gp, ir;
     std::vector<double> consts;  // per-node constants of the sweep (13 x M)
+    std::vector<double> consts1; // and of the modes = 1 sweep (9 x M)
     // device
-    double *d_r = nullptr, *d_inv_h = nullptr, *d_inv_V = nullptr, *d_consts = nullptr;
+    double *d_r = nullptr, *d_inv_h = nullptr, *d_inv_V = nullptr, *d_consts = nullptr, *d_consts1 = nullptr;
     ~qz_grid() {
-        for (double* p : {d_r, d_inv_h, d_inv_V, d_consts})
+        for (double* p : {d_r, d_inv_h, d_inv_V, d_consts, d_consts1})
             if (p) cudaFree(p);
     }
 };
@@ -175,10 +176,29 @@ extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
         put(7, g->opa[1]); put(8, g->opb[1]); put(9, g->opc[1]);
         put(10, g->opa[2]); put(11, g->opb[2]); put(12, g->opc[2]);
         g->consts = cs;
+        // modes = 1: Thomas factors of L1D (its Dirichlet rows 0 and N are rows b = 1), L0 and L2D rows
+        std::vector<double> c1((size_t)9 * M, 0.0);
+        const std::vector<double>&a1 = g->opa[1], &b1 = g->opb[1], &cc1 = g->opc[1];
+        cp = 0.0;
+        for (int i = 0; i < M; ++i) {
+            const double rr = 1.0 / (b1[i] - (i > 0 ? a1[i] * cp : 0.0));
+            cp = cc1[i] * rr;
+            c1[i] = rr;
+            c1[(size_t)M + i] = -rr * a1[i];
+            c1[(size_t)2 * M + i] = -cp;
+        }
+        std::copy(a0.begin(), a0.end(), c1.begin() + (size_t)3 * M);
+        std::copy(b0.begin(), b0.end(), c1.begin() + (size_t)4 * M);
+        std::copy(c0.begin(), c0.end(), c1.begin() + (size_t)5 * M);
+        std::copy(g->opa[3].begin(), g->opa[3].end(), c1.begin() + (size_t)6 * M);
+        std::copy(g->opb[3].begin(), g->opb[3].end(), c1.begin() + (size_t)7 * M);
+        std::copy(g->opc[3].begin(), g->opc[3].end(), c1.begin() + (size_t)8 * M);
+        g->consts1 = c1;
     }
     qz_status st;
     if ((st = dev_upload(&g->d_r, g->r)) || (st = dev_upload(&g->d_inv_h, g->inv_h)) ||
-        (st = dev_upload(&g->d_inv_V, g->inv_V)) || (st = dev_upload(&g->d_consts, g->consts))) {
+        (st = dev_upload(&g->d_inv_V, g->inv_V)) || (st = dev_upload(&g->d_consts, g->consts)) ||
+        (st = dev_upload(&g->d_consts1, g->consts1))) {
         delete g;
         return st;
     }
@@ -214,12 +234,13 @@ struct qz_sweep {
     double* d_pinit = nullptr;
     double* d_bg = nullptr;
     double* d_ps = nullptr;
+    double* d_bgs = nullptr;              // modes = 1: background (3, M) and two source buffers (2 x 30, M)
     unsigned long long* d_cnt = nullptr;
     unsigned long long* d_tim = nullptr;
     bool timing = false;
     qzb::SweepArgs base{};
     ~qz_sweep() {
-        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_cnt, (void*)d_tim})
+        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_bgs, (void*)d_cnt, (void*)d_tim})
             if (q) cudaFree(q);
     }
 };
@@ -262,8 +283,9 @@ void load_species(const qz_grid& g, const qz_species& sp, std::vector<double> co
 extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p, qz_sweep** out) {
     if (!g || !p || !out) return fail(QZ_ERR_ARG, "qz_sweep_create: null pointer");
     *out = nullptr;
-    if (p->modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_create: modes = 1 is not built yet");
+    if (p->modes != 0 && p->modes != 1) return fail(QZ_ERR_ARG, "qz_sweep_create: modes must be 0 or 1");
     if (p->ab_order < 1 || p->ab_order > 5) return fail(QZ_ERR_ARG, "pusher.ab_order must be 1..5");
+    if (p->modes == 1 && p->picard < 1) return fail(QZ_ERR_ARG, "solver.picard must be >= 1");
     if (p->K < 1 || !(p->dxi > 0)) return fail(QZ_ERR_ARG, "xi: need K >= 1 and dxi > 0");
     if (p->nspecies < 0 || p->nspecies > 4) return fail(QZ_ERR_ARG, "nspecies must be 0..4");
     const int M = g->M;
@@ -277,6 +299,9 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     for (int i = 0; i < 4 && lay < 0; ++i)
         if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1]) <= (size_t)optin) lay = i;
     const int rpt = (M + qzb::kSweepThreads - 1) / qzb::kSweepThreads;
+    if (p->modes == 1 && (M > qzb::kSweepThreads || qzb::sweep_m1_smem_bytes(M) > (size_t)optin))
+        return fail(QZ_ERR_SIZE, "qz_sweep_create: the modes = 1 sweep holds one radial node per thread: M = " +
+                                     std::to_string(M) + " > " + std::to_string(qzb::kSweepThreads));
     if (lay < 0 || rpt > 4)
         return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " is too large for one CTA (" +
                                      std::to_string(qzb::sweep_m0_smem_bytes(M, false, false)) + " B of shared memory, "
@@ -325,6 +350,7 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     }
     const size_t nps = (size_t)(6 + 5 * p->ab_order) * s->npad;
     if (cudaMalloc((void**)&s->d_ps, sizeof(double) * nps) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_bgs, sizeof(double) * 63 * M) != cudaSuccess ||
         cudaMalloc((void**)&s->d_cnt, sizeof(unsigned long long) * 4) != cudaSuccess ||
         cudaMalloc((void**)&s->d_tim, sizeof(unsigned long long) * 16) != cudaSuccess) {
         delete s;
@@ -362,6 +388,10 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     A.timing = nullptr;
     A.dbuf = kLayouts[lay][0];
     A.const_smem = kLayouts[lay][1];
+    A.picard = p->picard;
+    A.consts1 = g->d_consts1;
+    A.bgs = s->d_bgs;
+    A.srcs = s->d_bgs + 3 * (size_t)M;
     *out = s;
     return QZ_OK;
 }
@@ -384,7 +414,7 @@ extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, 
         QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 16, st));
         A.timing = s->d_tim;
     }
-    QZ_CUDA(qzb::launch_sweep_m0(A, st));
+    QZ_CUDA(s->p.modes == 1 ? qzb::launch_sweep_m1(A, st) : qzb::launch_sweep_m0(A, st));
     if (cnt) {
         unsigned long long h[4];
         QZ_CUDA(cudaMemcpyAsync(h, s->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));

@@ -42,10 +42,18 @@ struct SweepArgs {
     unsigned long long* timing;     // optional: clock cycles per phase [6]
     int dbuf;                       // double-buffered slice sources (push fused with the next deposit)
     int const_smem;                 // per-node constants copied into shared memory
+    // modes = 1 only
+    int picard;                     // B+ iterations (src/Simulation.cpp:560)
+    const double* consts1;          // 9 x M: L1D Thomas 1/u, -a/u, -c/u; L0 rows a b c; L2D rows a b c
+    double* bgs;                    // (3, M) scratch: background rho - J_z in modes 0 / 1
+    double* srcs;                   // (2 x 30, M) scratch: the sources of this slice and of the next
 };
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem);
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
+// the modes = 1 sweep: one CTA, one radial row per thread (M <= kSweepThreads), plasma in A.ps
+size_t sweep_m1_smem_bytes(int M);
+cudaError_t launch_sweep_m1(const SweepArgs& A, cudaStream_t stream);
 
 // Beam particles (SoA, device) and the box they live in.
 struct BeamArgs {

@@ -46,6 +46,7 @@ struct NoGate {
     __device__ double* fld(const SweepArgs& A) const { return A.fld; }
     __device__ double* diag(const SweepArgs& A) const { return A.diag; }
     __device__ double* ps(const SweepArgs& A) const { return A.ps; }
+    __device__ double* srcs(const SweepArgs& A) const { return A.srcs; }
 };
 
 // ---------------------------------------------------------------- block scans

@@ -8,6 +8,9 @@ All are synthetic: seeded gaussian beams from the reference's generator, uniform
                     xi length 12 with dxi 0.005 (2400 slices), ppc 1; driver as above with 1e6 particles;
                     witness sigma_r 0.02 / sigma_xi 0.1 / 4.5 behind the driver / n_b 20 / gamma 1000 /
                     emit_n 1e-3, 1e6 particles; dt 5, 100 steps, m = 0
+  hosing            the pinched-witness grid and box with azimuthal modes m = 0, 1 (Picard 3, 8 azimuths
+                    per plasma ring: 4088 particles per slice); driver offset 0.1 in x and tilted 1e-3 in
+                    x-xi, witness offset 0.02; 2e6 + 2e6 particles; dt 5, 200 steps
 """
 from __future__ import annotations
 
@@ -103,6 +106,18 @@ witness.seed = 1001
 """
 
 
+def hosing_deck(xi_min: float = -11.995, driver_np: int = 2000000, witness_np: int = 2000000,
+                steps: int = 200) -> str:
+    return pinched_witness_deck(xi_min, driver_np, witness_np, steps) + """
+modes = 1
+solver.picard = 3
+electrons.ntheta = 8
+driver.x0 = 0.1
+driver.x_slope = 1e-3
+witness.x0 = 0.02
+"""
+
+
 def spec_from_text(text: str, overrides=()) -> deck.RunSpec:
     """RunSpec of a deck; grid.file = PINCHED_WITNESS_GRID selects the generated 512-node grid."""
     cfg = deck.parse_deck(text, overrides)
@@ -123,3 +138,7 @@ def plain_blowout() -> deck.RunSpec:
 
 def pinched_witness(**kw) -> deck.RunSpec:
     return spec_from_text(pinched_witness_deck(**kw))
+
+
+def hosing(**kw) -> deck.RunSpec:
+    return spec_from_text(hosing_deck(**kw))

@@ -2,7 +2,8 @@
 container that has it):  python tests/golden/make_validation_fixtures.py /root/reference
 
   validation_numbers.json  printed results of validation/reference_full.txt and reference_quick.txt
-                           for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain)
+                           for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain,
+                           7 centroid betatron oscillation with azimuthal mode 1)
   decks/*.in               the validation decks those numbers come from (blowout, gain, betatron, linear)
 """
 import json
@@ -24,6 +25,9 @@ for tag, fn in (("full", "reference_full.txt"), ("quick", "reference_quick.txt")
         m = re.match(r"max \|r_rms - r0 \|cos\(w_b t\)\|\| / r0 = (\S+)", line)
         if m:
             out["betatron_" + tag] = m.group(1)
+        m = re.match(r"max \|x_c - x0 cos\(w_b t\)\|/x0 = (\S+),\s+max \|y_c\|/x0 = (\S+)", line)
+        if m:
+            out["m1_centroid_" + tag] = {"x": m.group(1), "y": m.group(2)}
         m = re.match(r"d<gamma>/dt = (\S+)", line)
         if m:
             out["gain_" + tag] = m.group(1)

@@ -2,7 +2,7 @@
 
 Unit tests restated from the reference's tests/test_solvers.cpp, tests/test_pushers.cpp and
 tests/test_ab.cpp (same cases, same thresholds), and the printed numbers of its validation suite
-(validation/reference_full.txt / reference_quick.txt, sections 2-4, fixtures in tests/golden)
+(validation/reference_full.txt / reference_quick.txt, sections 2-4 and 7, fixtures in tests/golden)
 reproduced from the same decks with the same sampled beams.
 """
 import json
@@ -187,3 +187,20 @@ def test_validation_gain_quick():
     t = np.arange(spec.steps + 1) * spec.dt
     g = np.array([O.from_sums(mom[n, bi], gref, xiref)["gamma_mean"] for n in range(spec.steps + 1)])
     assert f"{np.polyfit(t, g, 1)[0]:.4f}" == VAL["gain_quick"]
+
+
+# ------------------------------------------------------------------ section 7: azimuthal mode 1
+def test_validation_m1_centroid_betatron():
+    # validation/run_validation.sh:101-109: betatron.in with modes = 1 and the witness offset by 0.05
+    spec = _deck("betatron.in", ["modes=1", "witness.x0=0.05", "witness.nsym=4"])
+    sim = O.OracleSim(spec)
+    mom = sim.run(spec.steps, spec.dt)
+    _, gref, xiref = sim.beam_data[0]
+    t = np.arange(spec.steps + 1) * spec.dt
+    d = [O.from_sums(mom[n, 0], gref, xiref, m1=True) for n in range(spec.steps + 1)]
+    xc = np.array([q["x_mean"] for q in d])
+    yc = np.array([q["y_mean"] for q in d])
+    w = 1 / np.sqrt(2 * 1000)
+    ref = VAL["m1_centroid_full"]
+    assert f"{abs(xc - xc[0] * np.cos(w * t)).max() / xc[0]:.2e}" == ref["x"]
+    assert f"{abs(yc).max() / xc[0]:.1e}" == ref["y"]
