@@ -163,7 +163,7 @@ qz_status qz_sim_destroy(qz_sim* s);
 qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q, double m, int rigid,
                           double gref, double xiref);
 /* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
-   By default (m = 0, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
+   By default (modes 0 or 1, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
    consecutive steps run concurrently on different SMs, each slice gated on the beam pushes of the
    previous step that can deposit into it, and the pushes are gated on the fields they gather: the
    same arithmetic as the step-by-step loop of Simulation::run (src/Simulation.cpp:1370-1448), with

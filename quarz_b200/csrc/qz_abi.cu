@@ -679,6 +679,8 @@ struct qz_sim {
         bool clean = false;                        // every beam-source slot is zero
         double* ps = nullptr;
         size_t ps_n = 0;
+        double* m1s = nullptr;                     // modes = 1 scratch of the sweep CTAs
+        size_t m1s_n = 0;
         int* sync = nullptr;
         size_t sync_n = 0;
         int* bk = nullptr;                         // beam, start, end, cmax (4 x nbk), then cnt_le (K)
@@ -695,7 +697,7 @@ struct qz_sim {
             for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
                 if (q) cudaFree(q);
         for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom, pipe.fld, pipe.diag, pipe.bsrc, pipe.ps,
-                          pipe.pmom, pipe.mom})
+                          pipe.m1s, pipe.pmom, pipe.mom})
             if (q) cudaFree(q);
         for (void* q : {(void*)pipe.sync, (void*)pipe.bk, (void*)pipe.sort.keys[0], (void*)pipe.sort.keys[1],
                         (void*)pipe.sort.vals[0], (void*)pipe.sort.vals[1], pipe.sort.tmp, (void*)pipe.sort.nlive,
@@ -876,6 +878,8 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     // 2. schedule: one CTA per SM; sweeps for every step up to the SMs left after the workers
     qzb::PipeArgs A{};
     A.sw = s->sw->base;
+    A.modes = s->p.modes;
+    A.bnc = s->bnc;
     A.sw.counters = s->sw->d_cnt;
     A.sw.timing = nullptr;
     int sms = 0;
@@ -906,6 +910,9 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     P_.clean = false;
     const size_t ps_slot = (size_t)(6 + 5 * s->p.ab_order) * std::max(1, s->sw->npad);
     if (qz_status e = grow(&P_.ps, &P_.ps_n, ps_slot * nsweep, "plasma scratch")) return e;
+    const size_t m1s_slot = s->p.modes == 1 ? (size_t)63 * M : 0;
+    if (m1s_slot)
+        if (qz_status e = grow(&P_.m1s, &P_.m1s_n, m1s_slot * nsweep, "mode-1 scratch")) return e;
     const size_t nsync = 4 * (size_t)(nsteps + 1) + nbk + 2;
     if (qz_status e = grow(&P_.sync, &P_.sync_n, nsync, "sync words")) return e;
     QZ_CUDA(cudaMemsetAsync(P_.sync, 0, sizeof(int) * nsync, st));
@@ -936,6 +943,8 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.diag = P_.diag;
     A.bsrc = P_.bsrc;
     A.ps = P_.ps;
+    A.m1s = P_.m1s;
+    A.m1s_slot = m1s_slot;
     A.nbeams = nb;
     for (int q = 0; q < nb; ++q) {
         const auto& b = s->beams[q];
@@ -1068,7 +1077,7 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
     if (!(dt > 0.0)) return fail(QZ_ERR_ARG, "qz_sim_run: dt must be positive");
     cudaStream_t st = (cudaStream_t)stream;
-    if (s->pipe.enabled && s->p.modes == 0) return run_pipelined(s, nsteps, dt, mom_host, st);
+    if (s->pipe.enabled) return run_pipelined(s, nsteps, dt, mom_host, st);
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 

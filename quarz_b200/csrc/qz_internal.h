@@ -102,8 +102,11 @@ struct PipeArgs {
     int nsteps;                     // sweeps 0..nsteps, pushes 0..nsteps-1
     int nsweep;                     // CTAs running sweeps
     int ring;                       // slots of the field / diagnostics / beam-source rings
+    int modes, bnc;                 // azimuthal modes (0 / 1), beam-source components per node
     size_t fld_slot, diag_slot, bsrc_slot, ps_slot;   // doubles per slot (ps: per sweep CTA)
     double *fld, *diag, *bsrc, *ps;
+    double* m1s;                    // modes = 1: per sweep CTA, background (3 M) + source buffers (60 M)
+    size_t m1s_slot;
     int nbeams;
     BeamArgs beam[kMaxBeams];
     int rigid[kMaxBeams], startup[kMaxBeams];
@@ -130,7 +133,7 @@ struct PipeArgs {
 };
 constexpr int kTraceStride = 22;
 
-size_t pipeline_smem_bytes(int M, bool dbuf, bool const_smem);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem);
 // resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count
 int pipeline_max_grid(const PipeArgs& P, int* sms);
 // cooperative launch of grid CTAs (fails unless all of them can be resident at once)

@@ -23,6 +23,7 @@
 // is read with ld.global.cg, so that no stale L1 line is used.
 #include "qz_beam_body.cuh"
 #include "qz_sweep_body.cuh"
+#include "qz_sweep_m1_body.cuh"
 
 #include <cub/device/device_radix_sort.cuh>
 
@@ -90,6 +91,8 @@ struct PipeGate {
     __device__ double* fld(const SweepArgs&) const { return g->fld; }
     __device__ double* diag(const SweepArgs&) const { return g->diag; }
     __device__ double* ps(const SweepArgs&) const { return g->ps; }
+    __device__ double* bgs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot; }
+    __device__ double* srcs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot + 3 * (size_t)P->sw.M; }
 
     // thread 0: beam-source rows <= r are final
     __device__ bool before_rows(int r) {
@@ -117,7 +120,7 @@ struct PipeGate {
     // every thread, after its stores of slice k: row k-1 of the beam sources is no longer needed
     __device__ void slice_done_all(int k) {
         if (k >= 1) {
-            const int nr = P->sw.M * B_NC0;
+            const int nr = P->sw.M * P->bnc;
             double* row = const_cast<double*>(g->bsrc) + (size_t)(k - 1) * nr;
             for (int i = threadIdx.x; i < nr; i += kT) __stcg(row + i, 0.0);
         }
@@ -137,7 +140,7 @@ struct PipeGate {
     }
 };
 
-template <int ORD, bool REG, int kMaxR>
+template <int MODES, int ORD, bool REG, int kMaxR>
 __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
     __shared__ int s_ok;
     __shared__ GateState gs;
@@ -158,10 +161,12 @@ __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
         if (!s_ok) return;
         if (P.trace && tid == 0) P.trace[(size_t)kTraceStride * n] = gtimer();
         PipeGate g{&P, &gs};
-        if (!sweep_body<ORD, REG, kMaxR>(P.sw, smem, g)) return;
+        const bool ok = MODES == 1 ? sweep_m1_body<ORD>(P.sw, smem, g) : sweep_body<ORD, REG, kMaxR>(P.sw, smem, g);
+        if (!ok) return;
         // the last row (the others were zeroed slice by slice)
-        double* row = P.bsrc + slot * P.bsrc_slot + (size_t)(K - 1) * M * B_NC0;
-        for (int i = tid; i < M * B_NC0; i += kT) __stcg(row + i, 0.0);
+        const int nr = M * P.bnc;
+        double* row = P.bsrc + slot * P.bsrc_slot + (size_t)(K - 1) * nr;
+        for (int i = tid; i < nr; i += kT) __stcg(row + i, 0.0);
         __syncthreads();
         if (tid == 0) {
             __threadfence();
@@ -326,11 +331,11 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     }
 }
 
-template <int ORD, bool REG, int kMaxR>
+template <int MODES, int ORD, bool REG, int kMaxR>
 __global__ void __launch_bounds__(kSweepThreads, 1) pipeline_kernel(const __grid_constant__ PipeArgs P) {
     extern __shared__ double smem_raw[];
     if ((int)blockIdx.x < P.nsweep)
-        sweep_role<ORD, REG, kMaxR>(P, smem_raw);
+        sweep_role<MODES, ORD, REG, kMaxR>(P, smem_raw);
     else
         worker_role(P, smem_raw);
 }
@@ -345,37 +350,41 @@ __global__ void moments_reduce_kernel(const __grid_constant__ PipeArgs P, double
     mom[((size_t)n * P.nbeams + q) * 17 + c] = v;
 }
 
-template <int ORD, bool REG, int RM>
+template <int MODES, int ORD, bool REG, int RM>
 cudaError_t launch_t(const PipeArgs& P, int grid, size_t smem, cudaStream_t stream) {
-    auto fn = pipeline_kernel<ORD, REG, RM>;
+    auto fn = pipeline_kernel<MODES, ORD, REG, RM>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&P};
     return cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(kSweepThreads), args, smem, stream);
 }
 
-template <int ORD, bool REG, int RM>
+template <int MODES, int ORD, bool REG, int RM>
 int occupancy_t(size_t smem) {
-    auto fn = pipeline_kernel<ORD, REG, RM>;
+    auto fn = pipeline_kernel<MODES, ORD, REG, RM>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, smem) != cudaSuccess) return 0;
     return nb;
 }
 
+// modes = 1 runs one row per thread with the plasma in the scratch (REG and kMaxR unused: false, 1)
 template <int ORD>
 cudaError_t launch_o(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
+    if (P.modes == 1) return launch_t<1, ORD, false, 1>(P, grid, smem, s);
     const bool reg = P.sw.np <= kSweepThreads;
     if (P.sw.rows_per_thread == 1)
-        return reg ? launch_t<ORD, true, 1>(P, grid, smem, s) : launch_t<ORD, false, 1>(P, grid, smem, s);
-    return reg ? launch_t<ORD, true, 4>(P, grid, smem, s) : launch_t<ORD, false, 4>(P, grid, smem, s);
+        return reg ? launch_t<0, ORD, true, 1>(P, grid, smem, s) : launch_t<0, ORD, false, 1>(P, grid, smem, s);
+    return reg ? launch_t<0, ORD, true, 4>(P, grid, smem, s) : launch_t<0, ORD, false, 4>(P, grid, smem, s);
 }
 
 template <int ORD>
 int occupancy_o(const PipeArgs& P, size_t smem) {
+    if (P.modes == 1) return occupancy_t<1, ORD, false, 1>(smem);
     const bool reg = P.sw.np <= kSweepThreads;
-    if (P.sw.rows_per_thread == 1) return reg ? occupancy_t<ORD, true, 1>(smem) : occupancy_t<ORD, false, 1>(smem);
-    return reg ? occupancy_t<ORD, true, 4>(smem) : occupancy_t<ORD, false, 4>(smem);
+    if (P.sw.rows_per_thread == 1)
+        return reg ? occupancy_t<0, ORD, true, 1>(smem) : occupancy_t<0, ORD, false, 1>(smem);
+    return reg ? occupancy_t<0, ORD, true, 4>(smem) : occupancy_t<0, ORD, false, 4>(smem);
 }
 
 // ---------------------------------------------------------------- ordering the beam by xi cell
@@ -491,8 +500,8 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngrou
     return cudaGetLastError();
 }
 
-size_t pipeline_smem_bytes(int M, bool dbuf, bool const_smem) {
-    const size_t sweep = sweep_m0_smem_bytes(M, dbuf, const_smem);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem) {
+    const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem);
     const size_t worker = sizeof(double) * 3 * (size_t)M + 64;
     return sweep > worker ? sweep : worker;
 }
@@ -502,7 +511,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    const size_t smem = pipeline_smem_bytes(P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem);
     int per = 0;
     switch (P.sw.ord) {
         case 1: per = occupancy_o<1>(P, smem); break;
@@ -518,7 +527,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
 cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream) {
     if (P.sw.rows_per_thread < 1 || P.sw.rows_per_thread > 4) return cudaErrorInvalidValue;
     if (P.nsweep < 1 || grid <= P.nsweep || P.ring < 2 || P.nbeams > kMaxBeams) return cudaErrorInvalidValue;
-    const size_t smem = pipeline_smem_bytes(P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem);
     switch (P.sw.ord) {
         case 1: return launch_o<1>(P, grid, smem, stream);
         case 2: return launch_o<2>(P, grid, smem, stream);

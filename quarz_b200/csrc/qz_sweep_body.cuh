@@ -47,6 +47,7 @@ struct NoGate {
     __device__ double* diag(const SweepArgs& A) const { return A.diag; }
     __device__ double* ps(const SweepArgs& A) const { return A.ps; }
     __device__ double* srcs(const SweepArgs& A) const { return A.srcs; }
+    __device__ double* bgs(const SweepArgs& A) const { return A.bgs; }
 };
 
 // ---------------------------------------------------------------- block scans

@@ -647,7 +647,7 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
     const Consts1 C = consts1(A);
     const int np = A.np, npad = A.npad, lane = tid & 31;
     const double R = A.R;
-    double* bg = A.bgs;                                          // (3, M) background, global scratch
+    double* bg = gate.bgs(A);                                    // (3, M) background, global scratch
     unsigned long long* tim = A.timing;                          // optional: clock cycles per phase
     long long t_prev = (tim && tid == 0) ? clock64() : 0;
 #define M1_MARK(ph)                                                           \

@@ -76,13 +76,17 @@ def test_sweep_m1_one_step_against_oracle():
     assert lost == a.lost()
 
 
-def test_run_m1_moments_against_oracle():
+@pytest.mark.parametrize("pipelined", [True, False])
+def test_run_m1_moments_against_oracle(pipelined):
+    # the whole run as one pipelined launch (sweeps of consecutive steps concurrent), and step by step
     spec = _spec(steps=3)
     beams = [Q.sample_beam(b) for b in spec.beams]
     ref = O.OracleSim(spec, beams=beams)
     mom_ref = ref.run(spec.steps, spec.dt)
     sim = Q.Simulation(spec, beams=beams)
+    sim.set_schedule(pipelined)
     mom = sim.run(spec.steps, spec.dt)
+    assert sim.schedule()["pipelined"] == (1 if pipelined else 0)
     L = spec.K * spec.dxi
     for q, (_, gref, xiref) in enumerate(beams):
         for n in range(spec.steps + 1):
@@ -97,3 +101,7 @@ def test_run_m1_moments_against_oracle():
     F = ref.fld()
     for c in (4, 5, 14, 15):                 # E_z, B_z modes 0 and 1 after the last sweep
         assert rel_l2(fld[..., c], F[..., c]) < 1e-8, c
+    for q in range(len(beams)):
+        got, want = sim.beam(q), ref.beam(q)
+        for c in range(6):
+            assert rel_l2(got[:, c], want[:, c]) < 1e-9, (q, c)
