@@ -212,6 +212,25 @@ qz_status qz_sim_counters(qz_sim* s, qz_counters* out);
 qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, double dt_drift, int push,
                            double* moments_host, void* stream);
 
+/* ------------------------------------------------------------------ batched independent runs
+ * A parameter scan: many independent small runs (each its own grid, box, plasma and up to 2 beams,
+ * m = 0, one AB order for all) in ONE persistent launch, a CTA per instance taken from a queue
+ * (largest first). No counterpart in the reference, which runs one deck per process; each instance
+ * is Simulation::run (src/Simulation.cpp:1370-1448) for constant dt. */
+typedef struct qz_batch qz_batch;
+qz_status qz_batch_create(qz_batch** out);
+qz_status qz_batch_destroy(qz_batch* b);
+/* adds an instance: its grid nodes, sweep parameters and beams (host rows of 7: x y px py pz xi w,
+   internal xi); *index = its position */
+qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const qz_sweep_params* p, int nbeams,
+                       const double* const* p7_host, const int64_t* n, const double* q, const double* m,
+                       const int* rigid, const double* gref, const double* xiref, int* index);
+/* runs every instance nsteps (nsteps+1 sweeps); moments_host: for each instance in order of addition,
+   (nsteps+1, nbeams, 17) moment sums, concatenated; the beams stay on the device (advanced) */
+qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* moments_host, void* stream);
+/* instances, CTAs of the last run, its kernel time (ms), 0 */
+qz_status qz_batch_info(qz_batch* b, double* out4);
+
 #ifdef __cplusplus
 }
 #endif

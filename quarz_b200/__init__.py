@@ -8,14 +8,15 @@ surface:
     Sweep        -> Simulation::step_fields slice loop (src/Simulation.cpp:636-795)
     BeamOps      -> Beam::deposit / Beam::push / Beam::sums (src/Beam.cpp)
     Simulation   -> Simulation::run for constant dt    (src/Simulation.cpp:1370-1448)
+    Batch        -> many independent Simulation::run in one launch (a parameter scan)
 
 There is no CPU fallback: if the library cannot be loaded every entry point raises.
 """
 from __future__ import annotations
 
 from ._lib import QZError, lib, library_path  # noqa: F401
-from .api import (BeamOps, RadialGrid, Simulation, Sweep, sample_beam, sample_gaussian,  # noqa: F401
+from .api import (Batch, BeamOps, RadialGrid, Simulation, Sweep, sample_beam, sample_gaussian,  # noqa: F401
                   sweep_params)
 
-__all__ = ["QZError", "lib", "library_path", "RadialGrid", "Sweep", "BeamOps", "Simulation", "sample_gaussian",
-           "sample_beam", "sweep_params"]
+__all__ = ["QZError", "lib", "library_path", "RadialGrid", "Sweep", "BeamOps", "Simulation", "Batch",
+           "sample_gaussian", "sample_beam", "sweep_params"]

@@ -305,3 +305,57 @@ class Simulation:
             except Exception:
                 pass
             self.h = None
+
+
+# ---------------------------------------------------------------- batched independent runs
+class Batch:
+    """Many independent runs (a parameter scan) in one persistent launch (qz_batch)."""
+
+    def __init__(self):
+        h = C.c_void_p()
+        check(lib().qz_batch_create(C.byref(h)))
+        self.h = h
+        self.specs = []
+
+    def add(self, spec: "_deck.RunSpec", beams: Optional[List[Tuple[np.ndarray, float, float]]] = None) -> int:
+        beams = beams if beams is not None else [sample_beam(b) for b in spec.beams]
+        nb = len(spec.beams)
+        rows = [np.ascontiguousarray(p, dtype=np.float64) for p, _, _ in beams]
+        nodes = np.ascontiguousarray(spec.nodes, dtype=np.float64)
+        params = sweep_params(spec)
+        ptrs = (C.c_void_p * max(nb, 1))(*[r.ctypes.data for r in rows])
+        n = (C.c_int64 * max(nb, 1))(*[len(r) for r in rows])
+        q = np.array([b.q for b in spec.beams] or [0.0])
+        m = np.array([b.m for b in spec.beams] or [1.0])
+        rigid = (C.c_int * max(nb, 1))(*[1 if b.rigid else 0 for b in spec.beams])
+        gref = np.array([g for _, g, _ in beams] or [0.0])
+        xiref = np.array([x for _, _, x in beams] or [0.0])
+        idx = C.c_int()
+        check(lib().qz_batch_add(self.h, _p(nodes), len(nodes), C.byref(params), nb, ptrs, n, _p(q), _p(m), rigid,
+                                 _p(gref), _p(xiref), C.byref(idx)))
+        self.specs.append((spec, beams))
+        return idx.value
+
+    def run(self, nsteps: int, dt: float, stream=None) -> List[np.ndarray]:
+        """Runs every instance; returns per instance its (nsteps+1, nbeams, 17) moment sums."""
+        sizes = [(nsteps + 1) * max(1, len(sp.beams)) * 17 for sp, _ in self.specs]
+        out = np.zeros(sum(sizes))
+        check(lib().qz_batch_run(self.h, int(nsteps), float(dt), _p(out), _stream_ptr(stream)))
+        res, off = [], 0
+        for (sp, _), sz in zip(self.specs, sizes):
+            res.append(out[off:off + sz].reshape(nsteps + 1, max(1, len(sp.beams)), 17)[:, :len(sp.beams)])
+            off += sz
+        return res
+
+    def info(self) -> dict:
+        v = np.zeros(4)
+        check(lib().qz_batch_info(self.h, _p(v)))
+        return {"instances": int(v[0]), "ctas": int(v[1]), "kernel_ms": float(v[2])}
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().qz_batch_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None

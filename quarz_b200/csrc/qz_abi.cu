@@ -1217,3 +1217,203 @@ extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_
     s->bsrc_valid = false;
     return QZ_OK;
 }
+
+// ===================================================================== batched independent runs
+// A parameter scan: many small runs, each with its own grid, box, plasma and beams, in one persistent
+// launch (qz_batch.cu). No counterpart in the reference, which runs one deck per process.
+struct qz_batch {
+    struct Inst {
+        qz_grid* g = nullptr;
+        qz_sweep* sw = nullptr;
+        std::vector<double*> beam_d;       // 7 columns of n per beam
+        std::vector<int64_t> beam_n;
+        qzb::BatchInst dev{};
+        double cost = 0;
+        ~Inst() {
+            for (double* d : beam_d)
+                if (d) cudaFree(d);
+            qz_sweep_destroy(sw);
+            qz_grid_destroy(g);
+        }
+    };
+    std::vector<Inst*> inst;
+    int ord = 0;
+    qzb::BatchInst* d_inst = nullptr;
+    int* d_order = nullptr;
+    int* d_next = nullptr;
+    double *d_fld = nullptr, *d_diag = nullptr, *d_bsrc = nullptr, *d_mom = nullptr;
+    size_t slots_alloc = 0, mom_alloc = 0;
+    float last_ms = 0;
+    int last_grid = 0;
+    ~qz_batch() {
+        for (Inst* i : inst) delete i;
+        for (void* q : {(void*)d_inst, (void*)d_order, (void*)d_next, (void*)d_fld, (void*)d_diag, (void*)d_bsrc,
+                        (void*)d_mom})
+            if (q) cudaFree(q);
+    }
+};
+
+extern "C" qz_status qz_batch_create(qz_batch** out) {
+    if (!out) return fail(QZ_ERR_ARG, "qz_batch_create: null pointer");
+    *out = new (std::nothrow) qz_batch;
+    return *out ? QZ_OK : fail(QZ_ERR_NOMEM, "qz_batch_create: out of host memory");
+}
+
+extern "C" qz_status qz_batch_destroy(qz_batch* b) {
+    delete b;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const qz_sweep_params* p, int nbeams,
+                                  const double* const* p7_host, const int64_t* n, const double* q, const double* m,
+                                  const int* rigid, const double* gref, const double* xiref, int* index) {
+    if (!b || !nodes || !p || nbeams < 0 || nbeams > qzb::kBatchBeams || (nbeams > 0 && (!p7_host || !n || !q ||
+        !m || !rigid || !gref || !xiref)))
+        return fail(QZ_ERR_ARG, "qz_batch_add: bad argument (at most 2 beams per instance)");
+    if (p->modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_add: batched runs are built for modes = 0");
+    if (b->ord && p->ab_order != b->ord) return fail(QZ_ERR_ARG, "qz_batch_add: every instance needs the same AB order");
+    auto* I = new (std::nothrow) qz_batch::Inst;
+    if (!I) return fail(QZ_ERR_NOMEM, "qz_batch_add: out of host memory");
+    if (qz_status st = qz_grid_create(nodes, M, &I->g)) { delete I; return st; }
+    if (qz_status st = qz_sweep_create(I->g, p, &I->sw)) { delete I; return st; }
+    qzb::BatchInst& D = I->dev;
+    D.sw = I->sw->base;
+    {
+        // the batch kernel holds the instance record and a reduction scratch in static shared memory:
+        // the sweep's layout must leave room for them
+        int dev = 0, optin = 0;
+        QZ_CUDA(cudaGetDevice(&dev));
+        QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        const size_t reserve = sizeof(qzb::BatchInst) + sizeof(double) * 17 * (qzb::kSweepThreads / 32) + 256;
+        static const bool kLay[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
+        int lay = -1;
+        for (int l = 0; l < 4 && lay < 0; ++l)
+            if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1]) + reserve <= (size_t)optin) lay = l;
+        if (lay < 0) { delete I; return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep"); }
+        D.sw.dbuf = kLay[lay][0];
+        D.sw.const_smem = kLay[lay][1];
+    }
+    D.nbeams = nbeams;
+    qz_box box;
+    box.xi_min = p->xi_min; box.dxi = p->dxi; box.K = p->K; box.ngp = p->ngp; box.modes = 0;
+    long ntot = 0;
+    for (int k = 0; k < nbeams; ++k) {
+        if (n[k] < 0 || (n[k] > 0 && !p7_host[k])) { delete I; return fail(QZ_ERR_ARG, "qz_batch_add: bad beam"); }
+        std::vector<double> cols((size_t)7 * (n[k] > 0 ? n[k] : 1), 0.0);
+        for (int64_t i = 0; i < n[k]; ++i)
+            for (int c = 0; c < 7; ++c) cols[(size_t)c * n[k] + i] = p7_host[k][7 * i + c];
+        double* d = nullptr;
+        if (qz_status st = dev_upload(&d, cols)) { delete I; return st; }
+        I->beam_d.push_back(d);
+        I->beam_n.push_back(n[k]);
+        qz_beam_view v;
+        v.x = d; v.y = d + n[k]; v.px = d + 2 * n[k]; v.py = d + 3 * n[k]; v.pz = d + 4 * n[k];
+        v.xi = d + 5 * n[k]; v.w = d + 6 * n[k]; v.n = n[k]; v.q = q[k]; v.m = m[k];
+        D.beam[k] = beam_args(I->g, &v, &box);
+        D.rigid[k] = rigid[k];
+        D.gref[k] = gref[k];
+        D.xiref[k] = xiref[k];
+        ntot += n[k];
+    }
+    // cost estimate (queue order): the sweeps plus the beam work
+    I->cost = (double)p->K * (M + 4.0 * I->sw->np) + 2.0 * ntot;
+    b->ord = p->ab_order;
+    b->inst.push_back(I);
+    if (index) *index = (int)b->inst.size() - 1;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mom_host, void* stream) {
+    if (!b || nsteps < 0 || !(dt > 0)) return fail(QZ_ERR_ARG, "qz_batch_run: bad argument");
+    const int ni = (int)b->inst.size();
+    if (ni == 0) return QZ_OK;
+    cudaStream_t st = (cudaStream_t)stream;
+    // slot sizes and shared memory: the largest instance
+    size_t fmax = 0, bmax = 0, smem = 0, mom_total = 0;
+    std::vector<size_t> mom_off(ni);
+    for (int i = 0; i < ni; ++i) {
+        const auto& A = b->inst[i]->dev.sw;
+        const size_t km = (size_t)A.K * A.M;
+        fmax = std::max(fmax, km);
+        bmax = std::max(bmax, km);
+        smem = std::max(smem, qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem));
+        mom_off[i] = mom_total;
+        mom_total += (size_t)(nsteps + 1) * std::max(1, b->inst[i]->dev.nbeams) * 17;
+    }
+    int sms = 0;
+    const int grid = std::min(qzb::batch_max_grid(b->ord, smem, &sms), ni);
+    if (grid < 1) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the batch kernel cannot be resident here");
+    const size_t need = (size_t)grid;
+    if (b->slots_alloc < need * fmax) {
+        for (double* q : {b->d_fld, b->d_diag, b->d_bsrc})
+            if (q) cudaFree(q);
+        b->d_fld = b->d_diag = b->d_bsrc = nullptr;
+        b->slots_alloc = 0;
+        if (cudaMalloc((void**)&b->d_fld, sizeof(double) * need * fmax * 6) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_diag, sizeof(double) * need * fmax * 3) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_bsrc, sizeof(double) * need * bmax * 5) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(QZ_ERR_NOMEM, "qz_batch_run: device allocation failed (slot buffers)");
+        }
+        b->slots_alloc = need * fmax;
+    }
+    if (b->mom_alloc < mom_total) {
+        if (b->d_mom) cudaFree(b->d_mom);
+        b->d_mom = nullptr;
+        QZ_CUDA(cudaMalloc((void**)&b->d_mom, sizeof(double) * mom_total));
+        b->mom_alloc = mom_total;
+    }
+    std::vector<qzb::BatchInst> hi(ni);
+    for (int i = 0; i < ni; ++i) {
+        hi[i] = b->inst[i]->dev;
+        hi[i].mom = b->d_mom + mom_off[i];
+    }
+    std::vector<int> order(ni);
+    for (int i = 0; i < ni; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return b->inst[x]->cost > b->inst[y]->cost; });
+    if (!b->d_inst) {
+        QZ_CUDA(cudaMalloc((void**)&b->d_next, sizeof(int)));
+    }
+    if (b->d_inst) cudaFree(b->d_inst);
+    if (b->d_order) cudaFree(b->d_order);
+    b->d_inst = nullptr;
+    b->d_order = nullptr;
+    QZ_CUDA(cudaMalloc((void**)&b->d_inst, sizeof(qzb::BatchInst) * ni));
+    QZ_CUDA(cudaMalloc((void**)&b->d_order, sizeof(int) * ni));
+    QZ_CUDA(cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(qzb::BatchInst) * ni, cudaMemcpyHostToDevice, st));
+    QZ_CUDA(cudaMemcpyAsync(b->d_order, order.data(), sizeof(int) * ni, cudaMemcpyHostToDevice, st));
+    QZ_CUDA(cudaMemsetAsync(b->d_next, 0, sizeof(int), st));
+    qzb::BatchArgs B{};
+    B.inst = b->d_inst;
+    B.order = b->d_order;
+    B.ninst = ni;
+    B.nsteps = nsteps;
+    B.dt = dt;
+    B.ord = b->ord;
+    B.fld = b->d_fld; B.diag = b->d_diag; B.bsrc = b->d_bsrc;
+    B.fld_slot = fmax * 6; B.diag_slot = fmax * 3; B.bsrc_slot = bmax * 5;
+    B.next = b->d_next;
+    cudaEvent_t e0, e1;
+    QZ_CUDA(cudaEventCreate(&e0));
+    QZ_CUDA(cudaEventCreate(&e1));
+    QZ_CUDA(cudaEventRecord(e0, st));
+    QZ_CUDA(qzb::launch_batch(B, grid, smem, st));
+    QZ_CUDA(cudaEventRecord(e1, st));
+    if (mom_host) QZ_CUDA(cudaMemcpyAsync(mom_host, b->d_mom, sizeof(double) * mom_total, cudaMemcpyDeviceToHost, st));
+    QZ_CUDA(cudaStreamSynchronize(st));
+    QZ_CUDA(cudaEventElapsedTime(&b->last_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->last_grid = grid;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_info(qz_batch* b, double* out4) {
+    if (!b || !out4) return fail(QZ_ERR_ARG, "qz_batch_info: null pointer");
+    out4[0] = (double)b->inst.size();
+    out4[1] = b->last_grid;
+    out4[2] = b->last_ms;
+    out4[3] = 0;
+    return QZ_OK;
+}

@@ -1,0 +1,190 @@
+// qz_batch.cu -- many independent runs (a parameter scan) in one persistent launch.
+//
+// Each CTA takes the next instance from a queue (largest first) and runs all of it as
+// Simulation::run does (src/Simulation.cpp:1370-1448): the step-0 beam deposit, then per step the
+// sweep (qz_sweep_body.cuh), the moment sums of every beam (Beam::sums, src/Beam.cpp:1133-1155) and,
+// before the last sweep, the push of every beam with the next deposit (src/Beam.cpp:725-785,
+// :900-1131). Instances differ in grid, box, plasma and beams; their sweep arguments are copied into
+// shared memory, the field and beam-source buffers are the CTA's slot, and the beams are pushed by
+// the CTA itself with the grid arrays the sweep left in shared memory.
+#include "qz_beam_body.cuh"
+#include "qz_sweep_body.cuh"
+
+namespace qzb {
+
+namespace {
+
+using beam_detail::deposit_one;
+using beam_detail::PState7;
+using beam_detail::push_one;
+using beam_detail::sums_add;
+
+constexpr int kT = kSweepThreads;
+
+// beam work of one instance by the whole CTA: moments (step n) of every beam, then, when push,
+// the push with the fields of step n and the deposit into bsrc (zeroed first)
+__device__ void beam_phase(const BatchInst& I, const SweepArgs& A, const BatchArgs& B, int n, bool push, bool startup,
+                           double* red) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (push) {
+        const size_t nb = (size_t)A.K * A.M * B_NC0;
+        for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
+        __syncthreads();
+    }
+    // the sweep leaves the grid in shared memory (qz_sweep_body.cuh carve: r, 1/V, 1/h first)
+    extern __shared__ double smem_raw[];
+    const double* r = smem_raw;
+    const double* iV = smem_raw + A.M;
+    const double* ih = smem_raw + 2 * A.M;
+    for (int q = 0; q < I.nbeams; ++q) {
+        BeamArgs Bb = I.beam[q];
+        Bb.r = r;
+        Bb.inv_V = iV;
+        Bb.inv_h = ih;
+        const double qm = Bb.q / Bb.m;
+        const double h = 0.5 * qm * B.dt;
+        const double hs = startup ? 0.5 * qm * (-0.5 * B.dt) : 0.0;
+        double acc[17];
+#pragma unroll
+        for (int c = 0; c < 17; ++c) acc[c] = 0.0;
+        for (long i = tid; i < Bb.n; i += kT) {
+            PState7 p;
+            p.w = Bb.w[i];
+            if (p.w == 0.0) continue;
+            p.x = Bb.x[i]; p.y = Bb.y[i]; p.px = Bb.px[i]; p.py = Bb.py[i]; p.pz = Bb.pz[i]; p.xi = Bb.xi[i];
+            sums_add(acc, p, I.gref[q], I.xiref[q]);
+            if (!push) continue;
+            if (I.rigid[q]) {
+                deposit_one(Bb, const_cast<double*>(A.bsrc), p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
+                continue;
+            }
+            const bool alive = push_one<false>(Bb, A.fld, p, h, hs, B.dt);
+            Bb.x[i] = p.x; Bb.y[i] = p.y; Bb.px[i] = p.px; Bb.py[i] = p.py; Bb.pz[i] = p.pz; Bb.xi[i] = p.xi;
+            if (!alive) {
+                Bb.w[i] = 0.0;
+                continue;
+            }
+            deposit_one(Bb, const_cast<double*>(A.bsrc), p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
+        }
+        // deterministic block reduction of the 17 sums
+#pragma unroll
+        for (int c = 0; c < 17; ++c) {
+            double x = acc[c];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+            if (lane == 0) red[c * (kT / 32) + warp] = x;
+        }
+        __syncthreads();
+        if (tid < 17) {
+            double v = 0.0;
+            for (int w = 0; w < kT / 32; ++w) v += red[tid * (kT / 32) + w];
+            I.mom[((size_t)n * I.nbeams + q) * 17 + tid] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// the step-0 deposit of every beam into the (zeroed) slot
+__device__ void beam_deposit0(const BatchInst& I, const SweepArgs& A) {
+    const int tid = threadIdx.x;
+    const size_t nb = (size_t)A.K * A.M * B_NC0;
+    for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
+    __syncthreads();
+    for (int q = 0; q < I.nbeams; ++q) {
+        const BeamArgs& Bb = I.beam[q];
+        for (long i = tid; i < Bb.n; i += kT) {
+            const double w = Bb.w[i];
+            if (w == 0.0) continue;
+            deposit_one(Bb, const_cast<double*>(A.bsrc), Bb.x[i], Bb.y[i], Bb.px[i], Bb.py[i], Bb.pz[i], Bb.xi[i], w);
+        }
+    }
+    __syncthreads();
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_constant__ BatchArgs B) {
+    extern __shared__ double smem_raw[];
+    __shared__ BatchInst I;
+    __shared__ int s_inst;
+    __shared__ double red[17 * (kT / 32)];
+    const int tid = threadIdx.x;
+    for (;;) {
+        if (tid == 0) s_inst = atomicAdd(B.next, 1);
+        __syncthreads();
+        const int qi = s_inst;
+        if (qi >= B.ninst) break;
+        if (tid == 0) {
+            I = B.inst[B.order[qi]];
+            I.sw.bsrc = B.bsrc + blockIdx.x * B.bsrc_slot;
+            I.sw.fld = B.fld + blockIdx.x * B.fld_slot;
+            I.sw.diag = B.diag + blockIdx.x * B.diag_slot;
+            I.sw.timing = nullptr;
+        }
+        __syncthreads();
+        const SweepArgs& A = I.sw;
+        const bool reg = A.np <= kSweepThreads;
+        beam_deposit0(I, A);
+        for (int n = 0; n <= B.nsteps; ++n) {
+            NoGate g;
+            if (A.rows_per_thread == 1) {
+                if (reg) sweep_body<ORD, true, 1>(A, smem_raw, g);
+                else sweep_body<ORD, false, 1>(A, smem_raw, g);
+            } else {
+                sweep_body<ORD, false, 4>(A, smem_raw, g);
+            }
+            __syncthreads();
+            beam_phase(I, A, B, n, n < B.nsteps, n == 0, red);
+        }
+        __syncthreads();
+    }
+}
+
+template <int ORD>
+cudaError_t launch_t(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
+    cudaError_t e = cudaFuncSetAttribute(batch_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    batch_kernel<ORD><<<grid, kSweepThreads, smem, s>>>(B);
+    return cudaGetLastError();
+}
+
+template <int ORD>
+int occupancy_t(size_t smem) {
+    if (cudaFuncSetAttribute(batch_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD>, kSweepThreads, smem) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
+}  // namespace
+
+int batch_max_grid(int ord, size_t smem, int* sms) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    *sms = nsm;
+    int per = 0;
+    switch (ord) {
+        case 1: per = occupancy_t<1>(smem); break;
+        case 2: per = occupancy_t<2>(smem); break;
+        case 3: per = occupancy_t<3>(smem); break;
+        case 4: per = occupancy_t<4>(smem); break;
+        case 5: per = occupancy_t<5>(smem); break;
+        default: return 0;
+    }
+    return per * nsm;
+}
+
+cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
+    switch (B.ord) {
+        case 1: return launch_t<1>(B, grid, smem, s);
+        case 2: return launch_t<2>(B, grid, smem, s);
+        case 3: return launch_t<3>(B, grid, smem, s);
+        case 4: return launch_t<4>(B, grid, smem, s);
+        case 5: return launch_t<5>(B, grid, smem, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+}  // namespace qzb

@@ -161,4 +161,34 @@ cudaError_t unpermute7(const double* src, double* dst, const int* orig, long n, 
 // start[ngroups] = nlive
 cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngroups, int* start, cudaStream_t s);
 
+// ---------------------------------------------------------------- batched independent runs
+// Many independent instances (each its own grid, box, plasma and beams) in one persistent launch: a
+// CTA takes the next instance from a queue and runs all of it (Simulation::run: sweeps, moment sums,
+// pushes) with its own slot of field / beam-source buffers. Instances are queued largest first.
+constexpr int kBatchBeams = 2;
+
+struct BatchInst {
+    SweepArgs sw;                   // bsrc / fld / diag are the slot's, set by the kernel
+    int nbeams;
+    BeamArgs beam[kBatchBeams];     // grid pointers are set by the kernel (shared-memory copies)
+    int rigid[kBatchBeams];
+    double gref[kBatchBeams], xiref[kBatchBeams];
+    double* mom;                    // (nsteps + 1, nbeams, 17)
+};
+
+struct BatchArgs {
+    const BatchInst* inst;          // device array
+    const int* order;               // queue order (largest first)
+    int ninst;
+    int nsteps;
+    double dt;
+    int ord;
+    double *fld, *diag, *bsrc;      // per slot (= CTA)
+    size_t fld_slot, diag_slot, bsrc_slot;
+    int* next;                      // queue head (0)
+};
+
+cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t stream);
+int batch_max_grid(int ord, size_t smem, int* sms);
+
 }  // namespace qzb

@@ -1,0 +1,48 @@
+"""Batched parameter scan: every instance of one persistent launch (a CTA per instance) against the
+same instance run on its own (step by step) and, for two of them, against the oracle.
+
+Instances are drawn like the scan workload (quarz_b200.workloads.scan_instances: 128-1024 cells,
+stretched grids, xi lengths 8-16) with 4000 beam particles and 3 steps. Tolerances: derived beam
+moments 1e-10 relative to their natural scale against the single runs (only the summation order of
+the beam deposits differs), 1e-8 against the oracle."""
+import numpy as np
+import pytest
+
+import oracle as O
+import quarz_b200 as Q
+from quarz_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("gamma_mean", "gamma_rms", "xi_mean", "xi_rms", "r_rms", "emit_nx", "charge_w", "alive")
+
+
+def _close(spec, mom, ref, beams, tol):
+    L, R = spec.K * spec.dxi, spec.nodes[-1]
+    for q, (_, gref, xiref) in enumerate(beams):
+        for n in range(mom.shape[0]):
+            d, dr = O.from_sums(mom[n, q], gref, xiref), O.from_sums(ref[n, q], gref, xiref)
+            sc = {"gamma_rms": abs(dr.get("gamma_mean", 0.0)), "xi_mean": L, "xi_rms": L, "r_rms": R}
+            for k in KEYS:
+                if k not in dr:
+                    continue
+                assert abs(d[k] - dr[k]) <= tol * max(abs(dr[k]), sc.get(k, 0.0), 1e-300), (q, n, k, d[k], dr[k])
+
+
+def test_batch_equals_single_runs_and_oracle():
+    specs = workloads.scan_instances(6, seed=7, beam_particles=4000, steps=3)
+    assert min(s.M for s in specs) <= 513 < max(s.M for s in specs)      # both sweep variants
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    batch = Q.Batch()
+    for s, bm in zip(specs, beams):
+        batch.add(s, bm)
+    moms = batch.run(3, specs[0].dt)
+    info = batch.info()
+    assert info["instances"] == 6 and info["ctas"] == 6
+    for s, bm, mom in zip(specs, beams, moms):
+        sim = Q.Simulation(s, beams=bm)
+        sim.set_schedule(False)
+        _close(s, mom, sim.run(3, s.dt), bm, 1e-10)
+    for s, bm, mom in list(zip(specs, beams, moms))[:2]:
+        ref = O.OracleSim(s, beams=bm)
+        _close(s, mom, ref.run(3, s.dt), bm, 1e-8)
