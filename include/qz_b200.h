@@ -172,8 +172,8 @@ qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q,
 qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, void* stream);
 /* Schedule of qz_sim_run: pipelined = 0 runs the steps one kernel after another (one sweep launch,
    then one push launch per beam, per step); sweep_ctas = CTAs running sweeps (0: one per step, up to
-   the SMs left for at least max(8, SMs/5) push CTAs); a push task (bucket) holds at most `bucket`
-   particles (0: 1024) of at most `span` neighbouring xi cells (0: 2) -- the next step's sweep trails
+   the SMs left for at least max(8, 2 SMs/5) push CTAs); a push task (bucket) holds at most `bucket`
+   particles (0: 512) of at most `span` neighbouring xi cells (0: 2) -- the next step's sweep trails
    the previous one by about span + 5 slices; timeout_s = limit of every wait inside the pipelined
    launch (0: keep, default 20 s), after which the launch ends and qz_sim_run returns QZ_ERR_CUDA.
    No counterpart in the reference (its own pipelining over time steps is across MPI ranks,
@@ -190,9 +190,9 @@ qz_status qz_sim_times(qz_sim* s, double* ms3);
 qz_status qz_sim_set_beam(qz_sim* s, int b, const double* cols7, int on_device, void* stream);
 /* Timeline of the last pipelined run, 22 values per step n: GPU clock (ns, %globaltimer) at the start
    and the end of sweep n, when it had stored 1/16, 2/16, ... 16/16 of the slices, then its longest
-   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 3 totals of
-   the push workers: tasks, scans that found no ready task, claims lost to another worker.
-   Up to cap values; *n = 22 (nsteps+1) + 3. enable = 1 records it in later runs. */
+   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 4 totals of
+   the push workers (warps): tasks, scans that found no ready task, claims lost to another worker, ns
+   spent in tasks. Up to cap values; *n = 22 (nsteps+1) + 4. enable = 1 records it in later runs. */
 qz_status qz_sim_trace(qz_sim* s, int enable, unsigned long long* out, int cap, int* n);
 /* qz_sim_run with the beams in HOST memory: copies every beam in (cols_host[b]: 7 x n SoA in the
    caller's order, x y px py pz xi w), runs nsteps, and copies the particles back into cols_host in

@@ -665,7 +665,7 @@ struct qz_sim {
     qz_counters cnt{};
     // time-step pipeline (qz_pipeline.cu): options, last schedule, buffers kept between runs
     struct Pipe {
-        int enabled = 1, sweep_ctas = 0, bucket = 1024, span = 2;
+        int enabled = 1, sweep_ctas = 0, bucket = 512, span = 2;
         double timeout_s = 20.0;
         int info[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // grid, sweep CTAs, worker CTAs, ring, buckets, bucket size, pipelined
         int trace = 0;                             // record sweep start / end times
@@ -803,7 +803,9 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     if (!P_.ev[0])
         for (auto& e : P_.ev) QZ_CUDA(cudaEventCreate(&e));
     QZ_CUDA(cudaEventRecord(P_.ev[0], st));
-    // 1. order each beam by xi cell; buckets of P_.bucket live particles
+    // 1. order each beam by (xi cell, radial cell); buckets of at most P_.bucket live particles
+    if ((unsigned long long)(K + 2) * (unsigned long long)M >= (1ull << 31))
+        return fail(QZ_ERR_SIZE, "qz_sim_run: K * M too large for the pipelined run's sort keys");
     long nmax = 1;
     for (auto& b : s->beams) nmax = std::max<long>(nmax, (long)b.n);
     if (P_.sort_n < nmax) {
@@ -824,7 +826,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         }
         P_.sort_n = nmax;
     }
-    const int bk = P_.bucket > 0 ? P_.bucket : 1024;
+    const int bk = P_.bucket > 0 ? P_.bucket : 512;
     struct Bucket { int cmin, beam, start, end, cmax; };
     std::vector<Bucket> list;
     for (int q = 0; q < nb; ++q) {
@@ -846,7 +848,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         const int span = P_.span > 0 ? P_.span : 2;
         const int ngroups = (K + 1 + span - 1) / span;
         if (qz_status e = grow(&P_.cmin, &P_.cm_n, (size_t)ngroups + 1, "bucket groups")) return e;
-        QZ_CUDA(qzb::group_starts(P_.sort, nlive, span, ngroups, P_.cmin, st));
+        QZ_CUDA(qzb::group_starts(P_.sort, nlive, span * M, ngroups, P_.cmin, st));
         std::vector<int> gs(ngroups + 1);
         QZ_CUDA(cudaMemcpyAsync(gs.data(), P_.cmin, sizeof(int) * gs.size(), cudaMemcpyDeviceToHost, st));
         QZ_CUDA(cudaStreamSynchronize(st));
@@ -886,7 +888,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     const int grid = qzb::pipeline_max_grid(A, &sms);
     if (grid < 2) return fail(QZ_ERR_UNSUPPORTED, "qz_sim_run: the pipelined kernel cannot be resident here");
     const int g1 = std::min(grid, sms);
-    const int wmin = std::max(8, g1 / 5);
+    const int wmin = std::max(8, (2 * g1) / 5);             // measured best: ~2/5 of the SMs push
     int nsweep = P_.sweep_ctas > 0 ? P_.sweep_ctas : std::min(nsteps + 1, g1 - wmin);
     nsweep = std::max(1, std::min({nsweep, nsteps + 1, g1 - 1}));
     const int ring = std::max(2, std::min(nsteps + 1, nsweep + 2));
@@ -974,7 +976,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.timeout_ns = (unsigned long long)(P_.timeout_s * 1e9);
     A.trace = nullptr;
     if (P_.trace) {
-        const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + 3;
+        const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + 4;
         if (qz_status e = grow(&P_.d_trace, &P_.trace_n, ntr, "trace")) return e;
         QZ_CUDA(cudaMemsetAsync(P_.d_trace, 0, sizeof(unsigned long long) * ntr, st));
         A.trace = P_.d_trace;
@@ -996,7 +998,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     QZ_CUDA(cudaMemcpyAsync(s->d_diag, P_.diag + (size_t)last * A.diag_slot, sizeof(double) * A.diag_slot,
                             cudaMemcpyDeviceToDevice, st));
     if (P_.trace) {
-        P_.h_trace.assign((size_t)qzb::kTraceStride * (nsteps + 1) + 3, 0ull);
+        P_.h_trace.assign((size_t)qzb::kTraceStride * (nsteps + 1) + 4, 0ull);
         QZ_CUDA(cudaMemcpyAsync(P_.h_trace.data(), P_.d_trace, sizeof(unsigned long long) * P_.h_trace.size(),
                                 cudaMemcpyDeviceToHost, st));
     }
@@ -1089,7 +1091,7 @@ extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_cta
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_set_schedule: the pipelined run handles at most 4 beams");
     s->pipe.enabled = pipelined ? 1 : 0;
     s->pipe.sweep_ctas = sweep_ctas;
-    s->pipe.bucket = bucket > 0 ? bucket : 1024;
+    s->pipe.bucket = bucket > 0 ? bucket : 512;
     s->pipe.span = span > 0 ? span : 2;
     if (timeout_s > 0) s->pipe.timeout_s = timeout_s;
     return QZ_OK;

@@ -68,10 +68,71 @@ __device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restric
     }
 }
 
+// The same m = 0 deposit as deposit_one, returned instead of applied: the 20 contributions of one
+// particle, v[(2 a + b) * 5 + c] for row k + a, node j + b, component c (B_RT0 .. B_RHO0), rows out of
+// the box carrying zero. Returns false when the particle deposits nothing (outside the wall or box).
+// jguess: a nearby radial cell (the gather's, before the push moved the particle), or < 0
+__device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, double Y, double PX, double PY, double PZ,
+                                              double XI, double wi, int jguess, int& k, int& j, double (&v)[20]) {
+    const double R = B.R;
+    const double r = sqrt(X * X + Y * Y);
+    if (r > R) return false;
+    const double c = r > 0.0 ? X / r : 1.0, s = r > 0.0 ? Y / r : 0.0;
+    const double sx = (XI - B.xi_min) * B.idxi;
+    k = B.ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
+    const int nloc = B.K;
+    if (k < -1 || k >= nloc) return false;
+    const double tk = B.ngp ? 0.0 : sx - k;
+    const double p2 = PX * PX + PY * PY;
+    const double gam = sqrt(1.0 + p2 + PZ * PZ);
+    const double omvz = (1.0 + p2) / (gam * (gam + PZ));
+    const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
+    const double vr = c * vx + s * vy, vt = c * vy - s * vx;
+    // the cell of r (src/RadialGrid.hpp:84-88): a short walk from the guess, the search otherwise
+    j = locate_near(B.r, B.N, R, r, jguess);
+    double t = (r - B.r[j]) * B.inv_h[j];
+    t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    const double Wr[2] = {1.0 - t, t};
+    const double Wk[2] = {1.0 - tk, tk};
+    const double q = B.q;
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int kk = k + a;
+        const bool row = (a == 0 || !B.ngp) && kk >= 0 && kk < nloc;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const double d = row ? wi * q * Wk[a] * Wr[b] * B.inv_V[j + b] * B.idxi : 0.0;
+            double* o = v + (2 * a + b) * 5;
+            o[B_RT0] = d * omvz;
+            o[B_JZ0] = d * vz;
+            o[B_JP1R] = d * vr;
+            o[B_JP1I] = d * vt;
+            o[B_RHO0] = d;
+        }
+    }
+    return true;
+}
+
+// adds the 20 contributions of deposit_vals0 into bsrc (FP64 reductions into L2)
+__device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restrict__ bsrc, int k, int j,
+                                             const double (&v)[20]) {
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int kk = k + a;
+        if (kk < 0 || kk >= B.K || (a == 1 && B.ngp)) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            double* o = bsrc + ((size_t)kk * B.M + j + b) * B_NC0;
+#pragma unroll
+            for (int c = 0; c < 5; ++c) atomicAdd(o + c, v[(2 * a + b) * 5 + c]);
+        }
+    }
+}
+
 // bilinear (xi, r) gather and mode sums at the particle (src/Beam.cpp:972-1008)
 template <bool kL2>
 __device__ __forceinline__ void gather(const BeamArgs& B, const double* __restrict__ fld, double X, double Y,
-                                       double XI, double& c, double& sn, V3& E, V3& Bf) {
+                                       double XI, double& c, double& sn, V3& E, V3& Bf, int* jcell = nullptr) {
     const double r = sqrt(X * X + Y * Y);
     c = r > 0.0 ? X / r : 1.0;
     sn = r > 0.0 ? Y / r : 0.0;
@@ -93,6 +154,7 @@ __device__ __forceinline__ void gather(const BeamArgs& B, const double* __restri
     int j;
     double t;
     weights(B.r, B.inv_h, B.N, B.R, r, j, t);
+    if (jcell) *jcell = j;
     const int nc = B.modes ? F_NC1 : F_NC0;
     const double* f00 = fld + ((size_t)k * B.M + j) * nc;
     const double* f01 = f00 + nc;
@@ -144,10 +206,10 @@ struct PState7 {
 
 template <bool kL2>
 __device__ __forceinline__ bool push_one(const BeamArgs& B, const double* __restrict__ fld, PState7& p, double h,
-                                         double h_start, double dt) {
+                                         double h_start, double dt, int* jcell = nullptr) {
     double c, sn;
     V3 E, Bf;
-    gather<kL2>(B, fld, p.x, p.y, p.xi, c, sn, E, Bf);
+    gather<kL2>(B, fld, p.x, p.y, p.xi, c, sn, E, Bf, jcell);
     V3 u = {p.px, p.py, p.pz};
     if (h_start != 0.0) {
         const double g0 = sqrt(1.0 + dot3(u, u));

@@ -41,6 +41,20 @@ __device__ __forceinline__ int locate(const double* __restrict__ r, int N, doubl
     return lo;
 }
 
+// the cell locate() returns, found by walking up to 4 cells from a guess (particles move little per
+// step), the binary search when the walk fails or there is no guess (guess < 0)
+__device__ __forceinline__ int locate_near(const double* __restrict__ r, int N, double R, double x, int guess) {
+    if (guess < 0 || !(x > 0.0) || !(x < R)) return locate(r, N, R, x);
+    int j = guess > N - 1 ? N - 1 : guess;
+#pragma unroll 1
+    for (int step = 0; step < 4; ++step) {
+        if (r[j] > x) { if (j == 0) break; --j; continue; }
+        if (r[j + 1] <= x) { if (j == N - 1) break; ++j; continue; }
+        return j;
+    }
+    return locate(r, N, R, x);
+}
+
 // cell and clamped fractional position (src/RadialGrid.hpp:84-88)
 __device__ __forceinline__ void weights(const double* __restrict__ r, const double* __restrict__ inv_h, int N,
                                         double R, double x, int& j, double& t) {

@@ -141,7 +141,7 @@ cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream);
 // mom (nsteps + 1, nbeams, 17) from the bucket partials, in bucket order
 cudaError_t launch_moments_reduce(const PipeArgs& P, double* mom, cudaStream_t s);
 
-// Ordering a beam by xi cell (stable radix sort of the cell keys; removed particles last) for the
+// Ordering a beam by (xi cell, radial cell) (stable radix sort; removed particles last) for the
 // pipeline's buckets. Buffers of n entries: keys[2], vals[2]; tmp of cell_sort_temp_bytes(n).
 struct CellSortBuf {
     unsigned* keys[2];
@@ -157,9 +157,9 @@ cudaError_t cell_sort(const BeamArgs& B, double* cols, double* stage, int* orig,
 cudaError_t fill_iota(int* p, long n, cudaStream_t s);
 // dst (7 x n) = src in the caller's order: dst[c][orig[p]] = src[c][p]
 cudaError_t unpermute7(const double* src, double* dst, const int* orig, long n, cudaStream_t s);
-// start[g] = first live particle of the last sort in cells [g span - 1, g span + span - 2] (g < ngroups),
-// start[ngroups] = nlive
-cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngroups, int* start, cudaStream_t s);
+// start[g] = first live particle of the last sort in xi cells [g span - 1, g span + span - 2] (g < ngroups;
+// width = span * M), start[ngroups] = nlive
+cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngroups, int* start, cudaStream_t s);
 
 // ---------------------------------------------------------------- batched independent runs
 // Many independent instances (each its own grid, box, plasma and beams) in one persistent launch: a

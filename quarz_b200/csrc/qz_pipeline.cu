@@ -94,27 +94,41 @@ struct PipeGate {
     __device__ double* bgs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot; }
     __device__ double* srcs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot + 3 * (size_t)P->sw.M; }
 
-    // thread 0: beam-source rows <= r are final
+    // warp 0 (all 32 lanes): beam-source rows <= r are final. The lanes look at 32 buckets at once and
+    // advance over the finished prefix; the first unfinished one is waited for (bounded).
     __device__ bool before_rows(int r) {
+        const int lane = threadIdx.x & 31;
         const int need = P->cnt_le[r];
         int c = g->cursor;
         const int n = g->n;
         while (c < need) {
-            const unsigned long long t0 = P->trace ? gtimer() : 0ull;
-            if (!wait_ge(*P, P->bdone + c, n - 1, W_ROWS)) return false;
-            if (P->trace) {                           // the longest wait of this sweep: for which bucket
-                unsigned long long* tr = P->trace + (size_t)kTraceStride * n;
-                const unsigned long long dtw = gtimer() - t0;
-                if (dtw > tr[18]) {
-                    tr[18] = dtw;
-                    tr[19] = (unsigned long long)c;
-                    tr[20] = (unsigned long long)r;
-                    tr[21] = (unsigned long long)(long long)__ldcg(P->bk_cmax + c);
+            const int b = c + lane;
+            const bool done = b >= need || ld_acquire(P->bdone + b) >= n - 1;
+            const unsigned m = __ballot_sync(0xffffffffu, done);
+            const int run = (m == 0xffffffffu) ? 32 : __ffs(~m) - 1;   // finished buckets from c on
+            c = min(c + run, need);                   // lanes past `need` count as finished: never beyond it
+            if (run == 32 || c >= need) continue;
+            // bucket c is not finished yet: lane 0 waits for it
+            bool ok = true;
+            if (lane == 0) {
+                const unsigned long long t0 = P->trace ? gtimer() : 0ull;
+                ok = wait_ge(*P, P->bdone + c, n - 1, W_ROWS);
+                if (ok && P->trace) {                 // the longest wait of this sweep: for which bucket
+                    unsigned long long* tr = P->trace + (size_t)kTraceStride * n;
+                    const unsigned long long dtw = gtimer() - t0;
+                    if (dtw > tr[18]) {
+                        tr[18] = dtw;
+                        tr[19] = (unsigned long long)c;
+                        tr[20] = (unsigned long long)r;
+                        tr[21] = (unsigned long long)(long long)__ldcg(P->bk_cmax + c);
+                    }
                 }
             }
-            ++c;
+            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) return false;
         }
-        g->cursor = c;
+        __syncwarp();
+        if (lane == 0) g->cursor = c;
+        __syncwarp();
         return true;
     }
     // every thread, after its stores of slice k: row k-1 of the beam sources is no longer needed
@@ -256,8 +270,9 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     __syncthreads();
     const int last = P.pmom ? P.nsteps : P.nsteps - 1;     // the last step with tasks
     int n, b;
-    unsigned long long st[3] = {0, 0, 0};                  // tasks, scans that found nothing, lost claims
+    unsigned long long st[4] = {0, 0, 0, 0};               // tasks, scans that found nothing, lost claims, busy ns
     while (claim_task(P, last, n, b, st)) {
+        const unsigned long long t_task = P.trace ? gtimer() : 0ull;
         const bool push = n < P.nsteps;
         const int bb = __ldg(P.bk_beam + b);
         const long i0 = __ldg(P.bk_start + b), i1 = __ldg(P.bk_end + b);
@@ -276,6 +291,49 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
 #pragma unroll
         for (int c = 0; c < 17; ++c) acc[c] = 0.0;
         int cmax = -2;
+        if (P.modes == 0) {
+            // m = 0: particles are in (xi cell, r cell) order, so neighbouring lanes mostly deposit into
+            // the same 2 x 2 cells: sum runs of equal cells across the warp, one reduction per run
+            for (long base = i0; base < i1; base += 32) {
+                const long i = base + lane;
+                bool dep = false;
+                int dk = 0, dj = 0;
+                double v[20];
+                if (i < i1) {
+                    PState7 p;
+                    p.w = __ldcg(Bb.w + i);
+                    if (p.w != 0.0) {
+                        p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
+                        p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
+                        p.xi = __ldcg(Bb.xi + i);
+                        if (P.pmom) sums_add(acc, p, gref, xiref);
+                        if (push) {
+                            bool alive = true;
+                            int jg = 0;
+                            if (!rigid) {
+                                alive = push_one<true>(Bb, fld, p, h, hs, P.dt_drift, &jg);
+                                __stcg(Bb.x + i, p.x); __stcg(Bb.y + i, p.y);
+                                __stcg(Bb.px + i, p.px); __stcg(Bb.py + i, p.py); __stcg(Bb.pz + i, p.pz);
+                                __stcg(Bb.xi + i, p.xi);
+                                if (!alive) __stcg(Bb.w + i, 0.0);
+                            } else {
+                                jg = -1;
+                            }
+                            if (alive) {
+                                dep = beam_detail::deposit_vals0(Bb, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w, jg, dk,
+                                                                 dj, v);
+                                cmax = max(cmax, xi_cell(Bb, p.xi));
+                            }
+                        }
+                    }
+                }
+                if (!dep)
+#pragma unroll
+                    for (int c = 0; c < 20; ++c) v[c] = 0.0;
+                const int key = dep ? (dk + 1) * M + dj : -1 - lane;
+                if (warp_runs_sum<20>(key, v) && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
+            }
+        } else
         for (long i = i0 + lane; i < i1; i += 32) {
             PState7 p;
             p.w = __ldcg(Bb.w + i);
@@ -324,10 +382,11 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             atomicAdd(P.pdone + n, 1);
         }
         __syncwarp();
+        if (P.trace) st[3] += gtimer() - t_task;
     }
     if (P.trace && lane == 0) {
         unsigned long long* ws = P.trace + (size_t)kTraceStride * (P.nsteps + 1);
-        for (int c = 0; c < 3; ++c) atomicAdd(ws + c, st[c]);
+        for (int c = 0; c < 4; ++c) atomicAdd(ws + c, st[c]);
     }
 }
 
@@ -387,15 +446,20 @@ int occupancy_o(const PipeArgs& P, size_t smem) {
     return reg ? occupancy_t<0, ORD, true, 4>(smem) : occupancy_t<0, ORD, false, 4>(smem);
 }
 
-// ---------------------------------------------------------------- ordering the beam by xi cell
-// sort key of a particle: its xi cell + 1 (0 .. K), removed particles last (K + 1)
+// ---------------------------------------------------------------- ordering the beam by (xi cell, r cell)
+// sort key of a particle: (xi cell + 1) * M + radial cell, removed particles last ((K + 2) * M): the
+// xi cell orders the push tasks along the sweep, the radial cell puts particles that deposit into the
+// same nodes next to each other (the deposit sums runs of equal cells across a warp)
 __global__ void cell_keys_kernel(const BeamArgs B, unsigned* __restrict__ keys, int* __restrict__ vals,
                                  int* __restrict__ nlive) {
     int cnt = 0;
     const long stride = (long)gridDim.x * blockDim.x;
     for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += stride) {
         const bool live = B.w[i] != 0.0;
-        keys[i] = live ? (unsigned)(xi_cell(B, B.xi[i]) + 1) : (unsigned)(B.K + 1);
+        const double X = B.x[i], Y = B.y[i];
+        const int jr = locate(B.r, B.N, B.R, sqrt(X * X + Y * Y));
+        keys[i] = live ? (unsigned)(xi_cell(B, B.xi[i]) + 1) * (unsigned)B.M + (unsigned)jr
+                       : (unsigned)(B.K + 2) * (unsigned)B.M;
         vals[i] = (int)i;
         cnt += live ? 1 : 0;
     }
@@ -415,9 +479,9 @@ __global__ void gather7_kernel(const double* __restrict__ src, double* __restric
     }
 }
 
-// first sorted live particle of each group of span cells: start[g] = first i with key >= g * span
-// (keys sorted: cell + 1), start[ngroups] = nlive
-__global__ void group_starts_kernel(const unsigned* __restrict__ keys, long nlive, int span, int ngroups,
+// first sorted live particle of each group of xi cells: start[g] = first i with key >= g * width
+// (width = span * M: keys sorted by (xi cell + 1) * M + radial cell), start[ngroups] = nlive
+__global__ void group_starts_kernel(const unsigned* __restrict__ keys, long nlive, int width, int ngroups,
                                     int* __restrict__ start) {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g > ngroups) return;
@@ -425,7 +489,7 @@ __global__ void group_starts_kernel(const unsigned* __restrict__ keys, long nliv
         start[g] = (int)nlive;
         return;
     }
-    const unsigned key = (unsigned)g * (unsigned)span;
+    const unsigned key = (unsigned)g * (unsigned)width;
     long lo = 0, hi = nlive;                          // lower bound of key in keys[0, nlive)
     while (lo < hi) {
         const long mid = (lo + hi) >> 1;
@@ -474,7 +538,7 @@ cudaError_t cell_sort(const BeamArgs& B, double* cols, double* stage, int* orig,
     cell_keys_kernel<<<grid_of(n, 256), 256, 0, s>>>(B, buf.keys[0], buf.vals[0], buf.nlive);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     int bits = 1;
-    while ((1u << bits) <= (unsigned)(B.K + 1)) ++bits;
+    while (bits < 32 && (1ull << bits) <= (unsigned long long)(B.K + 2) * (unsigned long long)B.M) ++bits;
     size_t bytes = buf.tmp_bytes;
     e = cub::DeviceRadixSort::SortPairs(buf.tmp, bytes, buf.keys[0], buf.keys[1], buf.vals[0], buf.vals[1], n, 0, bits,
                                         s);
@@ -495,8 +559,8 @@ cudaError_t unpermute7(const double* src, double* dst, const int* orig, long n, 
     return cudaGetLastError();
 }
 
-cudaError_t group_starts(const CellSortBuf& buf, long nlive, int span, int ngroups, int* start, cudaStream_t s) {
-    group_starts_kernel<<<(ngroups + 1 + 127) / 128, 128, 0, s>>>(buf.keys[1], nlive, span, ngroups, start);
+cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngroups, int* start, cudaStream_t s) {
+    group_starts_kernel<<<(ngroups + 1 + 127) / 128, 128, 0, s>>>(buf.keys[1], nlive, width, ngroups, start);
     return cudaGetLastError();
 }
 

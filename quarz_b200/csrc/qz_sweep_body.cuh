@@ -38,7 +38,7 @@ constexpr unsigned FULL = 0xffffffffu;
 // Gate of a stand-alone sweep: no other CTA to wait for or to inform.
 struct NoGate {
     static constexpr bool kActive = false;
-    __device__ bool before_rows(int) { return true; }       // thread 0: beam-source rows <= row are final
+    __device__ bool before_rows(int) { return true; }       // warp 0: beam-source rows <= row are final
     __device__ void slice_done_all(int) {}                   // every thread, after its stores of slice k
     __device__ bool slice_done(int) { return true; }         // thread 0, after the barrier: publish slice k
     // this sweep's buffers
@@ -819,7 +819,10 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             add_multi<2>(adr, val);
         }
     }
-    if (Gate::kActive && tid == 0) *S.flag = gate.before_rows(K - 1 < 2 ? K - 1 : 2) ? 1 : 0;
+    if (Gate::kActive && tid < 32) {                     // warp 0 checks the beam-source rows
+        const bool ok = gate.before_rows(K - 1 < 2 ? K - 1 : 2);
+        if (tid == 0) *S.flag = ok ? 1 : 0;
+    }
     __syncthreads();
     if (Gate::kActive && !*S.flag) return false;
     for (int j = tid; j < M; j += kThreads) {
@@ -1160,7 +1163,13 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         __syncthreads();
         PHASE_MARK(4);
         if (Gate::kActive) {
-            if (tid == 0) *S.flag = (gate.slice_done(k) && (k + 1 >= K || gate.before_rows(k + 3 < K ? k + 3 : K - 1))) ? 1 : 0;
+            if (tid < 32) {                                   // warp 0: publish slice k, check the next rows
+                bool ok = true;
+                if (tid == 0) ok = gate.slice_done(k);
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                if (ok && k + 1 < K) ok = gate.before_rows(k + 3 < K ? k + 3 : K - 1);
+                if (tid == 0) *S.flag = ok ? 1 : 0;
+            }
             __syncthreads();
             if (!*S.flag) return false;
         }

@@ -715,7 +715,10 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
         bg[M + i] = lg(T.rhot.ar + i) - lg(T.drho.ar + i);
         bg[2 * M + i] = lg(T.rhot.ai + i) - lg(T.drho.ai + i);
     }
-    if (Gate::kActive && tid == 0) *S.flag = gate.before_rows(K - 1 < 2 ? K - 1 : 2) ? 1 : 0;
+    if (Gate::kActive && tid < 32) {                     // warp 0 checks the beam-source rows
+        const bool ok = gate.before_rows(K - 1 < 2 ? K - 1 : 2);
+        if (tid == 0) *S.flag = ok ? 1 : 0;
+    }
     __syncthreads();
     if (Gate::kActive && !*S.flag) return false;
     if (row) init_sources1(src1_of(scr, M, 0), bg, M, i, beam_row1<Gate::kActive>(A, gate.bsrc(A), 0, i));
@@ -1009,7 +1012,13 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
         if (Gate::kActive) gate.slice_done_all(k);
         __syncthreads();
         if (Gate::kActive) {
-            if (tid == 0) *S.flag = (gate.slice_done(k) && (k + 1 >= K || gate.before_rows(k + 3 < K ? k + 3 : K - 1))) ? 1 : 0;
+            if (tid < 32) {                                   // warp 0: publish slice k, check the next rows
+                bool ok = true;
+                if (tid == 0) ok = gate.slice_done(k);
+                ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
+                if (ok && k + 1 < K) ok = gate.before_rows(k + 3 < K ? k + 3 : K - 1);
+                if (tid == 0) *S.flag = ok ? 1 : 0;
+            }
             __syncthreads();
             if (!*S.flag) return false;
         }
