@@ -683,7 +683,7 @@ struct qz_sim {
         size_t m1s_n = 0;
         int* sync = nullptr;
         size_t sync_n = 0;
-        int* bk = nullptr;                         // beam, start, end, cmax (4 x nbk), then cnt_le (K)
+        int* bk = nullptr;                         // beam, start, end, cmax, cmin (5 x nbk), then cnt_le (K)
         size_t bk_n = 0;
         double *pmom = nullptr, *mom = nullptr;
         size_t pmom_n = 0, mom_n = 0;
@@ -863,16 +863,17 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     }
     std::stable_sort(list.begin(), list.end(), [](const Bucket& a, const Bucket& b) { return a.cmin < b.cmin; });
     const int nbk = (int)list.size();
-    std::vector<int> bkh((size_t)4 * nbk + K);
+    std::vector<int> bkh((size_t)5 * nbk + K);
     for (int i = 0; i < nbk; ++i) {
         bkh[i] = list[i].beam;
         bkh[nbk + i] = list[i].start;
         bkh[2 * nbk + i] = list[i].end;
         bkh[3 * nbk + i] = list[i].cmax;
+        bkh[4 * nbk + i] = list[i].cmin;
     }
     for (int r = 0, c = 0; r < K; ++r) {
         while (c < nbk && list[c].cmin <= r) ++c;
-        bkh[4 * nbk + r] = c;
+        bkh[5 * nbk + r] = c;
     }
     if (qz_status e = grow(&P_.bk, &P_.bk_n, bkh.size(), "buckets")) return e;
     QZ_CUDA(cudaMemcpyAsync(P_.bk, bkh.data(), sizeof(int) * bkh.size(), cudaMemcpyHostToDevice, st));
@@ -964,7 +965,8 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.bk_start = P_.bk + nbk;
     A.bk_end = P_.bk + 2 * nbk;
     A.bk_cmax = P_.bk + 3 * nbk;
-    A.cnt_le = P_.bk + 4 * nbk;
+    A.bk_cmin = P_.bk + 4 * nbk;
+    A.cnt_le = P_.bk + 5 * nbk;
     A.pmom = moms ? P_.pmom : nullptr;
     A.prog = P_.sync;
     A.sdone = P_.sync + (nsteps + 1);

@@ -115,6 +115,7 @@ struct PipeArgs {
     int nbk;                        // buckets, ordered by their initial lowest xi cell
     const int *bk_beam, *bk_start, *bk_end;
     int* bk_cmax;                   // highest xi cell of the bucket's live particles (before the next push)
+    const int* bk_cmin;             // lowest xi cell of the bucket when it was formed (a lower bound after)
     const int* cnt_le;              // [K]: number of buckets whose initial lowest cell is <= row
     double* pmom;                   // (nsteps + 1, nbk, 17) partial moment sums, or null
     // synchronisation words (device; set before the launch)

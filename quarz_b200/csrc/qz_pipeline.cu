@@ -47,6 +47,7 @@ __device__ __forceinline__ int ld_acquire(const int* p) {
 __device__ __forceinline__ void st_release(int* p, int v) {
     asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
+__device__ __forceinline__ void prefetch_l2(const void* p) { asm volatile("prefetch.global.L2 [%0];" ::"l"(p)); }
 __device__ __forceinline__ unsigned long long gtimer() {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
@@ -257,7 +258,7 @@ __device__ __forceinline__ bool claim_task(const PipeArgs& P, int last, int& n, 
 // Worker CTAs: every warp is an independent worker that claims (step, bucket) tasks.
 __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     const int tid = threadIdx.x, lane = tid & 31;
-    const int M = P.sw.M, N = P.sw.N;
+    const int M = P.sw.M, N = P.sw.N, K = P.sw.K;
     // grid arrays in shared memory: the binary search of every lookup stays on chip
     double* r = smem;
     double* ih = r + M;
@@ -282,16 +283,60 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
         Bb.inv_V = iV;
         const double* fld = P.fld + (size_t)(n % P.ring) * P.fld_slot;
         double* bnext = P.bsrc + (size_t)((n + 1) % P.ring) * P.bsrc_slot;
+        // bring the task's inputs towards L2 while it starts: the particle columns, the field rows it
+        // gathers and the beam-source rows it deposits into (a warp issues one prefetch per 128 B line)
+        if (push) {
+            const int c0 = max(__ldg(P.bk_cmin + b), 0);
+            const int c1 = min(__ldcg(P.bk_cmax + b) + 2, K - 1);
+            if (c1 >= c0) {
+                const double* f0 = fld + (size_t)c0 * M * (P.modes ? F_NC1 : F_NC0);
+                const long fl = (long)(c1 - c0 + 1) * M * (P.modes ? F_NC1 : F_NC0);
+                for (long o = (long)lane * 16; o < fl; o += 32 * 16) prefetch_l2(f0 + o);
+                const double* b0 = bnext + (size_t)c0 * M * P.bnc;
+                const long bl = (long)(c1 - c0 + 1) * M * P.bnc;
+                for (long o = (long)lane * 16; o < bl; o += 32 * 16) prefetch_l2(b0 + o);
+            }
+            const long pn = i1 - i0;
+            for (long o = (long)lane * 16; o < pn; o += 32 * 16) {
+                prefetch_l2(Bb.x + i0 + o); prefetch_l2(Bb.y + i0 + o); prefetch_l2(Bb.px + i0 + o);
+                prefetch_l2(Bb.py + i0 + o); prefetch_l2(Bb.pz + i0 + o); prefetch_l2(Bb.xi + i0 + o);
+                prefetch_l2(Bb.w + i0 + o);
+            }
+        }
         const double qm = Bb.q / Bb.m;
         const double h = 0.5 * qm * P.dt_kick;
         const double hs = (n == 0 && P.startup[bb]) ? 0.5 * qm * (-0.5 * P.dt_kick) : 0.0;
         const bool rigid = P.rigid[bb] != 0;
         const double gref = P.gref[bb], xiref = P.xiref[bb];
-        double acc[17];
+        // moments of step n (before the push), a pass of their own so that the 17 sums are not live
+        // during the push; it also brings the bucket's particles into L1 for the push
+        if (P.pmom) {
+            double acc[17];
 #pragma unroll
-        for (int c = 0; c < 17; ++c) acc[c] = 0.0;
+            for (int c = 0; c < 17; ++c) acc[c] = 0.0;
+            for (long i = i0 + lane; i < i1; i += 32) {
+                PState7 p;
+                p.w = __ldcg(Bb.w + i);
+                if (p.w == 0.0) continue;
+                p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
+                p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
+                p.xi = __ldcg(Bb.xi + i);
+                sums_add(acc, p, gref, xiref);
+            }
+            double mine = 0.0;
+#pragma unroll
+            for (int c = 0; c < 17; ++c) {
+                double x = acc[c];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == c) mine = x;
+            }
+            if (lane < 17) P.pmom[((size_t)n * P.nbk + b) * 17 + lane] = mine;
+        }
         int cmax = -2;
-        if (P.modes == 0) {
+        if (!push) {
+            // moments only (the state after the last push)
+        } else if (P.modes == 0) {
             // m = 0: particles are in (xi cell, r cell) order, so neighbouring lanes mostly deposit into
             // the same 2 x 2 cells: sum runs of equal cells across the warp, one reduction per run
             for (long base = i0; base < i1; base += 32) {
@@ -306,7 +351,6 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                         p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
                         p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
                         p.xi = __ldcg(Bb.xi + i);
-                        if (P.pmom) sums_add(acc, p, gref, xiref);
                         if (push) {
                             bool alive = true;
                             int jg = 0;
@@ -341,7 +385,6 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
             p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
             p.xi = __ldcg(Bb.xi + i);
-            if (P.pmom) sums_add(acc, p, gref, xiref);
             if (!push) continue;
             if (rigid) {
                 deposit_one(Bb, bnext, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
@@ -359,20 +402,9 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             deposit_one(Bb, bnext, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
             cmax = max(cmax, xi_cell(Bb, p.xi));
         }
-        // bucket results: moments of step n (before the push) in lane order, highest live cell after it
+        // bucket result: the highest live cell after the push
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, o));
-        if (P.pmom) {
-            double mine = 0.0;
-#pragma unroll
-            for (int c = 0; c < 17; ++c) {
-                double x = acc[c];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
-                if (lane == c) mine = x;
-            }
-            if (lane < 17) P.pmom[((size_t)n * P.nbk + b) * 17 + lane] = mine;
-        }
         __syncwarp();
         if (lane == 0) {
             // never below the previous bound: cells only grow, and a bucket may have no live particle
