@@ -173,7 +173,7 @@ qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, voi
 /* Schedule of qz_sim_run: pipelined = 0 runs the steps one kernel after another (one sweep launch,
    then one push launch per beam, per step); sweep_ctas = CTAs running sweeps (0: one per step, up to
    the SMs left for at least max(8, 2 SMs/5) push CTAs); a push task (bucket) holds at most `bucket`
-   particles (0: 512) of at most `span` neighbouring xi cells (0: 2) -- the next step's sweep trails
+   particles (0: 512) of at most `span` neighbouring xi cells (0: 1) -- the next step's sweep trails
    the previous one by about span + 5 slices; timeout_s = limit of every wait inside the pipelined
    launch (0: keep, default 20 s), after which the launch ends and qz_sim_run returns QZ_ERR_CUDA.
    No counterpart in the reference (its own pipelining over time steps is across MPI ranks,

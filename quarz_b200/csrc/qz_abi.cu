@@ -665,7 +665,7 @@ struct qz_sim {
     qz_counters cnt{};
     // time-step pipeline (qz_pipeline.cu): options, last schedule, buffers kept between runs
     struct Pipe {
-        int enabled = 1, sweep_ctas = 0, bucket = 512, span = 2;
+        int enabled = 1, sweep_ctas = 0, bucket = 512, span = 1;
         double timeout_s = 20.0;
         int info[8] = {0, 0, 0, 0, 0, 0, 0, 0};   // grid, sweep CTAs, worker CTAs, ring, buckets, bucket size, pipelined
         int trace = 0;                             // record sweep start / end times
@@ -845,7 +845,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         QZ_CUDA(cudaMemcpyAsync(&nlive, P_.sort.nlive, sizeof(int), cudaMemcpyDeviceToHost, st));
         QZ_CUDA(cudaStreamSynchronize(st));
         // buckets: never across a group of span cells, at most bk particles (near-equal parts)
-        const int span = P_.span > 0 ? P_.span : 2;
+        const int span = P_.span > 0 ? P_.span : 1;
         const int ngroups = (K + 1 + span - 1) / span;
         if (qz_status e = grow(&P_.cmin, &P_.cm_n, (size_t)ngroups + 1, "bucket groups")) return e;
         QZ_CUDA(qzb::group_starts(P_.sort, nlive, span * M, ngroups, P_.cmin, st));
@@ -1009,7 +1009,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     for (int i = 0; i < 3; ++i) QZ_CUDA(cudaEventElapsedTime(&P_.times[i], P_.ev[i], P_.ev[i + 1]));
     s->cnt.lost += h[0];
     s->bsrc_valid = false;
-    const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 2};
+    const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 1};
     std::copy(info, info + 8, P_.info);
     if (err) {
         static const char* site[] = {"?", "field ring slot", "beam-source rows", "no push task ready"};
@@ -1094,7 +1094,7 @@ extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_cta
     s->pipe.enabled = pipelined ? 1 : 0;
     s->pipe.sweep_ctas = sweep_ctas;
     s->pipe.bucket = bucket > 0 ? bucket : 512;
-    s->pipe.span = span > 0 ? span : 2;
+    s->pipe.span = span > 0 ? span : 1;
     if (timeout_s > 0) s->pipe.timeout_s = timeout_s;
     return QZ_OK;
 }
