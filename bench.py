@@ -12,7 +12,13 @@ Metric: slice-solves/s = K * (time steps + 1) / time (whole job: summed over GPU
 independent replica -- the sweep is sequential in xi, so there is no data-path collective). Also
 reported: beam pushes/s.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+Other workloads (not the headline; their lines are recorded beside it):
+  --workload hosing   the same run with azimuthal modes 0 and 1 (8 azimuths per ring, Picard 3),
+                      offset / tilted driver, 2e6 + 2e6 particles, 200 steps
+  --workload scan     512 independent runs of 20 steps (a parameter scan) in one launch: runs/s, with
+                      the plain loop over single runs (step by step, and pipelined) timed on a sample
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 """
 from __future__ import annotations
 
@@ -58,8 +64,8 @@ def _traffic_ratio():
         return None
 
 
-def _config(spec, nb_total, steps, extra=None):
-    c = {"workload": WORKLOAD, "modes": spec.modes, "radial_nodes": spec.M, "xi_slices": spec.K,
+def _config(spec, nb_total, steps, extra=None, workload=WORKLOAD):
+    c = {"workload": workload, "modes": spec.modes, "radial_nodes": spec.M, "xi_slices": spec.K,
          "dxi": spec.dxi, "plasma_ppc": spec.species[0].ppc, "plasma_particles_per_slice": spec.M - 1,
          "beam_particles": nb_total, "ab_order": spec.ab_order, "dt": spec.dt, "time_steps_per_run": steps,
          "l2": "inputs larger than L2: beams 112 MB + a field store of 59 MB and beam sources of 49 MB per step "
@@ -133,7 +139,7 @@ class ClockSampler:
 def _workload(args):
     from quarz_b200 import workloads
 
-    spec = workloads.pinched_witness()
+    spec = workloads.hosing() if args.workload == "hosing" else workloads.pinched_witness()
     if args.time_steps:
         spec.steps = args.time_steps
     return spec
@@ -216,6 +222,67 @@ def run_e2e(args, spec, beams, sim, dev):
             "d2h_bytes_per_step": nbytes + 17 * 8 * len(beams) * (spec.steps + 1)}
 
 
+def run_scan(args, rank, world, local_rank):
+    """The batched scan: 512 runs of 20 steps in one launch (qz_batch), runs/s; beside it the plain loop
+    over single runs on 6 sampled instances (step by step and pipelined)."""
+    import numpy as np
+    import torch
+
+    import quarz_b200 as Q
+    from quarz_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    specs = workloads.scan_instances(512, seed=2024 + rank)
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    batch = Q.Batch()
+    for s_, b_ in zip(specs, beams):
+        batch.add(s_, b_)
+    T, dt = specs[0].steps, specs[0].dt
+    for _ in range(args.warmup):
+        batch.run(T, dt)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        torch.distributed.barrier()
+    kms = []
+    with ClockSampler(local_rank) as clk:
+        for _ in range(args.steps):
+            batch.run(T, dt)          # (the beams restart from where the previous batch left them)
+            kms.append(batch.info()["kernel_ms"])
+    ms = sum(kms)
+    if world > 1:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms = float(t.item())
+    loop = {}
+    idx = np.linspace(0, len(specs) - 1, 6).astype(int)
+    for name, pipelined in (("step_by_step", False), ("pipelined", True)):
+        tt = 0.0
+        for i in idx:
+            sim = Q.Simulation(specs[i], beams=beams[i])
+            sim.set_schedule(pipelined)
+            sim.run(T, dt)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            sim2 = Q.Simulation(specs[i], beams=beams[i])
+            sim2.set_schedule(pipelined)
+            torch.cuda.synchronize(dev)
+            e0.record()
+            sim2.run(T, dt)
+            e1.record()
+            torch.cuda.synchronize(dev)
+            tt += e0.elapsed_time(e1)
+        loop[name] = 1e3 * len(idx) / tt
+    value = world * len(specs) * args.steps / (ms * 1e-3)
+    return {"metric": "runs/s", "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "scan", "instances": len(specs), "time_steps_per_run": T,
+                       "beam_particles_per_run": 100000, "radial_nodes": "129..1025", "xi_slices": "801..1601",
+                       "parallelism": "a CTA per instance, one launch per batch"},
+            "loop_runs_per_s": loop, "speedup_vs_step_by_step_loop": value / world / loop["step_by_step"],
+            "clocks": clk.result(), "gpu_launches": args.steps}
+
+
 def oracle_rate(time_steps, warmup, spec):
     """The CPU oracle (serial restatement of the reference path) on the same workload: slice-solves/s
     over time_steps full time steps (sweep + moment sums + push), after warm-up steps."""
@@ -240,6 +307,38 @@ def oracle_rate(time_steps, warmup, spec):
     return spec.K * time_steps / el, el
 
 
+def oracle_scan_rate(time_steps, warmup):
+    """The CPU oracle on the scan: one full time step (sweep + moment sums + push) of each of
+    `time_steps` instances sampled across the 512, after warm-up steps of the first; a run of T steps
+    costs T + 1 sweeps, so runs/s = 1 / ((T + 1) x the mean time of a step)."""
+    import numpy as np
+
+    from quarz_b200 import workloads
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    O.build()
+    specs = workloads.scan_instances(512, seed=2024)
+    idx = np.linspace(0, len(specs) - 1, max(1, time_steps)).astype(int)
+    sim = O.OracleSim(specs[idx[0]])
+    for _ in range(warmup):
+        sim.step_fields(0.0)
+        sim.push_beams(specs[idx[0]].dt, specs[idx[0]].dt)
+    el = 0.0
+    for i in idx[:time_steps]:
+        spec = specs[i]
+        sim = O.OracleSim(spec)
+        t = time.perf_counter()
+        sim.step_fields(0.0)
+        for b in range(len(spec.beams)):
+            sim.beam_sums(b)
+        sim.push_beams(spec.dt, spec.dt)
+        el += time.perf_counter() - t
+    T = specs[0].steps
+    return 1.0 / ((T + 1) * el / max(1, time_steps)), el
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -249,7 +348,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3, help="timed runs through the host-buffer call")
     ap.add_argument("--cpu-steps", type=int, default=10, help="oracle time steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's 100)")
+    ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
+    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan"], default="pinched_witness")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -258,6 +358,19 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
+        if args.workload == "scan":
+            rate, el = oracle_scan_rate(args.steps, args.warmup)
+            line = {"impl": "reference", "metric": "runs/s", "value": rate, "unit": "runs/s", "n_gpus": args.gpus,
+                    "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
+                    "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                    "data": "synthetic", "config": {"workload": "scan", "instances": 512, "time_steps_per_run": 20,
+                                                    "beam_particles_per_run": 100000},
+                    "cpu_baseline": {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
+                                     "sample": f"one full time step of each of {args.steps} instances sampled "
+                                               f"across the scan, serial oracle; a run = 21 such steps"},
+                    "e2e": {"value": rate, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            print(json.dumps(line))
+            return
         spec = _workload(args)
         # each bench step is one full time step of the oracle (a bounded sample of the run)
         rate, el = oracle_rate(args.steps, args.warmup, spec)
@@ -265,7 +378,7 @@ def main():
         line = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                "data": "synthetic", "config": _config(spec, nb, spec.steps),
+                "data": "synthetic", "config": _config(spec, nb, spec.steps, None, args.workload),
                 "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
                                  "sample": f"{args.steps} full time steps of the workload (sweep + moment sums + "
                                            f"beam push) after {args.warmup} warm-up steps, serial oracle"},
@@ -279,6 +392,20 @@ def main():
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "scan":
+        line = run_scan(args, rank, world, local_rank)
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            rate, el = oracle_scan_rate(args.cpu_steps, 1)
+            line["cpu_baseline"] = {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
+                                    "sample": f"one full time step of each of {args.cpu_steps} instances sampled "
+                                              f"across the scan, serial oracle, {el:.1f} s; a run = 21 such steps"}
+        if rank == 0:
+            print(json.dumps(line))
+        return
     r = run_b200(args, rank, world, local_rank)
     spec = r["spec"]
     K, T = spec.K, spec.steps
@@ -294,7 +421,7 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": _config(spec, nbt, T, {"schedule": r["schedule"]}),
+        "data": "synthetic", "config": _config(spec, nbt, T, {"schedule": r["schedule"]}, args.workload),
         "beam_pushes_per_s": world * nbt * T * args.steps / (r["ms"] * 1e-3),
         "kernel_ms_per_run": kms, "per_sweep_ms": kms / (T + 1),
         "roofline": {"bound": "hbm", "kernel": "pipeline_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
