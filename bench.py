@@ -17,6 +17,7 @@ Other workloads (not the headline; their lines are recorded beside it):
                       offset / tilted driver, 2e6 + 2e6 particles, 200 steps
   --workload scan     512 independent runs of 20 steps (a parameter scan) in one launch: runs/s, with
                       the plain loop over single runs (step by step, and pipelined) timed on a sample
+  --workload scan_m1  the same scan with azimuthal modes 0 and 1 (M <= 512)
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 """
@@ -233,8 +234,15 @@ def run_scan(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    specs = workloads.scan_instances(512, seed=2024 + rank)
-    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    from quarz_b200 import scan
+
+    modes = 1 if args.workload == "scan_m1" else 0
+    # 512 instances per GPU, the whole scan split over the ranks by estimated cost
+    all_specs = workloads.scan_instances(512 * world, seed=2024, modes=modes)
+    all_beams = [[Q.sample_beam(b) for b in s.beams] for s in all_specs]
+    costs = [scan.instance_cost(s, sum(len(p) for p, _, _ in bm)) for s, bm in zip(all_specs, all_beams)]
+    mine = scan.partition(costs, world)[rank]
+    specs, beams = [all_specs[i] for i in mine], [all_beams[i] for i in mine]
     batch = Q.Batch()
     for s_, b_ in zip(specs, beams):
         batch.add(s_, b_)
@@ -244,16 +252,19 @@ def run_scan(args, rank, world, local_rank):
     torch.cuda.synchronize(dev)
     if world > 1:
         torch.distributed.barrier()
-    kms = []
+    kms, last = [], None
     with ClockSampler(local_rank) as clk:
         for _ in range(args.steps):
-            batch.run(T, dt)          # (the beams restart from where the previous batch left them)
+            last = batch.run(T, dt)   # (the beams restart from where the previous batch left them)
             kms.append(batch.info()["kernel_ms"])
     ms = sum(kms)
     if world > 1:
         t = torch.tensor([ms], dtype=torch.float64, device=dev)
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
+    # the final gather of per-instance results (last-step moment sums), outside the timed region
+    gathered = scan.run_sharded(all_specs, all_beams, lambda s, b: last, device=dev)
+    done = int(np.count_nonzero(np.abs(gathered).sum(axis=(1, 2))))
     loop = {}
     idx = np.linspace(0, len(specs) - 1, 6).astype(int)
     for name, pipelined in (("step_by_step", False), ("pipelined", True)):
@@ -272,13 +283,15 @@ def run_scan(args, rank, world, local_rank):
             torch.cuda.synchronize(dev)
             tt += e0.elapsed_time(e1)
         loop[name] = 1e3 * len(idx) / tt
-    value = world * len(specs) * args.steps / (ms * 1e-3)
+    value = len(all_specs) * args.steps / (ms * 1e-3)
     return {"metric": "runs/s", "value": value, "unit": "runs/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": "scan", "instances": len(specs), "time_steps_per_run": T,
-                       "beam_particles_per_run": 100000, "radial_nodes": "129..1025", "xi_slices": "801..1601",
-                       "parallelism": "a CTA per instance, one launch per batch"},
+            "config": {"workload": args.workload, "modes": modes, "instances": len(all_specs),
+                       "instances_with_results": done, "time_steps_per_run": T,
+                       "beam_particles_per_run": 100000, "radial_nodes": "129..1025" if modes == 0 else "129..512",
+                       "xi_slices": "801..1601",
+                       "parallelism": "a CTA per instance, one launch per batch; instances split over GPUs by cost"},
             "loop_runs_per_s": loop, "speedup_vs_step_by_step_loop": value / world / loop["step_by_step"],
             "clocks": clk.result(), "gpu_launches": args.steps}
 
@@ -307,7 +320,7 @@ def oracle_rate(time_steps, warmup, spec):
     return spec.K * time_steps / el, el
 
 
-def oracle_scan_rate(time_steps, warmup):
+def oracle_scan_rate(time_steps, warmup, modes=0):
     """The CPU oracle on the scan: one full time step (sweep + moment sums + push) of each of
     `time_steps` instances sampled across the 512, after warm-up steps of the first; a run of T steps
     costs T + 1 sweeps, so runs/s = 1 / ((T + 1) x the mean time of a step)."""
@@ -319,7 +332,7 @@ def oracle_scan_rate(time_steps, warmup):
     import oracle as O
 
     O.build()
-    specs = workloads.scan_instances(512, seed=2024)
+    specs = workloads.scan_instances(512, seed=2024, modes=modes)
     idx = np.linspace(0, len(specs) - 1, max(1, time_steps)).astype(int)
     sim = O.OracleSim(specs[idx[0]])
     for _ in range(warmup):
@@ -349,7 +362,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10, help="oracle time steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
-    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan"], default="pinched_witness")
+    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1"], default="pinched_witness")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -358,12 +371,12 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return
-        if args.workload == "scan":
-            rate, el = oracle_scan_rate(args.steps, args.warmup)
+        if args.workload in ("scan", "scan_m1"):
+            rate, el = oracle_scan_rate(args.steps, args.warmup, 1 if args.workload == "scan_m1" else 0)
             line = {"impl": "reference", "metric": "runs/s", "value": rate, "unit": "runs/s", "n_gpus": args.gpus,
                     "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-                    "data": "synthetic", "config": {"workload": "scan", "instances": 512, "time_steps_per_run": 20,
+                    "data": "synthetic", "config": {"workload": args.workload, "instances": 512, "time_steps_per_run": 20,
                                                     "beam_particles_per_run": 100000},
                     "cpu_baseline": {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
                                      "sample": f"one full time step of each of {args.steps} instances sampled "
@@ -392,14 +405,14 @@ def main():
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-    if args.workload == "scan":
+    if args.workload in ("scan", "scan_m1"):
         line = run_scan(args, rank, world, local_rank)
         if world > 1:
             import torch
 
             torch.distributed.destroy_process_group()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
-            rate, el = oracle_scan_rate(args.cpu_steps, 1)
+            rate, el = oracle_scan_rate(args.cpu_steps, 1, 1 if args.workload == "scan_m1" else 0)
             line["cpu_baseline"] = {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
                                     "sample": f"one full time step of each of {args.cpu_steps} instances sampled "
                                               f"across the scan, serial oracle, {el:.1f} s; a run = 21 such steps"}

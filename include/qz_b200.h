@@ -214,7 +214,8 @@ qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, 
 
 /* ------------------------------------------------------------------ batched independent runs
  * A parameter scan: many independent small runs (each its own grid, box, plasma and up to 2 beams,
- * m = 0, one AB order for all) in ONE persistent launch, a CTA per instance taken from a queue
+ * modes 0 or 1 (M <= 512 for modes 1), one AB order for all) in ONE persistent launch, a CTA per
+ * instance taken from a queue
  * (largest first). No counterpart in the reference, which runs one deck per process; each instance
  * is Simulation::run (src/Simulation.cpp:1370-1448) for constant dt. */
 typedef struct qz_batch qz_batch;

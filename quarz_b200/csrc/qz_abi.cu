@@ -1246,7 +1246,7 @@ struct qz_batch {
     int* d_order = nullptr;
     int* d_next = nullptr;
     double *d_fld = nullptr, *d_diag = nullptr, *d_bsrc = nullptr, *d_mom = nullptr;
-    size_t slots_alloc = 0, mom_alloc = 0;
+    size_t fld_alloc = 0, diag_alloc = 0, bsrc_alloc = 0, mom_alloc = 0;   // doubles
     float last_ms = 0;
     int last_grid = 0;
     ~qz_batch() {
@@ -1274,7 +1274,9 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
     if (!b || !nodes || !p || nbeams < 0 || nbeams > qzb::kBatchBeams || (nbeams > 0 && (!p7_host || !n || !q ||
         !m || !rigid || !gref || !xiref)))
         return fail(QZ_ERR_ARG, "qz_batch_add: bad argument (at most 2 beams per instance)");
-    if (p->modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_add: batched runs are built for modes = 0");
+    if (p->modes != 0 && p->modes != 1) return fail(QZ_ERR_ARG, "qz_batch_add: modes must be 0 or 1");
+    if (p->modes == 1 && M > qzb::kSweepThreads)
+        return fail(QZ_ERR_SIZE, "qz_batch_add: modes = 1 instances need M <= 512 (one radial row per thread)");
     if (b->ord && p->ab_order != b->ord) return fail(QZ_ERR_ARG, "qz_batch_add: every instance needs the same AB order");
     auto* I = new (std::nothrow) qz_batch::Inst;
     if (!I) return fail(QZ_ERR_NOMEM, "qz_batch_add: out of host memory");
@@ -1289,17 +1291,25 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         QZ_CUDA(cudaGetDevice(&dev));
         QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         const size_t reserve = sizeof(qzb::BatchInst) + sizeof(double) * 17 * (qzb::kSweepThreads / 32) + 256;
-        static const bool kLay[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
-        int lay = -1;
-        for (int l = 0; l < 4 && lay < 0; ++l)
-            if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1]) + reserve <= (size_t)optin) lay = l;
-        if (lay < 0) { delete I; return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep"); }
-        D.sw.dbuf = kLay[lay][0];
-        D.sw.const_smem = kLay[lay][1];
+        if (p->modes == 1) {
+            if (qzb::sweep_m1_smem_bytes(M) + reserve > (size_t)optin) {
+                delete I;
+                return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep");
+            }
+        } else {
+            static const bool kLay[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
+            int lay = -1;
+            for (int l = 0; l < 4 && lay < 0; ++l)
+                if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1]) + reserve <= (size_t)optin) lay = l;
+            if (lay < 0) { delete I; return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep"); }
+            D.sw.dbuf = kLay[lay][0];
+            D.sw.const_smem = kLay[lay][1];
+        }
     }
+    D.modes = p->modes;
     D.nbeams = nbeams;
     qz_box box;
-    box.xi_min = p->xi_min; box.dxi = p->dxi; box.K = p->K; box.ngp = p->ngp; box.modes = 0;
+    box.xi_min = p->xi_min; box.dxi = p->dxi; box.K = p->K; box.ngp = p->ngp; box.modes = p->modes;
     long ntot = 0;
     for (int k = 0; k < nbeams; ++k) {
         if (n[k] < 0 || (n[k] > 0 && !p7_host[k])) { delete I; return fail(QZ_ERR_ARG, "qz_batch_add: bad beam"); }
@@ -1320,7 +1330,8 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         ntot += n[k];
     }
     // cost estimate (queue order): the sweeps plus the beam work
-    I->cost = (double)p->K * (M + 4.0 * I->sw->np) + 2.0 * ntot;
+    // (the m = 1 slice costs about 7x the m = 0 one at the same M and particles)
+    I->cost = (p->modes ? 7.0 : 1.0) * (double)p->K * (M + 4.0 * I->sw->np) + 2.0 * ntot * (p->modes ? 3.0 : 1.0);
     b->ord = p->ab_order;
     b->inst.push_back(I);
     if (index) *index = (int)b->inst.size() - 1;
@@ -1333,33 +1344,39 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     if (ni == 0) return QZ_OK;
     cudaStream_t st = (cudaStream_t)stream;
     // slot sizes and shared memory: the largest instance
-    size_t fmax = 0, bmax = 0, smem = 0, mom_total = 0;
+    size_t fmax = 0, dmax = 0, bmax = 0, smem = 0, mom_total = 0;
+    bool with_m1 = false;
     std::vector<size_t> mom_off(ni);
     for (int i = 0; i < ni; ++i) {
         const auto& A = b->inst[i]->dev.sw;
+        const bool m1 = b->inst[i]->dev.modes == 1;
+        with_m1 = with_m1 || m1;
         const size_t km = (size_t)A.K * A.M;
-        fmax = std::max(fmax, km);
-        bmax = std::max(bmax, km);
-        smem = std::max(smem, qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem));
+        fmax = std::max(fmax, km * (m1 ? 18 : 6));           // fld (K, M, 18 / 6)
+        dmax = std::max(dmax, km * (m1 ? 9 : 3));            // diag (K, M, 9 / 3)
+        bmax = std::max(bmax, km * (m1 ? 15 : 5));           // bsrc (K, M, 15 / 5)
+        smem = std::max(smem, m1 ? qzb::sweep_m1_smem_bytes(A.M) : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem));
         mom_off[i] = mom_total;
         mom_total += (size_t)(nsteps + 1) * std::max(1, b->inst[i]->dev.nbeams) * 17;
     }
     int sms = 0;
-    const int grid = std::min(qzb::batch_max_grid(b->ord, smem, &sms), ni);
+    const int grid = std::min(qzb::batch_max_grid(b->ord, with_m1, smem, &sms), ni);
     if (grid < 1) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the batch kernel cannot be resident here");
     const size_t need = (size_t)grid;
-    if (b->slots_alloc < need * fmax) {
+    if (b->fld_alloc < need * fmax || b->diag_alloc < need * dmax || b->bsrc_alloc < need * bmax) {
         for (double* q : {b->d_fld, b->d_diag, b->d_bsrc})
             if (q) cudaFree(q);
         b->d_fld = b->d_diag = b->d_bsrc = nullptr;
-        b->slots_alloc = 0;
-        if (cudaMalloc((void**)&b->d_fld, sizeof(double) * need * fmax * 6) != cudaSuccess ||
-            cudaMalloc((void**)&b->d_diag, sizeof(double) * need * fmax * 3) != cudaSuccess ||
-            cudaMalloc((void**)&b->d_bsrc, sizeof(double) * need * bmax * 5) != cudaSuccess) {
+        b->fld_alloc = b->diag_alloc = b->bsrc_alloc = 0;
+        if (cudaMalloc((void**)&b->d_fld, sizeof(double) * need * fmax) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_diag, sizeof(double) * need * dmax) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_bsrc, sizeof(double) * need * bmax) != cudaSuccess) {
             cudaGetLastError();
             return fail(QZ_ERR_NOMEM, "qz_batch_run: device allocation failed (slot buffers)");
         }
-        b->slots_alloc = need * fmax;
+        b->fld_alloc = need * fmax;
+        b->diag_alloc = need * dmax;
+        b->bsrc_alloc = need * bmax;
     }
     if (b->mom_alloc < mom_total) {
         if (b->d_mom) cudaFree(b->d_mom);
@@ -1395,8 +1412,9 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     B.nsteps = nsteps;
     B.dt = dt;
     B.ord = b->ord;
+    B.with_m1 = with_m1 ? 1 : 0;
     B.fld = b->d_fld; B.diag = b->d_diag; B.bsrc = b->d_bsrc;
-    B.fld_slot = fmax * 6; B.diag_slot = fmax * 3; B.bsrc_slot = bmax * 5;
+    B.fld_slot = fmax; B.diag_slot = dmax; B.bsrc_slot = bmax;
     B.next = b->d_next;
     cudaEvent_t e0, e1;
     QZ_CUDA(cudaEventCreate(&e0));

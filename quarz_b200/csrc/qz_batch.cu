@@ -6,9 +6,11 @@
 // before the last sweep, the push of every beam with the next deposit (src/Beam.cpp:725-785,
 // :900-1131). Instances differ in grid, box, plasma and beams; their sweep arguments are copied into
 // shared memory, the field and beam-source buffers are the CTA's slot, and the beams are pushed by
-// the CTA itself with the grid arrays the sweep left in shared memory.
+// the CTA itself with the grid arrays the sweep left in shared memory. Instances with modes = 1 run
+// the m = 1 sweep (qz_sweep_m1_body.cuh) with their own source scratch.
 #include "qz_beam_body.cuh"
 #include "qz_sweep_body.cuh"
+#include "qz_sweep_m1_body.cuh"
 
 namespace qzb {
 
@@ -27,7 +29,7 @@ __device__ void beam_phase(const BatchInst& I, const SweepArgs& A, const BatchAr
                            double* red) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (push) {
-        const size_t nb = (size_t)A.K * A.M * B_NC0;
+        const size_t nb = (size_t)A.K * A.M * (I.modes ? B_NC1 : B_NC0);
         for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
         __syncthreads();
     }
@@ -87,7 +89,7 @@ __device__ void beam_phase(const BatchInst& I, const SweepArgs& A, const BatchAr
 // the step-0 deposit of every beam into the (zeroed) slot
 __device__ void beam_deposit0(const BatchInst& I, const SweepArgs& A) {
     const int tid = threadIdx.x;
-    const size_t nb = (size_t)A.K * A.M * B_NC0;
+    const size_t nb = (size_t)A.K * A.M * (I.modes ? B_NC1 : B_NC0);
     for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
     __syncthreads();
     for (int q = 0; q < I.nbeams; ++q) {
@@ -101,7 +103,9 @@ __device__ void beam_deposit0(const BatchInst& I, const SweepArgs& A) {
     __syncthreads();
 }
 
-template <int ORD>
+// WITH_M1: the batch holds modes = 1 instances (the m = 0 only variant keeps the m = 1 body out of the
+// kernel and its register allocation)
+template <int ORD, bool WITH_M1>
 __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_constant__ BatchArgs B) {
     extern __shared__ double smem_raw[];
     __shared__ BatchInst I;
@@ -126,7 +130,9 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
         beam_deposit0(I, A);
         for (int n = 0; n <= B.nsteps; ++n) {
             NoGate g;
-            if (A.rows_per_thread == 1) {
+            if (WITH_M1 && I.modes) {
+                if constexpr (WITH_M1) sweep_m1_body<ORD>(A, smem_raw, g);
+            } else if (A.rows_per_thread == 1) {
                 if (reg) sweep_body<ORD, true, 1>(A, smem_raw, g);
                 else sweep_body<ORD, false, 1>(A, smem_raw, g);
             } else {
@@ -139,52 +145,63 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
     }
 }
 
-template <int ORD>
+template <int ORD, bool WITH_M1>
 cudaError_t launch_t(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    cudaError_t e = cudaFuncSetAttribute(batch_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e =
+        cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    batch_kernel<ORD><<<grid, kSweepThreads, smem, s>>>(B);
+    batch_kernel<ORD, WITH_M1><<<grid, kSweepThreads, smem, s>>>(B);
     return cudaGetLastError();
 }
 
-template <int ORD>
+template <int ORD, bool WITH_M1>
 int occupancy_t(size_t smem) {
-    if (cudaFuncSetAttribute(batch_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
         return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD>, kSweepThreads, smem) != cudaSuccess)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD, WITH_M1>, kSweepThreads, smem) !=
+        cudaSuccess)
         return 0;
     return nb;
 }
 
+template <bool WITH_M1>
+int occupancy_any(int ord, size_t smem) {
+    switch (ord) {
+        case 1: return occupancy_t<1, WITH_M1>(smem);
+        case 2: return occupancy_t<2, WITH_M1>(smem);
+        case 3: return occupancy_t<3, WITH_M1>(smem);
+        case 4: return occupancy_t<4, WITH_M1>(smem);
+        case 5: return occupancy_t<5, WITH_M1>(smem);
+        default: return 0;
+    }
+}
+
+template <bool WITH_M1>
+cudaError_t launch_any(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
+    switch (B.ord) {
+        case 1: return launch_t<1, WITH_M1>(B, grid, smem, s);
+        case 2: return launch_t<2, WITH_M1>(B, grid, smem, s);
+        case 3: return launch_t<3, WITH_M1>(B, grid, smem, s);
+        case 4: return launch_t<4, WITH_M1>(B, grid, smem, s);
+        case 5: return launch_t<5, WITH_M1>(B, grid, smem, s);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
 }  // namespace
 
-int batch_max_grid(int ord, size_t smem, int* sms) {
+int batch_max_grid(int ord, bool with_m1, size_t smem, int* sms) {
     int dev = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    int per = 0;
-    switch (ord) {
-        case 1: per = occupancy_t<1>(smem); break;
-        case 2: per = occupancy_t<2>(smem); break;
-        case 3: per = occupancy_t<3>(smem); break;
-        case 4: per = occupancy_t<4>(smem); break;
-        case 5: per = occupancy_t<5>(smem); break;
-        default: return 0;
-    }
-    return per * nsm;
+    return (with_m1 ? occupancy_any<true>(ord, smem) : occupancy_any<false>(ord, smem)) * nsm;
 }
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    switch (B.ord) {
-        case 1: return launch_t<1>(B, grid, smem, s);
-        case 2: return launch_t<2>(B, grid, smem, s);
-        case 3: return launch_t<3>(B, grid, smem, s);
-        case 4: return launch_t<4>(B, grid, smem, s);
-        case 5: return launch_t<5>(B, grid, smem, s);
-        default: return cudaErrorInvalidValue;
-    }
+    return B.with_m1 ? launch_any<true>(B, grid, smem, s) : launch_any<false>(B, grid, smem, s);
 }
 
 }  // namespace qzb

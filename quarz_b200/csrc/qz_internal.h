@@ -170,6 +170,7 @@ constexpr int kBatchBeams = 2;
 
 struct BatchInst {
     SweepArgs sw;                   // bsrc / fld / diag are the slot's, set by the kernel
+    int modes;                      // 0, or 1 (the m = 1 sweep: M <= kSweepThreads)
     int nbeams;
     BeamArgs beam[kBatchBeams];     // grid pointers are set by the kernel (shared-memory copies)
     int rigid[kBatchBeams];
@@ -184,12 +185,13 @@ struct BatchArgs {
     int nsteps;
     double dt;
     int ord;
+    int with_m1;                    // some instances have modes = 1
     double *fld, *diag, *bsrc;      // per slot (= CTA)
     size_t fld_slot, diag_slot, bsrc_slot;
     int* next;                      // queue head (0)
 };
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t stream);
-int batch_max_grid(int ord, size_t smem, int* sms);
+int batch_max_grid(int ord, bool with_m1, size_t smem, int* sms);
 
 }  // namespace qzb

@@ -17,6 +17,9 @@ All are synthetic: seeded gaussian beams from the reference's generator, uniform
                     log-uniform in [3, 6] behind the driver centre, witness/driver charge ratio
                     log-uniform in [0.05, 0.3] (set through the witness n_b, pinched-witness shape),
                     5e4 + 5e4 beam particles, dt 5, 20 steps, m = 0
+  scan, modes = 1   the same draws with azimuthal modes m = 0, 1 (Picard 3, 4 azimuths per plasma ring,
+                    driver offset 0.1 in x) and N_r uniform in 128..511 cells: the m = 1 sweep keeps one
+                    radial row per thread, so M <= 512
 """
 from __future__ import annotations
 
@@ -169,13 +172,14 @@ def scan_nodes(n_nodes: int, h0: float, R: float = 6.0):
     return nodes
 
 
-def scan_instances(count: int = 512, seed: int = 2024, beam_particles: int = 100000, steps: int = 20):
+def scan_instances(count: int = 512, seed: int = 2024, beam_particles: int = 100000, steps: int = 20,
+                   modes: int = 0):
     """The instances of the batched scan, drawn from numpy's PCG64 with `seed` (see the module doc)."""
     rng = np.random.default_rng(seed)
     logu = lambda a, b: float(np.exp(rng.uniform(np.log(a), np.log(b))))  # noqa: E731
     out = []
     for i in range(count):
-        ncell = int(rng.integers(128, 1025))
+        ncell = int(rng.integers(128, 1025 if modes == 0 else 512))
         h0 = logu(5e-4, 5e-3)
         L = float(rng.uniform(8.0, 16.0))
         n0d = logu(1.0, 10.0)
@@ -215,6 +219,8 @@ witness.emit_n = 1e-3
 witness.nparticles = {beam_particles - half}
 witness.seed = {seed + 2 * i + 1}
 """
+        if modes == 1:
+            text += "modes = 1\nsolver.picard = 3\nelectrons.ntheta = 4\ndriver.x0 = 0.1\n"
         spec = spec_from_text(text)
         spec.nodes = scan_nodes(ncell + 1, h0)
         out.append(spec)

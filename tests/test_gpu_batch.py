@@ -4,7 +4,8 @@ same instance run on its own (step by step) and, for two of them, against the or
 Instances are drawn like the scan workload (quarz_b200.workloads.scan_instances: 128-1024 cells,
 stretched grids, xi lengths 8-16) with 4000 beam particles and 3 steps. Tolerances: derived beam
 moments 1e-10 relative to their natural scale against the single runs (only the summation order of
-the beam deposits differs), 1e-8 against the oracle."""
+the beam deposits differs), 1e-8 against the oracle. The m = 1 case draws the same way with modes 0, 1
+(Picard 3, 4 azimuths per ring, 128-511 cells), mixed in one batch with m = 0 instances."""
 import numpy as np
 import pytest
 
@@ -46,3 +47,28 @@ def test_batch_equals_single_runs_and_oracle():
     for s, bm, mom in list(zip(specs, beams, moms))[:2]:
         ref = O.OracleSim(s, beams=bm)
         _close(s, mom, ref.run(3, s.dt), bm, 1e-8)
+
+
+def test_batch_m1_and_mixed_modes():
+    m1 = workloads.scan_instances(3, seed=11, beam_particles=2000, steps=2, modes=1)
+    m0 = workloads.scan_instances(2, seed=12, beam_particles=2000, steps=2)
+    specs = m1 + m0
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    batch = Q.Batch()
+    for s, bm in zip(specs, beams):
+        batch.add(s, bm)
+    moms = batch.run(2, specs[0].dt)
+    for s, bm, mom in zip(specs, beams, moms):
+        sim = Q.Simulation(s, beams=bm)
+        sim.set_schedule(False)
+        _close(s, mom, sim.run(2, s.dt), bm, 1e-10)
+    ref = O.OracleSim(specs[0], beams=beams[0])
+    _close(specs[0], moms[0], ref.run(2, specs[0].dt), beams[0], 1e-8)
+
+
+def test_batch_m1_refuses_wide_grids():
+    spec = workloads.scan_instances(1, seed=3, beam_particles=1000, steps=1, modes=1)[0]
+    spec.modes = 1
+    spec.nodes = workloads.scan_nodes(700, 1e-3)
+    with pytest.raises(Q.QZError, match="M <= 512"):
+        Q.Batch().add(spec)
