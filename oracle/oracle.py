@@ -67,6 +67,7 @@ def lib():
         L.qzo_sim_plasma_get.argtypes = [C.c_void_p, C.c_int, dp, C.c_int]
         L.qzo_sim_run.argtypes = [C.c_void_p, C.c_int, C.c_double, dp]
         L.qzo_sim_deposit_beams.argtypes = [C.c_void_p]
+        L.qzo_sim_adjoint.argtypes = [C.c_void_p, C.c_int, C.c_double, dp, dp, dp]
         L.qzo_sample_gaussian.restype = C.c_long
         L.qzo_sample_gaussian.argtypes = [C.c_double] * 14 + [C.c_long, C.c_int, C.c_int, C.c_uint64, C.c_double,
                                                               dp, dp, dp]
@@ -265,6 +266,24 @@ class OracleSim:
         mom = np.zeros((nsteps + 1, max(nb, 1), 17))
         lib().qzo_sim_run(self.h, int(nsteps), float(dt), _p(mom))
         return mom[:, :nb, :]
+
+    def adjoint(self, nsteps, dt, lamS):
+        """Runs nsteps (like run) and then the adjoint: lamS (nbeams, 17) is the adjoint of the last
+        step's moment sums. Returns (per beam its (n, 7) adjoint of the initial particles, moments)."""
+        nb = len(self.spec.beams)
+        counts = [int(lib().qzo_sim_beam_count(self.h, b)) for b in range(nb)]
+        lam = np.zeros(7 * sum(counts) + 1)
+        mom = np.zeros((nsteps + 1, max(nb, 1), 17))
+        seeds = np.ascontiguousarray(np.asarray(lamS, dtype=np.float64).reshape(nb, 17))
+        rc = lib().qzo_sim_adjoint(self.h, int(nsteps), float(dt), _p(seeds), _p(lam), _p(mom))
+        if rc != 0:
+            raise ValueError("qzo_sim_adjoint: deck outside the adjoint's scope (m = 0, linear xi shape, one "
+                             "mobile species, fresh beams)")
+        out, off = [], 0
+        for n in counts:
+            out.append(lam[7 * off:7 * (off + n)].reshape(n, 7).copy())
+            off += n
+        return out, mom[:, :nb, :]
 
     def _view(self, f, nc):
         ptr = getattr(lib(), f)(self.h)

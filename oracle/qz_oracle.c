@@ -591,6 +591,9 @@ struct qzo_sim {
     int fnc, bnc, dnc;
     long lost;
     double* pool;
+    /* optional (the adjoint's recomputation): the mobile species' state at the start of every
+       slice, (K, 6 + 5 * ab_order, cap) -- x y px py dl w, then the AB history */
+    double* traj;
 };
 
 static double* take(double** cur, int M) { double* r = *cur; *cur += M; return r; }
@@ -1335,6 +1338,17 @@ int qzo_sim_step_fields(qzo_sim* s, double t) {
     memset(s->bguard, 0, sizeof(double) * 15 * M);
     const double dxi = s->p.dxi;
     for (int k = 0; k < K; ++k) {
+        if (s->traj)
+            for (int i = 0; i < s->nsp; ++i)
+                if (s->sp[i].p.mobile) {
+                    const species_t* q = &s->sp[i];
+                    const size_t cap = (size_t)q->cap, nv = 6 + 5 * (size_t)s->p.ab_order;
+                    double* o = s->traj + (size_t)k * nv * cap;
+                    const double* cols[6] = {q->x, q->y, q->px, q->py, q->dl, q->w};
+                    for (int c = 0; c < 6; ++c) memcpy(o + c * cap, cols[c], sizeof(double) * cap);
+                    memcpy(o + 6 * cap, q->hist, sizeof(double) * (nv - 6) * cap);
+                    break;
+                }
         zero_sources(s);
         for (int i = 0; i < s->nsp; ++i)
             if (s->sp[i].p.mobile) species_deposit(s, &s->sp[i]);

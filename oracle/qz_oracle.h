@@ -17,6 +17,8 @@
  *   beam                 src/Beam.cpp:483-570 (gaussian sampler), :725-785 (deposit), :900-905 (push),
  *                        :948-1131 (advance, Vay only), :1133-1192 (sums / from_sums)
  *   pushers              src/Pushers.hpp:144-176 (gamma2_root, solve_implicit, vay)
+ *   adjoint (m = 0)      qz_oracle_adj.c: the reverse of all of the above for one run (no
+ *                        reference counterpart; pinned by central differences of this forward)
  *   mode sums            src/SliceData.hpp:70-83
  *
  * Parity is pinned against the reference's own unit tests (tests/test_solvers.cpp,
@@ -119,6 +121,12 @@ int      qzo_sim_plasma_get(const qzo_sim* s, int sp, double* out6, int cap);
 int      qzo_sim_run(qzo_sim* s, int nsteps, double dt, double* mom);
 /* beam deposit only (into the sim's bsrc, which is zeroed first) */
 int      qzo_sim_deposit_beams(qzo_sim* s);
+/* the adjoint of a run (qz_oracle_adj.c; m = 0, linear xi shape, one mobile species): runs nsteps
+   like qzo_sim_run from the current (not yet pushed) beams, then in reverse returns in lam_out, for
+   every beam in order, its (n, 7) rows d(J)/d(x y px py pz xi w of each initial particle) with
+   J = sum(lamS * last step's moment sums), lamS (nb, 17). mom as in qzo_sim_run. 0, or -2 when the
+   deck is outside the adjoint's scope. */
+int      qzo_sim_adjoint(qzo_sim* s, int nsteps, double dt, const double* lamS, double* lam_out, double* mom);
 
 #ifdef __cplusplus
 }

@@ -1,0 +1,116 @@
+"""Gradients of witness energy gain and energy spread with respect to the driver current profile and
+the witness delay: the host side of the adjoint run.
+
+The reference has no gradients. The parameterisation follows the adjoint workload of the benchmark:
+
+- The driver current profile is a piecewise-linear function of xi on `nbins` nodes, spread evenly
+  over the sampled driver's extent (xi0 +- cut sigma_xi). It starts as the Gaussian exp(-(xi - xi0)^2 /
+  (2 sigma_xi^2)) at the nodes. A profile f gives each sampled driver particle the weight
+  w_i = w_i^s f(xi_i) / f0(xi_i): the sample's own weight times the profile's ratio to its initial
+  piecewise-linear interpolant. So at f = f0 the weights are exactly the sampled ones.
+- The witness delay d shifts the witness in xi: internal xi_i = xi_i^s + (d - d0), because the witness
+  sits at user xi0 = driver xi0 - d and the library's internal xi is minus the user's.
+- The objectives come from the witness's moment sums at the last step (Beam::sums,
+  src/Beam.cpp:1133-1155; from_sums, :1157-1192): the mean energy gain <gamma>_T - <gamma>_0, and the
+  rms energy spread sqrt(<G^2> - <G>^2) at the last step.
+
+The adjoint run returns dJ/d(initial particle) for a seed dJ/d(last moment sums). This module turns
+the seeds and the particle adjoints into the parameter gradients.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+from typing import Tuple
+
+import numpy as np
+
+# moment-sum indices (Beam::sums order): 0 sum w, 1 sum w G, 2 sum w G^2 (G = gamma - gref)
+_SW, _SG, _SG2 = 0, 1, 2
+
+
+@dataclass
+class DriverProfile:
+    """Piecewise-linear current profile on nodes xi_nodes (internal xi, increasing)."""
+    xi_nodes: np.ndarray
+    f0: np.ndarray
+
+    @classmethod
+    def gaussian(cls, xi0_internal: float, sigma_xi: float, cut: float = 3.0, nbins: int = 64) -> "DriverProfile":
+        nodes = np.linspace(xi0_internal - cut * sigma_xi, xi0_internal + cut * sigma_xi, nbins)
+        return cls(nodes, np.exp(-0.5 * ((nodes - xi0_internal) / sigma_xi) ** 2))
+
+    def hat(self, xi: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+        """(left node index, weight of the right node) of each xi, clamped to the node span."""
+        x = np.clip(np.asarray(xi, dtype=np.float64), self.xi_nodes[0], self.xi_nodes[-1])
+        h = self.xi_nodes[1] - self.xi_nodes[0]
+        i = np.minimum(((x - self.xi_nodes[0]) / h).astype(np.int64), len(self.xi_nodes) - 2)
+        t = (x - self.xi_nodes[i]) / h
+        return i, t
+
+    def interp(self, f: np.ndarray, xi: np.ndarray) -> np.ndarray:
+        i, t = self.hat(xi)
+        return (1.0 - t) * f[i] + t * f[i + 1]
+
+
+def driver_rows(sample: np.ndarray, prof: DriverProfile, f: np.ndarray) -> np.ndarray:
+    """The driver's particle rows (n, 7: x y px py pz xi w) with the weights of profile f."""
+    out = np.array(sample, dtype=np.float64, copy=True)
+    out[:, 6] = sample[:, 6] * prof.interp(f, sample[:, 5]) / prof.interp(prof.f0, sample[:, 5])
+    return out
+
+
+def witness_rows(sample: np.ndarray, shift: float) -> np.ndarray:
+    """The witness rows shifted by `shift` in internal xi (= the change of the delay)."""
+    out = np.array(sample, dtype=np.float64, copy=True)
+    out[:, 5] += shift
+    return out
+
+
+def _moments(S: np.ndarray) -> Tuple[float, float, float]:
+    sw = S[_SW]
+    return sw, S[_SG] / sw, S[_SG2] / sw
+
+
+def gain(S_last: np.ndarray, S_first: np.ndarray, gref: float) -> float:
+    return (gref + S_last[_SG] / S_last[_SW]) - (gref + S_first[_SG] / S_first[_SW])
+
+
+def spread(S_last: np.ndarray) -> float:
+    _, m0, m1 = _moments(S_last)
+    return float(np.sqrt(max(0.0, m1 - m0 * m0)))
+
+
+def gain_seed(S_last: np.ndarray) -> np.ndarray:
+    """dJ/dS (17) of the gain at the last step (the first step's sums do not depend on the driver
+    profile or the witness delay)."""
+    d = np.zeros(17)
+    d[_SG] = 1.0 / S_last[_SW]
+    d[_SW] = -S_last[_SG] / S_last[_SW] ** 2
+    return d
+
+
+def spread_seed(S_last: np.ndarray) -> np.ndarray:
+    sw = S_last[_SW]
+    J = spread(S_last)
+    d = np.zeros(17)
+    if J <= 0.0:
+        return d
+    d[_SG2] = 1.0 / sw
+    d[_SG] = -2.0 * S_last[_SG] / sw ** 2
+    d[_SW] = -S_last[_SG2] / sw ** 2 + 2.0 * S_last[_SG] ** 2 / sw ** 3
+    return d / (2.0 * J)
+
+
+def profile_gradient(lam_driver: np.ndarray, sample: np.ndarray, prof: DriverProfile) -> np.ndarray:
+    """dJ/df (nbins) from the driver particles' adjoint (n, 7): w_i = w_i^s f(xi_i) / f0(xi_i)."""
+    i, t = prof.hat(sample[:, 5])
+    c = lam_driver[:, 6] * sample[:, 6] / prof.interp(prof.f0, sample[:, 5])
+    g = np.zeros(len(prof.xi_nodes))
+    np.add.at(g, i, c * (1.0 - t))
+    np.add.at(g, i + 1, c * t)
+    return g
+
+
+def delay_gradient(lam_witness: np.ndarray) -> float:
+    """dJ/d(delay) from the witness particles' adjoint (n, 7): internal xi moves by +1 per unit."""
+    return float(np.sum(lam_witness[:, 5]))
