@@ -18,6 +18,8 @@ Other workloads (not the headline; their lines are recorded beside it):
   --workload scan     512 independent runs of 20 steps (a parameter scan) in one launch: runs/s, with
                       the plain loop over single runs (step by step, and pipelined) timed on a sample
   --workload scan_m1  the same scan with azimuthal modes 0 and 1 (M <= 512)
+  --workload adjoint  the gradient of witness energy gain and spread with respect to a 64-bin driver
+                      profile and the witness delay, pinched witness over 50 steps: adjoint / forward time
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
 """
@@ -296,6 +298,62 @@ def run_scan(args, rank, world, local_rank):
             "clocks": clk.result(), "gpu_launches": args.steps}
 
 
+def run_adjoint(args, rank, world, local_rank):
+    """One bench step = one gradient (qz_sim_adjoint: forward keeping the beams of every step, then the
+    reverse pass) of the witness energy gain with respect to the 64 driver-profile bins and the witness
+    delay, on the pinched-witness run over 50 steps; the forward it is compared with is the same run
+    through qz_sim_run (pipelined), both timed on the device."""
+    import numpy as np
+    import torch
+
+    import quarz_b200 as Q
+    from quarz_b200 import adjoint as A
+    from quarz_b200 import workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    spec = workloads.pinched_witness(steps=args.time_steps or 50)
+    T, dt = spec.steps, spec.dt
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    drv = spec.beams[0]
+    prof = A.DriverProfile.gaussian(-drv.xi0_user, drv.sigma_xi, drv.cut, 64)
+    sim = Q.Simulation(spec, beams=beams)
+    init = [torch.from_numpy(np.ascontiguousarray(p.T)).to(dev).contiguous() for p, _, _ in beams]
+    fwd, mom = [], None
+    for it in range(args.warmup + args.steps):
+        for b in range(len(init)):
+            sim.set_beam(b, init[b])
+        mom = sim.run(T, dt)
+        if it >= args.warmup:
+            fwd.append(sim.times()["kernel_ms"])
+    seeds = np.zeros((len(beams), 17))
+    seeds[1] = A.gain_seed(mom[-1, 1])
+    adj, split, grads = [], [], None
+    with ClockSampler(local_rank) as clk:
+        for it in range(max(1, args.steps)):
+            s2 = Q.Simulation(spec, beams=beams)
+            lam, _, ms = s2.adjoint(T, dt, seeds)
+            adj.append(ms[0] + ms[1])
+            split.append(ms)
+            del s2
+    grads = (A.profile_gradient(lam[0], beams[0][0], prof), A.delay_gradient(lam[1]))
+    f_ms, a_ms = float(np.median(fwd)), float(np.median(adj))
+    nbt = sum(len(p) for p, _, _ in beams)
+    return {"metric": "adjoint/forward time ratio", "value": a_ms / f_ms, "unit": "x", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": a_ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(spec, nbt, T, {"objective": "witness mean energy gain",
+                                             "parameters": "64 driver-profile bins + witness delay",
+                                             "adjoint": "step by step, beams of every step kept in HBM, "
+                                                        "sweep recomputed per step with its plasma trajectory"},
+                              "adjoint"),
+            "forward_ms": f_ms, "adjoint_ms": a_ms,
+            "adjoint_split_ms": {"forward_keeping_beams": float(np.median([m[0] for m in split])),
+                                 "reverse": float(np.median([m[1] for m in split]))},
+            "gradient_norm_profile": float(np.linalg.norm(grads[0])), "gradient_delay": grads[1],
+            "clocks": clk.result(), "gpu_launches": None}
+
+
 def oracle_rate(time_steps, warmup, spec):
     """The CPU oracle (serial restatement of the reference path) on the same workload: slice-solves/s
     over time_steps full time steps (sweep + moment sums + push), after warm-up steps."""
@@ -362,7 +420,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=10, help="oracle time steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
-    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1"], default="pinched_witness")
+    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1", "adjoint"],
+                    default="pinched_witness")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -405,6 +464,11 @@ def main():
         import torch
 
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.workload == "adjoint":
+        line = run_adjoint(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line))
+        return
     if args.workload in ("scan", "scan_m1"):
         line = run_scan(args, rank, world, local_rank)
         if world > 1:

@@ -212,6 +212,20 @@ qz_status qz_sim_counters(qz_sim* s, qz_counters* out);
 qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, double dt_drift, int push,
                            double* moments_host, void* stream);
 
+/* The adjoint of a run (no reference counterpart; modes = 0, linear xi shape, one mobile plasma
+ * species with at most 512 particles per slice, M <= 512). Runs nsteps like qz_sim_run (step by step,
+ * keeping the beams of every step on the device; the beams must not have been pushed yet), then the
+ * reverse pass: the beam pushes, sweeps and beam deposits of every step in reverse order.
+ *   lamS_host  (nbeams, 17): the adjoint of the last step's moment sums (Beam::sums order), i.e. J is
+ *              sum(lamS * sums) or the linearisation of a function of the sums
+ *   lam_host   per beam a 7 x n SoA host array (x y px py pz xi w, the caller's particle order):
+ *              receives dJ / d(initial particle)
+ *   mom_host   optional ((nsteps+1), nbeams, 17): the forward's moment sums
+ *   ms2        optional: the forward's and the reverse pass's device time (ms)
+ * The sim ends at the last step, as after qz_sim_run. */
+qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
+                         double* mom_host, double* ms2, void* stream);
+
 /* ------------------------------------------------------------------ batched independent runs
  * A parameter scan: many independent small runs (each its own grid, box, plasma and up to 2 beams,
  * modes 0 or 1 (M <= 512 for modes 1), one AB order for all) in ONE persistent launch, a CTA per

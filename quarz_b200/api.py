@@ -280,6 +280,21 @@ class Simulation:
                                     _stream_ptr(stream)))
         return mom[:, :nb, :]
 
+    def adjoint(self, nsteps: int, dt: float, lamS, stream=None):
+        """qz_sim_adjoint: runs nsteps (step by step, keeping the beams of every step) and the reverse
+        pass. lamS (nbeams, 17): the adjoint of the last step's moment sums. Returns (per beam its (n, 7)
+        adjoint of the initial particles (x y px py pz xi w), the forward's moment sums, (forward ms,
+        reverse ms))."""
+        nb = len(self.spec.beams)
+        seeds = np.ascontiguousarray(np.asarray(lamS, dtype=np.float64).reshape(nb, 17))
+        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nb)]
+        ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) for c in cols])
+        mom = np.zeros((nsteps + 1, max(nb, 1), 17))
+        ms = np.zeros(2)
+        check(lib().qz_sim_adjoint(self.h, int(nsteps), float(dt), _p(seeds), ptrs, _p(mom), _p(ms),
+                                   _stream_ptr(stream)))
+        return [c.T.copy() for c in cols], mom[:, :nb, :], (float(ms[0]), float(ms[1]))
+
     def fields(self):
         K, M = self.spec.K, self.spec.M
         fld = np.zeros(K * M * self.fnc)

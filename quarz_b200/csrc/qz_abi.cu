@@ -1085,6 +1085,162 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 
+// The adjoint of a run (qz_adjoint.cu). Forward: step by step like run_sequential, keeping the
+// beams of every step on the device. Reverse, for n = nsteps-1 .. 0: the beam deposit and the sweep
+// of step n again (recording the plasma trajectory), the beam pushes in reverse (field-store
+// adjoint), the sweep in reverse (beam-source adjoint), the beam deposits in reverse.
+extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
+                                    double* mom_host, double* ms2, void* stream) {
+    if (!s || nsteps < 1 || !(dt > 0.0) || !lamS_host || (!s->beams.empty() && !lam_host))
+        return fail(QZ_ERR_ARG, "qz_sim_adjoint: bad argument");
+    const qzb::SweepArgs& base = s->sw->base;
+    if (s->p.modes != 0 || s->p.ngp || s->p.K < 2)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2");
+    if (base.M > qzb::kSweepThreads || base.np > qzb::kSweepThreads || base.nsp != 1)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
+                                        "particles per slice");
+    for (size_t b = 0; b < s->beams.size(); ++b) {
+        if (s->beams[b].started)
+            return fail(QZ_ERR_ARG, "qz_sim_adjoint: the beams were pushed already (the adjoint starts a run)");
+        if (!lam_host[b]) return fail(QZ_ERR_ARG, "qz_sim_adjoint: null adjoint buffer");
+    }
+    cudaStream_t st = (cudaStream_t)stream;
+    void* sv = (void*)st;
+    const int nb = (int)s->beams.size();
+    for (auto& b : s->beams)                         // the caller's particle order
+        if (!b.orig_identity) {
+            QZ_CUDA(qzb::unpermute7(b.d, b.d2, b.orig, b.n, st));
+            std::swap(b.d, b.d2);
+            b.orig_identity = true;
+        }
+    std::vector<size_t> off(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) off[b + 1] = off[b] + (size_t)s->beams[b].n;
+    const size_t per = 7 * off[nb];
+    const int K = s->p.K, M = s->g->M;
+    const size_t KM = (size_t)K * M;
+    const size_t nv = 6 + 5 * (size_t)base.ord;
+    double *snap = nullptr, *traj = nullptr, *lfld = nullptr, *lbsrc = nullptr, *lam = nullptr, *lamS = nullptr;
+    auto release = [&]() {
+        for (double* q : {snap, traj, lfld, lbsrc, lam, lamS})
+            if (q) cudaFree(q);
+    };
+    if (cudaMalloc((void**)&snap, sizeof(double) * (per * (nsteps + 1) + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&traj, sizeof(double) * (size_t)K * nv * base.npad) != cudaSuccess ||
+        cudaMalloc((void**)&lfld, sizeof(double) * KM * 6) != cudaSuccess ||
+        cudaMalloc((void**)&lbsrc, sizeof(double) * KM * 5) != cudaSuccess ||
+        cudaMalloc((void**)&lam, sizeof(double) * (per + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&lamS, sizeof(double) * 17 * (nb + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return fail(QZ_ERR_NOMEM, "qz_sim_adjoint: device allocation failed (beams of every step, trajectory)");
+    }
+    const qz_box box = sim_box(s);
+    double* bsrc = s->d_bsrc[0];
+    auto view_at = [&](int b, double* base_ptr) {
+        const auto& B = s->beams[b];
+        qz_beam_view v = B.view();
+        double* d = base_ptr + 7 * off[b];
+        v.x = d; v.y = d + B.n; v.px = d + 2 * B.n; v.py = d + 3 * B.n; v.pz = d + 4 * B.n; v.xi = d + 5 * B.n;
+        v.w = d + 6 * B.n;
+        return v;
+    };
+    auto deposit_all = [&](double* beams_ptr) -> qz_status {
+        QZ_CUDA(cudaMemsetAsync(bsrc, 0, sizeof(double) * KM * 5, st));
+        for (int b = 0; b < nb; ++b) {
+            const qz_beam_view v = view_at(b, beams_ptr);
+            if (qz_status e = qz_beam_deposit(s->g, &v, &box, bsrc, sv)) return e;
+        }
+        return QZ_OK;
+    };
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    // the whole pass; QZ_CUDA returns from it, the buffers are released below in every case
+    auto pass = [&]() -> qz_status {
+        qz_status status = QZ_OK;
+        for (auto& e : ev) QZ_CUDA(cudaEventCreate(&e));
+        QZ_CUDA(cudaEventRecord(ev[0], st));
+        // ---- forward, keeping the beams of every step
+        for (int n = 0; n <= nsteps && status == QZ_OK; ++n) {
+            double* sn = snap + per * n;
+            for (int b = 0; b < nb; ++b)
+                QZ_CUDA(cudaMemcpyAsync(sn + 7 * off[b], s->beams[b].d, sizeof(double) * 7 * s->beams[b].n,
+                                        cudaMemcpyDeviceToDevice, st));
+            if ((status = deposit_all(sn))) break;
+            if ((status = qz_sweep_run(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, sv))) break;
+            if (mom_host) {
+                for (int b = 0; b < nb; ++b) {
+                    const qz_beam_view v = s->beams[b].view();
+                    if ((status = qz_beam_sums(&v, s->beams[b].gref, s->beams[b].xiref, s->d_mom + 17 * b, sv))) break;
+                }
+                if (status) return status;
+                QZ_CUDA(cudaMemcpyAsync(mom_host + (size_t)n * nb * 17, s->d_mom, sizeof(double) * 17 * nb,
+                                        cudaMemcpyDeviceToHost, st));
+            }
+            if (n < nsteps)
+                for (int b = 0; b < nb && status == QZ_OK; ++b) {
+                    auto& B = s->beams[b];
+                    if (B.rigid) continue;
+                    qz_beam_view v = B.view();
+                    status = qz_beam_push(s->g, &v, &box, s->d_fld, dt, dt, &B.started, sv);
+                }
+        }
+        if (status) return status;
+        QZ_CUDA(cudaEventRecord(ev[1], st));
+        // ---- seed: the last step's moment sums
+        QZ_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * per, st));
+        QZ_CUDA(cudaMemcpyAsync(lamS, lamS_host, sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
+        for (int b = 0; b < nb; ++b) {
+            const qz_beam_view v = view_at(b, snap + per * nsteps);
+            const qzb::BeamArgs BA = beam_args(s->g, &v, &box);
+            QZ_CUDA(qzb::launch_sums_back(BA, s->beams[b].gref, s->beams[b].xiref, lamS + 17 * b, lam + 7 * off[b], st));
+        }
+        // ---- reverse
+        qzb::SweepArgs A = base;
+        A.traj = traj;
+        A.bsrc = bsrc;
+        A.fld = s->d_fld;
+        A.diag = s->d_diag;
+        for (int n = nsteps - 1; n >= 0 && status == QZ_OK; --n) {
+            double* sn = snap + per * n;
+            if ((status = deposit_all(sn))) break;
+            QZ_CUDA(qzb::launch_sweep_m0(A, st));
+            QZ_CUDA(cudaMemsetAsync(lfld, 0, sizeof(double) * KM * 6, st));
+            for (int b = 0; b < nb; ++b) {
+                if (s->beams[b].rigid) continue;
+                const qz_beam_view v = view_at(b, sn);
+                QZ_CUDA(qzb::launch_push_back(beam_args(s->g, &v, &box), s->d_fld, lam + 7 * off[b], lfld, dt, dt,
+                                              n == 0 ? 1 : 0, st));
+            }
+            QZ_CUDA(cudaMemsetAsync(lbsrc, 0, sizeof(double) * KM * 5, st));
+            QZ_CUDA(qzb::launch_sweep_back(A, traj, s->d_fld, lfld, lbsrc, st));
+            for (int b = 0; b < nb; ++b) {
+                const qz_beam_view v = view_at(b, sn);
+                QZ_CUDA(qzb::launch_deposit_back(beam_args(s->g, &v, &box), lbsrc, lam + 7 * off[b], st));
+            }
+        }
+        if (status) return status;
+        QZ_CUDA(cudaEventRecord(ev[2], st));
+        for (int b = 0; b < nb; ++b)
+            QZ_CUDA(cudaMemcpyAsync(lam_host[b], lam + 7 * off[b], sizeof(double) * 7 * s->beams[b].n,
+                                    cudaMemcpyDeviceToHost, st));
+        // leave the fields of the last step, as qz_sim_run does
+        if ((status = deposit_all(snap + per * nsteps))) return status;
+        if ((status = qz_sweep_run(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, sv))) return status;
+        QZ_CUDA(cudaStreamSynchronize(st));
+        float t0 = 0, t1 = 0;
+        QZ_CUDA(cudaEventElapsedTime(&t0, ev[0], ev[1]));
+        QZ_CUDA(cudaEventElapsedTime(&t1, ev[1], ev[2]));
+        if (ms2) { ms2[0] = t0; ms2[1] = t1; }
+        return QZ_OK;
+    };
+    const qz_status status = pass();
+    cudaStreamSynchronize(st);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    release();
+    s->bsrc_valid = false;
+    return status;
+}
+
 extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span,
                                          double timeout_s) {
     if (!s || sweep_ctas < 0 || bucket < 0 || span < 0 || timeout_s < 0)

@@ -47,6 +47,9 @@ struct SweepArgs {
     const double* consts1;          // 9 x M: L1D Thomas 1/u, -a/u, -c/u; L0 rows a b c; L2D rows a b c
     double* bgs;                    // (3, M) scratch: background rho - J_z in modes 0 / 1
     double* srcs;                   // (2 x 30, M) scratch: the sources of this slice and of the next
+    // optional, m = 0 (the adjoint's recomputation): the plasma state at the start of every slice,
+    // (K, 6 + 5 * ord, npad): x y px py Delta w, then the AB history h[m][v] (m pushes ago)
+    double* traj;
 };
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem);
@@ -54,6 +57,13 @@ cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
 // the modes = 1 sweep: one CTA, one radial row per thread (M <= kSweepThreads), plasma in A.ps
 size_t sweep_m1_smem_bytes(int M);
 cudaError_t launch_sweep_m1(const SweepArgs& A, cudaStream_t stream);
+
+// the adjoint of an m = 0 run (qz_adjoint.cu): one CTA runs the sweep of one step in reverse, from
+// the field-store adjoint lfld (K, M, 6) to the beam-source adjoint lbsrc (K, M, 5, accumulated),
+// with the plasma trajectory recorded by the forward sweep; M and np at most kSweepThreads
+size_t adjoint_sweep_smem_bytes(int M);
+cudaError_t launch_sweep_back(const SweepArgs& A, const double* traj, const double* fld, const double* lfld,
+                              double* lbsrc, cudaStream_t stream);
 
 // Beam particles (SoA, device) and the box they live in.
 struct BeamArgs {
@@ -167,6 +177,13 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
 // CTA takes the next instance from a queue and runs all of it (Simulation::run: sweeps, moment sums,
 // pushes) with its own slot of field / beam-source buffers. Instances are queued largest first.
 constexpr int kBatchBeams = 2;
+
+// beam adjoints (qz_adjoint.cu); lam: 7 columns of n (x y px py pz xi w)
+cudaError_t launch_sums_back(const BeamArgs& B, double gref, double xiref, const double* lamS, double* lam,
+                             cudaStream_t stream);
+cudaError_t launch_push_back(const BeamArgs& B, const double* fld, double* lam, double* lfld, double dt_kick,
+                             double dt, int startup, cudaStream_t stream);
+cudaError_t launch_deposit_back(const BeamArgs& B, const double* lbsrc, double* lam, cudaStream_t stream);
 
 struct BatchInst {
     SweepArgs sw;                   // bsrc / fld / diag are the slot's, set by the kernel

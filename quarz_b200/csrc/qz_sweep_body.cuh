@@ -868,6 +868,23 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     int scan_par = 0;                                            // alternates the scan scratch
     const double fc = A.flux_coef;
     for (int k = 0; k < K; ++k) {
+        if (A.traj) {                                  // the plasma state at the start of slice k
+            double* T = A.traj + (size_t)k * (6 + 5 * (size_t)ORD) * npad;
+            if (REG) {
+                if (tid < np) {
+                    T[tid] = P.x; T[npad + tid] = P.y; T[2 * (size_t)npad + tid] = P.px;
+                    T[3 * (size_t)npad + tid] = P.py; T[4 * (size_t)npad + tid] = P.dl;
+                    T[5 * (size_t)npad + tid] = P.w;
+#pragma unroll
+                    for (int m = 0; m < ORD; ++m)
+#pragma unroll
+                        for (int v = 0; v < 5; ++v) T[(6 + (size_t)m * 5 + v) * npad + tid] = P.h[m][v];
+                }
+            } else {
+                for (int p = tid; p < np; p += kThreads)
+                    for (int v = 0; v < 6 + 5 * ORD; ++v) T[(size_t)v * npad + p] = gate.ps(A)[(size_t)v * npad + p];
+            }
+        }
         const Src s = src_of(S, M, A.dbuf ? (k & 1) : 0);
         const Src sn = src_of(S, M, A.dbuf ? ((k + 1) & 1) : 0);
         if (tim && tid == 0) t_sub = clock64();
