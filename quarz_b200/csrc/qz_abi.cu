@@ -796,7 +796,18 @@ qz_status grow(T** p, size_t* have, size_t need, const char* what) {
 // Simulation::run for constant dt as one pipelined launch (qz_pipeline.cu): the beams are put in
 // xi-cell order (their caller order is kept in orig), cut into buckets, the step-0 beam sources are
 // deposited into ring slot 0, then all sweeps and pushes run concurrently.
-qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cudaStream_t st) {
+// what a forward run records for the adjoint (qz_sim_adjoint): the plasma trajectory of every sweep
+// and the beams of every step before its push; with it the rings keep every step
+struct FwdRecord {
+    double* traj = nullptr;
+    size_t traj_slot = 0;
+    double* snap = nullptr;
+    size_t snap_step = 0;
+    long snap_off[qzb::kMaxBeams] = {0, 0, 0, 0};
+};
+
+qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cudaStream_t st,
+                        const FwdRecord* rec = nullptr) {
     auto& P_ = s->pipe;
     const int K = s->p.K, M = s->g->M, nb = (int)s->beams.size();
     const qz_box box = sim_box(s);
@@ -892,7 +903,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     const int wmin = std::max(8, (2 * g1) / 5);             // measured best: ~2/5 of the SMs push
     int nsweep = P_.sweep_ctas > 0 ? P_.sweep_ctas : std::min(nsteps + 1, g1 - wmin);
     nsweep = std::max(1, std::min({nsweep, nsteps + 1, g1 - 1}));
-    const int ring = std::max(2, std::min(nsteps + 1, nsweep + 2));
+    const int ring = rec ? std::max(2, nsteps + 1) : std::max(2, std::min(nsteps + 1, nsweep + 2));
     // 3. buffers
     const size_t KM = (size_t)K * M;
     if (P_.ring < ring) {
@@ -976,6 +987,13 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.err = bdone + nbk;
     A.lo = bdone + nbk + 1;
     A.timeout_ns = (unsigned long long)(P_.timeout_s * 1e9);
+    if (rec) {
+        A.traj = rec->traj;
+        A.traj_slot = rec->traj_slot;
+        A.snap = rec->snap;
+        A.snap_step = rec->snap_step;
+        for (int q = 0; q < qzb::kMaxBeams; ++q) A.snap_off[q] = rec->snap_off[q];
+    }
     A.trace = nullptr;
     if (P_.trace) {
         const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + 4;
@@ -1085,6 +1103,166 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 
+namespace {
+// The adjoint with both passes pipelined: the forward pipeline records the trajectories and the beams
+// of every step (rings of one slot per step), the reverse pipeline runs the reverse sweeps of
+// consecutive steps concurrently with the beam adjoint tasks (qz_adjoint.cu).
+qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
+                            double* mom_host, double* ms2, cudaStream_t st) {
+    auto& P_ = s->pipe;
+    const qzb::SweepArgs& base = s->sw->base;
+    const int nb = (int)s->beams.size();
+    const int K = s->p.K, M = s->g->M, T = nsteps;
+    const size_t KM = (size_t)K * M;
+    std::vector<size_t> off(nb + 1, 0);
+    for (int b = 0; b < nb; ++b) off[b + 1] = off[b] + (size_t)s->beams[b].n;
+    const size_t per = 7 * off[nb];
+    const size_t traj_slot = (size_t)K * (6 + 5 * (size_t)base.ord) * base.npad;
+    double *snap = nullptr, *traj = nullptr, *lam = nullptr, *lam2 = nullptr, *lfld = nullptr, *lbsrc = nullptr,
+           *lamS = nullptr;
+    int* ints = nullptr;
+    auto release = [&]() {
+        for (void* q : {(void*)snap, (void*)traj, (void*)lam, (void*)lam2, (void*)lfld, (void*)lbsrc, (void*)lamS,
+                        (void*)ints})
+            if (q) cudaFree(q);
+    };
+    if (cudaMalloc((void**)&snap, sizeof(double) * (per * (T + 1) + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&traj, sizeof(double) * traj_slot * (T + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&lam, sizeof(double) * (per + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&lam2, sizeof(double) * (per + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&lfld, sizeof(double) * KM * 6 * T) != cudaSuccess ||
+        cudaMalloc((void**)&lbsrc, sizeof(double) * KM * 5 * T) != cudaSuccess ||
+        cudaMalloc((void**)&lamS, sizeof(double) * 17 * (nb + 1)) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return fail(QZ_ERR_NOMEM, "qz_sim_adjoint: device allocation failed (records of every step)");
+    }
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+    auto pass = [&]() -> qz_status {
+        for (auto& e : ev) QZ_CUDA(cudaEventCreate(&e));
+        QZ_CUDA(cudaEventRecord(ev[0], st));
+        // ---- forward with records
+        FwdRecord rec;
+        rec.traj = traj;
+        rec.traj_slot = traj_slot;
+        rec.snap = snap;
+        rec.snap_step = per;
+        for (int b = 0; b < nb; ++b) rec.snap_off[b] = (long)(7 * off[b]);
+        if (qz_status e = run_pipelined(s, T, dt, mom_host, st, &rec)) return e;
+        for (int b = 0; b < nb; ++b)                   // the beams after the last push
+            QZ_CUDA(cudaMemcpyAsync(snap + per * T + 7 * off[b], s->beams[b].d, sizeof(double) * 7 * s->beams[b].n,
+                                    cudaMemcpyDeviceToDevice, st));
+        QZ_CUDA(cudaEventRecord(ev[1], st));
+        // ---- reverse
+        const int nbk = P_.info[4];
+        const size_t nints = (size_t)(T + 1) * nbk * 2 + (size_t)T * nbk + T + nbk + (T + 1) + 2;
+        QZ_CUDA(cudaMalloc((void**)&ints, sizeof(int) * (nints + 1)));
+        int* cmin = ints;
+        int* cmax = cmin + (size_t)(T + 1) * nbk;
+        int* pmax = cmax + (size_t)(T + 1) * nbk;
+        int* sync = pmax + (size_t)T * nbk;
+        qzb::AdjPipeArgs A{};
+        A.sw = base;
+        A.sw.timing = nullptr;
+        A.nsteps = T;
+        A.fld = P_.fld;
+        A.fld_slot = KM * 6;
+        A.traj = traj;
+        A.traj_slot = traj_slot;
+        A.lfld = lfld;
+        A.lfld_slot = KM * 6;
+        A.lbsrc = lbsrc;
+        A.lbsrc_slot = KM * 5;
+        A.nbeams = nb;
+        const qz_box box = sim_box(s);
+        for (int q = 0; q < nb; ++q) {
+            const qz_beam_view v = s->beams[q].view();
+            A.beam[q] = beam_args(s->g, &v, &box);
+            A.rigid[q] = s->beams[q].rigid;
+            A.startup[q] = s->beams[q].rigid ? 0 : 1;
+            A.snap_off[q] = (long)(7 * off[q]);
+            A.lam_off[q] = (long)(7 * off[q]);
+        }
+        A.snap = snap;
+        A.snap_step = per;
+        A.lam = lam;
+        A.dt = dt;
+        A.nbk = nbk;
+        A.bk_beam = P_.bk;
+        A.bk_start = P_.bk + nbk;
+        A.bk_end = P_.bk + 2 * nbk;
+        A.cmin = cmin;
+        A.pmax = pmax;
+        A.prog = sync;
+        A.bdone = sync + T;
+        A.next = sync + T + nbk;
+        A.err = A.next + (T + 1);
+        A.lo = A.err + 1;
+        A.timeout_ns = (unsigned long long)(P_.timeout_s * 1e9);
+        QZ_CUDA(qzb::launch_bucket_cells(A, cmin, cmax, pmax, st));
+        {
+            std::vector<int> init((size_t)T + nbk + (T + 1) + 2, 0);
+            for (int n = 0; n < T; ++n) init[n] = K;
+            for (int b = 0; b < nbk; ++b) init[T + b] = T;
+            QZ_CUDA(cudaMemcpyAsync(sync, init.data(), sizeof(int) * init.size(), cudaMemcpyHostToDevice, st));
+            QZ_CUDA(cudaStreamSynchronize(st));          // init is a host temporary
+        }
+        QZ_CUDA(cudaMemsetAsync(lfld, 0, sizeof(double) * KM * 6 * T, st));
+        QZ_CUDA(cudaMemsetAsync(lbsrc, 0, sizeof(double) * KM * 5 * T, st));
+        QZ_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * per, st));
+        QZ_CUDA(cudaMemcpyAsync(lamS, lamS_host, sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
+        for (int b = 0; b < nb; ++b) {
+            qz_beam_view v = s->beams[b].view();
+            double* d = snap + per * T + 7 * off[b];
+            v.x = d; v.y = d + v.n; v.px = d + 2 * v.n; v.py = d + 3 * v.n; v.pz = d + 4 * v.n; v.xi = d + 5 * v.n;
+            v.w = d + 6 * v.n;
+            QZ_CUDA(qzb::launch_sums_back(beam_args(s->g, &v, &box), s->beams[b].gref, s->beams[b].xiref, lamS + 17 * b,
+                                          lam + 7 * off[b], st));
+        }
+        int sms = 0;
+        const int grid = qzb::adjoint_pipeline_max_grid(A, &sms);
+        if (grid < 2) return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: the reverse pipeline cannot be resident here");
+        const int g1 = std::min(grid, sms);
+        const int wmin = std::max(8, (2 * g1) / 5);
+        A.nsweep = std::max(1, std::min(T, g1 - wmin));
+        QZ_CUDA(qzb::launch_adjoint_pipeline(A, g1, st));
+        int err = 0;
+        QZ_CUDA(cudaMemcpyAsync(&err, A.err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        QZ_CUDA(cudaEventRecord(ev[2], st));
+        // the caller's particle order
+        for (int b = 0; b < nb; ++b) {
+            const auto& B = s->beams[b];
+            if (B.orig_identity)
+                QZ_CUDA(cudaMemcpyAsync(lam2 + 7 * off[b], lam + 7 * off[b], sizeof(double) * 7 * B.n,
+                                        cudaMemcpyDeviceToDevice, st));
+            else
+                QZ_CUDA(qzb::unpermute7(lam + 7 * off[b], lam2 + 7 * off[b], B.orig, B.n, st));
+            QZ_CUDA(cudaMemcpyAsync(lam_host[b], lam2 + 7 * off[b], sizeof(double) * 7 * B.n, cudaMemcpyDeviceToHost,
+                                    st));
+        }
+        QZ_CUDA(cudaStreamSynchronize(st));
+        if (err) {
+            static const char* site[] = {"?", "beam adjoint rows", "no beam adjoint task ready"};
+            const int w = (err >> 8) & 0xff;
+            return fail(QZ_ERR_CUDA, std::string("qz_sim_adjoint: reverse pipeline wait timed out (") +
+                                         site[w <= 2 ? w : 0] + "); results of this call are invalid");
+        }
+        float t0 = 0, t1 = 0;
+        QZ_CUDA(cudaEventElapsedTime(&t0, ev[0], ev[1]));
+        QZ_CUDA(cudaEventElapsedTime(&t1, ev[1], ev[2]));
+        if (ms2) { ms2[0] = t0; ms2[1] = t1; }
+        return QZ_OK;
+    };
+    const qz_status status = pass();
+    cudaStreamSynchronize(st);
+    for (auto& e : ev)
+        if (e) cudaEventDestroy(e);
+    release();
+    s->bsrc_valid = false;
+    return status;
+}
+}  // namespace
+
 // The adjoint of a run (qz_adjoint.cu). Forward: step by step like run_sequential, keeping the
 // beams of every step on the device. Reverse, for n = nsteps-1 .. 0: the beam deposit and the sweep
 // of step n again (recording the plasma trajectory), the beam pushes in reverse (field-store
@@ -1105,6 +1283,8 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
         if (!lam_host[b]) return fail(QZ_ERR_ARG, "qz_sim_adjoint: null adjoint buffer");
     }
     cudaStream_t st = (cudaStream_t)stream;
+    if (s->pipe.enabled && s->beams.size() <= (size_t)qzb::kMaxBeams)
+        return adjoint_pipelined(s, nsteps, dt, lamS_host, lam_host, mom_host, ms2, st);
     void* sv = (void*)st;
     const int nb = (int)s->beams.size();
     for (auto& b : s->beams)                         // the caller's particle order

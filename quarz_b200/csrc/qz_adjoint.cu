@@ -125,194 +125,206 @@ __global__ void sums_back_kernel(BeamArgs B, double gref, double xiref, const do
     }
 }
 
-// One push (start-up half kick when startup, gather, Vay, drift) in reverse. On entry lam is the
-// adjoint after the push, on exit before it; the field adjoint is added to lfld (K, M, 6).
-__global__ void push_back_kernel(BeamArgs B, const double* __restrict__ fld, double* __restrict__ lam,
-                                 double* __restrict__ lfld, double dt_kick, double dt, int startup) {
-    const long n = B.n;
+// One push of particle i (start-up half kick when startup, gather, Vay, drift) in reverse. On entry
+// l7 is the adjoint after the push, on exit before it; the field adjoint is added to lfld (K, M, 6).
+__device__ void push_back_one(const BeamArgs& B, const double* __restrict__ fld, long i, double (&l7)[7],
+                              double* __restrict__ lfld, double dt_kick, double dt, int startup) {
     const int M = B.M, nloc = B.K;
     const double qm = B.q / B.m;
     const double xmin = B.xi_min, xmax = B.xi_min + (B.K - 1) * B.dxi;
+    if (B.w[i] == 0.0) {
+#pragma unroll
+        for (int c = 0; c < 6; ++c) l7[c] = 0.0;
+        return;
+    }
+    const double X = B.x[i], Y = B.y[i], XI = B.xi[i];
+    const double r = sqrt(X * X + Y * Y);
+    const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
+    double sl = (XI - xmin) * B.idxi;
+    int k = (int)floor(sl);
+    bool kclamp = false;
+    if (k < 0) { k = 0; sl = 0; kclamp = true; }
+    if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = true; }
+    const double tk = sl - k;
+    const int k1 = k + 1;
+    int j;
+    double t;
+    weights(B.r, B.inv_h, B.N, B.R, r, j, t);
+    const double* f00 = fld + ((size_t)k * M + j) * F_NC0;
+    const double* f01 = f00 + F_NC0;
+    const double* f10 = fld + ((size_t)k1 * M + j) * F_NC0;
+    const double* f11 = f10 + F_NC0;
+    auto bil = [&](int cm) {
+        return (1.0 - tk) * ((1.0 - t) * f00[cm] + t * f01[cm]) + tk * ((1.0 - t) * f10[cm] + t * f11[cm]);
+    };
+    const double er = bil(F_EP1R), ei = bil(F_EP1I), br = bil(F_BP1R), bi = bil(F_BP1I);
+    const V3 E = {er * c - ei * sn, er * sn + ei * c, bil(F_EZ0)};
+    const V3 Bf = {br * c - bi * sn, br * sn + bi * c, bil(F_BZ0)};
+    const V3 u0 = {B.px[i], B.py[i], B.pz[i]};
+    V3 u1 = u0;
+    const double hs = 0.5 * qm * (-0.5 * dt_kick);
+    double g00 = 1.0;
+    if (startup) {
+        g00 = sqrt(1.0 + dot3(u0, u0));
+        const double ig = 1.0 / g00;
+        const V3 v = {ig * u0.x, ig * u0.y, ig * u0.z};
+        const V3 vxb = cross3(v, Bf);
+        const double h2 = 2.0 * hs;
+        u1 = {u0.x + h2 * (E.x + vxb.x), u0.y + h2 * (E.y + vxb.y), u0.z + h2 * (E.z + vxb.z)};
+    }
+    const double h = 0.5 * qm * dt_kick;
+    const V3 u2 = vay(u1, E, Bf, h);
+    const double p2 = u2.x * u2.x + u2.y * u2.y;
+    const double gam = sqrt(1.0 + p2 + u2.z * u2.z);
+    const double omvz = (1.0 + p2) / (gam * (gam + u2.z));
+    const double xn = X + u2.x / gam * dt, yn = Y + u2.y / gam * dt;
+    const double xin = XI + omvz * dt;
+    if (xn * xn + yn * yn >= B.R * B.R || xin < xmin || xin > xmax) {     // removed by this push
+#pragma unroll
+        for (int cc = 0; cc < 7; ++cc) l7[cc] = 0.0;
+        return;
+    }
+    // drift
+    double lX = l7[0], lY = l7[1], lxi = l7[5];
+    V3 lu2 = {l7[2], l7[3], l7[4]};
+    const double lgam = -(l7[0] * u2.x + l7[1] * u2.y) * dt / (gam * gam);
+    lu2.x += l7[0] * dt / gam;
+    lu2.y += l7[1] * dt / gam;
+    double lp[3] = {0.0, 0.0, 0.0};
+    omvz_back(u2.x, u2.y, u2.z, l7[5] * dt, lp);
+    lu2 = {lu2.x + lp[0] + lgam * u2.x / gam, lu2.y + lp[1] + lgam * u2.y / gam, lu2.z + lp[2] + lgam * u2.z / gam};
+    V3 lu1 = {0, 0, 0}, lE = {0, 0, 0}, lB = {0, 0, 0};
+    vay_back(u1, E, Bf, h, lu2, lu1, lE, lB);
+    V3 lu0 = lu1;
+    if (startup) {
+        const V3 lw = mul3(2.0 * hs, lu1);                  // w = E + (u0 x B) / g00
+        lE = add3(lE, lw);
+        const V3 lcr = mul3(1.0 / g00, lw);
+        lu0 = add3(lu0, cross3(Bf, lcr));
+        lB = add3(lB, cross3(lcr, u0));
+        const double l_ig = dot3(lw, cross3(u0, Bf));
+        lu0 = add3(lu0, mul3(-l_ig / (g00 * g00 * g00), u0));
+    }
+    const double l_er = lE.x * c + lE.y * sn, l_ei = -lE.x * sn + lE.y * c;
+    const double l_br = lB.x * c + lB.y * sn, l_bi = -lB.x * sn + lB.y * c;
+    const double l_c = lE.x * er + lE.y * ei + lB.x * br + lB.y * bi;
+    const double l_s = -lE.x * ei + lE.y * er - lB.x * bi + lB.y * br;
+    const double lcomp[6] = {l_er, l_ei, l_br, l_bi, lE.z, lB.z};
+    const int comp[6] = {F_EP1R, F_EP1I, F_BP1R, F_BP1I, F_EZ0, F_BZ0};
+    double* g00p = lfld + ((size_t)k * M + j) * F_NC0;
+    double* g01p = g00p + F_NC0;
+    double* g10p = lfld + ((size_t)k1 * M + j) * F_NC0;
+    double* g11p = g10p + F_NC0;
+    double l_tk = 0.0, l_t = 0.0;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int cm = comp[q];
+        const double l = lcomp[q];
+        atomicAdd(g00p + cm, l * (1.0 - tk) * (1.0 - t));
+        atomicAdd(g01p + cm, l * (1.0 - tk) * t);
+        atomicAdd(g10p + cm, l * tk * (1.0 - t));
+        atomicAdd(g11p + cm, l * tk * t);
+        l_tk += l * (((1.0 - t) * f10[cm] + t * f11[cm]) - ((1.0 - t) * f00[cm] + t * f01[cm]));
+        l_t += l * ((1.0 - tk) * (f01[cm] - f00[cm]) + tk * (f11[cm] - f10[cm]));
+    }
+    if (!kclamp) lxi += l_tk * B.idxi;
+    const double tt = (r - B.r[j]) * B.inv_h[j];
+    const double l_r = (tt > 0.0 && tt < 1.0) ? l_t * B.inv_h[j] : 0.0;
+    polar_back(r, c, sn, l_r, l_c, l_s, lX, lY);
+    l7[0] = lX; l7[1] = lY; l7[2] = lu0.x; l7[3] = lu0.y; l7[4] = lu0.z; l7[5] = lxi;
+    // l7[6] (w) is carried unchanged: the push does not change the weight
+}
+
+__global__ void push_back_kernel(BeamArgs B, const double* __restrict__ fld, double* __restrict__ lam,
+                                 double* __restrict__ lfld, double dt_kick, double dt, int startup) {
+    const long n = B.n;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
         double l7[7];
 #pragma unroll
         for (int c = 0; c < 7; ++c) l7[c] = lam[c * n + i];
-        if (B.w[i] == 0.0) {
+        push_back_one(B, fld, i, l7, lfld, dt_kick, dt, startup);
 #pragma unroll
-            for (int c = 0; c < 6; ++c) lam[c * n + i] = 0.0;
-            continue;
-        }
-        const double X = B.x[i], Y = B.y[i], XI = B.xi[i];
-        const double r = sqrt(X * X + Y * Y);
-        const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
-        double sl = (XI - xmin) * B.idxi;
-        int k = (int)floor(sl);
-        bool kclamp = false;
-        if (k < 0) { k = 0; sl = 0; kclamp = true; }
-        if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = true; }
-        const double tk = sl - k;
-        const int k1 = k + 1;
-        int j;
-        double t;
-        weights(B.r, B.inv_h, B.N, B.R, r, j, t);
-        const double* f00 = fld + ((size_t)k * M + j) * F_NC0;
-        const double* f01 = f00 + F_NC0;
-        const double* f10 = fld + ((size_t)k1 * M + j) * F_NC0;
-        const double* f11 = f10 + F_NC0;
-        auto bil = [&](int cm) {
-            return (1.0 - tk) * ((1.0 - t) * f00[cm] + t * f01[cm]) + tk * ((1.0 - t) * f10[cm] + t * f11[cm]);
-        };
-        const double er = bil(F_EP1R), ei = bil(F_EP1I), br = bil(F_BP1R), bi = bil(F_BP1I);
-        const V3 E = {er * c - ei * sn, er * sn + ei * c, bil(F_EZ0)};
-        const V3 Bf = {br * c - bi * sn, br * sn + bi * c, bil(F_BZ0)};
-        const V3 u0 = {B.px[i], B.py[i], B.pz[i]};
-        V3 u1 = u0;
-        const double hs = 0.5 * qm * (-0.5 * dt_kick);
-        double g00 = 1.0;
-        if (startup) {
-            g00 = sqrt(1.0 + dot3(u0, u0));
-            const double ig = 1.0 / g00;
-            const V3 v = {ig * u0.x, ig * u0.y, ig * u0.z};
-            const V3 vxb = cross3(v, Bf);
-            const double h2 = 2.0 * hs;
-            u1 = {u0.x + h2 * (E.x + vxb.x), u0.y + h2 * (E.y + vxb.y), u0.z + h2 * (E.z + vxb.z)};
-        }
-        const double h = 0.5 * qm * dt_kick;
-        const V3 u2 = vay(u1, E, Bf, h);
-        const double p2 = u2.x * u2.x + u2.y * u2.y;
-        const double gam = sqrt(1.0 + p2 + u2.z * u2.z);
-        const double omvz = (1.0 + p2) / (gam * (gam + u2.z));
-        const double xn = X + u2.x / gam * dt, yn = Y + u2.y / gam * dt;
-        const double xin = XI + omvz * dt;
-        if (xn * xn + yn * yn >= B.R * B.R || xin < xmin || xin > xmax) {   // removed by this push
-#pragma unroll
-            for (int cc = 0; cc < 7; ++cc) lam[cc * n + i] = 0.0;
-            continue;
-        }
-        // drift
-        double lX = l7[0], lY = l7[1], lxi = l7[5];
-        V3 lu2 = {l7[2], l7[3], l7[4]};
-        const double lgam = -(l7[0] * u2.x + l7[1] * u2.y) * dt / (gam * gam);
-        lu2.x += l7[0] * dt / gam;
-        lu2.y += l7[1] * dt / gam;
-        double lp[3] = {0.0, 0.0, 0.0};
-        omvz_back(u2.x, u2.y, u2.z, l7[5] * dt, lp);
-        lu2 = {lu2.x + lp[0] + lgam * u2.x / gam, lu2.y + lp[1] + lgam * u2.y / gam, lu2.z + lp[2] + lgam * u2.z / gam};
-        V3 lu1 = {0, 0, 0}, lE = {0, 0, 0}, lB = {0, 0, 0};
-        vay_back(u1, E, Bf, h, lu2, lu1, lE, lB);
-        V3 lu0 = lu1;
-        if (startup) {
-            const V3 lw = mul3(2.0 * hs, lu1);                  // w = E + (u0 x B) / g00
-            lE = add3(lE, lw);
-            const V3 lcr = mul3(1.0 / g00, lw);
-            lu0 = add3(lu0, cross3(Bf, lcr));
-            lB = add3(lB, cross3(lcr, u0));
-            const double l_ig = dot3(lw, cross3(u0, Bf));
-            lu0 = add3(lu0, mul3(-l_ig / (g00 * g00 * g00), u0));
-        }
-        const double l_er = lE.x * c + lE.y * sn, l_ei = -lE.x * sn + lE.y * c;
-        const double l_br = lB.x * c + lB.y * sn, l_bi = -lB.x * sn + lB.y * c;
-        const double l_c = lE.x * er + lE.y * ei + lB.x * br + lB.y * bi;
-        const double l_s = -lE.x * ei + lE.y * er - lB.x * bi + lB.y * br;
-        const double lcomp[6] = {l_er, l_ei, l_br, l_bi, lE.z, lB.z};
-        const int comp[6] = {F_EP1R, F_EP1I, F_BP1R, F_BP1I, F_EZ0, F_BZ0};
-        double* g00p = lfld + ((size_t)k * M + j) * F_NC0;
-        double* g01p = g00p + F_NC0;
-        double* g10p = lfld + ((size_t)k1 * M + j) * F_NC0;
-        double* g11p = g10p + F_NC0;
-        double l_tk = 0.0, l_t = 0.0;
-#pragma unroll
-        for (int q = 0; q < 6; ++q) {
-            const int cm = comp[q];
-            const double l = lcomp[q];
-            atomicAdd(g00p + cm, l * (1.0 - tk) * (1.0 - t));
-            atomicAdd(g01p + cm, l * (1.0 - tk) * t);
-            atomicAdd(g10p + cm, l * tk * (1.0 - t));
-            atomicAdd(g11p + cm, l * tk * t);
-            l_tk += l * (((1.0 - t) * f10[cm] + t * f11[cm]) - ((1.0 - t) * f00[cm] + t * f01[cm]));
-            l_t += l * ((1.0 - tk) * (f01[cm] - f00[cm]) + tk * (f11[cm] - f10[cm]));
-        }
-        if (!kclamp) lxi += l_tk * B.idxi;
-        const double tt = (r - B.r[j]) * B.inv_h[j];
-        const double l_r = (tt > 0.0 && tt < 1.0) ? l_t * B.inv_h[j] : 0.0;
-        polar_back(r, c, sn, l_r, l_c, l_s, lX, lY);
-        lam[i] = lX;
-        lam[n + i] = lY;
-        lam[2 * n + i] = lu0.x;
-        lam[3 * n + i] = lu0.y;
-        lam[4 * n + i] = lu0.z;
-        lam[5 * n + i] = lxi;
-        // lam[6] (w) is carried unchanged: the push does not change the weight
+        for (int c = 0; c < 7; ++c) lam[c * n + i] = l7[c];
     }
 }
 
-// Beam::deposit in reverse (m = 0, linear xi shape): lam += d(lbsrc . bsrc)/d(particle)
+// Beam::deposit of particle i in reverse (m = 0, linear xi shape): l7 += d(lbsrc . bsrc)/d(particle);
+// kL2: lbsrc was written by other SMs during the same launch
+template <bool kL2>
+__device__ void deposit_back_one(const BeamArgs& B, const double* __restrict__ lbsrc, long i, double (&l7)[7]) {
+    const int M = B.M, nloc = B.K;
+    const double wi = B.w[i];
+    if (wi == 0.0) return;
+    const double X = B.x[i], Y = B.y[i];
+    const double r = sqrt(X * X + Y * Y);
+    if (r > B.R) return;
+    const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
+    const double sx = (B.xi[i] - B.xi_min) * B.idxi;
+    const int k = (int)floor(sx);
+    if (k < -1 || k >= nloc) return;
+    const double tk = sx - k;
+    const double PX = B.px[i], PY = B.py[i], PZ = B.pz[i];
+    const double p2 = PX * PX + PY * PY;
+    const double gam = sqrt(1.0 + p2 + PZ * PZ);
+    const double omvz = (1.0 + p2) / (gam * (gam + PZ));
+    const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
+    const double vr = c * vx + sn * vy, vt = c * vy - sn * vx;
+    int j;
+    double t;
+    weights(B.r, B.inv_h, B.N, B.R, r, j, t);
+    const double Wr[2] = {1.0 - t, t};
+    const double Wk[2] = {1.0 - tk, tk};
+    double l_omvz = 0, l_vz = 0, l_vr = 0, l_vt = 0, l_w = 0, lWk[2] = {0, 0}, lWr[2] = {0, 0};
+#pragma unroll
+    for (int a = 0; a < 2; ++a) {
+        const int kk = k + a;
+        if (kk < 0 || kk >= nloc) continue;
+#pragma unroll
+        for (int b = 0; b < 2; ++b) {
+            const int jj = j + b;
+            const double* L = lbsrc + ((size_t)kk * M + jj) * B_NC0;
+            const double base = B.q * B.inv_V[jj] * B.idxi;
+            const double d = wi * Wk[a] * Wr[b] * base;
+            const double L0 = beam_detail::fload<kL2>(L + B_RT0), L1 = beam_detail::fload<kL2>(L + B_JZ0);
+            const double L2 = beam_detail::fload<kL2>(L + B_JP1R), L3 = beam_detail::fload<kL2>(L + B_JP1I);
+            const double ld = L0 * omvz + L1 * vz + L2 * vr + L3 * vt;
+            l_omvz += L0 * d;
+            l_vz += L1 * d;
+            l_vr += L2 * d;
+            l_vt += L3 * d;
+            l_w += ld * Wk[a] * Wr[b] * base;
+            lWk[a] += ld * wi * Wr[b] * base;
+            lWr[b] += ld * wi * Wk[a] * base;
+        }
+    }
+    l7[6] += l_w;
+    l7[5] += (lWk[1] - lWk[0]) * B.idxi;
+    const double tt = (r - B.r[j]) * B.inv_h[j];
+    const double l_r = (tt > 0.0 && tt < 1.0) ? (lWr[1] - lWr[0]) * B.inv_h[j] : 0.0;
+    const double l_vx = l_vr * c - l_vt * sn, l_vy = l_vr * sn + l_vt * c;
+    const double l_c = l_vr * vx + l_vt * vy, l_s = l_vr * vy - l_vt * vx;
+    polar_back(r, c, sn, l_r, l_c, l_s, l7[0], l7[1]);
+    double lp[3] = {l_vx / gam, l_vy / gam, l_vz / gam};
+    const double l_g = -(l_vx * PX + l_vy * PY + l_vz * PZ) / (gam * gam);
+    lp[0] += l_g * PX / gam;
+    lp[1] += l_g * PY / gam;
+    lp[2] += l_g * PZ / gam;
+    omvz_back(PX, PY, PZ, l_omvz, lp);
+    l7[2] += lp[0];
+    l7[3] += lp[1];
+    l7[4] += lp[2];
+}
+
 __global__ void deposit_back_kernel(BeamArgs B, const double* __restrict__ lbsrc, double* __restrict__ lam) {
     const long n = B.n;
-    const int M = B.M, nloc = B.K;
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
-        const double wi = B.w[i];
-        if (wi == 0.0) continue;
-        const double X = B.x[i], Y = B.y[i];
-        const double r = sqrt(X * X + Y * Y);
-        if (r > B.R) continue;
-        const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
-        const double sx = (B.xi[i] - B.xi_min) * B.idxi;
-        const int k = (int)floor(sx);
-        if (k < -1 || k >= nloc) continue;
-        const double tk = sx - k;
-        const double PX = B.px[i], PY = B.py[i], PZ = B.pz[i];
-        const double p2 = PX * PX + PY * PY;
-        const double gam = sqrt(1.0 + p2 + PZ * PZ);
-        const double omvz = (1.0 + p2) / (gam * (gam + PZ));
-        const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
-        const double vr = c * vx + sn * vy, vt = c * vy - sn * vx;
-        int j;
-        double t;
-        weights(B.r, B.inv_h, B.N, B.R, r, j, t);
-        const double Wr[2] = {1.0 - t, t};
-        const double Wk[2] = {1.0 - tk, tk};
-        double l_omvz = 0, l_vz = 0, l_vr = 0, l_vt = 0, l_w = 0, lWk[2] = {0, 0}, lWr[2] = {0, 0};
+        if (B.w[i] == 0.0) continue;
+        double l7[7];
 #pragma unroll
-        for (int a = 0; a < 2; ++a) {
-            const int kk = k + a;
-            if (kk < 0 || kk >= nloc) continue;
+        for (int c = 0; c < 7; ++c) l7[c] = lam[c * n + i];
+        deposit_back_one<false>(B, lbsrc, i, l7);
 #pragma unroll
-            for (int b = 0; b < 2; ++b) {
-                const int jj = j + b;
-                const double* L = lbsrc + ((size_t)kk * M + jj) * B_NC0;
-                const double base = B.q * B.inv_V[jj] * B.idxi;
-                const double d = wi * Wk[a] * Wr[b] * base;
-                const double L0 = L[B_RT0], L1 = L[B_JZ0], L2 = L[B_JP1R], L3 = L[B_JP1I];
-                const double ld = L0 * omvz + L1 * vz + L2 * vr + L3 * vt;
-                l_omvz += L0 * d;
-                l_vz += L1 * d;
-                l_vr += L2 * d;
-                l_vt += L3 * d;
-                l_w += ld * Wk[a] * Wr[b] * base;
-                lWk[a] += ld * wi * Wr[b] * base;
-                lWr[b] += ld * wi * Wk[a] * base;
-            }
-        }
-        lam[6 * n + i] += l_w;
-        lam[5 * n + i] += (lWk[1] - lWk[0]) * B.idxi;
-        const double tt = (r - B.r[j]) * B.inv_h[j];
-        const double l_r = (tt > 0.0 && tt < 1.0) ? (lWr[1] - lWr[0]) * B.inv_h[j] : 0.0;
-        const double l_vx = l_vr * c - l_vt * sn, l_vy = l_vr * sn + l_vt * c;
-        const double l_c = l_vr * vx + l_vt * vy, l_s = l_vr * vy - l_vt * vx;
-        double lx = 0.0, ly = 0.0;
-        polar_back(r, c, sn, l_r, l_c, l_s, lx, ly);
-        lam[i] += lx;
-        lam[n + i] += ly;
-        double lp[3] = {l_vx / gam, l_vy / gam, l_vz / gam};
-        const double l_g = -(l_vx * PX + l_vy * PY + l_vz * PZ) / (gam * gam);
-        lp[0] += l_g * PX / gam;
-        lp[1] += l_g * PY / gam;
-        lp[2] += l_g * PZ / gam;
-        omvz_back(PX, PY, PZ, l_omvz, lp);
-        lam[2 * n + i] += lp[0];
-        lam[3 * n + i] += lp[1];
-        lam[4 * n + i] += lp[2];
+        for (int c = 0; c < 7; ++c) lam[c * n + i] = l7[c];
     }
 }
 
@@ -325,6 +337,7 @@ struct AdjSm {
     double *l_rhot, *l_drho, *l_jz, *l_chi, *l_jpi, *l_Sr, *l_Si;   // adjoints of the sources
     double *t0, *t1;                                // scratch
     double* tot;                                    // scan scratch (2 x 8 x kW)
+    int* flag;                                      // gate result broadcast
 };
 constexpr int kAdjArrays = 22;
 
@@ -336,7 +349,8 @@ __device__ __forceinline__ AdjSm carve_adj(double* p, int M) {
     for (int i = 0; i < kAdjArrays; ++i) { *a[i] = p; p += M; }
     S.t0 = p; p += M;
     S.t1 = p; p += M;
-    S.tot = p;
+    S.tot = p; p += 2 * 8 * kW;
+    S.flag = reinterpret_cast<int*>(p);
     return S;
 }
 
@@ -640,13 +654,19 @@ __device__ __forceinline__ double grad_T_at(const SweepArgs& A, const double* gm
     return v;
 }
 
-template <int ORD>
-__global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __grid_constant__ SweepArgs A,
-                                                                       const double* __restrict__ traj,
-                                                                       const double* __restrict__ fld,
-                                                                       const double* __restrict__ lfld,
-                                                                       double* __restrict__ lbsrc) {
-    extern __shared__ double smem_raw[];
+// the gate of a stand-alone reverse sweep: nothing to wait for
+struct AdjNoGate {
+    static constexpr bool kActive = false;
+    __device__ bool before_slice(int) { return true; }    // warp 0: the field adjoint of row k is final
+    __device__ void slice_done(int) {}                     // thread 0, after the barrier ending slice k
+};
+
+// One sweep in reverse by the calling CTA (all kSweepThreads threads): slices K-1 .. 0. The gate
+// orders it against the beam adjoint tasks when several steps run concurrently. Returns false when a
+// gate wait gave up.
+template <int ORD, class Gate>
+__device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ traj, const double* __restrict__ fld,
+                                const double* lfld, double* __restrict__ lbsrc, double* smem_raw, Gate& gate) {
     const int M = A.M, N = A.N, K = A.K, tid = threadIdx.x;
     const int np = A.np, npad = A.npad;
     const AdjSm S = carve_adj(smem_raw, M);
@@ -680,6 +700,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __gr
     if (has_p) species_params(A, tid, qsp, qmsp);
     int par = 0;
     for (int k = K - 1; k >= 0; --k) {
+        if (Gate::kActive) {                         // the field adjoint of row k is complete
+            if (tid < 32) {
+                const bool ok = gate.before_slice(k);
+                if (tid == 0) *S.flag = ok ? 1 : 0;
+            }
+            __syncthreads();
+            if (!*S.flag) return false;
+        }
         // ---- this slice's plasma state P_k, fields and field adjoints (store in reverse)
         PState<ORD> P;
         P.q = qsp; P.qm = qmsp;
@@ -703,11 +731,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __gr
             S.ez[i] = F[F_EZ0];
             S.bz[i] = F[F_BZ0];
             S.chi[i] = 0.0;
-            S.l_wpr[i] = LF[F_EP1R];
-            S.l_bpi[i] = LF[F_EP1R] + LF[F_BP1I];
-            S.l_bpr[i] = LF[F_BP1R] - LF[F_EP1I];
-            S.l_ez[i] = LF[F_EZ0];
-            S.l_bz[i] = LF[F_BZ0];
+            double lf[6];
+#pragma unroll
+            for (int c = 0; c < 6; ++c) lf[c] = beam_detail::fload<Gate::kActive>(LF + c);
+            S.l_wpr[i] = lf[F_EP1R];
+            S.l_bpi[i] = lf[F_EP1R] + lf[F_BP1I];
+            S.l_bpr[i] = lf[F_BP1R] - lf[F_EP1I];
+            S.l_ez[i] = lf[F_EZ0];
+            S.l_bz[i] = lf[F_BZ0];
             S.l_rhot[i] = S.l_drho[i] = S.l_jz[i] = S.l_chi[i] = S.l_jpi[i] = S.l_Sr[i] = S.l_Si[i] = 0.0;
         }
         __syncthreads();
@@ -850,7 +881,301 @@ __global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __gr
         if (alive) deposit_back<ORD>(S, A, P, Ln);
         L = Ln;
         __syncthreads();
+        if (Gate::kActive && tid == 0) gate.slice_done(k);   // beam-source adjoint rows > k are final
     }
+    return true;
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __grid_constant__ SweepArgs A,
+                                                                       const double* __restrict__ traj,
+                                                                       const double* __restrict__ fld,
+                                                                       const double* __restrict__ lfld,
+                                                                       double* __restrict__ lbsrc) {
+    extern __shared__ double smem_raw[];
+    AdjNoGate g;
+    sweep_back_body<ORD>(A, traj, fld, lfld, lbsrc, smem_raw, g);
+}
+
+// ------------------------------------------------------------------ the reverse pass as a pipeline
+// Every wait spins on an acquire load, bounded by %globaltimer: on time-out it records the place in
+// *err and returns, and every other wait gives up as soon as *err is set.
+__device__ __forceinline__ int ld_acquire(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+enum AdjWaitSite { AW_ROWS = 1, AW_TASK = 2 };
+
+// wait until *p <= v
+__device__ bool wait_le(const AdjPipeArgs& P, const int* p, int v, int site) {
+    if (ld_acquire(p) <= v) return true;
+    const unsigned long long t0 = gtimer();
+    for (;;) {
+        __nanosleep(64);
+        if (ld_acquire(p) <= v) return true;
+        if (ld_acquire(P.err) != 0) return false;
+        if (gtimer() - t0 > P.timeout_ns) {
+            atomicCAS(P.err, 0, (site << 8) | 1);
+            return false;
+        }
+    }
+}
+
+struct AdjGateState {
+    int n;          // step of this reverse sweep
+    int cursor;     // buckets [cursor, nbk) are known to have finished their task of step n
+};
+
+struct AdjPipeGate {
+    static constexpr bool kActive = true;
+    const AdjPipeArgs* P;
+    AdjGateState* g;    // shared
+    // warp 0: every bucket that can add to the field adjoint of row k has finished its push of step n
+    // in reverse. Those are the buckets from the first whose running maximum of (highest cell + 1)
+    // reaches k; they finish from the tail, so the lanes walk 32 buckets at a time downwards.
+    __device__ bool before_slice(int k) {
+        const int lane = threadIdx.x & 31;
+        const int n = g->n, nbk = P->nbk;
+        const int* pm = P->pmax + (size_t)n * nbk;
+        int lo = 0, hi = nbk;                                 // first b with pm[b] >= k
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (__ldg(pm + mid) >= k) hi = mid; else lo = mid + 1;
+        }
+        const int need = lo;
+        int c = g->cursor;
+        while (c > need) {
+            const int b = c - 1 - lane;
+            const bool done = b < need || ld_acquire(P->bdone + b) <= n;
+            const unsigned m = __ballot_sync(0xffffffffu, done);
+            const int run = (m == 0xffffffffu) ? 32 : __ffs(~m) - 1;
+            c = max(c - run, need);
+            if (run == 32 || c <= need) continue;
+            bool ok = true;
+            if (lane == 0) ok = wait_le(*P, P->bdone + (c - 1), n, AW_ROWS);
+            if (!__shfl_sync(0xffffffffu, ok ? 1 : 0, 0)) return false;
+        }
+        __syncwarp();
+        if (lane == 0) g->cursor = c;
+        __syncwarp();
+        return ld_acquire(P->err) == 0;
+    }
+    // thread 0 after the barrier ending slice k: the beam-source adjoint rows > k are final
+    __device__ void slice_done(int k) {
+        __threadfence();
+        st_release(P->prog + g->n, k);
+    }
+};
+
+template <int ORD>
+__device__ void adj_sweep_role(const AdjPipeArgs& P, double* smem) {
+    __shared__ AdjGateState gs;
+    const int T = P.nsteps;
+    for (int l = blockIdx.x; l < T; l += P.nsweep) {
+        const int n = T - 1 - l;
+        if (threadIdx.x == 0) {
+            gs.n = n;
+            gs.cursor = P.nbk;
+        }
+        __syncthreads();
+        AdjPipeGate g{&P, &gs};
+        if (!sweep_back_body<ORD>(P.sw, P.traj + (size_t)n * P.traj_slot, P.fld + (size_t)n * P.fld_slot,
+                                  P.lfld + (size_t)n * P.lfld_slot, P.lbsrc + (size_t)n * P.lbsrc_slot, smem, g))
+            return;
+        __syncthreads();
+    }
+}
+
+// task (layer l, bucket b), step n = nsteps - 1 - l: bucket b finished step n + 1, and the beam-source
+// adjoint of step n + 1 is final on the bucket's rows there
+__device__ __forceinline__ bool adj_task_ready(const AdjPipeArgs& P, int l, int b) {
+    const int T = P.nsteps, n = T - 1 - l;
+    if (n + 1 <= T - 1) {
+        if (ld_acquire(P.bdone + b) > n + 1) return false;
+        const int cm = __ldg(P.cmin + (size_t)(n + 1) * P.nbk + b);
+        if (cm != 0x7fffffff && ld_acquire(P.prog + n + 1) > max(max(cm, 0) - 1, 0)) return false;
+    }
+    return true;
+}
+
+// warp-collective: claim a ready task, lowest layer first (tail buckets first within a layer)
+__device__ __forceinline__ bool adj_claim(const AdjPipeArgs& P, int& l, int& b) {
+    const int lane = threadIdx.x & 31;
+    const int last = P.nsteps;                                 // layers 0 .. nsteps
+    const unsigned long long t0 = gtimer();
+    unsigned sleep_ns = 64;
+    for (;;) {
+        if (ld_acquire(P.err) != 0) return false;
+        const int lo = __shfl_sync(0xffffffffu, lane == 0 ? ld_acquire(P.lo) : 0, 0);
+        if (lo > last) return false;
+        for (int base = lo; base <= last; base += 32) {
+            const int m = base + lane;
+            int idx = P.nbk;
+            bool ready = false;
+            if (m <= last) {
+                idx = ld_acquire(P.next + m);
+                if (idx < P.nbk) ready = adj_task_ready(P, m, P.nbk - 1 - idx);
+            }
+            const unsigned full = __ballot_sync(0xffffffffu, idx >= P.nbk);
+            if (base == lo && (full & 1u)) {
+                const int c = (~full == 0u) ? 32 : __ffs(~full) - 1;
+                if (lane == 0) atomicMax(P.lo, base + c);
+            }
+            unsigned rm = __ballot_sync(0xffffffffu, ready);
+            const int rot = (int)((blockIdx.x * (kSweepThreads / 32) + (threadIdx.x >> 5)) & 31);
+            while (rm) {
+                const unsigned hi = rm >> rot, low = rm & ((1u << rot) - 1u);
+                const int src = hi ? rot + __ffs(hi) - 1 : __ffs(low) - 1;
+                int got = 0;
+                if (lane == src) got = atomicCAS(P.next + m, idx, idx + 1) == idx ? 1 : 0;
+                if (__shfl_sync(0xffffffffu, got, src)) {
+                    l = base + src;
+                    b = P.nbk - 1 - __shfl_sync(0xffffffffu, idx, src);
+                    return true;
+                }
+                rm &= ~(1u << src);
+            }
+        }
+        __nanosleep(sleep_ns);
+        sleep_ns = min(2 * sleep_ns, 8192u);
+        if (gtimer() - t0 > P.timeout_ns) {
+            if (lane == 0) atomicCAS(P.err, 0, (AW_TASK << 8) | 1);
+            return false;
+        }
+    }
+}
+
+__device__ __forceinline__ void beam_at(BeamArgs& B, const AdjPipeArgs& P, int bb, int step) {
+    const double* d = P.snap + (size_t)step * P.snap_step + P.snap_off[bb];
+    const long n = B.n;
+    B.x = const_cast<double*>(d); B.y = B.x + n; B.px = B.x + 2 * n; B.py = B.x + 3 * n; B.pz = B.x + 4 * n;
+    B.xi = B.x + 5 * n; B.w = B.x + 6 * n;
+}
+
+__device__ void adj_worker_role(const AdjPipeArgs& P, double* smem) {
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int M = P.sw.M, N = P.sw.N;
+    double* r = smem;
+    double* ih = r + M;
+    double* iV = ih + M;
+    for (int j = tid; j < M; j += kSweepThreads) {
+        r[j] = P.sw.r[j];
+        iV[j] = P.sw.inv_V[j];
+        if (j < N) ih[j] = P.sw.inv_h[j];
+    }
+    __syncthreads();
+    const int T = P.nsteps;
+    int l, b;
+    while (adj_claim(P, l, b)) {
+        const int n = T - 1 - l;
+        const int bb = __ldg(P.bk_beam + b);
+        const long i0 = __ldg(P.bk_start + b), i1 = __ldg(P.bk_end + b);
+        BeamArgs B1 = P.beam[bb], B0 = P.beam[bb];
+        B1.r = B0.r = r;
+        B1.inv_h = B0.inv_h = ih;
+        B1.inv_V = B0.inv_V = iV;
+        if (n + 1 <= T - 1) beam_at(B1, P, bb, n + 1);
+        if (n >= 0) beam_at(B0, P, bb, n);
+        const long nn = B0.n;
+        double* lam = P.lam + P.lam_off[bb];
+        const double* lb1 = P.lbsrc + (size_t)(n + 1) * P.lbsrc_slot;
+        const double* fld = P.fld + (size_t)(n >= 0 ? n : 0) * P.fld_slot;
+        double* lfld = P.lfld + (size_t)(n >= 0 ? n : 0) * P.lfld_slot;
+        const int startup = (n == 0 && P.startup[bb]) ? 1 : 0;
+        const bool rigid = P.rigid[bb] != 0;
+        for (long i = i0 + lane; i < i1; i += 32) {
+            double l7[7];
+#pragma unroll
+            for (int c = 0; c < 7; ++c) l7[c] = __ldcg(lam + c * nn + i);
+            if (n + 1 <= T - 1) deposit_back_one<true>(B1, lb1, i, l7);
+            if (n >= 0 && !rigid) push_back_one(B0, fld, i, l7, lfld, P.dt, P.dt, startup);
+#pragma unroll
+            for (int c = 0; c < 7; ++c) __stcg(lam + c * nn + i, l7[c]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence();
+            st_release(P.bdone + b, n);
+        }
+        __syncwarp();
+    }
+}
+
+template <int ORD>
+__global__ void __launch_bounds__(kSweepThreads, 1) adjoint_pipeline_kernel(const __grid_constant__ AdjPipeArgs P) {
+    extern __shared__ double smem_raw[];
+    if ((int)blockIdx.x < P.nsweep)
+        adj_sweep_role<ORD>(P, smem_raw);
+    else
+        adj_worker_role(P, smem_raw);
+}
+
+// lowest / highest live xi cell of bucket b at step n, from the snapshots (one warp per (n, b))
+__global__ void bucket_cells_kernel(const __grid_constant__ AdjPipeArgs P, int* __restrict__ cmin,
+                                    int* __restrict__ cmax) {
+    const int lane = threadIdx.x & 31;
+    const long w = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const long total = (long)(P.nsteps + 1) * P.nbk;
+    if (w >= total) return;
+    const int n = (int)(w / P.nbk), b = (int)(w % P.nbk);
+    const int bb = P.bk_beam[b];
+    BeamArgs B = P.beam[bb];
+    beam_at(B, P, bb, n);
+    int lo = 0x7fffffff, hi = -2;
+    for (long i = P.bk_start[b] + lane; i < P.bk_end[b]; i += 32) {
+        if (B.w[i] == 0.0) continue;
+        const int c = beam_detail::xi_cell(B, B.xi[i]);
+        lo = min(lo, c);
+        hi = max(hi, c);
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        lo = min(lo, __shfl_xor_sync(0xffffffffu, lo, o));
+        hi = max(hi, __shfl_xor_sync(0xffffffffu, hi, o));
+    }
+    if (lane == 0) {
+        cmin[w] = lo;
+        cmax[w] = hi;
+    }
+}
+
+// per step: pmax[b] = max over b' <= b of (cmax + 1) (a serial scan per step: nbk is a few thousand)
+__global__ void bucket_pmax_kernel(const __grid_constant__ AdjPipeArgs P, const int* __restrict__ cmax,
+                                   int* __restrict__ pmax) {
+    const int n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= P.nsteps) return;
+    int m = -1;
+    for (int b = 0; b < P.nbk; ++b) {
+        m = max(m, cmax[(size_t)n * P.nbk + b] + 1);
+        pmax[(size_t)n * P.nbk + b] = m;
+    }
+}
+
+template <int ORD>
+cudaError_t launch_adj_pipe_t(const AdjPipeArgs& P, int grid, size_t smem, cudaStream_t st) {
+    auto fn = adjoint_pipeline_kernel<ORD>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    void* args[] = {(void*)&P};
+    return cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(kSweepThreads), args, smem, st);
+}
+
+template <int ORD>
+int adj_pipe_occupancy_t(size_t smem) {
+    auto fn = adjoint_pipeline_kernel<ORD>;
+    if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, smem) != cudaSuccess) return 0;
+    return nb;
 }
 
 template <int ORD>
@@ -866,7 +1191,7 @@ cudaError_t launch_sweep_back_t(const SweepArgs& A, const double* traj, const do
 }  // namespace adj
 
 size_t adjoint_sweep_smem_bytes(int M) {
-    return sizeof(double) * ((size_t)(adj::kAdjArrays + 2) * M + 2 * 8 * (kSweepThreads / 32));
+    return sizeof(double) * ((size_t)(adj::kAdjArrays + 2) * M + 2 * 8 * (kSweepThreads / 32)) + 16;
 }
 
 cudaError_t launch_sweep_back(const SweepArgs& A, const double* traj, const double* fld, const double* lfld,
@@ -880,6 +1205,55 @@ cudaError_t launch_sweep_back(const SweepArgs& A, const double* traj, const doub
         case 5: return adj::launch_sweep_back_t<5>(A, traj, fld, lfld, lbsrc, st);
         default: return cudaErrorInvalidValue;
     }
+}
+
+size_t adjoint_pipeline_smem_bytes(int M) {
+    const size_t worker = sizeof(double) * 3 * (size_t)M + 64;
+    const size_t sweep = adjoint_sweep_smem_bytes(M);
+    return sweep > worker ? sweep : worker;
+}
+
+int adjoint_pipeline_max_grid(const AdjPipeArgs& P, int* sms) {
+    int dev = 0, nsm = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+    if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
+    *sms = nsm;
+    const size_t smem = adjoint_pipeline_smem_bytes(P.sw.M);
+    int per = 0;
+    switch (P.sw.ord) {
+        case 1: per = adj::adj_pipe_occupancy_t<1>(smem); break;
+        case 2: per = adj::adj_pipe_occupancy_t<2>(smem); break;
+        case 3: per = adj::adj_pipe_occupancy_t<3>(smem); break;
+        case 4: per = adj::adj_pipe_occupancy_t<4>(smem); break;
+        case 5: per = adj::adj_pipe_occupancy_t<5>(smem); break;
+        default: return 0;
+    }
+    return per * nsm;
+}
+
+cudaError_t launch_adjoint_pipeline(const AdjPipeArgs& P, int grid, cudaStream_t st) {
+    if (P.sw.M > kSweepThreads || P.sw.np > kSweepThreads || P.nsweep < 1 || grid <= P.nsweep ||
+        P.nbeams > kMaxBeams || P.nsteps < 1)
+        return cudaErrorInvalidValue;
+    const size_t smem = adjoint_pipeline_smem_bytes(P.sw.M);
+    switch (P.sw.ord) {
+        case 1: return adj::launch_adj_pipe_t<1>(P, grid, smem, st);
+        case 2: return adj::launch_adj_pipe_t<2>(P, grid, smem, st);
+        case 3: return adj::launch_adj_pipe_t<3>(P, grid, smem, st);
+        case 4: return adj::launch_adj_pipe_t<4>(P, grid, smem, st);
+        case 5: return adj::launch_adj_pipe_t<5>(P, grid, smem, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t launch_bucket_cells(const AdjPipeArgs& P, int* cmin, int* cmax, int* pmax, cudaStream_t st) {
+    if (P.nbk <= 0) return cudaSuccess;
+    const long warps = (long)(P.nsteps + 1) * P.nbk;
+    adj::bucket_cells_kernel<<<(unsigned)((warps * 32 + 255) / 256), 256, 0, st>>>(P, cmin, cmax);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    adj::bucket_pmax_kernel<<<(P.nsteps + 63) / 64, 64, 0, st>>>(P, cmax, pmax);
+    return cudaGetLastError();
 }
 
 static int beam_grid(long n) {

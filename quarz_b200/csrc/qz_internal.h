@@ -137,6 +137,14 @@ struct PipeArgs {
     int* err;                       // != 0: a wait gave up, (site << 8) | 1 (0)
     int* lo;                        // steps below *lo have every task claimed (0)
     unsigned long long timeout_ns;  // limit of every wait
+    // optional, for the adjoint (m = 0): the plasma trajectory of every sweep (slot per step, see
+    // SweepArgs::traj) and the beams of every step before its push (snap + n * snap_step + snap_off[beam],
+    // 7 columns of the beam's n, the run's particle order); with them the rings hold every step
+    double* traj;
+    size_t traj_slot;
+    double* snap;
+    size_t snap_step;
+    long snap_off[kMaxBeams];
     unsigned long long* trace;      // optional, kTraceStride per step: %globaltimer at the start and end of
                                     // sweep n, when it passed each 16th of the box, then its longest wait
                                     // for beam rows (ns, bucket, row, bucket's cmax); after the steps:
@@ -177,6 +185,42 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
 // CTA takes the next instance from a queue and runs all of it (Simulation::run: sweeps, moment sums,
 // pushes) with its own slot of field / beam-source buffers. Instances are queued largest first.
 constexpr int kBatchBeams = 2;
+
+// The reverse pass of a pipelined run in one cooperative launch (qz_adjoint.cu): reverse sweeps on
+// CTAs [0, nsweep) (step n on CTA (nsteps - 1 - n) % nsweep), warp workers elsewhere claiming layer
+// tasks (n, b) for n = nsteps-1 .. -1: the beam-deposit adjoint of step n + 1 and the push adjoint of
+// step n of bucket b. Inputs from the forward pipeline with recording: fields and trajectories of
+// every step, the beams of every step (snap).
+struct AdjPipeArgs {
+    SweepArgs sw;
+    int nsteps, nsweep;
+    const double* fld;  size_t fld_slot;      // forward fields, slot n = step n
+    const double* traj; size_t traj_slot;     // plasma trajectories, slot n
+    double* lfld;       size_t lfld_slot;     // field-store adjoint of step n (zero before the launch)
+    double* lbsrc;      size_t lbsrc_slot;    // beam-source adjoint of step n (zero before the launch)
+    int nbeams;
+    BeamArgs beam[kMaxBeams];                 // grid and box; the particle pointers are set per task
+    int rigid[kMaxBeams], startup[kMaxBeams];
+    const double* snap; size_t snap_step; long snap_off[kMaxBeams];
+    double* lam; long lam_off[kMaxBeams];     // particle adjoint, 7 columns of n per beam (run order)
+    double dt;
+    int nbk;
+    const int *bk_beam, *bk_start, *bk_end;
+    const int* cmin;                          // [(nsteps + 1) * nbk] lowest live xi cell of bucket b at step n
+    const int* pmax;                          // [nsteps * nbk] max over buckets <= b of (highest cell + 1)
+    int* prog;                                // [nsteps] lowest slice finished by reverse sweep n (K)
+    int* bdone;                               // [nbk] lowest step whose task finished (nsteps; -1 at the end)
+    int* next;                                // [nsteps + 1] claimed tasks of layer l = nsteps - 1 - n (0)
+    int* err;                                 // (site << 8) | 1 when a wait gave up (0)
+    int* lo;                                  // layers below *lo have every task claimed (0)
+    unsigned long long timeout_ns;
+};
+size_t adjoint_pipeline_smem_bytes(int M);
+int adjoint_pipeline_max_grid(const AdjPipeArgs& P, int* sms);
+cudaError_t launch_adjoint_pipeline(const AdjPipeArgs& P, int grid, cudaStream_t stream);
+// per (step, bucket) the lowest and highest live xi cells of the snapshots (empty: INT_MAX / -2), and
+// per step < nsteps the running maximum over buckets of (highest + 1)
+cudaError_t launch_bucket_cells(const AdjPipeArgs& P, int* cmin, int* cmax, int* pmax, cudaStream_t stream);
 
 // beam adjoints (qz_adjoint.cu); lam: 7 columns of n (x y px py pz xi w)
 cudaError_t launch_sums_back(const BeamArgs& B, double gref, double xiref, const double* lamS, double* lam,

@@ -94,6 +94,7 @@ struct PipeGate {
     __device__ double* ps(const SweepArgs&) const { return g->ps; }
     __device__ double* bgs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot; }
     __device__ double* srcs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot + 3 * (size_t)P->sw.M; }
+    __device__ double* traj(const SweepArgs&) const { return P->traj ? P->traj + (size_t)g->n * P->traj_slot : nullptr; }
 
     // warp 0 (all 32 lanes): beam-source rows <= r are final. The lanes look at 32 buckets at once and
     // advance over the finished prefix; the first unfinished one is waited for (bounded).
@@ -332,6 +333,13 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 if (lane == c) mine = x;
             }
             if (lane < 17) P.pmom[((size_t)n * P.nbk + b) * 17 + lane] = mine;
+        }
+        if (push && P.snap) {                        // the bucket before its push (for the adjoint)
+            double* sn = P.snap + (size_t)n * P.snap_step + P.snap_off[bb];
+            const double* cols[7] = {Bb.x, Bb.y, Bb.px, Bb.py, Bb.pz, Bb.xi, Bb.w};
+#pragma unroll
+            for (int c = 0; c < 7; ++c)
+                for (long i = i0 + lane; i < i1; i += 32) __stcg(sn + (size_t)c * Bb.n + i, __ldcg(cols[c] + i));
         }
         int cmax = -2;
         if (!push) {

@@ -48,6 +48,7 @@ struct NoGate {
     __device__ double* ps(const SweepArgs& A) const { return A.ps; }
     __device__ double* srcs(const SweepArgs& A) const { return A.srcs; }
     __device__ double* bgs(const SweepArgs& A) const { return A.bgs; }
+    __device__ double* traj(const SweepArgs& A) const { return A.traj; }
 };
 
 // ---------------------------------------------------------------- block scans
@@ -868,8 +869,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     int scan_par = 0;                                            // alternates the scan scratch
     const double fc = A.flux_coef;
     for (int k = 0; k < K; ++k) {
-        if (A.traj) {                                  // the plasma state at the start of slice k
-            double* T = A.traj + (size_t)k * (6 + 5 * (size_t)ORD) * npad;
+        if (double* const trj = gate.traj(A)) {        // the plasma state at the start of slice k
+            double* T = trj + (size_t)k * (6 + 5 * (size_t)ORD) * npad;
             if (REG) {
                 if (tid < np) {
                     T[tid] = P.x; T[npad + tid] = P.y; T[2 * (size_t)npad + tid] = P.px;

@@ -5,7 +5,8 @@ Deck: the one of tests/test_oracle_adjoint.py (24 uniform cells, 71 slices, AB3,
 with 300 particles each, 2 steps) and a stretched-grid variant with 3 steps. Tolerances: every
 component of the particle adjoint 1e-8 relative L2 against the oracle (the forwards differ in the
 order of their deposit sums, about 1e-13); the profile and delay gradients 1e-5 relative against
-central differences with h = 1e-6 (their error is that of the differences)."""
+central differences with h = 1e-6 (their error is that of the differences). Both schedules: the
+pipelined passes (the default) and step by step."""
 import numpy as np
 import pytest
 
@@ -25,8 +26,9 @@ def _specs():
     return [spec, st]
 
 
+@pytest.mark.parametrize("pipelined", [True, False])
 @pytest.mark.parametrize("which", [0, 1])
-def test_adjoint_against_oracle(which):
+def test_adjoint_against_oracle(which, pipelined):
     spec = _specs()[which]
     beams = [Q.sample_beam(b) for b in spec.beams]
     T, dt = spec.steps, spec.dt
@@ -36,6 +38,7 @@ def test_adjoint_against_oracle(which):
     seeds[:, 16] = 0.0
     lam_ref, mom_ref = O.OracleSim(spec, beams=beams).adjoint(T, dt, seeds)
     sim = Q.Simulation(spec, beams=beams)
+    sim.set_schedule(pipelined)
     lam, mom, ms = sim.adjoint(T, dt, seeds)
     assert ms[0] > 0 and ms[1] > 0
     np.testing.assert_allclose(mom, mom_ref, rtol=1e-10, atol=1e-12 * np.abs(mom_ref).max())
