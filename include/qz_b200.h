@@ -225,6 +225,10 @@ qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, 
  * The sim ends at the last step, as after qz_sim_run. */
 qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
                          double* mom_host, double* ms2, void* stream);
+/* Clock cycles per phase of the run's sweeps (qz_sweep_timing of the sim's sweep): 16 counters,
+   accumulated by thread 0 of stand-alone sweeps while enabled; 0..8 the forward sweep's phases,
+   9..15 those of the step-by-step adjoint's reverse sweep. cycles16 may be NULL. */
+qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16);
 
 /* ------------------------------------------------------------------ batched independent runs
  * A parameter scan: many independent small runs (each its own grid, box, plasma and up to 2 beams,

@@ -280,6 +280,12 @@ class Simulation:
                                     _stream_ptr(stream)))
         return mom[:, :nb, :]
 
+    def timing(self, enable: bool = True) -> np.ndarray:
+        """qz_sim_timing: the 16 phase-cycle counters of the stand-alone sweeps; enables or disables them."""
+        out = (C.c_ulonglong * 16)()
+        check(lib().qz_sim_timing(self.h, 1 if enable else 0, out))
+        return np.array(list(out), dtype=np.uint64)
+
     def adjoint(self, nsteps: int, dt: float, lamS, stream=None):
         """qz_sim_adjoint: runs nsteps (step by step, keeping the beams of every step) and the reverse
         pass. lamS (nbeams, 17): the adjoint of the last step's moment sums. Returns (per beam its (n, 7)

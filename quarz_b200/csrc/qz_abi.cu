@@ -1375,6 +1375,7 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
         }
         // ---- reverse
         qzb::SweepArgs A = base;
+        if (s->sw->timing) A.timing = s->sw->d_tim;     // phase cycles (qz_sim_timing)
         A.traj = traj;
         A.bsrc = bsrc;
         A.fld = s->d_fld;
@@ -1404,7 +1405,9 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
                                     cudaMemcpyDeviceToHost, st));
         // leave the fields of the last step, as qz_sim_run does
         if ((status = deposit_all(snap + per * nsteps))) return status;
-        if ((status = qz_sweep_run(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, sv))) return status;
+        A.traj = nullptr;
+        A.timing = nullptr;
+        QZ_CUDA(qzb::launch_sweep_m0(A, st));
         QZ_CUDA(cudaStreamSynchronize(st));
         float t0 = 0, t1 = 0;
         QZ_CUDA(cudaEventElapsedTime(&t0, ev[0], ev[1]));
@@ -1419,6 +1422,11 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
     release();
     s->bsrc_valid = false;
     return status;
+}
+
+extern "C" qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sim_timing: null pointer");
+    return qz_sweep_timing(s->sw, enable, cycles16);
 }
 
 extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span,

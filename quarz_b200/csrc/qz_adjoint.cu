@@ -127,8 +127,13 @@ __global__ void sums_back_kernel(BeamArgs B, double gref, double xiref, const do
 
 // One push of particle i (start-up half kick when startup, gather, Vay, drift) in reverse. On entry
 // l7 is the adjoint after the push, on exit before it; the field adjoint is added to lfld (K, M, 6).
+// kAgg: instead of adding to lfld, return the 24 contributions (6 components x corners (k, j), (k, j+1),
+// (k+1, j), (k+1, j+1)) in g with key = k M + j (-1 when none), for a warp-aggregated update
+template <bool kAgg>
 __device__ void push_back_one(const BeamArgs& B, const double* __restrict__ fld, long i, double (&l7)[7],
-                              double* __restrict__ lfld, double dt_kick, double dt, int startup) {
+                              double* __restrict__ lfld, double dt_kick, double dt, int startup, double (&g)[24],
+                              int& key) {
+    key = -1;
     const int M = B.M, nloc = B.K;
     const double qm = B.q / B.m;
     const double xmin = B.xi_min, xmax = B.xi_min + (B.K - 1) * B.dxi;
@@ -211,19 +216,25 @@ __device__ void push_back_one(const BeamArgs& B, const double* __restrict__ fld,
     const double l_s = -lE.x * ei + lE.y * er - lB.x * bi + lB.y * br;
     const double lcomp[6] = {l_er, l_ei, l_br, l_bi, lE.z, lB.z};
     const int comp[6] = {F_EP1R, F_EP1I, F_BP1R, F_BP1I, F_EZ0, F_BZ0};
-    double* g00p = lfld + ((size_t)k * M + j) * F_NC0;
-    double* g01p = g00p + F_NC0;
-    double* g10p = lfld + ((size_t)k1 * M + j) * F_NC0;
-    double* g11p = g10p + F_NC0;
     double l_tk = 0.0, l_t = 0.0;
+    if (kAgg) key = k * M + j;
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
         const int cm = comp[q];
         const double l = lcomp[q];
-        atomicAdd(g00p + cm, l * (1.0 - tk) * (1.0 - t));
-        atomicAdd(g01p + cm, l * (1.0 - tk) * t);
-        atomicAdd(g10p + cm, l * tk * (1.0 - t));
-        atomicAdd(g11p + cm, l * tk * t);
+        if (kAgg) {
+            g[q * 4 + 0] = l * (1.0 - tk) * (1.0 - t);
+            g[q * 4 + 1] = l * (1.0 - tk) * t;
+            g[q * 4 + 2] = l * tk * (1.0 - t);
+            g[q * 4 + 3] = l * tk * t;
+        } else {
+            double* g00p = lfld + ((size_t)k * M + j) * F_NC0;
+            double* g10p = lfld + ((size_t)k1 * M + j) * F_NC0;
+            atomicAdd(g00p + cm, l * (1.0 - tk) * (1.0 - t));
+            atomicAdd(g00p + F_NC0 + cm, l * (1.0 - tk) * t);
+            atomicAdd(g10p + cm, l * tk * (1.0 - t));
+            atomicAdd(g10p + F_NC0 + cm, l * tk * t);
+        }
         l_tk += l * (((1.0 - t) * f10[cm] + t * f11[cm]) - ((1.0 - t) * f00[cm] + t * f01[cm]));
         l_t += l * ((1.0 - tk) * (f01[cm] - f00[cm]) + tk * (f11[cm] - f10[cm]));
     }
@@ -242,7 +253,9 @@ __global__ void push_back_kernel(BeamArgs B, const double* __restrict__ fld, dou
         double l7[7];
 #pragma unroll
         for (int c = 0; c < 7; ++c) l7[c] = lam[c * n + i];
-        push_back_one(B, fld, i, l7, lfld, dt_kick, dt, startup);
+        double g[24];
+        int key;
+        push_back_one<false>(B, fld, i, l7, lfld, dt_kick, dt, startup, g, key);
 #pragma unroll
         for (int c = 0; c < 7; ++c) lam[c * n + i] = l7[c];
     }
@@ -337,9 +350,11 @@ struct AdjSm {
     double *l_rhot, *l_drho, *l_jz, *l_chi, *l_jpi, *l_Sr, *l_Si;   // adjoints of the sources
     double *t0, *t1;                                // scratch
     double* tot;                                    // scan scratch (2 x 8 x kW)
+    double* lam;                                    // particle adjoints ((5 + 5 ord) x kSweepThreads)
     int* flag;                                      // gate result broadcast
 };
 constexpr int kAdjArrays = 22;
+constexpr int kMaxOrd = 5;                          // the particle adjoints' room: AB order up to 5
 
 __device__ __forceinline__ AdjSm carve_adj(double* p, int M) {
     AdjSm S;
@@ -350,6 +365,7 @@ __device__ __forceinline__ AdjSm carve_adj(double* p, int M) {
     S.t0 = p; p += M;
     S.t1 = p; p += M;
     S.tot = p; p += 2 * 8 * kW;
+    S.lam = p; p += (size_t)(5 + 5 * kMaxOrd) * kSweepThreads;
     S.flag = reinterpret_cast<int*>(p);
     return S;
 }
@@ -388,8 +404,11 @@ struct PAdj {
 // PlasmaSpecies::push (src/PlasmaSpecies.cpp:561-668) of one particle in reverse, with the forward's
 // history rotation (h[0] newest). L: adjoint after the push (in), before (out). Returns false when the
 // push removed the particle (no adjoint flows through it).
+// The field adjoints at the particle's nodes j, j+1 are returned in sc (W+, E_z, B_z, B_r, B_theta; node j
+// then j+1 each) with jc = j, for a warp-aggregated update by the caller.
 template <int ORD>
-__device__ bool push_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, bool first, PAdj<ORD>& L) {
+__device__ bool push_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, bool first, PAdj<ORD>& L,
+                          double (&sc)[10], int& jc) {
     const double qm = P.qm;
     const PGeo g = geometry(S.r, S.ih, A.N, A.R, P.x, P.y);
     const double R1 = lin(S.wpr, g), Ez = lin(S.ez, g), Bz = lin(S.bz, g);
@@ -505,16 +524,19 @@ __device__ bool push_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>&
     lin_back(g, S.bz, l_Bz, S.l_bz, ga, adr, val, na);
     lin_back(g, S.bpr, l_Bx * g.c + l_By * g.s, S.l_bpr, ga, adr, val, na);
     lin_back(g, S.bpi, -l_Bx * g.s + l_By * g.c, S.l_bpi, ga, adr, val, na);
-    add_multi<10>(adr, val);
+#pragma unroll
+    for (int c = 0; c < 10; ++c) sc[c] = val[c];
+    jc = g.j;
     geo_back(S, g, ga, l_X, l_Y);
     L.x = l_X; L.y = l_Y; L.px = l_PX; L.py = l_PY; L.dl = l_D;
     return true;
 }
 
 // PlasmaSpecies::deposit_S (src/PlasmaSpecies.cpp:508-559, m = 0) of one particle in reverse:
-// L += state adjoint; the field adjoints (W+, E_z, B_z) go to shared memory
+// L += state adjoint; the field adjoints (W+, E_z, B_z at nodes j, j+1) are returned in sc, jc = j
 template <int ORD>
-__device__ void S_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, PAdj<ORD>& L) {
+__device__ void S_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, double (&L)[5], double (&sc)[6],
+                       int& jc) {
     const double q0 = P.q, qm = P.qm;
     const PGeo g = geometry(S.r, S.ih, A.N, A.R, P.x, P.y);
     const double R1 = lin(S.wpr, g), Ez = lin(S.ez, g), Bz = lin(S.bz, g);
@@ -591,18 +613,18 @@ __device__ void S_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P,
     lin_back(g, S.wpr, l_Wx * g.c + l_Wy * g.s, S.l_wpr, ga, adr, val, na);
     lin_back(g, S.ez, l_Ez, S.l_ez, ga, adr, val, na);
     lin_back(g, S.bz, l_Bz, S.l_bz, ga, adr, val, na);
-    double* adr6[6] = {adr[0], adr[1], adr[2], adr[3], adr[4], adr[5]};
-    const double val6[6] = {val[0], val[1], val[2], val[3], val[4], val[5]};
-    add_multi<6>(adr6, val6);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) sc[c] = val[c];
+    jc = g.j;
     double lx = 0.0, ly = 0.0;
     geo_back(S, g, ga, lx, ly);
-    L.x += lx; L.y += ly; L.px += l_PX; L.py += l_PY; L.dl += l_D;
+    L[0] += lx; L[1] += ly; L[2] += l_PX; L[3] += l_PY; L[4] += l_D;
 }
 
 // PlasmaSpecies::deposit (src/PlasmaSpecies.cpp:409-478, m = 0) of one particle in reverse, from the
 // source adjoints (rho and the densities feed nothing downstream; J_r is not used at m = 0)
 template <int ORD>
-__device__ void deposit_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, PAdj<ORD>& L) {
+__device__ void deposit_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P, double (&L)[5]) {
     const double q0 = P.q, qm = P.qm;
     const PGeo g = geometry(S.r, S.ih, A.N, A.R, P.x, P.y);
     const double PX = P.px, PY = P.py, D = P.dl;
@@ -637,7 +659,7 @@ __device__ void deposit_back(const AdjSm& S, const SweepArgs& A, const PState<OR
     l_D -= l_invd * invd * invd;
     double lx = 0.0, ly = 0.0;
     geo_back(S, g, ga, lx, ly);
-    L.x += lx; L.y += ly; L.px += l_PX; L.py += l_PY; L.dl += l_D;
+    L[0] += lx; L[1] += ly; L[2] += l_PX; L[3] += l_PY; L[4] += l_D;
 }
 
 // lam_f[j] of f -> grad f (src/FieldSolver.cpp:263-281) transposed, gathered at node j from l (shared)
@@ -675,7 +697,7 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
     const double *l0r = q + 4 * M, *l0f = q + 5 * M, *l0b = q + 6 * M;
     const double *l1a = q + 7 * M, *l1b = q + 8 * M, *l1c = q + 9 * M;
     const double *lfa = q + 10 * M, *lfb = q + 11 * M, *lfc = q + 12 * M;
-    const int i = tid;                               // this thread's row
+    const int i = tid, lane = tid & 31;              // this thread's row
     const bool row = i < M;
     if (row) {
         S.r[i] = A.r[i];
@@ -683,22 +705,55 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
         S.ih[i] = i < N ? A.inv_h[i] : 0.0;
     }
     __syncthreads();
+    // this thread's row constants: the symmetrisers F = r_j dV_j of L1D / L1F (dV_N = h_{N-1} / 2) and
+    // V_j of L0, with their reciprocals (no divide inside the slice loop)
+    double F1i = 1.0, iF1i = 1.0, Vi = 1.0, iVi = 1.0;
     if (row) {
         const double hm = i > 0 ? A.r[i] - A.r[i - 1] : 0.0, hp = i < N ? A.r[i + 1] - A.r[i] : 0.0;
-        S.F1[i] = A.r[i] * 0.5 * (hm + hp);          // r_j dV_j (dV_N = h_{N-1} / 2)
+        F1i = A.r[i] * 0.5 * (hm + hp);
+        iF1i = F1i > 0.0 ? 1.0 / F1i : 0.0;
+        iVi = A.inv_V[i];
+        Vi = 1.0 / iVi;
+        S.F1[i] = F1i;
     }
     const size_t nv = 6 + 5 * (size_t)ORD;
     const double fcoef = A.flux_coef;
-    PAdj<ORD> L;                                     // adjoint of this thread's particle after slice k
-    L.x = L.y = L.px = L.py = L.dl = 0.0;
+    // the adjoint of this thread's particle, carried from slice k + 1 to slice k: shared memory, so
+    // that no particle value stays in registers across the block scans
+    constexpr int NL = 5 + 5 * ORD;
+    double* Lsm = S.lam;                             // (NL, kSweepThreads)
 #pragma unroll
-    for (int m = 0; m < ORD; ++m)
-#pragma unroll
-        for (int v = 0; v < 5; ++v) L.h[m][v] = 0.0;
+    for (int v = 0; v < NL; ++v) Lsm[v * kSweepThreads + tid] = 0.0;
     const bool has_p = tid < np;
     double qsp = -1.0, qmsp = -1.0;
     if (has_p) species_params(A, tid, qsp, qmsp);
     int par = 0;
+    unsigned long long* tim = A.timing;              // optional: clock cycles per phase, slots 9..15
+    long long t_prev = (tim && tid == 0) ? clock64() : 0;
+#define ADJ_MARK(ph)                                                          \
+    do {                                                                      \
+        if (tim && tid == 0) {                                                \
+            const long long tn = clock64();                                   \
+            tim[9 + (ph)] += (unsigned long long)(tn - t_prev);               \
+            t_prev = tn;                                                      \
+        }                                                                     \
+    } while (0)
+    // this thread's particle P_k from the trajectory (the history only when asked)
+    auto load_p = [&](int k, PState<ORD>& P, bool hist) {
+        P.q = qsp; P.qm = qmsp;
+        P.w = 0.0;
+        P.x = P.y = P.px = P.py = 0.0;
+        P.dl = 1.0;
+        if (!has_p) return;
+        const double* T = traj + (size_t)k * nv * npad + tid;
+        P.x = T[0]; P.y = T[npad]; P.px = T[2 * (size_t)npad]; P.py = T[3 * (size_t)npad];
+        P.dl = T[4 * (size_t)npad]; P.w = T[5 * (size_t)npad];
+        if (hist)
+#pragma unroll
+            for (int m = 0; m < ORD; ++m)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) P.h[m][v] = T[(6 + (size_t)m * 5 + v) * npad];
+    };
     for (int k = K - 1; k >= 0; --k) {
         if (Gate::kActive) {                         // the field adjoint of row k is complete
             if (tid < 32) {
@@ -708,20 +763,10 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             __syncthreads();
             if (!*S.flag) return false;
         }
-        // ---- this slice's plasma state P_k, fields and field adjoints (store in reverse)
-        PState<ORD> P;
-        P.q = qsp; P.qm = qmsp;
-        P.w = 0.0;
-        if (has_p) {
-            const double* T = traj + (size_t)k * nv * npad + tid;
-            P.x = T[0]; P.y = T[npad]; P.px = T[2 * (size_t)npad]; P.py = T[3 * (size_t)npad];
-            P.dl = T[4 * (size_t)npad]; P.w = T[5 * (size_t)npad];
-#pragma unroll
-            for (int m = 0; m < ORD; ++m)
-#pragma unroll
-                for (int v = 0; v < 5; ++v) P.h[m][v] = T[(6 + (size_t)m * 5 + v) * npad];
-        }
-        const bool alive = has_p && P.w != 0.0;
+        // ---- this slice's fields and field adjoints (store in reverse)
+        bool alive = false;
+        if (has_p) alive = traj[(size_t)k * nv * npad + 5 * (size_t)npad + tid] != 0.0;
+        ADJ_MARK(0);
         if (row) {
             const double* F = fld + ((size_t)k * M + i) * F_NC0;
             const double* LF = lfld + ((size_t)k * M + i) * F_NC0;
@@ -742,25 +787,61 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             S.l_rhot[i] = S.l_drho[i] = S.l_jz[i] = S.l_chi[i] = S.l_jpi[i] = S.l_Sr[i] = S.l_Si[i] = 0.0;
         }
         __syncthreads();
-        // ---- chi of the slice (the plasma deposit of P_k) and the push of slice k in reverse
-        if (alive) {
-            const PGeo g = geometry(S.r, S.ih, N, A.R, P.x, P.y);
-            const double a0 = P.w * P.q * g.W0 * S.iv[g.j], a1 = P.w * P.q * g.W1 * S.iv[g.j + 1];
-            double* adr[2] = {S.chi + g.j, S.chi + g.j + 1};
-            const double val[2] = {a0 * P.qm / P.dl, a1 * P.qm / P.dl};
-            add_multi<2>(adr, val);
-        }
-        PAdj<ORD> Ln;                                 // adjoint of P_k being built
-        Ln.x = Ln.y = Ln.px = Ln.py = Ln.dl = 0.0;
+        // ---- chi of the slice (the plasma deposit of P_k) and the push of slice k in reverse; the
+        // shared-memory updates are summed over runs of lanes on the same node first (blowout piles
+        // many particles into a few sheath and axis cells)
+        {
+            PState<ORD> P;
+            load_p(k, P, k + 1 < K);
+            double cv[2] = {0.0, 0.0};
+            int key = -1 - lane;
+            if (alive) {
+                const PGeo g = geometry(S.r, S.ih, N, A.R, P.x, P.y);
+                cv[0] = P.w * P.q * g.W0 * S.iv[g.j] * P.qm / P.dl;
+                cv[1] = P.w * P.q * g.W1 * S.iv[g.j + 1] * P.qm / P.dl;
+                key = g.j;
+            }
+            if (warp_runs_sum<2>(key, cv) && key >= 0) {
+                double* adr[2] = {S.chi + key, S.chi + key + 1};
+                add_multi<2>(adr, cv);
+            }
+            PAdj<ORD> Lp;
+            bool kept = false;
+            double sc[10];
+            int jc = -1;
+            if (alive && k + 1 < K) {
+                Lp.x = Lsm[0 * kSweepThreads + tid]; Lp.y = Lsm[1 * kSweepThreads + tid];
+                Lp.px = Lsm[2 * kSweepThreads + tid]; Lp.py = Lsm[3 * kSweepThreads + tid];
+                Lp.dl = Lsm[4 * kSweepThreads + tid];
 #pragma unroll
-        for (int m = 0; m < ORD; ++m)
+                for (int m = 0; m < ORD; ++m)
 #pragma unroll
-            for (int v = 0; v < 5; ++v) Ln.h[m][v] = 0.0;
-        if (alive && k + 1 < K) {
-            PAdj<ORD> Lp = L;
-            if (push_back<ORD>(S, A, P, k == 0, Lp)) Ln = Lp;
+                    for (int v = 0; v < 5; ++v) Lp.h[m][v] = Lsm[(5 + m * 5 + v) * kSweepThreads + tid];
+                kept = push_back<ORD>(S, A, P, k == 0, Lp, sc, jc);
+            }
+            if (!kept) {
+#pragma unroll
+                for (int c = 0; c < 10; ++c) sc[c] = 0.0;
+            }
+            key = kept ? jc : -1 - lane;
+            if (warp_runs_sum<10>(key, sc) && key >= 0) {
+                double* adr[10] = {S.l_wpr + key, S.l_wpr + key + 1, S.l_ez + key, S.l_ez + key + 1, S.l_bz + key,
+                                   S.l_bz + key + 1, S.l_bpr + key, S.l_bpr + key + 1, S.l_bpi + key, S.l_bpi + key + 1};
+                add_multi<10>(adr, sc);
+            }
+            // the adjoint of P_k so far: the push's, or nothing
+            Lsm[0 * kSweepThreads + tid] = kept ? Lp.x : 0.0;
+            Lsm[1 * kSweepThreads + tid] = kept ? Lp.y : 0.0;
+            Lsm[2 * kSweepThreads + tid] = kept ? Lp.px : 0.0;
+            Lsm[3 * kSweepThreads + tid] = kept ? Lp.py : 0.0;
+            Lsm[4 * kSweepThreads + tid] = kept ? Lp.dl : 0.0;
+#pragma unroll
+            for (int m = 0; m < ORD; ++m)
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Lsm[(5 + m * 5 + v) * kSweepThreads + tid] = kept ? Lp.h[m][v] : 0.0;
         }
         __syncthreads();
+        ADJ_MARK(1);
         // ---- B+ (src/Simulation.cpp:535-591) in reverse: mu = F (L - chi)^-1 (F^-1 lam) per system
         {
             double m[2][4], ra[2], rbv[2], rc[2], rd[2];
@@ -772,9 +853,9 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             if (row) {
                 // sys 0: L1D - chi (rows 0, N Dirichlet); sys 1: L1F - chi (row 0 Dirichlet)
                 ra[0] = l1a[i]; rbv[0] = l1b[i]; rc[0] = i > 0 ? l1c[i - 1] : 0.0;
-                if (i >= 1 && i < N) { rbv[0] -= S.chi[i]; rd[0] = S.l_bpr[i] / S.F1[i]; }
+                if (i >= 1 && i < N) { rbv[0] -= S.chi[i]; rd[0] = S.l_bpr[i] * iF1i; }
                 ra[1] = lfa[i]; rbv[1] = lfb[i]; rc[1] = i > 0 ? lfc[i - 1] : 0.0;
-                if (i >= 1) { rbv[1] -= S.chi[i]; rd[1] = S.l_bpi[i] / S.F1[i]; }
+                if (i >= 1) { rbv[1] -= S.chi[i]; rd[1] = S.l_bpi[i] * iF1i; }
 #pragma unroll
                 for (int sy = 0; sy < 2; ++sy) {
                     m[sy][0] = rbv[sy]; m[sy][1] = -ra[sy] * rc[sy]; m[sy][2] = 1.0; m[sy][3] = 0.0;
@@ -806,8 +887,8 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             double xx[2];
             scan_bwd_n<2>(bA, bB, xx, S.tot + (par++ & 1) * 8 * kW);
             if (row) {
-                const double mu0 = (i >= 1 && i < N) ? fma(bA[0], xx[0], y[0]) * S.F1[i] : 0.0;
-                const double mu1 = (i >= 1) ? fma(bA[1], xx[1], y[1]) * S.F1[i] : 0.0;
+                const double mu0 = (i >= 1 && i < N) ? fma(bA[0], xx[0], y[0]) * F1i : 0.0;
+                const double mu1 = (i >= 1) ? fma(bA[1], xx[1], y[1]) * F1i : 0.0;
                 S.l_chi[i] = mu0 * S.bpr[i] + mu1 * S.bpi[i];
                 S.l_Si[i] = -mu0;
                 S.l_Sr[i] = mu1;                     // lam of the B_theta right-hand side (J_z' + S_r)
@@ -815,10 +896,30 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             }
         }
         __syncthreads();
+        ADJ_MARK(2);
         if (row) S.l_jz[i] = grad_T_at(A, gm, g0, gp, S.t0, i) - (i == N ? fcoef * S.t0[N] : 0.0);
         // ---- the S deposit in reverse (adds to lam of W+, E_z, B_z)
-        if (alive) S_back<ORD>(S, A, P, Ln);
+        {
+            double sc[6] = {0, 0, 0, 0, 0, 0};
+            int key = -1 - lane;
+            if (alive) {
+                PState<ORD> P;
+                load_p(k, P, false);
+                double l5[5] = {0, 0, 0, 0, 0};
+                int jc = 0;
+                S_back<ORD>(S, A, P, l5, sc, jc);
+                key = jc;
+#pragma unroll
+                for (int v = 0; v < 5; ++v) Lsm[v * kSweepThreads + tid] += l5[v];
+            }
+            if (warp_runs_sum<6>(key, sc) && key >= 0) {
+                double* adr[6] = {S.l_wpr + key, S.l_wpr + key + 1, S.l_ez + key, S.l_ez + key + 1, S.l_bz + key,
+                                  S.l_bz + key + 1};
+                add_multi<6>(adr, sc);
+            }
+        }
         __syncthreads();
+        ADJ_MARK(3);
         // ---- psi (W+ = -psi'), E_z, B_z: three L0 systems, mu = V L0^-1 (lam / V) on rows < N
         if (row) S.t1[i] = -S.l_wpr[i];
         __syncthreads();
@@ -828,10 +929,9 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             if (row) {
                 af = l0f[i]; rr = l0r[i]; ab = l0b[i];
                 if (i < N) {
-                    const double V = 1.0 / S.iv[i];
-                    d[0] = S.l_bz[i] / V;
-                    d[1] = grad_T_at(A, gm, g0, gp, S.t1, i) / V;     // lam of psi
-                    d[2] = S.l_ez[i] / V;
+                    d[0] = S.l_bz[i] * iVi;
+                    d[1] = grad_T_at(A, gm, g0, gp, S.t1, i) * iVi;   // lam of psi
+                    d[2] = S.l_ez[i] * iVi;
                 }
             }
             double cB[3];
@@ -847,9 +947,8 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             if (row) {
                 double mu[3] = {0.0, 0.0, 0.0};
                 if (i < N) {
-                    const double V = 1.0 / S.iv[i];
 #pragma unroll
-                    for (int e = 0; e < 3; ++e) mu[e] = fma(ab, xa[e], y[e]) * V;
+                    for (int e = 0; e < 3; ++e) mu[e] = fma(ab, xa[e], y[e]) * Vi;
                 }
                 S.t0[i] = -mu[0];                    // lam of the B_z right-hand side -(J_th' + J_th / r)
                 S.l_rhot[i] = -mu[1];
@@ -857,6 +956,7 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             }
         }
         __syncthreads();
+        ADJ_MARK(4);
         if (row) {
             // J_theta: (grad_odd + over_r)^T of t0, the adjoint of (grad_odd + over_r) J_theta
             double v = grad_T_at(A, gm, g0, gp, S.t0, i);
@@ -877,12 +977,21 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             }
         }
         __syncthreads();
+        ADJ_MARK(5);
         // ---- the plasma deposit of P_k in reverse
-        if (alive) deposit_back<ORD>(S, A, P, Ln);
-        L = Ln;
+        if (alive) {
+            PState<ORD> P;
+            load_p(k, P, false);
+            double l5[5] = {0, 0, 0, 0, 0};
+            deposit_back<ORD>(S, A, P, l5);
+#pragma unroll
+            for (int v = 0; v < 5; ++v) Lsm[v * kSweepThreads + tid] += l5[v];
+        }
         __syncthreads();
+        ADJ_MARK(6);
         if (Gate::kActive && tid == 0) gate.slice_done(k);   // beam-source adjoint rows > k are final
     }
+#undef ADJ_MARK
     return true;
 }
 
@@ -1092,14 +1201,39 @@ __device__ void adj_worker_role(const AdjPipeArgs& P, double* smem) {
         double* lfld = P.lfld + (size_t)(n >= 0 ? n : 0) * P.lfld_slot;
         const int startup = (n == 0 && P.startup[bb]) ? 1 : 0;
         const bool rigid = P.rigid[bb] != 0;
-        for (long i = i0 + lane; i < i1; i += 32) {
-            double l7[7];
+        // lanes in step over the bucket (runs of equal cells sum their field adjoints across the warp)
+        for (long base = i0; base < i1; base += 32) {
+            const long i = base + lane;
+            double g[24];
+            int key = -1;
+            if (i < i1) {
+                double l7[7];
 #pragma unroll
-            for (int c = 0; c < 7; ++c) l7[c] = __ldcg(lam + c * nn + i);
-            if (n + 1 <= T - 1) deposit_back_one<true>(B1, lb1, i, l7);
-            if (n >= 0 && !rigid) push_back_one(B0, fld, i, l7, lfld, P.dt, P.dt, startup);
+                for (int c = 0; c < 7; ++c) l7[c] = __ldcg(lam + c * nn + i);
+                if (n + 1 <= T - 1) deposit_back_one<true>(B1, lb1, i, l7);
+                if (n >= 0 && !rigid) push_back_one<true>(B0, fld, i, l7, lfld, P.dt, P.dt, startup, g, key);
 #pragma unroll
-            for (int c = 0; c < 7; ++c) __stcg(lam + c * nn + i, l7[c]);
+                for (int c = 0; c < 7; ++c) __stcg(lam + c * nn + i, l7[c]);
+            }
+            if (n >= 0 && !rigid) {
+                if (key < 0) {
+                    key = -1 - lane;
+#pragma unroll
+                    for (int c = 0; c < 24; ++c) g[c] = 0.0;
+                }
+                if (warp_runs_sum<24>(key, g) && key >= 0) {
+                    double* g0 = lfld + (size_t)key * F_NC0;             // (k, j); (k+1, j) is M rows on
+                    double* g1 = g0 + (size_t)M * F_NC0;
+                    const int comp[6] = {F_EP1R, F_EP1I, F_BP1R, F_BP1I, F_EZ0, F_BZ0};
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) {
+                        atomicAdd(g0 + comp[q], g[q * 4 + 0]);
+                        atomicAdd(g0 + F_NC0 + comp[q], g[q * 4 + 1]);
+                        atomicAdd(g1 + comp[q], g[q * 4 + 2]);
+                        atomicAdd(g1 + F_NC0 + comp[q], g[q * 4 + 3]);
+                    }
+                }
+            }
         }
         __syncwarp();
         if (lane == 0) {
@@ -1191,7 +1325,8 @@ cudaError_t launch_sweep_back_t(const SweepArgs& A, const double* traj, const do
 }  // namespace adj
 
 size_t adjoint_sweep_smem_bytes(int M) {
-    return sizeof(double) * ((size_t)(adj::kAdjArrays + 2) * M + 2 * 8 * (kSweepThreads / 32)) + 16;
+    return sizeof(double) * ((size_t)(adj::kAdjArrays + 2) * M + 2 * 8 * (kSweepThreads / 32) +
+                             (size_t)(5 + 5 * adj::kMaxOrd) * kSweepThreads) + 16;
 }
 
 cudaError_t launch_sweep_back(const SweepArgs& A, const double* traj, const double* fld, const double* lfld,
