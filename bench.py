@@ -344,14 +344,19 @@ def run_adjoint(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": _config(spec, nbt, T, {"objective": "witness mean energy gain",
                                              "parameters": "64 driver-profile bins + witness delay",
-                                             "adjoint": "step by step, beams of every step kept in HBM, "
-                                                        "sweep recomputed per step with its plasma trajectory"},
+                                             "adjoint": "pipelined forward recording the plasma trajectory and "
+                                                        "the beams of every step in HBM, then the pipelined "
+                                                        "reverse pass (reverse sweeps + beam adjoint tasks)"},
                               "adjoint"),
             "forward_ms": f_ms, "adjoint_ms": a_ms,
             "adjoint_split_ms": {"forward_keeping_beams": float(np.median([m[0] for m in split])),
                                  "reverse": float(np.median([m[1] for m in split]))},
             "gradient_norm_profile": float(np.linalg.norm(grads[0])), "gradient_delay": grads[1],
-            "clocks": clk.result(), "gpu_launches": None}
+            "clocks": clk.result(),
+            # per gradient: the forward run's own kernels (per beam: iota, cell keys, reorder, group starts,
+            # step-0 deposit; the pipeline, the moment reduction), the reverse pass's (bucket cells, running
+            # maximum, per beam the seed and the reorder back; the reverse pipeline)
+            "gpu_launches": args.steps * (OWN_LAUNCHES_PER_BEAM * len(beams) + OWN_LAUNCHES_PER_RUN + 3 + 2 * len(beams))}
 
 
 def oracle_rate(time_steps, warmup, spec):

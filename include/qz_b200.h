@@ -225,6 +225,13 @@ qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, 
  * The sim ends at the last step, as after qz_sim_run. */
 qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
                          double* mom_host, double* ms2, void* stream);
+/* The same with the seed computed from the forward's moment sums: after the forward, fn(moments
+   ((nsteps+1), nbeams, 17, host), nsteps, nbeams, lamS (nbeams x 17, to fill), user) is called once on
+   the calling thread -- for an objective such as the witness energy spread, whose linearisation
+   depends on the last step's sums, without a second forward run. */
+typedef void (*qz_adjoint_seed_fn)(const double* moments, int nsteps, int nbeams, double* lamS, void* user);
+qz_status qz_sim_adjoint_fn(qz_sim* s, int nsteps, double dt, qz_adjoint_seed_fn fn, void* user,
+                            double* const* lam_host, double* mom_host, double* ms2, void* stream);
 /* Clock cycles per phase of the run's sweeps (qz_sweep_timing of the sim's sweep): 16 counters,
    accumulated by thread 0 of stand-alone sweeps while enabled; 0..8 the forward sweep's phases,
    9..15 those of the step-by-step adjoint's reverse sweep. cycles16 may be NULL. */

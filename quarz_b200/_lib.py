@@ -83,6 +83,8 @@ SIGNATURES = {
     "qz_sim_trace": [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong), C.c_int, C.POINTER(C.c_int)],
     "qz_sim_run_host": [C.c_void_p, C.c_int, C.c_double, C.POINTER(C.c_void_p), _dp, C.c_void_p],
     "qz_sim_timing": [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)],
+    "qz_sim_adjoint_fn": [C.c_void_p, C.c_int, C.c_double, C.c_void_p, C.c_void_p, C.POINTER(C.c_void_p), _dp, _dp,
+                          C.c_void_p],
     "qz_sim_adjoint": [C.c_void_p, C.c_int, C.c_double, _dp, C.POINTER(C.c_void_p), _dp, _dp, C.c_void_p],
     "qz_batch_create": [C.POINTER(C.c_void_p)],
     "qz_batch_destroy": [C.c_void_p],

@@ -114,3 +114,68 @@ def profile_gradient(lam_driver: np.ndarray, sample: np.ndarray, prof: DriverPro
 def delay_gradient(lam_witness: np.ndarray) -> float:
     """dJ/d(delay) from the witness particles' adjoint (n, 7): internal xi moves by +1 per unit."""
     return float(np.sum(lam_witness[:, 5]))
+
+
+# ---------------------------------------------------------------------------- torch interface
+def _objective_and_gradient(spec, samples, prof: DriverProfile, f: np.ndarray, shift: float, which: str,
+                            stream=None):
+    """One forward run with the driver profile f and the witness shifted by `shift`, then the adjoint
+    (qz_sim_adjoint): (J, dJ/df (nbins), dJ/d(delay)). samples: [(rows, gref, xiref)] of driver and witness
+    as sampled (the profile and shift are applied here)."""
+    from .api import Simulation
+
+    (ds, dg, dx), (ws, wg, wx) = samples[0], samples[1]
+    beams = [(driver_rows(ds, prof, f), dg, dx), (witness_rows(ws, shift), wg, wx)] + list(samples[2:])
+    if which not in ("gain", "spread"):
+        raise ValueError("which must be 'gain' or 'spread'")
+    sim = Simulation(spec, beams=beams)
+    out = {}
+
+    def seed_fn(mom):                     # the linearisation at this run's last moment sums
+        S_last, S_first = mom[-1, 1], mom[0, 1]
+        out["J"] = gain(S_last, S_first, wg) if which == "gain" else spread(S_last)
+        seeds = np.zeros((len(beams), 17))
+        seeds[1] = gain_seed(S_last) if which == "gain" else spread_seed(S_last)
+        return seeds
+
+    lam, _, _ = sim.adjoint_fn(spec.steps, spec.dt, seed_fn, stream=stream)
+    J = out["J"]
+    # lam is dJ/d(rows as run); w_i = w_i^s f(xi_i) / f0(xi_i) is linear in f with the sampled xi
+    return J, profile_gradient(lam[0], ds, prof), delay_gradient(lam[1])
+
+
+class WitnessObjective:
+    """Witness energy gain or energy spread of a run as a differentiable function of the driver profile
+    (torch tensor of nbins nodal values) and the witness delay change (0-d tensor), for torch.autograd.
+
+        obj = WitnessObjective(spec, samples, prof, "gain")
+        J = obj(f, d)          # f: (64,) float64, d: () float64, both may require grad
+        J.backward()           # f.grad, d.grad from one adjoint run
+
+    The forward computes J and its gradient together (one adjoint run: its forward gives J and the
+    seed), and the backward scales the stored gradient by the incoming one."""
+
+    def __init__(self, spec, samples, prof: DriverProfile, which: str = "gain"):
+        self.spec, self.samples, self.prof, self.which = spec, samples, prof, which
+
+    def __call__(self, f, delay):
+        import torch
+
+        obj = self
+
+        class _Fn(torch.autograd.Function):
+            @staticmethod
+            def forward(ctx, f_t, d_t):
+                J, gf, gd = _objective_and_gradient(obj.spec, obj.samples, obj.prof,
+                                                    f_t.detach().cpu().numpy().astype(np.float64),
+                                                    float(d_t.detach().cpu()), obj.which)
+                ctx.save_for_backward(torch.as_tensor(gf, dtype=torch.float64, device=f_t.device),
+                                      torch.as_tensor(gd, dtype=torch.float64, device=d_t.device))
+                return torch.as_tensor(J, dtype=torch.float64, device=f_t.device)
+
+            @staticmethod
+            def backward(ctx, g):
+                gf, gd = ctx.saved_tensors
+                return g * gf, g * gd
+
+        return _Fn.apply(f, delay)

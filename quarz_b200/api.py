@@ -301,6 +301,33 @@ class Simulation:
                                    _stream_ptr(stream)))
         return [c.T.copy() for c in cols], mom[:, :nb, :], (float(ms[0]), float(ms[1]))
 
+    def adjoint_fn(self, nsteps: int, dt: float, seed_fn, stream=None):
+        """qz_sim_adjoint_fn: as adjoint(), with the seed computed after the forward by
+        seed_fn(moments ((nsteps+1), nbeams, 17)) -> (nbeams, 17)."""
+        nb = len(self.spec.beams)
+        SEED = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_double), C.c_void_p)
+        err = []
+
+        def _cb(mom_p, ns, nbm, out_p, _user):
+            try:
+                mom = np.ctypeslib.as_array(mom_p, shape=((ns + 1) * nbm * 17,)).reshape(ns + 1, nbm, 17).copy()
+                seeds = np.asarray(seed_fn(mom), dtype=np.float64).reshape(nbm * 17)
+                out = np.ctypeslib.as_array(out_p, shape=(nbm * 17,))
+                out[:] = seeds
+            except Exception as e:                      # a Python error must not unwind through C
+                err.append(e)
+
+        cb = SEED(_cb)
+        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nb)]
+        ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) for c in cols])
+        mom = np.zeros((nsteps + 1, max(nb, 1), 17))
+        ms = np.zeros(2)
+        check(lib().qz_sim_adjoint_fn(self.h, int(nsteps), float(dt), C.cast(cb, C.c_void_p), None, ptrs, _p(mom),
+                                      _p(ms), _stream_ptr(stream)))
+        if err:
+            raise err[0]
+        return [c.T.copy() for c in cols], mom[:, :nb, :], (float(ms[0]), float(ms[1]))
+
     def fields(self):
         K, M = self.spec.K, self.spec.M
         fld = np.zeros(K * M * self.fnc)

@@ -1104,10 +1104,23 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
 }
 
 namespace {
+// where the adjoint's seed comes from: given values, or a function of the forward's moment sums
+struct AdjSeed {
+    const double* fixed = nullptr;
+    qz_adjoint_seed_fn fn = nullptr;
+    void* user = nullptr;
+    // the seed (nb x 17) once the forward's moments (host, (nsteps+1, nb, 17)) are known
+    void values(const double* mom, int nsteps, int nb, std::vector<double>& out) const {
+        out.assign((size_t)17 * nb, 0.0);
+        if (fixed) std::copy(fixed, fixed + 17 * (size_t)nb, out.begin());
+        else fn(mom, nsteps, nb, out.data(), user);
+    }
+};
+
 // The adjoint with both passes pipelined: the forward pipeline records the trajectories and the beams
 // of every step (rings of one slot per step), the reverse pipeline runs the reverse sweeps of
 // consecutive steps concurrently with the beam adjoint tasks (qz_adjoint.cu).
-qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
+qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, double* const* lam_host,
                             double* mom_host, double* ms2, cudaStream_t st) {
     auto& P_ = s->pipe;
     const qzb::SweepArgs& base = s->sw->base;
@@ -1148,7 +1161,11 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const double* lamS
         rec.snap = snap;
         rec.snap_step = per;
         for (int b = 0; b < nb; ++b) rec.snap_off[b] = (long)(7 * off[b]);
-        if (qz_status e = run_pipelined(s, T, dt, mom_host, st, &rec)) return e;
+        std::vector<double> momv(mom_host ? 0 : (size_t)(T + 1) * nb * 17);
+        double* mom = mom_host ? mom_host : momv.data();
+        if (qz_status e = run_pipelined(s, T, dt, mom, st, &rec)) return e;     // (synchronises)
+        std::vector<double> seedv;
+        seed.values(mom, T, nb, seedv);
         for (int b = 0; b < nb; ++b)                   // the beams after the last push
             QZ_CUDA(cudaMemcpyAsync(snap + per * T + 7 * off[b], s->beams[b].d, sizeof(double) * 7 * s->beams[b].n,
                                     cudaMemcpyDeviceToDevice, st));
@@ -1210,7 +1227,7 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const double* lamS
         QZ_CUDA(cudaMemsetAsync(lfld, 0, sizeof(double) * KM * 6 * T, st));
         QZ_CUDA(cudaMemsetAsync(lbsrc, 0, sizeof(double) * KM * 5 * T, st));
         QZ_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * per, st));
-        QZ_CUDA(cudaMemcpyAsync(lamS, lamS_host, sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
+        QZ_CUDA(cudaMemcpyAsync(lamS, seedv.data(), sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
         for (int b = 0; b < nb; ++b) {
             qz_beam_view v = s->beams[b].view();
             double* d = snap + per * T + 7 * off[b];
@@ -1267,9 +1284,10 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const double* lamS
 // beams of every step on the device. Reverse, for n = nsteps-1 .. 0: the beam deposit and the sweep
 // of step n again (recording the plasma trajectory), the beam pushes in reverse (field-store
 // adjoint), the sweep in reverse (beam-source adjoint), the beam deposits in reverse.
-extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
-                                    double* mom_host, double* ms2, void* stream) {
-    if (!s || nsteps < 1 || !(dt > 0.0) || !lamS_host || (!s->beams.empty() && !lam_host))
+namespace {
+qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, double* const* lam_host,
+                      double* mom_host, double* ms2, void* stream) {
+    if (!s || nsteps < 1 || !(dt > 0.0) || (!seed.fixed && !seed.fn) || (!s->beams.empty() && !lam_host))
         return fail(QZ_ERR_ARG, "qz_sim_adjoint: bad argument");
     const qzb::SweepArgs& base = s->sw->base;
     if (s->p.modes != 0 || s->p.ngp || s->p.K < 2)
@@ -1284,7 +1302,7 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
     }
     cudaStream_t st = (cudaStream_t)stream;
     if (s->pipe.enabled && s->beams.size() <= (size_t)qzb::kMaxBeams)
-        return adjoint_pipelined(s, nsteps, dt, lamS_host, lam_host, mom_host, ms2, st);
+        return adjoint_pipelined(s, nsteps, dt, seed, lam_host, mom_host, ms2, st);
     void* sv = (void*)st;
     const int nb = (int)s->beams.size();
     for (auto& b : s->beams)                         // the caller's particle order
@@ -1304,6 +1322,8 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
         for (double* q : {snap, traj, lfld, lbsrc, lam, lamS})
             if (q) cudaFree(q);
     };
+    std::vector<double> momv(mom_host ? 0 : (size_t)(nsteps + 1) * nb * 17);
+    if (!mom_host) mom_host = momv.data();
     if (cudaMalloc((void**)&snap, sizeof(double) * (per * (nsteps + 1) + 1)) != cudaSuccess ||
         cudaMalloc((void**)&traj, sizeof(double) * (size_t)K * nv * base.npad) != cudaSuccess ||
         cudaMalloc((void**)&lfld, sizeof(double) * KM * 6) != cudaSuccess ||
@@ -1367,7 +1387,10 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
         QZ_CUDA(cudaEventRecord(ev[1], st));
         // ---- seed: the last step's moment sums
         QZ_CUDA(cudaMemsetAsync(lam, 0, sizeof(double) * per, st));
-        QZ_CUDA(cudaMemcpyAsync(lamS, lamS_host, sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
+        QZ_CUDA(cudaStreamSynchronize(st));              // the moments are on the host
+        std::vector<double> seedv;
+        seed.values(mom_host, nsteps, nb, seedv);
+        QZ_CUDA(cudaMemcpyAsync(lamS, seedv.data(), sizeof(double) * 17 * nb, cudaMemcpyHostToDevice, st));
         for (int b = 0; b < nb; ++b) {
             const qz_beam_view v = view_at(b, snap + per * nsteps);
             const qzb::BeamArgs BA = beam_args(s->g, &v, &box);
@@ -1422,6 +1445,23 @@ extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const doub
     release();
     s->bsrc_valid = false;
     return status;
+}
+
+}  // namespace
+
+extern "C" qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_host, double* const* lam_host,
+                                    double* mom_host, double* ms2, void* stream) {
+    AdjSeed seed;
+    seed.fixed = lamS_host;
+    return sim_adjoint(s, nsteps, dt, seed, lam_host, mom_host, ms2, stream);
+}
+
+extern "C" qz_status qz_sim_adjoint_fn(qz_sim* s, int nsteps, double dt, qz_adjoint_seed_fn fn, void* user,
+                                       double* const* lam_host, double* mom_host, double* ms2, void* stream) {
+    AdjSeed seed;
+    seed.fn = fn;
+    seed.user = user;
+    return sim_adjoint(s, nsteps, dt, seed, lam_host, mom_host, ms2, stream);
 }
 
 extern "C" qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16) {

@@ -83,3 +83,28 @@ def test_gain_and_spread_gradients_against_differences():
         h = 1e-6
         fd = (run(prof.f0, h)[k] - run(prof.f0, -h)[k]) / (2 * h)
         assert abs(fd - gd) <= 1e-5 * abs(fd), (k, "delay", fd, gd)
+
+
+def test_torch_function_matches_adjoint_and_differences():
+    import torch
+
+    spec = _specs()[0]
+    samples = [Q.sample_beam(b) for b in spec.beams]
+    drv = spec.beams[0]
+    prof = A.DriverProfile.gaussian(-drv.xi0_user, drv.sigma_xi, drv.cut, 64)
+    obj = A.WitnessObjective(spec, samples, prof, "gain")
+    f = torch.tensor(prof.f0, dtype=torch.float64, requires_grad=True)
+    d = torch.tensor(0.0, dtype=torch.float64, requires_grad=True)
+    J = obj(f, d)
+    (2.0 * J).backward()
+    h = 1e-6
+    Jp = float(obj(torch.tensor(prof.f0), torch.tensor(h)))
+    Jm = float(obj(torch.tensor(prof.f0), torch.tensor(-h)))
+    assert abs(float(d.grad) - 2.0 * (Jp - Jm) / (2 * h)) <= 1e-5 * abs(float(d.grad))
+    b = 32
+    fp, fm = prof.f0.copy(), prof.f0.copy()
+    fp[b] += h * prof.f0[b]
+    fm[b] -= h * prof.f0[b]
+    fd = (float(obj(torch.tensor(fp), torch.tensor(0.0))) - float(obj(torch.tensor(fm), torch.tensor(0.0)))) / (
+        2 * h * prof.f0[b])
+    assert abs(float(f.grad[b]) - 2.0 * fd) <= 1e-5 * abs(2.0 * fd)
