@@ -359,13 +359,27 @@ def run_adjoint(args, rank, world, local_rank):
             "gpu_launches": args.steps * (OWN_LAUNCHES_PER_BEAM * len(beams) + OWN_LAUNCHES_PER_RUN + 3 + 2 * len(beams))}
 
 
-def oracle_rate(time_steps, warmup, spec):
-    """The CPU oracle (serial restatement of the reference path) on the same workload: slice-solves/s
-    over time_steps full time steps (sweep + moment sums + push), after warm-up steps."""
+def _oracle_openmp():
+    """The oracle's timing build (per-particle loops on all host threads) and its thread count; the
+    serial build and 1 thread when the timing build cannot be made."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    O.build()
+    try:
+        O.build(omp=True)
+        O.use_openmp(True)
+        threads = int(os.environ.get("OMP_NUM_THREADS", "0") or 0) or (os.cpu_count() or 1)
+    except Exception:
+        O.build()
+        threads = 1
+    return O, threads
+
+
+def oracle_rate(time_steps, warmup, spec):
+    """The CPU oracle (restatement of the reference path) on the same workload, on all host threads:
+    slice-solves/s over time_steps full time steps (sweep + moment sums + push), after warm-up steps."""
+    O, threads = _oracle_openmp()
+    oracle_rate.threads = threads
     sim = O.OracleSim(spec)
     dt = spec.dt
     sim.step_fields(0.0)
@@ -391,10 +405,8 @@ def oracle_scan_rate(time_steps, warmup, modes=0):
 
     from quarz_b200 import workloads
 
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
-
-    O.build()
+    O, threads = _oracle_openmp()
+    oracle_scan_rate.threads = threads
     specs = workloads.scan_instances(512, seed=2024, modes=modes)
     idx = np.linspace(0, len(specs) - 1, max(1, time_steps)).astype(int)
     sim = O.OracleSim(specs[idx[0]])
@@ -442,9 +454,10 @@ def main():
                     "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                     "data": "synthetic", "config": {"workload": args.workload, "instances": 512, "time_steps_per_run": 20,
                                                     "beam_particles_per_run": 100000},
-                    "cpu_baseline": {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
+                    "cpu_baseline": {"value": rate, "unit": "runs/s", "cores": oracle_scan_rate.threads, "kind": "port",
                                      "sample": f"one full time step of each of {args.steps} instances sampled "
-                                               f"across the scan, serial oracle; a run = 21 such steps"},
+                                               f"across the scan, oracle on {oracle_scan_rate.threads} host "
+                                               f"threads; a run = 21 such steps"},
                     "e2e": {"value": rate, "unit": "runs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line))
             return
@@ -456,9 +469,10 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic", "config": _config(spec, nb, spec.steps, None, args.workload),
-                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+                "cpu_baseline": {"value": rate, "unit": UNIT, "cores": oracle_rate.threads, "kind": "port",
                                  "sample": f"{args.steps} full time steps of the workload (sweep + moment sums + "
-                                           f"beam push) after {args.warmup} warm-up steps, serial oracle"},
+                                           f"beam push) after {args.warmup} warm-up steps, oracle on "
+                                           f"{oracle_rate.threads} host threads"},
                 "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
         return
@@ -482,9 +496,11 @@ def main():
             torch.distributed.destroy_process_group()
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             rate, el = oracle_scan_rate(args.cpu_steps, 1, 1 if args.workload == "scan_m1" else 0)
-            line["cpu_baseline"] = {"value": rate, "unit": "runs/s", "cores": 1, "kind": "port",
+            line["cpu_baseline"] = {"value": rate, "unit": "runs/s", "cores": oracle_scan_rate.threads,
+                                    "kind": "port",
                                     "sample": f"one full time step of each of {args.cpu_steps} instances sampled "
-                                              f"across the scan, serial oracle, {el:.1f} s; a run = 21 such steps"}
+                                              f"across the scan, oracle on {oracle_scan_rate.threads} host threads, "
+                                              f"{el:.1f} s; a run = 21 such steps"}
         if rank == 0:
             print(json.dumps(line))
         return
@@ -521,9 +537,10 @@ def main():
                        "ms_per_step": e["ms_per_run"]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         rate, el = oracle_rate(args.cpu_steps, 1, spec)
-        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": 1, "kind": "port",
+        line["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": oracle_rate.threads, "kind": "port",
                                 "sample": f"{args.cpu_steps} full time steps of the same workload (sweep + moment "
-                                          f"sums + beam push), serial oracle, {el:.1f} s"}
+                                          f"sums + beam push), oracle on {oracle_rate.threads} host threads, "
+                                          f"{el:.1f} s"}
     if world > 1:
         import torch
 

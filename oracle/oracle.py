@@ -15,14 +15,17 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "build", "libqz_oracle.so")
+# the timing build: per-particle loops on all host threads (OpenMP), for the CPU baseline only; the
+# parity checks use the serial build, whose summation order is fixed
+OMP_LIB_PATH = os.path.join(HERE, "build", "libqz_oracle_omp.so")
 
 THOMAS, PCR, PARTITION = 0, 1, 2
 _METHODS = {"auto": THOMAS, "thomas": THOMAS, "pcr": PCR, "partition": PARTITION}
 
 
-def build() -> str:
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
-    return LIB_PATH
+def build(omp: bool = False) -> str:
+    subprocess.run(["make", "-s", "-C", HERE] + (["omp"] if omp else []), check=True)
+    return OMP_LIB_PATH if omp else LIB_PATH
 
 
 class _Params(C.Structure):
@@ -38,14 +41,24 @@ class _SpParams(C.Structure):
 
 
 _lib = None
+_use_omp = False
+
+
+def use_openmp(on: bool = True):
+    """Select the OpenMP timing build for every later call (before the first one)."""
+    global _use_omp
+    if _lib is not None and on != _use_omp:
+        raise RuntimeError("oracle library already loaded")
+    _use_omp = on
 
 
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB_PATH):
-            build()
-        L = C.CDLL(LIB_PATH)
+        path = OMP_LIB_PATH if _use_omp else LIB_PATH
+        if not os.path.exists(path):
+            build(_use_omp)
+        L = C.CDLL(path)
         dp = C.POINTER(C.c_double)
         L.qzo_sim_create.restype = C.c_void_p
         L.qzo_sim_create.argtypes = [C.POINTER(_Params), dp, C.c_int]

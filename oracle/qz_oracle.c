@@ -541,6 +541,17 @@ int qzo_ab_variable(int order, const double* t, double h, double* c) {
     return 0;
 }
 
+/* Timing build (the reference's OpenMP backend stand-in): compiled with -fopenmp, the per-particle
+   loops run on all host threads with atomic source updates; without it these expand to the serial
+   code, whose fixed summation order is the oracle's. */
+#ifdef _OPENMP
+#define QZO_ADD(x, v) do { _Pragma("omp atomic") (x) += (v); } while (0)
+#define QZO_PFOR _Pragma("omp parallel for schedule(static)")
+#else
+#define QZO_ADD(x, v) ((x) += (v))
+#define QZO_PFOR
+#endif
+
 /* ===================================================================== simulation */
 /* field / beam-source / diagnostic components (src/FieldStore.hpp:9-21, src/Simulation.hpp:44) */
 enum { F_EP1R = 0, F_EP1I, F_BP1R, F_BP1I, F_EZ0, F_BZ0, F_EP0R, F_EP0I, F_EP2R, F_EP2I, F_BP0R, F_BP0I, F_BP2R,
@@ -779,6 +790,7 @@ static void species_deposit(qzo_sim* s, const species_t* q) {
     const int m1 = s->m1;
     const double chif = 1.0;
     msc_t* dens = neg ? &s->ne : &s->ni;
+    QZO_PFOR
     for (int i = 0; i < q->Np; ++i) {
         const double wi = q->w[i];
         if (wi == 0.0) continue;
@@ -798,34 +810,34 @@ static void species_deposit(qzo_sim* s, const species_t* q) {
             const double dr = wq * ur * p.dW[cc] * iv;
             const double vjz = a * pz * invd, vchi = chif * a * qm * invd, vrho = a * gam * invd;
             const double vn = wi * p.W[cc] * iv * gam * invd;
-            s->rhot.a0[jj] += a;
-            s->drho.a0[jj] += dr;
-            s->jz.a0[jj] += vjz;
-            s->chi.a0[jj] += vchi;
-            s->rho.a0[jj] += vrho;
-            dens->a0[jj] += vn;
-            s->jp.r1[jj] += a * ur;
-            s->jp.i1[jj] += a * uth;
+            QZO_ADD(s->rhot.a0[jj], a);
+            QZO_ADD(s->drho.a0[jj], dr);
+            QZO_ADD(s->jz.a0[jj], vjz);
+            QZO_ADD(s->chi.a0[jj], vchi);
+            QZO_ADD(s->rho.a0[jj], vrho);
+            QZO_ADD(dens->a0[jj], vn);
+            QZO_ADD(s->jp.r1[jj], a * ur);
+            QZO_ADD(s->jp.i1[jj], a * uth);
             if (m1) {
                 const double c = p.c, sn = p.s;
-                s->rhot.ar[jj] += a * c;
-                s->rhot.ai[jj] += -a * sn;
+                QZO_ADD(s->rhot.ar[jj], a * c);
+                QZO_ADD(s->rhot.ai[jj], -a * sn);
                 const double th = wq * uth * p.Wor[cc] * iv;
-                s->drho.ar[jj] += dr * c - th * sn;
-                s->drho.ai[jj] += -dr * sn - th * c;
-                s->jz.ar[jj] += vjz * c;
-                s->jz.ai[jj] += -vjz * sn;
-                s->chi.ar[jj] += vchi * c;
-                s->chi.ai[jj] += -vchi * sn;
-                s->rho.ar[jj] += vrho * c;
-                s->rho.ai[jj] += -vrho * sn;
-                dens->ar[jj] += vn * c;
-                dens->ai[jj] += -vn * sn;
-                s->jp.r0[jj] += a * ux;
-                s->jp.i0[jj] += a * uy;
+                QZO_ADD(s->drho.ar[jj], dr * c - th * sn);
+                QZO_ADD(s->drho.ai[jj], -dr * sn - th * c);
+                QZO_ADD(s->jz.ar[jj], vjz * c);
+                QZO_ADD(s->jz.ai[jj], -vjz * sn);
+                QZO_ADD(s->chi.ar[jj], vchi * c);
+                QZO_ADD(s->chi.ai[jj], -vchi * sn);
+                QZO_ADD(s->rho.ar[jj], vrho * c);
+                QZO_ADD(s->rho.ai[jj], -vrho * sn);
+                QZO_ADD(dens->ar[jj], vn * c);
+                QZO_ADD(dens->ai[jj], -vn * sn);
+                QZO_ADD(s->jp.r0[jj], a * ux);
+                QZO_ADD(s->jp.i0[jj], a * uy);
                 const double c2 = c * c - sn * sn, s2 = 2.0 * c * sn;
-                s->jp.r2[jj] += a * (ux * c2 + uy * s2);
-                s->jp.i2[jj] += a * (uy * c2 - ux * s2);
+                QZO_ADD(s->jp.r2[jj], a * (ux * c2 + uy * s2));
+                QZO_ADD(s->jp.i2[jj], a * (uy * c2 - ux * s2));
             }
         }
     }
@@ -867,8 +879,8 @@ static void add_mode_S(const grid_t* g, const pgeo_t* p, int k, double* Sr, doub
             Ar += f2 * uy;
             Ai -= f2 * ux;
         }
-        Sr[jj] += iv * (Ar * ck + Ai * sk);
-        Si[jj] += iv * (Ai * ck - Ar * sk);
+        QZO_ADD(Sr[jj], iv * (Ar * ck + Ai * sk));
+        QZO_ADD(Si[jj], iv * (Ai * ck - Ar * sk));
     }
 }
 
@@ -877,6 +889,7 @@ static void species_deposit_S(qzo_sim* s, const species_t* q) {
     const grid_t* g = &s->fs.g;
     const double q0 = q->p.q, qm = q->p.q / q->p.m;
     const int m1 = s->m1;
+    QZO_PFOR
     for (int i = 0; i < q->Np; ++i) {
         const double wi = q->w[i];
         if (wi == 0.0) continue;
@@ -925,6 +938,7 @@ static void species_push(qzo_sim* s, species_t* q, double dxi) {
     const double R = g->R;
     const int m1 = s->m1;
     const int cap = q->cap;
+    QZO_PFOR
     for (int i = 0; i < q->Np; ++i) {
         const double wi = q->w[i];
         if (wi == 0.0) continue;
@@ -957,14 +971,14 @@ static void species_push(qzo_sim* s, species_t* q, double dxi) {
         const double gn = (1.0 + pxn * pxn + pyn * pyn + dn * dn) / (2.0 * dn);
         if (!(dn > dmin) || gn > qsamax * dn) {
             q->w[i] = 0.0;
-            s->lost += 1;
+            QZO_ADD(s->lost, 1);
             continue;
         }
         const double rn = sqrt(xn * xn + yn * yn);
         if (rn > R) {
             const double nx = xn / rn, ny = yn / rn;
             const double rr = 2.0 * R - rn;
-            if (rr < 0.0) { q->w[i] = 0.0; s->lost += 1; continue; }
+            if (rr < 0.0) { q->w[i] = 0.0; QZO_ADD(s->lost, 1); continue; }
             xn = nx * rr; yn = ny * rr;
             const double pn = pxn * nx + pyn * ny;
             pxn -= 2.0 * pn * nx; pyn -= 2.0 * pn * ny;
@@ -1188,6 +1202,7 @@ static void beam_deposit(qzo_sim* s, const beam_t* B) {
     const double xmin = s->p.xi_min, idxi = 1.0 / s->p.dxi;
     const int k0 = 0, nloc = s->p.K;
     const double R = g->R;
+    QZO_PFOR
     for (long i = 0; i < B->n; ++i) {
         const double wi = B->w[i];
         if (wi == 0.0) continue;
@@ -1216,23 +1231,23 @@ static void beam_deposit(qzo_sim* s, const beam_t* B) {
                 const int jj = j + b;
                 double* o = s->bsrc + ((size_t)kk * M + jj) * bnc;
                 const double d = wi * q * Wk[a] * Wr[b] * g->inv_V[jj] * idxi;
-                o[B_RT0] += d * omvz;
-                o[B_JZ0] += d * vz;
-                o[B_JP1R] += d * vr;
-                o[B_JP1I] += d * vt;
-                o[B_RHO0] += d;
+                QZO_ADD(o[B_RT0], d * omvz);
+                QZO_ADD(o[B_JZ0], d * vz);
+                QZO_ADD(o[B_JP1R], d * vr);
+                QZO_ADD(o[B_JP1I], d * vt);
+                QZO_ADD(o[B_RHO0], d);
                 if (m1) {
-                    o[B_RT1R] += d * omvz * c;
-                    o[B_RT1I] += -d * omvz * sn;
-                    o[B_JZ1R] += d * vz * c;
-                    o[B_JZ1I] += -d * vz * sn;
-                    o[B_RHO1R] += d * c;
-                    o[B_RHO1I] += -d * sn;
-                    o[B_JP0R] += d * vx;
-                    o[B_JP0I] += d * vy;
+                    QZO_ADD(o[B_RT1R], d * omvz * c);
+                    QZO_ADD(o[B_RT1I], -d * omvz * sn);
+                    QZO_ADD(o[B_JZ1R], d * vz * c);
+                    QZO_ADD(o[B_JZ1I], -d * vz * sn);
+                    QZO_ADD(o[B_RHO1R], d * c);
+                    QZO_ADD(o[B_RHO1I], -d * sn);
+                    QZO_ADD(o[B_JP0R], d * vx);
+                    QZO_ADD(o[B_JP0I], d * vy);
                     const double c2 = c * c - sn * sn, s2 = 2.0 * c * sn;
-                    o[B_JP2R] += d * (vx * c2 + vy * s2);
-                    o[B_JP2I] += d * (vy * c2 - vx * s2);
+                    QZO_ADD(o[B_JP2R], d * (vx * c2 + vy * s2));
+                    QZO_ADD(o[B_JP2I], d * (vy * c2 - vx * s2));
                 }
             }
         }
@@ -1249,6 +1264,7 @@ static void beam_advance(qzo_sim* s, beam_t* B, double dt_kick, double dt, int m
     const int k0 = 0, nloc = s->p.K;
     const double R = g->R;
     const double* fld = s->fld;
+    QZO_PFOR
     for (long i = 0; i < B->n; ++i) {
         if (B->w[i] == 0.0) continue;
         const double X = B->x[i], Y = B->y[i];
@@ -1378,6 +1394,9 @@ int qzo_sim_beam_sums(const qzo_sim* s, int b, double S[17]) {
     if (b < 0 || b >= s->nb) return -1;
     const beam_t* B = &s->bm[b];
     for (int c = 0; c < 17; ++c) S[c] = 0;
+#ifdef _OPENMP
+#pragma omp parallel for reduction(+ : S[:17])
+#endif
     for (long i = 0; i < B->n; ++i) {
         const double w = B->w[i];
         if (w == 0) continue;
