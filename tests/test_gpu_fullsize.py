@@ -1,0 +1,118 @@
+"""Size-independent properties at the benchmark configurations' full sizes (the oracle is too slow
+there, so these compare the library with itself through properties the path must have).
+
+- Config 1 (512 stretched nodes, 2400 slices, 2 x 1e6 beam particles), 3 steps: the pipelined run
+  equals the step-by-step run (schedule invariance): derived moments 1e-10 relative to their natural
+  scale, E_z / B_z 1e-9 relative L2 against the field scale (the larger of the component's norm and
+  E_z's), particles 1e-9; and charge is conserved while no particle is lost.
+- Config 2 (modes 0 and 1, Picard 3, 8 azimuths, 2 x 2e6 particles), 2 steps: the same.
+- Config 4 (config 1 through the adjoint), 4 steps: the pipelined adjoint equals the step-by-step
+  adjoint (1e-8 relative L2 per particle component), and the witness-delay gradient equals central
+  differences of the forward (h = 1e-6) to 1e-4. Central differences along the driver profile are no
+  check at this size: pinched plasma electrons pass within ~1e-6 of the axis, where c = x / r swings
+  sign and the u_r-weighted deposit of d(rho - J_z)/dxi with it, so J has near-jumps at the scale of
+  the perturbation (the oracle's own forward shows the same); the adjoint differentiates the smooth
+  pieces, and is checked against differences on decks without pinching (test_gpu_adjoint.py).
+- Config 3 (512 instances x 20 steps): three instances of the batch equal the same instances run on
+  their own, moments 1e-10 relative to their natural scale.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+import quarz_b200 as Q
+from quarz_b200 import adjoint as A
+from quarz_b200 import workloads
+from test_gpu_pipeline import _close
+
+pytestmark = pytest.mark.gpu
+
+
+def _runs(spec, steps, tol_f=1e-9):
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    out = []
+    for pipelined in (True, False):
+        sim = Q.Simulation(spec, beams=beams)
+        sim.set_schedule(pipelined)
+        mom = sim.run(steps, spec.dt)
+        fld, _ = sim.fields()
+        out.append((mom, fld, [sim.beam(b) for b in range(len(beams))]))
+    (mp, fp, pp), (ms, fs, ps) = out
+    for q, (_, gref, xiref) in enumerate(beams):
+        for n in range(steps + 1):
+            d = O.from_sums(mp[n, q], gref, xiref, m1=spec.modes == 1)
+            dr = O.from_sums(ms[n, q], gref, xiref, m1=spec.modes == 1)
+            _close(spec, d, dr, 1e-10, (q, n))
+    comps = (4, 5) if spec.modes == 0 else (4, 5, 14, 15)
+    ez = np.linalg.norm(fs[..., 4])
+    for c in comps:
+        # relative to the field scale: B_z comes from the small J_theta alone, so the deposit order's
+        # round-off is large against its own norm
+        err = np.linalg.norm(fp[..., c] - fs[..., c]) / max(np.linalg.norm(fs[..., c]), ez, 1e-300)
+        assert err < tol_f, (c, err)
+    for a, b in zip(pp, ps):
+        assert np.array_equal(a[:, 6] == 0, b[:, 6] == 0)
+        for c in range(6):
+            assert np.linalg.norm(a[:, c] - b[:, c]) <= tol_f * max(np.linalg.norm(b[:, c]), 1e-300), c
+    return mp
+
+
+def test_config1_full_size_schedule_invariance_and_charge():
+    spec = workloads.pinched_witness(steps=3)
+    mom = _runs(spec, 3)
+    for q in range(mom.shape[1]):
+        alive = mom[:, q, 16]
+        if np.all(alive == alive[0]):
+            np.testing.assert_allclose(mom[:, q, 0], mom[0, q, 0], rtol=1e-14)
+
+
+def test_config2_full_size_schedule_invariance():
+    spec = workloads.hosing(steps=2)
+    _runs(spec, 2)
+
+
+def test_config4_full_size_adjoint_schedules_and_delay():
+    spec = workloads.pinched_witness(steps=4)
+    samples = [Q.sample_beam(b) for b in spec.beams]
+    (ds, dg, dx), (ws, wg, wx) = samples
+    m = Q.Simulation(spec, beams=samples).run(spec.steps, spec.dt)
+    seeds = np.zeros((2, 17))
+    seeds[1] = A.gain_seed(m[-1, 1])
+    lams = []
+    for pipelined in (True, False):
+        sim = Q.Simulation(spec, beams=samples)
+        sim.set_schedule(pipelined)
+        lams.append(sim.adjoint(spec.steps, spec.dt, seeds)[0])
+    for b in range(2):
+        for c in range(7):
+            ref = lams[1][b][:, c]
+            err = np.linalg.norm(lams[0][b][:, c] - ref) / max(np.linalg.norm(ref), 1e-300)
+            assert err < 1e-8, (b, c, err)
+    gd = A.delay_gradient(lams[0][1])
+
+    def J(shift):
+        bm = [(ds, dg, dx), (A.witness_rows(ws, shift), wg, wx)]
+        mm = Q.Simulation(spec, beams=bm).run(spec.steps, spec.dt)
+        return A.gain(mm[-1, 1], mm[0, 1], wg)
+
+    h = 1e-6
+    fd = (J(h) - J(-h)) / (2 * h)
+    assert abs(fd - gd) <= 1e-4 * abs(fd), (fd, gd)
+
+
+def test_config3_full_size_batch_equals_single_runs():
+    specs = workloads.scan_instances(512, seed=2024)
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    batch = Q.Batch()
+    for s, bm in zip(specs, beams):
+        batch.add(s, bm)
+    T, dt = specs[0].steps, specs[0].dt
+    moms = batch.run(T, dt)
+    for i in (0, 255, 511):
+        sim = Q.Simulation(specs[i], beams=beams[i])
+        sim.set_schedule(False)
+        ref = sim.run(T, dt)
+        for q, (_, gref, xiref) in enumerate(beams[i]):
+            for n in range(T + 1):
+                _close(specs[i], O.from_sums(moms[i][n, q], gref, xiref), O.from_sums(ref[n, q], gref, xiref),
+                       1e-10, (i, q, n))
