@@ -190,9 +190,12 @@ qz_status qz_sim_times(qz_sim* s, double* ms3);
 qz_status qz_sim_set_beam(qz_sim* s, int b, const double* cols7, int on_device, void* stream);
 /* Timeline of the last pipelined run, 22 values per step n: GPU clock (ns, %globaltimer) at the start
    and the end of sweep n, when it had stored 1/16, 2/16, ... 16/16 of the slices, then its longest
-   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 4 totals of
+   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 10 totals of
    the push workers (warps): tasks, scans that found no ready task, claims lost to another worker, ns
-   spent in tasks. Up to cap values; *n = 22 (nsteps+1) + 4. enable = 1 records it in later runs. */
+   spent in tasks, ns waiting for a ready task, ns in the moments passes, then for the m = 0 push loop
+   its iterations (32 particles) and their SM cycles in load + push + deposit values, in the warp's run
+   sums and in the deposit atomics. Up to cap values; *n = 22 (nsteps+1) + 10. enable = 1 records it in
+   later runs. */
 qz_status qz_sim_trace(qz_sim* s, int enable, unsigned long long* out, int cap, int* n);
 /* qz_sim_run with the beams in HOST memory: copies every beam in (cols_host[b]: 7 x n SoA in the
    caller's order, x y px py pz xi w), runs nsteps, and copies the particles back into cols_host in
@@ -233,8 +236,9 @@ typedef void (*qz_adjoint_seed_fn)(const double* moments, int nsteps, int nbeams
 qz_status qz_sim_adjoint_fn(qz_sim* s, int nsteps, double dt, qz_adjoint_seed_fn fn, void* user,
                             double* const* lam_host, double* mom_host, double* ms2, void* stream);
 /* Clock cycles per phase of the run's sweeps (qz_sweep_timing of the sim's sweep): 16 counters,
-   accumulated by thread 0 of stand-alone sweeps while enabled; 0..8 the forward sweep's phases,
-   9..15 those of the step-by-step adjoint's reverse sweep. cycles16 may be NULL. */
+   accumulated by thread 0 of every sweep while enabled (all sweeps of a pipelined run together);
+   0..8 the forward sweep's phases, 9..15 those of the step-by-step adjoint's reverse sweep.
+   cycles16 may be NULL. */
 qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16);
 
 /* ------------------------------------------------------------------ batched independent runs

@@ -896,6 +896,10 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.bnc = s->bnc;
     A.sw.counters = s->sw->d_cnt;
     A.sw.timing = nullptr;
+    if (s->sw->timing) {                               // phase cycles of every sweep (qz_sim_timing)
+        QZ_CUDA(cudaMemsetAsync(s->sw->d_tim, 0, sizeof(unsigned long long) * 16, st));
+        A.sw.timing = s->sw->d_tim;
+    }
     int sms = 0;
     const int grid = qzb::pipeline_max_grid(A, &sms);
     if (grid < 2) return fail(QZ_ERR_UNSUPPORTED, "qz_sim_run: the pipelined kernel cannot be resident here");
@@ -996,7 +1000,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     }
     A.trace = nullptr;
     if (P_.trace) {
-        const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + 4;
+        const size_t ntr = (size_t)qzb::kTraceStride * (nsteps + 1) + qzb::kWorkerTotals;
         if (qz_status e = grow(&P_.d_trace, &P_.trace_n, ntr, "trace")) return e;
         QZ_CUDA(cudaMemsetAsync(P_.d_trace, 0, sizeof(unsigned long long) * ntr, st));
         A.trace = P_.d_trace;
@@ -1018,7 +1022,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     QZ_CUDA(cudaMemcpyAsync(s->d_diag, P_.diag + (size_t)last * A.diag_slot, sizeof(double) * A.diag_slot,
                             cudaMemcpyDeviceToDevice, st));
     if (P_.trace) {
-        P_.h_trace.assign((size_t)qzb::kTraceStride * (nsteps + 1) + 4, 0ull);
+        P_.h_trace.assign((size_t)qzb::kTraceStride * (nsteps + 1) + qzb::kWorkerTotals, 0ull);
         QZ_CUDA(cudaMemcpyAsync(P_.h_trace.data(), P_.d_trace, sizeof(unsigned long long) * P_.h_trace.size(),
                                 cudaMemcpyDeviceToHost, st));
     }

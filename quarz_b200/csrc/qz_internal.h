@@ -148,9 +148,10 @@ struct PipeArgs {
     unsigned long long* trace;      // optional, kTraceStride per step: %globaltimer at the start and end of
                                     // sweep n, when it passed each 16th of the box, then its longest wait
                                     // for beam rows (ns, bucket, row, bucket's cmax); after the steps:
-                                    // worker totals (tasks, empty scans, lost claims)
+                                    // kWorkerTotals worker totals (see worker_role)
 };
 constexpr int kTraceStride = 22;
+constexpr int kWorkerTotals = 10;   // trace totals of the push workers after the steps
 
 size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem);
 // resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count

@@ -740,7 +740,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     do {                                                                      \
         if (tim && tid == 0) {                                                \
             const long long tn = clock64();                                   \
-            tim[ph] += (unsigned long long)(tn - t_prev);                     \
+            atomicAdd(tim + (ph), (unsigned long long)(tn - t_prev));         \
             t_prev = tn;                                                      \
         }                                                                     \
     } while (0)
@@ -748,7 +748,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     do {                                                                      \
         if (tim && tid == 0) {                                                \
             const long long tn = clock64();                                   \
-            tim[slot] += (unsigned long long)(tn - t_sub);                    \
+            atomicAdd(tim + (slot), (unsigned long long)(tn - t_sub));        \
             t_sub = tn;                                                       \
         }                                                                     \
     } while (0)
