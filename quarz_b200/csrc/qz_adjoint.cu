@@ -253,7 +253,7 @@ __global__ void push_back_kernel(BeamArgs B, const double* __restrict__ fld, dou
         double l7[7];
 #pragma unroll
         for (int c = 0; c < 7; ++c) l7[c] = lam[c * n + i];
-        double g[24];
+        double g[24];                                // (unused: this kernel adds to lfld directly)
         int key;
         push_back_one<false>(B, fld, i, l7, lfld, dt_kick, dt, startup, g, key);
 #pragma unroll
@@ -384,12 +384,12 @@ __device__ __forceinline__ void geo_back(const AdjSm& S, const PGeo& g, GeoAdj& 
     polar_back(g.r, g.c, g.s, a.r, a.c, a.s, lx, ly);
 }
 
-// lin(f) at the particle in reverse: the node adjoints (to the shared array lf, through the batched
-// adds) and the weight adjoints
-__device__ __forceinline__ void lin_back(const PGeo& g, const double* f, double l, double* lf, GeoAdj& a,
-                                         double* (&adr)[10], double (&val)[10], int& na) {
-    adr[na] = lf + g.j; val[na++] = l * g.W0;
-    adr[na] = lf + g.j + 1; val[na++] = l * g.W1;
+// lin(f) at the particle in reverse: the adjoints of the nodes j, j+1 (appended to val, which the caller
+// scatters) and of the weights
+__device__ __forceinline__ void lin_back(const PGeo& g, const double* f, double l, GeoAdj& a, double (&val)[10],
+                                         int& na) {
+    val[na++] = l * g.W0;
+    val[na++] = l * g.W1;
     a.W0 += l * f[g.j];
     a.W1 += l * f[g.j + 1];
 }
@@ -516,14 +516,13 @@ __device__ bool push_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>&
     GeoAdj ga = {0, 0, 0, 0, 0, 0, 0};
     ga.c = l_Wx * R1 + l_Bx * BR + l_By * BI;
     ga.s = l_Wy * R1 - l_Bx * BI + l_By * BR;
-    double* adr[10];
     double val[10];
     int na = 0;
-    lin_back(g, S.wpr, l_Wx * g.c + l_Wy * g.s, S.l_wpr, ga, adr, val, na);
-    lin_back(g, S.ez, l_Ez, S.l_ez, ga, adr, val, na);
-    lin_back(g, S.bz, l_Bz, S.l_bz, ga, adr, val, na);
-    lin_back(g, S.bpr, l_Bx * g.c + l_By * g.s, S.l_bpr, ga, adr, val, na);
-    lin_back(g, S.bpi, -l_Bx * g.s + l_By * g.c, S.l_bpi, ga, adr, val, na);
+    lin_back(g, S.wpr, l_Wx * g.c + l_Wy * g.s, ga, val, na);
+    lin_back(g, S.ez, l_Ez, ga, val, na);
+    lin_back(g, S.bz, l_Bz, ga, val, na);
+    lin_back(g, S.bpr, l_Bx * g.c + l_By * g.s, ga, val, na);
+    lin_back(g, S.bpi, -l_Bx * g.s + l_By * g.c, ga, val, na);
 #pragma unroll
     for (int c = 0; c < 10; ++c) sc[c] = val[c];
     jc = g.j;
@@ -607,12 +606,11 @@ __device__ void S_back(const AdjSm& S, const SweepArgs& A, const PState<ORD>& P,
     l_D -= l_invd * invd2;
     ga.c += l_Wx * R1;
     ga.s += l_Wy * R1;
-    double* adr[10];
     double val[10];
     int na = 0;
-    lin_back(g, S.wpr, l_Wx * g.c + l_Wy * g.s, S.l_wpr, ga, adr, val, na);
-    lin_back(g, S.ez, l_Ez, S.l_ez, ga, adr, val, na);
-    lin_back(g, S.bz, l_Bz, S.l_bz, ga, adr, val, na);
+    lin_back(g, S.wpr, l_Wx * g.c + l_Wy * g.s, ga, val, na);
+    lin_back(g, S.ez, l_Ez, ga, val, na);
+    lin_back(g, S.bz, l_Bz, ga, val, na);
 #pragma unroll
     for (int c = 0; c < 6; ++c) sc[c] = val[c];
     jc = g.j;
