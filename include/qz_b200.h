@@ -190,12 +190,10 @@ qz_status qz_sim_times(qz_sim* s, double* ms3);
 qz_status qz_sim_set_beam(qz_sim* s, int b, const double* cols7, int on_device, void* stream);
 /* Timeline of the last pipelined run, 22 values per step n: GPU clock (ns, %globaltimer) at the start
    and the end of sweep n, when it had stored 1/16, 2/16, ... 16/16 of the slices, then its longest
-   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 10 totals of
+   wait for beam-source rows (ns, bucket, row, the bucket's highest cell); after the steps 6 totals of
    the push workers (warps): tasks, scans that found no ready task, claims lost to another worker, ns
-   spent in tasks, ns waiting for a ready task, ns in the moments passes, then for the m = 0 push loop
-   its iterations (32 particles) and their SM cycles in load + push + deposit values, in the warp's run
-   sums and in the deposit atomics. Up to cap values; *n = 22 (nsteps+1) + 10. enable = 1 records it in
-   later runs. */
+   spent in tasks, ns waiting for a ready task, ns in the moments passes. Up to cap values;
+   *n = 22 (nsteps+1) + 6. enable = 1 records it in later runs. */
 qz_status qz_sim_trace(qz_sim* s, int enable, unsigned long long* out, int cap, int* n);
 /* qz_sim_run with the beams in HOST memory: copies every beam in (cols_host[b]: 7 x n SoA in the
    caller's order, x y px py pz xi w), runs nsteps, and copies the particles back into cols_host in

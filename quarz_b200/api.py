@@ -261,15 +261,14 @@ class Simulation:
 
     def trace(self, enable: bool = True) -> np.ndarray:
         """Timeline of the last pipelined run (qz_sim_trace): per step (start, end, 16 progress marks, longest
-        wait) in ns of GPU clock, and the push workers' 10 totals (tasks, empty scans, lost claims, ns in tasks,
-        ns waiting for a task, ns in moments passes, m = 0 push iterations, their cycles in push, run sums and
-        atomics); enable turns the recording on for later runs."""
+        wait) in ns of GPU clock, and the push workers' 6 totals (tasks, empty scans, lost claims, ns in tasks,
+        ns waiting for a task, ns in moments passes); enable turns the recording on for later runs."""
         n = C.c_int()
         check(lib().qz_sim_trace(self.h, 1 if enable else 0, None, 0, C.byref(n)))
         out = (C.c_ulonglong * max(n.value, 1))()
         check(lib().qz_sim_trace(self.h, 1 if enable else 0, out, n.value, C.byref(n)))
         v = np.array(list(out)[: n.value], dtype=np.float64)
-        return v[:-10].reshape(-1, 22), v[-10:]
+        return v[:-6].reshape(-1, 22), v[-6:]
 
     def run_host(self, nsteps: int, dt: float, cols_host, stream=None) -> np.ndarray:
         """qz_sim_run_host: beams in host memory (list of (7, n) float64 arrays, updated in place)."""

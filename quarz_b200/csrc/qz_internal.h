@@ -151,7 +151,7 @@ struct PipeArgs {
                                     // kWorkerTotals worker totals (see worker_role)
 };
 constexpr int kTraceStride = 22;
-constexpr int kWorkerTotals = 10;   // trace totals of the push workers after the steps
+constexpr int kWorkerTotals = 6;    // trace totals of the push workers after the steps
 
 size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem);
 // resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count

@@ -272,14 +272,14 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     __syncthreads();
     const int last = P.pmom ? P.nsteps : P.nsteps - 1;     // the last step with tasks
     int n, b;
-    // trace totals: tasks, scans that found nothing, lost claims, ns in tasks, ns waiting for a task, ns in
-    // the moments pass, m = 0 push iterations, their cycles in load + push + deposit values, in run sums, in
-    // the deposit atomics
-    unsigned long long st[kWorkerTotals] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // trace totals: tasks, scans that found nothing, lost claims, ns in tasks (registers); ns waiting for a
+    // task and ns in the moments passes are added to the trace directly (no register held for them)
+    unsigned long long st[4] = {0, 0, 0, 0};
+    unsigned long long* const wtot = P.trace ? P.trace + (size_t)kTraceStride * (P.nsteps + 1) : nullptr;
     unsigned long long t_idle = P.trace ? gtimer() : 0ull;
     while (claim_task(P, last, n, b, st)) {
         const unsigned long long t_task = P.trace ? gtimer() : 0ull;
-        if (P.trace) st[4] += t_task - t_idle;
+        if (P.trace && lane == 0) atomicAdd(wtot + 4, t_task - t_idle);
         const bool push = n < P.nsteps;
         const int bb = __ldg(P.bk_beam + b);
         const long i0 = __ldg(P.bk_start + b), i1 = __ldg(P.bk_end + b);
@@ -346,7 +346,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             for (int c = 0; c < 7; ++c)
                 for (long i = i0 + lane; i < i1; i += 32) __stcg(sn + (size_t)c * Bb.n + i, __ldcg(cols[c] + i));
         }
-        if (P.trace) st[5] += gtimer() - t_task;
+        if (P.trace && lane == 0) atomicAdd(wtot + 5, gtimer() - t_task);
         int cmax = -2;
         if (!push) {
             // moments only (the state after the last push)
@@ -354,7 +354,6 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             // m = 0: particles are in (xi cell, r cell) order, so neighbouring lanes mostly deposit into
             // the same 2 x 2 cells: sum runs of equal cells across the warp, one reduction per run
             for (long base = i0; base < i1; base += 32) {
-                const long long c0 = P.trace ? clock64() : 0;
                 const long i = base + lane;
                 bool dep = false;
                 int dk = 0, dj = 0;
@@ -389,19 +388,8 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 if (!dep)
 #pragma unroll
                     for (int c = 0; c < 20; ++c) v[c] = 0.0;
-                long long c1 = 0, c2 = 0;
-                if (P.trace) { __syncwarp(); c1 = clock64(); }
                 const int key = dep ? (dk + 1) * M + dj : -1 - lane;
-                const bool lead = warp_runs_sum<20>(key, v);
-                if (P.trace) { __syncwarp(); c2 = clock64(); }
-                if (lead && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
-                if (P.trace) {
-                    __syncwarp();
-                    st[6] += 1;
-                    st[7] += (unsigned long long)(c1 - c0);
-                    st[8] += (unsigned long long)(c2 - c1);
-                    st[9] += (unsigned long long)(clock64() - c2);
-                }
+                if (warp_runs_sum<20>(key, v) && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
             }
         } else
         for (long i = i0 + lane; i < i1; i += 32) {
@@ -447,7 +435,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     }
     if (P.trace && lane == 0) {
         unsigned long long* ws = P.trace + (size_t)kTraceStride * (P.nsteps + 1);
-        for (int c = 0; c < kWorkerTotals; ++c) atomicAdd(ws + c, st[c]);
+        for (int c = 0; c < 4; ++c) atomicAdd(ws + c, st[c]);
     }
 }
 
