@@ -246,6 +246,18 @@ __device__ __forceinline__ void sums_add(double* acc, const PState7& p, double g
     for (int c = 0; c < 15; ++c) acc[c + 1] += p.w * v[c];
 }
 
+// sums_add into one lane's accumulators in shared memory (a[c * 32], c = 0..16): the same operations
+__device__ __forceinline__ void sums_add_lane(double* a, const PState7& p, double gref, double xiref) {
+    const double g = sqrt(1.0 + p.px * p.px + p.py * p.py + p.pz * p.pz);
+    const double G = g - gref, XI = p.xi - xiref;
+    const double v[15] = {G, G * G, XI, XI * XI, p.x * p.x + p.y * p.y, p.x, p.y, p.x * p.x, p.y * p.y,
+                          p.px, p.py, p.px * p.px, p.py * p.py, p.x * p.px, p.y * p.py};
+    a[16 * 32] += 1.0;
+    a[0] += p.w;
+#pragma unroll
+    for (int c = 0; c < 15; ++c) a[(c + 1) * 32] += p.w * v[c];
+}
+
 // the xi cell of a particle for bucketing: floor((xi - xi_min)/dxi) clamped to [-1, K-1]
 __device__ __forceinline__ int xi_cell(const BeamArgs& B, double xi) {
     const double s = (xi - B.xi_min) * B.idxi;

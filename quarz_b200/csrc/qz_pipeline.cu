@@ -316,7 +316,14 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
         const double gref = P.gref[bb], xiref = P.xiref[bb];
         // moments of step n (before the push), a pass of their own so that the 17 sums are not live
         // during the push; it also brings the bucket's particles into L1 for the push
-        if (P.pmom) {
+        // m = 0 pushes add the moment sums inside the push loop, each lane into its own shared-memory
+        // accumulators in the same particle order as this separate pass (the result is the same bits)
+        const bool fuse = P.pmom && push && P.modes == 0;
+        double* macc = iV + M + (size_t)(tid >> 5) * 17 * 32;        // this warp's [17][32]
+        if (fuse)
+#pragma unroll
+            for (int c = 0; c < 17; ++c) macc[c * 32 + lane] = 0.0;
+        if (P.pmom && !fuse) {
             double acc[17];
 #pragma unroll
             for (int c = 0; c < 17; ++c) acc[c] = 0.0;
@@ -365,6 +372,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                         p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
                         p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
                         p.xi = __ldcg(Bb.xi + i);
+                        if (fuse) beam_detail::sums_add_lane(macc + lane, p, gref, xiref);
                         if (push) {
                             bool alive = true;
                             int jg = 0;
@@ -415,6 +423,17 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
             }
             deposit_one(Bb, bnext, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
             cmax = max(cmax, xi_cell(Bb, p.xi));
+        }
+        if (fuse) {
+            double mine = 0.0;
+#pragma unroll
+            for (int c = 0; c < 17; ++c) {
+                double x = macc[c * 32 + lane];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+                if (lane == c) mine = x;
+            }
+            if (lane < 17) P.pmom[((size_t)n * P.nbk + b) * 17 + lane] = mine;
         }
         // bucket result: the highest live cell after the push
 #pragma unroll
@@ -615,7 +634,7 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
 
 size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem) {
     const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem);
-    const size_t worker = sizeof(double) * 3 * (size_t)M + 64;
+    const size_t worker = sizeof(double) * (3 * (size_t)M + (size_t)(kSweepThreads / 32) * 17 * 32) + 64;
     return sweep > worker ? sweep : worker;
 }
 
