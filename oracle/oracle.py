@@ -31,7 +31,7 @@ def build(omp: bool = False) -> str:
 class _Params(C.Structure):
     _fields_ = [("modes", C.c_int), ("picard", C.c_int), ("ab_order", C.c_int), ("delta_min", C.c_double),
                 ("max_qsa", C.c_double), ("xi_min", C.c_double), ("dxi", C.c_double), ("K", C.c_int),
-                ("ngp", C.c_int), ("tridiag", C.c_int), ("neutralize", C.c_int)]
+                ("ngp", C.c_int), ("tridiag", C.c_int), ("neutralize", C.c_int), ("smooth_length", C.c_double)]
 
 
 class _SpParams(C.Structure):
@@ -85,6 +85,9 @@ def lib():
         L.qzo_sample_gaussian.argtypes = [C.c_double] * 14 + [C.c_long, C.c_int, C.c_int, C.c_uint64, C.c_double,
                                                               dp, dp, dp]
         L.qzo_tridiag.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp]
+        L.qzo_filter.argtypes = [dp, C.c_int, C.c_double, C.c_int, dp]
+        L.qzo_bessel_i01_scaled.argtypes = [C.c_double, dp, dp]
+        L.qzo_sim_add_analytic_beam.argtypes = [C.c_void_p] + [C.c_double] * 5 + [C.c_int] + [C.c_double] * 7
         L.qzo_field_solve.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp, dp, dp, C.c_double, dp]
         L.qzo_operator_rows.argtypes = [dp, C.c_int, C.c_int, dp, dp, dp, dp]
         L.qzo_stencils.argtypes = [dp, C.c_int, dp, dp, dp, dp]
@@ -119,6 +122,21 @@ def tridiag(a, b, c, d, method="thomas"):
     x = np.zeros_like(d)
     lib().qzo_tridiag(_METHODS[method], len(d), _p(a), _p(b), _p(c), _p(d), _p(x))
     return x
+
+
+def smooth(nodes, a2, n, f):
+    """The radial smoothing filter F_n^{-1} f with a^2 = a2 in every cell (FieldSolver::filter)."""
+    nodes, out = _c(nodes), _c(f).copy()
+    if lib().qzo_filter(_p(nodes), len(nodes), float(a2), int(n), _p(out)) != 0:
+        raise ValueError("qzo_filter failed")
+    return out
+
+
+def bessel_i01_scaled(z):
+    """(e^-z I0(z), e^-z I1(z)) by Abramowitz & Stegun 9.8.1-9.8.4."""
+    a, b = np.zeros(1), np.zeros(1)
+    lib().qzo_bessel_i01_scaled(float(z), _p(a), _p(b))
+    return float(a[0]), float(b[0])
 
 
 def field_solve(nodes, op, rhs, chi=None, wall=None, scale=1.0, method="thomas"):
@@ -235,7 +253,8 @@ class OracleSim:
         self.spec = spec
         p = _Params(modes=spec.modes, picard=spec.picard, ab_order=spec.ab_order, delta_min=spec.delta_min,
                     max_qsa=spec.max_qsa, xi_min=spec.xi_min, dxi=spec.dxi, K=spec.K, ngp=1 if spec.ngp else 0,
-                    tridiag=_METHODS[tridiag or spec.tridiag], neutralize=1 if spec.neutralize else 0)
+                    tridiag=_METHODS[tridiag or spec.tridiag], neutralize=1 if spec.neutralize else 0,
+                    smooth_length=getattr(spec, "smooth_length", 0.0))
         self._nodes = _c(spec.nodes)
         self.h = lib().qzo_sim_create(C.byref(p), _p(self._nodes), len(self._nodes))
         if not self.h:
@@ -247,6 +266,15 @@ class OracleSim:
             lib().qzo_sim_add_species(self.h, C.byref(sp_p))
         self.beam_data = []
         for i, b in enumerate(spec.beams):
+            if b.analytic:
+                self.beam_data.append((np.zeros((0, 7)), 0.0, 0.0))
+                xcut = (0.0 - b.xi_cut_head_user) if b.xi_cut_head_user is not None else -1e300
+                rc = lib().qzo_sim_add_analytic_beam(self.h, b.q, b.n0, b.sigma_r, 0.0 - b.xi0_user, b.sigma_xi,
+                                                     1 if b.sigma_xi <= 0 else 0, b.flattop_length, xcut, b.x0,
+                                                     b.y0, -b.x_slope, -b.y_slope, b.gamma)
+                if rc != 0:
+                    raise ValueError("qzo_sim_add_analytic_beam failed")
+                continue
             if beams is not None:
                 parts, gref, xiref = beams[i]
             else:

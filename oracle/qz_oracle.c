@@ -309,6 +309,9 @@ typedef struct {
     double flux_coef;
     double *gm, *g0, *gp, *ir;
     double *bw, *dw, *work;
+    op_t F[3];             /* smoothing filter operators, angular number n = 0, 1, 2 */
+    int filter_on;
+    double* fw;
 } solver_t;
 
 enum { OP_L0 = 0, OP_L1D = 1, OP_L1F = 2, OP_L2D = 3 };
@@ -332,6 +335,9 @@ static void fv_rows(const grid_t* g, int n, double* a, double* b, double* c) {
 
 /* src/FieldSolver.cpp:113-179 */
 static int solver_init(solver_t* s, const double* nodes, int M, int method) {
+    s->filter_on = 0;
+    s->fw = NULL;
+    for (int n = 0; n < 3; ++n) s->F[n].a = s->F[n].b = s->F[n].c = NULL;
     if (grid_init(&s->g, nodes, M)) return -1;
     const grid_t* g = &s->g;
     const int N = g->N;
@@ -396,6 +402,8 @@ static int solver_init(solver_t* s, const double* nodes, int M, int method) {
 
 static void solver_free(solver_t* s) {
     for (int k = 0; k < 4; ++k) { free(s->L[k].a); free(s->L[k].b); free(s->L[k].c); }
+    for (int n = 0; n < 3; ++n) { free(s->F[n].a); free(s->F[n].b); free(s->F[n].c); }
+    free(s->fw);
     free(s->gm); free(s->g0); free(s->gp); free(s->ir); free(s->bw); free(s->dw); free(s->work);
     grid_free(&s->g);
 }
@@ -413,6 +421,68 @@ static void solver_solve(solver_t* s, int k, const double* rhs, double* f, const
         if (j == N && o->flux) s->dw[j] -= s->flux_coef * wall[N];
     }
     tridiag_any(s->method, N + 1, o->a, s->bw, o->c, s->dw, f, s->work);
+}
+
+/* FieldSolver::set_filter (src/FieldSolver.cpp:111-146): the implicit radial diffusion
+   1 - div a^2 grad of angular number n with a^2 = a2[j] in cell j. n = 0 in flux form on the node
+   volumes with a zero-flux wall (charge conserving); n = 1, 2 as the finite-volume L_n with a^2 inside
+   the flux, identity rows on the axis and at the wall. */
+static void solver_set_filter(solver_t* s, const double* a2) {
+    const grid_t* g = &s->g;
+    const int N = g->N, M = N + 1;
+    s->filter_on = 0;
+    for (int j = 0; j < N; ++j)
+        if (a2[j] > 0) s->filter_on = 1;
+    if (!s->filter_on) return;
+    for (int n = 0; n < 3; ++n) {
+        s->F[n].a = (double*)calloc(M, sizeof(double));
+        s->F[n].b = (double*)calloc(M, sizeof(double));
+        s->F[n].c = (double*)calloc(M, sizeof(double));
+        for (int j = 0; j < M; ++j) s->F[n].b[j] = 1.0;
+    }
+    s->fw = (double*)calloc(M, sizeof(double));
+    for (int j = 0; j <= N; ++j) {
+        const double invV = 2 * PI / g->V[j];
+        const double am = (j > 0) ? a2[j - 1] * g->rmid[j - 1] / g->h[j - 1] * invV : 0.0;
+        const double cp = (j < N) ? a2[j] * g->rmid[j] / g->h[j] * invV : 0.0;
+        s->F[0].a[j] = -am;
+        s->F[0].c[j] = -cp;
+        s->F[0].b[j] = 1 + am + cp;
+    }
+    for (int n = 1; n <= 2; ++n)
+        for (int j = 1; j < N; ++j) {
+            const double dV = 0.5 * (g->h[j] + g->h[j - 1]);
+            const double pre = pow(g->r[j], n - 1) / dV;
+            const double kpj = a2[j] / (g->h[j] * pow(g->rmid[j], 2 * n - 1));
+            const double kpm = a2[j - 1] / (g->h[j - 1] * pow(g->rmid[j - 1], 2 * n - 1));
+            s->F[n].c[j] = -pre * pow(g->r[j + 1], n) * kpj;
+            s->F[n].a[j] = -pre * pow(g->r[j - 1], n) * kpm;
+            s->F[n].b[j] = 1 + pre * pow(g->r[j], n) * (kpj + kpm);
+        }
+}
+
+/* FieldSolver::filter (src/FieldSolver.cpp:148-161): f <- F_n^{-1} f */
+static void solver_filter(solver_t* s, int n, double* f) {
+    if (!s->filter_on) return;
+    const op_t* o = &s->F[n];
+    const int M = s->g.N + 1;
+    for (int j = 0; j < M; ++j) { s->bw[j] = o->b[j]; s->dw[j] = f[j]; }
+    tridiag_any(s->method, M, o->a, s->bw, o->c, s->dw, s->fw, s->work);
+    memcpy(f, s->fw, sizeof(double) * M);
+}
+
+int qzo_filter(const double* nodes, int M, double a2, int n, double* f) {
+    if (n < 0 || n > 2) return -1;
+    solver_t s;
+    memset(&s, 0, sizeof(s));
+    if (solver_init(&s, nodes, M, QZO_THOMAS)) return -1;
+    double* a = (double*)malloc(sizeof(double) * M);
+    for (int j = 0; j < M; ++j) a[j] = a2;
+    solver_set_filter(&s, a);
+    solver_filter(&s, n, f);
+    free(a);
+    solver_free(&s);
+    return 0;
 }
 
 /* src/FieldSolver.cpp:263-289 */
@@ -579,6 +649,9 @@ typedef struct {
     long n;
     double *x, *y, *px, *py, *pz, *xi, *w;
     double gref, xiref;
+    /* analytic rigid beam (no particles): src/Beam.hpp:153-160 */
+    int analytic, an_flat;
+    double an_n0, an_sr, an_xi0, an_sxi, an_len, an_cut, an_x0, an_y0, an_xs, an_ys, an_gamma;
 } beam_t;
 
 struct qzo_sim {
@@ -627,6 +700,13 @@ qzo_sim* qzo_sim_create(const qzo_params* p, const double* nodes, int M) {
     if (solver_init(&s->fs, nodes, M, p->tridiag)) { free(s); return NULL; }
     s->M = M;
     s->m1 = p->modes == 1;
+    if (p->smooth_length < 0) { solver_free(&s->fs); free(s); return NULL; }
+    if (p->smooth_length > 0) {   /* src/Simulation.cpp:63-66: a^2 in every cell */
+        double* a2 = (double*)malloc(sizeof(double) * M);
+        for (int j = 0; j < M; ++j) a2[j] = p->smooth_length * p->smooth_length;
+        solver_set_filter(&s->fs, a2);
+        free(a2);
+    }
     const int narr = 7 * 3 + 2 * 6 + 3 * 3 + 3 * 6 + 5 + 2 * 3 + 6;
     s->pool = (double*)calloc((size_t)narr * M + 15 * (size_t)M, sizeof(double));
     double* cur = s->pool;
@@ -692,6 +772,81 @@ int qzo_sim_add_beam(qzo_sim* s, const double* p7, long n, double q, double m, i
         for (long i = 0; i < n; ++i) (*cols[c])[i] = p7[7 * i + c];
     }
     return 0;
+}
+
+int qzo_sim_add_analytic_beam(qzo_sim* s, double q, double n0, double sigma_r, double xi0, double sigma_xi,
+                              int flattop, double length, double xi_cut, double x0, double y0, double xs,
+                              double ys, double gamma) {
+    if (s->nb >= 8 || !(sigma_r > 0) || !(gamma >= 1) || (!flattop && !(sigma_xi > 0))) return -1;
+    if (!s->m1 && (x0 != 0 || y0 != 0 || xs != 0 || ys != 0)) return -1;   /* src/Beam.cpp:197-198 */
+    beam_t* B = &s->bm[s->nb++];
+    memset(B, 0, sizeof(*B));
+    B->q = q; B->m = 1.0; B->rigid = 1; B->n = 0; B->analytic = 1;
+    double** cols[7] = {&B->x, &B->y, &B->px, &B->py, &B->pz, &B->xi, &B->w};
+    for (int c = 0; c < 7; ++c) *cols[c] = (double*)malloc(sizeof(double));
+    B->an_flat = flattop; B->an_n0 = n0; B->an_sr = sigma_r; B->an_xi0 = xi0; B->an_sxi = sigma_xi;
+    B->an_len = length; B->an_cut = xi_cut; B->an_x0 = x0; B->an_y0 = y0; B->an_xs = xs; B->an_ys = ys;
+    B->an_gamma = gamma;
+    return 0;
+}
+
+/* Abramowitz & Stegun 9.8.1-9.8.4: I0, I1 as polynomials in (z / 3.75)^2 below 3.75, and
+   sqrt(z) e^{-z} I0,1 as polynomials in 3.75 / z above (relative error below 2e-7) */
+void qzo_bessel_i01_scaled(double z, double* i0, double* i1) {
+    if (z < 3.75) {
+        const double t = (z / 3.75) * (z / 3.75);
+        const double I0 = 1.0 + t * (3.5156229 + t * (3.0899424 + t * (1.2067492 + t * (0.2659732
+                          + t * (0.0360768 + t * 0.0045813)))));
+        const double I1 = z * (0.5 + t * (0.87890594 + t * (0.51498869 + t * (0.15084934 + t * (0.02658733
+                          + t * (0.00301532 + t * 0.00032411))))));
+        const double e = exp(-z);
+        *i0 = I0 * e;
+        *i1 = I1 * e;
+    } else {
+        const double u = 3.75 / z, sq = 1.0 / sqrt(z);
+        *i0 = sq * (0.39894228 + u * (0.01328592 + u * (0.00225319 + u * (-0.00157565 + u * (0.00916281
+              + u * (-0.02057706 + u * (0.02635537 + u * (-0.01647633 + u * 0.00392377))))))));
+        *i1 = sq * (0.39894228 + u * (-0.03988024 + u * (-0.00362018 + u * (0.00163801 + u * (-0.01031555
+              + u * (0.02282967 + u * (-0.02895312 + u * (0.01787654 - u * 0.00420059))))))));
+    }
+}
+
+/* src/Beam.cpp:236-279: rho = q n0 f(xi) exp(-|x_perp - c(xi)|^2 / 2 sigma_r^2) moving at v_z(gamma), its
+   azimuthal modes at every node through the scaled Bessel functions of z = r d / sigma_r^2 */
+static void deposit_analytic(qzo_sim* s, const beam_t* B) {
+    const grid_t* g = &s->fs.g;
+    const int M = s->M, K = s->p.K, bnc = s->bnc, m1 = s->m1;
+    const double s2 = B->an_sr * B->an_sr;
+    const double gam = B->an_gamma;
+    const double vz = sqrt(1.0 - 1.0 / (gam * gam));
+    const double omvz = 1.0 / (gam * gam * (1.0 + vz));
+    for (int k = 0; k < K; ++k) {
+        const double xi = s->p.xi_min + k * s->p.dxi;
+        if (xi < B->an_cut) continue;
+        double fxi;
+        if (B->an_flat) fxi = (fabs(xi - B->an_xi0) <= 0.5 * B->an_len) ? 1.0 : 0.0;
+        else fxi = exp(-0.5 * (xi - B->an_xi0) * (xi - B->an_xi0) / (B->an_sxi * B->an_sxi));
+        if (fxi == 0.0) continue;
+        const double cx = B->an_x0 + B->an_xs * (xi - B->an_xi0), cy = B->an_y0 + B->an_ys * (xi - B->an_xi0);
+        const double d = sqrt(cx * cx + cy * cy);
+        for (int j = 0; j < M; ++j) {
+            const double r = g->r[j];
+            double i0, i1;
+            qzo_bessel_i01_scaled(r * d / s2, &i0, &i1);
+            const double env = B->q * B->an_n0 * fxi * exp(-0.5 * (r - d) * (r - d) / s2);
+            const double rho0 = env * i0;
+            double* o = s->bsrc + ((size_t)k * M + j) * bnc;
+            o[B_RHO0] += rho0;
+            o[B_RT0] += rho0 * omvz;
+            o[B_JZ0] += rho0 * vz;
+            if (m1 && d > 0.0) {
+                const double f1r = env * i1 * (cx / d), f1i = -env * i1 * (cy / d);
+                o[B_RHO1R] += f1r; o[B_RHO1I] += f1i;
+                o[B_RT1R] += f1r * omvz; o[B_RT1I] += f1i * omvz;
+                o[B_JZ1R] += f1r * vz; o[B_JZ1I] += f1i * vz;
+            }
+        }
+    }
 }
 
 /* ---- plasma ---- */
@@ -1190,6 +1345,13 @@ static void solve_slice_fields(qzo_sim* s) {
     compute_bz(s);
     for (int i = 0; i < s->nsp; ++i)
         if (s->sp[i].p.mobile) species_deposit_S(s, &s->sp[i]);
+    if (s->fs.filter_on) {   /* src/Simulation.cpp:810-816 */
+        solver_filter(&s->fs, 1, s->S.r1); solver_filter(&s->fs, 1, s->S.i1);
+        if (s->m1) {
+            solver_filter(&s->fs, 0, s->S.r0); solver_filter(&s->fs, 0, s->S.i0);
+            solver_filter(&s->fs, 2, s->S.r2); solver_filter(&s->fs, 2, s->S.i2);
+        }
+    }
     solve_bplus(s);
 }
 
@@ -1326,8 +1488,28 @@ static void beam_advance(qzo_sim* s, beam_t* B, double dt_kick, double dt, int m
 
 int qzo_sim_deposit_beams(qzo_sim* s) {
     memset(s->bsrc, 0, sizeof(double) * (size_t)s->p.K * s->M * s->bnc);
-    for (int b = 0; b < s->nb; ++b) beam_deposit(s, &s->bm[b]);
+    for (int b = 0; b < s->nb; ++b) {
+        if (s->bm[b].analytic) deposit_analytic(s, &s->bm[b]);
+        else beam_deposit(s, &s->bm[b]);
+    }
     return 0;
+}
+
+/* Simulation::filter_plasma_sources (src/Simulation.cpp:821-835): the plasma deposit of the slice, before
+   the beams and the background are added */
+static void filter_plasma_sources(qzo_sim* s) {
+    if (!s->fs.filter_on) return;
+    msc_t* sc[7] = {&s->rhot, &s->drho, &s->jz, &s->chi, &s->rho, &s->ne, &s->ni};
+    for (int c = 0; c < 7; ++c) {
+        solver_filter(&s->fs, 0, sc[c]->a0);
+        if (s->m1) { solver_filter(&s->fs, 1, sc[c]->ar); solver_filter(&s->fs, 1, sc[c]->ai); }
+    }
+    solver_filter(&s->fs, 1, s->jp.r1);
+    solver_filter(&s->fs, 1, s->jp.i1);
+    if (s->m1) {
+        solver_filter(&s->fs, 0, s->jp.r0); solver_filter(&s->fs, 0, s->jp.i0);
+        solver_filter(&s->fs, 2, s->jp.r2); solver_filter(&s->fs, 2, s->jp.i2);
+    }
 }
 
 /* src/Simulation.cpp:636-795 (single rank: bguard = 0, B+ starts at 0, one sub-slice) */
@@ -1350,6 +1532,12 @@ int qzo_sim_step_fields(qzo_sim* s, double t) {
             s->bg_rho.a0[j] -= s->rho.a0[j]; s->bg_rho.ar[j] -= s->rho.ar[j]; s->bg_rho.ai[j] -= s->rho.ai[j];
         }
     }
+    if (s->fs.filter_on)   /* src/Simulation.cpp:685-690 */
+        for (int c = 0; c < 2; ++c) {
+            msc_t* m = c == 0 ? &s->bg_rhot : &s->bg_rho;
+            solver_filter(&s->fs, 0, m->a0);
+            if (s->m1) { solver_filter(&s->fs, 1, m->ar); solver_filter(&s->fs, 1, m->ai); }
+        }
     mvec_zero(&s->bp, M);
     memset(s->bguard, 0, sizeof(double) * 15 * M);
     const double dxi = s->p.dxi;
@@ -1368,6 +1556,7 @@ int qzo_sim_step_fields(qzo_sim* s, double t) {
         zero_sources(s);
         for (int i = 0; i < s->nsp; ++i)
             if (s->sp[i].p.mobile) species_deposit(s, &s->sp[i]);
+        filter_plasma_sources(s);
         combine_sources(s, k);
         solve_slice_fields(s);
         store_slice(s, k);

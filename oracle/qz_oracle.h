@@ -76,6 +76,7 @@ typedef struct {
     int ngp;              /* beams.xi_shape = ngp */
     int tridiag;          /* QZO_THOMAS / PCR / PARTITION */
     int neutralize;
+    double smooth_length; /* plasma.smooth_length: radial smoothing of the plasma sources (0: off) */
 } qzo_params;
 
 typedef struct {
@@ -101,6 +102,18 @@ long     qzo_sample_gaussian(double n0, double sr, double xi0_int, double sxi, d
                              double emit, double cut, double cx0, double cy0, double cxs, double cys,
                              double xp0, double yp0, long np, int nrot, int mirror, uint64_t seed, double xcut,
                              double* out, double* gref, double* xiref);
+/* a noise-free rigid beam deposited on the grid (<name>.analytic = 1, src/Beam.cpp:183-203):
+   charge q, density n0, radius sigma_r, centre xi0 (internal), sigma_xi (gaussian) or length (flattop = 1),
+   head cut xi_cut (internal; -1e300 for none), centroid (x0, y0) + (xs, ys) (xi - xi0), gamma. No particles:
+   its moment sums are zero and it is never pushed. */
+int      qzo_sim_add_analytic_beam(qzo_sim* s, double q, double n0, double sigma_r, double xi0, double sigma_xi,
+                                   int flattop, double length, double xi_cut, double x0, double y0, double xs,
+                                   double ys, double gamma);
+/* the radial smoothing filter f <- (1 - div a^2 grad)^{-1} f of angular number n = 0, 1, 2 with a^2 = a2 in
+   every cell (FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161), in place on f (M) */
+int      qzo_filter(const double* nodes, int M, double a2, int n, double* f);
+/* e^{-z} I0(z), e^{-z} I1(z) by the polynomial approximations of Abramowitz & Stegun 9.8.1-9.8.4 */
+void     qzo_bessel_i01_scaled(double z, double* i0, double* i1);
 /* one quasi-static sweep (beam deposit + plasma load + sweep), as Simulation::step_fields */
 int      qzo_sim_step_fields(qzo_sim* s, double t);
 /* beam push of every non-rigid beam */

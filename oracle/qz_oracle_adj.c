@@ -795,7 +795,7 @@ static void beams_load(qzo_sim* s, const double* in) {
    J = sum lamS * sums. mom (optional): the forward's moment sums ((nsteps + 1), nb, 17).
    Returns 0, or -2 when the deck is outside the adjoint's scope. The sim ends at the last step. */
 int qzo_sim_adjoint(qzo_sim* s, int nsteps, double dt, const double* lamS, double* lam_out, double* mom) {
-    if (s->m1 || s->p.ngp || nsteps < 1) return -2;
+    if (s->m1 || s->p.ngp || s->fs.filter_on || nsteps < 1) return -2;
     int isp = -1;
     for (int i = 0; i < s->nsp; ++i)
         if (s->sp[i].p.mobile) { if (isp >= 0) return -2; isp = i; }

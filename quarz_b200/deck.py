@@ -9,6 +9,8 @@ beams, pusher / solver options, time stepping). Semantics follow the reference:
   * species defaults (ppc 4, ntheta 8 with m = 1)  src/PlasmaSpecies.cpp:92-150
   * beam keys of the gaussian generator           src/Beam.cpp:483-570
   * neutralising background when no positive species   src/Simulation.cpp:124-134
+  * radial smoothing of the plasma sources (plasma.smooth_length)   src/Simulation.cpp:63-66
+  * analytic rigid beams (<beam>.analytic = 1)     src/Beam.cpp:183-203
 
 Keys this module does not know raise ``ValueError`` (the reference's strict unknown-key check,
 src/main.cpp:100-116, restricted to the hot-path subset).
@@ -30,11 +32,12 @@ _GLOBAL_KEYS = {
     "solver.tridiag", "pusher.ab_order", "pusher.delta_min", "pusher.max_qsa_factor", "plasma.species",
     "plasma.seed", "plasma.neutralize", "plasma.rmax", "plasma.radial", "plasma.channel_depth",
     "plasma.channel_radius", "beams", "beams.xi_shape", "output.dir", "output.every", "pusher.beam",
+    "plasma.smooth_length",
 }
 _SPECIES_KEYS = {"charge", "mass", "mobile", "ppc", "ntheta", "density"}
 _BEAM_KEYS = {"n0", "sigma_r", "sigma_xi", "xi0", "gamma", "espread", "emit_n", "cut", "nparticles", "seed",
               "rigid", "charge", "mass", "x0", "y0", "x_slope", "y_slope", "xp0", "yp0", "nsym", "mirror_y",
-              "profile", "length", "xi_cut_head", "pusher"}
+              "profile", "length", "xi_cut_head", "pusher", "analytic"}
 
 
 def parse_deck(text: str, overrides: Sequence[str] = ()) -> Dict[str, str]:
@@ -177,6 +180,7 @@ class BeamSpec:
     mirror_y: bool = False
     flattop_length: float = 0.0
     xi_cut_head_user: Optional[float] = None
+    analytic: bool = False      # noise-free rigid beam deposited on the grid, no particles
 
 
 @dataclass
@@ -193,6 +197,7 @@ class RunSpec:
     ngp: bool = False
     tridiag: str = "auto"
     neutralize: bool = True
+    smooth_length: float = 0.0   # plasma.smooth_length (0: no smoothing)
     dt: float = 0.0
     steps: int = 0
     species: List[SpeciesSpec] = field(default_factory=list)
@@ -259,6 +264,9 @@ def run_spec(cfg: Dict[str, str], base_dir: str = ".") -> RunSpec:
         dt=float(cfg.get("time.dt", "0")),
         steps=int(cfg.get("time.steps", "0")),
     )
+    spec.smooth_length = float(cfg.get("plasma.smooth_length", "0"))
+    if spec.smooth_length < 0:
+        raise ValueError("plasma.smooth_length must be >= 0")
     if not 1 <= spec.ab_order <= 5:
         raise ValueError("pusher.ab_order must be 1..5")
     if cfg.get("pusher.beam", "vay") != "vay":
@@ -309,6 +317,9 @@ def run_spec(cfg: Dict[str, str], base_dir: str = ".") -> RunSpec:
         b.nparticles = int(float(cfg.get(n + ".nparticles", "100000")))
         b.seed = int(cfg.get(n + ".seed", "12345"))
         b.rigid = _b(cfg.get(n + ".rigid", "0"))
+        b.analytic = _b(cfg.get(n + ".analytic", "0"))
+        if b.analytic:
+            b.rigid = True
         b.q = float(cfg.get(n + ".charge", "-1"))
         b.m = float(cfg.get(n + ".mass", "1"))
         b.x0 = float(cfg.get(n + ".x0", "0"))

@@ -1,0 +1,164 @@
+"""The oracle's radial smoothing filter (plasma.smooth_length) and analytic rigid beams, pinned against the
+reference's own checks.
+
+Filter (FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161), the three checks of
+tests/test_filter.cpp:36-105 with their grids and thresholds:
+  1. manufactured solutions f = r^n exp(-r^2/w^2), n = 0, 1, 2, on a stretched grid refined once:
+     second order (observed order > 1.8) and max error < 1e-4 on the fine grid;
+  2. n = 0: total charge sum V_j f_j conserved and constants preserved to 1e-12;
+  3. n = 0: a point charge on the axis gives the 2D Green's function K0(r/a) / (2 pi a^2) to 1 %
+     for a <= r <= 8a.
+
+Analytic beam (Beam::deposit_analytic, src/Beam.cpp:215-279):
+  - the scaled Bessel functions against scipy's i0e / i1e to the Abramowitz & Stegun bound;
+  - the deposited modes 0 and 1 of a displaced Gaussian against a direct azimuthal quadrature of
+    q n0 f(xi) exp(-|x - c|^2 / 2 sigma^2) (f = f0 + 2 Re f1 e^{i theta}), and the rho - J_z and J_z
+    parts against (1 - v_z) rho and v_z rho;
+  - a smoothed run of the oracle keeps the fresh uniform plasma of slice 0 unchanged and differs from
+    the unsmoothed run behind the driver (the filter is reached from the deck)."""
+import numpy as np
+import pytest
+from scipy import special
+
+import oracle as O
+from quarz_b200 import deck
+
+
+def _nodes(h0, hmax, R, q=1.05):
+    """the stretched grid of tests/test_filter.cpp:16-21"""
+    r = [0.0]
+    h = h0
+    while r[-1] < R - 1e-12:
+        r.append(min(R, r[-1] + h))
+        h = min(hmax, h * q)
+    return np.array(r)
+
+
+A, W, R = 0.05, 0.5, 4.0
+
+
+@pytest.mark.parametrize("n", [0, 1, 2])
+def test_filter_manufactured_second_order(n):
+    err = []
+    for lev in range(2):
+        s = 0.5 if lev else 1.0
+        r = _nodes(0.004 * s, 0.04 * s, R, np.sqrt(1.1) if lev else 1.1)
+        g = np.exp(-r * r / (W * W))
+        ex = r ** n * g
+        src = ex - A * A * ex * (4 * r * r / W ** 4 - 4.0 * (n + 1) / (W * W))
+        f = O.smooth(r, A * A, n, src)
+        err.append(np.abs(f - ex).max())
+    order = np.log2(err[0] / err[1])
+    assert order > 1.8 and err[1] < 1e-4, (n, err, order)
+
+
+def test_filter_conserves_charge_and_constants():
+    r = _nodes(0.0005, 0.02, R)
+    V = O.volumes(r)
+    s = np.random.default_rng(1).uniform(-1, 1, len(r))
+    f = O.smooth(r, A * A, 0, s)
+    c = O.smooth(r, A * A, 0, np.ones(len(r)))
+    assert abs(V @ f - V @ s) / abs(V @ s) < 1e-12
+    assert np.abs(c - 1).max() < 1e-12
+
+
+def test_filter_point_charge_green_function():
+    r = _nodes(0.0005, 0.02, R)
+    V = O.volumes(r)
+    s = np.zeros(len(r))
+    s[0] = 1.0 / V[0]
+    f = O.smooth(r, A * A, 0, s)
+    m = (r >= A) & (r <= 8 * A)
+    G = special.k0(r[m] / A) / (2 * np.pi * A * A)
+    assert np.abs(f[m] - G).max() < 0.01 * G.max() and np.max(np.abs(f[m] - G) / G) < 0.01
+
+
+def test_bessel_scaled_against_scipy():
+    # the published error bounds: 9.8.1 |e| < 1.6e-7 on I0, 9.8.3 |e| < 8e-9 on I1 / z (z < 3.75);
+    # 9.8.2 |e| < 1.9e-7 and 9.8.4 |e| < 2.2e-7 on sqrt(z) e^-z I0,1 (z >= 3.75); a little slack for rounding
+    for z in np.concatenate([np.linspace(1e-8, 3.75, 200, endpoint=False), np.linspace(3.75, 200, 400), [1e4]]):
+        i0, i1 = O.bessel_i01_scaled(z)
+        if z < 3.75:
+            e = np.exp(z)
+            assert abs(i0 * e - special.i0(z)) <= 1.7e-7, z
+            assert abs(i1 * e / z - special.i1(z) / z) <= 9e-9, z
+        else:
+            sq = np.sqrt(z)
+            assert abs(sq * (i0 - special.i0e(z))) <= 2.0e-7, z
+            assert abs(sq * (i1 - special.i1e(z))) <= 2.3e-7, z
+
+
+TEXT = """
+xi.convention = z-t
+modes = {modes}
+grid.type = uniform
+grid.rmax = 3
+grid.dr = 0.05
+xi.min = -6
+xi.max = 0
+xi.step = 0.1
+plasma.species = electrons
+electrons.ppc = 1
+electrons.ntheta = {ntheta}
+beams = driver
+driver.analytic = 1
+driver.n0 = 2
+driver.sigma_r = 0.4
+driver.sigma_xi = 1
+driver.xi0 = -3
+driver.gamma = 200
+driver.x0 = {x0}
+driver.x_slope = {xs}
+"""
+
+
+def test_analytic_deposit_modes_against_quadrature():
+    spec = deck.run_spec(deck.parse_deck(TEXT.format(modes=1, ntheta=4, x0=0.15, xs=0.05)))
+    sim = O.OracleSim(spec)
+    sim.deposit_beams()
+    K, M = spec.K, spec.M
+    b = np.ctypeslib.as_array(O.lib().qzo_sim_bsrc(sim.h), shape=(K * M * 15,)).reshape(K, M, 15).copy()
+    bs = spec.beams[0]
+    r = spec.nodes
+    th = np.linspace(0, 2 * np.pi, 4096, endpoint=False)
+    vz = np.sqrt(1 - 1 / bs.gamma ** 2)
+    omvz = 1 / (bs.gamma ** 2 * (1 + vz))
+    worst = 0.0
+    for k in range(0, K, 7):
+        xi = spec.xi_min + k * spec.dxi
+        xi0 = -bs.xi0_user
+        fx = np.exp(-0.5 * (xi - xi0) ** 2 / bs.sigma_xi ** 2)
+        cx = bs.x0 - bs.x_slope * (xi - xi0)
+        x = r[:, None] * np.cos(th)[None, :]
+        y = r[:, None] * np.sin(th)[None, :]
+        rho = bs.q * bs.n0 * fx * np.exp(-((x - cx) ** 2 + y ** 2) / (2 * bs.sigma_r ** 2))
+        m0 = rho.mean(axis=1)
+        m1 = (rho * np.exp(-1j * th)[None, :]).mean(axis=1)
+        scale = np.abs(m0).max()
+        worst = max(worst, np.abs(b[k, :, 4] - m0).max() / scale, np.abs(b[k, :, 13] - m1.real).max() / scale,
+                    np.abs(b[k, :, 14] - m1.imag).max() / scale)
+        np.testing.assert_allclose(b[k, :, 0], omvz * b[k, :, 4], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(b[k, :, 1], vz * b[k, :, 4], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(b[k, :, 5], omvz * b[k, :, 13], rtol=1e-14, atol=0)
+        np.testing.assert_allclose(b[k, :, 8], vz * b[k, :, 14], rtol=1e-14, atol=0)
+        assert np.all(b[k, :, 2:4] == 0) and np.all(b[k, :, 9:13] == 0)
+    assert worst < 1e-6, worst
+
+
+def test_smoothing_reaches_the_sweep():
+    base = TEXT.format(modes=0, ntheta=1, x0=0, xs=0).replace("driver.n0 = 2", "driver.n0 = 4")
+    out = []
+    for a in ("0", "0.1"):
+        spec = deck.run_spec(deck.parse_deck(base + f"\nplasma.smooth_length = {a}\n"))
+        sim = O.OracleSim(spec)
+        sim.step_fields()
+        K, M = spec.K, spec.M
+        d = np.ctypeslib.as_array(O.lib().qzo_sim_diag(sim.h), shape=(K * M * 3,)).reshape(K, M, 3).copy()
+        f = np.ctypeslib.as_array(O.lib().qzo_sim_fld(sim.h), shape=(K * M * 6,)).reshape(K, M, 6).copy()
+        out.append((d, f, O.volumes(spec.nodes)))
+    (d0, f0, V), (d1, f1, _) = out
+    # slice 0 is the fresh uniform plasma: the filter keeps constants, so its density is unchanged; behind
+    # the driver head the smoothed run differs
+    np.testing.assert_allclose(d1[0, :, 1], d0[0, :, 1], rtol=1e-12)
+    assert np.abs(d1[:, :, 1] - d0[:, :, 1]).max() > 1e-3
+    assert np.abs(f1[:, :, 4] - f0[:, :, 4]).max() > 1e-4
