@@ -55,8 +55,9 @@ qz_status qz_grid_operator(const qz_grid* g, int op, double* a_host, double* b_h
  * Replaces Simulation::step_fields' per-slice chain (src/Simulation.cpp:636-795) with the plasma of
  * PlasmaSpecies (load src/PlasmaSpecies.cpp:202-295, deposit :409-478, deposit_rho :480-506,
  * deposit_S :508-559, push :561-668) and the field solves of Simulation::solve_slice_fields
- * (src/Simulation.cpp:797-819). Single rank, constant dxi (no sub-slicing), no laser / ionization /
- * smoothing filter. */
+ * (src/Simulation.cpp:797-819). Single rank, constant dxi (no sub-slicing), no laser / ionization.
+ * The radial smoothing of the plasma sources (plasma.smooth_length, src/Simulation.cpp:63-66, :685-690,
+ * :810-835; FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161) is on this path for modes = 0. */
 typedef struct {
     double q, m;             /* <name>.charge, <name>.mass */
     int ppc, ntheta;         /* <name>.ppc, <name>.ntheta */
@@ -79,6 +80,7 @@ typedef struct {
     int neutralize;          /* plasma.neutralize */
     int nspecies;
     qz_species species[4];
+    double smooth_length;    /* plasma.smooth_length (0: off; > 0 with modes = 0 only) */
 } qz_sweep_params;
 
 typedef struct {
@@ -130,6 +132,25 @@ qz_status qz_beam_push(const qz_grid* g, qz_beam_view* b, const qz_box* box, con
 qz_status qz_beam_push_deposit(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld_dev,
                                double dt_kick, double dt_drift, int* started, double* bsrc_next_dev,
                                void* stream);
+/* A noise-free rigid beam deposited directly on the grid (<name>.analytic = 1, src/Beam.cpp:183-203):
+   rho = q n0 f(xi) exp(-|x_perp - c(xi)|^2 / 2 sigma_r^2) moving at v_z(gamma), f gaussian (sigma_xi) or
+   flat-top (length), centroid c = (x0, y0) + (x_slope, y_slope) (xi - xi0). Internal xi for xi0 and xi_cut
+   (slices with xi < xi_cut get nothing; -1e300 for none) and internal slopes (d x_c / d xi_internal). */
+typedef struct {
+    double q, n0, sigma_r;
+    double xi0, sigma_xi;
+    int flattop;
+    double length;
+    double xi_cut;
+    double x0, y0, x_slope, y_slope;
+    double gamma;
+} qz_analytic_beam;
+
+/* Beam::deposit_analytic (src/Beam.cpp:236-279): adds the beam's sources to bsrc (dev, (K, M, B_NC), not
+   cleared); offsets and slopes need box->modes = 1 */
+qz_status qz_beam_deposit_analytic(const qz_grid* g, const qz_analytic_beam* b, const qz_box* box, double* bsrc_dev,
+                                   void* stream);
+
 /* the 17 moment sums of Beam::sums into out17 (dev); deterministic order */
 qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
 /* qz_beam_sums without any device allocation, for callers that cannot allocate (a host whose
@@ -162,6 +183,10 @@ qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, qz_sim** out
 qz_status qz_sim_destroy(qz_sim* s);
 qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q, double m, int rigid,
                           double gref, double xiref);
+/* an analytic rigid beam (qz_beam_deposit_analytic): deposited once into a static source array that every
+   sweep of the sim adds to the pushed beams' sources. It has no particles, so it is not one of the sim's
+   beams: nbeams, the moments and qz_sim_beam count only the particle beams. */
+qz_status qz_sim_add_analytic_beam(qz_sim* s, const qz_analytic_beam* b);
 /* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
    By default (modes 0 or 1, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
    consecutive steps run concurrently on different SMs, each slice gated on the beam pushes of the

@@ -25,7 +25,8 @@ class Species(C.Structure):
 class SweepParams(C.Structure):
     _fields_ = [("modes", C.c_int), ("picard", C.c_int), ("ab_order", C.c_int), ("delta_min", C.c_double),
                 ("max_qsa", C.c_double), ("xi_min", C.c_double), ("dxi", C.c_double), ("K", C.c_int),
-                ("ngp", C.c_int), ("neutralize", C.c_int), ("nspecies", C.c_int), ("species", Species * 4)]
+                ("ngp", C.c_int), ("neutralize", C.c_int), ("nspecies", C.c_int), ("species", Species * 4),
+                ("smooth_length", C.c_double)]
 
 
 class Counters(C.Structure):
@@ -39,6 +40,13 @@ class BeamView(C.Structure):
 
 class Box(C.Structure):
     _fields_ = [("xi_min", C.c_double), ("dxi", C.c_double), ("K", C.c_int), ("ngp", C.c_int), ("modes", C.c_int)]
+
+
+class AnalyticBeam(C.Structure):
+    _fields_ = [("q", C.c_double), ("n0", C.c_double), ("sigma_r", C.c_double), ("xi0", C.c_double),
+                ("sigma_xi", C.c_double), ("flattop", C.c_int), ("length", C.c_double), ("xi_cut", C.c_double),
+                ("x0", C.c_double), ("y0", C.c_double), ("x_slope", C.c_double), ("y_slope", C.c_double),
+                ("gamma", C.c_double)]
 
 
 _lib = None
@@ -64,6 +72,7 @@ SIGNATURES = {
                      C.POINTER(C.c_int), C.c_void_p],
     "qz_beam_push_deposit": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,
                              C.POINTER(C.c_int), C.c_void_p, C.c_void_p],
+    "qz_beam_deposit_analytic": [C.c_void_p, C.POINTER(AnalyticBeam), C.POINTER(Box), C.c_void_p, C.c_void_p],
     "qz_beam_sums": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "qz_beam_sums_noalloc": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "qz_sample_gaussian": [C.c_double] * 14 + [C.c_int64, C.c_int, C.c_int, C.c_uint64, C.c_double, _dp, _dp, _dp,
@@ -71,6 +80,7 @@ SIGNATURES = {
     "qz_sim_create": [C.c_void_p, C.POINTER(SweepParams), C.POINTER(C.c_void_p)],
     "qz_sim_destroy": [C.c_void_p],
     "qz_sim_add_beam": [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double],
+    "qz_sim_add_analytic_beam": [C.c_void_p, C.POINTER(AnalyticBeam)],
     "qz_sim_run": [C.c_void_p, C.c_int, C.c_double, _dp, C.c_void_p],
     "qz_sim_fields": [C.c_void_p, _dp, _dp],
     "qz_sim_beam": [C.c_void_p, C.c_int, _dp],

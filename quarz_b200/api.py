@@ -11,7 +11,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import deck as _deck
-from ._lib import BeamView, Box, Counters, QZError, Species, SweepParams, check, lib
+from ._lib import AnalyticBeam, BeamView, Box, Counters, QZError, Species, SweepParams, check, lib
 
 _dp = C.POINTER(C.c_double)
 
@@ -81,6 +81,7 @@ def sweep_params(spec: "_deck.RunSpec") -> SweepParams:
     p.K = spec.K
     p.ngp = 1 if spec.ngp else 0
     p.neutralize = 1 if spec.neutralize else 0
+    p.smooth_length = float(getattr(spec, "smooth_length", 0.0))
     if len(spec.species) > 4:
         raise QZError(1, "at most 4 plasma species")
     p.nspecies = len(spec.species)
@@ -177,6 +178,12 @@ class BeamOps:
         return st.value
 
     @staticmethod
+    def deposit_analytic(grid: RadialGrid, b: "_deck.BeamSpec", box: Box, bsrc, stream=None):
+        """qz_beam_deposit_analytic: adds an analytic beam's sources to bsrc."""
+        a = analytic_beam(b)
+        check(lib().qz_beam_deposit_analytic(grid.h, C.byref(a), C.byref(box), _dev(bsrc), _stream_ptr(stream)))
+
+    @staticmethod
     def sums(cols, gref, xiref, out17, stream=None):
         v = BeamOps.view(cols, -1.0, 1.0)
         check(lib().qz_beam_sums(C.byref(v), gref, xiref, _dev(out17), _stream_ptr(stream)))
@@ -201,14 +208,29 @@ def sample_gaussian(n0, sr, xi0, sxi, gamma0, espread, emit, cut, cx0, cy0, cxs,
 
 
 def sample_beam(b: "_deck.BeamSpec"):
+    """The beam's particles (n, 7), gref, xiref; an analytic beam has none."""
+    if b.analytic:
+        return np.zeros((0, 7)), 0.0, 0.0
     a = _deck.sampler_args(b)
     a["np_"] = a.pop("np")
     return sample_gaussian(**a)
 
 
+def analytic_beam(b: "_deck.BeamSpec") -> AnalyticBeam:
+    """qz_analytic_beam of an analytic deck beam, in internal coordinates."""
+    flat = b.sigma_xi <= 0
+    return AnalyticBeam(q=b.q, n0=b.n0, sigma_r=b.sigma_r, xi0=0.0 - b.xi0_user, sigma_xi=0.0 if flat else b.sigma_xi,
+                        flattop=1 if flat else 0, length=b.flattop_length,
+                        xi_cut=(0.0 - b.xi_cut_head_user) if b.xi_cut_head_user is not None else -1e300,
+                        x0=b.x0, y0=b.y0, x_slope=-b.x_slope, y_slope=-b.y_slope, gamma=b.gamma)
+
+
 # ---------------------------------------------------------------- whole time steps
 class Simulation:
-    """Simulation::run for constant dt on one GPU (qz_sim): sweeps, moments, fused push + deposit."""
+    """Simulation::run for constant dt on one GPU (qz_sim): sweeps, moments, fused push + deposit.
+
+    Beams are indexed as in the deck. Analytic beams have no particles: their moment rows are zero and their
+    adjoint has no rows; inside qz_sim they are static sources, not beams."""
 
     def __init__(self, spec: "_deck.RunSpec", beams: Optional[List[Tuple[np.ndarray, float, float]]] = None):
         self.spec = spec
@@ -218,19 +240,41 @@ class Simulation:
         check(lib().qz_sim_create(self.grid.h, C.byref(self.params), C.byref(h)))
         self.h = h
         self.beam_data = []
+        self._cidx = []                 # deck beam -> index of the particle beam in qz_sim (None: analytic)
         for i, b in enumerate(spec.beams):
+            if b.analytic:
+                a = analytic_beam(b)
+                check(lib().qz_sim_add_analytic_beam(self.h, C.byref(a)))
+                self.beam_data.append((np.zeros((0, 7)), 0.0, 0.0))
+                self._cidx.append(None)
+                continue
             parts, gref, xiref = beams[i] if beams is not None else sample_beam(b)
             parts = np.ascontiguousarray(parts, dtype=np.float64)
             self.beam_data.append((parts, gref, xiref))
             check(lib().qz_sim_add_beam(self.h, _p(parts), len(parts), b.q, b.m, 1 if b.rigid else 0, gref, xiref))
+            self._cidx.append(sum(c is not None for c in self._cidx))
+        self._pb = [i for i, c in enumerate(self._cidx) if c is not None]   # deck indices of particle beams
         self.fnc = 18 if spec.modes else 6
         self.dnc = 9 if spec.modes else 3
 
+    def _expand(self, mom_c: np.ndarray) -> np.ndarray:
+        """moments of the particle beams (steps, npb, 17) -> one row per deck beam (analytic rows zero)"""
+        out = np.zeros((mom_c.shape[0], len(self.spec.beams), 17))
+        for c, i in enumerate(self._pb):
+            out[:, i] = mom_c[:, c]
+        return out
+
+    def _c(self, b: int) -> int:
+        c = self._cidx[b]
+        if c is None:
+            raise QZError(1, f"beam {b} is analytic: it has no particles")
+        return c
+
     def run(self, nsteps: int, dt: float, stream=None) -> np.ndarray:
-        nb = len(self.spec.beams)
+        nb = len(self._pb)
         mom = np.zeros((nsteps + 1, max(nb, 1), 17))
         check(lib().qz_sim_run(self.h, int(nsteps), float(dt), _p(mom) if nb else None, _stream_ptr(stream)))
-        return mom[:, :nb, :]
+        return self._expand(mom[:, :nb, :])
 
     def set_schedule(self, pipelined: bool = True, sweep_ctas: int = 0, bucket: int = 0, span: int = 0,
                      timeout_s: float = 0.0):
@@ -255,9 +299,9 @@ class Simulation:
         """qz_sim_set_beam: beam b's particles from a (7, n) float64 array, numpy (host) or torch (device)."""
         if isinstance(cols, np.ndarray):
             cols = np.ascontiguousarray(cols, dtype=np.float64)
-            check(lib().qz_sim_set_beam(self.h, int(b), cols.ctypes.data, 0, _stream_ptr(stream)))
+            check(lib().qz_sim_set_beam(self.h, self._c(int(b)), cols.ctypes.data, 0, _stream_ptr(stream)))
         else:
-            check(lib().qz_sim_set_beam(self.h, int(b), _dev(cols), 1, _stream_ptr(stream)))
+            check(lib().qz_sim_set_beam(self.h, self._c(int(b)), _dev(cols), 1, _stream_ptr(stream)))
 
     def trace(self, enable: bool = True) -> np.ndarray:
         """Timeline of the last pipelined run (qz_sim_trace): per step (start, end, 16 progress marks, longest
@@ -271,14 +315,15 @@ class Simulation:
         return v[:-6].reshape(-1, 22), v[-6:]
 
     def run_host(self, nsteps: int, dt: float, cols_host, stream=None) -> np.ndarray:
-        """qz_sim_run_host: beams in host memory (list of (7, n) float64 arrays, updated in place)."""
-        nb = len(self.spec.beams)
+        """qz_sim_run_host: the particle beams in host memory (list of (7, n) float64 arrays in deck order,
+        analytic beams left out, updated in place)."""
+        nb = len(self._pb)
         ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) if isinstance(c, np.ndarray) else int(c.data_ptr())
                                            for c in cols_host])
         mom = np.zeros((nsteps + 1, max(nb, 1), 17))
         check(lib().qz_sim_run_host(self.h, int(nsteps), float(dt), ptrs, _p(mom) if nb else None,
                                     _stream_ptr(stream)))
-        return mom[:, :nb, :]
+        return self._expand(mom[:, :nb, :])
 
     def timing(self, enable: bool = True) -> np.ndarray:
         """qz_sim_timing: the 16 phase-cycle counters of the stand-alone sweeps; enables or disables them."""
@@ -291,42 +336,47 @@ class Simulation:
         pass. lamS (nbeams, 17): the adjoint of the last step's moment sums. Returns (per beam its (n, 7)
         adjoint of the initial particles (x y px py pz xi w), the forward's moment sums, (forward ms,
         reverse ms))."""
-        nb = len(self.spec.beams)
-        seeds = np.ascontiguousarray(np.asarray(lamS, dtype=np.float64).reshape(nb, 17))
-        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nb)]
-        ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) for c in cols])
+        nbd = len(self.spec.beams)
+        seeds_d = np.asarray(lamS, dtype=np.float64).reshape(nbd, 17)
+        pb = self._pb
+        nb = len(pb)
+        seeds = np.ascontiguousarray(seeds_d[pb] if nb else np.zeros((1, 17)))
+        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nbd)]
+        ptrs = (C.c_void_p * max(nb, 1))(*[int(cols[b].ctypes.data) for b in pb])
         mom = np.zeros((nsteps + 1, max(nb, 1), 17))
         ms = np.zeros(2)
         check(lib().qz_sim_adjoint(self.h, int(nsteps), float(dt), _p(seeds), ptrs, _p(mom), _p(ms),
                                    _stream_ptr(stream)))
-        return [c.T.copy() for c in cols], mom[:, :nb, :], (float(ms[0]), float(ms[1]))
+        return [c.T.copy() for c in cols], self._expand(mom[:, :nb, :]), (float(ms[0]), float(ms[1]))
 
     def adjoint_fn(self, nsteps: int, dt: float, seed_fn, stream=None):
         """qz_sim_adjoint_fn: as adjoint(), with the seed computed after the forward by
         seed_fn(moments ((nsteps+1), nbeams, 17)) -> (nbeams, 17)."""
-        nb = len(self.spec.beams)
+        nbd = len(self.spec.beams)
+        pb = self._pb
+        nb = len(pb)
         SEED = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.c_int, C.c_int, C.POINTER(C.c_double), C.c_void_p)
         err = []
 
         def _cb(mom_p, ns, nbm, out_p, _user):
             try:
                 mom = np.ctypeslib.as_array(mom_p, shape=((ns + 1) * nbm * 17,)).reshape(ns + 1, nbm, 17).copy()
-                seeds = np.asarray(seed_fn(mom), dtype=np.float64).reshape(nbm * 17)
+                seeds = np.asarray(seed_fn(self._expand(mom)), dtype=np.float64).reshape(nbd, 17)[pb]
                 out = np.ctypeslib.as_array(out_p, shape=(nbm * 17,))
-                out[:] = seeds
+                out[:] = seeds.reshape(nbm * 17)
             except Exception as e:                      # a Python error must not unwind through C
                 err.append(e)
 
         cb = SEED(_cb)
-        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nb)]
-        ptrs = (C.c_void_p * max(nb, 1))(*[int(c.ctypes.data) for c in cols])
+        cols = [np.zeros((7, len(self.beam_data[b][0]))) for b in range(nbd)]
+        ptrs = (C.c_void_p * max(nb, 1))(*[int(cols[b].ctypes.data) for b in pb])
         mom = np.zeros((nsteps + 1, max(nb, 1), 17))
         ms = np.zeros(2)
         check(lib().qz_sim_adjoint_fn(self.h, int(nsteps), float(dt), C.cast(cb, C.c_void_p), None, ptrs, _p(mom),
                                       _p(ms), _stream_ptr(stream)))
         if err:
             raise err[0]
-        return [c.T.copy() for c in cols], mom[:, :nb, :], (float(ms[0]), float(ms[1]))
+        return [c.T.copy() for c in cols], self._expand(mom[:, :nb, :]), (float(ms[0]), float(ms[1]))
 
     def fields(self):
         K, M = self.spec.K, self.spec.M
@@ -338,7 +388,8 @@ class Simulation:
     def beam(self, b: int) -> np.ndarray:
         n = len(self.beam_data[b][0])
         out = np.zeros((n, 7))
-        check(lib().qz_sim_beam(self.h, b, _p(out)))
+        if self._cidx[b] is not None:
+            check(lib().qz_sim_beam(self.h, self._cidx[b], _p(out)))
         return out
 
     def lost(self) -> int:

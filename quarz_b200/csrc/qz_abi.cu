@@ -235,12 +235,14 @@ struct qz_sweep {
     double* d_bg = nullptr;
     double* d_ps = nullptr;
     double* d_bgs = nullptr;              // modes = 1: background (3, M) and two source buffers (2 x 30, M)
+    double* d_fconsts = nullptr;          // smoothing filter: Thomas factors of F0 and F1 (6 x M)
     unsigned long long* d_cnt = nullptr;
     unsigned long long* d_tim = nullptr;
     bool timing = false;
     qzb::SweepArgs base{};
     ~qz_sweep() {
-        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_bgs, (void*)d_cnt, (void*)d_tim})
+        for (void* q : {(void*)d_pinit, (void*)d_bg, (void*)d_ps, (void*)d_bgs, (void*)d_cnt, (void*)d_tim,
+                        (void*)d_fconsts})
             if (q) cudaFree(q);
     }
 };
@@ -278,6 +280,40 @@ void load_species(const qz_grid& g, const qz_species& sp, std::vector<double> co
     }
 }
 
+// Thomas factors 1/u, -a/u, -c/u (3 x M) of the smoothing filter F_n with a^2 in every cell
+// (FieldSolver::set_filter, src/FieldSolver.cpp:111-146): n = 0 in flux form on the node volumes with a
+// zero-flux wall, n = 1 as the finite-volume L_1 with a^2 inside the flux and identity rows 0 and N
+void filter_factors(const qz_grid& g, double a2, int n, double* out) {
+    const int N = g.N, M = N + 1;
+    std::vector<double> a(M, 0.0), b(M, 1.0), c(M, 0.0);
+    if (n == 0) {
+        for (int j = 0; j <= N; ++j) {
+            const double invV = 2 * PI / g.V[j];
+            const double am = (j > 0) ? a2 * g.rmid[j - 1] / g.h[j - 1] * invV : 0.0;
+            const double cp = (j < N) ? a2 * g.rmid[j] / g.h[j] * invV : 0.0;
+            a[j] = -am; c[j] = -cp; b[j] = 1 + am + cp;
+        }
+    } else {
+        for (int j = 1; j < N; ++j) {
+            const double dV = 0.5 * (g.h[j] + g.h[j - 1]);
+            const double pre = std::pow(g.r[j], n - 1) / dV;
+            const double kpj = a2 / (g.h[j] * std::pow(g.rmid[j], 2 * n - 1));
+            const double kpm = a2 / (g.h[j - 1] * std::pow(g.rmid[j - 1], 2 * n - 1));
+            c[j] = -pre * std::pow(g.r[j + 1], n) * kpj;
+            a[j] = -pre * std::pow(g.r[j - 1], n) * kpm;
+            b[j] = 1 + pre * std::pow(g.r[j], n) * (kpj + kpm);
+        }
+    }
+    double cp = 0.0;
+    for (int i = 0; i < M; ++i) {
+        const double rr = 1.0 / (b[i] - (i > 0 ? a[i] * cp : 0.0));
+        cp = c[i] * rr;
+        out[i] = rr;
+        out[(size_t)M + i] = -rr * a[i];
+        out[(size_t)2 * M + i] = -cp;
+    }
+}
+
 }  // namespace
 
 extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p, qz_sweep** out) {
@@ -288,6 +324,10 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     if (p->modes == 1 && p->picard < 1) return fail(QZ_ERR_ARG, "solver.picard must be >= 1");
     if (p->K < 1 || !(p->dxi > 0)) return fail(QZ_ERR_ARG, "xi: need K >= 1 and dxi > 0");
     if (p->nspecies < 0 || p->nspecies > 4) return fail(QZ_ERR_ARG, "nspecies must be 0..4");
+    if (!(p->smooth_length >= 0)) return fail(QZ_ERR_ARG, "plasma.smooth_length must be >= 0");
+    const bool filter = p->smooth_length > 0;
+    if (filter && p->modes == 1)
+        return fail(QZ_ERR_UNSUPPORTED, "plasma.smooth_length: the smoothing filter is on this path for modes = 0");
     const int M = g->M;
     int dev = 0, optin = 0;
     QZ_CUDA(cudaGetDevice(&dev));
@@ -297,14 +337,14 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     static const bool kLayouts[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
     int lay = -1;
     for (int i = 0; i < 4 && lay < 0; ++i)
-        if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1]) <= (size_t)optin) lay = i;
+        if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1], filter) <= (size_t)optin) lay = i;
     const int rpt = (M + qzb::kSweepThreads - 1) / qzb::kSweepThreads;
     if (p->modes == 1 && (M > qzb::kSweepThreads || qzb::sweep_m1_smem_bytes(M) > (size_t)optin))
         return fail(QZ_ERR_SIZE, "qz_sweep_create: the modes = 1 sweep holds one radial node per thread: M = " +
                                      std::to_string(M) + " > " + std::to_string(qzb::kSweepThreads));
     if (lay < 0 || rpt > 4)
         return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " is too large for one CTA (" +
-                                     std::to_string(qzb::sweep_m0_smem_bytes(M, false, false)) + " B of shared memory, "
+                                     std::to_string(qzb::sweep_m0_smem_bytes(M, false, false, filter)) + " B of shared memory, "
                                      "the device allows " + std::to_string(optin) + ")");
     qz_sweep* s = new (std::nothrow) qz_sweep;
     if (!s) return fail(QZ_ERR_NOMEM, "qz_sweep_create: out of host memory");
@@ -392,6 +432,21 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     A.consts1 = g->d_consts1;
     A.bgs = s->d_bgs;
     A.srcs = s->d_bgs + 3 * (size_t)M;
+    A.filter = 0;
+    A.fconsts = nullptr;
+    A.bstat = nullptr;
+    if (filter) {
+        std::vector<double> fc((size_t)6 * M);
+        const double a2 = p->smooth_length * p->smooth_length;
+        filter_factors(*g, a2, 0, fc.data());
+        filter_factors(*g, a2, 1, fc.data() + (size_t)3 * M);
+        if ((st = dev_upload(&s->d_fconsts, fc))) {
+            delete s;
+            return st;
+        }
+        A.filter = 1;
+        A.fconsts = s->d_fconsts;
+    }
     *out = s;
     return QZ_OK;
 }
@@ -481,6 +536,43 @@ extern "C" qz_status qz_beam_deposit(const qz_grid* g, const qz_beam_view* b, co
     if (qz_status st = check_beam(g, b, box)) return st;
     if (!bsrc) return fail(QZ_ERR_ARG, "qz_beam_deposit: null bsrc");
     QZ_CUDA(qzb::launch_beam_deposit(beam_args(g, b, box), bsrc, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+namespace {
+
+qz_status analytic_args(const qz_grid* g, const qz_analytic_beam* b, const qz_box* box, qzb::AnalyticArgs& P) {
+    if (!g || !b || !box) return fail(QZ_ERR_ARG, "analytic beam: null pointer");
+    if (box->modes != 0 && box->modes != 1) return fail(QZ_ERR_ARG, "analytic beam: modes must be 0 or 1");
+    if (box->K < 1 || !(box->dxi > 0)) return fail(QZ_ERR_ARG, "analytic beam: need K >= 1 and dxi > 0");
+    if (!(b->sigma_r > 0) || !(b->gamma >= 1) || (b->flattop ? !(b->length >= 0) : !(b->sigma_xi > 0)))
+        return fail(QZ_ERR_ARG, "analytic beam: need sigma_r > 0, gamma >= 1 and sigma_xi > 0 (or length >= 0)");
+    if (box->modes == 0 && (b->x0 != 0 || b->y0 != 0 || b->x_slope != 0 || b->y_slope != 0))
+        return fail(QZ_ERR_ARG, "analytic beam: transverse offsets/tilts need azimuthal mode 1 (modes = 1)");
+    P.q = b->q; P.n0 = b->n0; P.s2 = b->sigma_r * b->sigma_r;
+    P.xi0 = b->xi0; P.sxi = b->sigma_xi; P.len = b->length; P.cut = b->xi_cut;
+    P.x0 = b->x0; P.y0 = b->y0; P.xs = b->x_slope; P.ys = b->y_slope;
+    P.vz = std::sqrt(1.0 - 1.0 / (b->gamma * b->gamma));
+    P.omvz = 1.0 / (b->gamma * b->gamma * (1.0 + P.vz));
+    P.flat = b->flattop ? 1 : 0;
+    P.m1 = box->modes;
+    P.r = g->d_r;
+    P.M = g->M;
+    P.K = box->K;
+    P.bnc = box->modes ? 15 : 5;
+    P.xi_min = box->xi_min;
+    P.dxi = box->dxi;
+    return QZ_OK;
+}
+
+}  // namespace
+
+extern "C" qz_status qz_beam_deposit_analytic(const qz_grid* g, const qz_analytic_beam* b, const qz_box* box,
+                                              double* bsrc, void* stream) {
+    qzb::AnalyticArgs P;
+    if (qz_status st = analytic_args(g, b, box, P)) return st;
+    if (!bsrc) return fail(QZ_ERR_ARG, "qz_beam_deposit_analytic: null bsrc");
+    QZ_CUDA(qzb::launch_deposit_analytic(P, bsrc, (cudaStream_t)stream));
     return QZ_OK;
 }
 
@@ -643,6 +735,8 @@ struct qz_sim {
     qz_sweep_params p{};
     int fnc = 6, bnc = 5, dnc = 3;
     double *d_fld = nullptr, *d_diag = nullptr, *d_bsrc[2] = {nullptr, nullptr}, *d_mom = nullptr;
+    double* d_bstat = nullptr;   // sources of the analytic rigid beams (K, M, B_NC), added by every sweep
+    int nanalytic = 0;
     int cur = 0;
     bool bsrc_valid = false;
     struct Beam {
@@ -696,7 +790,7 @@ struct qz_sim {
         for (auto& b : beams)
             for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
                 if (q) cudaFree(q);
-        for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom, pipe.fld, pipe.diag, pipe.bsrc, pipe.ps,
+        for (double* q : {d_fld, d_diag, d_bsrc[0], d_bsrc[1], d_mom, d_bstat, pipe.fld, pipe.diag, pipe.bsrc, pipe.ps,
                           pipe.m1s, pipe.pmom, pipe.mom})
             if (q) cudaFree(q);
         for (void* q : {(void*)pipe.sync, (void*)pipe.bk, (void*)pipe.sort.keys[0], (void*)pipe.sort.keys[1],
@@ -734,6 +828,27 @@ extern "C" qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, q
 
 extern "C" qz_status qz_sim_destroy(qz_sim* s) {
     delete s;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_add_analytic_beam(qz_sim* s, const qz_analytic_beam* b) {
+    if (!s || !b) return fail(QZ_ERR_ARG, "qz_sim_add_analytic_beam: null pointer");
+    qz_box box;
+    box.xi_min = s->p.xi_min; box.dxi = s->p.dxi; box.K = s->p.K; box.ngp = s->p.ngp; box.modes = s->p.modes;
+    qzb::AnalyticArgs P;
+    if (qz_status st = analytic_args(s->g, b, &box, P)) return st;
+    const size_t n = (size_t)s->p.K * s->g->M * s->bnc;
+    if (!s->d_bstat) {
+        if (cudaMalloc((void**)&s->d_bstat, sizeof(double) * n) != cudaSuccess) {
+            s->d_bstat = nullptr;
+            return fail(QZ_ERR_NOMEM, "qz_sim_add_analytic_beam: device allocation failed");
+        }
+        QZ_CUDA(cudaMemset(s->d_bstat, 0, sizeof(double) * n));
+    }
+    QZ_CUDA(qzb::launch_deposit_analytic(P, s->d_bstat, nullptr));
+    QZ_CUDA(cudaDeviceSynchronize());
+    s->sw->base.bstat = s->d_bstat;
+    ++s->nanalytic;
     return QZ_OK;
 }
 
@@ -1103,7 +1218,7 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
     if (!(dt > 0.0)) return fail(QZ_ERR_ARG, "qz_sim_run: dt must be positive");
     cudaStream_t st = (cudaStream_t)stream;
-    if (s->pipe.enabled) return run_pipelined(s, nsteps, dt, mom_host, st);
+    if (s->pipe.enabled && !s->beams.empty()) return run_pipelined(s, nsteps, dt, mom_host, st);
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 
@@ -1296,6 +1411,8 @@ qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, dou
     const qzb::SweepArgs& base = s->sw->base;
     if (s->p.modes != 0 || s->p.ngp || s->p.K < 2)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2");
+    if (base.filter)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: the smoothing filter (plasma.smooth_length) has no adjoint");
     if (base.M > qzb::kSweepThreads || base.np > qzb::kSweepThreads || base.nsp != 1)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
                                         "particles per slice");
@@ -1663,6 +1780,9 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         !m || !rigid || !gref || !xiref)))
         return fail(QZ_ERR_ARG, "qz_batch_add: bad argument (at most 2 beams per instance)");
     if (p->modes != 0 && p->modes != 1) return fail(QZ_ERR_ARG, "qz_batch_add: modes must be 0 or 1");
+    if (p->smooth_length != 0)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_batch_add: the smoothing filter (plasma.smooth_length) is not in the "
+                                        "batched sweep; run such instances with qz_sim");
     if (p->modes == 1 && M > qzb::kSweepThreads)
         return fail(QZ_ERR_SIZE, "qz_batch_add: modes = 1 instances need M <= 512 (one radial row per thread)");
     if (b->ord && p->ab_order != b->ord) return fail(QZ_ERR_ARG, "qz_batch_add: every instance needs the same AB order");

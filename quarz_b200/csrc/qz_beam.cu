@@ -26,6 +26,60 @@ __global__ void __launch_bounds__(kBeamThreads) beam_deposit_kernel(const BeamAr
     }
 }
 
+// e^{-z} I0(z), e^{-z} I1(z) by the polynomial approximations of Abramowitz & Stegun 9.8.1-9.8.4
+// (relative error below 2e-7; the reference's choice, src/Beam.cpp:215-234)
+__device__ __forceinline__ void bessel_i01_scaled(double z, double& i0, double& i1) {
+    if (z < 3.75) {
+        const double t = (z / 3.75) * (z / 3.75);
+        const double I0 = 1.0 + t * (3.5156229 + t * (3.0899424 + t * (1.2067492 + t * (0.2659732
+                          + t * (0.0360768 + t * 0.0045813)))));
+        const double I1 = z * (0.5 + t * (0.87890594 + t * (0.51498869 + t * (0.15084934 + t * (0.02658733
+                          + t * (0.00301532 + t * 0.00032411))))));
+        const double e = exp(-z);
+        i0 = I0 * e;
+        i1 = I1 * e;
+    } else {
+        const double u = 3.75 / z, sq = 1.0 / sqrt(z);
+        i0 = sq * (0.39894228 + u * (0.01328592 + u * (0.00225319 + u * (-0.00157565 + u * (0.00916281
+             + u * (-0.02057706 + u * (0.02635537 + u * (-0.01647633 + u * 0.00392377))))))));
+        i1 = sq * (0.39894228 + u * (-0.03988024 + u * (-0.00362018 + u * (0.00163801 + u * (-0.01031555
+             + u * (0.02282967 + u * (-0.02895312 + u * (0.01787654 - u * 0.00420059))))))));
+    }
+}
+
+// one thread per (slice, node): the displaced Gaussian's azimuthal modes 0 and 1 through the scaled Bessel
+// functions of z = r d / sigma_r^2, added to rho, rho - J_z = (1 - v_z) rho and J_z = v_z rho
+__global__ void __launch_bounds__(kBeamThreads) deposit_analytic_kernel(const AnalyticArgs P,
+                                                                        double* __restrict__ bsrc) {
+    const long n = (long)P.K * P.M;
+    for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (long)gridDim.x * blockDim.x) {
+        const int k = (int)(t / P.M), j = (int)(t - (long)k * P.M);
+        const double xi = P.xi_min + k * P.dxi;
+        if (xi < P.cut) continue;
+        double fxi;
+        if (P.flat) fxi = (fabs(xi - P.xi0) <= 0.5 * P.len) ? 1.0 : 0.0;
+        else fxi = exp(-0.5 * (xi - P.xi0) * (xi - P.xi0) / (P.sxi * P.sxi));
+        if (fxi == 0.0) continue;
+        const double cx = P.x0 + P.xs * (xi - P.xi0), cy = P.y0 + P.ys * (xi - P.xi0);
+        const double d = sqrt(cx * cx + cy * cy);
+        const double r = P.r[j];
+        double i0, i1;
+        bessel_i01_scaled(r * d / P.s2, i0, i1);
+        const double env = P.q * P.n0 * fxi * exp(-0.5 * (r - d) * (r - d) / P.s2);
+        const double rho0 = env * i0;
+        double* o = bsrc + (size_t)t * P.bnc;
+        o[B_RHO0] += rho0;
+        o[B_RT0] += rho0 * P.omvz;
+        o[B_JZ0] += rho0 * P.vz;
+        if (P.m1 && d > 0.0) {
+            const double f1r = env * i1 * (cx / d), f1i = -env * i1 * (cy / d);
+            o[B_RHO1R] += f1r; o[B_RHO1I] += f1i;
+            o[B_RT1R] += f1r * P.omvz; o[B_RT1I] += f1i * P.omvz;
+            o[B_JZ1R] += f1r * P.vz; o[B_JZ1I] += f1i * P.vz;
+        }
+    }
+}
+
 template <bool kDeposit>
 __global__ void __launch_bounds__(kBeamThreads) beam_push_kernel(const BeamArgs B, const double* __restrict__ fld,
                                                                  double dt_kick, double dt, int move,
@@ -135,6 +189,13 @@ int beam_sums_blocks(long n) {
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s) {
     if (B.n <= 0) return cudaSuccess;
     beam_deposit_kernel<<<grid_for(B.n), kBeamThreads, 0, s>>>(B, bsrc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_deposit_analytic(const AnalyticArgs& P, double* bsrc, cudaStream_t s) {
+    const long n = (long)P.K * P.M;
+    if (n <= 0) return cudaSuccess;
+    deposit_analytic_kernel<<<grid_for(n), kBeamThreads, 0, s>>>(P, bsrc);
     return cudaGetLastError();
 }
 

@@ -50,9 +50,16 @@ struct SweepArgs {
     // optional, m = 0 (the adjoint's recomputation): the plasma state at the start of every slice,
     // (K, 6 + 5 * ord, npad): x y px py Delta w, then the AB history h[m][v] (m pushes ago)
     double* traj;
+    // optional, m = 0: radial smoothing of the plasma sources (plasma.smooth_length,
+    // src/Simulation.cpp:63-66, :685-690, :810-835)
+    int filter;
+    const double* fconsts;          // 6 x M: Thomas factors 1/u, -a/u, -c/u of F0, then of F1
+    // optional: beam sources that do not change between steps (analytic rigid beams), (K, M, B_NC),
+    // added to bsrc wherever the sweep reads it
+    const double* bstat;
 };
 
-size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem);
+size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter = false);
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
 // the modes = 1 sweep: one CTA, one radial row per thread (M <= kSweepThreads), plasma in A.ps
 size_t sweep_m1_smem_bytes(int M);
@@ -82,6 +89,15 @@ struct BeamArgs {
 };
 
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s);
+// Beam::deposit_analytic (src/Beam.cpp:236-279): a rigid beam's sources at every (slice, node)
+struct AnalyticArgs {
+    double q, n0, s2, xi0, sxi, len, cut, x0, y0, xs, ys, vz, omvz;
+    int flat, m1;
+    const double* r;            // nodes [M] (device)
+    int M, K, bnc;
+    double xi_min, dxi;
+};
+cudaError_t launch_deposit_analytic(const AnalyticArgs& P, double* bsrc, cudaStream_t s);
 cudaError_t launch_beam_push(const BeamArgs& B, const double* fld, double dt_kick, double dt_drift, int move,
                              cudaStream_t s);
 cudaError_t launch_beam_push_deposit(const BeamArgs& B, const double* fld, double dt_kick, double dt_drift,
@@ -153,7 +169,7 @@ struct PipeArgs {
 constexpr int kTraceStride = 22;
 constexpr int kWorkerTotals = 6;    // trace totals of the push workers after the steps
 
-size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter = false);
 // resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count
 int pipeline_max_grid(const PipeArgs& P, int* sms);
 // cooperative launch of grid CTAs (fails unless all of them can be resident at once)

@@ -156,7 +156,7 @@ struct PipeGate {
     }
 };
 
-template <int MODES, int ORD, bool REG, int kMaxR>
+template <int MODES, int ORD, bool REG, int kMaxR, bool EXT>
 __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
     __shared__ int s_ok;
     __shared__ GateState gs;
@@ -177,7 +177,8 @@ __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
         if (!s_ok) return;
         if (P.trace && tid == 0) P.trace[(size_t)kTraceStride * n] = gtimer();
         PipeGate g{&P, &gs};
-        const bool ok = MODES == 1 ? sweep_m1_body<ORD>(P.sw, smem, g) : sweep_body<ORD, REG, kMaxR>(P.sw, smem, g);
+        const bool ok = MODES == 1 ? sweep_m1_body<ORD>(P.sw, smem, g)
+                                   : sweep_body<ORD, REG, kMaxR, PipeGate, EXT>(P.sw, smem, g);
         if (!ok) return;
         // the last row (the others were zeroed slice by slice)
         const int nr = M * P.bnc;
@@ -458,11 +459,12 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     }
 }
 
-template <int MODES, int ORD, bool REG, int kMaxR>
+// EXT: the variant whose sweeps handle the smoothing filter and static (analytic) beam sources
+template <int MODES, int ORD, bool REG, int kMaxR, bool EXT = false>
 __global__ void __launch_bounds__(kSweepThreads, 1) pipeline_kernel(const __grid_constant__ PipeArgs P) {
     extern __shared__ double smem_raw[];
     if ((int)blockIdx.x < P.nsweep)
-        sweep_role<MODES, ORD, REG, kMaxR>(P, smem_raw);
+        sweep_role<MODES, ORD, REG, kMaxR, EXT>(P, smem_raw);
     else
         worker_role(P, smem_raw);
 }
@@ -477,18 +479,18 @@ __global__ void moments_reduce_kernel(const __grid_constant__ PipeArgs P, double
     mom[((size_t)n * P.nbeams + q) * 17 + c] = v;
 }
 
-template <int MODES, int ORD, bool REG, int RM>
+template <int MODES, int ORD, bool REG, int RM, bool EXT = false>
 cudaError_t launch_t(const PipeArgs& P, int grid, size_t smem, cudaStream_t stream) {
-    auto fn = pipeline_kernel<MODES, ORD, REG, RM>;
+    auto fn = pipeline_kernel<MODES, ORD, REG, RM, EXT>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&P};
     return cudaLaunchCooperativeKernel((const void*)fn, dim3(grid), dim3(kSweepThreads), args, smem, stream);
 }
 
-template <int MODES, int ORD, bool REG, int RM>
+template <int MODES, int ORD, bool REG, int RM, bool EXT = false>
 int occupancy_t(size_t smem) {
-    auto fn = pipeline_kernel<MODES, ORD, REG, RM>;
+    auto fn = pipeline_kernel<MODES, ORD, REG, RM, EXT>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, smem) != cudaSuccess) return 0;
@@ -496,22 +498,32 @@ int occupancy_t(size_t smem) {
 }
 
 // modes = 1 runs one row per thread with the plasma in the scratch (REG and kMaxR unused: false, 1)
+template <int ORD, bool EXT>
+cudaError_t launch_e(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
+    const bool reg = P.sw.np <= kSweepThreads;
+    if (P.sw.rows_per_thread == 1)
+        return reg ? launch_t<0, ORD, true, 1, EXT>(P, grid, smem, s) : launch_t<0, ORD, false, 1, EXT>(P, grid, smem, s);
+    return reg ? launch_t<0, ORD, true, 4, EXT>(P, grid, smem, s) : launch_t<0, ORD, false, 4, EXT>(P, grid, smem, s);
+}
+
 template <int ORD>
 cudaError_t launch_o(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
     if (P.modes == 1) return launch_t<1, ORD, false, 1>(P, grid, smem, s);
+    return (P.sw.filter || P.sw.bstat) ? launch_e<ORD, true>(P, grid, smem, s) : launch_e<ORD, false>(P, grid, smem, s);
+}
+
+template <int ORD, bool EXT>
+int occupancy_e(const PipeArgs& P, size_t smem) {
     const bool reg = P.sw.np <= kSweepThreads;
     if (P.sw.rows_per_thread == 1)
-        return reg ? launch_t<0, ORD, true, 1>(P, grid, smem, s) : launch_t<0, ORD, false, 1>(P, grid, smem, s);
-    return reg ? launch_t<0, ORD, true, 4>(P, grid, smem, s) : launch_t<0, ORD, false, 4>(P, grid, smem, s);
+        return reg ? occupancy_t<0, ORD, true, 1, EXT>(smem) : occupancy_t<0, ORD, false, 1, EXT>(smem);
+    return reg ? occupancy_t<0, ORD, true, 4, EXT>(smem) : occupancy_t<0, ORD, false, 4, EXT>(smem);
 }
 
 template <int ORD>
 int occupancy_o(const PipeArgs& P, size_t smem) {
     if (P.modes == 1) return occupancy_t<1, ORD, false, 1>(smem);
-    const bool reg = P.sw.np <= kSweepThreads;
-    if (P.sw.rows_per_thread == 1)
-        return reg ? occupancy_t<0, ORD, true, 1>(smem) : occupancy_t<0, ORD, false, 1>(smem);
-    return reg ? occupancy_t<0, ORD, true, 4>(smem) : occupancy_t<0, ORD, false, 4>(smem);
+    return (P.sw.filter || P.sw.bstat) ? occupancy_e<ORD, true>(P, smem) : occupancy_e<ORD, false>(P, smem);
 }
 
 // ---------------------------------------------------------------- ordering the beam by (xi cell, r cell)
@@ -632,8 +644,8 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
     return cudaGetLastError();
 }
 
-size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem) {
-    const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter) {
+    const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem, filter);
     const size_t worker = sizeof(double) * (3 * (size_t)M + (size_t)(kSweepThreads / 32) * 17 * 32) + 64;
     return sweep > worker ? sweep : worker;
 }
@@ -643,7 +655,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0);
     int per = 0;
     switch (P.sw.ord) {
         case 1: per = occupancy_o<1>(P, smem); break;
@@ -659,7 +671,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
 cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream) {
     if (P.sw.rows_per_thread < 1 || P.sw.rows_per_thread > 4) return cudaErrorInvalidValue;
     if (P.nsweep < 1 || grid <= P.nsweep || P.ring < 2 || P.nbeams > kMaxBeams) return cudaErrorInvalidValue;
-    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0);
     switch (P.sw.ord) {
         case 1: return launch_o<1>(P, grid, smem, stream);
         case 2: return launch_o<2>(P, grid, smem, stream);

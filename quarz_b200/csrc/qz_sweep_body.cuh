@@ -375,6 +375,8 @@ struct Smem {
     double *bgt, *bgr;                                    // neutralising background
     double *psi, *ez, *bz, *wr1, *bpr, *bpi;              // fields of the slice (wr1 = -psi')
     double* tot;                                          // scan scratch, 2 x 8 x kW
+    double* stage;                                        // A.filter: beam + background part of the next slice (4 x M)
+    double* ftot;                                         // A.filter: scan scratch of the filter, 2 x 14 x kW
     int* lost;
     int* flag;                                            // gate result broadcast
 };
@@ -395,6 +397,8 @@ __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
     S.bgt = p; p += M; S.bgr = p; p += M;
     S.psi = p; p += M; S.ez = p; p += M; S.bz = p; p += M; S.wr1 = p; p += M; S.bpr = p; p += M; S.bpi = p; p += M;
     S.tot = p; p += 2 * 8 * kW;
+    S.stage = S.ftot = nullptr;
+    if (A.filter) { S.stage = p; p += 4 * (size_t)M; S.ftot = p; p += 2 * 14 * kW; }
     S.lost = reinterpret_cast<int*>(p);
     S.flag = S.lost + 1;
     return S;
@@ -415,41 +419,158 @@ struct BeamRow { double rt, drt, jz, jt; };
 template <bool kL2>                       // kL2: the rows were written by other SMs, read them from L2
 __device__ __forceinline__ double ldb(const double* p) { return kL2 ? __ldcg(p) : *p; }
 
-template <bool kL2>
+// one beam-source value: the pushed beams' deposit plus, in kernels built for it (kStat), the static
+// (analytic) sources when present
+template <bool kL2, bool kStat>
+__device__ __forceinline__ double ldbs(const SweepArgs& A, const double* bsrc, size_t off) {
+    const double v = ldb<kL2>(bsrc + off);
+    if constexpr (kStat) return A.bstat ? v + __ldg(A.bstat + off) : v;
+    return v;
+}
+
+template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
-    const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC0;
+    const size_t bk = (size_t)k * st + (size_t)j * B_NC0;
     BeamRow r;
-    r.rt = ldb<kL2>(bk + B_RT0);
-    r.jz = ldb<kL2>(bk + B_JZ0);
-    r.jt = ldb<kL2>(bk + B_JP1I);
+    r.rt = ldbs<kL2, kStat>(A, bsrc, bk + B_RT0);
+    r.jz = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ0);
+    r.jt = ldbs<kL2, kStat>(A, bsrc, bk + B_JP1I);
     const int K = A.K;
     if (A.ngp) {
-        const double prev = (k > 0) ? ldb<kL2>(bk + B_RT0 - (ptrdiff_t)st) : 0.0;
+        const double prev = (k > 0) ? ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st) : 0.0;
         r.drt = (r.rt - prev) * A.idxi;
     } else if (K == 1) {
         r.drt = 0.0;
     } else if (k == 0) {
-        r.drt = (ldb<kL2>(bk + st + B_RT0) - r.rt) * A.idxi;
+        r.drt = (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) - r.rt) * A.idxi;
     } else if (k == K - 1) {
-        r.drt = (r.rt - ldb<kL2>(bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
+        r.drt = (r.rt - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st)) * A.idxi;
     } else {
-        r.drt = 0.5 * (ldb<kL2>(bk + st + B_RT0) - ldb<kL2>(bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
+        r.drt = 0.5 * (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st)) * A.idxi;
     }
     return r;
 }
 
-// initial source values of a slice: background + beam; the plasma deposit is added on top
-__device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j, const BeamRow& br) {
-    s.rhot[j] = S.bgt[j] + br.rt;
-    s.drho[j] = br.drt;
-    s.jz[j] = br.jz;
-    s.jpi1[j] = br.jt;
+// initial source values of a slice: background + beam; the plasma deposit is added on top. With the
+// smoothing filter (kernels built with kExt only) the plasma deposit starts from zero and the beam +
+// background part is staged, to be added after the filter (filter_sources).
+template <bool kExt>
+__device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j, const BeamRow& br, int M) {
+    if (kExt && S.stage) {
+        S.stage[j] = S.bgt[j] + br.rt;
+        S.stage[M + j] = br.drt;
+        S.stage[2 * M + j] = br.jz;
+        S.stage[3 * M + j] = br.jt;
+        s.rhot[j] = 0.0;
+        s.drho[j] = 0.0;
+        s.jz[j] = 0.0;
+        s.jpi1[j] = 0.0;
+        s.ni[j] = 0.0;
+    } else {
+        s.rhot[j] = S.bgt[j] + br.rt;
+        s.drho[j] = br.drt;
+        s.jz[j] = br.jz;
+        s.jpi1[j] = br.jt;
+        s.ni[j] = S.bgr[j] > 0.0 ? S.bgr[j] : 0.0;
+    }
     s.chi[j] = 0.0;
     s.ne[j] = 0.0;
-    s.ni[j] = S.bgr[j] > 0.0 ? S.bgr[j] : 0.0;
     s.S1r[j] = 0.0;
     s.S1i[j] = 0.0;
+}
+
+// The radial smoothing filter f <- F_n^{-1} f (FieldSolver::filter, src/FieldSolver.cpp:148-161) of NS
+// shared-memory arrays in place, each with F0 (op 0) or F1 (op 1): Thomas with the host-factored pivots
+// A.fconsts, its two substitutions as block scans over the thread's rows [row0, row0 + Rw). Every thread
+// reads and writes only its own rows; the caller puts a barrier before (the arrays are complete) and, when
+// other threads read them next, after. Kept out of line: only decks with plasma.smooth_length reach it.
+template <int NS>
+struct FilterSet { double* f[NS]; int op[NS]; };
+
+template <int NS, int kMaxR>
+__device__ __noinline__ void filter_rows(const FilterSet<NS> fs, const double* __restrict__ fc, int M, int Rw,
+                                         double* tot) {
+    const int row0 = threadIdx.x * Rw;
+    double a[NS], b[NS], d[kMaxR][NS];
+#pragma unroll
+    for (int e = 0; e < NS; ++e) { a[e] = 1.0; b[e] = 0.0; }
+#pragma unroll
+    for (int u = 0; u < kMaxR; ++u) {
+        const int i = row0 + u;
+#pragma unroll
+        for (int e = 0; e < NS; ++e) {
+            d[u][e] = 0.0;
+            if (u >= Rw || i >= M) continue;
+            const double* F = fc + (size_t)fs.op[e] * 3 * M;
+            d[u][e] = fs.f[e][i];
+            const double rr = F[i], af = F[M + i];
+            b[e] = fma(af, b[e], rr * d[u][e]);
+            a[e] *= af;
+        }
+    }
+    double y[NS];
+    scan_fwd_n<NS>(a, b, y, tot);
+#pragma unroll
+    for (int u = 0; u < kMaxR; ++u) {
+        const int i = row0 + u;
+#pragma unroll
+        for (int e = 0; e < NS; ++e) {
+            if (u >= Rw || i >= M) continue;
+            const double* F = fc + (size_t)fs.op[e] * 3 * M;
+            y[e] = fma(F[M + i], y[e], F[i] * d[u][e]);
+            d[u][e] = y[e];
+        }
+    }
+#pragma unroll
+    for (int e = 0; e < NS; ++e) { a[e] = 1.0; b[e] = 0.0; }
+#pragma unroll
+    for (int u = kMaxR - 1; u >= 0; --u) {
+        const int i = row0 + u;
+        if (u >= Rw || i >= M) continue;
+#pragma unroll
+        for (int e = 0; e < NS; ++e) {
+            const double ab = fc[(size_t)fs.op[e] * 3 * M + 2 * M + i];
+            b[e] = fma(ab, b[e], d[u][e]);
+            a[e] *= ab;
+        }
+    }
+    double x[NS];
+    scan_bwd_n<NS>(a, b, x, tot + 2 * NS * kW);
+#pragma unroll
+    for (int u = kMaxR - 1; u >= 0; --u) {
+        const int i = row0 + u;
+        if (u >= Rw || i >= M) continue;
+#pragma unroll
+        for (int e = 0; e < NS; ++e) {
+            x[e] = fma(fc[(size_t)fs.op[e] * 3 * M + 2 * M + i], x[e], d[u][e]);
+            fs.f[e][i] = x[e];
+        }
+    }
+}
+
+// Simulation::filter_plasma_sources (src/Simulation.cpp:823-835, m = 0) on the plasma deposit of a slice,
+// then the staged beam + background part added as combine_sources does (src/Simulation.cpp:430-437):
+// rho - J_z, its xi-derivative, J_z, chi, n_e, n_i with F0 and J_theta with F1. Ends with a barrier.
+template <int kMaxR>
+__device__ __forceinline__ void filter_sources(const Src& s, const Smem& S, const SweepArgs& A, int Rw) {
+    FilterSet<7> fs;
+    double* arr[7] = {s.rhot, s.drho, s.jz, s.chi, s.ne, s.ni, s.jpi1};
+#pragma unroll
+    for (int e = 0; e < 7; ++e) { fs.f[e] = arr[e]; fs.op[e] = e == 6 ? 1 : 0; }
+    filter_rows<7, kMaxR>(fs, A.fconsts, A.M, Rw, S.ftot);
+    const int M = A.M, row0 = threadIdx.x * Rw;
+#pragma unroll
+    for (int u = 0; u < kMaxR; ++u) {
+        const int i = row0 + u;
+        if (u >= Rw || i >= M) continue;
+        s.rhot[i] += S.stage[i];
+        s.drho[i] += S.stage[M + i];
+        s.jz[i] += S.stage[2 * M + i];
+        s.jpi1[i] += S.stage[3 * M + i];
+        if (S.bgr[i] > 0.0) s.ni[i] += S.bgr[i];
+    }
+    __syncthreads();
 }
 
 // 3-point non-uniform gradient at node i (src/FieldSolver.cpp:263-281); odd: axis value f1/r1
@@ -724,8 +845,10 @@ using namespace sweep_detail;
 
 // One sweep by the calling CTA (all kThreads threads). The gate G orders it against other CTAs when
 // several time steps run concurrently (NoGate: a stand-alone sweep). Returns false if a gate wait
-// gave up (the CTA then stops at the next slice boundary).
-template <int ORD, bool REG, int kMaxR, class Gate>
+// gave up (the CTA then stops at the next slice boundary). EXT: the kernel also handles the smoothing
+// filter (A.filter) and static beam sources (A.bstat); without it both are ignored, and the kernel of
+// plain decks carries none of their code.
+template <int ORD, bool REG, int kMaxR, class Gate, bool EXT = false>
 __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw, Gate& gate) {
     const int M = A.M, N = A.N, K = A.K, Rw = kMaxR == 1 ? 1 : A.rows_per_thread;   // rows per thread
     const int tid = threadIdx.x;
@@ -826,10 +949,26 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     }
     __syncthreads();
     if (Gate::kActive && !*S.flag) return false;
-    for (int j = tid; j < M; j += kThreads) {
-        const Src s0 = src_of(S, M, 0);
-        if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
-        init_sources(s0, S, j, beam_row<Gate::kActive>(A, gate.bsrc(A), 0, j));
+    if (EXT && A.filter) {              // the background is smoothed like the plasma (src/Simulation.cpp:685-690)
+        if (A.neutralize)
+            for (int j = tid; j < M; j += kThreads) {
+                const Src s0 = src_of(S, M, 0);
+                S.bgt[j] -= s0.ne[j];
+                S.bgr[j] -= s0.ne[j];
+            }
+        __syncthreads();
+        FilterSet<2> fb;
+        fb.f[0] = S.bgt; fb.f[1] = S.bgr; fb.op[0] = fb.op[1] = 0;
+        filter_rows<2, kMaxR>(fb, A.fconsts, M, Rw, S.ftot);
+        __syncthreads();
+        for (int j = tid; j < M; j += kThreads)
+            init_sources<EXT>(src_of(S, M, 0), S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M);
+    } else {
+        for (int j = tid; j < M; j += kThreads) {
+            const Src s0 = src_of(S, M, 0);
+            if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
+            init_sources<EXT>(s0, S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M);
+        }
     }
     __syncthreads();
     // deposit of slice 0
@@ -888,13 +1027,15 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         }
         const Src s = src_of(S, M, A.dbuf ? (k & 1) : 0);
         const Src sn = src_of(S, M, A.dbuf ? ((k + 1) & 1) : 0);
+        if constexpr (EXT)
+            if (A.filter) filter_sources<kMaxR>(s, S, A, Rw);
         if (tim && tid == 0) t_sub = clock64();
         // beam rows of slice k+1 for this thread's nodes (consumed below, latency overlaps the solves)
         BeamRow pre[kMaxR];
         if (A.dbuf && k + 1 < K)
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u)
-                if (u < Rw && row0 + u < M) pre[u] = beam_row<Gate::kActive>(A, gate.bsrc(A), k + 1, row0 + u);
+                if (u < Rw && row0 + u < M) pre[u] = beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u);
 
         // ---------------- P2: psi, E_z, B_z with L0 (src/Simulation.cpp:797-807, :501-532)
         {
@@ -982,7 +1123,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             if (A.dbuf && k + 1 < K)
 #pragma unroll
                 for (int u = 0; u < kMaxR; ++u)
-                    if (u < Rw && row0 + u < M) init_sources(sn, S, row0 + u, pre[u]);
+                    if (u < Rw && row0 + u < M) init_sources<EXT>(sn, S, row0 + u, pre[u], M);
             SUB_MARK(8);
         }
         __syncthreads();
@@ -1019,6 +1160,11 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
 
         // ---------------- P4: B+ (src/Simulation.cpp:535-591, m = 0: one pass)
         //   (L1D - chi) B_r0 = -S_i (rows 0, N Dirichlet); (L1F - chi) B_theta0 = J_z' + S_r, flux wall J_z(R)
+        if (EXT && A.filter) {              // S+ smoothed with F1 (src/Simulation.cpp:810-812): the rows of
+            FilterSet<2> fsS;               // this thread, which are the only ones its B+ rows read
+            fsS.f[0] = s.S1r; fsS.f[1] = s.S1i; fsS.op[0] = fsS.op[1] = 1;
+            filter_rows<2, kMaxR>(fsS, A.fconsts, M, Rw, S.ftot);
+        }
         {
             // pivots: product of T_i = [[b_i, -a_i c_{i-1}], [1, 0]] over the thread's rows
             double m[2][4];
@@ -1132,7 +1278,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         if (k + 1 < K) {
             if (!A.dbuf) {
                 __syncthreads();                                    // the store read the sources
-                for (int j = tid; j < M; j += kThreads) init_sources(sn, S, j, beam_row<Gate::kActive>(A, gate.bsrc(A), k + 1, j));
+                for (int j = tid; j < M; j += kThreads)
+                    init_sources<EXT>(sn, S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, j), M);
                 __syncthreads();
             }
             const bool first = (k == 0);

@@ -265,31 +265,32 @@ struct BeamRow1 { double rt[3], drt[3], jz[3], jp[6]; };
 template <bool kL2>
 __device__ __forceinline__ BeamRow1 beam_row1(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC1;
-    const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC1;
+    const size_t bk = (size_t)k * st + (size_t)j * B_NC1;
     BeamRow1 r;
     const int rc[3] = {B_RT0, B_RT1R, B_RT1I};
     const int K = A.K;
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
         const int c = rc[e];
-        r.rt[e] = ldb<kL2>(bk + c);
+        r.rt[e] = ldbs<kL2, true>(A, bsrc, bk + c);
         if (A.ngp) {
-            const double prev = (k > 0) ? ldb<kL2>(bk + c - (ptrdiff_t)st) : 0.0;
+            const double prev = (k > 0) ? ldbs<kL2, true>(A, bsrc, bk + c - st) : 0.0;
             r.drt[e] = (r.rt[e] - prev) * A.idxi;
         } else if (K == 1) {
             r.drt[e] = 0.0;
         } else if (k == 0) {
-            r.drt[e] = (ldb<kL2>(bk + st + c) - r.rt[e]) * A.idxi;
+            r.drt[e] = (ldbs<kL2, true>(A, bsrc, bk + st + c) - r.rt[e]) * A.idxi;
         } else if (k == K - 1) {
-            r.drt[e] = (r.rt[e] - ldb<kL2>(bk + c - (ptrdiff_t)st)) * A.idxi;
+            r.drt[e] = (r.rt[e] - ldbs<kL2, true>(A, bsrc, bk + c - st)) * A.idxi;
         } else {
-            r.drt[e] = 0.5 * (ldb<kL2>(bk + st + c) - ldb<kL2>(bk + c - (ptrdiff_t)st)) * A.idxi;
+            r.drt[e] = 0.5 * (ldbs<kL2, true>(A, bsrc, bk + st + c) - ldbs<kL2, true>(A, bsrc, bk + c - st)) * A.idxi;
         }
     }
-    r.jz[0] = ldb<kL2>(bk + B_JZ0); r.jz[1] = ldb<kL2>(bk + B_JZ1R); r.jz[2] = ldb<kL2>(bk + B_JZ1I);
-    r.jp[0] = ldb<kL2>(bk + B_JP0R); r.jp[1] = ldb<kL2>(bk + B_JP0I);
-    r.jp[2] = ldb<kL2>(bk + B_JP1R); r.jp[3] = ldb<kL2>(bk + B_JP1I);
-    r.jp[4] = ldb<kL2>(bk + B_JP2R); r.jp[5] = ldb<kL2>(bk + B_JP2I);
+    r.jz[0] = ldbs<kL2, true>(A, bsrc, bk + B_JZ0); r.jz[1] = ldbs<kL2, true>(A, bsrc, bk + B_JZ1R);
+    r.jz[2] = ldbs<kL2, true>(A, bsrc, bk + B_JZ1I);
+    r.jp[0] = ldbs<kL2, true>(A, bsrc, bk + B_JP0R); r.jp[1] = ldbs<kL2, true>(A, bsrc, bk + B_JP0I);
+    r.jp[2] = ldbs<kL2, true>(A, bsrc, bk + B_JP1R); r.jp[3] = ldbs<kL2, true>(A, bsrc, bk + B_JP1I);
+    r.jp[4] = ldbs<kL2, true>(A, bsrc, bk + B_JP2R); r.jp[5] = ldbs<kL2, true>(A, bsrc, bk + B_JP2I);
     return r;
 }
 
