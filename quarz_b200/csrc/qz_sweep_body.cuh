@@ -419,35 +419,36 @@ struct BeamRow { double rt, drt, jz, jt; };
 template <bool kL2>                       // kL2: the rows were written by other SMs, read them from L2
 __device__ __forceinline__ double ldb(const double* p) { return kL2 ? __ldcg(p) : *p; }
 
-// one beam-source value: the pushed beams' deposit plus, in kernels built for it (kStat), the static
-// (analytic) sources when present
+// one beam-source value at p (inside bsrc): the pushed beams' deposit plus, in kernels built for it
+// (kStat), the static (analytic) sources when present
 template <bool kL2, bool kStat>
-__device__ __forceinline__ double ldbs(const SweepArgs& A, const double* bsrc, size_t off) {
-    const double v = ldb<kL2>(bsrc + off);
-    if constexpr (kStat) return A.bstat ? v + __ldg(A.bstat + off) : v;
+__device__ __forceinline__ double ldbs(const SweepArgs& A, const double* bsrc, const double* p) {
+    const double v = ldb<kL2>(p);
+    if constexpr (kStat) return A.bstat ? v + __ldg(A.bstat + (p - bsrc)) : v;
     return v;
 }
 
 template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
-    const size_t bk = (size_t)k * st + (size_t)j * B_NC0;
+    const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC0;
     BeamRow r;
     r.rt = ldbs<kL2, kStat>(A, bsrc, bk + B_RT0);
     r.jz = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ0);
     r.jt = ldbs<kL2, kStat>(A, bsrc, bk + B_JP1I);
     const int K = A.K;
     if (A.ngp) {
-        const double prev = (k > 0) ? ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st) : 0.0;
+        const double prev = (k > 0) ? ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st) : 0.0;
         r.drt = (r.rt - prev) * A.idxi;
     } else if (K == 1) {
         r.drt = 0.0;
     } else if (k == 0) {
         r.drt = (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) - r.rt) * A.idxi;
     } else if (k == K - 1) {
-        r.drt = (r.rt - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st)) * A.idxi;
+        r.drt = (r.rt - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
     } else {
-        r.drt = 0.5 * (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - st)) * A.idxi;
+        r.drt = 0.5 * (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) -
+                       ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
     }
     return r;
 }

@@ -265,7 +265,7 @@ struct BeamRow1 { double rt[3], drt[3], jz[3], jp[6]; };
 template <bool kL2>
 __device__ __forceinline__ BeamRow1 beam_row1(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC1;
-    const size_t bk = (size_t)k * st + (size_t)j * B_NC1;
+    const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC1;
     BeamRow1 r;
     const int rc[3] = {B_RT0, B_RT1R, B_RT1I};
     const int K = A.K;
@@ -274,16 +274,16 @@ __device__ __forceinline__ BeamRow1 beam_row1(const SweepArgs& A, const double* 
         const int c = rc[e];
         r.rt[e] = ldbs<kL2, true>(A, bsrc, bk + c);
         if (A.ngp) {
-            const double prev = (k > 0) ? ldbs<kL2, true>(A, bsrc, bk + c - st) : 0.0;
+            const double prev = (k > 0) ? ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st) : 0.0;
             r.drt[e] = (r.rt[e] - prev) * A.idxi;
         } else if (K == 1) {
             r.drt[e] = 0.0;
         } else if (k == 0) {
             r.drt[e] = (ldbs<kL2, true>(A, bsrc, bk + st + c) - r.rt[e]) * A.idxi;
         } else if (k == K - 1) {
-            r.drt[e] = (r.rt[e] - ldbs<kL2, true>(A, bsrc, bk + c - st)) * A.idxi;
+            r.drt[e] = (r.rt[e] - ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
         } else {
-            r.drt[e] = 0.5 * (ldbs<kL2, true>(A, bsrc, bk + st + c) - ldbs<kL2, true>(A, bsrc, bk + c - st)) * A.idxi;
+            r.drt[e] = 0.5 * (ldbs<kL2, true>(A, bsrc, bk + st + c) - ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
         }
     }
     r.jz[0] = ldbs<kL2, true>(A, bsrc, bk + B_JZ0); r.jz[1] = ldbs<kL2, true>(A, bsrc, bk + B_JZ1R);

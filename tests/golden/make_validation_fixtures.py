@@ -3,7 +3,8 @@ container that has it):  python tests/golden/make_validation_fixtures.py /root/r
 
   validation_numbers.json  printed results of validation/reference_full.txt and reference_quick.txt
                            for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain,
-                           7 centroid betatron oscillation with azimuthal mode 1)
+                           6 displaced analytic driver in mode 1 (linear regime), 7 centroid betatron
+                           oscillation with azimuthal mode 1)
   decks/*.in               the validation decks those numbers come from (blowout, gain, betatron, linear)
 """
 import json
@@ -16,7 +17,14 @@ ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
 here = os.path.dirname(os.path.abspath(__file__))
 out = {}
 for tag, fn in (("full", "reference_full.txt"), ("quick", "reference_quick.txt")):
+    prev = ""
     for line in open(os.path.join(ref, "validation", fn)):
+        if "linear regime (d = 0.01)" in prev and "L2 rel. errors:" in line:
+            errs, _, sin = line.split("L2 rel. errors:")[1].partition("|")
+            vals = dict(tok.strip().split() for tok in errs.split(","))
+            vals["sin_max"] = sin.split(":")[1].strip()
+            out["m1_shift_linear_" + tag] = vals
+        prev = line
         m = re.match(r"(uniform_dr0\.01_dxi0\.01|stretched_dxi0\.005|stretched_dxi0\.005_PCR)\s+Ez\(-5\)=(\S+) "
                      r"Ez\(-7\)=(\S+) Ez\(-8\)=(\S+) Ezmin=(\S+) @xi=(\S+)\s+Wr/r\(r=\.5,xi=-6\)=(\S+)", line)
         if m:
