@@ -109,6 +109,8 @@ typedef struct {
     double *x, *y, *px, *py, *pz, *xi, *w;
     int64_t n;
     double q, m;
+    int pusher;              /* <name>.pusher (src/Beam.cpp:72-78): 0 vay (default, also when left zero),
+                                1 boris, 2 hc (Higuera-Cary), 3 imp (implicit midpoint); imp_rr is not here */
 } qz_beam_view;
 
 typedef struct {
@@ -151,6 +153,13 @@ typedef struct {
 qz_status qz_beam_deposit_analytic(const qz_grid* g, const qz_analytic_beam* b, const qz_box* box, double* bsrc_dev,
                                    void* stream);
 
+/* Beam::slice_sums (src/Beam.cpp:1195-1217), the per-slice beam diagnostics of output.beam_slices: nbins
+   equal bins of the USER xi (= -internal xi) over [lo, hi), 9 sums per bin into out_dev (9 x nbins, dev,
+   overwritten): w, w x, w y, w x^2, w y^2, w gamma, w px, w px^2, w x px. The reference copies the beam to
+   the host for this; here it stays on the device. FP64 atomics: the order of summation, and so the last
+   bits, can differ from call to call. */
+qz_status qz_beam_slice_sums(const qz_beam_view* b, double lo, double hi, int nbins, double* out_dev, void* stream);
+
 /* the 17 moment sums of Beam::sums into out17 (dev); deterministic order */
 qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
 /* qz_beam_sums without any device allocation, for callers that cannot allocate (a host whose
@@ -187,6 +196,12 @@ qz_status qz_sim_add_beam(qz_sim* s, const double* p7_host, int64_t n, double q,
    sweep of the sim adds to the pushed beams' sources. It has no particles, so it is not one of the sim's
    beams: nbeams, the moments and qz_sim_beam count only the particle beams. */
 qz_status qz_sim_add_analytic_beam(qz_sim* s, const qz_analytic_beam* b);
+/* the pusher of particle beam b (qz_beam_view.pusher). A run with a pusher other than Vay goes step by step
+   (the time-step pipeline pushes with Vay); the adjoint refuses it. */
+qz_status qz_sim_set_beam_pusher(qz_sim* s, int b, int pusher);
+/* qz_beam_slice_sums of particle beam b of the sim as it stands (after the last run), into out_host
+   (9 x nbins, host) */
+qz_status qz_sim_beam_slice_sums(qz_sim* s, int b, double lo, double hi, int nbins, double* out_host);
 /* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
    By default (modes 0 or 1, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
    consecutive steps run concurrently on different SMs, each slice gated on the beam pushes of the

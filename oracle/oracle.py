@@ -86,6 +86,9 @@ def lib():
                                                               dp, dp, dp]
         L.qzo_tridiag.argtypes = [C.c_int, C.c_int, dp, dp, dp, dp, dp]
         L.qzo_filter.argtypes = [dp, C.c_int, C.c_double, C.c_int, dp]
+        L.qzo_push.argtypes = [C.c_int, C.c_long, dp, dp, dp, dp, dp]
+        L.qzo_slice_sums.argtypes = [dp, C.c_long, C.c_double, C.c_double, C.c_int, dp]
+        L.qzo_sim_set_beam_pusher.argtypes = [C.c_void_p, C.c_int, C.c_int]
         L.qzo_bessel_i01_scaled.argtypes = [C.c_double, dp, dp]
         L.qzo_sim_add_analytic_beam.argtypes = [C.c_void_p] + [C.c_double] * 5 + [C.c_int] + [C.c_double] * 7
         L.qzo_field_solve.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp, dp, dp, C.c_double, dp]
@@ -122,6 +125,25 @@ def tridiag(a, b, c, d, method="thomas"):
     x = np.zeros_like(d)
     lib().qzo_tridiag(_METHODS[method], len(d), _p(a), _p(b), _p(c), _p(d), _p(x))
     return x
+
+
+def push(kind, u, E, B, eps):
+    """The beam pushers of src/Pushers.hpp on rows of momenta: kind 0 vay, 1 boris, 2 hc, 3 imp."""
+    u, E, B = (_c(np.atleast_2d(a)) for a in (u, E, B))
+    eps = _c(np.broadcast_to(np.asarray(eps, dtype=np.float64), (len(u),)))
+    out = np.zeros_like(u)
+    if lib().qzo_push(int(kind), len(u), _p(u), _p(E), _p(B), _p(eps), _p(out)) != 0:
+        raise ValueError("qzo_push: kind must be 0..3")
+    return out
+
+
+def slice_sums(p7, lo, hi, nbins):
+    """Beam::slice_sums of (n, 7) particle rows: (nbins, 9) sums over bins of the user xi in [lo, hi)."""
+    p7 = _c(p7)
+    out = np.zeros(9 * int(nbins))
+    if lib().qzo_slice_sums(_p(p7), len(p7), float(lo), float(hi), int(nbins), _p(out)) != 0:
+        raise ValueError("qzo_slice_sums: need nbins >= 1 and hi > lo")
+    return out.reshape(int(nbins), 9)
 
 
 def smooth(nodes, a2, n, f):
@@ -283,6 +305,7 @@ class OracleSim:
             parts = _c(parts)
             self.beam_data.append((parts, gref, xiref))
             lib().qzo_sim_add_beam(self.h, _p(parts), len(parts), b.q, b.m, 1 if b.rigid else 0, gref, xiref)
+            lib().qzo_sim_set_beam_pusher(self.h, i, getattr(b, "pusher", 0))
         M, K = spec.M, spec.K
         self.fnc = 18 if spec.modes == 1 else 6
         self.bnc = 15 if spec.modes == 1 else 5

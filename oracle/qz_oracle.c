@@ -578,6 +578,55 @@ void qzo_vay(const double u[3], const double E[3], const double B[3], double eps
     out[0] = r.x; out[1] = r.y; out[2] = r.z;
 }
 
+/* src/Pushers.hpp:64-95, the other beam pushers. Boris (1970): half electric kick, rotation by
+   t = eps B / gamma(u-), half kick. */
+static inline v3 boris(v3 u, v3 E, v3 B, double eps) {
+    const v3 um = v3add(u, v3mul(eps, E));
+    const double g = sqrt(1.0 + v3dot(um, um));
+    const v3 t = v3mul(eps / g, B);
+    const v3 s = v3mul(2.0 / (1.0 + v3dot(t, t)), t);
+    const v3 up = v3add(um, v3cross(v3add(um, v3cross(um, t)), s));
+    return v3add(up, v3mul(eps, E));
+}
+/* Higuera & Cary (2017): the rotation with the gamma of the time-centred momentum, from the
+   quadratic for gamma+^2 */
+static inline v3 higuera_cary(v3 u, v3 E, v3 B, double eps) {
+    const v3 um = v3add(u, v3mul(eps, E));
+    const v3 tau = v3mul(eps, B);
+    const double us = v3dot(um, tau), tt = v3dot(tau, tau);
+    const double sig = 1.0 + v3dot(um, um) - tt;
+    const double gp = sqrt(0.5 * (sig + sqrt(sig * sig + 4.0 * (tt + us * us))));
+    const v3 t = v3mul(1.0 / gp, tau);
+    const double s = 1.0 / (1.0 + v3dot(t, t));
+    const v3 upl = v3mul(s, v3add(v3add(um, v3mul(v3dot(um, t), t)), v3cross(um, t)));
+    return v3add(v3add(upl, v3mul(eps, E)), v3cross(upl, t));
+}
+/* the implicit midpoint push: ubar = (u + eps E) + (ubar / gamma(ubar)) x eps B solved exactly,
+   u+ = 2 ubar - u */
+static inline v3 imp(v3 u, v3 E, v3 B, double eps) {
+    const v3 ub = solve_implicit(v3add(u, v3mul(eps, E)), v3mul(eps, B));
+    return v3add(v3mul(2.0, ub), v3mul(-1.0, u));
+}
+/* pusher kinds of <beam>.pusher: 0 vay, 1 boris, 2 hc, 3 imp (src/Beam.cpp:72-78) */
+static inline v3 push_u(int kind, v3 u, v3 E, v3 B, double eps) {
+    switch (kind) {
+        case 1: return boris(u, E, B, eps);
+        case 2: return higuera_cary(u, E, B, eps);
+        case 3: return imp(u, E, B, eps);
+        default: return vay(u, E, B, eps);
+    }
+}
+int qzo_push(int kind, long n, const double* u, const double* E, const double* B, const double* eps, double* out) {
+    if (kind < 0 || kind > 3) return -1;
+    for (long i = 0; i < n; ++i) {
+        const v3 uu = {u[3 * i], u[3 * i + 1], u[3 * i + 2]}, EE = {E[3 * i], E[3 * i + 1], E[3 * i + 2]};
+        const v3 BB = {B[3 * i], B[3 * i + 1], B[3 * i + 2]};
+        const v3 r = push_u(kind, uu, EE, BB, eps[i]);
+        out[3 * i] = r.x; out[3 * i + 1] = r.y; out[3 * i + 2] = r.z;
+    }
+    return 0;
+}
+
 /* ===================================================================== Adams-Bashforth (src/PlasmaSpecies.cpp:14-48) */
 int qzo_ab_coeffs(int order, double* c) {
     for (int m = 0; m < 5; ++m) c[m] = 0;
@@ -649,6 +698,7 @@ typedef struct {
     long n;
     double *x, *y, *px, *py, *pz, *xi, *w;
     double gref, xiref;
+    int pusher;            /* 0 vay, 1 boris, 2 hc, 3 imp */
     /* analytic rigid beam (no particles): src/Beam.hpp:153-160 */
     int analytic, an_flat;
     double an_n0, an_sr, an_xi0, an_sxi, an_len, an_cut, an_x0, an_y0, an_xs, an_ys, an_gamma;
@@ -771,6 +821,12 @@ int qzo_sim_add_beam(qzo_sim* s, const double* p7, long n, double q, double m, i
         *cols[c] = (double*)malloc(sizeof(double) * (n > 0 ? n : 1));
         for (long i = 0; i < n; ++i) (*cols[c])[i] = p7[7 * i + c];
     }
+    return 0;
+}
+
+int qzo_sim_set_beam_pusher(qzo_sim* s, int b, int kind) {
+    if (b < 0 || b >= s->nb || kind < 0 || kind > 3) return -1;
+    s->bm[b].pusher = kind;
     return 0;
 }
 
@@ -1474,7 +1530,7 @@ static void beam_advance(qzo_sim* s, beam_t* B, double dt_kick, double dt, int m
             B->px[i] = u.x; B->py[i] = u.y; B->pz[i] = u.z;
             continue;
         }
-        u = vay(u, E, Bf, h);
+        u = push_u(B->pusher, u, E, Bf, h);
         const double p2 = u.x * u.x + u.y * u.y;
         const double gam = sqrt(1.0 + p2 + u.z * u.z);
         const double omvz = (1.0 + p2) / (gam * (gam + u.z));
@@ -1597,6 +1653,25 @@ int qzo_sim_beam_sums(const qzo_sim* s, int b, double S[17]) {
                               X * PX, Y * PY};
         S[0] += w;
         for (int c = 0; c < 15; ++c) S[c + 1] += w * v[c];
+    }
+    return 0;
+}
+
+/* src/Beam.cpp:1195-1217: per-bin sums over [lo, hi) of the USER xi (= -internal xi), nbins bins, 9 per bin:
+   w, w x, w y, w x^2, w y^2, w gamma, w px, w px^2, w x px */
+int qzo_slice_sums(const double* p7, long n, double lo, double hi, int nbins, double* out) {
+    if (nbins < 1 || !(hi > lo)) return -1;
+    for (long c = 0; c < 9L * nbins; ++c) out[c] = 0.0;
+    const double db = (hi - lo) / nbins;
+    for (long i = 0; i < n; ++i) {
+        const double* p = p7 + 7 * i;
+        const double w = p[6];
+        if (w == 0) continue;
+        const int b = (int)floor(((0.0 - p[5]) - lo) / db);
+        if (b < 0 || b >= nbins) continue;
+        const double g = sqrt(1 + p[2] * p[2] + p[3] * p[3] + p[4] * p[4]);
+        const double v[9] = {1.0, p[0], p[1], p[0] * p[0], p[1] * p[1], g, p[2], p[2] * p[2], p[0] * p[2]};
+        for (int c = 0; c < 9; ++c) out[9 * b + c] += w * v[c];
     }
     return 0;
 }

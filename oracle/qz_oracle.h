@@ -62,6 +62,9 @@ int qzo_operator_rows(const double* nodes, int M, int op, double* a, double* b, 
 int qzo_stencils(const double* nodes, int M, double* gm, double* g0, double* gp, double* ir);
 int qzo_grid_volumes(const double* nodes, int M, double* V);
 void qzo_vay(const double u[3], const double E[3], const double B[3], double eps, double out[3]);
+/* the beam pushers of src/Pushers.hpp on n momenta (3 per row) with eps per row: kind 0 vay, 1 boris,
+   2 higuera-cary, 3 imp */
+int qzo_push(int kind, long n, const double* u, const double* E, const double* B, const double* eps, double* out);
 int qzo_ab_coeffs(int order, double* c);
 int qzo_ab_variable(int order, const double* t, double h, double* c);
 
@@ -109,6 +112,8 @@ long     qzo_sample_gaussian(double n0, double sr, double xi0_int, double sxi, d
 int      qzo_sim_add_analytic_beam(qzo_sim* s, double q, double n0, double sigma_r, double xi0, double sigma_xi,
                                    int flattop, double length, double xi_cut, double x0, double y0, double xs,
                                    double ys, double gamma);
+/* the pusher of beam b (<name>.pusher, src/Beam.cpp:72-78): 0 vay (default), 1 boris, 2 hc, 3 imp */
+int      qzo_sim_set_beam_pusher(qzo_sim* s, int b, int kind);
 /* the radial smoothing filter f <- (1 - div a^2 grad)^{-1} f of angular number n = 0, 1, 2 with a^2 = a2 in
    every cell (FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161), in place on f (M) */
 int      qzo_filter(const double* nodes, int M, double a2, int n, double* f);
@@ -121,6 +126,8 @@ int      qzo_sim_push_beams(qzo_sim* s, double dt_kick, double dt_drift);
 /* 17 moment sums of beam b (Beam::sums) */
 int      qzo_sim_beam_sums(const qzo_sim* s, int b, double out[17]);
 int      qzo_sim_beam_get(const qzo_sim* s, int b, double* p7);   /* n x 7 copy out */
+/* Beam::slice_sums (src/Beam.cpp:1195-1217) of n x 7 particle rows: 9 sums per bin of the user xi in [lo, hi) */
+int      qzo_slice_sums(const double* p7, long n, double lo, double hi, int nbins, double* out);
 long     qzo_sim_beam_count(const qzo_sim* s, int b);
 /* field store (K, M, F_NC), beam sources (K, M, B_NC), diagnostics (K, M, D_NC): read-only views */
 const double* qzo_sim_fld(const qzo_sim* s);

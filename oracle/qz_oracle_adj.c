@@ -801,7 +801,7 @@ int qzo_sim_adjoint(qzo_sim* s, int nsteps, double dt, const double* lamS, doubl
         if (s->sp[i].p.mobile) { if (isp >= 0) return -2; isp = i; }
     if (isp < 0) return -2;
     for (int b = 0; b < s->nb; ++b)
-        if (s->bm[b].started) return -2;
+        if (s->bm[b].started || s->bm[b].pusher != 0) return -2;
     size_t ntot = 0;
     for (int b = 0; b < s->nb; ++b) ntot += (size_t)s->bm[b].n;
     const size_t per = 7 * ntot;

@@ -35,7 +35,8 @@ class Counters(C.Structure):
 
 class BeamView(C.Structure):
     _fields_ = [("x", C.c_void_p), ("y", C.c_void_p), ("px", C.c_void_p), ("py", C.c_void_p), ("pz", C.c_void_p),
-                ("xi", C.c_void_p), ("w", C.c_void_p), ("n", C.c_int64), ("q", C.c_double), ("m", C.c_double)]
+                ("xi", C.c_void_p), ("w", C.c_void_p), ("n", C.c_int64), ("q", C.c_double), ("m", C.c_double),
+                ("pusher", C.c_int)]
 
 
 class Box(C.Structure):
@@ -73,6 +74,7 @@ SIGNATURES = {
     "qz_beam_push_deposit": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,
                              C.POINTER(C.c_int), C.c_void_p, C.c_void_p],
     "qz_beam_deposit_analytic": [C.c_void_p, C.POINTER(AnalyticBeam), C.POINTER(Box), C.c_void_p, C.c_void_p],
+    "qz_beam_slice_sums": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_int, C.c_void_p, C.c_void_p],
     "qz_beam_sums": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "qz_beam_sums_noalloc": [C.POINTER(BeamView), C.c_double, C.c_double, C.c_void_p, C.c_void_p],
     "qz_sample_gaussian": [C.c_double] * 14 + [C.c_int64, C.c_int, C.c_int, C.c_uint64, C.c_double, _dp, _dp, _dp,
@@ -81,6 +83,8 @@ SIGNATURES = {
     "qz_sim_destroy": [C.c_void_p],
     "qz_sim_add_beam": [C.c_void_p, _dp, C.c_int64, C.c_double, C.c_double, C.c_int, C.c_double, C.c_double],
     "qz_sim_add_analytic_beam": [C.c_void_p, C.POINTER(AnalyticBeam)],
+    "qz_sim_set_beam_pusher": [C.c_void_p, C.c_int, C.c_int],
+    "qz_sim_beam_slice_sums": [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, _dp],
     "qz_sim_run": [C.c_void_p, C.c_int, C.c_double, _dp, C.c_void_p],
     "qz_sim_fields": [C.c_void_p, _dp, _dp],
     "qz_sim_beam": [C.c_void_p, C.c_int, _dp],

@@ -137,13 +137,13 @@ class BeamOps:
     """Beam deposit / push / sums on 7 device columns (tensor (7, n): x y px py pz xi w)."""
 
     @staticmethod
-    def view(cols, q: float, m: float) -> BeamView:
+    def view(cols, q: float, m: float, pusher: int = 0) -> BeamView:
         base = _dev(cols)
         n = cols.shape[1]
         v = BeamView()
         for c, name in enumerate(("x", "y", "px", "py", "pz", "xi", "w")):
             setattr(v, name, base + 8 * n * c)
-        v.n, v.q, v.m = n, q, m
+        v.n, v.q, v.m, v.pusher = n, q, m, int(pusher)
         return v
 
     @staticmethod
@@ -156,22 +156,23 @@ class BeamOps:
         check(lib().qz_beam_deposit(grid.h, C.byref(v), C.byref(box), _dev(bsrc), _stream_ptr(stream)))
 
     @staticmethod
-    def advance(grid, cols, q, m, box, fld, dt_kick, dt_drift, move, stream=None):
-        v = BeamOps.view(cols, q, m)
+    def advance(grid, cols, q, m, box, fld, dt_kick, dt_drift, move, stream=None, pusher: int = 0):
+        v = BeamOps.view(cols, q, m, pusher)
         check(lib().qz_beam_advance(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift, int(move),
                                     _stream_ptr(stream)))
 
     @staticmethod
-    def push(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, stream=None) -> int:
-        v = BeamOps.view(cols, q, m)
+    def push(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, stream=None, pusher: int = 0) -> int:
+        v = BeamOps.view(cols, q, m, pusher)
         st = C.c_int(started)
         check(lib().qz_beam_push(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift, C.byref(st),
                                  _stream_ptr(stream)))
         return st.value
 
     @staticmethod
-    def push_deposit(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, bsrc_next, stream=None) -> int:
-        v = BeamOps.view(cols, q, m)
+    def push_deposit(grid, cols, q, m, box, fld, dt_kick, dt_drift, started: int, bsrc_next, stream=None,
+                     pusher: int = 0) -> int:
+        v = BeamOps.view(cols, q, m, pusher)
         st = C.c_int(started)
         check(lib().qz_beam_push_deposit(grid.h, C.byref(v), C.byref(box), _dev(fld), dt_kick, dt_drift,
                                          C.byref(st), _dev(bsrc_next), _stream_ptr(stream)))
@@ -182,6 +183,12 @@ class BeamOps:
         """qz_beam_deposit_analytic: adds an analytic beam's sources to bsrc."""
         a = analytic_beam(b)
         check(lib().qz_beam_deposit_analytic(grid.h, C.byref(a), C.byref(box), _dev(bsrc), _stream_ptr(stream)))
+
+    @staticmethod
+    def slice_sums(cols, lo: float, hi: float, nbins: int, out, stream=None):
+        """qz_beam_slice_sums: 9 sums per bin of the user xi over [lo, hi) into out (9 * nbins, device)."""
+        v = BeamOps.view(cols, -1.0, 1.0)
+        check(lib().qz_beam_slice_sums(C.byref(v), float(lo), float(hi), int(nbins), _dev(out), _stream_ptr(stream)))
 
     @staticmethod
     def sums(cols, gref, xiref, out17, stream=None):
@@ -214,6 +221,26 @@ def sample_beam(b: "_deck.BeamSpec"):
     a = _deck.sampler_args(b)
     a["np_"] = a.pop("np")
     return sample_gaussian(**a)
+
+
+def slice_table(B: np.ndarray, q: float, lo: float, hi: float) -> np.ndarray:
+    """The columns of the reference's slices file (Beam::write_slices_file, src/Beam.cpp:1219-1236) from the
+    (nbins, 9) slice sums: xi, charge, x_mean, y_mean, sigma_x, sigma_y, gamma_mean, emit_nx, one row per
+    bin with charge (empty bins are left out, as there)."""
+    B = np.asarray(B, dtype=np.float64).reshape(-1, 9)
+    nb = len(B)
+    db = (hi - lo) / nb
+    rows = []
+    for b in range(nb):
+        sw = B[b, 0]
+        if sw <= 0:
+            continue
+        m = B[b] / sw
+        xx, yy = m[3] - m[1] * m[1], m[4] - m[2] * m[2]
+        pxx, xpx = m[7] - m[6] * m[6], m[8] - m[1] * m[6]
+        rows.append([lo + (b + 0.5) * db, q * sw, m[1], m[2], np.sqrt(max(0.0, xx)), np.sqrt(max(0.0, yy)), m[5],
+                     np.sqrt(max(0.0, xx * pxx - xpx * xpx))])
+    return np.array(rows).reshape(-1, 8)
 
 
 def analytic_beam(b: "_deck.BeamSpec") -> AnalyticBeam:
@@ -253,6 +280,8 @@ class Simulation:
             self.beam_data.append((parts, gref, xiref))
             check(lib().qz_sim_add_beam(self.h, _p(parts), len(parts), b.q, b.m, 1 if b.rigid else 0, gref, xiref))
             self._cidx.append(sum(c is not None for c in self._cidx))
+            if getattr(b, "pusher", 0):
+                check(lib().qz_sim_set_beam_pusher(self.h, self._cidx[-1], int(b.pusher)))
         self._pb = [i for i, c in enumerate(self._cidx) if c is not None]   # deck indices of particle beams
         self.fnc = 18 if spec.modes else 6
         self.dnc = 9 if spec.modes else 3
@@ -391,6 +420,12 @@ class Simulation:
         if self._cidx[b] is not None:
             check(lib().qz_sim_beam(self.h, self._cidx[b], _p(out)))
         return out
+
+    def slice_sums(self, b: int, lo: float, hi: float, nbins: int) -> np.ndarray:
+        """qz_sim_beam_slice_sums of deck beam b as it stands: (nbins, 9) over bins of the user xi in [lo, hi)."""
+        out = np.zeros(9 * int(nbins))
+        check(lib().qz_sim_beam_slice_sums(self.h, self._c(int(b)), float(lo), float(hi), int(nbins), _p(out)))
+        return out.reshape(int(nbins), 9)
 
     def lost(self) -> int:
         c = Counters()

@@ -517,6 +517,7 @@ qzb::BeamArgs beam_args(const qz_grid* g, const qz_beam_view* b, const qz_box* b
     B.K = box->K;
     B.ngp = box->ngp;
     B.modes = box->modes;
+    B.pusher = b->pusher;
     return B;
 }
 
@@ -526,6 +527,7 @@ qz_status check_beam(const qz_grid* g, const qz_beam_view* b, const qz_box* box)
         return fail(QZ_ERR_ARG, "beam: null column");
     if (box->K < 2 || !(box->dxi > 0)) return fail(QZ_ERR_ARG, "beam: box needs K >= 2 and dxi > 0");
     if (box->modes != 0 && box->modes != 1) return fail(QZ_ERR_ARG, "beam: modes must be 0 or 1");
+    if (b->pusher < 0 || b->pusher > 3) return fail(QZ_ERR_ARG, "beam: pusher must be 0..3 (vay, boris, hc, imp)");
     return QZ_OK;
 }
 
@@ -573,6 +575,20 @@ extern "C" qz_status qz_beam_deposit_analytic(const qz_grid* g, const qz_analyti
     if (qz_status st = analytic_args(g, b, box, P)) return st;
     if (!bsrc) return fail(QZ_ERR_ARG, "qz_beam_deposit_analytic: null bsrc");
     QZ_CUDA(qzb::launch_deposit_analytic(P, bsrc, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_beam_slice_sums(const qz_beam_view* b, double lo, double hi, int nbins, double* out,
+                                        void* stream) {
+    if (!b || !out || nbins < 1 || !(hi > lo)) return fail(QZ_ERR_ARG, "qz_beam_slice_sums: need nbins >= 1, hi > lo");
+    if (b->n > 0 && (!b->x || !b->y || !b->px || !b->py || !b->pz || !b->xi || !b->w))
+        return fail(QZ_ERR_ARG, "qz_beam_slice_sums: null column");
+    qzb::BeamArgs B{};
+    B.x = b->x; B.y = b->y; B.px = b->px; B.py = b->py; B.pz = b->pz; B.xi = b->xi; B.w = b->w;
+    B.n = (long)b->n;
+    cudaStream_t st = (cudaStream_t)stream;
+    QZ_CUDA(cudaMemsetAsync(out, 0, sizeof(double) * 9 * (size_t)nbins, st));
+    QZ_CUDA(qzb::launch_slice_sums(B, lo, (hi - lo) / nbins, nbins, out, st));
     return QZ_OK;
 }
 
@@ -747,11 +763,11 @@ struct qz_sim {
         bool orig_identity = true;
         int64_t n = 0;
         double q = -1, m = 1, gref = 0, xiref = 0;
-        int rigid = 0, started = 0;
+        int rigid = 0, started = 0, pusher = 0;
         qz_beam_view view() const {
             qz_beam_view v;
             v.x = d; v.y = d + n; v.px = d + 2 * n; v.py = d + 3 * n; v.pz = d + 4 * n; v.xi = d + 5 * n; v.w = d + 6 * n;
-            v.n = n; v.q = q; v.m = m;
+            v.n = n; v.q = q; v.m = m; v.pusher = pusher;
             return v;
         }
     };
@@ -829,6 +845,27 @@ extern "C" qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, q
 extern "C" qz_status qz_sim_destroy(qz_sim* s) {
     delete s;
     return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_set_beam_pusher(qz_sim* s, int b, int pusher) {
+    if (!s || b < 0 || b >= (int)s->beams.size() || pusher < 0 || pusher > 3)
+        return fail(QZ_ERR_ARG, "qz_sim_set_beam_pusher: bad beam index or pusher (0..3)");
+    s->beams[b].pusher = pusher;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_beam_slice_sums(qz_sim* s, int b, double lo, double hi, int nbins, double* out_host) {
+    if (!s || b < 0 || b >= (int)s->beams.size() || !out_host || nbins < 1)
+        return fail(QZ_ERR_ARG, "qz_sim_beam_slice_sums: bad argument");
+    double* d = nullptr;
+    if (cudaMalloc((void**)&d, sizeof(double) * 9 * (size_t)nbins) != cudaSuccess)
+        return fail(QZ_ERR_NOMEM, "qz_sim_beam_slice_sums: device allocation failed");
+    const qz_beam_view v = s->beams[b].view();
+    qz_status st = qz_beam_slice_sums(&v, lo, hi, nbins, d, nullptr);
+    if (st == QZ_OK && cudaMemcpy(out_host, d, sizeof(double) * 9 * (size_t)nbins, cudaMemcpyDeviceToHost) != cudaSuccess)
+        st = fail(QZ_ERR_CUDA, "qz_sim_beam_slice_sums: copy failed");
+    cudaFree(d);
+    return st;
 }
 
 extern "C" qz_status qz_sim_add_analytic_beam(qz_sim* s, const qz_analytic_beam* b) {
@@ -1218,7 +1255,9 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     if (!s || nsteps < 0) return fail(QZ_ERR_ARG, "qz_sim_run: bad argument");
     if (!(dt > 0.0)) return fail(QZ_ERR_ARG, "qz_sim_run: dt must be positive");
     cudaStream_t st = (cudaStream_t)stream;
-    if (s->pipe.enabled && !s->beams.empty()) return run_pipelined(s, nsteps, dt, mom_host, st);
+    bool vay_only = true;                 // the pipeline's push workers use Vay
+    for (const auto& b : s->beams) vay_only = vay_only && b.pusher == 0;
+    if (s->pipe.enabled && !s->beams.empty() && vay_only) return run_pipelined(s, nsteps, dt, mom_host, st);
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 
@@ -1417,6 +1456,8 @@ qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, dou
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
                                         "particles per slice");
     for (size_t b = 0; b < s->beams.size(); ++b) {
+        if (s->beams[b].pusher != 0)
+            return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for the Vay pusher");
         if (s->beams[b].started)
             return fail(QZ_ERR_ARG, "qz_sim_adjoint: the beams were pushed already (the adjoint starts a run)");
         if (!lam_host[b]) return fail(QZ_ERR_ARG, "qz_sim_adjoint: null adjoint buffer");
@@ -1831,6 +1872,7 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         qz_beam_view v;
         v.x = d; v.y = d + n[k]; v.px = d + 2 * n[k]; v.py = d + 3 * n[k]; v.pz = d + 4 * n[k];
         v.xi = d + 5 * n[k]; v.w = d + 6 * n[k]; v.n = n[k]; v.q = q[k]; v.m = m[k];
+        v.pusher = 0;                                   // the batched runs push with Vay
         D.beam[k] = beam_args(I->g, &v, &box);
         D.rigid[k] = rigid[k];
         D.gref[k] = gref[k];

@@ -80,6 +80,51 @@ __global__ void __launch_bounds__(kBeamThreads) deposit_analytic_kernel(const An
     }
 }
 
+// Beam::slice_sums (src/Beam.cpp:1195-1217). Lanes of a warp that fall into the same bin in lane order
+// (the library keeps beams in xi order after a pipelined run) are summed by a segmented shuffle scan first;
+// the last lane of each run adds its 9 sums to L2 with FP64 atomics.
+__global__ void __launch_bounds__(kBeamThreads) slice_sums_kernel(const BeamArgs B, double lo, double db, int nbins,
+                                                                  double* __restrict__ out) {
+    const unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const long stride = (long)gridDim.x * blockDim.x;
+    const long nround = (B.n + 31) / 32 * 32;             // every lane of a warp runs the same iterations
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < nround; i += stride) {
+        double v[9];
+        int key = -1 - lane;
+        if (i < B.n && B.w[i] != 0.0) {
+            const double w = B.w[i];
+            const int b = (int)floor(((0.0 - B.xi[i]) - lo) / db);
+            if (b >= 0 && b < nbins) {
+                key = b;
+                const double X = B.x[i], Y = B.y[i], PX = B.px[i], PY = B.py[i], PZ = B.pz[i];
+                const double g = sqrt(1.0 + PX * PX + PY * PY + PZ * PZ);
+                v[0] = w; v[1] = w * X; v[2] = w * Y; v[3] = w * (X * X); v[4] = w * (Y * Y); v[5] = w * g;
+                v[6] = w * PX; v[7] = w * (PX * PX); v[8] = w * (X * PX);
+            }
+        }
+        if (key < 0)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) v[c] = 0.0;
+        const int kprev = __shfl_up_sync(FULL, key, 1);
+        const bool head = lane == 0 || kprev != key;
+        const int seg = __popc(__ballot_sync(FULL, head) & (FULL >> (31 - lane)));
+#pragma unroll
+        for (int st = 1; st < 32; st <<= 1) {
+            const int sp = __shfl_up_sync(FULL, seg, st);
+#pragma unroll
+            for (int c = 0; c < 9; ++c) {
+                const double vp = __shfl_up_sync(FULL, v[c], st);
+                if (lane >= st && sp == seg) v[c] += vp;
+            }
+        }
+        const int knext = __shfl_down_sync(FULL, key, 1);
+        if (key >= 0 && (lane == 31 || knext != key))
+#pragma unroll
+            for (int c = 0; c < 9; ++c) atomicAdd(out + 9 * (size_t)key + c, v[c]);
+    }
+}
+
 template <bool kDeposit>
 __global__ void __launch_bounds__(kBeamThreads) beam_push_kernel(const BeamArgs B, const double* __restrict__ fld,
                                                                  double dt_kick, double dt, int move,
@@ -107,7 +152,7 @@ __global__ void __launch_bounds__(kBeamThreads) beam_push_kernel(const BeamArgs 
             B.px[i] = u.x; B.py[i] = u.y; B.pz[i] = u.z;
             continue;
         }
-        u = vay(u, E, Bf, h);
+        u = B.pusher ? push_u(B.pusher, u, E, Bf, h) : vay(u, E, Bf, h);
         const double p2 = u.x * u.x + u.y * u.y;
         const double gam = sqrt(1.0 + p2 + u.z * u.z);
         const double omvz = (1.0 + p2) / (gam * (gam + u.z));
@@ -189,6 +234,12 @@ int beam_sums_blocks(long n) {
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s) {
     if (B.n <= 0) return cudaSuccess;
     beam_deposit_kernel<<<grid_for(B.n), kBeamThreads, 0, s>>>(B, bsrc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slice_sums(const BeamArgs& B, double lo, double db, int nbins, double* out, cudaStream_t s) {
+    if (B.n <= 0) return cudaSuccess;
+    slice_sums_kernel<<<grid_for(B.n), kBeamThreads, 0, s>>>(B, lo, db, nbins, out);
     return cudaGetLastError();
 }
 

@@ -127,6 +127,56 @@ __device__ __forceinline__ V3 solve_implicit(V3 a, V3 b) {
     return {inv * (g2 * a.x + g * axb.x + ab * b.x), inv * (g2 * a.y + g * axb.y + ab * b.y),
             inv * (g2 * a.z + g * axb.z + ab * b.z)};
 }
+__device__ __forceinline__ V3 vay(V3 u, V3 E, V3 B, double eps);
+
+// The other beam pushers of src/Pushers.hpp:64-95 (<beam>.pusher). Boris (1970): half electric kick,
+// rotation by t = eps B / gamma(u-), half kick.
+__device__ __forceinline__ V3 boris(V3 u, V3 E, V3 B, double eps) {
+    const V3 um = {u.x + eps * E.x, u.y + eps * E.y, u.z + eps * E.z};
+    const double g = sqrt(1.0 + dot3(um, um));
+    const double f = eps / g;
+    const V3 t = {f * B.x, f * B.y, f * B.z};
+    const double sf = 2.0 / (1.0 + dot3(t, t));
+    const V3 s = {sf * t.x, sf * t.y, sf * t.z};
+    const V3 c1 = cross3(um, t);
+    const V3 w = {um.x + c1.x, um.y + c1.y, um.z + c1.z};
+    const V3 c2 = cross3(w, s);
+    return {um.x + c2.x + eps * E.x, um.y + c2.y + eps * E.y, um.z + c2.z + eps * E.z};
+}
+
+// Higuera & Cary (2017): the rotation with the gamma of the time-centred momentum
+__device__ __forceinline__ V3 higuera_cary(V3 u, V3 E, V3 B, double eps) {
+    const V3 um = {u.x + eps * E.x, u.y + eps * E.y, u.z + eps * E.z};
+    const V3 tau = {eps * B.x, eps * B.y, eps * B.z};
+    const double us = dot3(um, tau), tt = dot3(tau, tau);
+    const double sig = 1.0 + dot3(um, um) - tt;
+    const double gp = sqrt(0.5 * (sig + sqrt(sig * sig + 4.0 * (tt + us * us))));
+    const double ig = 1.0 / gp;
+    const V3 t = {ig * tau.x, ig * tau.y, ig * tau.z};
+    const double s = 1.0 / (1.0 + dot3(t, t));
+    const double ut = dot3(um, t);
+    const V3 c = cross3(um, t);
+    const V3 upl = {s * (um.x + ut * t.x + c.x), s * (um.y + ut * t.y + c.y), s * (um.z + ut * t.z + c.z)};
+    const V3 c2 = cross3(upl, t);
+    return {upl.x + eps * E.x + c2.x, upl.y + eps * E.y + c2.y, upl.z + eps * E.z + c2.z};
+}
+
+// the implicit midpoint push: ubar = (u + eps E) + (ubar / gamma(ubar)) x eps B solved exactly, u+ = 2 ubar - u
+__device__ __forceinline__ V3 imp(V3 u, V3 E, V3 B, double eps) {
+    const V3 ub = solve_implicit({u.x + eps * E.x, u.y + eps * E.y, u.z + eps * E.z}, {eps * B.x, eps * B.y, eps * B.z});
+    return {2.0 * ub.x - u.x, 2.0 * ub.y - u.y, 2.0 * ub.z - u.z};
+}
+
+// <beam>.pusher (src/Beam.cpp:72-78): 0 vay, 1 boris, 2 hc, 3 imp
+__device__ __forceinline__ V3 push_u(int kind, V3 u, V3 E, V3 B, double eps) {
+    switch (kind) {
+        case 1: return boris(u, E, B, eps);
+        case 2: return higuera_cary(u, E, B, eps);
+        case 3: return imp(u, E, B, eps);
+        default: return vay(u, E, B, eps);
+    }
+}
+
 __device__ __forceinline__ V3 vay(V3 u, V3 E, V3 B, double eps) {
     const double g0 = sqrt(1.0 + dot3(u, u));
     const double e2 = 2.0 * eps, eg = eps / g0;

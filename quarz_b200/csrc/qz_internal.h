@@ -86,6 +86,7 @@ struct BeamArgs {
     // box
     double xi_min, dxi, idxi;
     int K, ngp, modes;
+    int pusher;                     // 0 vay, 1 boris, 2 hc, 3 imp (stand-alone push kernels only)
 };
 
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s);
@@ -98,6 +99,9 @@ struct AnalyticArgs {
     double xi_min, dxi;
 };
 cudaError_t launch_deposit_analytic(const AnalyticArgs& P, double* bsrc, cudaStream_t s);
+// Beam::slice_sums (src/Beam.cpp:1195-1217): 9 sums per bin of the user xi in [lo, lo + nbins db), added
+// into out (9 x nbins, cleared by the caller)
+cudaError_t launch_slice_sums(const BeamArgs& B, double lo, double db, int nbins, double* out, cudaStream_t s);
 cudaError_t launch_beam_push(const BeamArgs& B, const double* fld, double dt_kick, double dt_drift, int move,
                              cudaStream_t s);
 cudaError_t launch_beam_push_deposit(const BeamArgs& B, const double* fld, double dt_kick, double dt_drift,

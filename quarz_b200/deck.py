@@ -181,6 +181,7 @@ class BeamSpec:
     flattop_length: float = 0.0
     xi_cut_head_user: Optional[float] = None
     analytic: bool = False      # noise-free rigid beam deposited on the grid, no particles
+    pusher: int = 0             # <beam>.pusher / pusher.beam: 0 vay, 1 boris, 2 hc, 3 imp (src/Beam.cpp:72-78)
 
 
 @dataclass
@@ -269,8 +270,6 @@ def run_spec(cfg: Dict[str, str], base_dir: str = ".") -> RunSpec:
         raise ValueError("plasma.smooth_length must be >= 0")
     if not 1 <= spec.ab_order <= 5:
         raise ValueError("pusher.ab_order must be 1..5")
-    if cfg.get("pusher.beam", "vay") != "vay":
-        raise ValueError("pusher.beam: only vay is on this path")
 
     has_positive = False
     for n in species_names:
@@ -332,12 +331,17 @@ def run_spec(cfg: Dict[str, str], base_dir: str = ".") -> RunSpec:
         b.mirror_y = _b(cfg.get(n + ".mirror_y", "0"))
         if n + ".xi_cut_head" in cfg:
             b.xi_cut_head_user = float(cfg[n + ".xi_cut_head"])
-        if cfg.get(n + ".pusher", "vay") != "vay":
-            raise ValueError(f"{n}.pusher: only vay is on this path")
+        pm = cfg.get(n + ".pusher", cfg.get("pusher.beam", "vay"))
+        if pm not in PUSHERS:
+            raise ValueError(f"{n}.pusher must be vay|boris|hc|imp (imp_rr, radiation reaction, is not on this path)")
+        b.pusher = PUSHERS[pm]
         if modes == 0 and any(v != 0 for v in (b.x0, b.y0, b.x_slope, b.y_slope, b.xp0, b.yp0)):
             raise ValueError(n + ": transverse offsets/tilts need azimuthal mode 1 (modes = 1)")
         spec.beams.append(b)
     return spec
+
+
+PUSHERS = {"vay": 0, "boris": 1, "hc": 2, "imp": 3}
 
 
 def sampler_args(b: BeamSpec) -> dict:

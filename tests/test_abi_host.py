@@ -70,7 +70,9 @@ def test_deck_rejects_unknown_keys_and_unsupported_paths():
     with pytest.raises(ValueError):
         deck.run_spec(deck.parse_deck(base, ["laser.a0=1"]))
     with pytest.raises(ValueError):
-        deck.run_spec(deck.parse_deck(base, ["pusher.beam=boris"]))
+        deck.run_spec(deck.parse_deck(base, ["pusher.beam=imp_rr"]))    # radiation reaction is not on this path
+    assert deck.run_spec(deck.parse_deck(base, ["pusher.beam=boris"])).beams[0].pusher == 1
+    assert deck.run_spec(deck.parse_deck(base, ["pusher.beam=boris", "driver.pusher=hc"])).beams[0].pusher == 2
     with pytest.raises(ValueError):
         deck.run_spec(deck.parse_deck(base, ["driver.x0=0.1"]))   # offsets need modes = 1
 
