@@ -57,7 +57,7 @@ qz_status qz_grid_operator(const qz_grid* g, int op, double* a_host, double* b_h
  * deposit_S :508-559, push :561-668) and the field solves of Simulation::solve_slice_fields
  * (src/Simulation.cpp:797-819). Single rank, constant dxi (no sub-slicing), no laser / ionization.
  * The radial smoothing of the plasma sources (plasma.smooth_length, src/Simulation.cpp:63-66, :685-690,
- * :810-835; FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161) is on this path for modes = 0. */
+ * :810-835; FieldSolver::set_filter / filter, src/FieldSolver.cpp:111-161) is on this path for modes 0 and 1. */
 typedef struct {
     double q, m;             /* <name>.charge, <name>.mass */
     int ppc, ntheta;         /* <name>.ppc, <name>.ntheta */
@@ -80,7 +80,7 @@ typedef struct {
     int neutralize;          /* plasma.neutralize */
     int nspecies;
     qz_species species[4];
-    double smooth_length;    /* plasma.smooth_length (0: off; > 0 with modes = 0 only) */
+    double smooth_length;    /* plasma.smooth_length (0: off) */
 } qz_sweep_params;
 
 typedef struct {

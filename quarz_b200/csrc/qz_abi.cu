@@ -235,7 +235,7 @@ struct qz_sweep {
     double* d_bg = nullptr;
     double* d_ps = nullptr;
     double* d_bgs = nullptr;              // modes = 1: background (3, M) and two source buffers (2 x 30, M)
-    double* d_fconsts = nullptr;          // smoothing filter: Thomas factors of F0 and F1 (6 x M)
+    double* d_fconsts = nullptr;          // smoothing filter: Thomas factors of F0, F1, F2 (9 x M)
     unsigned long long* d_cnt = nullptr;
     unsigned long long* d_tim = nullptr;
     bool timing = false;
@@ -282,7 +282,7 @@ void load_species(const qz_grid& g, const qz_species& sp, std::vector<double> co
 
 // Thomas factors 1/u, -a/u, -c/u (3 x M) of the smoothing filter F_n with a^2 in every cell
 // (FieldSolver::set_filter, src/FieldSolver.cpp:111-146): n = 0 in flux form on the node volumes with a
-// zero-flux wall, n = 1 as the finite-volume L_1 with a^2 inside the flux and identity rows 0 and N
+// zero-flux wall, n = 1, 2 as the finite-volume L_n with a^2 inside the flux and identity rows 0 and N
 void filter_factors(const qz_grid& g, double a2, int n, double* out) {
     const int N = g.N, M = N + 1;
     std::vector<double> a(M, 0.0), b(M, 1.0), c(M, 0.0);
@@ -326,8 +326,6 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     if (p->nspecies < 0 || p->nspecies > 4) return fail(QZ_ERR_ARG, "nspecies must be 0..4");
     if (!(p->smooth_length >= 0)) return fail(QZ_ERR_ARG, "plasma.smooth_length must be >= 0");
     const bool filter = p->smooth_length > 0;
-    if (filter && p->modes == 1)
-        return fail(QZ_ERR_UNSUPPORTED, "plasma.smooth_length: the smoothing filter is on this path for modes = 0");
     const int M = g->M;
     int dev = 0, optin = 0;
     QZ_CUDA(cudaGetDevice(&dev));
@@ -436,10 +434,9 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     A.fconsts = nullptr;
     A.bstat = nullptr;
     if (filter) {
-        std::vector<double> fc((size_t)6 * M);
+        std::vector<double> fc((size_t)9 * M);
         const double a2 = p->smooth_length * p->smooth_length;
-        filter_factors(*g, a2, 0, fc.data());
-        filter_factors(*g, a2, 1, fc.data() + (size_t)3 * M);
+        for (int n = 0; n < 3; ++n) filter_factors(*g, a2, n, fc.data() + (size_t)3 * n * M);
         if ((st = dev_upload(&s->d_fconsts, fc))) {
             delete s;
             return st;

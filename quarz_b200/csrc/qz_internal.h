@@ -53,7 +53,7 @@ struct SweepArgs {
     // optional, m = 0: radial smoothing of the plasma sources (plasma.smooth_length,
     // src/Simulation.cpp:63-66, :685-690, :810-835)
     int filter;
-    const double* fconsts;          // 6 x M: Thomas factors 1/u, -a/u, -c/u of F0, then of F1
+    const double* fconsts;          // 9 x M: Thomas factors 1/u, -a/u, -c/u of F0, then of F1, then of F2
     // optional: beam sources that do not change between steps (analytic rigid beams), (K, M, B_NC),
     // added to bsrc wherever the sweep reads it
     const double* bstat;

@@ -177,7 +177,7 @@ __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
         if (!s_ok) return;
         if (P.trace && tid == 0) P.trace[(size_t)kTraceStride * n] = gtimer();
         PipeGate g{&P, &gs};
-        const bool ok = MODES == 1 ? sweep_m1_body<ORD>(P.sw, smem, g)
+        const bool ok = MODES == 1 ? sweep_m1_body<ORD, PipeGate, EXT>(P.sw, smem, g)
                                    : sweep_body<ORD, REG, kMaxR, PipeGate, EXT>(P.sw, smem, g);
         if (!ok) return;
         // the last row (the others were zeroed slice by slice)
@@ -508,8 +508,10 @@ cudaError_t launch_e(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
 
 template <int ORD>
 cudaError_t launch_o(const PipeArgs& P, int grid, size_t smem, cudaStream_t s) {
-    if (P.modes == 1) return launch_t<1, ORD, false, 1>(P, grid, smem, s);
-    return (P.sw.filter || P.sw.bstat) ? launch_e<ORD, true>(P, grid, smem, s) : launch_e<ORD, false>(P, grid, smem, s);
+    const bool ext = P.sw.filter || P.sw.bstat;
+    if (P.modes == 1)
+        return ext ? launch_t<1, ORD, false, 1, true>(P, grid, smem, s) : launch_t<1, ORD, false, 1, false>(P, grid, smem, s);
+    return ext ? launch_e<ORD, true>(P, grid, smem, s) : launch_e<ORD, false>(P, grid, smem, s);
 }
 
 template <int ORD, bool EXT>
@@ -522,8 +524,9 @@ int occupancy_e(const PipeArgs& P, size_t smem) {
 
 template <int ORD>
 int occupancy_o(const PipeArgs& P, size_t smem) {
-    if (P.modes == 1) return occupancy_t<1, ORD, false, 1>(smem);
-    return (P.sw.filter || P.sw.bstat) ? occupancy_e<ORD, true>(P, smem) : occupancy_e<ORD, false>(P, smem);
+    const bool ext = P.sw.filter || P.sw.bstat;
+    if (P.modes == 1) return ext ? occupancy_t<1, ORD, false, 1, true>(smem) : occupancy_t<1, ORD, false, 1, false>(smem);
+    return ext ? occupancy_e<ORD, true>(P, smem) : occupancy_e<ORD, false>(P, smem);
 }
 
 // ---------------------------------------------------------------- ordering the beam by (xi cell, r cell)

@@ -9,19 +9,26 @@ size_t sweep_m1_smem_bytes(int M) {
 }
 
 namespace {
-template <int ORD>
+// EXT: the variant for decks with the smoothing filter or static (analytic) beam sources
+template <int ORD, bool EXT>
 __global__ void __launch_bounds__(kSweepThreads, 1) sweep_m1_kernel(const SweepArgs A) {
     extern __shared__ double smem_raw[];
     NoGate g;
-    sweep_m1_body<ORD>(A, smem_raw, g);
+    sweep_m1_body<ORD, NoGate, EXT>(A, smem_raw, g);
+}
+
+template <int ORD, bool EXT>
+cudaError_t launch_e(const SweepArgs& A, size_t smem, cudaStream_t stream) {
+    cudaError_t e = cudaFuncSetAttribute(sweep_m1_kernel<ORD, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)smem);
+    if (e != cudaSuccess) return e;
+    sweep_m1_kernel<ORD, EXT><<<1, kSweepThreads, smem, stream>>>(A);
+    return cudaGetLastError();
 }
 
 template <int ORD>
 cudaError_t launch_t(const SweepArgs& A, size_t smem, cudaStream_t stream) {
-    cudaError_t e = cudaFuncSetAttribute(sweep_m1_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    sweep_m1_kernel<ORD><<<1, kSweepThreads, smem, stream>>>(A);
-    return cudaGetLastError();
+    return (A.filter || A.bstat) ? launch_e<ORD, true>(A, smem, stream) : launch_e<ORD, false>(A, smem, stream);
 }
 }  // namespace
 

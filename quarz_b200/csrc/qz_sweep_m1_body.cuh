@@ -262,7 +262,7 @@ __device__ __forceinline__ void scan_bwd_g(const double (&a)[NA], const double (
 // xi-derivative, J_z, J+ (rho itself feeds nothing on this path)
 struct BeamRow1 { double rt[3], drt[3], jz[3], jp[6]; };
 
-template <bool kL2>
+template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow1 beam_row1(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC1;
     const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC1;
@@ -272,25 +272,25 @@ __device__ __forceinline__ BeamRow1 beam_row1(const SweepArgs& A, const double* 
 #pragma unroll
     for (int e = 0; e < 3; ++e) {
         const int c = rc[e];
-        r.rt[e] = ldbs<kL2, true>(A, bsrc, bk + c);
+        r.rt[e] = ldbs<kL2, kStat>(A, bsrc, bk + c);
         if (A.ngp) {
-            const double prev = (k > 0) ? ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st) : 0.0;
+            const double prev = (k > 0) ? ldbs<kL2, kStat>(A, bsrc, bk + c - (ptrdiff_t)st) : 0.0;
             r.drt[e] = (r.rt[e] - prev) * A.idxi;
         } else if (K == 1) {
             r.drt[e] = 0.0;
         } else if (k == 0) {
-            r.drt[e] = (ldbs<kL2, true>(A, bsrc, bk + st + c) - r.rt[e]) * A.idxi;
+            r.drt[e] = (ldbs<kL2, kStat>(A, bsrc, bk + st + c) - r.rt[e]) * A.idxi;
         } else if (k == K - 1) {
-            r.drt[e] = (r.rt[e] - ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
+            r.drt[e] = (r.rt[e] - ldbs<kL2, kStat>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
         } else {
-            r.drt[e] = 0.5 * (ldbs<kL2, true>(A, bsrc, bk + st + c) - ldbs<kL2, true>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
+            r.drt[e] = 0.5 * (ldbs<kL2, kStat>(A, bsrc, bk + st + c) - ldbs<kL2, kStat>(A, bsrc, bk + c - (ptrdiff_t)st)) * A.idxi;
         }
     }
-    r.jz[0] = ldbs<kL2, true>(A, bsrc, bk + B_JZ0); r.jz[1] = ldbs<kL2, true>(A, bsrc, bk + B_JZ1R);
-    r.jz[2] = ldbs<kL2, true>(A, bsrc, bk + B_JZ1I);
-    r.jp[0] = ldbs<kL2, true>(A, bsrc, bk + B_JP0R); r.jp[1] = ldbs<kL2, true>(A, bsrc, bk + B_JP0I);
-    r.jp[2] = ldbs<kL2, true>(A, bsrc, bk + B_JP1R); r.jp[3] = ldbs<kL2, true>(A, bsrc, bk + B_JP1I);
-    r.jp[4] = ldbs<kL2, true>(A, bsrc, bk + B_JP2R); r.jp[5] = ldbs<kL2, true>(A, bsrc, bk + B_JP2I);
+    r.jz[0] = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ0); r.jz[1] = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ1R);
+    r.jz[2] = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ1I);
+    r.jp[0] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP0R); r.jp[1] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP0I);
+    r.jp[2] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP1R); r.jp[3] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP1I);
+    r.jp[4] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP2R); r.jp[5] = ldbs<kL2, kStat>(A, bsrc, bk + B_JP2I);
     return r;
 }
 
@@ -307,6 +307,87 @@ __device__ __forceinline__ void init_sources1(const Src1& T, const double* bg, i
     T.ne.a0[j] = 0.0; T.ne.ar[j] = 0.0; T.ne.ai[j] = 0.0;
     T.ni.a0[j] = g0 > 0.0 ? g0 : 0.0; T.ni.ar[j] = 0.0; T.ni.ai[j] = 0.0;
     T.S.r0[j] = 0.0; T.S.i0[j] = 0.0; T.S.r1[j] = 0.0; T.S.i1[j] = 0.0; T.S.r2[j] = 0.0; T.S.i2[j] = 0.0;
+}
+
+// with the filter: the plasma deposit of a slice starts from zero (beam and background come after the filter)
+__device__ __forceinline__ void init_sources1_zero(const Src1& T, int M, int j) {
+    const Msc sc[6] = {T.rhot, T.drho, T.jz, T.chi, T.ne, T.ni};
+#pragma unroll
+    for (int c = 0; c < 6; ++c) { sc[c].a0[j] = 0.0; sc[c].ar[j] = 0.0; sc[c].ai[j] = 0.0; }
+    T.jp.r0[j] = 0.0; T.jp.i0[j] = 0.0; T.jp.r1[j] = 0.0; T.jp.i1[j] = 0.0; T.jp.r2[j] = 0.0; T.jp.i2[j] = 0.0;
+    T.S.r0[j] = 0.0; T.S.i0[j] = 0.0; T.S.r1[j] = 0.0; T.S.i1[j] = 0.0; T.S.r2[j] = 0.0; T.S.i2[j] = 0.0;
+}
+
+// ---------------------------------------------------------------- smoothing filter (modes = 1)
+// FieldSolver::filter (src/FieldSolver.cpp:148-161) of NB source arrays of the global scratch, each with
+// F0, F1 or F2 (op), on one row per thread in place: Thomas with the host-factored pivots fc (3 x M per
+// operator), its substitutions as grouped block scans (tot, tot2: the two scratch halves). Every thread reads
+// and writes only its own row. Out of line: only the kernel variant for filtered decks calls it.
+template <int NB>
+__device__ __noinline__ void filter_rows1(const FilterSet<NB> fs, const double* __restrict__ fc, int M, double* tot,
+                                          double* tot2) {
+    const int i = threadIdx.x;
+    const bool row = i < M;
+    double a[3], d[NB], y[NB];
+#pragma unroll
+    for (int s = 0; s < 3; ++s) a[s] = row ? __ldg(fc + (size_t)s * 3 * M + M + i) : 1.0;
+#pragma unroll
+    for (int e = 0; e < NB; ++e) d[e] = row ? __ldg(fc + (size_t)fs.op[e] * 3 * M + i) * __ldcg(fs.f[e] + i) : 0.0;
+    scan_fwd_g<3, NB>(a, d, fs.op, y, tot);
+#pragma unroll
+    for (int e = 0; e < NB; ++e) y[e] = fma(a[fs.op[e]], y[e], d[e]);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) a[s] = row ? __ldg(fc + (size_t)s * 3 * M + 2 * M + i) : 1.0;
+    double x[NB];
+    scan_bwd_g<3, NB>(a, y, fs.op, x, tot2);
+    if (row)
+#pragma unroll
+        for (int e = 0; e < NB; ++e) fs.f[e][i] = fma(a[fs.op[e]], x[e], y[e]);
+}
+
+// Simulation::filter_plasma_sources (src/Simulation.cpp:823-835, modes = 1) on the plasma deposit of the
+// slice in buffer T, then combine_sources (src/Simulation.cpp:430-452): the background and the beam row
+// of slice k added, as the reference adds them after the filter. Ends with a barrier.
+template <bool kL2>
+__device__ __forceinline__ void filter_sources1(const SweepArgs& A, const Src1& T, const double* bg,
+                                                const double* bsrc, int k, double* tot, int& scan_par) {
+    const int M = A.M, i = threadIdx.x;
+    const Msc sc[6] = {T.rhot, T.drho, T.jz, T.chi, T.ne, T.ni};
+    FilterSet<12> fa, fb;
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        fa.f[3 * c] = sc[c].a0; fa.f[3 * c + 1] = sc[c].ar; fa.f[3 * c + 2] = sc[c].ai;
+        fa.op[3 * c] = 0; fa.op[3 * c + 1] = 1; fa.op[3 * c + 2] = 1;
+    }
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        fb.f[3 * c] = sc[4 + c].a0; fb.f[3 * c + 1] = sc[4 + c].ar; fb.f[3 * c + 2] = sc[4 + c].ai;
+        fb.op[3 * c] = 0; fb.op[3 * c + 1] = 1; fb.op[3 * c + 2] = 1;
+    }
+    fb.f[6] = T.jp.r0; fb.f[7] = T.jp.i0; fb.f[8] = T.jp.r1; fb.f[9] = T.jp.i1; fb.f[10] = T.jp.r2; fb.f[11] = T.jp.i2;
+    fb.op[6] = fb.op[7] = 0; fb.op[8] = fb.op[9] = 1; fb.op[10] = fb.op[11] = 2;
+    double* t0 = tot + (scan_par++ & 1) * 16 * kW;
+    double* t1 = tot + (scan_par++ & 1) * 16 * kW;
+    filter_rows1<12>(fa, A.fconsts, M, t0, t1);
+    filter_rows1<12>(fb, A.fconsts, M, t0, t1);
+    if (i < M) {
+        const BeamRow1 b = beam_row1<kL2, true>(A, bsrc, k, i);
+        const double g0 = __ldcg(bg + i), gr = __ldcg(bg + M + i), gi = __ldcg(bg + 2 * M + i);
+        T.rhot.a0[i] = lg(T.rhot.a0 + i) + (g0 + b.rt[0]);
+        T.rhot.ar[i] = lg(T.rhot.ar + i) + (gr + b.rt[1]);
+        T.rhot.ai[i] = lg(T.rhot.ai + i) + (gi + b.rt[2]);
+        T.drho.a0[i] = lg(T.drho.a0 + i) + b.drt[0];
+        T.drho.ar[i] = lg(T.drho.ar + i) + b.drt[1];
+        T.drho.ai[i] = lg(T.drho.ai + i) + b.drt[2];
+        T.jz.a0[i] = lg(T.jz.a0 + i) + b.jz[0];
+        T.jz.ar[i] = lg(T.jz.ar + i) + b.jz[1];
+        T.jz.ai[i] = lg(T.jz.ai + i) + b.jz[2];
+        double* jp[6] = {T.jp.r0, T.jp.i0, T.jp.r1, T.jp.i1, T.jp.r2, T.jp.i2};
+#pragma unroll
+        for (int c = 0; c < 6; ++c) jp[c][i] = lg(jp[c] + i) + b.jp[c];
+        if (g0 > 0.0) T.ni.a0[i] = lg(T.ni.a0 + i) + g0;
+    }
+    __syncthreads();
 }
 
 // ---------------------------------------------------------------- particles
@@ -637,7 +718,8 @@ using namespace m1_detail;
 size_t sweep_m1_smem_bytes(int M);
 
 // One m = 1 sweep by the calling CTA (kThreads threads, one radial row per thread: M <= kThreads).
-template <int ORD, class Gate>
+// EXT: the variant that also handles the smoothing filter (A.filter) and static beam sources (A.bstat)
+template <int ORD, class Gate, bool EXT = false>
 __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_raw, Gate& gate) {
     const int M = A.M, N = A.N, K = A.K;
     const int tid = threadIdx.x;
@@ -722,21 +804,36 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
     }
     __syncthreads();
     if (Gate::kActive && !*S.flag) return false;
-    if (row) init_sources1(src1_of(scr, M, 0), bg, M, i, beam_row1<Gate::kActive>(A, gate.bsrc(A), 0, i));
+    const bool filt = EXT && A.filter;
+    int scan_par = 0;
+    if (filt) {                     // the background is smoothed like the plasma (src/Simulation.cpp:685-690)
+        FilterSet<3> fg;
+        fg.f[0] = bg; fg.f[1] = bg + M; fg.f[2] = bg + 2 * M;
+        fg.op[0] = 0; fg.op[1] = fg.op[2] = 1;
+        double* t0 = S.tot + (scan_par++ & 1) * 16 * kW;
+        double* t1 = S.tot + (scan_par++ & 1) * 16 * kW;
+        filter_rows1<3>(fg, A.fconsts, M, t0, t1);
+        if (row) init_sources1_zero(src1_of(scr, M, 0), M, i);
+    } else if (row) {
+        init_sources1(src1_of(scr, M, 0), bg, M, i, beam_row1<Gate::kActive, EXT>(A, gate.bsrc(A), 0, i));
+    }
     __syncthreads();
     deposit_all1<ORD>(A, S, src1_of(scr, M, 0), gate);
     __syncthreads();
     M1_MARK(0);
 
-    int scan_par = 0;
     const double fc = A.flux_coef;
     const int niter = A.picard > 0 ? A.picard : 1;
     for (int k = 0; k < K; ++k) {
         const int cb = k & 1;                                    // this slice's source buffer
         // the next slice's sources: background + beam (the push of this slice deposits on top); the
         // buffer's previous content (slice k-1) was last read before the end of slice k-1
-        if (k + 1 < K && row)
-            init_sources1(src1_of(scr, M, cb ^ 1), bg, M, i, beam_row1<Gate::kActive>(A, gate.bsrc(A), k + 1, i));
+        if (filt) {
+            if (k + 1 < K && row) init_sources1_zero(src1_of(scr, M, cb ^ 1), M, i);
+            filter_sources1<Gate::kActive>(A, src1_of(scr, M, cb), bg, gate.bsrc(A), k, S.tot, scan_par);
+        } else if (k + 1 < K && row) {
+            init_sources1(src1_of(scr, M, cb ^ 1), bg, M, i, beam_row1<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, i));
+        }
         // ---------------- P2: psi, E_z, B_z (9 systems with fixed Thomas factors)
         //   L0: psi0 = -rhot0, ez0 = -drho0, bz0 = -(J_theta1' + J_theta1 / r)
         //   L1D: psi1 r/i, ez1 r/i, bz1 r/i
@@ -828,6 +925,16 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
         M1_MARK(2);
 
         // ---------------- P4: B+ (src/Simulation.cpp:535-591)
+        if (filt) {                 // S+ smoothed (src/Simulation.cpp:810-816): each thread's own row, the only
+            const Src1 T = src1_of(scr, M, cb);                  // one its B+ right-hand sides read
+            FilterSet<6> fsS;
+            fsS.f[0] = T.S.r0; fsS.f[1] = T.S.i0; fsS.f[2] = T.S.r1; fsS.f[3] = T.S.i1; fsS.f[4] = T.S.r2;
+            fsS.f[5] = T.S.i2;
+            fsS.op[0] = fsS.op[1] = 0; fsS.op[2] = fsS.op[3] = 1; fsS.op[4] = fsS.op[5] = 2;
+            double* t0 = S.tot + (scan_par++ & 1) * 16 * kW;
+            double* t1 = S.tot + (scan_par++ & 1) * 16 * kW;
+            filter_rows1<6>(fsS, A.fconsts, M, t0, t1);
+        }
         {
             const Src1 T = src1_of(scr, M, cb);
             // fixed part of the right-hand sides: (d/dx + i d/dy) J_z + S

@@ -5,7 +5,8 @@ Decks: the plain blowout (config 0's deck, 257 uniform nodes, one thread row per
 uniform grid of 801 nodes (two rows per thread, plasma state in global memory), both with
 plasma.smooth_length = 0.05 and 2e4 driver particles, box cut to xi in [-8, 0]; an analytic driver
 (m = 0) with a particle witness on the stretched 512-node grid; and an analytic driver displaced by
-0.05 in x with modes = 1.
+0.05 in x with modes = 1; the hosing deck (modes = 1, 8 azimuths, Picard 3) cut to xi in [-9, 0] with
+plasma.smooth_length = 0.02.
 
 Tolerances as in the other parity tests: beam sources 1e-12 (FP64 reductions in another order); fields
 and diagnostics after one sweep, relative L2 per stored component, within max(1e-10, 4 x the reference
@@ -109,8 +110,9 @@ def _runs_against_oracle(spec, steps):
             if b.analytic:
                 assert np.all(mom[:, q] == 0) and np.all(mom_ref[:, q] == 0)
                 continue
+            m1 = spec.modes == 1
             for n in range(steps + 1):
-                d, dr = O.from_sums(mom[n, q], gref, xiref), O.from_sums(mom_ref[n, q], gref, xiref)
+                d, dr = O.from_sums(mom[n, q], gref, xiref, m1=m1), O.from_sums(mom_ref[n, q], gref, xiref, m1=m1)
                 _close(spec, d, dr, 1e-8, (pipelined, q, n))
         fld, _ = sim.fields()
         for c in (4, 5):
@@ -139,11 +141,20 @@ def test_analytic_driver_m1_displaced_one_sweep():
     _one_sweep(_analytic_m1())
 
 
+def _hosing_filtered():
+    text = workloads.hosing_deck(xi_min=-9.0, driver_np=20000, witness_np=20000, steps=2)
+    return workloads.spec_from_text(text, ["xi.step=0.01", "plasma.smooth_length=0.02"])
+
+
+def test_filter_m1_one_sweep():
+    _one_sweep(_hosing_filtered())
+
+
+def test_filter_m1_runs_against_oracle():
+    _runs_against_oracle(_hosing_filtered(), 2)
+
+
 def test_filter_refusals():
-    with pytest.raises(Q.QZError) as e:
-        Q.Simulation(workloads.spec_from_text(workloads.hosing_deck(xi_min=-2.0, driver_np=100, witness_np=100,
-                                                                     steps=1), ["plasma.smooth_length=0.05"]))
-    assert e.value.code == 3
     spec = _blowout()
     sim = Q.Simulation(spec)
     with pytest.raises(Q.QZError) as e:
