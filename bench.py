@@ -74,6 +74,8 @@ def _config(spec, nb_total, steps, extra=None, workload=WORKLOAD):
          "l2": "inputs larger than L2: beams 112 MB + a field store of 59 MB and beam sources of 49 MB per step "
                "in flight (rings of one slot per step)",
          "parallelism": "replicas"}
+    if getattr(spec, "smooth_length", 0.0):
+        c["smooth_length"] = spec.smooth_length
     if extra:
         c.update(extra)
     return c
@@ -145,6 +147,8 @@ def _workload(args):
     spec = workloads.hosing() if args.workload == "hosing" else workloads.pinched_witness()
     if args.time_steps:
         spec.steps = args.time_steps
+    if args.smooth:
+        spec.smooth_length = args.smooth
     return spec
 
 
@@ -439,6 +443,8 @@ def main():
     ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
     ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1", "adjoint"],
                     default="pinched_witness")
+    ap.add_argument("--smooth", type=float, default=0.0,
+                    help="plasma.smooth_length of the pinched-witness / hosing run (0: none, the headline)")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

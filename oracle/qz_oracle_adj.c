@@ -50,6 +50,26 @@ static void solve_T(solver_t* s, int op, const double* chi, const double* lam, d
     free(at); free(ct); free(bw); free(cp); free(dp);
 }
 
+/* the smoothing filter in reverse: lam <- F_n^-T lam in place (solver_filter builds x = F_n^-1 f with
+   every row of F_n, identity rows included, so the transpose is the transposed Thomas solve) */
+static void filter_T(solver_t* s, int n, double* lam) {
+    if (!s->filter_on) return;
+    const op_t* o = &s->F[n];
+    const int N = s->g.N, M = N + 1;
+    double* at = (double*)malloc(sizeof(double) * M);
+    double* ct = (double*)malloc(sizeof(double) * M);
+    double* mu = (double*)malloc(sizeof(double) * M);
+    double* cp = (double*)malloc(sizeof(double) * M);
+    double* dp = (double*)malloc(sizeof(double) * M);
+    for (int j = 0; j <= N; ++j) {
+        at[j] = j > 0 ? o->c[j - 1] : 0.0;
+        ct[j] = j < N ? o->a[j + 1] : 0.0;
+    }
+    thomas(M, at, o->b, ct, lam, mu, cp, dp);
+    memcpy(lam, mu, sizeof(double) * M);
+    free(at); free(ct); free(mu); free(cp); free(dp);
+}
+
 /* lam_f += grad^T lam_df (solver_gradient) */
 static void gradient_T(const solver_t* s, const double* ldf, double* lf) {
     const int N = s->g.N;
@@ -435,6 +455,7 @@ static void sweep_back(qzo_sim* s, int isp, const double* lfld, double* lbsrc) {
                 A.chi[jj] += a * qm / D;
             }
         }
+        solver_filter(&s->fs, 0, A.chi);             /* B+ saw the smoothed chi (src/Simulation.cpp:823-835) */
         /* store (src/Simulation.cpp:594-633): EP1R = wp.r1 + bp.i1, EP1I = -bp.r1, BP1R, BP1I, EZ0, BZ0 */
         for (int j = 0; j < M; ++j) {
             A.l_wpr[j] += LF[j * 6 + F_EP1R];
@@ -472,6 +493,9 @@ static void sweep_back(qzo_sim* s, int isp, const double* lfld, double* lbsrc) {
             for (int j = 0; j <= N; ++j) A.l_Sr[j] += A.l_t[j];
             gradient_T(&s->fs, A.l_t, A.l_jz);
         }
+        /* the S+ filter (src/Simulation.cpp:810-812) in reverse */
+        filter_T(&s->fs, 1, A.l_Sr);
+        filter_T(&s->fs, 1, A.l_Si);
         /* S deposit (needs lam_S; adds to lam of W+, E_z, B_z) */
         for (int i = 0; i < np; ++i) {
             const double w = T[5 * cap + i];
@@ -504,6 +528,14 @@ static void sweep_back(qzo_sim* s, int isp, const double* lfld, double* lbsrc) {
             else if (k == K - 1) { LB(K - 1, j, B_RT0) += ld; LB(K - 2, j, B_RT0) -= ld; }
             else { LB(k + 1, j, B_RT0) += 0.5 * ld; LB(k - 1, j, B_RT0) -= 0.5 * ld; }
         }
+        /* the filter of the plasma deposit (src/Simulation.cpp:823-835) in reverse: the beams were added after
+           it, so their adjoints above are those of the combined sources */
+        filter_T(&s->fs, 0, A.l_rhot);
+        filter_T(&s->fs, 0, A.l_drho);
+        filter_T(&s->fs, 0, A.l_jz);
+        filter_T(&s->fs, 0, A.l_chi);
+        filter_T(&s->fs, 1, A.l_jpr);
+        filter_T(&s->fs, 1, A.l_jpi);
         /* plasma deposit of P_k */
         for (int i = 0; i < np; ++i) {
             const double w = T[5 * cap + i];
@@ -795,7 +827,7 @@ static void beams_load(qzo_sim* s, const double* in) {
    J = sum lamS * sums. mom (optional): the forward's moment sums ((nsteps + 1), nb, 17).
    Returns 0, or -2 when the deck is outside the adjoint's scope. The sim ends at the last step. */
 int qzo_sim_adjoint(qzo_sim* s, int nsteps, double dt, const double* lamS, double* lam_out, double* mom) {
-    if (s->m1 || s->p.ngp || s->fs.filter_on || nsteps < 1) return -2;
+    if (s->m1 || s->p.ngp || nsteps < 1) return -2;
     int isp = -1;
     for (int i = 0; i < s->nsp; ++i)
         if (s->sp[i].p.mobile) { if (isp >= 0) return -2; isp = i; }

@@ -485,12 +485,12 @@ __device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j,
 // shared-memory arrays in place, each with F0 (op 0) or F1 (op 1): Thomas with the host-factored pivots
 // A.fconsts, its two substitutions as block scans over the thread's rows [row0, row0 + Rw). Every thread
 // reads and writes only its own rows; the caller puts a barrier before (the arrays are complete) and, when
-// other threads read them next, after. Kept out of line: only decks with plasma.smooth_length reach it.
+// other threads read them next, after. Only the kernel variants for filtered decks (EXT) contain it.
 template <int NS>
 struct FilterSet { double* f[NS]; int op[NS]; };
 
 template <int NS, int kMaxR>
-__device__ __noinline__ void filter_rows(const FilterSet<NS> fs, const double* __restrict__ fc, int M, int Rw,
+__device__ __forceinline__ void filter_rows(const FilterSet<NS> fs, const double* __restrict__ fc, int M, int Rw,
                                          double* tot) {
     const int row0 = threadIdx.x * Rw;
     double a[NS], b[NS], d[kMaxR][NS];

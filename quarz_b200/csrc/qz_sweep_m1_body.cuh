@@ -322,9 +322,9 @@ __device__ __forceinline__ void init_sources1_zero(const Src1& T, int M, int j) 
 // FieldSolver::filter (src/FieldSolver.cpp:148-161) of NB source arrays of the global scratch, each with
 // F0, F1 or F2 (op), on one row per thread in place: Thomas with the host-factored pivots fc (3 x M per
 // operator), its substitutions as grouped block scans (tot, tot2: the two scratch halves). Every thread reads
-// and writes only its own row. Out of line: only the kernel variant for filtered decks calls it.
+// and writes only its own row. Only the kernel variants for filtered decks (EXT) contain it.
 template <int NB>
-__device__ __noinline__ void filter_rows1(const FilterSet<NB> fs, const double* __restrict__ fc, int M, double* tot,
+__device__ __forceinline__ void filter_rows1(const FilterSet<NB> fs, const double* __restrict__ fc, int M, double* tot,
                                           double* tot2) {
     const int i = threadIdx.x;
     const bool row = i < M;
