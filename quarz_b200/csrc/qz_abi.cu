@@ -1447,8 +1447,6 @@ qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, dou
     const qzb::SweepArgs& base = s->sw->base;
     if (s->p.modes != 0 || s->p.ngp || s->p.K < 2)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2");
-    if (base.filter)
-        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: the smoothing filter (plasma.smooth_length) has no adjoint");
     if (base.M > qzb::kSweepThreads || base.np > qzb::kSweepThreads || base.nsp != 1)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
                                         "particles per slice");

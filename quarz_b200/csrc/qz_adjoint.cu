@@ -684,7 +684,56 @@ struct AdjNoGate {
 // One sweep in reverse by the calling CTA (all kSweepThreads threads): slices K-1 .. 0. The gate
 // orders it against the beam adjoint tasks when several steps run concurrently. Returns false when a
 // gate wait gave up.
-template <int ORD, class Gate>
+// The smoothing filter of the forward (plasma.smooth_length) on NS shared arrays of one operator, one row per
+// thread (row i). transpose = false: f <- F^-1 f (the forward filter, for chi). transpose = true:
+// lam <- F^-T lam. F0 = D^-1 S with D = V / 2 pi and S symmetric, so F0^-T lam = V F0^-1 (lam / V). F1 is Q^-1 S
+// on its interior rows (Q = r dV, the symmetriser of L1D) with identity rows 0 and N, row N - 1 coupled to
+// x_N: F1^-T lam = Q F1^-1 (lam / Q) on the interior, lam_0 on row 0 and lam_N - c_{N-1} mu_{N-1} on row N.
+// The Thomas factors fc (3 x M per operator) are the forward's. Ends with a barrier.
+template <int NS>
+__device__ __noinline__ void filter_rows_adj(double* const (&arr)[NS], int op, bool transpose, const double* fc,
+                                             int M, int N, double Vi, double iVi, double F1i, double iF1i,
+                                             double* tot, double* tot2) {
+    const int i = threadIdx.x;
+    const bool row = i < M, inner = i >= 1 && i < N;
+    const double* F = fc + (size_t)op * 3 * M;
+    double rr = 0.0, af = 1.0, ab = 1.0;
+    if (row) { rr = F[i]; af = F[M + i]; ab = F[2 * M + i]; }
+    double scale_in = 1.0, scale_out = 1.0;
+    if (transpose) {
+        scale_in = op == 0 ? iVi : (inner ? iF1i : 0.0);
+        scale_out = op == 0 ? Vi : F1i;
+    }
+    double lam[NS], d[NS];
+#pragma unroll
+    for (int e = 0; e < NS; ++e) {
+        lam[e] = row ? arr[e][i] : 0.0;
+        d[e] = rr * (lam[e] * scale_in);
+    }
+    double y[NS];
+    scan_fwd<NS>(af, d, y, tot);
+#pragma unroll
+    for (int e = 0; e < NS; ++e) y[e] = row ? fma(af, y[e], d[e]) : 0.0;
+    double x[NS];
+    scan_bwd<NS>(row ? ab : 1.0, y, x, tot2);
+    if (row)
+#pragma unroll
+        for (int e = 0; e < NS; ++e) {
+            const double v = fma(ab, x[e], y[e]);
+            if (!transpose || op == 0) arr[e][i] = v * scale_out;
+            else if (inner) arr[e][i] = v * scale_out;
+            else if (i == 0) arr[e][i] = lam[e];
+        }
+    __syncthreads();
+    if (transpose && op == 1 && i == N) {
+        const double cN1 = -fc[(size_t)3 * M + 2 * M + N - 1] / fc[(size_t)3 * M + N - 1];   // c_{N-1} of F1
+#pragma unroll
+        for (int e = 0; e < NS; ++e) arr[e][N] = lam[e] - cN1 * arr[e][N - 1];
+    }
+    __syncthreads();
+}
+
+template <int ORD, class Gate, bool FILT = false>
 __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ traj, const double* __restrict__ fld,
                                 const double* lfld, double* __restrict__ lbsrc, double* smem_raw, Gate& gate) {
     const int M = A.M, N = A.N, K = A.K, tid = threadIdx.x;
@@ -839,6 +888,11 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
                 for (int v = 0; v < 5; ++v) Lsm[(5 + m * 5 + v) * kSweepThreads + tid] = kept ? Lp.h[m][v] : 0.0;
         }
         __syncthreads();
+        if constexpr (FILT) {                         // B+ saw the smoothed chi (src/Simulation.cpp:823-835)
+            double* const fa[1] = {S.chi};
+            filter_rows_adj<1>(fa, 0, false, A.fconsts, M, N, Vi, iVi, F1i, iF1i, S.tot + (par++ & 1) * 8 * kW,
+                               S.tot + (par++ & 1) * 8 * kW);
+        }
         ADJ_MARK(1);
         // ---- B+ (src/Simulation.cpp:535-591) in reverse: mu = F (L - chi)^-1 (F^-1 lam) per system
         {
@@ -896,6 +950,11 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
         __syncthreads();
         ADJ_MARK(2);
         if (row) S.l_jz[i] = grad_T_at(A, gm, g0, gp, S.t0, i) - (i == N ? fcoef * S.t0[N] : 0.0);
+        if constexpr (FILT) {                         // the S+ filter (src/Simulation.cpp:810-812) in reverse
+            double* const fa[2] = {S.l_Sr, S.l_Si};
+            filter_rows_adj<2>(fa, 1, true, A.fconsts, M, N, Vi, iVi, F1i, iF1i, S.tot + (par++ & 1) * 8 * kW,
+                               S.tot + (par++ & 1) * 8 * kW);
+        }
         // ---- the S deposit in reverse (adds to lam of W+, E_z, B_z)
         {
             double sc[6] = {0, 0, 0, 0, 0, 0};
@@ -975,6 +1034,14 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             }
         }
         __syncthreads();
+        if constexpr (FILT) {   // the filter of the plasma deposit in reverse (the beams came after it)
+            double* const f0[4] = {S.l_rhot, S.l_drho, S.l_jz, S.l_chi};
+            filter_rows_adj<4>(f0, 0, true, A.fconsts, M, N, Vi, iVi, F1i, iF1i, S.tot + (par++ & 1) * 8 * kW,
+                               S.tot + (par++ & 1) * 8 * kW);
+            double* const f1[1] = {S.l_jpi};
+            filter_rows_adj<1>(f1, 1, true, A.fconsts, M, N, Vi, iVi, F1i, iF1i, S.tot + (par++ & 1) * 8 * kW,
+                               S.tot + (par++ & 1) * 8 * kW);
+        }
         ADJ_MARK(5);
         // ---- the plasma deposit of P_k in reverse
         if (alive) {
@@ -993,7 +1060,7 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
     return true;
 }
 
-template <int ORD>
+template <int ORD, bool FILT>
 __global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __grid_constant__ SweepArgs A,
                                                                        const double* __restrict__ traj,
                                                                        const double* __restrict__ fld,
@@ -1001,7 +1068,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) sweep_back_kernel(const __gr
                                                                        double* __restrict__ lbsrc) {
     extern __shared__ double smem_raw[];
     AdjNoGate g;
-    sweep_back_body<ORD>(A, traj, fld, lfld, lbsrc, smem_raw, g);
+    sweep_back_body<ORD, AdjNoGate, FILT>(A, traj, fld, lfld, lbsrc, smem_raw, g);
 }
 
 // ------------------------------------------------------------------ the reverse pass as a pipeline
@@ -1083,7 +1150,7 @@ struct AdjPipeGate {
     }
 };
 
-template <int ORD>
+template <int ORD, bool FILT>
 __device__ void adj_sweep_role(const AdjPipeArgs& P, double* smem) {
     __shared__ AdjGateState gs;
     const int T = P.nsteps;
@@ -1095,7 +1162,7 @@ __device__ void adj_sweep_role(const AdjPipeArgs& P, double* smem) {
         }
         __syncthreads();
         AdjPipeGate g{&P, &gs};
-        if (!sweep_back_body<ORD>(P.sw, P.traj + (size_t)n * P.traj_slot, P.fld + (size_t)n * P.fld_slot,
+        if (!sweep_back_body<ORD, AdjPipeGate, FILT>(P.sw, P.traj + (size_t)n * P.traj_slot, P.fld + (size_t)n * P.fld_slot,
                                   P.lfld + (size_t)n * P.lfld_slot, P.lbsrc + (size_t)n * P.lbsrc_slot, smem, g))
             return;
         __syncthreads();
@@ -1242,11 +1309,11 @@ __device__ void adj_worker_role(const AdjPipeArgs& P, double* smem) {
     }
 }
 
-template <int ORD>
+template <int ORD, bool FILT>
 __global__ void __launch_bounds__(kSweepThreads, 1) adjoint_pipeline_kernel(const __grid_constant__ AdjPipeArgs P) {
     extern __shared__ double smem_raw[];
     if ((int)blockIdx.x < P.nsweep)
-        adj_sweep_role<ORD>(P, smem_raw);
+        adj_sweep_role<ORD, FILT>(P, smem_raw);
     else
         adj_worker_role(P, smem_raw);
 }
@@ -1294,7 +1361,7 @@ __global__ void bucket_pmax_kernel(const __grid_constant__ AdjPipeArgs P, const 
 
 template <int ORD>
 cudaError_t launch_adj_pipe_t(const AdjPipeArgs& P, int grid, size_t smem, cudaStream_t st) {
-    auto fn = adjoint_pipeline_kernel<ORD>;
+    auto fn = P.sw.filter ? adjoint_pipeline_kernel<ORD, true> : adjoint_pipeline_kernel<ORD, false>;
     cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     void* args[] = {(void*)&P};
@@ -1302,8 +1369,8 @@ cudaError_t launch_adj_pipe_t(const AdjPipeArgs& P, int grid, size_t smem, cudaS
 }
 
 template <int ORD>
-int adj_pipe_occupancy_t(size_t smem) {
-    auto fn = adjoint_pipeline_kernel<ORD>;
+int adj_pipe_occupancy_t(size_t smem, bool filt) {
+    auto fn = filt ? adjoint_pipeline_kernel<ORD, true> : adjoint_pipeline_kernel<ORD, false>;
     if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess) return 0;
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, kSweepThreads, smem) != cudaSuccess) return 0;
@@ -1314,9 +1381,10 @@ template <int ORD>
 cudaError_t launch_sweep_back_t(const SweepArgs& A, const double* traj, const double* fld, const double* lfld,
                                 double* lbsrc, cudaStream_t st) {
     const size_t smem = adjoint_sweep_smem_bytes(A.M);
-    cudaError_t e = cudaFuncSetAttribute(sweep_back_kernel<ORD>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    auto fn = A.filter ? sweep_back_kernel<ORD, true> : sweep_back_kernel<ORD, false>;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    sweep_back_kernel<ORD><<<1, kSweepThreads, smem, st>>>(A, traj, fld, lfld, lbsrc);
+    fn<<<1, kSweepThreads, smem, st>>>(A, traj, fld, lfld, lbsrc);
     return cudaGetLastError();
 }
 
@@ -1354,11 +1422,11 @@ int adjoint_pipeline_max_grid(const AdjPipeArgs& P, int* sms) {
     const size_t smem = adjoint_pipeline_smem_bytes(P.sw.M);
     int per = 0;
     switch (P.sw.ord) {
-        case 1: per = adj::adj_pipe_occupancy_t<1>(smem); break;
-        case 2: per = adj::adj_pipe_occupancy_t<2>(smem); break;
-        case 3: per = adj::adj_pipe_occupancy_t<3>(smem); break;
-        case 4: per = adj::adj_pipe_occupancy_t<4>(smem); break;
-        case 5: per = adj::adj_pipe_occupancy_t<5>(smem); break;
+        case 1: per = adj::adj_pipe_occupancy_t<1>(smem, P.sw.filter != 0); break;
+        case 2: per = adj::adj_pipe_occupancy_t<2>(smem, P.sw.filter != 0); break;
+        case 3: per = adj::adj_pipe_occupancy_t<3>(smem, P.sw.filter != 0); break;
+        case 4: per = adj::adj_pipe_occupancy_t<4>(smem, P.sw.filter != 0); break;
+        case 5: per = adj::adj_pipe_occupancy_t<5>(smem, P.sw.filter != 0); break;
         default: return 0;
     }
     return per * nsm;

@@ -2,7 +2,8 @@
 and the gradients of witness energy gain and spread against central differences of the CUDA forward.
 
 Deck: the one of tests/test_oracle_adjoint.py (24 uniform cells, 71 slices, AB3, driver and witness
-with 300 particles each, 2 steps) and a stretched-grid variant with 3 steps. Tolerances: every
+with 300 particles each, 2 steps) and a stretched-grid variant with 3 steps, each also with the smoothing
+filter (plasma.smooth_length 0.3 and 0.05: the adjoint then runs the filters in reverse). Tolerances: every
 component of the particle adjoint 1e-8 relative L2 against the oracle (the forwards differ in the
 order of their deposit sums, about 1e-13); the profile and delay gradients 1e-5 relative against
 central differences with h = 1e-6 (their error is that of the differences). Both schedules: the
@@ -23,11 +24,14 @@ def _specs():
     spec = deck.run_spec(deck.parse_deck(TEXT))
     st = deck.run_spec(deck.parse_deck(TEXT, ["time.steps=3"]))
     st.nodes = workloads.scan_nodes(129, 2e-3)
-    return [spec, st]
+    sm = deck.run_spec(deck.parse_deck(TEXT, ["plasma.smooth_length=0.3"]))
+    sms = deck.run_spec(deck.parse_deck(TEXT, ["time.steps=3", "plasma.smooth_length=0.05"]))
+    sms.nodes = workloads.scan_nodes(129, 2e-3)
+    return [spec, st, sm, sms]
 
 
 @pytest.mark.parametrize("pipelined", [True, False])
-@pytest.mark.parametrize("which", [0, 1])
+@pytest.mark.parametrize("which", [0, 1, 2, 3])
 def test_adjoint_against_oracle(which, pipelined):
     spec = _specs()[which]
     beams = [Q.sample_beam(b) for b in spec.beams]

@@ -156,10 +156,6 @@ def test_filter_m1_runs_against_oracle():
 
 def test_filter_refusals():
     spec = _blowout()
-    sim = Q.Simulation(spec)
-    with pytest.raises(Q.QZError) as e:
-        sim.adjoint(1, spec.dt, np.zeros((1, 17)))
-    assert e.value.code == 3
     with pytest.raises(Q.QZError) as e:
         Q.Batch().add(spec)
     assert e.value.code == 3
