@@ -160,6 +160,15 @@ qz_status qz_beam_deposit_analytic(const qz_grid* g, const qz_analytic_beam* b, 
    bits, can differ from call to call. */
 qz_status qz_beam_slice_sums(const qz_beam_view* b, double lo, double hi, int nbins, double* out_dev, void* stream);
 
+/* Simulation::write_fields (src/Simulation.cpp:878-993): the field file fields_NNNNNN.bin, version 3, of one
+   sweep, as the reference writes it without output groups: int32 {3, M, K, mode1}, float64 t, r[M], xi[K]
+   (user xi, increasing: the head of the box is the last row), int32 ncomp, then ncomp x {char name[16],
+   float64 data[K][M]}; names psi ez er eth br bth bz ne ni rhob, and with modes = 1 <name>_c / <name>_s of
+   psi ez bz ne ni rhob er eth br bth. fld (K, M, F_NC), diag (K, M, D_NC), bsrc (K, M, B_NC; NULL writes a
+   zero rhob) are device arrays when on_device != 0, else host arrays; nodes_host: the M radial nodes. */
+qz_status qz_write_fields(const char* path, const double* nodes_host, int M, const qz_box* box, double t,
+                          const double* fld, const double* diag, const double* bsrc, int on_device);
+
 /* the 17 moment sums of Beam::sums into out17 (dev); deterministic order */
 qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17_dev, void* stream);
 /* qz_beam_sums without any device allocation, for callers that cannot allocate (a host whose
@@ -202,6 +211,9 @@ qz_status qz_sim_set_beam_pusher(qz_sim* s, int b, int pusher);
 /* qz_beam_slice_sums of particle beam b of the sim as it stands (after the last run), into out_host
    (9 x nbins, host) */
 qz_status qz_sim_beam_slice_sums(qz_sim* s, int b, double lo, double hi, int nbins, double* out_host);
+/* qz_write_fields of the sim's last sweep (fields, diagnostics and the beam sources it read: the beams as
+   they stand plus the analytic ones) at time t */
+qz_status qz_sim_write_fields(qz_sim* s, double t, const char* path);
 /* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
    By default (modes 0 or 1, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of
    consecutive steps run concurrently on different SMs, each slice gated on the beam pushes of the

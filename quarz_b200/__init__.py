@@ -16,7 +16,7 @@ from __future__ import annotations
 
 from ._lib import QZError, lib, library_path  # noqa: F401
 from .api import (Batch, BeamOps, RadialGrid, Simulation, Sweep, analytic_beam, sample_beam,  # noqa: F401
-                  sample_gaussian, slice_table, sweep_params)
+                  sample_gaussian, slice_table, sweep_params, write_fields)
 
 __all__ = ["QZError", "lib", "library_path", "RadialGrid", "Sweep", "BeamOps", "Simulation", "Batch",
-           "sample_gaussian", "sample_beam", "sweep_params", "slice_table", "analytic_beam"]
+           "sample_gaussian", "sample_beam", "sweep_params", "slice_table", "analytic_beam", "write_fields"]

@@ -85,6 +85,9 @@ SIGNATURES = {
     "qz_sim_add_analytic_beam": [C.c_void_p, C.POINTER(AnalyticBeam)],
     "qz_sim_set_beam_pusher": [C.c_void_p, C.c_int, C.c_int],
     "qz_sim_beam_slice_sums": [C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int, _dp],
+    "qz_write_fields": [C.c_char_p, _dp, C.c_int, C.POINTER(Box), C.c_double, C.c_void_p, C.c_void_p, C.c_void_p,
+                        C.c_int],
+    "qz_sim_write_fields": [C.c_void_p, C.c_double, C.c_char_p],
     "qz_sim_run": [C.c_void_p, C.c_int, C.c_double, _dp, C.c_void_p],
     "qz_sim_fields": [C.c_void_p, _dp, _dp],
     "qz_sim_beam": [C.c_void_p, C.c_int, _dp],

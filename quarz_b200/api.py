@@ -243,6 +243,18 @@ def slice_table(B: np.ndarray, q: float, lo: float, hi: float) -> np.ndarray:
     return np.array(rows).reshape(-1, 8)
 
 
+def write_fields(path: str, spec: "_deck.RunSpec", fld: np.ndarray, diag: np.ndarray, bsrc=None,
+                 t: float = 0.0) -> None:
+    """qz_write_fields from host arrays: the reference's fields_NNNNNN.bin (version 3) of one sweep."""
+    nodes = np.ascontiguousarray(spec.nodes, dtype=np.float64)
+    box = Box(xi_min=spec.xi_min, dxi=spec.dxi, K=spec.K, ngp=1 if spec.ngp else 0, modes=spec.modes)
+    F = np.ascontiguousarray(fld, dtype=np.float64)
+    D = np.ascontiguousarray(diag, dtype=np.float64)
+    B = None if bsrc is None else np.ascontiguousarray(bsrc, dtype=np.float64)
+    check(lib().qz_write_fields(str(path).encode(), _p(nodes), len(nodes), C.byref(box), float(t), F.ctypes.data,
+                                D.ctypes.data, None if B is None else B.ctypes.data, 0))
+
+
 def analytic_beam(b: "_deck.BeamSpec") -> AnalyticBeam:
     """qz_analytic_beam of an analytic deck beam, in internal coordinates."""
     flat = b.sigma_xi <= 0
@@ -426,6 +438,10 @@ class Simulation:
         out = np.zeros(9 * int(nbins))
         check(lib().qz_sim_beam_slice_sums(self.h, self._c(int(b)), float(lo), float(hi), int(nbins), _p(out)))
         return out.reshape(int(nbins), 9)
+
+    def write_fields(self, path: str, t: float = 0.0) -> None:
+        """qz_sim_write_fields: the field file of the last sweep."""
+        check(lib().qz_sim_write_fields(self.h, float(t), str(path).encode()))
 
     def lost(self) -> int:
         c = Counters()

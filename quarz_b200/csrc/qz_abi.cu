@@ -4,11 +4,13 @@
 // generator, and the time-step runner.
 #include "qz_b200.h"
 #include "qz_internal.h"
+#include "qz_device.cuh"
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <new>
 #include <random>
 #include <string>
@@ -1702,6 +1704,114 @@ extern "C" qz_status qz_sim_fields(qz_sim* s, double* fld, double* diag) {
     if (fld) QZ_CUDA(cudaMemcpy(fld, s->d_fld, sizeof(double) * KM * s->fnc, cudaMemcpyDeviceToHost));
     if (diag) QZ_CUDA(cudaMemcpy(diag, s->d_diag, sizeof(double) * KM * s->dnc, cudaMemcpyDeviceToHost));
     return QZ_OK;
+}
+
+// ===================================================================== field files
+namespace {
+
+// Simulation::field_table / write_fields (src/Simulation.cpp:878-993) for this path: no ion, laser or
+// output-group columns, every slice and node. Layout (version 3): int32 {3, M, K, mode1}, float64 t,
+// float64 r[M], float64 xi[K] (user xi, increasing: slice k is row K-1-k), int32 ncomp, then per component
+// char name[16] and float64 data[K][M].
+qz_status write_fields_host(const char* path, const double* nodes, int M, const qz_box* box, double t,
+                            const double* F, const double* D, const double* B) {
+    const int K = box->K, m1 = box->modes == 1;
+    const int fnc = m1 ? 18 : 6, dnc = m1 ? 9 : 3, bnc = m1 ? 15 : 5;
+    using Fn = std::function<double(size_t)>;        // value at (k, j), index k * M + j
+    std::vector<std::pair<std::string, Fn>> comps;
+    auto f = [&](int c) { return Fn([F, fnc, c](size_t kj) { return F[kj * fnc + c]; }); };
+    auto d = [&](int c) { return Fn([D, dnc, c](size_t kj) { return D[kj * dnc + c]; }); };
+    auto b = [&](int c) { return Fn([B, bnc, c](size_t kj) { return B ? B[kj * bnc + c] : 0.0; }); };
+    auto scaled = [](Fn a, double s) { return Fn([a, s](size_t kj) { return s * a(kj); }); };
+    auto sum = [](Fn a, Fn c, double sc) { return Fn([a, c, sc](size_t kj) { return a(kj) + sc * c(kj); }); };
+    using namespace qzb;
+    comps.push_back({"psi", d(D_PSI0)});
+    comps.push_back({"ez", f(F_EZ0)});
+    comps.push_back({"er", f(F_EP1R)});
+    comps.push_back({"eth", f(F_EP1I)});
+    comps.push_back({"br", f(F_BP1R)});
+    comps.push_back({"bth", f(F_BP1I)});
+    comps.push_back({"bz", f(F_BZ0)});
+    comps.push_back({"ne", d(D_NE0)});
+    comps.push_back({"ni", d(D_NI0)});
+    comps.push_back({"rhob", b(B_RHO0)});
+    if (m1) {   // f = f0 + 2 Re[f1 e^{i th}]: f_c = 2 Re f1, f_s = -2 Im f1; vectors from the V+ modes 0 and 2
+        const std::pair<const char*, std::pair<Fn, Fn>> sc[] = {
+            {"psi", {d(D_PSI1R), d(D_PSI1I)}}, {"ez", {f(F_EZ1R), f(F_EZ1I)}}, {"bz", {f(F_BZ1R), f(F_BZ1I)}},
+            {"ne", {d(D_NE1R), d(D_NE1I)}}, {"ni", {d(D_NI1R), d(D_NI1I)}}, {"rhob", {b(B_RHO1R), b(B_RHO1I)}}};
+        for (const auto& e : sc) {
+            comps.push_back({std::string(e.first) + "_c", scaled(e.second.first, 2.0)});
+            comps.push_back({std::string(e.first) + "_s", scaled(e.second.second, -2.0)});
+        }
+        const int vr[2][4] = {{F_EP0R, F_EP0I, F_EP2R, F_EP2I}, {F_BP0R, F_BP0I, F_BP2R, F_BP2I}};
+        const char* nm[2][2] = {{"er", "eth"}, {"br", "bth"}};
+        for (int v = 0; v < 2; ++v) {
+            const Fn r0 = f(vr[v][0]), i0 = f(vr[v][1]), r2 = f(vr[v][2]), i2 = f(vr[v][3]);
+            comps.push_back({std::string(nm[v][0]) + "_c", sum(r0, r2, 1.0)});
+            comps.push_back({std::string(nm[v][0]) + "_s", sum(i0, i2, -1.0)});
+            comps.push_back({std::string(nm[v][1]) + "_c", sum(i0, i2, 1.0)});
+            comps.push_back({std::string(nm[v][1]) + "_s", sum(r2, r0, -1.0)});
+        }
+    }
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(QZ_ERR_ARG, std::string("qz_write_fields: cannot open ") + path);
+    const int32_t hdr[4] = {3, M, K, m1};
+    bool ok = std::fwrite(hdr, sizeof(hdr), 1, fp) == 1 && std::fwrite(&t, 8, 1, fp) == 1 &&
+              std::fwrite(nodes, 8, (size_t)M, fp) == (size_t)M;
+    std::vector<double> xi(K);
+    for (int k = 0; k < K; ++k) xi[k] = 0.0 - (box->xi_min + (K - 1 - k) * box->dxi);
+    const int32_t nc = (int32_t)comps.size();
+    ok = ok && std::fwrite(xi.data(), 8, (size_t)K, fp) == (size_t)K && std::fwrite(&nc, 4, 1, fp) == 1;
+    std::vector<double> v((size_t)K * M);
+    for (const auto& c : comps) {
+        char name[16] = {0};
+        std::strncpy(name, c.first.c_str(), 15);
+        for (int k = 0; k < K; ++k)
+            for (int j = 0; j < M; ++j) v[(size_t)(K - 1 - k) * M + j] = c.second((size_t)k * M + j);
+        ok = ok && std::fwrite(name, 16, 1, fp) == 1 && std::fwrite(v.data(), 8, v.size(), fp) == v.size();
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    return ok ? QZ_OK : fail(QZ_ERR_ARG, std::string("qz_write_fields: write failed: ") + path);
+}
+
+}  // namespace
+
+extern "C" qz_status qz_write_fields(const char* path, const double* nodes, int M, const qz_box* box, double t,
+                                     const double* fld, const double* diag, const double* bsrc, int on_device) {
+    if (!path || !nodes || !box || !fld || !diag) return fail(QZ_ERR_ARG, "qz_write_fields: null pointer");
+    if ((box->modes != 0 && box->modes != 1) || box->K < 1 || M < 2) return fail(QZ_ERR_ARG, "qz_write_fields: bad size");
+    if (!on_device) return write_fields_host(path, nodes, M, box, t, fld, diag, bsrc);
+    const size_t KM = (size_t)box->K * M;
+    const int m1 = box->modes == 1;
+    std::vector<double> F(KM * (m1 ? 18 : 6)), D(KM * (m1 ? 9 : 3)), B(bsrc ? KM * (m1 ? 15 : 5) : 0);
+    QZ_CUDA(cudaMemcpy(F.data(), fld, sizeof(double) * F.size(), cudaMemcpyDeviceToHost));
+    QZ_CUDA(cudaMemcpy(D.data(), diag, sizeof(double) * D.size(), cudaMemcpyDeviceToHost));
+    if (bsrc) QZ_CUDA(cudaMemcpy(B.data(), bsrc, sizeof(double) * B.size(), cudaMemcpyDeviceToHost));
+    return write_fields_host(path, nodes, M, box, t, F.data(), D.data(), bsrc ? B.data() : nullptr);
+}
+
+extern "C" qz_status qz_sim_write_fields(qz_sim* s, double t, const char* path) {
+    if (!s || !path) return fail(QZ_ERR_ARG, "qz_sim_write_fields: null pointer");
+    const qz_box box = sim_box(s);
+    const size_t nb = (size_t)s->p.K * s->g->M * s->bnc;
+    double* d = nullptr;
+    if (cudaMalloc((void**)&d, sizeof(double) * nb) != cudaSuccess)
+        return fail(QZ_ERR_NOMEM, "qz_sim_write_fields: device allocation failed");
+    // the beam sources of the last sweep: the beams as they stand (not pushed after it) and the static ones
+    qz_status st = QZ_OK;
+    if (s->d_bstat) {
+        if (cudaMemcpy(d, s->d_bstat, sizeof(double) * nb, cudaMemcpyDeviceToDevice) != cudaSuccess)
+            st = fail(QZ_ERR_CUDA, "qz_sim_write_fields: copy failed");
+    } else if (cudaMemset(d, 0, sizeof(double) * nb) != cudaSuccess) {
+        st = fail(QZ_ERR_CUDA, "qz_sim_write_fields: memset failed");
+    }
+    for (size_t b = 0; st == QZ_OK && b < s->beams.size(); ++b) {
+        const qz_beam_view v = s->beams[b].view();
+        st = qz_beam_deposit(s->g, &v, &box, d, nullptr);
+    }
+    if (st == QZ_OK) st = qz_write_fields(path, s->g->r.data(), s->g->M, &box, t, s->d_fld, s->d_diag, d, 1);
+    cudaFree(d);
+    return st;
 }
 
 extern "C" qz_status qz_sim_beam(qz_sim* s, int b, double* p7) {

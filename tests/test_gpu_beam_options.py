@@ -8,7 +8,8 @@ oracle on the same inputs.
   goes step by step for them): moments within 1e-8 of the oracle's relative to their natural scale;
 - the adjoint refuses a beam whose pusher is not Vay;
 - the per-slice beam sums of output.beam_slices (qz_beam_slice_sums, src/Beam.cpp:1195-1217) against the
-  oracle's."""
+  oracle's;
+- the field file of a run (qz_sim_write_fields) against the run's own arrays."""
 import numpy as np
 import pytest
 
@@ -107,3 +108,27 @@ def test_slice_sums_against_oracle():
         assert np.all(np.abs(got - want) <= 1e-12 * scale), (b, np.abs(got - want).max(axis=0) / scale)
         tab = Q.slice_table(got, spec.beams[b].q, -9.0, 0.0)
         assert tab.shape[1] == 8 and len(tab) > 0
+
+
+# ---------------------------------------------------------------- field files (src/Simulation.cpp:878-993)
+def test_sim_write_fields(tmp_path):
+    """qz_sim_write_fields after a run: the field values are those of qz_sim_fields bit for bit, and rhob (the
+    beam sources the last sweep read, re-deposited from the beams as they stand) equals the oracle's beam
+    deposit of the same particles to 1e-12 relative L2."""
+    from test_fields_file import read_fields
+
+    text = workloads.pinched_witness_deck(xi_min=-9.0, driver_np=20000, witness_np=20000, steps=2)
+    spec = workloads.spec_from_text(text)
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    sim = Q.Simulation(spec, beams=beams)
+    sim.run(2, spec.dt)
+    path = tmp_path / "fields_000002.bin"
+    sim.write_fields(path, t=10.0)
+    got = read_fields(path)
+    F, D = sim.fields()
+    np.testing.assert_array_equal(got["psi"], D[::-1, :, 0])
+    np.testing.assert_array_equal(got["ez"], F[::-1, :, 4])
+    np.testing.assert_array_equal(got["bth"], F[::-1, :, 3])
+    ref = O.OracleSim(spec, beams=[(sim.beam(b), g, x) for b, (_, g, x) in enumerate(beams)])
+    ref.deposit_beams()
+    assert rel_l2(got["rhob"], ref.bsrc()[::-1, :, 4]) < 1e-12
