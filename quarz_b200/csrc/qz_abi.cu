@@ -1926,9 +1926,6 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         !m || !rigid || !gref || !xiref)))
         return fail(QZ_ERR_ARG, "qz_batch_add: bad argument (at most 2 beams per instance)");
     if (p->modes != 0 && p->modes != 1) return fail(QZ_ERR_ARG, "qz_batch_add: modes must be 0 or 1");
-    if (p->smooth_length != 0)
-        return fail(QZ_ERR_UNSUPPORTED, "qz_batch_add: the smoothing filter (plasma.smooth_length) is not in the "
-                                        "batched sweep; run such instances with qz_sim");
     if (p->modes == 1 && M > qzb::kSweepThreads)
         return fail(QZ_ERR_SIZE, "qz_batch_add: modes = 1 instances need M <= 512 (one radial row per thread)");
     if (b->ord && p->ab_order != b->ord) return fail(QZ_ERR_ARG, "qz_batch_add: every instance needs the same AB order");
@@ -1954,7 +1951,8 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
             static const bool kLay[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
             int lay = -1;
             for (int l = 0; l < 4 && lay < 0; ++l)
-                if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1]) + reserve <= (size_t)optin) lay = l;
+                if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1], p->smooth_length > 0) + reserve <= (size_t)optin)
+                    lay = l;
             if (lay < 0) { delete I; return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep"); }
             D.sw.dbuf = kLay[lay][0];
             D.sw.const_smem = kLay[lay][1];
@@ -2000,22 +1998,24 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     cudaStream_t st = (cudaStream_t)stream;
     // slot sizes and shared memory: the largest instance
     size_t fmax = 0, dmax = 0, bmax = 0, smem = 0, mom_total = 0;
-    bool with_m1 = false;
+    bool with_m1 = false, with_ext = false;
     std::vector<size_t> mom_off(ni);
     for (int i = 0; i < ni; ++i) {
         const auto& A = b->inst[i]->dev.sw;
         const bool m1 = b->inst[i]->dev.modes == 1;
         with_m1 = with_m1 || m1;
+        with_ext = with_ext || A.filter;
         const size_t km = (size_t)A.K * A.M;
         fmax = std::max(fmax, km * (m1 ? 18 : 6));           // fld (K, M, 18 / 6)
         dmax = std::max(dmax, km * (m1 ? 9 : 3));            // diag (K, M, 9 / 3)
         bmax = std::max(bmax, km * (m1 ? 15 : 5));           // bsrc (K, M, 15 / 5)
-        smem = std::max(smem, m1 ? qzb::sweep_m1_smem_bytes(A.M) : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem));
+        smem = std::max(smem, m1 ? qzb::sweep_m1_smem_bytes(A.M)
+                                 : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0));
         mom_off[i] = mom_total;
         mom_total += (size_t)(nsteps + 1) * std::max(1, b->inst[i]->dev.nbeams) * 17;
     }
     int sms = 0;
-    const int grid = std::min(qzb::batch_max_grid(b->ord, with_m1, smem, &sms), ni);
+    const int grid = std::min(qzb::batch_max_grid(b->ord, with_m1, with_ext, smem, &sms), ni);
     if (grid < 1) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the batch kernel cannot be resident here");
     const size_t need = (size_t)grid;
     if (b->fld_alloc < need * fmax || b->diag_alloc < need * dmax || b->bsrc_alloc < need * bmax) {
@@ -2068,6 +2068,7 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     B.dt = dt;
     B.ord = b->ord;
     B.with_m1 = with_m1 ? 1 : 0;
+    B.with_ext = with_ext ? 1 : 0;
     B.fld = b->d_fld; B.diag = b->d_diag; B.bsrc = b->d_bsrc;
     B.fld_slot = fmax; B.diag_slot = dmax; B.bsrc_slot = bmax;
     B.next = b->d_next;

@@ -105,7 +105,8 @@ __device__ void beam_deposit0(const BatchInst& I, const SweepArgs& A) {
 
 // WITH_M1: the batch holds modes = 1 instances (the m = 0 only variant keeps the m = 1 body out of the
 // kernel and its register allocation)
-template <int ORD, bool WITH_M1>
+// EXT: the variant whose sweeps handle the smoothing filter (some instance has plasma.smooth_length)
+template <int ORD, bool WITH_M1, bool EXT>
 __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_constant__ BatchArgs B) {
     extern __shared__ double smem_raw[];
     __shared__ BatchInst I;
@@ -131,12 +132,12 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
         for (int n = 0; n <= B.nsteps; ++n) {
             NoGate g;
             if (WITH_M1 && I.modes) {
-                if constexpr (WITH_M1) sweep_m1_body<ORD>(A, smem_raw, g);
+                if constexpr (WITH_M1) sweep_m1_body<ORD, NoGate, EXT>(A, smem_raw, g);
             } else if (A.rows_per_thread == 1) {
-                if (reg) sweep_body<ORD, true, 1>(A, smem_raw, g);
-                else sweep_body<ORD, false, 1>(A, smem_raw, g);
+                if (reg) sweep_body<ORD, true, 1, NoGate, EXT>(A, smem_raw, g);
+                else sweep_body<ORD, false, 1, NoGate, EXT>(A, smem_raw, g);
             } else {
-                sweep_body<ORD, false, 4>(A, smem_raw, g);
+                sweep_body<ORD, false, 4, NoGate, EXT>(A, smem_raw, g);
             }
             __syncthreads();
             beam_phase(I, A, B, n, n < B.nsteps, n == 0, red);
@@ -145,63 +146,66 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
     }
 }
 
-template <int ORD, bool WITH_M1>
+template <int ORD, bool WITH_M1, bool EXT>
 cudaError_t launch_t(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
     cudaError_t e =
-        cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    batch_kernel<ORD, WITH_M1><<<grid, kSweepThreads, smem, s>>>(B);
+    batch_kernel<ORD, WITH_M1, EXT><<<grid, kSweepThreads, smem, s>>>(B);
     return cudaGetLastError();
 }
 
-template <int ORD, bool WITH_M1>
+template <int ORD, bool WITH_M1, bool EXT>
 int occupancy_t(size_t smem) {
-    if (cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-        cudaSuccess)
+    if (cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
         return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD, WITH_M1>, kSweepThreads, smem) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD, WITH_M1, EXT>, kSweepThreads, smem) !=
         cudaSuccess)
         return 0;
     return nb;
 }
 
-template <bool WITH_M1>
+template <bool WITH_M1, bool EXT>
 int occupancy_any(int ord, size_t smem) {
     switch (ord) {
-        case 1: return occupancy_t<1, WITH_M1>(smem);
-        case 2: return occupancy_t<2, WITH_M1>(smem);
-        case 3: return occupancy_t<3, WITH_M1>(smem);
-        case 4: return occupancy_t<4, WITH_M1>(smem);
-        case 5: return occupancy_t<5, WITH_M1>(smem);
+        case 1: return occupancy_t<1, WITH_M1, EXT>(smem);
+        case 2: return occupancy_t<2, WITH_M1, EXT>(smem);
+        case 3: return occupancy_t<3, WITH_M1, EXT>(smem);
+        case 4: return occupancy_t<4, WITH_M1, EXT>(smem);
+        case 5: return occupancy_t<5, WITH_M1, EXT>(smem);
         default: return 0;
     }
 }
 
-template <bool WITH_M1>
+template <bool WITH_M1, bool EXT>
 cudaError_t launch_any(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
     switch (B.ord) {
-        case 1: return launch_t<1, WITH_M1>(B, grid, smem, s);
-        case 2: return launch_t<2, WITH_M1>(B, grid, smem, s);
-        case 3: return launch_t<3, WITH_M1>(B, grid, smem, s);
-        case 4: return launch_t<4, WITH_M1>(B, grid, smem, s);
-        case 5: return launch_t<5, WITH_M1>(B, grid, smem, s);
+        case 1: return launch_t<1, WITH_M1, EXT>(B, grid, smem, s);
+        case 2: return launch_t<2, WITH_M1, EXT>(B, grid, smem, s);
+        case 3: return launch_t<3, WITH_M1, EXT>(B, grid, smem, s);
+        case 4: return launch_t<4, WITH_M1, EXT>(B, grid, smem, s);
+        case 5: return launch_t<5, WITH_M1, EXT>(B, grid, smem, s);
         default: return cudaErrorInvalidValue;
     }
 }
 
 }  // namespace
 
-int batch_max_grid(int ord, bool with_m1, size_t smem, int* sms) {
+int batch_max_grid(int ord, bool with_m1, bool with_ext, size_t smem, int* sms) {
     int dev = 0, nsm = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    return (with_m1 ? occupancy_any<true>(ord, smem) : occupancy_any<false>(ord, smem)) * nsm;
+    const int per = with_m1 ? (with_ext ? occupancy_any<true, true>(ord, smem) : occupancy_any<true, false>(ord, smem))
+                            : (with_ext ? occupancy_any<false, true>(ord, smem) : occupancy_any<false, false>(ord, smem));
+    return per * nsm;
 }
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    return B.with_m1 ? launch_any<true>(B, grid, smem, s) : launch_any<false>(B, grid, smem, s);
+    if (B.with_m1) return B.with_ext ? launch_any<true, true>(B, grid, smem, s) : launch_any<true, false>(B, grid, smem, s);
+    return B.with_ext ? launch_any<false, true>(B, grid, smem, s) : launch_any<false, false>(B, grid, smem, s);
 }
 
 }  // namespace qzb

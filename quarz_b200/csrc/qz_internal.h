@@ -268,12 +268,13 @@ struct BatchArgs {
     double dt;
     int ord;
     int with_m1;                    // some instances have modes = 1
+    int with_ext;                   // some instances use the smoothing filter (the kernel variant with it)
     double *fld, *diag, *bsrc;      // per slot (= CTA)
     size_t fld_slot, diag_slot, bsrc_slot;
     int* next;                      // queue head (0)
 };
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t stream);
-int batch_max_grid(int ord, bool with_m1, size_t smem, int* sms);
+int batch_max_grid(int ord, bool with_m1, bool with_ext, size_t smem, int* sms);
 
 }  // namespace qzb

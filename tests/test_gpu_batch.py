@@ -5,7 +5,9 @@ Instances are drawn like the scan workload (quarz_b200.workloads.scan_instances:
 stretched grids, xi lengths 8-16) with 4000 beam particles and 3 steps. Tolerances: derived beam
 moments 1e-10 relative to their natural scale against the single runs (only the summation order of
 the beam deposits differs), 1e-8 against the oracle. The m = 1 case draws the same way with modes 0, 1
-(Picard 3, 4 azimuths per ring, 128-511 cells), mixed in one batch with m = 0 instances."""
+(Picard 3, 4 azimuths per ring, 128-511 cells), mixed in one batch with m = 0 instances; and a batch of
+m = 0 and m = 1 instances of which three smooth their plasma sources (plasma.smooth_length = 0.02), run by
+the kernel variant with the filter."""
 import numpy as np
 import pytest
 
@@ -72,3 +74,22 @@ def test_batch_m1_refuses_wide_grids():
     spec.nodes = workloads.scan_nodes(700, 1e-3)
     with pytest.raises(Q.QZError, match="M <= 512"):
         Q.Batch().add(spec)
+
+
+def test_batch_with_smoothing():
+    m0 = workloads.scan_instances(3, seed=21, beam_particles=2000, steps=2)
+    m1 = workloads.scan_instances(2, seed=22, beam_particles=2000, steps=2, modes=1)
+    specs = m0 + m1
+    for i in (0, 2, 3):
+        specs[i].smooth_length = 0.02
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    batch = Q.Batch()
+    for s, bm in zip(specs, beams):
+        batch.add(s, bm)
+    moms = batch.run(2, specs[0].dt)
+    for s, bm, mom in zip(specs, beams, moms):
+        sim = Q.Simulation(s, beams=bm)
+        sim.set_schedule(False)
+        _close(s, mom, sim.run(2, s.dt), bm, 1e-10)
+    s, bm, mom = specs[0], beams[0], moms[0]
+    _close(s, mom, O.OracleSim(s, beams=bm).run(2, s.dt), bm, 1e-8)

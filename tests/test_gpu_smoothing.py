@@ -152,10 +152,3 @@ def test_filter_m1_one_sweep():
 
 def test_filter_m1_runs_against_oracle():
     _runs_against_oracle(_hosing_filtered(), 2)
-
-
-def test_filter_refusals():
-    spec = _blowout()
-    with pytest.raises(Q.QZError) as e:
-        Q.Batch().add(spec)
-    assert e.value.code == 3
