@@ -20,8 +20,10 @@ Other workloads (not the headline; their lines are recorded beside it):
   --workload scan_m1  the same scan with azimuthal modes 0 and 1 (M <= 512)
   --workload adjoint  the gradient of witness energy gain and spread with respect to a 64-bin driver
                       profile and the witness delay, pinched witness over 50 steps: adjoint / forward time
+  --smooth A          the pinched-witness or hosing run with plasma.smooth_length = A (the radial
+                      smoothing of the plasma sources; 0.005 in the reference's validation section 14)
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--workload ...] [--smooth A]
 """
 from __future__ import annotations
 
