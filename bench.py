@@ -56,17 +56,29 @@ def _peaks():
         return 6650.0, "fallback"
 
 
+def _library_source():
+    """The source hash the loaded library was built from (qz_version: '... src <hash>')."""
+    import quarz_b200 as Q
+
+    v = Q.lib().qz_version()
+    v = v.decode() if isinstance(v, bytes) else str(v)
+    m = re.search(r"src ([0-9a-f]+|unknown)", v)
+    return m.group(1) if m else "unknown"
+
+
 def _traffic_ratio():
     """DRAM bytes per algorithmic byte of the pipelined kernel, from the ncu capture of a shorter run of
     the same workload summarised in profiles/ (traffic grows with the steps like the algorithmic bytes),
-    or None."""
+    and the library source hash that capture measured. Returns (ratio or None, measured hash or None)."""
     path = os.path.join(ROOT, "profiles", "pipeline_kernel_pinched_witness.md")
     try:
         with open(path) as f:
-            m = re.search(r"dram_bytes_per_algorithmic_byte:\s*([0-9.eE+]+)", f.read())
-        return float(m.group(1)) if m else None
+            text = f.read()
     except OSError:
-        return None
+        return None, None
+    m = re.search(r"dram_bytes_per_algorithmic_byte:\s*([0-9.eE+]+)", text)
+    h = re.search(r"library source:\s*([0-9a-f]+)", text)
+    return (float(m.group(1)) if m else None), (h.group(1) if h else None)
 
 
 def _config(spec, nb_total, steps, extra=None, workload=WORKLOAD):
@@ -93,11 +105,109 @@ def algorithmic_bytes(spec, nb_total, steps):
     return (steps + 1) * sweep + steps * push
 
 
+# FP64 operations of the reference algorithm, counted from the cited reference lines (per plasma particle
+# per slice; per radial node per slice; per beam particle per time step). m = 0:
+#   plasma particle: deposit (src/PlasmaSpecies.cpp:409-478) 47 + S deposit with its field gather
+#   (:508-559) 102 + AB3 push with its gather (:561-668) 110 + two cell lookups / weights 24 + the 12
+#   deposit additions of the warp sums = 295;
+#   radial node: 5 Thomas solves x 8 (psi, E_z, B_z, B_r, B_theta; src/Tridiag.cpp:111-125) + source
+#   combination, stencils, W+, the B+ right-hand sides and the slice store (src/Simulation.cpp:408-633)
+#   60 = 100;
+#   beam particle: bilinear gather of 6 components 36 + Vay (src/Pushers.hpp:36-68) 60 + drift and
+#   weights 24 + the linear deposit of 5 components on 4 points (src/Beam.cpp:725-785) 60 = 180.
+# m = 1 (8 azimuths, 27 solves, Picard 3; gathers of 18 components, deposits of 15):
+#   plasma particle 470, radial node 400, beam particle 330.
+FLOPS = {0: (295, 100, 180), 1: (470, 400, 330)}
+
+
+def run_flops(spec, nb_total, steps):
+    """FP64 operations of a run: (steps + 1) sweeps of K slices and `steps` pushes of every beam particle."""
+    fp, fm, fb = FLOPS[spec.modes]
+    npl = (spec.M - 1) * (spec.species[0].ntheta if spec.modes == 1 else 1) * spec.species[0].ppc
+    return (steps + 1) * spec.K * (npl * fp + spec.M * fm) + steps * nb_total * fb
+
+
+# Latency floor of one m = 0 slice on one SM (cycles): its dependent chain. Per slice the sweep runs 5
+# block scans (psi / E_z / B_z forward and backward, the B+ pivot scan and its two substitutions share
+# one pass each way) and 4 further barriers. A block scan is a 5-level warp-shuffle scan (shuffle ~24 +
+# FP64 FMA ~8 cycles per level), two shared-memory round trips (~60), the scan of the 16 warp carries
+# (~130) and its barrier (~45): ~400 cycles. A plasma particle's chain per slice (push, cell lookup by
+# a 9-level binary search in shared memory, two divides of ~68 cycles, the S and plasma deposits with
+# their warp sums) is ~2,000 cycles. Barrier and divide costs are the ones measured on this part with
+# clock64 counters; the shuffle and FMA latencies are those of the CUDA documentation's latency tables.
+SLICE_FLOOR_CYCLES = {"block_scans": 5 * 400, "barriers": 4 * 45, "particle_chain": 2000}
+
+
+def fp64_gemm_tflops(dev, n=8192, reps=3):
+    """Measured FP64 peak: cuBLAS DGEMM (torch.matmul, float64, n^3) on this GPU, best of reps."""
+    import torch
+
+    a = torch.randn(n, n, dtype=torch.float64, device=dev)
+    b = torch.randn(n, n, dtype=torch.float64, device=dev)
+    torch.matmul(a, b)
+    torch.cuda.synchronize(dev)
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        torch.matmul(a, b)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        best = min(best, e0.elapsed_time(e1))
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def sweep_latency(spec, beams, dev, sim, steps_traced):
+    """Per-slice latency of the sweep: stand-alone (one qz_sweep_run of the initial beams' sources, on one
+    SM) and inside the pipelined run (from the run trace: the time sweep n takes from its first to its
+    last slice, median over the steps), in us; the stand-alone sweep's phase cycles per slice."""
+    import numpy as np
+    import torch
+
+    import quarz_b200 as Q
+
+    grid = Q.RadialGrid(spec.nodes)
+    sw = Q.Sweep(grid, Q.sweep_params(spec))
+    K, M = spec.K, spec.M
+    f64 = dict(dtype=torch.float64, device=dev)
+    bsrc = torch.zeros(K * M * 5, **f64)
+    fld = torch.zeros(K * M * 6, **f64)
+    diag = torch.zeros(K * M * 3, **f64)
+    box = Q.BeamOps.box(spec.xi_min, spec.dxi, K, spec.ngp, spec.modes)
+    for b, (parts, _, _) in zip(spec.beams, beams):
+        cols = torch.from_numpy(np.ascontiguousarray(parts.T)).to(dev).contiguous()
+        Q.BeamOps.deposit(grid, cols, b.q, b.m, box, bsrc)
+    sw.run(bsrc, fld, diag)
+    ms = []
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sw.run_async(bsrc, fld, diag)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms.append(e0.elapsed_time(e1))
+    alone = 1e3 * min(ms) / K
+    sw.timing(True)
+    sw.run(bsrc, fld, diag)
+    cyc = sw.timing(False).astype(np.float64) / K
+    del sw, bsrc, fld, diag
+    sim.trace(True)
+    sim.run(steps_traced, spec.dt)
+    per, _ = sim.trace(False)
+    pace = float(np.median((per[:, 1] - per[:, 0]) / K)) * 1e-3
+    return {"sweep_us_per_slice_standalone": alone, "sweep_us_per_slice_in_pipeline": pace,
+            "standalone_phase_cycles_per_slice": {"psi_ez_bz": float(cyc[1]), "s_deposit": float(cyc[2]),
+                                                  "bplus": float(cyc[3]), "store_push_deposit": float(cyc[4])}}
+
+
 class ClockSampler:
     """NVML samples of SM clock and throttle reasons during the timed region."""
 
     def __init__(self, index):
         self.samples, self.reasons, self.max_mhz = [], set(), None
+        self.mem_used_max = 0
         self._stop = threading.Event()
         try:
             import pynvml
@@ -116,6 +226,7 @@ class ClockSampler:
         while not self._stop.is_set():
             try:
                 self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                self.mem_used_max = max(self.mem_used_max, int(nv.nvmlDeviceGetMemoryInfo(self.h).used))
                 r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
                 for k, bit in names.items():
                     if r & bit:
@@ -202,7 +313,7 @@ def run_b200(args, rank, world, local_rank):
     e2e = run_e2e(args, spec, beams, sim, dev) if args.e2e_steps > 0 else None
     launches = (OWN_LAUNCHES_PER_BEAM * len(beams) + OWN_LAUNCHES_PER_RUN) * args.steps
     return {"ms": ms, "kernel_ms": kernel_ms, "clocks": clk.result(), "spec": spec, "nb_total": nb_total,
-            "launches": launches, "e2e": e2e, "schedule": sched}
+            "launches": launches, "e2e": e2e, "schedule": sched, "beams": beams, "sim": sim, "dev": dev}
 
 
 def run_e2e(args, spec, beams, sim, dev):
@@ -229,6 +340,46 @@ def run_e2e(args, spec, beams, sim, dev):
     nbytes = sum(7 * 8 * len(p) for p, _, _ in beams)
     return {"ms_per_run": sum(ms) / len(ms), "h2d_bytes_per_step": nbytes,
             "d2h_bytes_per_step": nbytes + 17 * 8 * len(beams) * (spec.steps + 1)}
+
+
+def run_hosing_extra(dev, steps=2, warmup=1, cpu_steps=1):
+    """The hosing run (modes 0 and 1, 2e6 + 2e6 particles, 200 steps) through qz_sim_run: slice-solves/s
+    on the device, and the oracle on the host threads for the same unit."""
+    import numpy as np
+    import torch
+
+    import quarz_b200 as Q
+    from quarz_b200 import workloads
+
+    spec = workloads.hosing()
+    T = spec.steps
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    sim = Q.Simulation(spec, beams=beams)
+    init = [torch.from_numpy(np.ascontiguousarray(p.T)).to(dev).contiguous() for p, _, _ in beams]
+    ms = []
+    for it in range(warmup + steps):
+        for b in range(len(init)):
+            sim.set_beam(b, init[b])
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sim.run(T, spec.dt)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        if it >= warmup:
+            ms.append(e0.elapsed_time(e1))
+    del sim, init
+    torch.cuda.empty_cache()
+    nb = sum(len(p) for p, _, _ in beams)
+    per = sum(ms) / len(ms)
+    out = {"metric": METRIC, "value": spec.K * (T + 1) / (per * 1e-3), "unit": UNIT, "ms_per_run": per,
+           "runs_timed": steps, "config": _config(spec, nb, T, None, "hosing"),
+           "beam_pushes_per_s": nb * T / (per * 1e-3)}
+    rate, el = oracle_rate(cpu_steps, 0, spec)
+    out["cpu_baseline"] = {"value": rate, "unit": UNIT, "cores": oracle_rate.threads, "kind": "port",
+                           "sample": f"{cpu_steps} full time step(s) of the hosing run (sweep + moment sums + push "
+                                     f"of 4e6 particles), oracle on {oracle_rate.threads} host threads, {el:.1f} s"}
+    return out
 
 
 def run_scan(args, rank, world, local_rank):
@@ -358,6 +509,9 @@ def run_adjoint(args, rank, world, local_rank):
             "adjoint_split_ms": {"forward_keeping_beams": float(np.median([m[0] for m in split])),
                                  "reverse": float(np.median([m[1] for m in split]))},
             "gradient_norm_profile": float(np.linalg.norm(grads[0])), "gradient_delay": grads[1],
+            "peak_device_bytes": clk.mem_used_max,
+            "peak_device_bytes_note": "NVML memory used on the device during the gradients (the whole process: "
+                                      "the forward run's own buffers and torch's cache included)",
             "clocks": clk.result(),
             # per gradient: the forward run's own kernels (per beam: iota, cell keys, reorder, group starts,
             # step-0 deposit; the pipeline, the moment reduction), the reverse pass's (bucket cells, running
@@ -442,6 +596,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3, help="timed runs through the host-buffer call")
     ap.add_argument("--cpu-steps", type=int, default=10, help="oracle time steps of the cpu_baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline only: no latency roofline, FP64 rate or hosing / scan / adjoint lines")
     ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
     ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1", "adjoint"],
                     default="pinched_witness")
@@ -523,7 +679,9 @@ def main():
     alg = algorithmic_bytes(spec, nbt, T)
     hbm, peak_kind = _peaks()
     achieved = alg / (kms * 1e-3) / 1e9
-    ratio = _traffic_ratio()
+    ratio, measured_src = _traffic_ratio()
+    lib_src = _library_source()
+    fresh = ratio is not None and measured_src == lib_src
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
@@ -532,10 +690,14 @@ def main():
         "kernel_ms_per_run": kms, "per_sweep_ms": kms / (T + 1),
         "roofline": {"bound": "hbm", "kernel": "pipeline_kernel", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                      "frac": achieved / hbm, "peak_kind": peak_kind,
-                     "traffic": ratio * alg if ratio else None,
+                     "traffic": ratio * alg if fresh else None,
+                     "traffic_source": (f"ncu capture of this library build (src {lib_src}), scaled by steps"
+                                        if fresh else
+                                        f"stale: the ncu capture measured src {measured_src}, this library is "
+                                        f"src {lib_src}"),
                      "algorithmic_bytes": alg,
                      "note": "one launch per run; its floor is one sweep's dependent chain (K slices, one SM) "
-                             "plus the step-to-step stagger, not HBM: see DESIGN.md"},
+                             "plus the step-to-step stagger, not HBM: the latency and fp64 entries measure it"},
         "clocks": r["clocks"], "gpu_launches": r["launches"],
     }
     if r["e2e"]:
@@ -549,12 +711,70 @@ def main():
                                 "sample": f"{args.cpu_steps} full time steps of the same workload (sweep + moment "
                                           f"sums + beam push), oracle on {oracle_rate.threads} host threads, "
                                           f"{el:.1f} s"}
+    if rank == 0 and world == 1 and not args.no_extras:
+        line.update(extras(args, r, line))
     if world > 1:
         import torch
 
         torch.distributed.destroy_process_group()
     if rank == 0:
         print(json.dumps(line))
+
+
+def extras(args, r, line):
+    """Measurements beside the headline (one GPU, default run): the sweep's latency roofline and FP64
+    rate, and the other configurations' lines (hosing, the batched scan, the adjoint), each bounded to
+    a few runs."""
+    import types
+
+    import torch
+
+    spec, dev = r["spec"], r["dev"]
+    T = spec.steps
+    out = {}
+    lat = sweep_latency(spec, r["beams"], dev, r["sim"], T)
+    sm_mhz = (r["clocks"] or {}).get("sm_mhz") or 1965.0
+    floor_cyc = sum(SLICE_FLOOR_CYCLES.values())
+    floor_us = floor_cyc / sm_mhz
+    lat.update({"floor_us_per_slice": floor_us, "floor_cycles_per_slice": floor_cyc,
+                "floor_model": "per slice: 5 block scans x ~400 cycles (5 warp-shuffle levels, two shared-memory "
+                               "round trips, the scan of 16 warp carries, one barrier) + 4 barriers x 45 cycles + one "
+                               "plasma particle's dependent chain ~2,000 cycles, at the median SM clock under load",
+                "frac_standalone": floor_us / lat["sweep_us_per_slice_standalone"],
+                "frac_in_pipeline": floor_us / lat["sweep_us_per_slice_in_pipeline"]})
+    del r["sim"]
+    torch.cuda.empty_cache()
+    line["roofline"]["latency"] = lat
+    kms = line["kernel_ms_per_run"]
+    fl = run_flops(spec, r["nb_total"], T)
+    peak64 = fp64_gemm_tflops(dev)
+    sweeps = r["schedule"].get("sweep_ctas") or 1
+    achieved = fl / (kms * 1e-3) / 1e12
+    line["roofline"]["fp64"] = {
+        "flops_per_run": fl, "achieved_tflops": achieved, "peak_tflops": peak64,
+        "peak_kind": "measured here: cuBLAS DGEMM (torch.matmul float64 8192^3, best of 3); MEASURED_PEAKS.json "
+                     "has no FP64 figure", "frac": achieved / peak64,
+        "sweep_sms": sweeps, "frac_of_sweep_sms": achieved / (peak64 * sweeps / 148.0),
+        "flops_model": "per plasma particle per slice 295, per radial node per slice 100, per beam particle per "
+                       "step 180 (m = 0; counted from the reference lines the kernels restate)"}
+    out["hosing"] = run_hosing_extra(dev)
+    sub = types.SimpleNamespace(workload="scan", steps=1, warmup=1, time_steps=0)
+    sc = run_scan(sub, 0, 1, dev.index or 0)
+    rate, el = oracle_scan_rate(4, 0, 0)
+    sc["cpu_baseline"] = {"value": rate, "unit": "runs/s", "cores": oracle_scan_rate.threads, "kind": "port",
+                          "sample": f"one full time step of each of 4 instances sampled across the scan, oracle on "
+                                    f"{oracle_scan_rate.threads} host threads, {el:.1f} s; a run = 21 such steps"}
+    sc["speedup_vs_pipelined_loop"] = sc["value"] / sc["loop_runs_per_s"]["pipelined"]
+    out["scan"] = {k: sc[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "loop_runs_per_s",
+                                      "speedup_vs_step_by_step_loop", "speedup_vs_pipelined_loop", "cpu_baseline")}
+    torch.cuda.empty_cache()
+    sub = types.SimpleNamespace(workload="adjoint", steps=2, warmup=1, time_steps=50)
+    ad = run_adjoint(sub, 0, 1, dev.index or 0)
+    out["adjoint"] = {k: ad[k] for k in ("metric", "value", "unit", "forward_ms", "adjoint_ms", "adjoint_split_ms",
+                                         "config") if k in ad}
+    if "peak_device_bytes" in ad:
+        out["adjoint"]["peak_device_bytes"] = ad["peak_device_bytes"]
+    return out
 
 
 if __name__ == "__main__":

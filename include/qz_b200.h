@@ -39,7 +39,7 @@ const char* qz_last_error(void);
 const char* qz_version(void);
 
 /* ------------------------------------------------------------------ radial grid + operators
- * Replaces RadialGrid::RadialGrid(nodes) + RadialGrid::finalize (src/RadialGrid.cpp:229-273) and
+ * Replaces RadialGrid::RadialGrid(nodes) + RadialGrid::finalize (src/RadialGrid.cpp:104-148) and
  * FieldSolver::FieldSolver (src/FieldSolver.cpp:113-179): hat-function volumes, the tridiagonal
  * rows of L0 / L1D / L1F / L2D and the gradient stencils, uploaded to the device.
  * nodes: host, M values, 0 = r_0 < r_1 < ... < r_{M-1} = R. */
@@ -165,7 +165,9 @@ qz_status qz_beam_slice_sums(const qz_beam_view* b, double lo, double hi, int nb
    (user xi, increasing: the head of the box is the last row), int32 ncomp, then ncomp x {char name[16],
    float64 data[K][M]}; names psi ez er eth br bth bz ne ni rhob, and with modes = 1 <name>_c / <name>_s of
    psi ez bz ne ni rhob er eth br bth. fld (K, M, F_NC), diag (K, M, D_NC), bsrc (K, M, B_NC; NULL writes a
-   zero rhob) are device arrays when on_device != 0, else host arrays; nodes_host: the M radial nodes. */
+   zero rhob) are device arrays when on_device != 0, else host arrays; nodes_host: the M radial nodes.
+   Columns of parts this library does not build are not written: the densities of ionizable species
+   (nz_<species>) and the laser envelope (a_re, a_im). */
 qz_status qz_write_fields(const char* path, const double* nodes_host, int M, const qz_box* box, double t,
                           const double* fld, const double* diag, const double* bsrc, int on_device);
 
@@ -211,8 +213,10 @@ qz_status qz_sim_set_beam_pusher(qz_sim* s, int b, int pusher);
 /* qz_beam_slice_sums of particle beam b of the sim as it stands (after the last run), into out_host
    (9 x nbins, host) */
 qz_status qz_sim_beam_slice_sums(qz_sim* s, int b, double lo, double hi, int nbins, double* out_host);
-/* qz_write_fields of the sim's last sweep (fields, diagnostics and the beam sources it read: the beams as
-   they stand plus the analytic ones) at time t */
+/* qz_write_fields of the sim's last sweep at time t: its fields and diagnostics, and as rhob the beam
+   sources re-deposited from the beams as they stand (not pushed after that sweep) plus the analytic
+   ones. The re-deposit sums in another order than the deposit the sweep read, so rhob agrees with
+   the sources of that sweep to rounding, not bit for bit. */
 qz_status qz_sim_write_fields(qz_sim* s, double t, const char* path);
 /* run nsteps (nsteps+1 sweeps); moments_host: (nsteps+1, nbeams, 17) or NULL.
    By default (modes 0 or 1, at most 4 beams) the whole run is ONE cooperative launch in which the sweeps of

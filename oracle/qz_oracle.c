@@ -81,7 +81,7 @@ int qzo_make_uniform(double R, double dr, double* out, int cap) {
     return (int)(n + 1);
 }
 
-/* src/RadialGrid.cpp:152-196 */
+/* src/RadialGrid.cpp:27-71 */
 static double regions_target(double x, const double* ends, const double* hs, int nreg, double g) {
     double ht = hs[nreg - 1];
     for (int i = 0; i < nreg; ++i)
@@ -125,7 +125,7 @@ typedef struct {
     double *r, *h, *rmid, *V, *inv_h, *inv_V;
 } grid_t;
 
-/* src/RadialGrid.cpp:231-273 */
+/* src/RadialGrid.cpp:106-148 */
 static int grid_init(grid_t* g, const double* nodes, int M) {
     if (M < 3 || nodes[0] != 0.0) return -1;
     for (int j = 1; j < M; ++j)
@@ -159,7 +159,7 @@ static void grid_free(grid_t* g) {
     free(g->r); free(g->V); free(g->inv_V); free(g->h); free(g->rmid); free(g->inv_h);
 }
 
-/* src/RadialGrid.hpp:73-88 */
+/* src/RadialGrid.hpp:35-50 */
 static inline int grid_locate(const grid_t* g, double x) {
     if (x <= 0.0) return 0;
     if (x >= g->R) return g->N - 1;
@@ -179,7 +179,7 @@ static inline void grid_weights(const grid_t* g, double x, int* j, double* t) {
 }
 
 /* ===================================================================== tridiagonal */
-/* src/Tridiag.cpp:445-459 */
+/* src/Tridiag.cpp:111-125 */
 static void thomas(int M, const double* a, const double* b, const double* c, const double* d, double* x,
                    double* cp, double* dp) {
     cp[0] = c[0] / b[0];
@@ -193,7 +193,7 @@ static void thomas(int M, const double* a, const double* b, const double* c, con
     for (int i = M - 2; i >= 0; --i) x[i] = dp[i] - cp[i] * x[i + 1];
 }
 
-/* src/Tridiag.cpp:462-496: PCR over the whole system (work: 8*M doubles) */
+/* src/Tridiag.cpp:127-162: PCR over the whole system (work: 8*M doubles) */
 static void pcr(int M, const double* a, const double* b, const double* c, const double* d, double* x,
                 double* work) {
     double *pa[2], *pb[2], *pc[2], *pd[2];
@@ -220,7 +220,7 @@ static void pcr(int M, const double* a, const double* b, const double* c, const 
     for (int i = 0; i < M; ++i) x[i] = pd[src][i] / pb[src][i];
 }
 
-/* src/Tridiag.cpp:341-443: Laszlo-Giles-Appleyard partition, P = min(256, M/8) chunks */
+/* src/Tridiag.cpp:30-109: Laszlo-Giles-Appleyard partition, P = min(256, M/8) chunks */
 static void partition(int M, const double* a, const double* b, const double* c, const double* d, double* x,
                       double* work) {
     const int P = M / 8 < 256 ? M / 8 : 256, R = 2 * P;
@@ -408,7 +408,7 @@ static void solver_free(solver_t* s) {
     grid_free(&s->g);
 }
 
-/* src/FieldSolver.cpp:242-261 */
+/* src/FieldSolver.cpp:172-191 */
 static void solver_solve(solver_t* s, int k, const double* rhs, double* f, const double* chi, const double* wall,
                          double scale) {
     const op_t* o = &s->L[k];
@@ -485,7 +485,7 @@ int qzo_filter(const double* nodes, int M, double a2, int n, double* f) {
     return 0;
 }
 
-/* src/FieldSolver.cpp:263-289 */
+/* src/FieldSolver.cpp:193-219 */
 static void solver_gradient(const solver_t* s, const double* f, double* df) {
     const int N = s->g.N;
     for (int j = 0; j <= N; ++j) {
@@ -544,7 +544,7 @@ int qzo_grid_volumes(const double* nodes, int M, double* V) {
     return 0;
 }
 
-/* ===================================================================== pushers (src/Pushers.hpp:144-176) */
+/* ===================================================================== pushers (src/Pushers.hpp:36-68) */
 typedef struct { double x, y, z; } v3;
 static inline v3 v3add(v3 a, v3 b) { v3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
 static inline v3 v3mul(double s, v3 a) { v3 r = {s * a.x, s * a.y, s * a.z}; return r; }

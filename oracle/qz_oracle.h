@@ -6,17 +6,17 @@
  * host cores.
  *
  * What it restates (QUARZ v2.0.0, file:line within the reference project):
- *   radial grid          src/RadialGrid.cpp:139-196 (generators), :231-273 (volumes)
+ *   radial grid          src/RadialGrid.cpp:14-86 (generators), :106-148 (volumes)
  *   field operators      src/FieldSolver.cpp:90-103 (fv_rows), :113-179 (L0/L1D/L1F/L2D, stencils)
- *   solve / gradients    src/FieldSolver.cpp:242-289
- *   tridiagonal          src/Tridiag.cpp:362-496 (Thomas, PCR, partition)
+ *   solve / gradients    src/FieldSolver.cpp:172-219
+ *   tridiagonal          src/Tridiag.cpp:28-162 (Thomas, PCR, partition)
  *   plasma species      src/PlasmaSpecies.cpp:14-48 (AB), :57-89 (geometry/gather), :202-295 (load),
  *                        :409-478 (deposit), :480-506 (deposit_rho), :508-559 (deposit_S), :561-668 (push)
  *   sweep                src/Simulation.cpp:394-457 (zero/combine), :477-633 (W+, Bz, B+, store),
  *                        :636-795 (step_fields), :797-819 (solve_slice_fields), :1370-1448 (run)
  *   beam                 src/Beam.cpp:483-570 (gaussian sampler), :725-785 (deposit), :900-905 (push),
  *                        :948-1131 (advance, Vay only), :1133-1192 (sums / from_sums)
- *   pushers              src/Pushers.hpp:144-176 (gamma2_root, solve_implicit, vay)
+ *   pushers              src/Pushers.hpp:36-68 (gamma2_root, solve_implicit, vay)
  *   adjoint (m = 0)      qz_oracle_adj.c: the reverse of all of the above for one run (no
  *                        reference counterpart; pinned by central differences of this forward)
  *   mode sums            src/SliceData.hpp:70-83

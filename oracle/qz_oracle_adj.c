@@ -10,10 +10,10 @@
  * What it differentiates (QUARZ file:line of the forward steps, in reverse order):
  *   beam moment sums         src/Beam.cpp:1133-1155
  *   beam push                src/Beam.cpp:900-905 (start-up half kick), :948-1131 (gather, Vay, drift)
- *   Vay                      src/Pushers.hpp:144-176
+ *   Vay                      src/Pushers.hpp:36-68
  *   slice store              src/Simulation.cpp:594-633
  *   plasma push (AB, wall)   src/PlasmaSpecies.cpp:561-668
- *   B+ solves with chi       src/Simulation.cpp:535-591, src/FieldSolver.cpp:242-261
+ *   B+ solves with chi       src/Simulation.cpp:535-591, src/FieldSolver.cpp:172-191
  *   S deposit                src/PlasmaSpecies.cpp:508-559
  *   B_z, W+, psi, E_z        src/Simulation.cpp:477-532, :797-819
  *   combine sources          src/Simulation.cpp:408-457

@@ -9,7 +9,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 
 def build(verbose: bool = False) -> str:
     """Compile quarz_b200/csrc into quarz_b200/libqz_b200.so; returns its path."""
-    cmd = ["make", "-C", os.path.join(HERE, "csrc")]
+    cmd = ["make", "-j", str(max(1, min(8, os.cpu_count() or 1))), "-C", os.path.join(HERE, "csrc")]
     if not verbose:
         cmd.insert(1, "-s")
     subprocess.run(cmd, check=True)

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <functional>
+#include <mutex>
 #include <new>
 #include <random>
 #include <string>
@@ -85,7 +86,10 @@ void fv_rows(const qz_grid& g, int n, std::vector<double>& a, std::vector<double
 }  // namespace
 
 extern "C" const char* qz_last_error(void) { return g_err.c_str(); }
-extern "C" const char* qz_version(void) { return "qz_b200 0.1 (sm_100a, FP64)"; }
+#ifndef QZ_SRC_HASH
+#define QZ_SRC_HASH "unknown"
+#endif
+extern "C" const char* qz_version(void) { return "qz_b200 0.2 (sm_100a, FP64) src " QZ_SRC_HASH; }
 
 extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
     if (!nodes || !out) return fail(QZ_ERR_ARG, "qz_grid_create: null pointer");
@@ -96,7 +100,7 @@ extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
         if (!(nodes[j] > nodes[j - 1])) return fail(QZ_ERR_ARG, "grid: nodes must be strictly increasing");
     qz_grid* g = new (std::nothrow) qz_grid;
     if (!g) return fail(QZ_ERR_NOMEM, "qz_grid_create: out of host memory");
-    // src/RadialGrid.cpp:231-273
+    // src/RadialGrid.cpp:106-148
     g->M = M;
     g->N = M - 1;
     const int N = g->N;
@@ -165,7 +169,7 @@ extern "C" qz_status qz_grid_create(const double* nodes, int M, qz_grid** out) {
         std::vector<double> cs((size_t)13 * M, 0.0);
         auto put = [&](int k, const std::vector<double>& v) { std::copy(v.begin(), v.end(), cs.begin() + (size_t)k * M); };
         put(0, g->gm); put(1, g->g0); put(2, g->gp); put(3, g->ir);
-        // Thomas on L0 with its Dirichlet row N (src/Tridiag.cpp:445-459): u_i = b_i - a_i c_{i-1}/u_{i-1}
+        // Thomas on L0 with its Dirichlet row N (src/Tridiag.cpp:111-125): u_i = b_i - a_i c_{i-1}/u_{i-1}
         const std::vector<double>&a0 = g->opa[0], &b0 = g->opb[0], &c0 = g->opc[0];
         double cp = 0.0;
         for (int i = 0; i < M; ++i) {
@@ -627,25 +631,40 @@ extern "C" qz_status qz_beam_push_deposit(const qz_grid* g, qz_beam_view* b, con
 }
 
 namespace {
-// partial-sum scratch of qz_beam_sums, per device, grown on demand
-double* g_sum_scratch = nullptr;
-int g_sum_blocks = 0;
+// partial-sum scratch of qz_beam_sums, per device, grown on demand; kept with the context it was
+// allocated in (a cudaDeviceReset frees it with the context, and the next call allocates afresh)
+struct SumScratch {
+    unsigned long long ctx = 0;
+    double* ptr = nullptr;
+    int blocks = 0;
+};
+constexpr int kSumDevices = 64;
+SumScratch g_sum_scratch[kSumDevices];
+std::mutex g_sum_mu;
 }  // namespace
 
 extern "C" qz_status qz_beam_sums(const qz_beam_view* b, double gref, double xiref, double* out17, void* stream) {
     if (!b || !out17) return fail(QZ_ERR_ARG, "qz_beam_sums: null pointer");
+    if (b->n < 0) return fail(QZ_ERR_ARG, "qz_beam_sums: negative particle count");
     qzb::BeamArgs B{};
     B.x = b->x; B.y = b->y; B.px = b->px; B.py = b->py; B.pz = b->pz; B.xi = b->xi; B.w = b->w;
     B.n = (long)b->n;
     const int nb = qzb::beam_sums_blocks(B.n);
-    if (nb > g_sum_blocks) {
-        if (g_sum_scratch) cudaFree(g_sum_scratch);
-        g_sum_scratch = nullptr;
-        g_sum_blocks = 0;
-        QZ_CUDA(cudaMalloc((void**)&g_sum_scratch, sizeof(double) * 17 * nb));
-        g_sum_blocks = nb;
+    int dev = 0;
+    QZ_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kSumDevices) return fail(QZ_ERR_ARG, "qz_beam_sums: device ordinal out of range");
+    std::lock_guard<std::mutex> lock(g_sum_mu);
+    SumScratch& sc = g_sum_scratch[dev];
+    const unsigned long long ctx = qzb::current_context_id();
+    if (sc.ptr && ctx != 0 && ctx != sc.ctx) sc = SumScratch{};   // its context has ended, and the memory with it
+    if (nb > sc.blocks) {
+        if (sc.ptr) cudaFree(sc.ptr);
+        sc = SumScratch{};
+        QZ_CUDA(cudaMalloc((void**)&sc.ptr, sizeof(double) * 17 * nb));
+        sc.blocks = nb;
+        sc.ctx = qzb::current_context_id();
     }
-    QZ_CUDA(qzb::launch_beam_sums(B, gref, xiref, g_sum_scratch, nb, out17, (cudaStream_t)stream));
+    QZ_CUDA(qzb::launch_beam_sums(B, gref, xiref, sc.ptr, nb, out17, (cudaStream_t)stream));
     return QZ_OK;
 }
 
@@ -1717,40 +1736,44 @@ qz_status write_fields_host(const char* path, const double* nodes, int M, const 
                             const double* F, const double* D, const double* B) {
     const int K = box->K, m1 = box->modes == 1;
     const int fnc = m1 ? 18 : 6, dnc = m1 ? 9 : 3, bnc = m1 ? 15 : 5;
-    using Fn = std::function<double(size_t)>;        // value at (k, j), index k * M + j
-    std::vector<std::pair<std::string, Fn>> comps;
-    auto f = [&](int c) { return Fn([F, fnc, c](size_t kj) { return F[kj * fnc + c]; }); };
-    auto d = [&](int c) { return Fn([D, dnc, c](size_t kj) { return D[kj * dnc + c]; }); };
-    auto b = [&](int c) { return Fn([B, bnc, c](size_t kj) { return B ? B[kj * bnc + c] : 0.0; }); };
-    auto scaled = [](Fn a, double s) { return Fn([a, s](size_t kj) { return s * a(kj); }); };
-    auto sum = [](Fn a, Fn c, double sc) { return Fn([a, c, sc](size_t kj) { return a(kj) + sc * c(kj); }); };
+    // every written component is s0 * a[kj * na + ca] + s1 * b[kj * nb + cb] of the stored arrays (one
+    // or two columns), copied by a plain strided loop
+    struct Col { const double* p; int n, c; double s; };
+    struct Comp { std::string name; Col a, b; };
+    std::vector<Comp> comps;
+    const Col none{nullptr, 1, 0, 0.0};
+    auto f = [&](int c, double sc = 1.0) { return Col{F, fnc, c, sc}; };
+    auto d = [&](int c, double sc = 1.0) { return Col{D, dnc, c, sc}; };
+    auto b = [&](int c, double sc = 1.0) { return Col{B, bnc, c, sc}; };     // B == nullptr: zero
     using namespace qzb;
-    comps.push_back({"psi", d(D_PSI0)});
-    comps.push_back({"ez", f(F_EZ0)});
-    comps.push_back({"er", f(F_EP1R)});
-    comps.push_back({"eth", f(F_EP1I)});
-    comps.push_back({"br", f(F_BP1R)});
-    comps.push_back({"bth", f(F_BP1I)});
-    comps.push_back({"bz", f(F_BZ0)});
-    comps.push_back({"ne", d(D_NE0)});
-    comps.push_back({"ni", d(D_NI0)});
-    comps.push_back({"rhob", b(B_RHO0)});
+    comps.push_back({"psi", d(D_PSI0), none});
+    comps.push_back({"ez", f(F_EZ0), none});
+    comps.push_back({"er", f(F_EP1R), none});
+    comps.push_back({"eth", f(F_EP1I), none});
+    comps.push_back({"br", f(F_BP1R), none});
+    comps.push_back({"bth", f(F_BP1I), none});
+    comps.push_back({"bz", f(F_BZ0), none});
+    comps.push_back({"ne", d(D_NE0), none});
+    comps.push_back({"ni", d(D_NI0), none});
+    comps.push_back({"rhob", b(B_RHO0), none});
     if (m1) {   // f = f0 + 2 Re[f1 e^{i th}]: f_c = 2 Re f1, f_s = -2 Im f1; vectors from the V+ modes 0 and 2
-        const std::pair<const char*, std::pair<Fn, Fn>> sc[] = {
+        const std::pair<const char*, std::pair<Col, Col>> sc[] = {
             {"psi", {d(D_PSI1R), d(D_PSI1I)}}, {"ez", {f(F_EZ1R), f(F_EZ1I)}}, {"bz", {f(F_BZ1R), f(F_BZ1I)}},
             {"ne", {d(D_NE1R), d(D_NE1I)}}, {"ni", {d(D_NI1R), d(D_NI1I)}}, {"rhob", {b(B_RHO1R), b(B_RHO1I)}}};
         for (const auto& e : sc) {
-            comps.push_back({std::string(e.first) + "_c", scaled(e.second.first, 2.0)});
-            comps.push_back({std::string(e.first) + "_s", scaled(e.second.second, -2.0)});
+            Col re = e.second.first, im = e.second.second;
+            re.s = 2.0;
+            im.s = -2.0;
+            comps.push_back({std::string(e.first) + "_c", re, none});
+            comps.push_back({std::string(e.first) + "_s", im, none});
         }
         const int vr[2][4] = {{F_EP0R, F_EP0I, F_EP2R, F_EP2I}, {F_BP0R, F_BP0I, F_BP2R, F_BP2I}};
         const char* nm[2][2] = {{"er", "eth"}, {"br", "bth"}};
         for (int v = 0; v < 2; ++v) {
-            const Fn r0 = f(vr[v][0]), i0 = f(vr[v][1]), r2 = f(vr[v][2]), i2 = f(vr[v][3]);
-            comps.push_back({std::string(nm[v][0]) + "_c", sum(r0, r2, 1.0)});
-            comps.push_back({std::string(nm[v][0]) + "_s", sum(i0, i2, -1.0)});
-            comps.push_back({std::string(nm[v][1]) + "_c", sum(i0, i2, 1.0)});
-            comps.push_back({std::string(nm[v][1]) + "_s", sum(r2, r0, -1.0)});
+            comps.push_back({std::string(nm[v][0]) + "_c", f(vr[v][0]), f(vr[v][2])});
+            comps.push_back({std::string(nm[v][0]) + "_s", f(vr[v][1]), f(vr[v][3], -1.0)});
+            comps.push_back({std::string(nm[v][1]) + "_c", f(vr[v][1]), f(vr[v][3])});
+            comps.push_back({std::string(nm[v][1]) + "_s", f(vr[v][2]), f(vr[v][0], -1.0)});
         }
     }
     FILE* fp = std::fopen(path, "wb");
@@ -1765,9 +1788,19 @@ qz_status write_fields_host(const char* path, const double* nodes, int M, const 
     std::vector<double> v((size_t)K * M);
     for (const auto& c : comps) {
         char name[16] = {0};
-        std::strncpy(name, c.first.c_str(), 15);
-        for (int k = 0; k < K; ++k)
-            for (int j = 0; j < M; ++j) v[(size_t)(K - 1 - k) * M + j] = c.second((size_t)k * M + j);
+        std::strncpy(name, c.name.c_str(), 15);
+        for (int k = 0; k < K; ++k) {
+            double* row = v.data() + (size_t)(K - 1 - k) * M;             // file rows: the box head last
+            const size_t kj0 = (size_t)k * M;
+            if (!c.a.p) {
+                std::fill(row, row + M, 0.0);
+            } else if (!c.b.p) {
+                for (int j = 0; j < M; ++j) row[j] = c.a.s * c.a.p[(kj0 + j) * c.a.n + c.a.c];
+            } else {
+                for (int j = 0; j < M; ++j)
+                    row[j] = c.a.s * c.a.p[(kj0 + j) * c.a.n + c.a.c] + c.b.s * c.b.p[(kj0 + j) * c.b.n + c.b.c];
+            }
+        }
         ok = ok && std::fwrite(name, 16, 1, fp) == 1 && std::fwrite(v.data(), 8, v.size(), fp) == v.size();
     }
     ok = (std::fclose(fp) == 0) && ok;

@@ -660,7 +660,7 @@ __device__ void deposit_back(const AdjSm& S, const SweepArgs& A, const PState<OR
     L[0] += lx; L[1] += ly; L[2] += l_PX; L[3] += l_PY; L[4] += l_D;
 }
 
-// lam_f[j] of f -> grad f (src/FieldSolver.cpp:263-281) transposed, gathered at node j from l (shared)
+// lam_f[j] of f -> grad f (src/FieldSolver.cpp:193-211) transposed, gathered at node j from l (shared)
 __device__ __forceinline__ double grad_T_at(const SweepArgs& A, const double* gm, const double* g0, const double* gp,
                                             const double* l, int j) {
     const int N = A.N;

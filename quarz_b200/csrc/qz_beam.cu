@@ -1,14 +1,17 @@
 // qz_beam.cu -- beam deposit, field gather + Vay push, and moment sums (sm_100a, FP64).
 //
 // Beam::deposit (src/Beam.cpp:725-785), Beam::advance with the Vay pusher (src/Beam.cpp:948-1131,
-// src/Pushers.hpp:171-176) and Beam::sums (src/Beam.cpp:1133-1155). The particle arrays are SoA in
+// src/Pushers.hpp:63-68) and Beam::sums (src/Beam.cpp:1133-1155). The particle arrays are SoA in
 // HBM; one thread owns one particle per grid-stride step, so every load and store of the 7
 // particle columns is coalesced. The field store is read through L2 (a bilinear gather of the
 // (xi, r) cell, 4 x 6 doubles for m = 0); deposits are FP64 reductions into L2. The push can be
 // fused with the deposit of the next time step (the particle is deposited right after it moved).
 #include "qz_beam_body.cuh"
 
+#include <atomic>
 #include <mutex>
+
+#include <cuda.h>
 
 namespace qzb {
 
@@ -271,6 +274,37 @@ cudaError_t launch_beam_sums(const BeamArgs& B, double gref, double xiref, doubl
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------- context identity
+// The unique id of the CUDA context current on this thread (cuCtxGetId), or 0 when there is none
+// or the driver cannot tell. Device memory and the addresses of a module's static arrays belong to
+// one context: a cudaDeviceReset ends it, and the next runtime call creates a new one with a new
+// id. Addresses cached per device are therefore cached together with this id. The driver entry
+// points are fetched through the runtime, so the library does not link libcuda.
+unsigned long long current_context_id() {
+    using GetCurrent = CUresult (*)(CUcontext*);
+    using GetId = CUresult (*)(CUcontext, unsigned long long*);
+    static GetCurrent get_current = nullptr;
+    static GetId get_id = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_current = reinterpret_cast<GetCurrent>(f);
+        f = nullptr;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetId", &f, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            get_id = reinterpret_cast<GetId>(f);
+    });
+    if (!get_current || !get_id) return 0;
+    CUcontext c = nullptr;
+    if (get_current(&c) != CUDA_SUCCESS || c == nullptr) return 0;
+    unsigned long long id = 0;
+    if (get_id(c, &id) != CUDA_SUCCESS) return 0;
+    return id;
+}
+
 // ---------------------------------------------------------------- moment sums without allocation
 // Partial-sum scratch of beam_sums_static in static device memory: one 17-double row per block of
 // beam_sums_partial, sized for the block cap of beam_sums_blocks (148 x 4 blocks, 80,512 bytes per
@@ -279,33 +313,49 @@ cudaError_t launch_beam_sums(const BeamArgs& B, double gref, double xiref, doubl
 // threads) share it and race.
 static __device__ __align__(256) double g_sums_static[17 * kSumsStaticBlocks];
 
-namespace {
 constexpr int kMaxDevices = 64;
+
+namespace {
+struct StaticAddr {
+    std::atomic<unsigned long long> ctx{0};     // context the address was looked up in
+    std::atomic<double*> ptr{nullptr};
+};
+StaticAddr g_static[kMaxDevices];
 std::mutex g_static_mu;
-double* g_static_ptr[kMaxDevices] = {};
 }  // namespace
 
 cudaError_t beam_sums_static(const BeamArgs& B, double gref, double xiref, double* out17, cudaStream_t s,
                              int* nblocks_needed) {
     const int nb = beam_sums_blocks(B.n);
     *nblocks_needed = nb;
+    // beam_sums_blocks caps the grid at the array's row count and the partial kernel strides over
+    // the particles, so this holds for every n; it guards that invariant
     if (nb > kSumsStaticBlocks) return cudaErrorInvalidValue;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    StaticAddr& a = g_static[dev];
+    // fast path: the address was looked up in the context that is current now
+    unsigned long long ctx = current_context_id();
     double* partial = nullptr;
-    {
-        // set-up, once per device, with that device current: the address of this device's copy
-        // of the static scratch (no allocation; the module's static memory already exists)
+    if (ctx != 0 && a.ctx.load(std::memory_order_acquire) == ctx) {
+        partial = a.ptr.load(std::memory_order_relaxed);
+    } else {
+        // set-up, once per device and context, with that device current: the address of this
+        // device's copy of the static scratch (no allocation; the module's static memory exists
+        // once the module is loaded). A cudaDeviceReset ends the context, and with it the
+        // address; the next call looks it up again in the new context.
         std::lock_guard<std::mutex> lock(g_static_mu);
-        if (!g_static_ptr[dev]) {
-            void* ptr = nullptr;
-            e = cudaGetSymbolAddress(&ptr, g_sums_static);
-            if (e != cudaSuccess) return e;
-            g_static_ptr[dev] = static_cast<double*>(ptr);
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_sums_static);
+        if (e != cudaSuccess) return e;
+        partial = static_cast<double*>(p);
+        ctx = current_context_id();           // the lookup made the device's primary context current
+        if (ctx != 0) {
+            a.ptr.store(partial, std::memory_order_relaxed);
+            a.ctx.store(ctx, std::memory_order_release);
         }
-        partial = g_static_ptr[dev];
     }
     return launch_beam_sums(B, gref, xiref, partial, nb, out17, s);
 }

@@ -2,7 +2,7 @@
 // shared by the stand-alone beam kernels (qz_beam.cu) and the time-step pipeline (qz_pipeline.cu).
 //
 // Beam::deposit (src/Beam.cpp:725-785), Beam::advance with the Vay pusher (src/Beam.cpp:948-1131,
-// src/Pushers.hpp:171-176), Beam::sums (src/Beam.cpp:1133-1155).
+// src/Pushers.hpp:63-68), Beam::sums (src/Beam.cpp:1133-1155).
 #pragma once
 #include "qz_device.cuh"
 #include "qz_internal.h"
@@ -88,7 +88,7 @@ __device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, doubl
     const double omvz = (1.0 + p2) / (gam * (gam + PZ));
     const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
     const double vr = c * vx + s * vy, vt = c * vy - s * vx;
-    // the cell of r (src/RadialGrid.hpp:84-88): a short walk from the guess, the search otherwise
+    // the cell of r (src/RadialGrid.hpp:35-50): a short walk from the guess, the search otherwise
     j = locate_near(B.r, B.N, R, r, jguess);
     double t = (r - B.r[j]) * B.inv_h[j];
     t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);

@@ -29,7 +29,7 @@ enum BeamComp : int {
 enum DiagComp : int { D_PSI0 = 0, D_NE0, D_NI0, D_PSI1R, D_PSI1I, D_NE1R, D_NE1I, D_NI1R, D_NI1I, D_NC0 = 3, D_NC1 = 9 };
 
 // Cell of x on the node array r[0..N] (r_j <= x < r_{j+1}), x clamped to [0, R];
-// src/RadialGrid.hpp:73-82 (binary search, same result for every x).
+// src/RadialGrid.hpp:35-44 (binary search, same result for every x).
 __device__ __forceinline__ int locate(const double* __restrict__ r, int N, double R, double x) {
     if (x <= 0.0) return 0;
     if (x >= R) return N - 1;
@@ -55,7 +55,7 @@ __device__ __forceinline__ int locate_near(const double* __restrict__ r, int N, 
     return locate(r, N, R, x);
 }
 
-// cell and clamped fractional position (src/RadialGrid.hpp:84-88)
+// cell and clamped fractional position (src/RadialGrid.hpp:35-50)
 __device__ __forceinline__ void weights(const double* __restrict__ r, const double* __restrict__ inv_h, int N,
                                         double R, double x, int& j, double& t) {
     j = locate(r, N, R, x);
@@ -108,7 +108,7 @@ __device__ __forceinline__ double lin(const double* __restrict__ f, const PGeo& 
     return p.W0 * f[p.j] + p.W1 * f[p.j + 1];
 }
 
-// ---------------------------------------------------------------- Vay pusher (src/Pushers.hpp:144-176)
+// ---------------------------------------------------------------- Vay pusher (src/Pushers.hpp:36-68)
 struct V3 { double x, y, z; };
 __device__ __forceinline__ double dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ V3 cross3(V3 a, V3 b) {

@@ -116,6 +116,9 @@ constexpr int kSumsStaticBlocks = 148 * 4;
 // *nblocks_needed: the rows the call needs (cudaErrorInvalidValue when above kSumsStaticBlocks).
 cudaError_t beam_sums_static(const BeamArgs& B, double gref, double xiref, double* out17, cudaStream_t s,
                              int* nblocks_needed);
+// Unique id of the CUDA context current on this thread (0 when none or unknown): device addresses
+// cached per device are valid only while the context they were taken in lives.
+unsigned long long current_context_id();
 
 // ---------------------------------------------------------------- time-step pipeline
 // Consecutive time steps of Simulation::run in one cooperative launch: CTAs [0, nsweep) each run whole

@@ -574,7 +574,7 @@ __device__ __forceinline__ void filter_sources(const Src& s, const Smem& S, cons
     __syncthreads();
 }
 
-// 3-point non-uniform gradient at node i (src/FieldSolver.cpp:263-281); odd: axis value f1/r1
+// 3-point non-uniform gradient at node i (src/FieldSolver.cpp:193-211); odd: axis value f1/r1
 __device__ __forceinline__ double grad_at(const Smem& S, int N, const double* f, int i, bool odd) {
     if (i == 0) return odd ? f[1] * S.ir[0] : 0.0;
     if (i == N) return S.g0[N] * f[N] + S.gm[N] * f[N - 1] + S.gp[N] * f[N - 2];
@@ -582,7 +582,7 @@ __device__ __forceinline__ double grad_at(const Smem& S, int N, const double* f,
 }
 
 // cell of x starting from a guess (the previous cell): walks for small moves, bisects otherwise;
-// the same cell as locate() (src/RadialGrid.hpp:73-82) for every x
+// the same cell as locate() (src/RadialGrid.hpp:35-44) for every x
 __device__ __forceinline__ int locate_from(const double* __restrict__ r, int N, double R, double x, int j) {
     if (x <= 0.0) return 0;
     if (x >= R) return N - 1;
@@ -822,7 +822,7 @@ __device__ __forceinline__ void rhs_l0(const Smem& S, const Src& s, int N, int i
 }
 
 // row i of (L1D - chi) (sys 0) and (L1F - chi) (sys 1) with its right-hand side
-// (src/FieldSolver.cpp:242-261, src/Simulation.cpp:535-591)
+// (src/FieldSolver.cpp:172-191, src/Simulation.cpp:535-591)
 __device__ __forceinline__ void row_b(const Smem& S, const Src& s, int N, double fc, int sys, int i, double& a,
                                       double& b, double& cm, double& d) {
     if (sys == 0) {

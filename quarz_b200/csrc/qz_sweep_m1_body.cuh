@@ -111,7 +111,7 @@ __device__ __forceinline__ Consts1 consts1(const SweepArgs& A) {
 
 __device__ __forceinline__ double ldc(const double* p) { return __ldg(p); }
 
-// 3-point non-uniform gradients (src/FieldSolver.cpp:263-289)
+// 3-point non-uniform gradients (src/FieldSolver.cpp:193-219)
 __device__ __forceinline__ double grad1(const Consts1& C, int N, const double* f, int i, bool odd) {
     if (i == 0) return odd ? f[1] * ldc(C.ir) : 0.0;
     if (i == N) return ldc(C.g0 + N) * f[N] + ldc(C.gm + N) * f[N - 1] + ldc(C.gp + N) * f[N - 2];
@@ -688,7 +688,7 @@ __device__ __forceinline__ void deposit_all1(const SweepArgs& A, const Smem1& S,
     }
 }
 
-// row i of the B+ systems (src/FieldSolver.cpp:242-261 with chi = chi_0):
+// row i of the B+ systems (src/FieldSolver.cpp:172-191 with chi = chi_0):
 //   sys 0: L1D - chi (Dirichlet 0, N)   sys 1: L1F - chi (Dirichlet 0, flux row N)
 //   sys 2: L0 - chi (regular axis, Dirichlet N)   sys 3: L2D - chi (Dirichlet 0, N)
 // a, b, c of the row and c_{i-1}; dir = the row is a Dirichlet row (its right-hand side is 0)

@@ -4,7 +4,7 @@ Only the keys that reach the hot path are interpreted (grid, box, plasma species
 beams, pusher / solver options, time stepping). Semantics follow the reference:
 
   * deck syntax and command-line overrides        src/Config.cpp, src/main.cpp:82-93
-  * grid generators (uniform / regions / file)    src/RadialGrid.cpp:139-227
+  * grid generators (uniform / regions / file)    src/RadialGrid.cpp:14-86
   * box: internal xi = -xi_user, K = lround(L/dxi)+1   src/Simulation.cpp:69-77, src/Types.hpp:30-31
   * species defaults (ppc 4, ntheta 8 with m = 1)  src/PlasmaSpecies.cpp:92-150
   * beam keys of the gaussian generator           src/Beam.cpp:483-570
@@ -80,7 +80,7 @@ def _lround(x: float) -> int:
 
 
 def make_regions(R: float, regions: Sequence[Tuple[float, float]], max_ratio: float) -> np.ndarray:
-    """src/RadialGrid.cpp:152-196"""
+    """src/RadialGrid.cpp:27-71"""
     if not regions:
         raise ValueError("grid: grid.regions is empty")
     if max_ratio < 1.0:

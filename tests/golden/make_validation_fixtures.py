@@ -1,5 +1,5 @@
-"""Generates the validation fixtures of tests/golden from the reference checkout (run once, in the
-container that has it):  python tests/golden/make_validation_fixtures.py /root/reference
+"""Generates the validation fixtures of tests/golden from the reference checkout (run once, where a
+checkout exists):  python tests/golden/make_validation_fixtures.py <path of the reference checkout>
 
   validation_numbers.json  printed results of validation/reference_full.txt and reference_quick.txt
                            for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain,
@@ -13,7 +13,9 @@ import re
 import shutil
 import sys
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit("usage: make_validation_fixtures.py <path of the reference checkout>")
+ref = sys.argv[1]
 here = os.path.dirname(os.path.abspath(__file__))
 out = {}
 for tag, fn in (("full", "reference_full.txt"), ("quick", "reference_quick.txt")):

@@ -91,5 +91,8 @@ def test_batch_with_smoothing():
         sim = Q.Simulation(s, beams=bm)
         sim.set_schedule(False)
         _close(s, mom, sim.run(2, s.dt), bm, 1e-10)
-    s, bm, mom = specs[0], beams[0], moms[0]
-    _close(s, mom, O.OracleSim(s, beams=bm).run(2, s.dt), bm, 1e-8)
+    # the filtered m = 0 instance and the filtered m = 1 instance (the batch's m = 1 filter path, which
+    # smooths the mode parts in place in the instance's scratch) against the independent oracle
+    for i in (0, 3):
+        s, bm, mom = specs[i], beams[i], moms[i]
+        _close(s, mom, O.OracleSim(s, beams=bm).run(2, s.dt), bm, 1e-8)
