@@ -459,14 +459,17 @@ extern "C" qz_status qz_sweep_destroy(qz_sweep* s) {
     return QZ_OK;
 }
 
-extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
-                                  void* stream) {
-    if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run: null pointer");
-    cudaStream_t st = (cudaStream_t)stream;
+namespace {
+// one sweep of s over bsrc; bqe set: bsrc in the exact two-limb format (qz_sim's m = 0 runs)
+qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
+                       cudaStream_t st, const int* bqe, int bfx_s, long bfx_lo) {
     qzb::SweepArgs A = s->base;
     A.bsrc = bsrc;
     A.fld = fld;
     A.diag = diag;
+    A.bqe = bqe;
+    A.bfx_s = bfx_s;
+    A.bfx_lo = bfx_lo;
     QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
     if (s->timing) {
         QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 16, st));
@@ -480,6 +483,13 @@ extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, 
         cnt->lost += h[0];
     }
     return QZ_OK;
+}
+}  // namespace
+
+extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
+                                  void* stream) {
+    if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run: null pointer");
+    return sweep_launch(s, bsrc, fld, diag, cnt, (cudaStream_t)stream, nullptr, 0, 0);
 }
 
 extern "C" qz_status qz_sweep_plasma(qz_sweep* s, double* out, int cap, int* n) {
@@ -773,6 +783,16 @@ struct qz_sim {
     int nanalytic = 0;
     int cur = 0;
     bool bsrc_valid = false;
+    // exact beam deposits of m = 0 runs (BeamArgs::fx_qe): per-node quantum exponents, the limb split,
+    // and the offset of the low limbs behind a (K, M, 5) block of high limbs
+    struct Fx {
+        int* d_qe = nullptr;
+        std::vector<int> qe;
+        double* d_wmax = nullptr;
+        int S = 0;
+        long lo = 0;
+        bool on = false;
+    } fx;
     struct Beam {
         double* d = nullptr;     // 7 columns of n (the library's order: sorted by xi cell after a pipelined run)
         double* d2 = nullptr;    // second copy for reordering
@@ -821,6 +841,8 @@ struct qz_sim {
         size_t cm_n = 0;
     } pipe;
     ~qz_sim() {
+        if (fx.d_qe) cudaFree(fx.d_qe);
+        if (fx.d_wmax) cudaFree(fx.d_wmax);
         for (auto& b : beams)
             for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
                 if (q) cudaFree(q);
@@ -851,8 +873,8 @@ extern "C" qz_status qz_sim_create(const qz_grid* g, const qz_sweep_params* p, q
     const size_t KM = (size_t)p->K * g->M;
     if (cudaMalloc((void**)&s->d_fld, sizeof(double) * KM * s->fnc) != cudaSuccess ||
         cudaMalloc((void**)&s->d_diag, sizeof(double) * KM * s->dnc) != cudaSuccess ||
-        cudaMalloc((void**)&s->d_bsrc[0], sizeof(double) * KM * s->bnc) != cudaSuccess ||
-        cudaMalloc((void**)&s->d_bsrc[1], sizeof(double) * KM * s->bnc) != cudaSuccess) {
+        cudaMalloc((void**)&s->d_bsrc[0], sizeof(double) * KM * s->bnc * (p->modes ? 1 : 2)) != cudaSuccess ||
+        cudaMalloc((void**)&s->d_bsrc[1], sizeof(double) * KM * s->bnc * (p->modes ? 1 : 2)) != cudaSuccess) {
         delete s;
         return fail(QZ_ERR_NOMEM, "qz_sim_create: device allocation failed");
     }
@@ -949,6 +971,117 @@ qz_box sim_box(const qz_sim* s) {
 
 namespace {
 
+// The exact beam deposits of an m = 0 run: every contribution to node j is bounded by
+// 2 (sum over beams of max |w q|) / V_j / dxi (the weights of the particles do not change during a run;
+// |1 - v_z| <= 2 and every other factor is at most 1), so the quantum of node j is that bound / 2^B.
+// With at most n contributions per value (n = all beam particles, 2^nbits > n) the limbs split at
+// S = 63 - nbits and B = 126 - 2 nbits keep both integer sums below 2^63. Returns whether the run
+// deposits exactly; it does for m = 0, while m = 1 runs keep FP64 reductions.
+qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
+    auto& F = s->fx;
+    F.on = false;
+    if (s->p.modes != 0 || s->beams.empty()) return QZ_OK;
+    const int M = s->g->M;
+    long ntot = 0;
+    for (const auto& b : s->beams) ntot += (long)b.n;
+    int nbits = 1;
+    while (nbits < 62 && (1L << nbits) <= ntot) ++nbits;
+    if (nbits > 30) return QZ_OK;                   // beyond 2^30 particles: FP64 reductions
+    const int S = 63 - nbits, B = 126 - 2 * nbits;
+    if (!F.d_wmax && cudaMalloc((void**)&F.d_wmax, sizeof(double) * qzb::kMaxBeams * 2) != cudaSuccess) {
+        F.d_wmax = nullptr;
+        return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");
+    }
+    const qz_box box = sim_box(s);
+    const int nb = std::min((int)s->beams.size(), 2 * qzb::kMaxBeams);
+    QZ_CUDA(cudaMemsetAsync(F.d_wmax, 0, sizeof(double) * nb, st));
+    double wq = 0.0;
+    std::vector<double> wm(nb, 0.0);
+    for (int b = 0; b < nb; ++b) {
+        const qz_beam_view v = s->beams[b].view();
+        QZ_CUDA(qzb::launch_beam_wmax(beam_args(s->g, &v, &box), F.d_wmax + b, st));
+    }
+    QZ_CUDA(cudaMemcpyAsync(wm.data(), F.d_wmax, sizeof(double) * nb, cudaMemcpyDeviceToHost, st));
+    QZ_CUDA(cudaStreamSynchronize(st));
+    if ((int)s->beams.size() > nb) return QZ_OK;    // more beams than bounds: FP64 reductions
+    for (int b = 0; b < nb; ++b) wq += wm[b] * std::fabs(s->beams[b].q);
+    std::vector<int> qe(M, 0);
+    for (int j = 0; j < M; ++j) {
+        const double bound = 2.0 * wq * s->g->inv_V[j] / s->p.dxi;
+        int e = 0;
+        if (bound > 0.0 && std::isfinite(bound)) std::frexp(bound, &e);    // bound < 2^e
+        qe[j] = e - B;
+    }
+    if (!F.d_qe && cudaMalloc((void**)&F.d_qe, sizeof(int) * M) != cudaSuccess) {
+        F.d_qe = nullptr;
+        return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");
+    }
+    if (qe != F.qe || F.S != S) {
+        QZ_CUDA(cudaMemcpyAsync(F.d_qe, qe.data(), sizeof(int) * M, cudaMemcpyHostToDevice, st));
+        F.qe = qe;
+        s->bsrc_valid = false;                      // sources kept from the last run used other quanta
+    }
+    F.S = S;
+    F.lo = (long)s->p.K * M * s->bnc;
+    F.on = true;
+    return QZ_OK;
+}
+
+// BeamArgs of beam b with the exact deposits of the run when they are on
+qzb::BeamArgs sim_beam_args(const qz_sim* s, const qz_beam_view* v, const qz_box* box) {
+    qzb::BeamArgs B = beam_args(s->g, v, box);
+    if (s->fx.on) {
+        B.fx_qe = s->fx.d_qe;
+        B.fx_s = s->fx.S;
+        B.fx_lo = s->fx.lo;
+    }
+    return B;
+}
+
+void sim_sweep_fx(const qz_sim* s, qzb::SweepArgs& A) {
+    A.bqe = s->fx.on ? s->fx.d_qe : nullptr;
+    A.bfx_s = s->fx.S;
+    A.bfx_lo = s->fx.lo;
+}
+
+// the sim's beam-source buffers: doubles for modes = 1, two limbs per value for m = 0
+size_t sim_bsrc_doubles(const qz_sim* s) { return (size_t)s->p.K * s->g->M * s->bnc * (s->p.modes ? 1 : 2); }
+
+// the deposit of every beam into bsrc (cleared first), exact when the run's quanta are set
+qz_status sim_deposit_all(qz_sim* s, double* bsrc, cudaStream_t st) {
+    const qz_box box = sim_box(s);
+    QZ_CUDA(cudaMemsetAsync(bsrc, 0, sizeof(double) * sim_bsrc_doubles(s), st));
+    for (auto& b : s->beams) {
+        const qz_beam_view v = b.view();
+        QZ_CUDA(qzb::launch_beam_deposit(sim_beam_args(s, &v, &box), bsrc, st));
+    }
+    return QZ_OK;
+}
+
+qz_status sim_sweep(qz_sim* s, const double* bsrc, cudaStream_t st) {
+    return sweep_launch(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, st, s->fx.on ? s->fx.d_qe : nullptr, s->fx.S,
+                        s->fx.lo);
+}
+
+// one time step's push of beam b with the deposit into bsrc_next (leapfrog start-up first); rigid
+// beams only deposit
+qz_status sim_push_deposit(qz_sim* s, qz_sim::Beam& b, double dt_kick, double dt_drift, double* bsrc_next,
+                           cudaStream_t st) {
+    const qz_box box = sim_box(s);
+    const qz_beam_view v = b.view();
+    const qzb::BeamArgs B = sim_beam_args(s, &v, &box);
+    if (b.rigid) {
+        QZ_CUDA(qzb::launch_beam_deposit(B, bsrc_next, st));
+        return QZ_OK;
+    }
+    if (!b.started) {
+        QZ_CUDA(qzb::launch_beam_push(B, s->d_fld, -0.5 * dt_kick, -0.5 * dt_kick, 0, st));
+        b.started = 1;
+    }
+    QZ_CUDA(qzb::launch_beam_push_deposit(B, s->d_fld, dt_kick, dt_drift, bsrc_next, st));
+    return QZ_OK;
+}
+
 template <class T>
 qz_status grow(T** p, size_t* have, size_t need, const char* what) {
     if (*have >= need && *p) return QZ_OK;
@@ -984,6 +1117,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     if (!P_.ev[0])
         for (auto& e : P_.ev) QZ_CUDA(cudaEventCreate(&e));
     QZ_CUDA(cudaEventRecord(P_.ev[0], st));
+    if (qz_status e = fx_prepare(s, st)) return e;
     // 1. order each beam by (xi cell, radial cell); buckets of at most P_.bucket live particles
     if ((unsigned long long)(K + 2) * (unsigned long long)M >= (1ull << 31))
         return fail(QZ_ERR_SIZE, "qz_sim_run: K * M too large for the pipelined run's sort keys");
@@ -1080,6 +1214,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     const int ring = rec ? std::max(2, nsteps + 1) : std::max(2, std::min(nsteps + 1, nsweep + 2));
     // 3. buffers
     const size_t KM = (size_t)K * M;
+    const size_t bslot = sim_bsrc_doubles(s);           // a beam-source slot: two limbs per value for m = 0
     if (P_.ring < ring) {
         for (double* q : {P_.fld, P_.diag, P_.bsrc})
             if (q) cudaFree(q);
@@ -1087,14 +1222,14 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
         P_.ring = 0;
         if (cudaMalloc((void**)&P_.fld, sizeof(double) * KM * s->fnc * ring) != cudaSuccess ||
             cudaMalloc((void**)&P_.diag, sizeof(double) * KM * s->dnc * ring) != cudaSuccess ||
-            cudaMalloc((void**)&P_.bsrc, sizeof(double) * KM * s->bnc * ring) != cudaSuccess) {
+            cudaMalloc((void**)&P_.bsrc, sizeof(double) * bslot * ring) != cudaSuccess) {
             cudaGetLastError();
             return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (field rings)");
         }
         P_.ring = ring;
         P_.clean = false;
     }
-    if (!P_.clean) QZ_CUDA(cudaMemsetAsync(P_.bsrc, 0, sizeof(double) * KM * s->bnc * P_.ring, st));
+    if (!P_.clean) QZ_CUDA(cudaMemsetAsync(P_.bsrc, 0, sizeof(double) * bslot * P_.ring, st));
     P_.clean = false;
     const size_t ps_slot = (size_t)(6 + 5 * s->p.ab_order) * std::max(1, s->sw->npad);
     if (qz_status e = grow(&P_.ps, &P_.ps_n, ps_slot * nsweep, "plasma scratch")) return e;
@@ -1117,15 +1252,16 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     // 4. beam sources of step 0 into slot 0
     for (auto& b : s->beams) {
         const qz_beam_view v = b.view();
-        if (qz_status e = qz_beam_deposit(s->g, &v, &box, P_.bsrc, st)) return e;
+        QZ_CUDA(qzb::launch_beam_deposit(sim_beam_args(s, &v, &box), P_.bsrc, st));
     }
+    sim_sweep_fx(s, A.sw);
     // 5. launch
     A.nsteps = nsteps;
     A.nsweep = nsweep;
     A.ring = ring;
     A.fld_slot = KM * s->fnc;
     A.diag_slot = KM * s->dnc;
-    A.bsrc_slot = KM * s->bnc;
+    A.bsrc_slot = bslot;
     A.ps_slot = ps_slot;
     A.fld = P_.fld;
     A.diag = P_.diag;
@@ -1137,7 +1273,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     for (int q = 0; q < nb; ++q) {
         const auto& b = s->beams[q];
         const qz_beam_view v = b.view();
-        A.beam[q] = beam_args(s->g, &v, &box);
+        A.beam[q] = sim_beam_args(s, &v, &box);
         A.rigid[q] = b.rigid;
         A.startup[q] = b.started ? 0 : 1;
         A.gref[q] = b.gref;
@@ -1218,20 +1354,15 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
 
 qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cudaStream_t st) {
     void* stream = (void*)st;
-    const size_t KMb = (size_t)s->p.K * s->g->M * s->bnc;
-    const qz_box box = sim_box(s);
     const int nb = (int)s->beams.size();
+    if (qz_status e = fx_prepare(s, st)) return e;
     if (!s->bsrc_valid) {
-        QZ_CUDA(cudaMemsetAsync(s->d_bsrc[s->cur], 0, sizeof(double) * KMb, st));
-        for (auto& b : s->beams) {
-            const qz_beam_view v = b.view();
-            if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[s->cur], stream)) return e;
-        }
+        if (qz_status e = sim_deposit_all(s, s->d_bsrc[s->cur], st)) return e;
         s->bsrc_valid = true;
     }
     double dt_prev = dt;
     for (int n = 0; n <= nsteps; ++n) {
-        if (qz_status e = qz_sweep_run(s->sw, s->d_bsrc[s->cur], s->d_fld, s->d_diag, nullptr, stream)) return e;
+        if (qz_status e = sim_sweep(s, s->d_bsrc[s->cur], st)) return e;
         if (mom_host) {
             for (int b = 0; b < nb; ++b) {
                 const qz_beam_view v = s->beams[b].view();
@@ -1244,17 +1375,9 @@ qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cud
         if (n < nsteps) {
             const double dkick = 0.5 * (dt_prev + dt), ddrift = dt;
             const int nxt = 1 - s->cur;
-            QZ_CUDA(cudaMemsetAsync(s->d_bsrc[nxt], 0, sizeof(double) * KMb, st));
-            for (auto& b : s->beams) {
-                qz_beam_view v = b.view();
-                if (b.rigid) {
-                    if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[nxt], stream)) return e;
-                } else {
-                    if (qz_status e = qz_beam_push_deposit(s->g, &v, &box, s->d_fld, dkick, ddrift, &b.started,
-                                                           s->d_bsrc[nxt], stream))
-                        return e;
-                }
-            }
+            QZ_CUDA(cudaMemsetAsync(s->d_bsrc[nxt], 0, sizeof(double) * sim_bsrc_doubles(s), st));
+            for (auto& b : s->beams)
+                if (qz_status e = sim_push_deposit(s, b, dkick, ddrift, s->d_bsrc[nxt], st)) return e;
             s->cur = nxt;
             dt_prev = dt;
         }
@@ -1871,7 +1994,6 @@ extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_
                                       double* mom_host, void* stream) {
     if (!s || (!s->beams.empty() && !cols)) return fail(QZ_ERR_ARG, "qz_sim_step_host: null pointer");
     cudaStream_t st = (cudaStream_t)stream;
-    const size_t KMb = (size_t)s->p.K * s->g->M * s->bnc;
     const qz_box box = sim_box(s);
     const int nb = (int)s->beams.size();
     for (int b = 0; b < nb; ++b) {
@@ -1880,12 +2002,9 @@ extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_
                                 st));
         s->beams[b].orig_identity = true;
     }
-    QZ_CUDA(cudaMemsetAsync(s->d_bsrc[s->cur], 0, sizeof(double) * KMb, st));
-    for (auto& b : s->beams) {
-        const qz_beam_view v = b.view();
-        if (qz_status e = qz_beam_deposit(s->g, &v, &box, s->d_bsrc[s->cur], stream)) return e;
-    }
-    if (qz_status e = qz_sweep_run(s->sw, s->d_bsrc[s->cur], s->d_fld, s->d_diag, nullptr, stream)) return e;
+    if (qz_status e = fx_prepare(s, st)) return e;
+    if (qz_status e = sim_deposit_all(s, s->d_bsrc[s->cur], st)) return e;
+    if (qz_status e = sim_sweep(s, s->d_bsrc[s->cur], st)) return e;
     for (int b = 0; b < nb; ++b) {
         const qz_beam_view v = s->beams[b].view();
         if (qz_status e = qz_beam_sums(&v, s->beams[b].gref, s->beams[b].xiref, s->d_mom + 17 * b, stream)) return e;

@@ -8,188 +8,14 @@
 // shared memory, the field and beam-source buffers are the CTA's slot, and the beams are pushed by
 // the CTA itself with the grid arrays the sweep left in shared memory. Instances with modes = 1 run
 // the m = 1 sweep (qz_sweep_m1_body.cuh) with their own source scratch.
-#include "qz_beam_body.cuh"
-#include "qz_sweep_body.cuh"
-#include "qz_sweep_m1_body.cuh"
+#include "qz_batch_kernels.cuh"
 
 namespace qzb {
 
 namespace {
 
-using beam_detail::deposit_one;
-using beam_detail::PState7;
-using beam_detail::push_one;
-using beam_detail::sums_add;
-
-constexpr int kT = kSweepThreads;
-
-// beam work of one instance by the whole CTA: moments (step n) of every beam, then, when push,
-// the push with the fields of step n and the deposit into bsrc (zeroed first)
-__device__ void beam_phase(const BatchInst& I, const SweepArgs& A, const BatchArgs& B, int n, bool push, bool startup,
-                           double* red) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    if (push) {
-        const size_t nb = (size_t)A.K * A.M * (I.modes ? B_NC1 : B_NC0);
-        for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
-        __syncthreads();
-    }
-    // the sweep leaves the grid in shared memory (qz_sweep_body.cuh carve: r, 1/V, 1/h first)
-    extern __shared__ double smem_raw[];
-    const double* r = smem_raw;
-    const double* iV = smem_raw + A.M;
-    const double* ih = smem_raw + 2 * A.M;
-    for (int q = 0; q < I.nbeams; ++q) {
-        BeamArgs Bb = I.beam[q];
-        Bb.r = r;
-        Bb.inv_V = iV;
-        Bb.inv_h = ih;
-        const double qm = Bb.q / Bb.m;
-        const double h = 0.5 * qm * B.dt;
-        const double hs = startup ? 0.5 * qm * (-0.5 * B.dt) : 0.0;
-        double acc[17];
-#pragma unroll
-        for (int c = 0; c < 17; ++c) acc[c] = 0.0;
-        for (long i = tid; i < Bb.n; i += kT) {
-            PState7 p;
-            p.w = Bb.w[i];
-            if (p.w == 0.0) continue;
-            p.x = Bb.x[i]; p.y = Bb.y[i]; p.px = Bb.px[i]; p.py = Bb.py[i]; p.pz = Bb.pz[i]; p.xi = Bb.xi[i];
-            sums_add(acc, p, I.gref[q], I.xiref[q]);
-            if (!push) continue;
-            if (I.rigid[q]) {
-                deposit_one(Bb, const_cast<double*>(A.bsrc), p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
-                continue;
-            }
-            const bool alive = push_one<false>(Bb, A.fld, p, h, hs, B.dt);
-            Bb.x[i] = p.x; Bb.y[i] = p.y; Bb.px[i] = p.px; Bb.py[i] = p.py; Bb.pz[i] = p.pz; Bb.xi[i] = p.xi;
-            if (!alive) {
-                Bb.w[i] = 0.0;
-                continue;
-            }
-            deposit_one(Bb, const_cast<double*>(A.bsrc), p.x, p.y, p.px, p.py, p.pz, p.xi, p.w);
-        }
-        // deterministic block reduction of the 17 sums
-#pragma unroll
-        for (int c = 0; c < 17; ++c) {
-            double x = acc[c];
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-            if (lane == 0) red[c * (kT / 32) + warp] = x;
-        }
-        __syncthreads();
-        if (tid < 17) {
-            double v = 0.0;
-            for (int w = 0; w < kT / 32; ++w) v += red[tid * (kT / 32) + w];
-            I.mom[((size_t)n * I.nbeams + q) * 17 + tid] = v;
-        }
-        __syncthreads();
-    }
-}
-
-// the step-0 deposit of every beam into the (zeroed) slot
-__device__ void beam_deposit0(const BatchInst& I, const SweepArgs& A) {
-    const int tid = threadIdx.x;
-    const size_t nb = (size_t)A.K * A.M * (I.modes ? B_NC1 : B_NC0);
-    for (size_t t = tid; t < nb; t += kT) const_cast<double*>(A.bsrc)[t] = 0.0;
-    __syncthreads();
-    for (int q = 0; q < I.nbeams; ++q) {
-        const BeamArgs& Bb = I.beam[q];
-        for (long i = tid; i < Bb.n; i += kT) {
-            const double w = Bb.w[i];
-            if (w == 0.0) continue;
-            deposit_one(Bb, const_cast<double*>(A.bsrc), Bb.x[i], Bb.y[i], Bb.px[i], Bb.py[i], Bb.pz[i], Bb.xi[i], w);
-        }
-    }
-    __syncthreads();
-}
-
-// WITH_M1: the batch holds modes = 1 instances (the m = 0 only variant keeps the m = 1 body out of the
-// kernel and its register allocation)
-// EXT: the variant whose sweeps handle the smoothing filter (some instance has plasma.smooth_length)
-template <int ORD, bool WITH_M1, bool EXT>
-__global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_constant__ BatchArgs B) {
-    extern __shared__ double smem_raw[];
-    __shared__ BatchInst I;
-    __shared__ int s_inst;
-    __shared__ double red[17 * (kT / 32)];
-    const int tid = threadIdx.x;
-    for (;;) {
-        if (tid == 0) s_inst = atomicAdd(B.next, 1);
-        __syncthreads();
-        const int qi = s_inst;
-        if (qi >= B.ninst) break;
-        if (tid == 0) {
-            I = B.inst[B.order[qi]];
-            I.sw.bsrc = B.bsrc + blockIdx.x * B.bsrc_slot;
-            I.sw.fld = B.fld + blockIdx.x * B.fld_slot;
-            I.sw.diag = B.diag + blockIdx.x * B.diag_slot;
-            I.sw.timing = nullptr;
-        }
-        __syncthreads();
-        const SweepArgs& A = I.sw;
-        const bool reg = A.np <= kSweepThreads;
-        beam_deposit0(I, A);
-        for (int n = 0; n <= B.nsteps; ++n) {
-            NoGate g;
-            if (WITH_M1 && I.modes) {
-                if constexpr (WITH_M1) sweep_m1_body<ORD, NoGate, EXT>(A, smem_raw, g);
-            } else if (A.rows_per_thread == 1) {
-                if (reg) sweep_body<ORD, true, 1, NoGate, EXT>(A, smem_raw, g);
-                else sweep_body<ORD, false, 1, NoGate, EXT>(A, smem_raw, g);
-            } else {
-                sweep_body<ORD, false, 4, NoGate, EXT>(A, smem_raw, g);
-            }
-            __syncthreads();
-            beam_phase(I, A, B, n, n < B.nsteps, n == 0, red);
-        }
-        __syncthreads();
-    }
-}
-
-template <int ORD, bool WITH_M1, bool EXT>
-cudaError_t launch_t(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    cudaError_t e =
-        cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    batch_kernel<ORD, WITH_M1, EXT><<<grid, kSweepThreads, smem, s>>>(B);
-    return cudaGetLastError();
-}
-
-template <int ORD, bool WITH_M1, bool EXT>
-int occupancy_t(size_t smem) {
-    if (cudaFuncSetAttribute(batch_kernel<ORD, WITH_M1, EXT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-        return 0;
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batch_kernel<ORD, WITH_M1, EXT>, kSweepThreads, smem) !=
-        cudaSuccess)
-        return 0;
-    return nb;
-}
-
-template <bool WITH_M1, bool EXT>
-int occupancy_any(int ord, size_t smem) {
-    switch (ord) {
-        case 1: return occupancy_t<1, WITH_M1, EXT>(smem);
-        case 2: return occupancy_t<2, WITH_M1, EXT>(smem);
-        case 3: return occupancy_t<3, WITH_M1, EXT>(smem);
-        case 4: return occupancy_t<4, WITH_M1, EXT>(smem);
-        case 5: return occupancy_t<5, WITH_M1, EXT>(smem);
-        default: return 0;
-    }
-}
-
-template <bool WITH_M1, bool EXT>
-cudaError_t launch_any(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    switch (B.ord) {
-        case 1: return launch_t<1, WITH_M1, EXT>(B, grid, smem, s);
-        case 2: return launch_t<2, WITH_M1, EXT>(B, grid, smem, s);
-        case 3: return launch_t<3, WITH_M1, EXT>(B, grid, smem, s);
-        case 4: return launch_t<4, WITH_M1, EXT>(B, grid, smem, s);
-        case 5: return launch_t<5, WITH_M1, EXT>(B, grid, smem, s);
-        default: return cudaErrorInvalidValue;
-    }
-}
+template <int ORD>
+int occ(bool m1, bool ext, size_t smem) { return batch_occupancy_ord<ORD>(m1, ext, smem); }
 
 }  // namespace
 
@@ -198,14 +24,27 @@ int batch_max_grid(int ord, bool with_m1, bool with_ext, size_t smem, int* sms) 
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    const int per = with_m1 ? (with_ext ? occupancy_any<true, true>(ord, smem) : occupancy_any<true, false>(ord, smem))
-                            : (with_ext ? occupancy_any<false, true>(ord, smem) : occupancy_any<false, false>(ord, smem));
+    int per = 0;
+    switch (ord) {
+        case 1: per = occ<1>(with_m1, with_ext, smem); break;
+        case 2: per = occ<2>(with_m1, with_ext, smem); break;
+        case 3: per = occ<3>(with_m1, with_ext, smem); break;
+        case 4: per = occ<4>(with_m1, with_ext, smem); break;
+        case 5: per = occ<5>(with_m1, with_ext, smem); break;
+        default: return 0;
+    }
     return per * nsm;
 }
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t s) {
-    if (B.with_m1) return B.with_ext ? launch_any<true, true>(B, grid, smem, s) : launch_any<true, false>(B, grid, smem, s);
-    return B.with_ext ? launch_any<false, true>(B, grid, smem, s) : launch_any<false, false>(B, grid, smem, s);
+    switch (B.ord) {
+        case 1: return batch_launch_ord<1>(B, grid, smem, s);
+        case 2: return batch_launch_ord<2>(B, grid, smem, s);
+        case 3: return batch_launch_ord<3>(B, grid, smem, s);
+        case 4: return batch_launch_ord<4>(B, grid, smem, s);
+        case 5: return batch_launch_ord<5>(B, grid, smem, s);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace qzb

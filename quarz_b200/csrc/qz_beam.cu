@@ -29,6 +29,18 @@ __global__ void __launch_bounds__(kBeamThreads) beam_deposit_kernel(const BeamAr
     }
 }
 
+// the largest |w| of a beam (non-negative doubles order like their bit patterns, so an integer
+// maximum of the bits is the maximum)
+__global__ void __launch_bounds__(kBeamThreads) beam_wmax_kernel(const BeamArgs B, double* __restrict__ wmax) {
+    const long stride = (long)gridDim.x * blockDim.x;
+    double m = 0.0;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < B.n; i += stride) m = fmax(m, fabs(B.w[i]));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0 && m > 0.0)
+        atomicMax(reinterpret_cast<unsigned long long*>(wmax), (unsigned long long)__double_as_longlong(m));
+}
+
 // e^{-z} I0(z), e^{-z} I1(z) by the polynomial approximations of Abramowitz & Stegun 9.8.1-9.8.4
 // (relative error below 2e-7; the reference's choice, src/Beam.cpp:215-234)
 __device__ __forceinline__ void bessel_i01_scaled(double z, double& i0, double& i1) {
@@ -237,6 +249,12 @@ int beam_sums_blocks(long n) {
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s) {
     if (B.n <= 0) return cudaSuccess;
     beam_deposit_kernel<<<grid_for(B.n), kBeamThreads, 0, s>>>(B, bsrc);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_beam_wmax(const BeamArgs& B, double* wmax, cudaStream_t s) {
+    if (B.n <= 0) return cudaSuccess;
+    beam_wmax_kernel<<<grid_for(B.n), kBeamThreads, 0, s>>>(B, wmax);
     return cudaGetLastError();
 }
 

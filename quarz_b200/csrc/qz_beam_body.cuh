@@ -46,6 +46,15 @@ __device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restric
             const int jj = j + b;
             double* o = bsrc + ((size_t)kk * B.M + jj) * nc;
             const double d = wi * q * Wk[a] * Wr[b] * B.inv_V[jj] * B.idxi;
+            if (B.fx_qe) {                          // exact (m = 0 runs of qz_sim)
+                const int qe = B.fx_qe[jj];
+                beam_fx_add(o + B_RT0, B.fx_lo, d * omvz, qe, B.fx_s);
+                beam_fx_add(o + B_JZ0, B.fx_lo, d * vz, qe, B.fx_s);
+                beam_fx_add(o + B_JP1R, B.fx_lo, d * vr, qe, B.fx_s);
+                beam_fx_add(o + B_JP1I, B.fx_lo, d * vt, qe, B.fx_s);
+                beam_fx_add(o + B_RHO0, B.fx_lo, d, qe, B.fx_s);
+                continue;
+            }
             atomicAdd(o + B_RT0, d * omvz);
             atomicAdd(o + B_JZ0, d * vz);
             atomicAdd(o + B_JP1R, d * vr);
@@ -113,7 +122,7 @@ __device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, doubl
     return true;
 }
 
-// adds the 20 contributions of deposit_vals0 into bsrc (FP64 reductions into L2)
+// adds the 20 contributions of deposit_vals0 into bsrc (FP64 reductions into L2, or exact)
 __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restrict__ bsrc, int k, int j,
                                              const double (&v)[20]) {
 #pragma unroll
@@ -123,8 +132,14 @@ __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restri
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             double* o = bsrc + ((size_t)kk * B.M + j + b) * B_NC0;
+            if (B.fx_qe) {
+                const int qe = B.fx_qe[j + b];
 #pragma unroll
-            for (int c = 0; c < 5; ++c) atomicAdd(o + c, v[(2 * a + b) * 5 + c]);
+                for (int c = 0; c < 5; ++c) beam_fx_add(o + c, B.fx_lo, v[(2 * a + b) * 5 + c], qe, B.fx_s);
+            } else {
+#pragma unroll
+                for (int c = 0; c < 5; ++c) atomicAdd(o + c, v[(2 * a + b) * 5 + c]);
+            }
         }
     }
 }

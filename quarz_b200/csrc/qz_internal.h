@@ -57,6 +57,10 @@ struct SweepArgs {
     // optional: beam sources that do not change between steps (analytic rigid beams), (K, M, B_NC),
     // added to bsrc wherever the sweep reads it
     const double* bstat;
+    // optional, m = 0: bsrc in the exact two-limb format of the beam deposits (BeamArgs::fx_qe)
+    const int* bqe;
+    int bfx_s;
+    long bfx_lo;
 };
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter = false);
@@ -87,9 +91,18 @@ struct BeamArgs {
     double xi_min, dxi, idxi;
     int K, ngp, modes;
     int pusher;                     // 0 vay, 1 boris, 2 hc, 3 imp (stand-alone push kernels only)
+    // exact deposits (m = 0 runs of qz_sim): when fx_qe is set, bsrc holds two 64-bit integer limbs per
+    // value, the high limb where the double would be and the low limb fx_lo doubles further; a
+    // contribution v to node j is t = v / 2^fx_qe[j] split at fx_s bits (beam_fx_add)
+    const int* fx_qe;
+    int fx_s;
+    long fx_lo;
 };
 
 cudaError_t launch_beam_deposit(const BeamArgs& B, double* bsrc, cudaStream_t s);
+// the largest |w| of the beam's particles into *wmax (device; start it at 0): the bound of the exact
+// deposits' quantum
+cudaError_t launch_beam_wmax(const BeamArgs& B, double* wmax, cudaStream_t s);
 // Beam::deposit_analytic (src/Beam.cpp:236-279): a rigid beam's sources at every (slice, node)
 struct AnalyticArgs {
     double q, n0, s2, xi0, sxi, len, cut, x0, y0, xs, ys, vz, omvz;

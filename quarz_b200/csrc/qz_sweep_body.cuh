@@ -361,6 +361,40 @@ __device__ __forceinline__ bool warp_runs_sum(int key, double (&v)[NV]) {
     return (lane == 31) || (knext != key);
 }
 
+// ---------------------------------------------------------------- exact, order-independent deposits
+// The contributions of a deposit to a node array are summed as 64-bit integers in units of a power-
+// of-two quantum q, so the sum is the same whatever order the warps add in: every deposit, and with
+// it the whole sweep, is reproducible bit for bit. q is chosen per deposit and per array from the
+// largest contribution (its binary exponent: a block-wide maximum taken before the adds) and from
+// the most contributions one node can receive (2^bits; every partial sum stays below 2^63 quanta).
+// Relative to the largest contribution of the deposit the quantum is 2^(bits - 62): about one unit
+// in the last place of FP64 for the 511 plasma particles of a slice. A non-finite contribution makes
+// its array's values of that deposit NaN.
+__device__ __forceinline__ int fx_bexp(double v) {         // biased exponent: 0 for 0, 2047 for Inf / NaN
+    return (int)((__double_as_longlong(v) >> 52) & 0x7ff);
+}
+__device__ __forceinline__ int fx_qexp(int e, int bits) { return e - 1085 + bits; }   // (e - 1022) + bits - 63
+__device__ __forceinline__ void fx_add(double* p, double v, int e, int bits) {
+    atomicAdd(reinterpret_cast<unsigned long long*>(p),
+              (unsigned long long)__double2ll_rn(scalbn(v, -fx_qexp(e, bits))));
+}
+// the value of an accumulator (its 64 bits as stored in the double slot p)
+__device__ __forceinline__ double fx_value(const double* p, int e, int bits) {
+    if (e == 2047) return __longlong_as_double(0x7ff8000000000000LL);
+    return scalbn((double)__double_as_longlong(*p), fx_qexp(e, bits));
+}
+// warp-wide: E[c] = max(E[c], the largest e[c] of the warp's lanes) (shared-memory block maxima)
+template <int NC>
+__device__ __forceinline__ void fx_max(const int (&e)[NC], int* E) {
+#pragma unroll
+    for (int c = 0; c < NC; ++c) {
+        const unsigned m = __reduce_max_sync(FULL, (unsigned)e[c]);
+        if ((threadIdx.x & 31) == 0 && m) atomicMax(E + c, (int)m);
+    }
+}
+// headroom bits for n contributions per node: 2^bits > 2 n
+__device__ __forceinline__ int fx_bits(int n) { return 34 - __clz(n > 1 ? n : 1); }
+
 // ---------------------------------------------------------------- shared-memory layout
 struct Src {                                              // plasma + beam sources of one slice
     double *rhot, *drho, *jz, *chi, *ne, *ni, *jpi1, *S1r, *S1i;
@@ -379,6 +413,9 @@ struct Smem {
     double* ftot;                                         // A.filter: scan scratch of the filter, 2 x 14 x kW
     int* lost;
     int* flag;                                            // gate result broadcast
+    // block maxima of the deposits' exponents: [0, 7) the plasma deposit (rho - J_z, d/dxi, J_z, chi,
+    // n_e, n_i, J_theta), [7, 9) the S deposit, [9, 12) the background and neutralising deposits
+    int* fx;
 };
 
 __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
@@ -401,6 +438,7 @@ __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
     if (A.filter) { S.stage = p; p += 4 * (size_t)M; S.ftot = p; p += 2 * 14 * kW; }
     S.lost = reinterpret_cast<int*>(p);
     S.flag = S.lost + 1;
+    S.fx = S.lost + 2;
     return S;
 }
 
@@ -432,23 +470,32 @@ template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
     const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC0;
+    // one value of node j: a double, or the exact two-limb accumulator (A.bqe) turned into its value
+    const int qe = A.bqe ? A.bqe[j] : 0;
+    auto ld = [&](const double* p) -> double {
+        if (A.bqe) {
+            const double v = beam_fx_value(ldb<kL2>(p), ldb<kL2>(p + A.bfx_lo), qe, A.bfx_s);
+            if constexpr (kStat) return A.bstat ? v + __ldg(A.bstat + (p - bsrc)) : v;
+            return v;
+        }
+        return ldbs<kL2, kStat>(A, bsrc, p);
+    };
     BeamRow r;
-    r.rt = ldbs<kL2, kStat>(A, bsrc, bk + B_RT0);
-    r.jz = ldbs<kL2, kStat>(A, bsrc, bk + B_JZ0);
-    r.jt = ldbs<kL2, kStat>(A, bsrc, bk + B_JP1I);
+    r.rt = ld(bk + B_RT0);
+    r.jz = ld(bk + B_JZ0);
+    r.jt = ld(bk + B_JP1I);
     const int K = A.K;
     if (A.ngp) {
-        const double prev = (k > 0) ? ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st) : 0.0;
+        const double prev = (k > 0) ? ld(bk + B_RT0 - (ptrdiff_t)st) : 0.0;
         r.drt = (r.rt - prev) * A.idxi;
     } else if (K == 1) {
         r.drt = 0.0;
     } else if (k == 0) {
-        r.drt = (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) - r.rt) * A.idxi;
+        r.drt = (ld(bk + st + B_RT0) - r.rt) * A.idxi;
     } else if (k == K - 1) {
-        r.drt = (r.rt - ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
+        r.drt = (r.rt - ld(bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
     } else {
-        r.drt = 0.5 * (ldbs<kL2, kStat>(A, bsrc, bk + st + B_RT0) -
-                       ldbs<kL2, kStat>(A, bsrc, bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
+        r.drt = 0.5 * (ld(bk + st + B_RT0) - ld(bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
     }
     return r;
 }
@@ -479,6 +526,29 @@ __device__ __forceinline__ void init_sources(const Src& s, const Smem& S, int j,
     s.ne[j] = 0.0;
     s.S1r[j] = 0.0;
     s.S1i[j] = 0.0;
+}
+
+// the values a slice's 7 deposit arrays start from at node j (init_sources' values, for deposits
+// whose accumulators cannot hold them); with the smoothing filter the beam + background part goes to
+// the stage and the arrays start from zero
+template <bool kExt>
+__device__ __forceinline__ void init_base(const Smem& S, int j, const BeamRow& br, int M, double (&base)[7]) {
+    if (kExt && S.stage) {
+        S.stage[j] = S.bgt[j] + br.rt;
+        S.stage[M + j] = br.drt;
+        S.stage[2 * M + j] = br.jz;
+        S.stage[3 * M + j] = br.jt;
+#pragma unroll
+        for (int c = 0; c < 7; ++c) base[c] = 0.0;
+    } else {
+        base[0] = S.bgt[j] + br.rt;
+        base[1] = br.drt;
+        base[2] = br.jz;
+        base[3] = 0.0;
+        base[4] = 0.0;
+        base[5] = S.bgr[j] > 0.0 ? S.bgr[j] : 0.0;
+        base[6] = br.jt;
+    }
 }
 
 // The radial smoothing filter f <- F_n^{-1} f (FieldSolver::filter, src/FieldSolver.cpp:148-161) of NS
@@ -668,28 +738,71 @@ __device__ __forceinline__ void deposit_values(const PState<ORD>& P, const PGeo&
     }
 }
 
-// warp-wide: every lane calls it (active = the lane has a particle); key = 2 j + (positive species)
-__device__ __forceinline__ void deposit_warp(bool active, int j, bool neg, double (&v)[12], const Src& s) {
+// The plasma deposit of a slice, exact (see fx_add): phase A sums each warp's runs of equal
+// (cell, species sign) and takes the block maxima of the run sums' exponents; after a barrier phase B
+// adds the quantised run sums into the accumulator arrays; after another barrier deposit_finish turns
+// the accumulators into values. The 7 arrays in this order: rho - J_z, d/dxi, J_z, chi, n_e, n_i,
+// J_theta (n_e takes the negative species, n_i the positive ones).
+__device__ __forceinline__ double* dep_arr(const Src& s, int c) {
+    switch (c) {
+        case 0: return s.rhot;
+        case 1: return s.drho;
+        case 2: return s.jz;
+        case 3: return s.chi;
+        case 4: return s.ne;
+        case 5: return s.ni;
+        default: return s.jpi1;
+    }
+}
+
+// warp-wide phase A: every lane calls it (active = the lane has a particle); key = 2 j + (positive
+// species). Returns whether the lane holds a run sum to add; kExp: also take the exponent maxima
+// into E (a deposit that recomputes its values for phase B calls it again without)
+template <bool kExp>
+__device__ __forceinline__ bool deposit_runs(bool active, int j, bool neg, double (&v)[12], int* E) {
     const int lane = threadIdx.x & 31;
     if (!active)
 #pragma unroll
         for (int i = 0; i < 12; ++i) v[i] = 0.0;
     const int key = active ? 2 * j + (neg ? 0 : 1) : -1 - lane;
-    if (warp_runs_sum<12>(key, v) && active) {
-        double* dens = neg ? s.ne : s.ni;
-        double* adr[12];
+    const bool tail = warp_runs_sum<12>(key, v) && active;
+    if constexpr (kExp) {
+        int e[7] = {0, 0, 0, 0, 0, 0, 0};
+        if (tail) {
 #pragma unroll
-        for (int cc = 0; cc < 2; ++cc) {
-            const int jj = j + cc;
-            adr[6 * cc + 0] = s.rhot + jj;
-            adr[6 * cc + 1] = s.drho + jj;
-            adr[6 * cc + 2] = s.jz + jj;
-            adr[6 * cc + 3] = s.chi + jj;
-            adr[6 * cc + 4] = dens + jj;
-            adr[6 * cc + 5] = s.jpi1 + jj;
+            for (int c = 0; c < 6; ++c) {
+                const int ec = max(fx_bexp(v[c]), fx_bexp(v[6 + c]));
+                if (c < 4) e[c] = ec;
+                else if (c == 4) e[neg ? 4 : 5] = ec;
+                else e[6] = ec;
+            }
         }
-        add_multi<12>(adr, v);
+        fx_max<7>(e, E);
     }
+    return tail;
+}
+
+// phase B: the run sum of a tail lane into the accumulators of nodes j and j + 1
+__device__ __forceinline__ void deposit_add(bool tail, int j, bool neg, const double (&v)[12], const Src& acc,
+                                            const int* E, int bits) {
+    if (!tail) return;
+#pragma unroll
+    for (int cc = 0; cc < 2; ++cc) {
+        const int jj = j + cc;
+        fx_add(acc.rhot + jj, v[6 * cc + 0], E[0], bits);
+        fx_add(acc.drho + jj, v[6 * cc + 1], E[1], bits);
+        fx_add(acc.jz + jj, v[6 * cc + 2], E[2], bits);
+        fx_add(acc.chi + jj, v[6 * cc + 3], E[3], bits);
+        fx_add((neg ? acc.ne : acc.ni) + jj, v[6 * cc + 4], E[neg ? 4 : 5], bits);
+        fx_add(acc.jpi1 + jj, v[6 * cc + 5], E[6], bits);
+    }
+}
+
+// the values of node j: dst = base + accumulated deposit (acc and dst may be the same arrays)
+__device__ __forceinline__ void deposit_finish(const Src& dst, const Src& acc, int j, const double (&base)[7],
+                                               const int* E, int bits) {
+#pragma unroll
+    for (int c = 0; c < 7; ++c) dep_arr(dst, c)[j] = base[c] + fx_value(dep_arr(acc, c) + j, E[c], bits);
 }
 
 // src/PlasmaSpecies.cpp:508-559, m = 0: S+ contributions to nodes j (v[0..1]) and j+1 (v[2..3])
@@ -726,16 +839,40 @@ __device__ __forceinline__ void depositS_values(const PState<ORD>& P, const PGeo
     }
 }
 
-__device__ __forceinline__ void depositS_warp(bool active, int j, double (&v)[4], const Src& s) {
+// the S deposit of a slice, exact like the plasma deposit: phase A (run sums, exponent maxima into
+// E[0..1] for S_r, S_i), phase B after a barrier (adds into the slice's S arrays, which start at 0),
+// then each thread turns its own rows into values (depositS_finish) before the B+ solve reads them
+template <bool kExp>
+__device__ __forceinline__ bool depositS_runs(bool active, int j, double (&v)[4], int* E) {
     const int lane = threadIdx.x & 31;
     if (!active)
 #pragma unroll
         for (int i = 0; i < 4; ++i) v[i] = 0.0;
     const int key = active ? j : -1 - lane;
-    if (warp_runs_sum<4>(key, v) && active) {
-        double* adr[4] = {s.S1r + j, s.S1i + j, s.S1r + j + 1, s.S1i + j + 1};
-        add_multi<4>(adr, v);
+    const bool tail = warp_runs_sum<4>(key, v) && active;
+    if constexpr (kExp) {
+        int e[2] = {0, 0};
+        if (tail) {
+            e[0] = max(fx_bexp(v[0]), fx_bexp(v[2]));
+            e[1] = max(fx_bexp(v[1]), fx_bexp(v[3]));
+        }
+        fx_max<2>(e, E);
     }
+    return tail;
+}
+
+__device__ __forceinline__ void depositS_add(bool tail, int j, const double (&v)[4], const Src& s, const int* E,
+                                             int bits) {
+    if (!tail) return;
+    fx_add(s.S1r + j, v[0], E[0], bits);
+    fx_add(s.S1i + j, v[1], E[1], bits);
+    fx_add(s.S1r + j + 1, v[2], E[0], bits);
+    fx_add(s.S1i + j + 1, v[3], E[1], bits);
+}
+
+__device__ __forceinline__ void depositS_finish(const Src& s, int i, const int* E, int bits) {
+    s.S1r[i] = fx_value(s.S1r + i, E[0], bits);
+    s.S1i[i] = fx_value(s.S1i + i, E[1], bits);
 }
 
 // src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns false
@@ -891,6 +1028,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     if (A.const_smem)
         for (int t = tid; t < 13 * M; t += kThreads) const_cast<double*>(S.gm)[t] = A.consts[t];
     if (tid == 0) *S.lost = 0;
+    if (tid < 14) S.fx[tid] = 0;
+    const int bits_p = fx_bits(np), bits_bg = fx_bits(A.nbg);
     PState<ORD> P;
     int J = 0;                                             // cell of the thread's particle
     if (REG) {
@@ -921,28 +1060,50 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     }
     __syncthreads();
     // immobile species deposit into the background; mobile ones are subtracted (neutralisation,
-    // src/Simulation.cpp:672-684); src[0].ne is the scratch of the mobile deposit
-    for (int p = tid; p < A.nbg; p += kThreads) {
-        const double x = A.bg_p[p], y = A.bg_p[A.nbg + p], wq = A.bg_p[2 * A.nbg + p];
-        if (wq == 0.0) continue;
-        const PGeo g = geometry(S.r, S.ih, N, R, x, y);
-        const double a0 = wq * g.W0 * S.iv[g.j], a1 = wq * g.W1 * S.iv[g.j + 1];
-        double* adr[4] = {S.bgt + g.j, S.bgr + g.j, S.bgt + g.j + 1, S.bgr + g.j + 1};
-        const double val[4] = {a0, a0, a1, a1};
-        add_multi<4>(adr, val);
-    }
-    if (A.neutralize) {
-        double* ne0 = src_of(S, M, 0).ne;
-        for (int p = tid; p < np; p += kThreads) {
-            const double w = A.p_init[5 * (size_t)npad + p];
-            if (w == 0.0) continue;
-            double q, qm;
-            species_params(A, p, q, qm);
-            const PGeo g = geometry(S.r, S.ih, N, R, A.p_init[p], A.p_init[npad + p]);
-            double* adr[2] = {ne0 + g.j, ne0 + g.j + 1};
-            const double val[2] = {w * q * g.W0 * S.iv[g.j], w * q * g.W1 * S.iv[g.j + 1]};
-            add_multi<2>(adr, val);
+    // src/Simulation.cpp:672-684); src[0].ne is the scratch of the mobile deposit. Both exact: a pass
+    // for the exponent maxima, a barrier, a pass of quantised adds, a barrier, then the values.
+    double* const ne0 = src_of(S, M, 0).ne;
+    for (int pass = 0; pass < 2; ++pass) {
+        int ebg = 0, ene = 0;
+        for (int p = tid; p < A.nbg; p += kThreads) {
+            const double x = A.bg_p[p], y = A.bg_p[A.nbg + p], wq = A.bg_p[2 * A.nbg + p];
+            if (wq == 0.0) continue;
+            const PGeo g = geometry(S.r, S.ih, N, R, x, y);
+            const double a0 = wq * g.W0 * S.iv[g.j], a1 = wq * g.W1 * S.iv[g.j + 1];
+            if (pass == 0) {
+                ebg = max(ebg, max(fx_bexp(a0), fx_bexp(a1)));
+            } else {
+                fx_add(S.bgt + g.j, a0, S.fx[9], bits_bg);
+                fx_add(S.bgr + g.j, a0, S.fx[9], bits_bg);
+                fx_add(S.bgt + g.j + 1, a1, S.fx[9], bits_bg);
+                fx_add(S.bgr + g.j + 1, a1, S.fx[9], bits_bg);
+            }
         }
+        if (A.neutralize)
+            for (int p = tid; p < np; p += kThreads) {
+                const double w = A.p_init[5 * (size_t)npad + p];
+                if (w == 0.0) continue;
+                double q, qm;
+                species_params(A, p, q, qm);
+                const PGeo g = geometry(S.r, S.ih, N, R, A.p_init[p], A.p_init[npad + p]);
+                const double a0 = w * q * g.W0 * S.iv[g.j], a1 = w * q * g.W1 * S.iv[g.j + 1];
+                if (pass == 0) {
+                    ene = max(ene, max(fx_bexp(a0), fx_bexp(a1)));
+                } else {
+                    fx_add(ne0 + g.j, a0, S.fx[10], bits_p);
+                    fx_add(ne0 + g.j + 1, a1, S.fx[10], bits_p);
+                }
+            }
+        if (pass == 0) {
+            const int e2[2] = {ebg, ene};
+            fx_max<2>(e2, S.fx + 9);
+        }
+        __syncthreads();
+    }
+    for (int j = tid; j < M; j += kThreads) {
+        S.bgt[j] = fx_value(S.bgt + j, S.fx[9], bits_bg);
+        S.bgr[j] = fx_value(S.bgr + j, S.fx[9], bits_bg);
+        ne0[j] = fx_value(ne0 + j, S.fx[10], bits_p);
     }
     if (Gate::kActive && tid < 32) {                     // warp 0 checks the beam-source rows
         const bool ok = gate.before_rows(K - 1 < 2 ? K - 1 : 2);
@@ -953,54 +1114,81 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     if (EXT && A.filter) {              // the background is smoothed like the plasma (src/Simulation.cpp:685-690)
         if (A.neutralize)
             for (int j = tid; j < M; j += kThreads) {
-                const Src s0 = src_of(S, M, 0);
-                S.bgt[j] -= s0.ne[j];
-                S.bgr[j] -= s0.ne[j];
+                S.bgt[j] -= ne0[j];
+                S.bgr[j] -= ne0[j];
             }
         __syncthreads();
         FilterSet<2> fb;
         fb.f[0] = S.bgt; fb.f[1] = S.bgr; fb.op[0] = fb.op[1] = 0;
         filter_rows<2, kMaxR>(fb, A.fconsts, M, Rw, S.ftot);
         __syncthreads();
-        for (int j = tid; j < M; j += kThreads)
-            init_sources<EXT>(src_of(S, M, 0), S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M);
-    } else {
+    } else if (A.neutralize) {
         for (int j = tid; j < M; j += kThreads) {
-            const Src s0 = src_of(S, M, 0);
-            if (A.neutralize) { S.bgt[j] -= s0.ne[j]; S.bgr[j] -= s0.ne[j]; }
-            init_sources<EXT>(s0, S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M);
+            S.bgt[j] -= ne0[j];
+            S.bgr[j] -= ne0[j];
+        }
+    }
+    // slice 0's arrays accumulate its plasma deposit from zero; its start values (background + beam,
+    // init_base) are added when the deposit is finished
+    {
+        const Src s0 = src_of(S, M, 0);
+        for (int j = tid; j < M; j += kThreads) {
+#pragma unroll
+            for (int c = 0; c < 7; ++c) dep_arr(s0, c)[j] = 0.0;
+            s0.S1r[j] = 0.0;
+            s0.S1i[j] = 0.0;
         }
     }
     __syncthreads();
     // deposit of slice 0
     const int lane = tid & 31;
-    if (REG) {
-        const bool act = tid < np && P.w != 0.0;
-        double v[12];
-        if (act) {
-            const PGeo G = geometry(S.r, S.ih, N, R, P.x, P.y);
-            J = G.j;
-            deposit_values(P, G, S, v);
-        }
-        deposit_warp(act, J, P.q < 0.0, v, src_of(S, M, 0));
-    } else {
-        for (int base = tid - lane; base < np; base += kThreads) {
-            const int p = base + lane;
-            PState<ORD> Q;
-            bool act = false;
-            int j = 0;
+    {
+        const Src s0 = src_of(S, M, 0);
+        if (REG) {
+            const bool act = tid < np && P.w != 0.0;
             double v[12];
-            if (p < np) {
-                pload(Q, gate.ps(A), npad, p);
-                species_params(A, p, Q.q, Q.qm);
-                act = Q.w != 0.0;
-                if (act) {
-                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                    j = g.j;
-                    deposit_values(Q, g, S, v);
+            if (act) {
+                const PGeo G = geometry(S.r, S.ih, N, R, P.x, P.y);
+                J = G.j;
+                deposit_values(P, G, S, v);
+            }
+            const bool tail = deposit_runs<true>(act, J, P.q < 0.0, v, S.fx);
+            __syncthreads();
+            deposit_add(tail, J, P.q < 0.0, v, s0, S.fx, bits_p);
+        } else {
+            for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1) __syncthreads();
+                for (int base = tid - lane; base < np; base += kThreads) {
+                    const int p = base + lane;
+                    PState<ORD> Q;
+                    bool act = false;
+                    int j = 0;
+                    double v[12];
+                    if (p < np) {
+                        pload(Q, gate.ps(A), npad, p);
+                        species_params(A, p, Q.q, Q.qm);
+                        act = Q.w != 0.0;
+                        if (act) {
+                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                            j = g.j;
+                            deposit_values(Q, g, S, v);
+                        }
+                    }
+                    const bool neg = act && Q.q < 0.0;
+                    if (pass == 0) {
+                        deposit_runs<true>(act, j, neg, v, S.fx);
+                    } else {
+                        const bool tail = deposit_runs<false>(act, j, neg, v, S.fx);
+                        deposit_add(tail, j, neg, v, s0, S.fx, bits_p);
+                    }
                 }
             }
-            deposit_warp(act, j, act && Q.q < 0.0, v, src_of(S, M, 0));
+        }
+        __syncthreads();
+        for (int j = tid; j < M; j += kThreads) {
+            double b0[7];
+            init_base<EXT>(S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M, b0);
+            deposit_finish(s0, s0, j, b0, S.fx, bits_p);
         }
     }
     __syncthreads();
@@ -1130,34 +1318,49 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         __syncthreads();
         PHASE_MARK(1);
 
-        // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559)
+        // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559), exact
+        if (tid < 7) S.fx[tid] = 0;           // the plasma deposit's maxima (read last before P2's barrier)
         if (REG) {
             const bool act = tid < np && P.w != 0.0;
             double v[4];
             if (act) depositS_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, N, v);
-            depositS_warp(act, J, v, s);
+            const bool tail = depositS_runs<true>(act, J, v, S.fx + 7);
+            __syncthreads();
+            depositS_add(tail, J, v, s, S.fx + 7, bits_p);
         } else {
-            for (int base = tid - lane; base < np; base += kThreads) {
-                const int p = base + lane;
-                bool act = false;
-                int j = 0;
-                double v[4];
-                if (p < np) {
-                    PState<ORD> Q;
-                    pload(Q, gate.ps(A), npad, p);
-                    species_params(A, p, Q.q, Q.qm);
-                    act = Q.w != 0.0;
-                    if (act) {
-                        const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                        j = g.j;
-                        depositS_values(Q, g, S, N, v);
+            for (int pass = 0; pass < 2; ++pass) {
+                if (pass == 1) __syncthreads();
+                for (int base = tid - lane; base < np; base += kThreads) {
+                    const int p = base + lane;
+                    bool act = false;
+                    int j = 0;
+                    double v[4];
+                    if (p < np) {
+                        PState<ORD> Q;
+                        pload(Q, gate.ps(A), npad, p);
+                        species_params(A, p, Q.q, Q.qm);
+                        act = Q.w != 0.0;
+                        if (act) {
+                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                            j = g.j;
+                            depositS_values(Q, g, S, N, v);
+                        }
+                    }
+                    if (pass == 0) {
+                        depositS_runs<true>(act, j, v, S.fx + 7);
+                    } else {
+                        const bool tail = depositS_runs<false>(act, j, v, S.fx + 7);
+                        depositS_add(tail, j, v, s, S.fx + 7, bits_p);
                     }
                 }
-                depositS_warp(act, j, v, s);
             }
         }
         __syncthreads();
         PHASE_MARK(2);
+        // this thread's rows of S+ into values: the only rows its B+ rows (and the filter) read
+#pragma unroll
+        for (int u = 0; u < kMaxR; ++u)
+            if (u < Rw && row0 + u < M) depositS_finish(s, row0 + u, S.fx + 7, bits_p);
 
         // ---------------- P4: B+ (src/Simulation.cpp:535-591, m = 0: one pass)
         //   (L1D - chi) B_r0 = -S_i (rows 0, N Dirichlet); (L1F - chi) B_theta0 = J_z' + S_r, flux wall J_z(R)
@@ -1260,6 +1463,11 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         PHASE_MARK(3);
 
         // ---------------- P5: store slice k; push k -> k+1 and deposit into slice k+1
+        if (tid >= 7 && tid < 9) S.fx[tid] = 0;   // the S deposit's maxima (read last before P4's barrier)
+        // The accumulators of the next slice's deposit: with double-buffered sources this slice's buffer,
+        // free once stored (the next slice's start values already sit in sn); with one buffer that
+        // buffer, its start values added when the deposit is finished. Either way zeroed by the store.
+        const Src acc = A.dbuf ? s : sn;
         {
             const size_t fb = (size_t)k * M;
             for (int j = tid; j < M; j += kThreads) {
@@ -1274,15 +1482,19 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 D[D_PSI0] = S.psi[j];
                 D[D_NE0] = s.ne[j];
                 D[D_NI0] = s.ni[j];
+                if (k + 1 < K) {
+#pragma unroll
+                    for (int c = 0; c < 7; ++c) dep_arr(acc, c)[j] = 0.0;
+                    if (!A.dbuf) { acc.S1r[j] = 0.0; acc.S1i[j] = 0.0; }
+                }
             }
         }
         if (k + 1 < K) {
-            if (!A.dbuf) {
-                __syncthreads();                                    // the store read the sources
-                for (int j = tid; j < M; j += kThreads)
-                    init_sources<EXT>(sn, S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, j), M);
-                __syncthreads();
-            }
+            BeamRow nxt[kMaxR];                 // one buffer: the beam rows of slice k+1 for this thread's rows
+            if (!A.dbuf)
+#pragma unroll
+                for (int u = 0; u < kMaxR; ++u)
+                    if (u < Rw && row0 + u < M) nxt[u] = beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u);
             const bool first = (k == 0);
             if (REG) {
                 bool act = tid < np && P.w != 0.0;
@@ -1297,32 +1509,66 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                         atomicAdd(S.lost, 1);
                     }
                 }
-                deposit_warp(act, J, P.q < 0.0, v, sn);
+                const bool tail = deposit_runs<true>(act, J, P.q < 0.0, v, S.fx);
+                __syncthreads();
+                deposit_add(tail, J, P.q < 0.0, v, acc, S.fx, bits_p);
             } else {
-                for (int base = tid - lane; base < np; base += kThreads) {
-                    const int p = base + lane;
-                    bool act = false;
-                    int j = 0;
-                    double v[12];
-                    PState<ORD> Q;
-                    if (p < np) {
-                        pload(Q, gate.ps(A), npad, p);
-                        species_params(A, p, Q.q, Q.qm);
-                        if (Q.w != 0.0) {
-                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                            if (push_particle(Q, g, S, A, first)) {
-                                const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                                j = g2.j;
-                                deposit_values(Q, g2, S, v);
-                                act = true;
-                            } else {
-                                atomicAdd(S.lost, 1);
+                // pass 0 pushes and takes the exponent maxima; pass 1 recomputes the deposit values of
+                // the pushed particles and adds them
+                for (int pass = 0; pass < 2; ++pass) {
+                    if (pass == 1) __syncthreads();
+                    for (int base = tid - lane; base < np; base += kThreads) {
+                        const int p = base + lane;
+                        bool act = false;
+                        int j = 0;
+                        double v[12];
+                        PState<ORD> Q;
+                        if (p < np) {
+                            pload(Q, gate.ps(A), npad, p);
+                            species_params(A, p, Q.q, Q.qm);
+                            if (Q.w != 0.0) {
+                                if (pass == 0) {
+                                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                    if (push_particle(Q, g, S, A, first)) {
+                                        const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                        j = g2.j;
+                                        deposit_values(Q, g2, S, v);
+                                        act = true;
+                                    } else {
+                                        atomicAdd(S.lost, 1);
+                                    }
+                                    pstore(Q, gate.ps(A), npad, p);
+                                } else {
+                                    const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                    j = g2.j;
+                                    deposit_values(Q, g2, S, v);
+                                    act = true;
+                                }
                             }
-                            pstore(Q, gate.ps(A), npad, p);
+                        }
+                        const bool neg = act && Q.q < 0.0;
+                        if (pass == 0) {
+                            deposit_runs<true>(act, j, neg, v, S.fx);
+                        } else {
+                            const bool tail = deposit_runs<false>(act, j, neg, v, S.fx);
+                            deposit_add(tail, j, neg, v, acc, S.fx, bits_p);
                         }
                     }
-                    deposit_warp(act, j, act && Q.q < 0.0, v, sn);
                 }
+            }
+            __syncthreads();
+#pragma unroll
+            for (int u = 0; u < kMaxR; ++u) {
+                const int i = row0 + u;
+                if (u >= Rw || i >= M) continue;
+                double b0[7];
+                if (A.dbuf) {
+#pragma unroll
+                    for (int c = 0; c < 7; ++c) b0[c] = dep_arr(sn, c)[i];
+                } else {
+                    init_base<EXT>(S, i, nxt[u], M, b0);
+                }
+                deposit_finish(sn, acc, i, b0, S.fx, bits_p);
             }
         }
         if (Gate::kActive) gate.slice_done_all(k);                     // every thread, before the barrier
