@@ -20,6 +20,8 @@ Other workloads (not the headline; their lines are recorded beside it):
   --workload scan_m1  the same scan with azimuthal modes 0 and 1 (M <= 512)
   --workload adjoint  the gradient of witness energy gain and spread with respect to a 64-bin driver
                       profile and the witness delay, pinched witness over 50 steps: adjoint / forward time
+  --workload stages   the xi-pipelined run over the ranks (one slab of the box per GPU, the reference's
+                      multi-rank mode), pinched witness with the ngp xi shape, 20 steps
   --smooth A          the pinched-witness or hosing run with plasma.smooth_length = A (the radial
                       smoothing of the plasma sources; 0.005 in the reference's validation section 14)
 
@@ -313,7 +315,8 @@ def run_b200(args, rank, world, local_rank):
     e2e = run_e2e(args, spec, beams, sim, dev) if args.e2e_steps > 0 else None
     launches = (OWN_LAUNCHES_PER_BEAM * len(beams) + OWN_LAUNCHES_PER_RUN) * args.steps
     return {"ms": ms, "kernel_ms": kernel_ms, "clocks": clk.result(), "spec": spec, "nb_total": nb_total,
-            "launches": launches, "e2e": e2e, "schedule": sched, "beams": beams, "sim": sim, "dev": dev}
+            "launches": launches, "e2e": e2e, "schedule": sched, "beams": beams, "sim": sim, "dev": dev,
+            "init": init}
 
 
 def run_e2e(args, spec, beams, sim, dev):
@@ -380,6 +383,53 @@ def run_hosing_extra(dev, steps=2, warmup=1, cpu_steps=1):
                            "sample": f"{cpu_steps} full time step(s) of the hosing run (sweep + moment sums + push "
                                      f"of 4e6 particles), oracle on {oracle_rate.threads} host threads, {el:.1f} s"}
     return out
+
+
+def run_stages(args, rank, world, local_rank):
+    """The xi-pipelined run (quarz_b200.stages): the pinched-witness deck with the ngp xi shape, the box cut
+    into one slab per rank; slice-solves/s of the whole job, timed on the device (max over ranks)."""
+    import numpy as np
+    import torch
+
+    import quarz_b200 as Q
+    from quarz_b200 import stages, workloads
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    spec = workloads.spec_from_text(workloads.pinched_witness_deck(steps=args.time_steps or 20),
+                                    ["beams.xi_shape=ngp"])
+    T = spec.steps
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    ms = []
+    for it in range(args.warmup + args.steps):
+        run = stages.Stages(spec, world, beams, ranks=[rank], device=dev)
+        if world > 1:
+            st = run.stages[0]
+            np_, npad, order = st.sweep.state_shape()
+            run.channel = stages.DistChannel(dev, len(beams), (6 + 5 * order, npad), spec.M)
+            run.local = False
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        run.run(T, spec.dt)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        if it >= args.warmup:
+            ms.append(e0.elapsed_time(e1))
+        del run
+    t = float(np.median(ms))
+    if world > 1:
+        tt = torch.tensor([t], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        t = float(tt.item())
+    nb = sum(len(p) for p, _, _ in beams)
+    return {"metric": METRIC, "value": spec.K * (T + 1) / (t * 1e-3), "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t, "higher_is_better": True,
+            "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": _config(spec, nb, T, {"xi_shape": "ngp", "parallelism": f"xi-pipelined over {world} slab(s)"},
+                              "stages"),
+            "gpu_launches": None}
 
 
 def run_scan(args, rank, world, local_rank):
@@ -486,13 +536,19 @@ def run_adjoint(args, rank, world, local_rank):
     seeds = np.zeros((len(beams), 17))
     seeds[1] = A.gain_seed(mom[-1, 1])
     adj, split, grads = [], [], None
+    # one simulation for every gradient, its beams reset before each (as for the forward runs above), so
+    # that its rings are allocated once and not inside a timed forward; the first gradient is a warm-up
+    s2 = Q.Simulation(spec, beams=beams)
     with ClockSampler(local_rank) as clk:
-        for it in range(max(1, args.steps)):
-            s2 = Q.Simulation(spec, beams=beams)
+        for it in range(max(1, args.steps) + 1):
+            for b in range(len(init)):
+                s2.set_beam(b, init[b])
+            s2.restart()
             lam, _, ms = s2.adjoint(T, dt, seeds)
-            adj.append(ms[0] + ms[1])
-            split.append(ms)
-            del s2
+            if it:
+                adj.append(ms[0] + ms[1])
+                split.append(ms)
+    del s2
     grads = (A.profile_gradient(lam[0], beams[0][0], prof), A.delay_gradient(lam[1]))
     f_ms, a_ms = float(np.median(fwd)), float(np.median(adj))
     nbt = sum(len(p) for p, _, _ in beams)
@@ -599,7 +655,7 @@ def main():
     ap.add_argument("--no-extras", action="store_true",
                     help="headline only: no latency roofline, FP64 rate or hosing / scan / adjoint lines")
     ap.add_argument("--time-steps", type=int, default=0, help="time steps per run (default: the workload's)")
-    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1", "adjoint"],
+    ap.add_argument("--workload", choices=["pinched_witness", "hosing", "scan", "scan_m1", "adjoint", "stages"],
                     default="pinched_witness")
     ap.add_argument("--smooth", type=float, default=0.0,
                     help="plasma.smooth_length of the pinched-witness / hosing run (0: none, the headline)")
@@ -649,6 +705,15 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     if args.workload == "adjoint":
         line = run_adjoint(args, rank, world, local_rank)
+        if rank == 0:
+            print(json.dumps(line))
+        return
+    if args.workload == "stages":
+        line = run_stages(args, rank, world, local_rank)
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
         if rank == 0:
             print(json.dumps(line))
         return
@@ -742,7 +807,22 @@ def extras(args, r, line):
                                "plasma particle's dependent chain ~2,000 cycles, at the median SM clock under load",
                 "frac_standalone": floor_us / lat["sweep_us_per_slice_standalone"],
                 "frac_in_pipeline": floor_us / lat["sweep_us_per_slice_in_pipeline"]})
-    del r["sim"]
+    # the cost of exact deposits: the same run with FP64 reductions for the beam deposits
+    sim = r["sim"]
+    sim.set_exact(False)
+    fms = []
+    for it in range(4):
+        for b in range(len(r["init"])):
+            sim.set_beam(b, r["init"][b])
+        sim.run(T, spec.dt)
+        if it:
+            fms.append(sim.times()["kernel_ms"])
+    sim.set_exact(True)
+    fk = sorted(fms)[len(fms) // 2]
+    out["fp64_beam_deposits"] = {"kernel_ms_per_run": fk, "value": spec.K * (T + 1) / (fk * 1e-3), "unit": UNIT,
+                                 "note": "the headline run with qz_sim_set_exact(0): FP64 reductions for the beam "
+                                         "deposits (run-to-run last-bit differences) instead of exact integer sums"}
+    del r["sim"], sim
     torch.cuda.empty_cache()
     line["roofline"]["latency"] = lat
     kms = line["kernel_ms_per_run"]

@@ -84,8 +84,12 @@ typedef struct {
 } qz_sweep_params;
 
 typedef struct {
-    unsigned long long lost;     /* plasma particles removed (trapped / beyond the wall) */
-    unsigned long long reserved[3];
+    unsigned long long lost;      /* plasma particles removed (trapped or beyond the wall; the reference's
+                                     lost counter, src/PlasmaSpecies.cpp:639-655) */
+    unsigned long long nonfinite; /* deposits (per slice and array) that met a NaN or Inf contribution: the
+                                     array's values of that slice are NaN */
+    unsigned long long trapped;   /* of lost: removed as trapped (Delta <= delta_min or gamma > max_qsa Delta) */
+    unsigned long long giveup;    /* pipelined runs that ended because a bounded wait timed out */
 } qz_counters;
 
 typedef struct qz_sweep qz_sweep;
@@ -96,6 +100,31 @@ qz_status qz_sweep_run(qz_sweep* s, const double* bsrc_dev, double* fld_dev, dou
                        qz_counters* counters_host, void* stream);
 /* plasma state after the last sweep: out_host (6, n) = x y px py Delta w; returns n in *n */
 qz_status qz_sweep_plasma(qz_sweep* s, double* out_host, int cap, int* n);
+
+/* The plasma a slab of a xi-pipelined run hands to the next one (the plasma part of the message of
+   Simulation::make_message, src/Simulation.cpp:851-870, and PlasmaSpecies::pack_state,
+   src/PlasmaSpecies.cpp:317-334): the sweep's np particles with stride npad as (6 + 5 order) device rows
+   x y px py Delta w, then the Adams-Bashforth history h[m][v] (the force m pushes ago, v = d/dxi of x, y,
+   px, py, Delta), and whether the particles have been pushed (their history is filled). */
+typedef struct {
+    double* state;
+    int np, npad, order;
+    int pushed;
+} qz_plasma_state;
+/* the shape of a sweep's plasma state (allocate (6 + 5 order) x npad doubles) */
+qz_status qz_sweep_state_shape(qz_sweep* s, int* np, int* npad, int* order);
+/* One sweep over a slab of the box, a stage of the reference's xi-pipelined multi-rank run
+   (Simulation::step_fields with a message, src/Simulation.cpp:714-731, :755, and Simulation::run,
+   :1380-1400). The sweep s was created with the slab's slices (K and xi_min of the slab). in: the
+   plasma entering the slab's first slice (NULL: the fresh plasma of the box head); bguard (dev, M x
+   B_NC of the slab's sweep, NULL: none): the beam sources of the slice just ahead of the slab (the
+   upstream slab's last row, Simulation::set_guard, :459-465); out (NULL: none): receives the plasma
+   after the push of the slab's last slice, the state entering the next slab. A slab that takes a guard
+   or hands its plasma on needs the ngp xi shape; modes = 0, without the smoothing filter. Two or more
+   slabs run one after the other give the fields and plasma of the whole sweep bit for bit. */
+qz_status qz_sweep_run_stage(qz_sweep* s, const double* bsrc_dev, const double* bguard_dev, const qz_plasma_state* in,
+                             double* fld_dev, double* diag_dev, qz_plasma_state* out, qz_counters* counters_host,
+                             void* stream);
 /* per-phase clock cycles of the last run, 16 counters: [0] prologue, [1] psi/E_z/B_z phase, [2] S+ deposit,
    [3] B+ phase, [4] store + push + deposit, [5..8] parts of phase 1; enable = 1 turns the counters on for
    later runs */
@@ -235,6 +264,15 @@ qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, voi
    No counterpart in the reference (its own pipelining over time steps is across MPI ranks,
    src/Simulation.cpp:851-870). */
 qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span, double timeout_s);
+/* exact = 1 (the default): the beam deposits of m = 0 runs are exact integer sums (two 64-bit limbs per
+   value), so runs repeat bit for bit; exact = 0: FP64 reductions, faster (one reduction per value and half
+   the beam-source memory) but their summation order, and so the last bits, vary from run to run. No
+   counterpart in the reference (its OpenMP and GPU deposits use atomic adds). */
+qz_status qz_sim_set_exact(qz_sim* s, int exact);
+/* The next run starts every beam's leapfrog again (the start-up half kick of Beam::push,
+   src/Beam.cpp:903, src/Simulation.cpp:1434-1436): a new run from beams set with qz_sim_set_beam, which
+   otherwise continue where the last run left them. */
+qz_status qz_sim_restart(qz_sim* s);
 /* the schedule of the last qz_sim_run: grid, sweep CTAs, push CTAs, ring slots, buckets, bucket size,
    pipelined (1/0), cell span of a bucket */
 qz_status qz_sim_schedule(qz_sim* s, int* info8);

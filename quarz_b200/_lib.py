@@ -30,7 +30,12 @@ class SweepParams(C.Structure):
 
 
 class Counters(C.Structure):
-    _fields_ = [("lost", C.c_ulonglong), ("reserved", C.c_ulonglong * 3)]
+    _fields_ = [("lost", C.c_ulonglong), ("nonfinite", C.c_ulonglong), ("trapped", C.c_ulonglong),
+                ("giveup", C.c_ulonglong)]
+
+
+class PlasmaState(C.Structure):
+    _fields_ = [("state", C.c_void_p), ("np", C.c_int), ("npad", C.c_int), ("order", C.c_int), ("pushed", C.c_int)]
 
 
 class BeamView(C.Structure):
@@ -65,6 +70,9 @@ SIGNATURES = {
     "qz_sweep_destroy": [C.c_void_p],
     "qz_sweep_run": [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(Counters), C.c_void_p],
     "qz_sweep_plasma": [C.c_void_p, _dp, C.c_int, C.POINTER(C.c_int)],
+    "qz_sweep_state_shape": [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int)],
+    "qz_sweep_run_stage": [C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(PlasmaState), C.c_void_p, C.c_void_p,
+                           C.POINTER(PlasmaState), C.POINTER(Counters), C.c_void_p],
     "qz_sweep_timing": [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)],
     "qz_beam_deposit": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_void_p],
     "qz_beam_advance": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,
@@ -93,6 +101,8 @@ SIGNATURES = {
     "qz_sim_beam": [C.c_void_p, C.c_int, _dp],
     "qz_sim_counters": [C.c_void_p, C.POINTER(Counters)],
     "qz_sim_step_host": [C.c_void_p, C.POINTER(C.c_void_p), C.c_double, C.c_double, C.c_int, _dp, C.c_void_p],
+    "qz_sim_restart": [C.c_void_p],
+    "qz_sim_set_exact": [C.c_void_p, C.c_int],
     "qz_sim_set_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double],
     "qz_sim_schedule": [C.c_void_p, C.POINTER(C.c_int)],
     "qz_sim_times": [C.c_void_p, _dp],

@@ -11,7 +11,7 @@ from typing import List, Optional, Sequence, Tuple
 import numpy as np
 
 from . import deck as _deck
-from ._lib import AnalyticBeam, BeamView, Box, Counters, QZError, Species, SweepParams, check, lib
+from ._lib import AnalyticBeam, BeamView, Box, Counters, PlasmaState, QZError, Species, SweepParams, check, lib
 
 _dp = C.POINTER(C.c_double)
 
@@ -110,6 +110,42 @@ class Sweep:
 
     def run_async(self, bsrc, fld, diag, stream=None) -> None:
         check(lib().qz_sweep_run(self.h, _dev(bsrc), _dev(fld), _dev(diag), None, _stream_ptr(stream)))
+
+    def state_shape(self) -> Tuple[int, int, int]:
+        """(np, npad, AB order) of the plasma state a slab hands on (qz_sweep_state_shape)."""
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        check(lib().qz_sweep_state_shape(self.h, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def new_state(self):
+        """An empty plasma state for this sweep: a (6 + 5 order, npad) float64 CUDA tensor with its pushed
+        flag (attribute .pushed)."""
+        import torch
+
+        np_, npad, order = self.state_shape()
+        t = torch.zeros((6 + 5 * order, npad), dtype=torch.float64, device="cuda")
+        t.pushed = False
+        return t
+
+    def _state(self, t) -> PlasmaState:
+        np_, npad, order = self.state_shape()
+        if tuple(t.shape) != (6 + 5 * order, npad):
+            raise QZError(1, f"plasma state of shape {tuple(t.shape)}, the sweep's is {(6 + 5 * order, npad)}")
+        return PlasmaState(state=_dev(t), np=np_, npad=npad, order=order, pushed=1 if getattr(t, "pushed", False) else 0)
+
+    def run_stage(self, bsrc, fld, diag, guard=None, state_in=None, state_out=None, stream=None) -> dict:
+        """qz_sweep_run_stage: one slab of a xi-pipelined sweep. state_in / state_out: plasma states
+        (new_state()); guard: the beam sources of the slice ahead of the slab (M x 5 CUDA tensor) or None.
+        Returns the counters of the sweep."""
+        cnt = Counters()
+        sin = self._state(state_in) if state_in is not None else None
+        sout = self._state(state_out) if state_out is not None else None
+        check(lib().qz_sweep_run_stage(self.h, _dev(bsrc), _dev(guard) if guard is not None else None,
+                                       C.byref(sin) if sin is not None else None, _dev(fld), _dev(diag),
+                                       C.byref(sout) if sout is not None else None, C.byref(cnt), _stream_ptr(stream)))
+        if state_out is not None:
+            state_out.pushed = True
+        return {"lost": int(cnt.lost), "nonfinite": int(cnt.nonfinite), "trapped": int(cnt.trapped)}
 
     def plasma(self) -> np.ndarray:
         cap = 1 << 22
@@ -323,6 +359,14 @@ class Simulation:
         check(lib().qz_sim_set_schedule(self.h, 1 if pipelined else 0, int(sweep_ctas), int(bucket), int(span),
                                         float(timeout_s)))
 
+    def restart(self):
+        """qz_sim_restart: the next run starts the beams' leapfrog again (a new run from set beams)."""
+        check(lib().qz_sim_restart(self.h))
+
+    def set_exact(self, exact: bool = True):
+        """qz_sim_set_exact: exact (reproducible) or FP64-reduction beam deposits for m = 0 runs."""
+        check(lib().qz_sim_set_exact(self.h, 1 if exact else 0))
+
     def schedule(self) -> dict:
         """The schedule of the last run (qz_sim_schedule)."""
         info = (C.c_int * 8)()
@@ -444,9 +488,14 @@ class Simulation:
         check(lib().qz_sim_write_fields(self.h, float(t), str(path).encode()))
 
     def lost(self) -> int:
+        return self.counters()["lost"]
+
+    def counters(self) -> dict:
+        """qz_sim_counters: plasma particles removed (of them trapped), deposits with a non-finite
+        contribution, pipelined runs that gave up on a wait."""
         c = Counters()
         check(lib().qz_sim_counters(self.h, C.byref(c)))
-        return int(c.lost)
+        return {"lost": int(c.lost), "nonfinite": int(c.nonfinite), "trapped": int(c.trapped), "giveup": int(c.giveup)}
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -460,16 +460,32 @@ extern "C" qz_status qz_sweep_destroy(qz_sweep* s) {
 }
 
 namespace {
-// one sweep of s over bsrc; bqe set: bsrc in the exact two-limb format (qz_sim's m = 0 runs)
+// the optional arguments of one sweep: bsrc in the exact two-limb format (qz_sim's m = 0 runs: the
+// node quanta bq, 2^S, the offset of the low limbs) and a slab of a staged run (qz_sweep_run_stage)
+struct SweepExtra {
+    const double* bq = nullptr;
+    double bfx_2s = 0.0;
+    long bfx_lo = 0;
+    const double* pin = nullptr;
+    int pin_pushed = 0;
+    const double* bguard = nullptr;
+    double* pout = nullptr;
+};
+
+// one sweep of s over bsrc
 qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
-                       cudaStream_t st, const int* bqe, int bfx_s, long bfx_lo) {
+                       cudaStream_t st, const SweepExtra& x = SweepExtra()) {
     qzb::SweepArgs A = s->base;
     A.bsrc = bsrc;
     A.fld = fld;
     A.diag = diag;
-    A.bqe = bqe;
-    A.bfx_s = bfx_s;
-    A.bfx_lo = bfx_lo;
+    A.bq = x.bq;
+    A.bfx_2s = x.bfx_2s;
+    A.bfx_lo = x.bfx_lo;
+    A.pin = x.pin;
+    A.pin_pushed = x.pin_pushed;
+    A.bguard = x.bguard;
+    A.pout = x.pout;
     QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
     if (s->timing) {
         QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 16, st));
@@ -481,6 +497,8 @@ qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* dia
         QZ_CUDA(cudaMemcpyAsync(h, s->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
         QZ_CUDA(cudaStreamSynchronize(st));
         cnt->lost += h[0];
+        cnt->nonfinite += h[1];
+        cnt->trapped += h[2];
     }
     return QZ_OK;
 }
@@ -489,7 +507,50 @@ qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* dia
 extern "C" qz_status qz_sweep_run(qz_sweep* s, const double* bsrc, double* fld, double* diag, qz_counters* cnt,
                                   void* stream) {
     if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run: null pointer");
-    return sweep_launch(s, bsrc, fld, diag, cnt, (cudaStream_t)stream, nullptr, 0, 0);
+    return sweep_launch(s, bsrc, fld, diag, cnt, (cudaStream_t)stream);
+}
+
+extern "C" qz_status qz_sweep_state_shape(qz_sweep* s, int* np, int* npad, int* order) {
+    if (!s || !np || !npad || !order) return fail(QZ_ERR_ARG, "qz_sweep_state_shape: null pointer");
+    *np = s->np;
+    *npad = s->npad;
+    *order = s->p.ab_order;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_run_stage(qz_sweep* s, const double* bsrc, const double* bguard,
+                                        const qz_plasma_state* in, double* fld, double* diag, qz_plasma_state* out,
+                                        qz_counters* cnt, void* stream) {
+    if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run_stage: null pointer");
+    if (s->p.modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: modes = 0 sweeps only");
+    if (s->base.filter || s->base.bstat)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: no smoothing filter or static beam sources in a stage");
+    if ((bguard || out) && !s->p.ngp)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: slabs that take a guard row or hand their plasma on "
+                                        "need the ngp xi shape (the last slice's derivative would need the next slab)");
+    auto check_state = [&](const qz_plasma_state* st, const char* what) -> qz_status {
+        if (!st->state) return fail(QZ_ERR_ARG, std::string("qz_sweep_run_stage: null ") + what + " state");
+        if (st->np != s->np || st->npad != s->npad || st->order != s->p.ab_order)
+            return fail(QZ_ERR_ARG, std::string("qz_sweep_run_stage: ") + what + " state of " + std::to_string(st->np) +
+                                        " particles (stride " + std::to_string(st->npad) + ", AB order " +
+                                        std::to_string(st->order) + "), the sweep has " + std::to_string(s->np) +
+                                        " (" + std::to_string(s->npad) + ", " + std::to_string(s->p.ab_order) + ")");
+        return QZ_OK;
+    };
+    SweepExtra x;
+    if (in) {
+        if (qz_status e = check_state(in, "input")) return e;
+        x.pin = in->state;
+        x.pin_pushed = in->pushed ? 1 : 0;
+    }
+    if (out) {
+        if (qz_status e = check_state(out, "output")) return e;
+        x.pout = out->state;
+    }
+    x.bguard = bguard;
+    if (qz_status e = sweep_launch(s, bsrc, fld, diag, cnt, (cudaStream_t)stream, x)) return e;
+    if (out) out->pushed = 1;
+    return QZ_OK;
 }
 
 extern "C" qz_status qz_sweep_plasma(qz_sweep* s, double* out, int cap, int* n) {
@@ -786,12 +847,13 @@ struct qz_sim {
     // exact beam deposits of m = 0 runs (BeamArgs::fx_qe): per-node quantum exponents, the limb split,
     // and the offset of the low limbs behind a (K, M, 5) block of high limbs
     struct Fx {
-        int* d_qe = nullptr;
+        double* d_q = nullptr;           // 2 M: 2^-qe_j (scales), then 2^qe_j (quanta)
         std::vector<int> qe;
         double* d_wmax = nullptr;
         int S = 0;
         long lo = 0;
         bool on = false;
+        bool wanted = true;              // qz_sim_set_exact
     } fx;
     struct Beam {
         double* d = nullptr;     // 7 columns of n (the library's order: sorted by xi cell after a pipelined run)
@@ -841,7 +903,7 @@ struct qz_sim {
         size_t cm_n = 0;
     } pipe;
     ~qz_sim() {
-        if (fx.d_qe) cudaFree(fx.d_qe);
+        if (fx.d_q) cudaFree(fx.d_q);
         if (fx.d_wmax) cudaFree(fx.d_wmax);
         for (auto& b : beams)
             for (void* q : {(void*)b.d, (void*)b.d2, (void*)b.orig, (void*)b.orig2})
@@ -979,8 +1041,10 @@ namespace {
 // deposits exactly; it does for m = 0, while m = 1 runs keep FP64 reductions.
 qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     auto& F = s->fx;
+    const bool was = F.on;
     F.on = false;
-    if (s->p.modes != 0 || s->beams.empty()) return QZ_OK;
+    if (was) s->bsrc_valid = false;             // the format of kept sources changes back to doubles
+    if (!F.wanted || s->p.modes != 0 || s->beams.empty()) return QZ_OK;
     const int M = s->g->M;
     long ntot = 0;
     for (const auto& b : s->beams) ntot += (long)b.n;
@@ -1012,15 +1076,21 @@ qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
         if (bound > 0.0 && std::isfinite(bound)) std::frexp(bound, &e);    // bound < 2^e
         qe[j] = e - B;
     }
-    if (!F.d_qe && cudaMalloc((void**)&F.d_qe, sizeof(int) * M) != cudaSuccess) {
-        F.d_qe = nullptr;
+    if (!F.d_q && cudaMalloc((void**)&F.d_q, sizeof(double) * 2 * M) != cudaSuccess) {
+        F.d_q = nullptr;
         return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");
     }
     if (qe != F.qe || F.S != S) {
-        QZ_CUDA(cudaMemcpyAsync(F.d_qe, qe.data(), sizeof(int) * M, cudaMemcpyHostToDevice, st));
+        std::vector<double> q(2 * (size_t)M);
+        for (int j = 0; j < M; ++j) {
+            q[j] = std::ldexp(1.0, -qe[j]);
+            q[M + j] = std::ldexp(1.0, qe[j]);
+        }
+        QZ_CUDA(cudaMemcpy(F.d_q, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
         F.qe = qe;
         s->bsrc_valid = false;                      // sources kept from the last run used other quanta
     }
+    if (!was) s->bsrc_valid = false;
     F.S = S;
     F.lo = (long)s->p.K * M * s->bnc;
     F.on = true;
@@ -1031,16 +1101,17 @@ qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
 qzb::BeamArgs sim_beam_args(const qz_sim* s, const qz_beam_view* v, const qz_box* box) {
     qzb::BeamArgs B = beam_args(s->g, v, box);
     if (s->fx.on) {
-        B.fx_qe = s->fx.d_qe;
-        B.fx_s = s->fx.S;
+        B.fx_scale = s->fx.d_q;
+        B.fx_inv2s = std::ldexp(1.0, -s->fx.S);
+        B.fx_2s = std::ldexp(1.0, s->fx.S);
         B.fx_lo = s->fx.lo;
     }
     return B;
 }
 
 void sim_sweep_fx(const qz_sim* s, qzb::SweepArgs& A) {
-    A.bqe = s->fx.on ? s->fx.d_qe : nullptr;
-    A.bfx_s = s->fx.S;
+    A.bq = s->fx.on ? s->fx.d_q + s->g->M : nullptr;
+    A.bfx_2s = std::ldexp(1.0, s->fx.S);
     A.bfx_lo = s->fx.lo;
 }
 
@@ -1059,8 +1130,13 @@ qz_status sim_deposit_all(qz_sim* s, double* bsrc, cudaStream_t st) {
 }
 
 qz_status sim_sweep(qz_sim* s, const double* bsrc, cudaStream_t st) {
-    return sweep_launch(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, st, s->fx.on ? s->fx.d_qe : nullptr, s->fx.S,
-                        s->fx.lo);
+    SweepExtra x;
+    if (s->fx.on) {
+        x.bq = s->fx.d_q + s->g->M;
+        x.bfx_2s = std::ldexp(1.0, s->fx.S);
+        x.bfx_lo = s->fx.lo;
+    }
+    return sweep_launch(s->sw, bsrc, s->d_fld, s->d_diag, nullptr, st, x);
 }
 
 // one time step's push of beam b with the deposit into bsrc_next (leapfrog start-up first); rigid
@@ -1336,10 +1412,13 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     QZ_CUDA(cudaStreamSynchronize(st));
     for (int i = 0; i < 3; ++i) QZ_CUDA(cudaEventElapsedTime(&P_.times[i], P_.ev[i], P_.ev[i + 1]));
     s->cnt.lost += h[0];
+    s->cnt.nonfinite += h[1];
+    s->cnt.trapped += h[2];
     s->bsrc_valid = false;
     const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 1};
     std::copy(info, info + 8, P_.info);
     if (err) {
+        s->cnt.giveup += 1;
         static const char* site[] = {"?", "field ring slot", "beam-source rows", "no push task ready"};
         const int w = (err >> 8) & 0xff;
         return fail(QZ_ERR_CUDA, std::string("qz_sim_run: pipeline wait timed out (") + site[w <= 3 ? w : 0] +
@@ -1386,6 +1465,8 @@ qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cud
     QZ_CUDA(cudaMemcpyAsync(h, s->sw->d_cnt, sizeof(h), cudaMemcpyDeviceToHost, st));
     QZ_CUDA(cudaStreamSynchronize(st));
     s->cnt.lost += h[0];
+    s->cnt.nonfinite += h[1];
+    s->cnt.trapped += h[2];
     s->pipe.info[6] = 0;
     return QZ_OK;
 }
@@ -1768,6 +1849,19 @@ extern "C" qz_status qz_sim_adjoint_fn(qz_sim* s, int nsteps, double dt, qz_adjo
 extern "C" qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16) {
     if (!s) return fail(QZ_ERR_ARG, "qz_sim_timing: null pointer");
     return qz_sweep_timing(s->sw, enable, cycles16);
+}
+
+extern "C" qz_status qz_sim_restart(qz_sim* s) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sim_restart: null pointer");
+    for (auto& b : s->beams) b.started = 0;
+    s->bsrc_valid = false;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_set_exact(qz_sim* s, int exact) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sim_set_exact: null pointer");
+    s->fx.wanted = exact != 0;
+    return QZ_OK;
 }
 
 extern "C" qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span,

@@ -46,13 +46,13 @@ __device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restric
             const int jj = j + b;
             double* o = bsrc + ((size_t)kk * B.M + jj) * nc;
             const double d = wi * q * Wk[a] * Wr[b] * B.inv_V[jj] * B.idxi;
-            if (B.fx_qe) {                          // exact (m = 0 runs of qz_sim)
-                const int qe = B.fx_qe[jj];
-                beam_fx_add(o + B_RT0, B.fx_lo, d * omvz, qe, B.fx_s);
-                beam_fx_add(o + B_JZ0, B.fx_lo, d * vz, qe, B.fx_s);
-                beam_fx_add(o + B_JP1R, B.fx_lo, d * vr, qe, B.fx_s);
-                beam_fx_add(o + B_JP1I, B.fx_lo, d * vt, qe, B.fx_s);
-                beam_fx_add(o + B_RHO0, B.fx_lo, d, qe, B.fx_s);
+            if (B.fx_scale) {                       // exact (m = 0 runs of qz_sim)
+                const double sc = B.fx_scale[jj];
+                beam_fx_add(o + B_RT0, B.fx_lo, d * omvz, sc, B.fx_inv2s, B.fx_2s);
+                beam_fx_add(o + B_JZ0, B.fx_lo, d * vz, sc, B.fx_inv2s, B.fx_2s);
+                beam_fx_add(o + B_JP1R, B.fx_lo, d * vr, sc, B.fx_inv2s, B.fx_2s);
+                beam_fx_add(o + B_JP1I, B.fx_lo, d * vt, sc, B.fx_inv2s, B.fx_2s);
+                beam_fx_add(o + B_RHO0, B.fx_lo, d, sc, B.fx_inv2s, B.fx_2s);
                 continue;
             }
             atomicAdd(o + B_RT0, d * omvz);
@@ -132,10 +132,11 @@ __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restri
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             double* o = bsrc + ((size_t)kk * B.M + j + b) * B_NC0;
-            if (B.fx_qe) {
-                const int qe = B.fx_qe[j + b];
+            if (B.fx_scale) {
+                const double sc = B.fx_scale[j + b];
 #pragma unroll
-                for (int c = 0; c < 5; ++c) beam_fx_add(o + c, B.fx_lo, v[(2 * a + b) * 5 + c], qe, B.fx_s);
+                for (int c = 0; c < 5; ++c)
+                    beam_fx_add(o + c, B.fx_lo, v[(2 * a + b) * 5 + c], sc, B.fx_inv2s, B.fx_2s);
             } else {
 #pragma unroll
                 for (int c = 0; c < 5; ++c) atomicAdd(o + c, v[(2 * a + b) * 5 + c]);

@@ -38,7 +38,9 @@ struct SweepArgs {
     int ngp;
     double* fld;                    // (K, M, 6)
     double* diag;                   // (K, M, 3)
-    unsigned long long* counters;   // [0] plasma particles removed
+    // [0] plasma particles removed, [1] deposits with a non-finite contribution (per slice and array),
+    // [2] plasma particles removed as trapped (Delta <= delta_min or gamma > max_qsa Delta)
+    unsigned long long* counters;
     unsigned long long* timing;     // optional: clock cycles per phase [6]
     int dbuf;                       // double-buffered slice sources (push fused with the next deposit)
     int const_smem;                 // per-node constants copied into shared memory
@@ -57,10 +59,20 @@ struct SweepArgs {
     // optional: beam sources that do not change between steps (analytic rigid beams), (K, M, B_NC),
     // added to bsrc wherever the sweep reads it
     const double* bstat;
-    // optional, m = 0: bsrc in the exact two-limb format of the beam deposits (BeamArgs::fx_qe)
-    const int* bqe;
-    int bfx_s;
+    // optional, m = 0: bsrc in the exact two-limb format of the beam deposits (BeamArgs::fx_scale):
+    // bq[j] the quantum of node j, bfx_2s = 2^S
+    const double* bq;
+    double bfx_2s;
     long bfx_lo;
+    // optional, m = 0: one slab of a xi-pipelined run (qz_sweep_run_stage). pin: the plasma entering
+    // the slab's first slice ((6 + 5 ord, npad) like ps; null: the fresh plasma of the box head) and
+    // pin_pushed: whether it has been pushed before (its AB history is filled); bguard: the beam sources
+    // of the slice just ahead of the slab (M x B_NC0 values, null: none); pout: where the plasma goes
+    // after the push of the slab's last slice (null: that slice is not pushed)
+    const double* pin;
+    int pin_pushed;
+    const double* bguard;
+    double* pout;
 };
 
 size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter = false);
@@ -91,11 +103,11 @@ struct BeamArgs {
     double xi_min, dxi, idxi;
     int K, ngp, modes;
     int pusher;                     // 0 vay, 1 boris, 2 hc, 3 imp (stand-alone push kernels only)
-    // exact deposits (m = 0 runs of qz_sim): when fx_qe is set, bsrc holds two 64-bit integer limbs per
-    // value, the high limb where the double would be and the low limb fx_lo doubles further; a
-    // contribution v to node j is t = v / 2^fx_qe[j] split at fx_s bits (beam_fx_add)
-    const int* fx_qe;
-    int fx_s;
+    // exact deposits (m = 0 runs of qz_sim): when fx_scale is set, bsrc holds two 64-bit integer limbs
+    // per value, the high limb where the double would be and the low limb fx_lo doubles further; a
+    // contribution v to node j is t = v fx_scale[j] (a power of two), split at S bits (beam_fx_add)
+    const double* fx_scale;
+    double fx_inv2s, fx_2s;         // 2^-S, 2^S
     long fx_lo;
 };
 

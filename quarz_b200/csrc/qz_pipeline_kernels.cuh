@@ -140,7 +140,7 @@ struct PipeGate {
             const int nr = P->sw.M * P->bnc;
             double* row = const_cast<double*>(g->bsrc) + (size_t)(k - 1) * nr;
             for (int i = threadIdx.x; i < nr; i += kT) __stcg(row + i, 0.0);
-            if (P->sw.bqe)                            // the low limbs of the exact deposits
+            if (P->sw.bq)                            // the low limbs of the exact deposits
                 for (int i = threadIdx.x; i < nr; i += kT) __stcg(row + P->sw.bfx_lo + i, 0.0);
         }
     }
@@ -187,7 +187,7 @@ __device__ __forceinline__ void sweep_role(const PipeArgs& P, double* smem) {
         const int nr = M * P.bnc;
         double* row = P.bsrc + slot * P.bsrc_slot + (size_t)(K - 1) * nr;
         for (int i = tid; i < nr; i += kT) __stcg(row + i, 0.0);
-        if (P.sw.bqe)
+        if (P.sw.bq)
             for (int i = tid; i < nr; i += kT) __stcg(row + P.sw.bfx_lo + i, 0.0);
         __syncthreads();
         if (tid == 0) {
@@ -307,7 +307,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 const double* b0 = bnext + (size_t)c0 * M * P.bnc;
                 const long bl = (long)(c1 - c0 + 1) * M * P.bnc;
                 for (long o = (long)lane * 16; o < bl; o += 32 * 16) prefetch_l2(b0 + o);
-                if (Bb.fx_qe)                            // the low limbs of the exact deposits
+                if (Bb.fx_scale)                            // the low limbs of the exact deposits
                     for (long o = (long)lane * 16; o < bl; o += 32 * 16) prefetch_l2(b0 + Bb.fx_lo + o);
             }
             const long pn = i1 - i0;

@@ -374,14 +374,17 @@ __device__ __forceinline__ int fx_bexp(double v) {         // biased exponent: 0
     return (int)((__double_as_longlong(v) >> 52) & 0x7ff);
 }
 __device__ __forceinline__ int fx_qexp(int e, int bits) { return e - 1085 + bits; }   // (e - 1022) + bits - 63
-__device__ __forceinline__ void fx_add(double* p, double v, int e, int bits) {
-    atomicAdd(reinterpret_cast<unsigned long long*>(p),
-              (unsigned long long)__double2ll_rn(scalbn(v, -fx_qexp(e, bits))));
+// 1 / quantum (0 when every contribution is zero) and the quantum of a block maximum e
+__device__ __forceinline__ double fx_scale(int e, int bits) { return e == 0 ? 0.0 : scalbn(1.0, -fx_qexp(e, bits)); }
+__device__ __forceinline__ double fx_quantum(int e, int bits) { return scalbn(1.0, fx_qexp(e, bits)); }
+__device__ __forceinline__ void fx_add(double* p, double v, double scale) {
+    if (v != 0.0) atomicAdd(reinterpret_cast<unsigned long long*>(p), (unsigned long long)__double2ll_rn(v * scale));
 }
-// the value of an accumulator (its 64 bits as stored in the double slot p)
-__device__ __forceinline__ double fx_value(const double* p, int e, int bits) {
+// the value of an accumulator (its 64 bits as stored in the double slot p); e == 2047: a non-finite
+// contribution was seen
+__device__ __forceinline__ double fx_value(const double* p, int e, double quantum) {
     if (e == 2047) return __longlong_as_double(0x7ff8000000000000LL);
-    return scalbn((double)__double_as_longlong(*p), fx_qexp(e, bits));
+    return (double)__double_as_longlong(*p) * quantum;
 }
 // warp-wide: E[c] = max(E[c], the largest e[c] of the warp's lanes) (shared-memory block maxima)
 template <int NC>
@@ -470,11 +473,11 @@ template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
     const double* bk = bsrc + (size_t)k * st + (size_t)j * B_NC0;
-    // one value of node j: a double, or the exact two-limb accumulator (A.bqe) turned into its value
-    const int qe = A.bqe ? A.bqe[j] : 0;
+    // one value of node j: a double, or the exact two-limb accumulator (A.bq) turned into its value
+    const double qj = A.bq ? A.bq[j] : 0.0;
     auto ld = [&](const double* p) -> double {
-        if (A.bqe) {
-            const double v = beam_fx_value(ldb<kL2>(p), ldb<kL2>(p + A.bfx_lo), qe, A.bfx_s);
+        if (A.bq) {
+            const double v = beam_fx_value(ldb<kL2>(p), ldb<kL2>(p + A.bfx_lo), qj, A.bfx_2s);
             if constexpr (kStat) return A.bstat ? v + __ldg(A.bstat + (p - bsrc)) : v;
             return v;
         }
@@ -485,13 +488,15 @@ __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bs
     r.jz = ld(bk + B_JZ0);
     r.jt = ld(bk + B_JP1I);
     const int K = A.K;
+    // the slice ahead of slice 0: none at the box head, the guard row in a later slab of a staged run
+    const double guard = A.bguard ? A.bguard[(size_t)j * B_NC0 + B_RT0] : 0.0;
     if (A.ngp) {
-        const double prev = (k > 0) ? ld(bk + B_RT0 - (ptrdiff_t)st) : 0.0;
+        const double prev = (k > 0) ? ld(bk + B_RT0 - (ptrdiff_t)st) : guard;
         r.drt = (r.rt - prev) * A.idxi;
     } else if (K == 1) {
         r.drt = 0.0;
     } else if (k == 0) {
-        r.drt = (ld(bk + st + B_RT0) - r.rt) * A.idxi;
+        r.drt = A.bguard ? 0.5 * (ld(bk + st + B_RT0) - guard) * A.idxi : (ld(bk + st + B_RT0) - r.rt) * A.idxi;
     } else if (k == K - 1) {
         r.drt = (r.rt - ld(bk + B_RT0 - (ptrdiff_t)st)) * A.idxi;
     } else {
@@ -786,15 +791,17 @@ __device__ __forceinline__ bool deposit_runs(bool active, int j, bool neg, doubl
 __device__ __forceinline__ void deposit_add(bool tail, int j, bool neg, const double (&v)[12], const Src& acc,
                                             const int* E, int bits) {
     if (!tail) return;
+    const double s0 = fx_scale(E[0], bits), s1 = fx_scale(E[1], bits), s2 = fx_scale(E[2], bits);
+    const double s3 = fx_scale(E[3], bits), s4 = fx_scale(E[neg ? 4 : 5], bits), s6 = fx_scale(E[6], bits);
 #pragma unroll
     for (int cc = 0; cc < 2; ++cc) {
         const int jj = j + cc;
-        fx_add(acc.rhot + jj, v[6 * cc + 0], E[0], bits);
-        fx_add(acc.drho + jj, v[6 * cc + 1], E[1], bits);
-        fx_add(acc.jz + jj, v[6 * cc + 2], E[2], bits);
-        fx_add(acc.chi + jj, v[6 * cc + 3], E[3], bits);
-        fx_add((neg ? acc.ne : acc.ni) + jj, v[6 * cc + 4], E[neg ? 4 : 5], bits);
-        fx_add(acc.jpi1 + jj, v[6 * cc + 5], E[6], bits);
+        fx_add(acc.rhot + jj, v[6 * cc + 0], s0);
+        fx_add(acc.drho + jj, v[6 * cc + 1], s1);
+        fx_add(acc.jz + jj, v[6 * cc + 2], s2);
+        fx_add(acc.chi + jj, v[6 * cc + 3], s3);
+        fx_add((neg ? acc.ne : acc.ni) + jj, v[6 * cc + 4], s4);
+        fx_add(acc.jpi1 + jj, v[6 * cc + 5], s6);
     }
 }
 
@@ -802,7 +809,8 @@ __device__ __forceinline__ void deposit_add(bool tail, int j, bool neg, const do
 __device__ __forceinline__ void deposit_finish(const Src& dst, const Src& acc, int j, const double (&base)[7],
                                                const int* E, int bits) {
 #pragma unroll
-    for (int c = 0; c < 7; ++c) dep_arr(dst, c)[j] = base[c] + fx_value(dep_arr(acc, c) + j, E[c], bits);
+    for (int c = 0; c < 7; ++c)
+        dep_arr(dst, c)[j] = base[c] + fx_value(dep_arr(acc, c) + j, E[c], fx_quantum(E[c], bits));
 }
 
 // src/PlasmaSpecies.cpp:508-559, m = 0: S+ contributions to nodes j (v[0..1]) and j+1 (v[2..3])
@@ -864,21 +872,23 @@ __device__ __forceinline__ bool depositS_runs(bool active, int j, double (&v)[4]
 __device__ __forceinline__ void depositS_add(bool tail, int j, const double (&v)[4], const Src& s, const int* E,
                                              int bits) {
     if (!tail) return;
-    fx_add(s.S1r + j, v[0], E[0], bits);
-    fx_add(s.S1i + j, v[1], E[1], bits);
-    fx_add(s.S1r + j + 1, v[2], E[0], bits);
-    fx_add(s.S1i + j + 1, v[3], E[1], bits);
+    const double sr = fx_scale(E[0], bits), si = fx_scale(E[1], bits);
+    fx_add(s.S1r + j, v[0], sr);
+    fx_add(s.S1i + j, v[1], si);
+    fx_add(s.S1r + j + 1, v[2], sr);
+    fx_add(s.S1i + j + 1, v[3], si);
 }
 
 __device__ __forceinline__ void depositS_finish(const Src& s, int i, const int* E, int bits) {
-    s.S1r[i] = fx_value(s.S1r + i, E[0], bits);
-    s.S1i[i] = fx_value(s.S1i + i, E[1], bits);
+    s.S1r[i] = fx_value(s.S1r + i, E[0], fx_quantum(E[0], bits));
+    s.S1i[i] = fx_value(s.S1i + i, E[1], fx_quantum(E[1], bits));
 }
 
-// src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns false
-// when the particle is removed (trapped or beyond the wall)
+// src/PlasmaSpecies.cpp:561-668 with uniform steps (the classical AB coefficients); returns 1 when the
+// particle moved, 0 when it was removed beyond the wall, -1 when removed as trapped (Delta <= delta_min
+// or gamma > max_qsa Delta: no longer quasi-static, src/PlasmaSpecies.cpp:636-650)
 template <int ORD>
-__device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, const Smem& S, const SweepArgs& A,
+__device__ __forceinline__ int push_particle(PState<ORD>& P, const PGeo& g, const Smem& S, const SweepArgs& A,
                                               bool first) {
     const double qm = P.qm;
     const double X = P.x, Y = P.y, PX = P.px, PY = P.py, D = P.dl;
@@ -922,14 +932,14 @@ __device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, con
     const double gn = (1.0 + pxn * pxn + pyn * pyn + dn * dn) / (2.0 * dn);
     if (!(dn > A.delta_min) || gn > A.max_qsa * dn) {
         P.w = 0.0;
-        return false;
+        return -1;
     }
     const double R = A.R;
     const double rn = sqrt(xn * xn + yn * yn);
     if (rn > R) {                    // specular reflection at the wall, incl. the history
         const double nx = xn / rn, ny = yn / rn;
         const double rr = 2.0 * R - rn;
-        if (rr < 0.0) { P.w = 0.0; return false; }
+        if (rr < 0.0) { P.w = 0.0; return 0; }
         xn = nx * rr; yn = ny * rr;
         const double pn = pxn * nx + pyn * ny;
         pxn -= 2.0 * pn * nx; pyn -= 2.0 * pn * ny;
@@ -942,7 +952,7 @@ __device__ __forceinline__ bool push_particle(PState<ORD>& P, const PGeo& g, con
         }
     }
     P.x = xn; P.y = yn; P.px = pxn; P.py = pyn; P.dl = dn;
-    return true;
+    return 1;
 }
 
 // right-hand sides of the psi, E_z, B_z systems at row i (src/Simulation.cpp:798-799, :517-527)
@@ -1034,12 +1044,16 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     int J = 0;                                             // cell of the thread's particle
     if (REG) {
         if (tid < np) {
-            P.x = A.p_init[tid]; P.y = A.p_init[npad + tid]; P.px = A.p_init[2 * npad + tid];
-            P.py = A.p_init[3 * npad + tid]; P.dl = A.p_init[4 * npad + tid]; P.w = A.p_init[5 * npad + tid];
+            if (A.pin) {                                  // a later slab: the plasma handed on, with its history
+                pload(P, A.pin, npad, tid);
+            } else {
+                P.x = A.p_init[tid]; P.y = A.p_init[npad + tid]; P.px = A.p_init[2 * npad + tid];
+                P.py = A.p_init[3 * npad + tid]; P.dl = A.p_init[4 * npad + tid]; P.w = A.p_init[5 * npad + tid];
 #pragma unroll
-            for (int m = 0; m < ORD; ++m)
+                for (int m = 0; m < ORD; ++m)
 #pragma unroll
-                for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
+                    for (int v = 0; v < 5; ++v) P.h[m][v] = 0.0;
+            }
             species_params(A, tid, P.q, P.qm);
         } else {
             P.x = P.y = P.px = P.py = 0.0;
@@ -1053,9 +1067,13 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         }
     } else {
         for (int p = tid; p < np; p += kThreads) {
+            if (A.pin) {
+                for (int v = 0; v < 6 + 5 * ORD; ++v) gate.ps(A)[(size_t)v * npad + p] = A.pin[(size_t)v * npad + p];
+            } else {
 #pragma unroll
-            for (int v = 0; v < 6; ++v) gate.ps(A)[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
-            for (int v = 0; v < 5 * ORD; ++v) gate.ps(A)[(size_t)(6 + v) * npad + p] = 0.0;
+                for (int v = 0; v < 6; ++v) gate.ps(A)[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
+                for (int v = 0; v < 5 * ORD; ++v) gate.ps(A)[(size_t)(6 + v) * npad + p] = 0.0;
+            }
         }
     }
     __syncthreads();
@@ -1073,10 +1091,11 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             if (pass == 0) {
                 ebg = max(ebg, max(fx_bexp(a0), fx_bexp(a1)));
             } else {
-                fx_add(S.bgt + g.j, a0, S.fx[9], bits_bg);
-                fx_add(S.bgr + g.j, a0, S.fx[9], bits_bg);
-                fx_add(S.bgt + g.j + 1, a1, S.fx[9], bits_bg);
-                fx_add(S.bgr + g.j + 1, a1, S.fx[9], bits_bg);
+                const double sc = fx_scale(S.fx[9], bits_bg);
+                fx_add(S.bgt + g.j, a0, sc);
+                fx_add(S.bgr + g.j, a0, sc);
+                fx_add(S.bgt + g.j + 1, a1, sc);
+                fx_add(S.bgr + g.j + 1, a1, sc);
             }
         }
         if (A.neutralize)
@@ -1090,8 +1109,9 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 if (pass == 0) {
                     ene = max(ene, max(fx_bexp(a0), fx_bexp(a1)));
                 } else {
-                    fx_add(ne0 + g.j, a0, S.fx[10], bits_p);
-                    fx_add(ne0 + g.j + 1, a1, S.fx[10], bits_p);
+                    const double sc = fx_scale(S.fx[10], bits_p);
+                    fx_add(ne0 + g.j, a0, sc);
+                    fx_add(ne0 + g.j + 1, a1, sc);
                 }
             }
         if (pass == 0) {
@@ -1101,9 +1121,10 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         __syncthreads();
     }
     for (int j = tid; j < M; j += kThreads) {
-        S.bgt[j] = fx_value(S.bgt + j, S.fx[9], bits_bg);
-        S.bgr[j] = fx_value(S.bgr + j, S.fx[9], bits_bg);
-        ne0[j] = fx_value(ne0 + j, S.fx[10], bits_p);
+        const double qb = fx_quantum(S.fx[9], bits_bg), qn = fx_quantum(S.fx[10], bits_p);
+        S.bgt[j] = fx_value(S.bgt + j, S.fx[9], qb);
+        S.bgr[j] = fx_value(S.bgr + j, S.fx[9], qb);
+        ne0[j] = fx_value(ne0 + j, S.fx[10], qn);
     }
     if (Gate::kActive && tid < 32) {                     // warp 0 checks the beam-source rows
         const bool ok = gate.before_rows(K - 1 < 2 ? K - 1 : 2);
@@ -1185,6 +1206,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             }
         }
         __syncthreads();
+        if (tid == 0)
+            for (int c = 0; c < 7; ++c) S.fx[13] += (S.fx[c] == 2047) + (c < 2 && S.fx[9 + c] == 2047);
         for (int j = tid; j < M; j += kThreads) {
             double b0[7];
             init_base<EXT>(S, j, beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), 0, j), M, b0);
@@ -1358,6 +1381,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         __syncthreads();
         PHASE_MARK(2);
         // this thread's rows of S+ into values: the only rows its B+ rows (and the filter) read
+        if (tid == 0) S.fx[13] += (S.fx[7] == 2047) + (S.fx[8] == 2047);
 #pragma unroll
         for (int u = 0; u < kMaxR; ++u)
             if (u < Rw && row0 + u < M) depositS_finish(s, row0 + u, S.fx + 7, bits_p);
@@ -1495,18 +1519,20 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
 #pragma unroll
                 for (int u = 0; u < kMaxR; ++u)
                     if (u < Rw && row0 + u < M) nxt[u] = beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u);
-            const bool first = (k == 0);
+            const bool first = (k == 0) && !A.pin_pushed;
             if (REG) {
                 bool act = tid < np && P.w != 0.0;
                 double v[12];
                 if (act) {
-                    if (push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first)) {
+                    const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first);
+                    if (pr > 0) {
                         const double rn = sqrt(P.x * P.x + P.y * P.y);
                         J = locate_from(S.r, N, R, rn, J);
                         deposit_values(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, v);
                     } else {
                         act = false;
                         atomicAdd(S.lost, 1);
+                        if (pr < 0) atomicAdd(S.fx + 12, 1);
                     }
                 }
                 const bool tail = deposit_runs<true>(act, J, P.q < 0.0, v, S.fx);
@@ -1529,13 +1555,15 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                             if (Q.w != 0.0) {
                                 if (pass == 0) {
                                     const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                                    if (push_particle(Q, g, S, A, first)) {
+                                    const int pr = push_particle(Q, g, S, A, first);
+                                    if (pr > 0) {
                                         const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
                                         j = g2.j;
                                         deposit_values(Q, g2, S, v);
                                         act = true;
                                     } else {
                                         atomicAdd(S.lost, 1);
+                                        if (pr < 0) atomicAdd(S.fx + 12, 1);
                                     }
                                     pstore(Q, gate.ps(A), npad, p);
                                 } else {
@@ -1557,6 +1585,8 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 }
             }
             __syncthreads();
+            if (tid == 0)
+                for (int c = 0; c < 7; ++c) S.fx[13] += S.fx[c] == 2047;
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u) {
                 const int i = row0 + u;
@@ -1586,8 +1616,37 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             if (!*S.flag) return false;
         }
     }
+    if (A.pout) {
+        // a slab that hands its plasma on: push the last slice too (src/Simulation.cpp:755, the push of the
+        // last local slice produces the state entering the next slab), no deposit
+        const bool first = (K == 1) && !A.pin_pushed;
+        if (REG) {
+            if (tid < np && P.w != 0.0) {
+                const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first);
+                if (pr <= 0) { atomicAdd(S.lost, 1); if (pr < 0) atomicAdd(S.fx + 12, 1); }
+            }
+            if (tid < np) pstore(P, A.pout, npad, tid);
+        } else {
+            for (int p = tid; p < np; p += kThreads) {
+                PState<ORD> Q;
+                pload(Q, gate.ps(A), npad, p);
+                species_params(A, p, Q.q, Q.qm);
+                if (Q.w != 0.0) {
+                    const int pr = push_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), S, A, first);
+                    if (pr <= 0) { atomicAdd(S.lost, 1); if (pr < 0) atomicAdd(S.fx + 12, 1); }
+                }
+                pstore(Q, gate.ps(A), npad, p);
+                pstore(Q, A.pout, npad, p);
+            }
+        }
+        __syncthreads();
+    }
     if (REG && tid < np) pstore(P, gate.ps(A), npad, tid);
-    if (tid == 0 && A.counters) atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
+    if (tid == 0 && A.counters) {
+        atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
+        if (S.fx[13]) atomicAdd(&A.counters[1], (unsigned long long)S.fx[13]);
+        if (S.fx[12]) atomicAdd(&A.counters[2], (unsigned long long)S.fx[12]);
+    }
     return true;
 #undef PHASE_MARK
 #undef SUB_MARK
