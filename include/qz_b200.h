@@ -81,6 +81,10 @@ typedef struct {
     int nspecies;
     qz_species species[4];
     double smooth_length;    /* plasma.smooth_length (0: off) */
+    double max_cells_per_step; /* pusher.max_cells_per_step: adaptive sub-slicing with variable-step AB
+                                  (src/Simulation.cpp:755-781, :837-847; 0: off); modes = 0, without the
+                                  smoothing filter, not in stages or the adjoint */
+    int substep_max;         /* pusher.substep_max (0: the reference's default, 64) */
 } qz_sweep_params;
 
 typedef struct {
@@ -90,6 +94,8 @@ typedef struct {
                                      array's values of that slice are NaN */
     unsigned long long trapped;   /* of lost: removed as trapped (Delta <= delta_min or gamma > max_qsa Delta) */
     unsigned long long giveup;    /* pipelined runs that ended because a bounded wait timed out */
+    unsigned long long subslices; /* sub-slices beyond the regular slices (adaptive sub-slicing; the
+                                     reference's "extra sub-slices", src/Simulation.cpp:782) */
 } qz_counters;
 
 typedef struct qz_sweep qz_sweep;

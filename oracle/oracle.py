@@ -31,7 +31,8 @@ def build(omp: bool = False) -> str:
 class _Params(C.Structure):
     _fields_ = [("modes", C.c_int), ("picard", C.c_int), ("ab_order", C.c_int), ("delta_min", C.c_double),
                 ("max_qsa", C.c_double), ("xi_min", C.c_double), ("dxi", C.c_double), ("K", C.c_int),
-                ("ngp", C.c_int), ("tridiag", C.c_int), ("neutralize", C.c_int), ("smooth_length", C.c_double)]
+                ("ngp", C.c_int), ("tridiag", C.c_int), ("neutralize", C.c_int), ("smooth_length", C.c_double),
+                ("max_cells", C.c_double), ("substep_max", C.c_int)]
 
 
 class _SpParams(C.Structure):
@@ -77,6 +78,8 @@ def lib():
             getattr(L, f).restype = dp
         L.qzo_sim_lost.argtypes = [C.c_void_p]
         L.qzo_sim_lost.restype = C.c_long
+        L.qzo_sim_subslices.argtypes = [C.c_void_p]
+        L.qzo_sim_subslices.restype = C.c_long
         L.qzo_sim_plasma_get.argtypes = [C.c_void_p, C.c_int, dp, C.c_int]
         L.qzo_sim_run.argtypes = [C.c_void_p, C.c_int, C.c_double, dp]
         L.qzo_sim_deposit_beams.argtypes = [C.c_void_p]
@@ -276,7 +279,8 @@ class OracleSim:
         p = _Params(modes=spec.modes, picard=spec.picard, ab_order=spec.ab_order, delta_min=spec.delta_min,
                     max_qsa=spec.max_qsa, xi_min=spec.xi_min, dxi=spec.dxi, K=spec.K, ngp=1 if spec.ngp else 0,
                     tridiag=_METHODS[tridiag or spec.tridiag], neutralize=1 if spec.neutralize else 0,
-                    smooth_length=getattr(spec, "smooth_length", 0.0))
+                    smooth_length=getattr(spec, "smooth_length", 0.0),
+                    max_cells=getattr(spec, "max_cells", 0.0), substep_max=getattr(spec, "substep_max", 64))
         self._nodes = _c(spec.nodes)
         self.h = lib().qzo_sim_create(C.byref(p), _p(self._nodes), len(self._nodes))
         if not self.h:
@@ -365,6 +369,10 @@ class OracleSim:
 
     def lost(self):
         return int(lib().qzo_sim_lost(self.h))
+
+    def subslices(self):
+        """Sub-slices beyond the regular slices so far (adaptive sub-slicing)."""
+        return int(lib().qzo_sim_subslices(self.h))
 
     def beam(self, b):
         n = lib().qzo_sim_beam_count(self.h, b)

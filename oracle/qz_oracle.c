@@ -724,6 +724,7 @@ struct qzo_sim {
     double *fld, *bsrc, *diag;
     int fnc, bnc, dnc;
     long lost;
+    long nsub_extra;       /* sub-slices beyond the regular slices, all sweeps */
     double* pool;
     /* optional (the adjoint's recomputation): the mobile species' state at the start of every
        slice, (K, 6 + 5 * ab_order, cap) -- x y px py dl w, then the AB history */
@@ -1205,6 +1206,51 @@ static void species_push(qzo_sim* s, species_t* q, double dxi) {
     }
 }
 
+/* src/PlasmaSpecies.cpp:814-830: the most radial cells a particle would cross in a step of dxi, its
+   straight path's length over the cell size at the path's closest approach to the axis */
+static double species_max_cells(const qzo_sim* s, const species_t* q, double dxi) {
+    if (!q->p.mobile || q->Np == 0) return 0.0;
+    const grid_t* g = &s->fs.g;
+    double mx = 0.0;
+    for (int i = 0; i < q->Np; ++i) {
+        if (q->w[i] == 0.0) continue;
+        const double X = q->x[i], Y = q->y[i], D = q->dl[i];
+        const double X1 = X + dxi * q->px[i] / D, Y1 = Y + dxi * q->py[i] / D;
+        const double dx = X1 - X, dy = Y1 - Y, l2 = dx * dx + dy * dy;
+        double t = l2 > 0.0 ? -(X * dx + Y * dy) / l2 : 0.0;
+        t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+        const double xm = X + t * dx, ym = Y + t * dy;
+        const double c = sqrt(l2) * g->inv_h[grid_locate(g, sqrt(xm * xm + ym * ym))];
+        if (c > mx) mx = c;
+    }
+    return mx;
+}
+
+/* src/PlasmaSpecies.hpp:63: the last push's step */
+static double species_last_step(const qzo_sim* s, const species_t* q) {
+    const int ord = s->p.ab_order;
+    return q->npush > 0 ? q->xi_cur - q->xi_slot[(q->npush - 1) % ord] : 0.0;
+}
+
+/* src/Simulation.cpp:837-847: sub-slices of the coming step */
+static int subslices(const qzo_sim* s, double dxi) {
+    if (!(s->p.max_cells > 0.0)) return 1;
+    double c = 0.0, hlast = 0.0;
+    for (int i = 0; i < s->nsp; ++i)
+        if (s->sp[i].p.mobile) {
+            const double ci = species_max_cells(s, &s->sp[i], dxi), hi = species_last_step(s, &s->sp[i]);
+            if (ci > c) c = ci;
+            if (hi > hlast) hlast = hi;
+        }
+    int n = c <= s->p.max_cells ? 1 : (int)ceil(c / s->p.max_cells);
+    if (hlast > 0.0) {
+        const int m = (int)ceil(dxi / (2.0 * hlast) - 1e-9);
+        if (m > n) n = m;
+    }
+    const int nmax = s->p.substep_max > 0 ? s->p.substep_max : 64;
+    return n < nmax ? n : nmax;
+}
+
 /* ---- slice steps (src/Simulation.cpp) ---- */
 static void zero_sources(qzo_sim* s) {
     const int M = s->M;
@@ -1215,16 +1261,18 @@ static void zero_sources(qzo_sim* s) {
 }
 
 #define BS(k, j, c) s->bsrc[((size_t)(k) * M + (j)) * bnc + (c)]
-static void combine_sources(qzo_sim* s, int k) {
+/* src/Simulation.cpp:408-457; ds != 0 (a sub-slice at xi_k + ds): the beam sources extrapolated linearly
+   with their xi-derivative */
+static void combine_sources(qzo_sim* s, int k, double ds) {
     const int M = s->M, KL = s->p.K, bnc = s->bnc;
     const double idxi = 1.0 / s->p.dxi;
-    const int m1 = s->m1, ngp = s->p.ngp;
+    const int m1 = s->m1, ngp = s->p.ngp, sub = ds != 0.0;
     for (int j = 0; j < M; ++j) {
 #define DXI_B(comp) ( ngp ? (BS(k, j, comp) - ((k > 0) ? BS(k - 1, j, comp) : s->bguard[15 * j + (comp)])) * idxi \
             : (KL == 1 ? 0.0 : (k == 0 ? (BS(1, j, comp) - BS(0, j, comp)) * idxi \
             : (k == KL - 1 ? (BS(KL - 1, j, comp) - BS(KL - 2, j, comp)) * idxi \
             : 0.5 * (BS(k + 1, j, comp) - BS(k - 1, j, comp)) * idxi))) )
-#define BV(comp) BS(k, j, comp)
+#define BV(comp) (sub ? BS(k, j, comp) + ds * DXI_B(comp) : BS(k, j, comp))
         s->rhot.a0[j] += s->bg_rhot.a0[j] + BV(B_RT0);
         s->drho.a0[j] += DXI_B(B_RT0);
         s->jz.a0[j] += BV(B_JZ0);
@@ -1613,15 +1661,33 @@ int qzo_sim_step_fields(qzo_sim* s, double t) {
         for (int i = 0; i < s->nsp; ++i)
             if (s->sp[i].p.mobile) species_deposit(s, &s->sp[i]);
         filter_plasma_sources(s);
-        combine_sources(s, k);
+        combine_sources(s, k, 0.0);
         solve_slice_fields(s);
         store_slice(s, k);
-        if (k < K - 1)
-            for (int i = 0; i < s->nsp; ++i)
-                if (s->sp[i].p.mobile) species_push(s, &s->sp[i], dxi);
+        if (k < K - 1) {
+            /* src/Simulation.cpp:755-781: adaptive sub-slicing, each sub-slice with its own deposit and
+               field solve (the beam sources extrapolated from this slice); only the slices are stored */
+            const int nsub = subslices(s, dxi);
+            const double h = dxi / nsub;
+            for (int ss = 0; ss < nsub; ++ss) {
+                if (ss > 0) {
+                    zero_sources(s);
+                    for (int i = 0; i < s->nsp; ++i)
+                        if (s->sp[i].p.mobile) species_deposit(s, &s->sp[i]);
+                    filter_plasma_sources(s);
+                    combine_sources(s, k, ss * h);
+                    solve_slice_fields(s);
+                }
+                for (int i = 0; i < s->nsp; ++i)
+                    if (s->sp[i].p.mobile) species_push(s, &s->sp[i], h);
+            }
+            s->nsub_extra += nsub - 1;
+        }
     }
     return 0;
 }
+
+long qzo_sim_subslices(const qzo_sim* s) { return s->nsub_extra; }
 
 /* src/Beam.cpp:900-905 */
 int qzo_sim_push_beams(qzo_sim* s, double dt_kick, double dt_drift) {

@@ -80,6 +80,8 @@ typedef struct {
     int tridiag;          /* QZO_THOMAS / PCR / PARTITION */
     int neutralize;
     double smooth_length; /* plasma.smooth_length: radial smoothing of the plasma sources (0: off) */
+    double max_cells;     /* pusher.max_cells_per_step: adaptive sub-slicing (0: off) */
+    int substep_max;      /* pusher.substep_max */
 } qzo_params;
 
 typedef struct {
@@ -120,6 +122,8 @@ int      qzo_filter(const double* nodes, int M, double a2, int n, double* f);
 /* e^{-z} I0(z), e^{-z} I1(z) by the polynomial approximations of Abramowitz & Stegun 9.8.1-9.8.4 */
 void     qzo_bessel_i01_scaled(double z, double* i0, double* i1);
 /* one quasi-static sweep (beam deposit + plasma load + sweep), as Simulation::step_fields */
+/* sub-slices beyond the regular slices so far (adaptive sub-slicing) */
+long     qzo_sim_subslices(const qzo_sim* s);
 int      qzo_sim_step_fields(qzo_sim* s, double t);
 /* beam push of every non-rigid beam */
 int      qzo_sim_push_beams(qzo_sim* s, double dt_kick, double dt_drift);

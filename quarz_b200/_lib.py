@@ -26,12 +26,12 @@ class SweepParams(C.Structure):
     _fields_ = [("modes", C.c_int), ("picard", C.c_int), ("ab_order", C.c_int), ("delta_min", C.c_double),
                 ("max_qsa", C.c_double), ("xi_min", C.c_double), ("dxi", C.c_double), ("K", C.c_int),
                 ("ngp", C.c_int), ("neutralize", C.c_int), ("nspecies", C.c_int), ("species", Species * 4),
-                ("smooth_length", C.c_double)]
+                ("smooth_length", C.c_double), ("max_cells_per_step", C.c_double), ("substep_max", C.c_int)]
 
 
 class Counters(C.Structure):
     _fields_ = [("lost", C.c_ulonglong), ("nonfinite", C.c_ulonglong), ("trapped", C.c_ulonglong),
-                ("giveup", C.c_ulonglong)]
+                ("giveup", C.c_ulonglong), ("subslices", C.c_ulonglong)]
 
 
 class PlasmaState(C.Structure):

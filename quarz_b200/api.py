@@ -82,6 +82,8 @@ def sweep_params(spec: "_deck.RunSpec") -> SweepParams:
     p.ngp = 1 if spec.ngp else 0
     p.neutralize = 1 if spec.neutralize else 0
     p.smooth_length = float(getattr(spec, "smooth_length", 0.0))
+    p.max_cells_per_step = float(getattr(spec, "max_cells", 0.0))
+    p.substep_max = int(getattr(spec, "substep_max", 64))
     if len(spec.species) > 4:
         raise QZError(1, "at most 4 plasma species")
     p.nspecies = len(spec.species)
@@ -106,6 +108,8 @@ class Sweep:
     def run(self, bsrc, fld, diag, stream=None) -> int:
         cnt = Counters()
         check(lib().qz_sweep_run(self.h, _dev(bsrc), _dev(fld), _dev(diag), C.byref(cnt), _stream_ptr(stream)))
+        self.last_counters = {"lost": int(cnt.lost), "nonfinite": int(cnt.nonfinite), "trapped": int(cnt.trapped),
+                              "subslices": int(cnt.subslices)}
         return int(cnt.lost)
 
     def run_async(self, bsrc, fld, diag, stream=None) -> None:
@@ -145,7 +149,8 @@ class Sweep:
                                        C.byref(sout) if sout is not None else None, C.byref(cnt), _stream_ptr(stream)))
         if state_out is not None:
             state_out.pushed = True
-        return {"lost": int(cnt.lost), "nonfinite": int(cnt.nonfinite), "trapped": int(cnt.trapped)}
+        return {"lost": int(cnt.lost), "nonfinite": int(cnt.nonfinite), "trapped": int(cnt.trapped),
+                "subslices": int(cnt.subslices)}
 
     def plasma(self) -> np.ndarray:
         cap = 1 << 22
@@ -495,7 +500,8 @@ class Simulation:
         contribution, pipelined runs that gave up on a wait."""
         c = Counters()
         check(lib().qz_sim_counters(self.h, C.byref(c)))
-        return {"lost": int(c.lost), "nonfinite": int(c.nonfinite), "trapped": int(c.trapped), "giveup": int(c.giveup)}
+        return {"lost": int(c.lost), "nonfinite": int(c.nonfinite), "trapped": int(c.trapped), "giveup": int(c.giveup),
+                "subslices": int(c.subslices)}
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -343,6 +343,11 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     for (int i = 0; i < 4 && lay < 0; ++i)
         if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1], filter) <= (size_t)optin) lay = i;
     const int rpt = (M + qzb::kSweepThreads - 1) / qzb::kSweepThreads;
+    if (!(p->max_cells_per_step >= 0.0) || p->substep_max < 0)
+        return fail(QZ_ERR_ARG, "qz_sweep_create: pusher.max_cells_per_step must be >= 0 and substep_max >= 1");
+    if (p->max_cells_per_step > 0.0 && (p->modes != 0 || p->smooth_length > 0.0))
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_create: adaptive sub-slicing (pusher.max_cells_per_step) runs with "
+                                        "modes = 0 and without plasma.smooth_length");
     if (p->modes == 1 && (M > qzb::kSweepThreads || qzb::sweep_m1_smem_bytes(M) > (size_t)optin))
         return fail(QZ_ERR_SIZE, "qz_sweep_create: the modes = 1 sweep holds one radial node per thread: M = " +
                                      std::to_string(M) + " > " + std::to_string(qzb::kSweepThreads));
@@ -422,6 +427,8 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     for (int m = 0; m < 5; ++m) A.ab[m] = AB[p->ab_order - 1][m];
     A.delta_min = p->delta_min;
     A.max_qsa = p->max_qsa;
+    A.max_cells = p->max_cells_per_step;
+    A.substep_max = p->substep_max > 0 ? p->substep_max : 64;
     A.p_init = s->d_pinit;
     A.nbg = s->nbg;
     A.bg_p = s->d_bg;
@@ -470,6 +477,7 @@ struct SweepExtra {
     int pin_pushed = 0;
     const double* bguard = nullptr;
     double* pout = nullptr;
+    bool accumulate = false;          // add to the sweep's device counters (a run's sweeps), do not clear them
 };
 
 // one sweep of s over bsrc
@@ -486,7 +494,7 @@ qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* dia
     A.pin_pushed = x.pin_pushed;
     A.bguard = x.bguard;
     A.pout = x.pout;
-    QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
+    if (!x.accumulate) QZ_CUDA(cudaMemsetAsync(s->d_cnt, 0, sizeof(unsigned long long) * 4, st));
     if (s->timing) {
         QZ_CUDA(cudaMemsetAsync(s->d_tim, 0, sizeof(unsigned long long) * 16, st));
         A.timing = s->d_tim;
@@ -499,6 +507,7 @@ qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* dia
         cnt->lost += h[0];
         cnt->nonfinite += h[1];
         cnt->trapped += h[2];
+        cnt->subslices += h[3];
     }
     return QZ_OK;
 }
@@ -523,8 +532,9 @@ extern "C" qz_status qz_sweep_run_stage(qz_sweep* s, const double* bsrc, const d
                                         qz_counters* cnt, void* stream) {
     if (!s || !bsrc || !fld || !diag) return fail(QZ_ERR_ARG, "qz_sweep_run_stage: null pointer");
     if (s->p.modes != 0) return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: modes = 0 sweeps only");
-    if (s->base.filter || s->base.bstat)
-        return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: no smoothing filter or static beam sources in a stage");
+    if (s->base.filter || s->base.bstat || s->base.max_cells > 0.0)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: no smoothing filter, static beam sources or adaptive "
+                                        "sub-slicing in a stage");
     if ((bguard || out) && !s->p.ngp)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_run_stage: slabs that take a guard row or hand their plasma on "
                                         "need the ngp xi shape (the last slice's derivative would need the next slab)");
@@ -1129,8 +1139,10 @@ qz_status sim_deposit_all(qz_sim* s, double* bsrc, cudaStream_t st) {
     return QZ_OK;
 }
 
+// one sweep of a run; its counters add to the sweep's device counters, which the run clears at its start
 qz_status sim_sweep(qz_sim* s, const double* bsrc, cudaStream_t st) {
     SweepExtra x;
+    x.accumulate = true;
     if (s->fx.on) {
         x.bq = s->fx.d_q + s->g->M;
         x.bfx_2s = std::ldexp(1.0, s->fx.S);
@@ -1414,6 +1426,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     s->cnt.lost += h[0];
     s->cnt.nonfinite += h[1];
     s->cnt.trapped += h[2];
+    s->cnt.subslices += h[3];
     s->bsrc_valid = false;
     const int info[8] = {g1, nsweep, g1 - nsweep, ring, nbk, bk, 1, P_.span > 0 ? P_.span : 1};
     std::copy(info, info + 8, P_.info);
@@ -1435,6 +1448,7 @@ qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cud
     void* stream = (void*)st;
     const int nb = (int)s->beams.size();
     if (qz_status e = fx_prepare(s, st)) return e;
+    QZ_CUDA(cudaMemsetAsync(s->sw->d_cnt, 0, sizeof(unsigned long long) * 4, st));   // the run's counters
     if (!s->bsrc_valid) {
         if (qz_status e = sim_deposit_all(s, s->d_bsrc[s->cur], st)) return e;
         s->bsrc_valid = true;
@@ -1467,6 +1481,7 @@ qz_status run_sequential(qz_sim* s, int nsteps, double dt, double* mom_host, cud
     s->cnt.lost += h[0];
     s->cnt.nonfinite += h[1];
     s->cnt.trapped += h[2];
+    s->cnt.subslices += h[3];
     s->pipe.info[6] = 0;
     return QZ_OK;
 }
@@ -1670,8 +1685,9 @@ qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, dou
     if (!s || nsteps < 1 || !(dt > 0.0) || (!seed.fixed && !seed.fn) || (!s->beams.empty() && !lam_host))
         return fail(QZ_ERR_ARG, "qz_sim_adjoint: bad argument");
     const qzb::SweepArgs& base = s->sw->base;
-    if (s->p.modes != 0 || s->p.ngp || s->p.K < 2)
-        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2");
+    if (s->p.modes != 0 || s->p.ngp || s->p.K < 2 || base.max_cells > 0.0)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2, "
+                                        "without adaptive sub-slicing");
     if (base.M > qzb::kSweepThreads || base.np > qzb::kSweepThreads || base.nsp != 1)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
                                         "particles per slice");
@@ -2097,6 +2113,7 @@ extern "C" qz_status qz_sim_step_host(qz_sim* s, double* const* cols, double dt_
         s->beams[b].orig_identity = true;
     }
     if (qz_status e = fx_prepare(s, st)) return e;
+    QZ_CUDA(cudaMemsetAsync(s->sw->d_cnt, 0, sizeof(unsigned long long) * 4, st));
     if (qz_status e = sim_deposit_all(s, s->d_bsrc[s->cur], st)) return e;
     if (qz_status e = sim_sweep(s, s->d_bsrc[s->cur], st)) return e;
     for (int b = 0; b < nb; ++b) {

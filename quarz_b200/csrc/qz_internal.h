@@ -29,6 +29,8 @@ struct SweepArgs {
     int ord;                        // Adams-Bashforth order
     double ab[5];                   // its coefficients (uniform steps)
     double delta_min, max_qsa;
+    double max_cells;               // pusher.max_cells_per_step: adaptive sub-slicing (0: off), m = 0
+    int substep_max;                // pusher.substep_max
     const double* p_init;           // fresh plasma at the head: (6, npad) x y px py Delta w
     int nbg;                        // immobile particles (background)
     const double* bg_p;             // (3, nbg): x, y, w*q
@@ -39,7 +41,8 @@ struct SweepArgs {
     double* fld;                    // (K, M, 6)
     double* diag;                   // (K, M, 3)
     // [0] plasma particles removed, [1] deposits with a non-finite contribution (per slice and array),
-    // [2] plasma particles removed as trapped (Delta <= delta_min or gamma > max_qsa Delta)
+    // [2] plasma particles removed as trapped (Delta <= delta_min or gamma > max_qsa Delta), [3] sub-slices
+    // beyond the regular slices (adaptive sub-slicing)
     unsigned long long* counters;
     unsigned long long* timing;     // optional: clock cycles per phase [6]
     int dbuf;                       // double-buffered slice sources (push fused with the next deposit)

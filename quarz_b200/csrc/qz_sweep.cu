@@ -16,7 +16,7 @@ size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter) {
     size_t d = (size_t)(3 + 2 + 6 + (dbuf ? 18 : 9)) * M + 2 * 8 * (kSweepThreads / 32);
     if (const_smem) d += 13 * (size_t)M;
     if (filter) d += 4 * (size_t)M + 2 * 14 * (kSweepThreads / 32);
-    return sizeof(double) * d + 16 + 4 * 16;       // + the int words: lost, flag, 14 exponent maxima
+    return sizeof(double) * d + 16 + 4 * 16;       // + lost, flag, 14 exponent maxima and counters, the cells-crossed word
 }
 
 namespace {

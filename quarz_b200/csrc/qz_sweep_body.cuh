@@ -417,8 +417,10 @@ struct Smem {
     int* lost;
     int* flag;                                            // gate result broadcast
     // block maxima of the deposits' exponents: [0, 7) the plasma deposit (rho - J_z, d/dxi, J_z, chi,
-    // n_e, n_i, J_theta), [7, 9) the S deposit, [9, 12) the background and neutralising deposits
+    // n_e, n_i, J_theta), [7, 9) the S deposit, [9, 11) the background and neutralising deposits; then
+    // counters: [11] extra sub-slices, [12] particles removed as trapped, [13] non-finite deposits
     int* fx;
+    unsigned long long* cmax;                             // most cells crossed (sub-slicing), as double bits
 };
 
 __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
@@ -442,6 +444,7 @@ __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
     S.lost = reinterpret_cast<int*>(p);
     S.flag = S.lost + 1;
     S.fx = S.lost + 2;
+    S.cmax = reinterpret_cast<unsigned long long*>(S.lost + 16);
     return S;
 }
 
@@ -889,7 +892,7 @@ __device__ __forceinline__ void depositS_finish(const Src& s, int i, const int* 
 // or gamma > max_qsa Delta: no longer quasi-static, src/PlasmaSpecies.cpp:636-650)
 template <int ORD>
 __device__ __forceinline__ int push_particle(PState<ORD>& P, const PGeo& g, const Smem& S, const SweepArgs& A,
-                                              bool first) {
+                                              bool first, const double (&ab)[5], double h) {
     const double qm = P.qm;
     const double X = P.x, Y = P.y, PX = P.px, PY = P.py, D = P.dl;
     const double r1 = w1_at(S, A.N, g);
@@ -921,11 +924,11 @@ __device__ __forceinline__ int push_particle(PState<ORD>& P, const PGeo& g, cons
     double sum[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int m = 0; m < ORD; ++m) {
-        const double cm = A.ab[m];
+        const double cm = ab[m];
 #pragma unroll
         for (int v = 0; v < 5; ++v) sum[v] += cm * P.h[m][v];
     }
-    const double dxi = A.dxi;
+    const double dxi = h;
     double xn = X + dxi * sum[0], yn = Y + dxi * sum[1];
     double pxn = PX + dxi * sum[2], pyn = PY + dxi * sum[3];
     const double dn = D + dxi * sum[4];
@@ -953,6 +956,70 @@ __device__ __forceinline__ int push_particle(PState<ORD>& P, const PGeo& g, cons
     }
     P.x = xn; P.y = yn; P.px = pxn; P.py = pyn; P.dl = dn;
     return 1;
+}
+
+// Adams-Bashforth coefficients for history points t[0..ord) (t[0] the newest push) and the step h: the
+// integrals over [t0, t0 + h] of the Lagrange basis, by 3-point Gauss-Legendre (exact for the degree <= 4
+// needed), src/PlasmaSpecies.cpp:30-48
+template <int ORD>
+__device__ __forceinline__ void ab_variable(const double (&t)[ORD], double h, double (&c)[5]) {
+    const double gx[3] = {-0.7745966692414834, 0.0, 0.7745966692414834};
+    const double gw[3] = {5.0 / 9.0, 8.0 / 9.0, 5.0 / 9.0};
+#pragma unroll
+    for (int m = 0; m < 5; ++m) c[m] = 0.0;
+#pragma unroll
+    for (int m = 0; m < ORD; ++m) {
+        double sm = 0.0;
+#pragma unroll
+        for (int q = 0; q < 3; ++q) {
+            const double tt = t[0] + 0.5 * h * (1.0 + gx[q]);
+            double l = 1.0;
+#pragma unroll
+            for (int n = 0; n < ORD; ++n)
+                if (n != m) l *= (tt - t[n]) / (t[m] - t[n]);
+            sm += 0.5 * gw[q] * l;
+        }
+        c[m] = sm;
+    }
+}
+
+// the radial cells a particle would cross in a step of dxi: its straight path's length over the cell
+// size at the path's closest approach to the axis (src/PlasmaSpecies.cpp:814-830)
+__device__ __forceinline__ double cells_crossed(const Smem& S, int N, double R, double X, double Y, double PX,
+                                                double PY, double D, double dxi) {
+    const double X1 = X + dxi * PX / D, Y1 = Y + dxi * PY / D;
+    const double dx = X1 - X, dy = Y1 - Y, l2 = dx * dx + dy * dy;
+    double t = l2 > 0.0 ? -(X * dx + Y * dy) / l2 : 0.0;
+    t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    const double xm = X + t * dx, ym = Y + t * dy;
+    return sqrt(l2) * S.ih[locate(S.r, N, R, sqrt(xm * xm + ym * ym))];
+}
+
+// the beam sources of a sub-slice at xi_k + ds: slice k's, extrapolated linearly with their xi-derivative
+// (src/Simulation.cpp:431-432); the derivative of rho - J_z itself is slice k's
+template <bool kL2, bool kStat>
+__device__ __forceinline__ BeamRow beam_row_at(const SweepArgs& A, const double* bsrc, int k, int j, double ds) {
+    BeamRow r = beam_row<kL2, kStat>(A, bsrc, k, j);
+    if (ds == 0.0) return r;
+    // the xi-derivatives of J_z and J_theta by the same difference as that of rho - J_z
+    const int K = A.K;
+    auto row = [&](int kk) { return beam_row<kL2, kStat>(A, bsrc, kk, j); };
+    double djz = 0.0, djt = 0.0;
+    if (A.ngp) {
+        const BeamRow p = k > 0 ? row(k - 1) : BeamRow{0.0, 0.0, A.bguard ? A.bguard[(size_t)j * B_NC0 + B_JZ0] : 0.0,
+                                                      A.bguard ? A.bguard[(size_t)j * B_NC0 + B_JP1I] : 0.0};
+        djz = (r.jz - p.jz) * A.idxi;
+        djt = (r.jt - p.jt) * A.idxi;
+    } else if (K > 1) {
+        const BeamRow a = k == 0 ? r : row(k - 1), b = k == K - 1 ? r : row(k + 1);
+        const double f = (k == 0 || k == K - 1) ? 1.0 : 0.5;
+        djz = f * (b.jz - a.jz) * A.idxi;
+        djt = f * (b.jt - a.jt) * A.idxi;
+    }
+    r.rt += ds * r.drt;
+    r.jz += ds * djz;
+    r.jt += ds * djt;
+    return r;
 }
 
 // right-hand sides of the psi, E_z, B_z systems at row i (src/Simulation.cpp:798-799, :517-527)
@@ -1219,8 +1286,41 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
 
     int scan_par = 0;                                            // alternates the scan scratch
     const double fc = A.flux_coef;
+    // The xi positions of the last ORD pushes (tn[0] the newest; the same in every thread) give the
+    // Adams-Bashforth coefficients of the next push: the classical ones for uniform steps, the
+    // variable-step ones after adaptive sub-slicing (src/PlasmaSpecies.cpp:561-580). A slab whose plasma
+    // was pushed before continues uniform steps of dxi.
+    double xcur = 0.0, hlast = A.pin_pushed ? A.dxi : 0.0, tn[ORD], abc[5];
+#pragma unroll
+    for (int m = 0; m < ORD; ++m) tn[m] = -(m + 1) * A.dxi;
+    auto coeffs = [&](double h, bool first) {
+        if (first) {
+#pragma unroll
+            for (int m = 0; m < ORD; ++m) tn[m] = xcur - m * h;
+        } else {
+#pragma unroll
+            for (int m = ORD - 1; m > 0; --m) tn[m] = tn[m - 1];
+            tn[0] = xcur;
+        }
+        bool uniform = true;
+#pragma unroll
+        for (int m = 1; m < ORD; ++m) uniform = uniform && fabs((tn[m - 1] - tn[m]) - h) <= 1e-9 * h;
+        if (uniform) {
+#pragma unroll
+            for (int m = 0; m < 5; ++m) abc[m] = A.ab[m];
+        } else {
+            ab_variable<ORD>(tn, h, abc);
+        }
+        xcur += h;
+        hlast = h;
+    };
     for (int k = 0; k < K; ++k) {
-        if (double* const trj = gate.traj(A)) {        // the plasma state at the start of slice k
+    // the passes of slice k: its own, then its sub-slices (adaptive sub-slicing, src/Simulation.cpp:755-781):
+    // each pushes by dxi / nsub; a sub-slice re-deposits the plasma and re-solves the fields with the beam
+    // sources extrapolated from slice k; only the slice itself is stored
+    int nsub = 1;
+    for (int ss = 0; ss < nsub; ++ss) {
+        if (double* const trj = ss == 0 ? gate.traj(A) : nullptr) {   // the plasma state at the start of slice k
             double* T = trj + (size_t)k * (6 + 5 * (size_t)ORD) * npad;
             if (REG) {
                 if (tid < np) {
@@ -1244,7 +1344,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         if (tim && tid == 0) t_sub = clock64();
         // beam rows of slice k+1 for this thread's nodes (consumed below, latency overlaps the solves)
         BeamRow pre[kMaxR];
-        if (A.dbuf && k + 1 < K)
+        if (A.dbuf && k + 1 < K && ss == 0)
 #pragma unroll
             for (int u = 0; u < kMaxR; ++u)
                 if (u < Rw && row0 + u < M) pre[u] = beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u);
@@ -1332,7 +1432,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                     S.wr1[N] = -(S.g0[N] * pw[u + 2] + S.gm[N] * pw[u + 1] + S.gp[N] * pw[u]);
                 }
             }
-            if (A.dbuf && k + 1 < K)
+            if (A.dbuf && k + 1 < K && ss == 0)
 #pragma unroll
                 for (int u = 0; u < kMaxR; ++u)
                     if (u < Rw && row0 + u < M) init_sources<EXT>(sn, S, row0 + u, pre[u], M);
@@ -1343,6 +1443,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
 
         // ---------------- P3: S+ (src/PlasmaSpecies.cpp:508-559), exact
         if (tid < 7) S.fx[tid] = 0;           // the plasma deposit's maxima (read last before P2's barrier)
+        if (tid == 7) *S.cmax = 0ull;         // the cells-crossed maximum (read last at the last P5)
         if (REG) {
             const bool act = tid < np && P.w != 0.0;
             double v[4];
@@ -1486,45 +1587,82 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         __syncthreads();
         PHASE_MARK(3);
 
-        // ---------------- P5: store slice k; push k -> k+1 and deposit into slice k+1
+        // ---------------- P5: store slice k; push k -> k+1 (or to the next sub-slice) and deposit
         if (tid >= 7 && tid < 9) S.fx[tid] = 0;   // the S deposit's maxima (read last before P4's barrier)
-        // The accumulators of the next slice's deposit: with double-buffered sources this slice's buffer,
-        // free once stored (the next slice's start values already sit in sn); with one buffer that
-        // buffer, its start values added when the deposit is finished. Either way zeroed by the store.
-        const Src acc = A.dbuf ? s : sn;
+        // adaptive sub-slicing, decided in the slice's own pass from the particles as they stand
+        // (src/Simulation.cpp:837-847): nsub = ceil(max cells crossed / max_cells_per_step), at least
+        // ceil(dxi / (2 h_last)) (the step at most doubles), at most substep_max
+        if (ss == 0 && A.max_cells > 0.0 && k + 1 < K) {
+            double c = 0.0;
+            if (REG) {
+                if (tid < np && P.w != 0.0) c = cells_crossed(S, N, R, P.x, P.y, P.px, P.py, P.dl, A.dxi);
+            } else {
+                for (int p = tid; p < np; p += kThreads) {
+                    const double* ps = gate.ps(A);
+                    if (ps[5 * (size_t)npad + p] == 0.0) continue;
+                    c = fmax(c, cells_crossed(S, N, R, ps[p], ps[npad + p], ps[2 * (size_t)npad + p],
+                                              ps[3 * (size_t)npad + p], ps[4 * (size_t)npad + p], A.dxi));
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) c = fmax(c, __shfl_xor_sync(FULL, c, o));
+            if (lane == 0 && c > 0.0) atomicMax(S.cmax, (unsigned long long)__double_as_longlong(c));
+            __syncthreads();
+            const double cm = __longlong_as_double((long long)*S.cmax);
+            int n = cm <= A.max_cells ? 1 : (int)ceil(cm / A.max_cells);
+            if (hlast > 0.0) n = max(n, (int)ceil(A.dxi / (2.0 * hlast) - 1e-9));
+            nsub = min(n, A.substep_max > 0 ? A.substep_max : 64);
+            if (tid == 0 && nsub > 1) S.fx[11] += nsub - 1;
+        }
+        const double hstep = A.dxi / nsub;
+        const bool to_next = ss == nsub - 1;       // this push's deposit builds slice k+1, else the next sub-slice
+        // The accumulators of the deposit: buffer s (with double-buffered sources its slice is stored and the
+        // next slice's start values already sit in sn; with one buffer s is sn). Its values go to sn for
+        // the next slice, or stay in s for the next sub-slice. Zeroed (all 9 arrays) after the store.
+        const Src acc = s;
+        const Src dst = to_next ? sn : s;
         {
             const size_t fb = (size_t)k * M;
             for (int j = tid; j < M; j += kThreads) {
-                double* F = gate.fld(A) + (fb + j) * F_NC0;
-                F[F_EP1R] = S.wr1[j] + S.bpi[j];
-                F[F_EP1I] = 0.0 - S.bpr[j];
-                F[F_BP1R] = S.bpr[j];
-                F[F_BP1I] = S.bpi[j];
-                F[F_EZ0] = S.ez[j];
-                F[F_BZ0] = S.bz[j];
-                double* D = gate.diag(A) + (fb + j) * D_NC0;
-                D[D_PSI0] = S.psi[j];
-                D[D_NE0] = s.ne[j];
-                D[D_NI0] = s.ni[j];
+                if (ss == 0) {
+                    double* F = gate.fld(A) + (fb + j) * F_NC0;
+                    F[F_EP1R] = S.wr1[j] + S.bpi[j];
+                    F[F_EP1I] = 0.0 - S.bpr[j];
+                    F[F_BP1R] = S.bpr[j];
+                    F[F_BP1I] = S.bpi[j];
+                    F[F_EZ0] = S.ez[j];
+                    F[F_BZ0] = S.bz[j];
+                    double* D = gate.diag(A) + (fb + j) * D_NC0;
+                    D[D_PSI0] = S.psi[j];
+                    D[D_NE0] = s.ne[j];
+                    D[D_NI0] = s.ni[j];
+                }
                 if (k + 1 < K) {
 #pragma unroll
                     for (int c = 0; c < 7; ++c) dep_arr(acc, c)[j] = 0.0;
-                    if (!A.dbuf) { acc.S1r[j] = 0.0; acc.S1i[j] = 0.0; }
+                    acc.S1r[j] = 0.0;
+                    acc.S1i[j] = 0.0;
                 }
             }
         }
         if (k + 1 < K) {
-            BeamRow nxt[kMaxR];                 // one buffer: the beam rows of slice k+1 for this thread's rows
-            if (!A.dbuf)
+            // the beam part the deposit's values start from, for this thread's rows: slice k+1's (one
+            // buffer), or slice k's extrapolated to the next sub-slice
+            BeamRow nxt[kMaxR];
+            if (!to_next || !A.dbuf)
 #pragma unroll
                 for (int u = 0; u < kMaxR; ++u)
-                    if (u < Rw && row0 + u < M) nxt[u] = beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u);
-            const bool first = (k == 0) && !A.pin_pushed;
+                    if (u < Rw && row0 + u < M)
+                        nxt[u] = to_next ? beam_row<Gate::kActive, EXT>(A, gate.bsrc(A), k + 1, row0 + u)
+                                         : beam_row_at<Gate::kActive, EXT>(A, gate.bsrc(A), k, row0 + u,
+                                                                            (ss + 1) * hstep);
+            const bool first = (k == 0) && (ss == 0) && !A.pin_pushed;
+            coeffs(hstep, first);
             if (REG) {
                 bool act = tid < np && P.w != 0.0;
                 double v[12];
                 if (act) {
-                    const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first);
+                    const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first, abc, hstep);
                     if (pr > 0) {
                         const double rn = sqrt(P.x * P.x + P.y * P.y);
                         J = locate_from(S.r, N, R, rn, J);
@@ -1555,7 +1693,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                             if (Q.w != 0.0) {
                                 if (pass == 0) {
                                     const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
-                                    const int pr = push_particle(Q, g, S, A, first);
+                                    const int pr = push_particle(Q, g, S, A, first, abc, hstep);
                                     if (pr > 0) {
                                         const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
                                         j = g2.j;
@@ -1592,19 +1730,19 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 const int i = row0 + u;
                 if (u >= Rw || i >= M) continue;
                 double b0[7];
-                if (A.dbuf) {
+                if (to_next && A.dbuf) {
 #pragma unroll
                     for (int c = 0; c < 7; ++c) b0[c] = dep_arr(sn, c)[i];
                 } else {
                     init_base<EXT>(S, i, nxt[u], M, b0);
                 }
-                deposit_finish(sn, acc, i, b0, S.fx, bits_p);
+                deposit_finish(dst, acc, i, b0, S.fx, bits_p);
             }
         }
-        if (Gate::kActive) gate.slice_done_all(k);                     // every thread, before the barrier
+        if (Gate::kActive && to_next) gate.slice_done_all(k);          // every thread, before the barrier
         __syncthreads();
         PHASE_MARK(4);
-        if (Gate::kActive) {
+        if (Gate::kActive && to_next) {
             if (tid < 32) {                                   // warp 0: publish slice k, check the next rows
                 bool ok = true;
                 if (tid == 0) ok = gate.slice_done(k);
@@ -1615,14 +1753,16 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
             __syncthreads();
             if (!*S.flag) return false;
         }
+    }   // the passes of slice k
     }
     if (A.pout) {
         // a slab that hands its plasma on: push the last slice too (src/Simulation.cpp:755, the push of the
         // last local slice produces the state entering the next slab), no deposit
         const bool first = (K == 1) && !A.pin_pushed;
+        coeffs(A.dxi, first);
         if (REG) {
             if (tid < np && P.w != 0.0) {
-                const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first);
+                const int pr = push_particle(P, geometry_in(S.r, S.ih, P.x, P.y, J), S, A, first, abc, A.dxi);
                 if (pr <= 0) { atomicAdd(S.lost, 1); if (pr < 0) atomicAdd(S.fx + 12, 1); }
             }
             if (tid < np) pstore(P, A.pout, npad, tid);
@@ -1632,7 +1772,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 pload(Q, gate.ps(A), npad, p);
                 species_params(A, p, Q.q, Q.qm);
                 if (Q.w != 0.0) {
-                    const int pr = push_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), S, A, first);
+                    const int pr = push_particle(Q, geometry(S.r, S.ih, N, R, Q.x, Q.y), S, A, first, abc, A.dxi);
                     if (pr <= 0) { atomicAdd(S.lost, 1); if (pr < 0) atomicAdd(S.fx + 12, 1); }
                 }
                 pstore(Q, gate.ps(A), npad, p);
@@ -1646,6 +1786,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
         atomicAdd(&A.counters[0], (unsigned long long)*S.lost);
         if (S.fx[13]) atomicAdd(&A.counters[1], (unsigned long long)S.fx[13]);
         if (S.fx[12]) atomicAdd(&A.counters[2], (unsigned long long)S.fx[12]);
+        if (S.fx[11]) atomicAdd(&A.counters[3], (unsigned long long)S.fx[11]);
     }
     return true;
 #undef PHASE_MARK

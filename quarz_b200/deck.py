@@ -30,6 +30,7 @@ _GLOBAL_KEYS = {
     "xi.convention", "grid.type", "grid.rmax", "grid.dr", "grid.regions", "grid.max_ratio", "grid.file",
     "xi.min", "xi.max", "xi.step", "time.dt", "time.steps", "time.start", "modes", "solver.picard",
     "solver.tridiag", "pusher.ab_order", "pusher.delta_min", "pusher.max_qsa_factor", "plasma.species",
+    "pusher.max_cells_per_step", "pusher.substep_max",
     "plasma.seed", "plasma.neutralize", "plasma.rmax", "plasma.radial", "plasma.channel_depth",
     "plasma.channel_radius", "beams", "beams.xi_shape", "output.dir", "output.every", "pusher.beam",
     "plasma.smooth_length",
@@ -199,6 +200,8 @@ class RunSpec:
     tridiag: str = "auto"
     neutralize: bool = True
     smooth_length: float = 0.0   # plasma.smooth_length (0: no smoothing)
+    max_cells: float = 0.0       # pusher.max_cells_per_step: adaptive sub-slicing (0: off)
+    substep_max: int = 64        # pusher.substep_max
     dt: float = 0.0
     steps: int = 0
     species: List[SpeciesSpec] = field(default_factory=list)
@@ -265,6 +268,10 @@ def run_spec(cfg: Dict[str, str], base_dir: str = ".") -> RunSpec:
         dt=float(cfg.get("time.dt", "0")),
         steps=int(cfg.get("time.steps", "0")),
     )
+    spec.max_cells = float(cfg.get("pusher.max_cells_per_step", "0"))
+    spec.substep_max = int(cfg.get("pusher.substep_max", "64"))
+    if spec.max_cells < 0 or spec.substep_max < 1:     # src/Simulation.cpp:51-54
+        raise ValueError("pusher.max_cells_per_step must be >= 0 and pusher.substep_max >= 1")
     spec.smooth_length = float(cfg.get("plasma.smooth_length", "0"))
     if spec.smooth_length < 0:
         raise ValueError("plasma.smooth_length must be >= 0")

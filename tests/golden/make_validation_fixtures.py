@@ -4,8 +4,9 @@ checkout exists):  python tests/golden/make_validation_fixtures.py <path of the 
   validation_numbers.json  printed results of validation/reference_full.txt and reference_quick.txt
                            for the hot-path sections (1 linear wake, 2 blowout, 3 betatron, 4 gain,
                            6 displaced analytic driver in mode 1 (linear regime), 7 centroid betatron
-                           oscillation with azimuthal mode 1)
-  decks/*.in               the validation decks those numbers come from (blowout, gain, betatron, linear)
+                           oscillation with azimuthal mode 1, 13 adaptive sub-slicing)
+  decks/*.in               the validation decks those numbers come from (blowout, gain, betatron, linear, and
+                           the paper case conv_s1 of section 13)
 """
 import json
 import os
@@ -38,6 +39,14 @@ for tag, fn in (("full", "reference_full.txt"), ("quick", "reference_quick.txt")
         m = re.match(r"max \|x_c - x0 cos\(w_b t\)\|/x0 = (\S+),\s+max \|y_c\|/x0 = (\S+)", line)
         if m:
             out["m1_centroid_" + tag] = {"x": m.group(1), "y": m.group(2)}
+        m = re.match(r"\s*(out_ss_plain|out_ss_sub)\s+extra sub-slices\s+(\d+) \| behind the spike: Ez (\S+) psi (\S+) \| "
+                     r"witness: Ez (\S+) psi (\S+) \| spike integral (\S+)", line)
+        if m:
+            out["subslice_" + m.group(1)[7:] + "_" + tag] = dict(
+                zip(["extra", "behind Ez", "behind psi", "witness Ez", "witness psi", "spike"], m.groups()[1:]))
+        m = re.match(r"\s*reference out_ss_ref: integral of Ez over the closure spike \(xi -9\.2\.\.-8\.9\) = (\S+)", line)
+        if m:
+            out["subslice_ref_" + tag] = {"spike": m.group(1)}
         m = re.match(r"d<gamma>/dt = (\S+)", line)
         if m:
             out["gain_" + tag] = m.group(1)
@@ -51,4 +60,5 @@ with open(os.path.join(here, "validation_numbers.json"), "w") as f:
 os.makedirs(os.path.join(here, "decks"), exist_ok=True)
 for d in ("blowout.in", "gain.in", "betatron.in", "linear.in"):
     shutil.copy(os.path.join(ref, "validation", d), os.path.join(here, "decks", d))
+shutil.copy(os.path.join(ref, "paper", "inputs", "conv_s1.in"), os.path.join(here, "decks", "conv_s1.in"))
 print(json.dumps(out, indent=1, sort_keys=True))

@@ -21,7 +21,7 @@ VAL = json.load(open(os.path.join(GOLDEN, "validation_numbers.json")))
 def _deck(name, overrides=()):
     with open(os.path.join(GOLDEN, "decks", name)) as f:
         cfg = deck.parse_deck(f.read(), overrides)
-    for k in ("output.dir", "output.every"):
+    for k in [k for k in cfg if k.startswith("output.")]:       # output settings: not part of the path
         cfg.pop(k, None)
     return deck.run_spec(cfg)
 
