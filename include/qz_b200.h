@@ -333,6 +333,13 @@ qz_status qz_sim_adjoint(qz_sim* s, int nsteps, double dt, const double* lamS_ho
 typedef void (*qz_adjoint_seed_fn)(const double* moments, int nsteps, int nbeams, double* lamS, void* user);
 qz_status qz_sim_adjoint_fn(qz_sim* s, int nsteps, double dt, qz_adjoint_seed_fn fn, void* user,
                             double* const* lam_host, double* mom_host, double* ms2, void* stream);
+/* Slice checkpointing of the pipelined adjoint: the forward keeps the plasma state of every C-th slice
+   of each step (and the W+ radial field of every slice), and the reverse sweep pushes the plasma again
+   from those checkpoints one segment of C slices at a time, reproducing the forward's states bit for
+   bit. every = 0 (the default): C = ceil(sqrt(K)); every = 1: the state of every slice is kept (no
+   recomputation; memory K / C times larger); every > 1: that C (at most K). The step-by-step adjoint
+   keeps one step's states at a time and ignores it. No counterpart in the reference. */
+qz_status qz_sim_set_adjoint_checkpoint(qz_sim* s, int every);
 /* Clock cycles per phase of the run's sweeps (qz_sweep_timing of the sim's sweep): 16 counters,
    accumulated by thread 0 of every sweep while enabled (all sweeps of a pipelined run together);
    0..8 the forward sweep's phases, 9..15 those of the step-by-step adjoint's reverse sweep.

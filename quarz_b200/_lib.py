@@ -103,6 +103,7 @@ SIGNATURES = {
     "qz_sim_step_host": [C.c_void_p, C.POINTER(C.c_void_p), C.c_double, C.c_double, C.c_int, _dp, C.c_void_p],
     "qz_sim_restart": [C.c_void_p],
     "qz_sim_set_exact": [C.c_void_p, C.c_int],
+    "qz_sim_set_adjoint_checkpoint": [C.c_void_p, C.c_int],
     "qz_sim_set_schedule": [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_double],
     "qz_sim_schedule": [C.c_void_p, C.POINTER(C.c_int)],
     "qz_sim_times": [C.c_void_p, _dp],

@@ -368,6 +368,11 @@ class Simulation:
         """qz_sim_restart: the next run starts the beams' leapfrog again (a new run from set beams)."""
         check(lib().qz_sim_restart(self.h))
 
+    def set_adjoint_checkpoint(self, every: int = 0):
+        """qz_sim_set_adjoint_checkpoint: slice checkpointing of the pipelined adjoint (0: every
+        ceil(sqrt(K))-th slice, 1: every slice, C > 1: every C-th)."""
+        check(lib().qz_sim_set_adjoint_checkpoint(self.h, int(every)))
+
     def set_exact(self, exact: bool = True):
         """qz_sim_set_exact: exact (reproducible) or FP64-reduction beam deposits for m = 0 runs."""
         check(lib().qz_sim_set_exact(self.h, 1 if exact else 0))

@@ -852,6 +852,7 @@ struct qz_sim {
     double *d_fld = nullptr, *d_diag = nullptr, *d_bsrc[2] = {nullptr, nullptr}, *d_mom = nullptr;
     double* d_bstat = nullptr;   // sources of the analytic rigid beams (K, M, B_NC), added by every sweep
     int nanalytic = 0;
+    int ckpt_every = 0;          // qz_sim_set_adjoint_checkpoint (0: ceil(sqrt(K)))
     int cur = 0;
     bool bsrc_valid = false;
     // exact beam deposits of m = 0 runs (BeamArgs::fx_qe): per-node quantum exponents, the limb split,
@@ -1192,6 +1193,8 @@ qz_status grow(T** p, size_t* have, size_t need, const char* what) {
 struct FwdRecord {
     double* traj = nullptr;
     size_t traj_slot = 0;
+    int traj_every = 1;                 // checkpoint slices k = 0, C, 2C, ... only (C > 1)
+    double* wrec = nullptr;             // W+ radial field per slice, K M per step
     double* snap = nullptr;
     size_t snap_step = 0;
     long snap_off[qzb::kMaxBeams] = {0, 0, 0, 0};
@@ -1388,6 +1391,8 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     if (rec) {
         A.traj = rec->traj;
         A.traj_slot = rec->traj_slot;
+        A.sw.traj_every = rec->traj_every;
+        A.wrec = rec->wrec;
         A.snap = rec->snap;
         A.snap_step = rec->snap_step;
         for (int q = 0; q < qzb::kMaxBeams; ++q) A.snap_off[q] = rec->snap_off[q];
@@ -1525,17 +1530,22 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const AdjSeed& see
     std::vector<size_t> off(nb + 1, 0);
     for (int b = 0; b < nb; ++b) off[b + 1] = off[b] + (size_t)s->beams[b].n;
     const size_t per = 7 * off[nb];
-    const size_t traj_slot = (size_t)K * (6 + 5 * (size_t)base.ord) * base.npad;
+    // slice checkpointing: the plasma state of every C-th slice per step, C = ceil(sqrt(K)) by default
+    const int every = s->ckpt_every > 0 ? std::min(s->ckpt_every, K) : (int)std::ceil(std::sqrt((double)K) - 1e-9);
+    const int nck = (K + every - 1) / every;
+    const size_t state = (6 + 5 * (size_t)base.ord) * base.npad;
+    const size_t traj_slot = (size_t)nck * state;
     double *snap = nullptr, *traj = nullptr, *lam = nullptr, *lam2 = nullptr, *lfld = nullptr, *lbsrc = nullptr,
-           *lamS = nullptr;
+           *lamS = nullptr, *wrec = nullptr, *seg = nullptr;
     int* ints = nullptr;
     auto release = [&]() {
         for (void* q : {(void*)snap, (void*)traj, (void*)lam, (void*)lam2, (void*)lfld, (void*)lbsrc, (void*)lamS,
-                        (void*)ints})
+                        (void*)ints, (void*)wrec, (void*)seg})
             if (q) cudaFree(q);
     };
     if (cudaMalloc((void**)&snap, sizeof(double) * (per * (T + 1) + 1)) != cudaSuccess ||
         cudaMalloc((void**)&traj, sizeof(double) * traj_slot * (T + 1)) != cudaSuccess ||
+        cudaMalloc((void**)&wrec, sizeof(double) * KM * (T + 1)) != cudaSuccess ||
         cudaMalloc((void**)&lam, sizeof(double) * (per + 1)) != cudaSuccess ||
         cudaMalloc((void**)&lam2, sizeof(double) * (per + 1)) != cudaSuccess ||
         cudaMalloc((void**)&lfld, sizeof(double) * KM * 6 * T) != cudaSuccess ||
@@ -1553,6 +1563,8 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const AdjSeed& see
         FwdRecord rec;
         rec.traj = traj;
         rec.traj_slot = traj_slot;
+        rec.traj_every = every;
+        rec.wrec = wrec;
         rec.snap = snap;
         rec.snap_step = per;
         for (int b = 0; b < nb; ++b) rec.snap_off[b] = (long)(7 * off[b]);
@@ -1581,6 +1593,8 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const AdjSeed& see
         A.fld_slot = KM * 6;
         A.traj = traj;
         A.traj_slot = traj_slot;
+        A.sw.traj_every = every;
+        A.wrec = wrec;
         A.lfld = lfld;
         A.lfld_slot = KM * 6;
         A.lbsrc = lbsrc;
@@ -1637,6 +1651,14 @@ qz_status adjoint_pipelined(qz_sim* s, int nsteps, double dt, const AdjSeed& see
         const int g1 = std::min(grid, sms);
         const int wmin = std::max(8, (2 * g1) / 5);
         A.nsweep = std::max(1, std::min(T, g1 - wmin));
+        if (every > 1) {                               // one segment buffer per reverse-sweep CTA
+            A.seg_slot = (size_t)every * state;
+            if (cudaMalloc((void**)&seg, sizeof(double) * A.seg_slot * A.nsweep) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(QZ_ERR_NOMEM, "qz_sim_adjoint: device allocation failed (checkpoint segments)");
+            }
+            A.seg = seg;
+        }
         QZ_CUDA(qzb::launch_adjoint_pipeline(A, g1, st));
         int err = 0;
         QZ_CUDA(cudaMemcpyAsync(&err, A.err, sizeof(int), cudaMemcpyDeviceToHost, st));
@@ -1871,6 +1893,12 @@ extern "C" qz_status qz_sim_restart(qz_sim* s) {
     if (!s) return fail(QZ_ERR_ARG, "qz_sim_restart: null pointer");
     for (auto& b : s->beams) b.started = 0;
     s->bsrc_valid = false;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sim_set_adjoint_checkpoint(qz_sim* s, int every) {
+    if (!s || every < 0) return fail(QZ_ERR_ARG, "qz_sim_set_adjoint_checkpoint: bad argument");
+    s->ckpt_every = every;
     return QZ_OK;
 }
 

@@ -733,9 +733,71 @@ __device__ __noinline__ void filter_rows_adj(double* const (&arr)[NS], int op, b
     __syncthreads();
 }
 
+// Slice checkpointing (SweepArgs::traj_every = C > 1): the forward kept the plasma state of the slices
+// k = 0, C, 2C, ... only. Before the reverse sweep reaches the last slice of segment [k0, k1] it pushes
+// its particle again from the checkpoint k0 through slices k0 .. k1 - 1, with the fields the forward
+// gathered there (the field store and the W+ record: the same inputs, the same push_particle), and
+// keeps the states P_k0 .. P_k1 in seg (slot k - k0): the forward's trajectory bit for bit, at
+// K / C + C states per sweep instead of K. The field arrays of S serve as scratch (the reverse loads
+// them again for every slice); only the calling thread's particle is written and read.
+template <int ORD>
+__device__ void recompute_segment(const SweepArgs& A, const AdjSm& S, const double* __restrict__ ck,
+                                  const double* __restrict__ fld, const double* __restrict__ wrec,
+                                  double* __restrict__ seg, int k0, int k1, bool has_p, double qsp, double qmsp) {
+    const int M = A.M, N = A.N, npad = A.npad, tid = threadIdx.x;
+    const size_t nv = 6 + 5 * (size_t)ORD;
+    PState<ORD> P;
+    P.q = qsp; P.qm = qmsp;
+    P.w = 0.0;
+    auto put = [&](int slot) {
+        double* T = seg + (size_t)slot * nv * npad + tid;
+        T[0] = P.x; T[npad] = P.y; T[2 * (size_t)npad] = P.px; T[3 * (size_t)npad] = P.py;
+        T[4 * (size_t)npad] = P.dl; T[5 * (size_t)npad] = P.w;
+#pragma unroll
+        for (int m = 0; m < ORD; ++m)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) T[(6 + (size_t)m * 5 + v) * npad] = P.h[m][v];
+    };
+    if (has_p) {
+        const double* T = ck + tid;
+        P.x = T[0]; P.y = T[npad]; P.px = T[2 * (size_t)npad]; P.py = T[3 * (size_t)npad];
+        P.dl = T[4 * (size_t)npad]; P.w = T[5 * (size_t)npad];
+#pragma unroll
+        for (int m = 0; m < ORD; ++m)
+#pragma unroll
+            for (int v = 0; v < 5; ++v) P.h[m][v] = T[(6 + (size_t)m * 5 + v) * npad];
+        put(0);
+    }
+    sweep_detail::Smem F{};
+    F.wr1 = S.wpr; F.ez = S.ez; F.bz = S.bz; F.bpr = S.bpr; F.bpi = S.bpi;
+    double ab[5];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) ab[m] = A.ab[m];
+    for (int k = k0; k < k1; ++k) {
+        __syncthreads();                             // the arrays' previous contents are no longer read
+        if (tid < M) {
+            const double* Fk = fld + ((size_t)k * M + tid) * F_NC0;
+            S.wpr[tid] = wrec ? wrec[(size_t)k * M + tid] : Fk[F_EP1R] - Fk[F_BP1I];
+            S.bpr[tid] = Fk[F_BP1R];
+            S.bpi[tid] = Fk[F_BP1I];
+            S.ez[tid] = Fk[F_EZ0];
+            S.bz[tid] = Fk[F_BZ0];
+        }
+        __syncthreads();
+        if (has_p) {
+            if (P.w != 0.0)
+                (void)sweep_detail::push_particle<ORD>(P, geometry(S.r, S.ih, N, A.R, P.x, P.y), F, A, k == 0, ab,
+                                                       A.dxi);
+            put(k + 1 - k0);
+        }
+    }
+    __syncthreads();
+}
+
 template <int ORD, class Gate, bool FILT = false>
 __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ traj, const double* __restrict__ fld,
-                                const double* lfld, double* __restrict__ lbsrc, double* smem_raw, Gate& gate) {
+                                const double* lfld, double* __restrict__ lbsrc, double* smem_raw, Gate& gate,
+                                const double* __restrict__ wrec = nullptr, double* __restrict__ seg = nullptr) {
     const int M = A.M, N = A.N, K = A.K, tid = threadIdx.x;
     const int np = A.np, npad = A.npad;
     const AdjSm S = carve_adj(smem_raw, M);
@@ -785,6 +847,12 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             t_prev = tn;                                                      \
         }                                                                     \
     } while (0)
+    // where the state of slice k is read: the whole trajectory (cur = traj, kbase = 0), or the
+    // recomputed segment of slice k (cur = seg, kbase = its first slice)
+    if (A.traj_every > 1 && !seg) return false;      // a checkpointed trajectory needs the segment buffer
+    const int every = A.traj_every > 1 ? A.traj_every : 1;
+    const double* cur = traj;
+    int kbase = 0;
     // this thread's particle P_k from the trajectory (the history only when asked)
     auto load_p = [&](int k, PState<ORD>& P, bool hist) {
         P.q = qsp; P.qm = qmsp;
@@ -792,7 +860,7 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
         P.x = P.y = P.px = P.py = 0.0;
         P.dl = 1.0;
         if (!has_p) return;
-        const double* T = traj + (size_t)k * nv * npad + tid;
+        const double* T = cur + (size_t)(k - kbase) * nv * npad + tid;
         P.x = T[0]; P.y = T[npad]; P.px = T[2 * (size_t)npad]; P.py = T[3 * (size_t)npad];
         P.dl = T[4 * (size_t)npad]; P.w = T[5 * (size_t)npad];
         if (hist)
@@ -802,6 +870,14 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
                 for (int v = 0; v < 5; ++v) P.h[m][v] = T[(6 + (size_t)m * 5 + v) * npad];
     };
     for (int k = K - 1; k >= 0; --k) {
+        if (every > 1 && (k == K - 1 || (k + 1) % every == 0)) {
+            // the segment ending at slice k, pushed again from its checkpoint (needs no gate: the
+            // forward's records are complete)
+            const int g = k / every;
+            recompute_segment<ORD>(A, S, traj + (size_t)g * nv * npad, fld, wrec, seg, g * every, k, has_p, qsp, qmsp);
+            cur = seg;
+            kbase = g * every;
+        }
         if (Gate::kActive) {                         // the field adjoint of row k is complete
             if (tid < 32) {
                 const bool ok = gate.before_slice(k);
@@ -812,12 +888,12 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
         }
         // ---- this slice's fields and field adjoints (store in reverse)
         bool alive = false;
-        if (has_p) alive = traj[(size_t)k * nv * npad + 5 * (size_t)npad + tid] != 0.0;
+        if (has_p) alive = cur[(size_t)(k - kbase) * nv * npad + 5 * (size_t)npad + tid] != 0.0;
         ADJ_MARK(0);
         if (row) {
             const double* F = fld + ((size_t)k * M + i) * F_NC0;
             const double* LF = lfld + ((size_t)k * M + i) * F_NC0;
-            S.wpr[i] = F[F_EP1R] - F[F_BP1I];
+            S.wpr[i] = wrec ? wrec[(size_t)k * M + i] : F[F_EP1R] - F[F_BP1I];
             S.bpr[i] = F[F_BP1R];
             S.bpi[i] = F[F_BP1I];
             S.ez[i] = F[F_EZ0];
@@ -1162,8 +1238,11 @@ __device__ void adj_sweep_role(const AdjPipeArgs& P, double* smem) {
         }
         __syncthreads();
         AdjPipeGate g{&P, &gs};
-        if (!sweep_back_body<ORD, AdjPipeGate, FILT>(P.sw, P.traj + (size_t)n * P.traj_slot, P.fld + (size_t)n * P.fld_slot,
-                                  P.lfld + (size_t)n * P.lfld_slot, P.lbsrc + (size_t)n * P.lbsrc_slot, smem, g))
+        if (!sweep_back_body<ORD, AdjPipeGate, FILT>(
+                P.sw, P.traj + (size_t)n * P.traj_slot, P.fld + (size_t)n * P.fld_slot,
+                P.lfld + (size_t)n * P.lfld_slot, P.lbsrc + (size_t)n * P.lbsrc_slot, smem, g,
+                P.wrec ? P.wrec + (size_t)n * (P.fld_slot / F_NC0) : nullptr,
+                P.seg ? P.seg + (size_t)blockIdx.x * P.seg_slot : nullptr))
             return;
         __syncthreads();
     }

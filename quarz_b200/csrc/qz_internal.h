@@ -53,8 +53,13 @@ struct SweepArgs {
     double* bgs;                    // (3, M) scratch: background rho - J_z in modes 0 / 1
     double* srcs;                   // (2 x 30, M) scratch: the sources of this slice and of the next
     // optional, m = 0 (the adjoint's recomputation): the plasma state at the start of every slice,
-    // (K, 6 + 5 * ord, npad): x y px py Delta w, then the AB history h[m][v] (m pushes ago)
+    // (K, 6 + 5 * ord, npad): x y px py Delta w, then the AB history h[m][v] (m pushes ago); with
+    // traj_every = C > 1 only at the checkpoint slices k = 0, C, 2C, ... (slot k / C), the reverse
+    // sweep pushing the plasma again from them. wrec (K, M): the W+ radial field the plasma push of
+    // every slice gathered (the field store holds it only summed with B_theta)
     double* traj;
+    int traj_every;
+    double* wrec;
     // optional, m = 0: radial smoothing of the plasma sources (plasma.smooth_length,
     // src/Simulation.cpp:63-66, :685-690, :810-835)
     int filter;
@@ -193,6 +198,7 @@ struct PipeArgs {
     // 7 columns of the beam's n, the run's particle order); with them the rings hold every step
     double* traj;
     size_t traj_slot;
+    double* wrec;                   // W+ radial field per slice (SweepArgs::wrec), slot of K M per step
     double* snap;
     size_t snap_step;
     long snap_off[kMaxBeams];
@@ -247,7 +253,10 @@ struct AdjPipeArgs {
     SweepArgs sw;
     int nsteps, nsweep;
     const double* fld;  size_t fld_slot;      // forward fields, slot n = step n
-    const double* traj; size_t traj_slot;     // plasma trajectories, slot n
+    const double* traj; size_t traj_slot;     // plasma trajectories, slot n (checkpoints when sw.traj_every > 1)
+    const double* wrec;                       // W+ radial field per slice, slot n of fld_slot / 6 (or null)
+    double* seg;        size_t seg_slot;      // sw.traj_every > 1: the recomputed states of one segment per
+                                              // sweep CTA (traj_every x (6 + 5 ord) x npad each)
     double* lfld;       size_t lfld_slot;     // field-store adjoint of step n (zero before the launch)
     double* lbsrc;      size_t lbsrc_slot;    // beam-source adjoint of step n (zero before the launch)
     int nbeams;

@@ -96,6 +96,9 @@ struct PipeGate {
     __device__ double* bgs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot; }
     __device__ double* srcs(const SweepArgs&) const { return P->m1s + blockIdx.x * P->m1s_slot + 3 * (size_t)P->sw.M; }
     __device__ double* traj(const SweepArgs&) const { return P->traj ? P->traj + (size_t)g->n * P->traj_slot : nullptr; }
+    __device__ double* wrec(const SweepArgs& A) const {
+        return P->wrec ? P->wrec + (size_t)g->n * A.K * A.M : nullptr;
+    }
 
     // warp 0 (all 32 lanes): beam-source rows <= r are final. The lanes look at 32 buckets at once and
     // advance over the finished prefix; the first unfinished one is waited for (bounded).

@@ -49,6 +49,7 @@ struct NoGate {
     __device__ double* srcs(const SweepArgs& A) const { return A.srcs; }
     __device__ double* bgs(const SweepArgs& A) const { return A.bgs; }
     __device__ double* traj(const SweepArgs& A) const { return A.traj; }
+    __device__ double* wrec(const SweepArgs& A) const { return A.wrec; }
 };
 
 // ---------------------------------------------------------------- block scans
@@ -1320,8 +1321,10 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
     // sources extrapolated from slice k; only the slice itself is stored
     int nsub = 1;
     for (int ss = 0; ss < nsub; ++ss) {
-        if (double* const trj = ss == 0 ? gate.traj(A) : nullptr) {   // the plasma state at the start of slice k
-            double* T = trj + (size_t)k * (6 + 5 * (size_t)ORD) * npad;
+        // the plasma state at the start of slice k (every slice, or the checkpoint slices)
+        const int tevery = A.traj_every > 1 ? A.traj_every : 1;
+        if (double* const trj = ss == 0 && k % tevery == 0 ? gate.traj(A) : nullptr) {
+            double* T = trj + (size_t)(k / tevery) * (6 + 5 * (size_t)ORD) * npad;
             if (REG) {
                 if (tid < np) {
                     T[tid] = P.x; T[npad + tid] = P.y; T[2 * (size_t)npad + tid] = P.px;
@@ -1636,6 +1639,7 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                     D[D_PSI0] = S.psi[j];
                     D[D_NE0] = s.ne[j];
                     D[D_NI0] = s.ni[j];
+                    if (double* const W = gate.wrec(A)) W[fb + j] = S.wr1[j];
                 }
                 if (k + 1 < K) {
 #pragma unroll

@@ -53,6 +53,30 @@ def test_adjoint_against_oracle(which, pipelined):
             assert err < 1e-8, (which, b, c, err)
 
 
+@pytest.mark.parametrize("every", [0, 5, 71])
+def test_checkpointed_adjoint_equals_full_record(every):
+    # slice checkpointing (qz_sim_set_adjoint_checkpoint): the reverse sweeps push the plasma again from
+    # every C-th slice (0: C = ceil(sqrt(71)) = 9; 5; 71: one segment per sweep) and reproduce the
+    # forward's states, so the gradient is the one of the fully recorded trajectory (C = 1) up to the
+    # summation order of the reverse pass's atomic adds
+    spec = _specs()[3]
+    beams = [Q.sample_beam(b) for b in spec.beams]
+    T, dt = spec.steps, spec.dt
+    seeds = np.random.default_rng(9).normal(size=(2, 17))
+    seeds[:, 16] = 0.0
+    out = []
+    for c in (1, every):
+        sim = Q.Simulation(spec, beams=beams)
+        sim.set_adjoint_checkpoint(c)
+        out.append(sim.adjoint(T, dt, seeds))
+    assert np.array_equal(out[0][1], out[1][1])          # the forwards' moments
+    for b in range(2):
+        for c in range(7):
+            ref = out[0][0][b][:, c]
+            err = np.linalg.norm(out[1][0][b][:, c] - ref) / max(np.linalg.norm(ref), 1e-300)
+            assert err < 1e-12, (every, b, c, err)
+
+
 def test_gain_and_spread_gradients_against_differences():
     spec = _specs()[0]
     beams = [Q.sample_beam(b) for b in spec.beams]

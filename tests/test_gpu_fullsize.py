@@ -6,8 +6,9 @@ there, so these compare the library with itself through properties the path must
   scale, E_z / B_z 1e-9 relative L2 against the field scale (the larger of the component's norm and
   E_z's), particles 1e-9; and charge is conserved while no particle is lost.
 - Config 2 (modes 0 and 1, Picard 3, 8 azimuths, 2 x 2e6 particles), 2 steps: the same.
-- Config 4 (config 1 through the adjoint), 4 steps: the pipelined adjoint equals the step-by-step
-  adjoint (1e-8 relative L2 per particle component), and the witness-delay gradient equals central
+- Config 4 (config 1 through the adjoint), 4 steps: the pipelined adjoint (slice checkpointing, every
+  49th slice) equals the step-by-step adjoint and the pipelined one that keeps every slice's state (1e-8
+  relative L2 per particle component), and the witness-delay gradient equals central
   differences of the forward (h = 1e-6) to 1e-4. Central differences along the driver profile are no
   check at this size: pinched plasma electrons pass within ~1e-6 of the axis, where c = x / r swings
   sign and the u_r-weighted deposit of d(rho - J_z)/dxi with it, so J has near-jumps at the scale of
@@ -79,15 +80,19 @@ def test_config4_full_size_adjoint_schedules_and_delay():
     seeds = np.zeros((2, 17))
     seeds[1] = A.gain_seed(m[-1, 1])
     lams = []
-    for pipelined in (True, False):
+    for pipelined, every in ((True, 0), (False, 0), (True, 1)):
         sim = Q.Simulation(spec, beams=samples)
         sim.set_schedule(pipelined)
+        sim.set_adjoint_checkpoint(every)
         lams.append(sim.adjoint(spec.steps, spec.dt, seeds)[0])
-    for b in range(2):
-        for c in range(7):
-            ref = lams[1][b][:, c]
-            err = np.linalg.norm(lams[0][b][:, c] - ref) / max(np.linalg.norm(ref), 1e-300)
-            assert err < 1e-8, (b, c, err)
+    # pipelined with slice checkpointing (every 49th slice) against step by step, and against the
+    # pipelined pass that keeps every slice's plasma state
+    for other in (1, 2):
+        for b in range(2):
+            for c in range(7):
+                ref = lams[other][b][:, c]
+                err = np.linalg.norm(lams[0][b][:, c] - ref) / max(np.linalg.norm(ref), 1e-300)
+                assert err < 1e-8, (other, b, c, err)
     gd = A.delay_gradient(lams[0][1])
 
     def J(shift):
