@@ -270,8 +270,9 @@ qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* moments_host, voi
    No counterpart in the reference (its own pipelining over time steps is across MPI ranks,
    src/Simulation.cpp:851-870). */
 qz_status qz_sim_set_schedule(qz_sim* s, int pipelined, int sweep_ctas, int bucket, int span, double timeout_s);
-/* exact = 1 (the default): the beam deposits of m = 0 runs are exact integer sums (two 64-bit limbs per
-   value), so runs repeat bit for bit; exact = 0: FP64 reductions, faster (one reduction per value and half
+/* exact = 1 (the default): the beam deposits of m = 0 runs (up to 2^25 beam particles) are exact integer
+   sums (two integer-valued limbs per value, each sum below 2^53, added with FP64 reductions), so runs
+   repeat bit for bit; exact = 0: FP64 reductions of the values, faster (one reduction per value and half
    the beam-source memory) but their summation order, and so the last bits, vary from run to run. No
    counterpart in the reference (its OpenMP and GPU deposits use atomic adds). */
 qz_status qz_sim_set_exact(qz_sim* s, int exact);

@@ -1048,8 +1048,9 @@ namespace {
 // 2 (sum over beams of max |w q|) / V_j / dxi (the weights of the particles do not change during a run;
 // |1 - v_z| <= 2 and every other factor is at most 1), so the quantum of node j is that bound / 2^B.
 // With at most n contributions per value (n = all beam particles, 2^nbits > n) the limbs split at
-// S = 63 - nbits and B = 126 - 2 nbits keep both integer sums below 2^63. Returns whether the run
-// deposits exactly; it does for m = 0, while m = 1 runs keep FP64 reductions.
+// S = 53 - nbits and B = 2 S keep both limb sums integers below 2^53 (exact in FP64, beam_fx_add).
+// The run deposits exactly for m = 0 up to 2^25 particles (B >= 56: the quantum is at most 2^-56 of
+// the bound); m = 1 runs and larger beams keep FP64 reductions.
 qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     auto& F = s->fx;
     const bool was = F.on;
@@ -1061,8 +1062,8 @@ qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     for (const auto& b : s->beams) ntot += (long)b.n;
     int nbits = 1;
     while (nbits < 62 && (1L << nbits) <= ntot) ++nbits;
-    if (nbits > 30) return QZ_OK;                   // beyond 2^30 particles: FP64 reductions
-    const int S = 63 - nbits, B = 126 - 2 * nbits;
+    if (nbits > 25) return QZ_OK;                   // beyond 2^25 particles: FP64 reductions
+    const int S = 53 - nbits, B = 2 * S;
     if (!F.d_wmax && cudaMalloc((void**)&F.d_wmax, sizeof(double) * qzb::kMaxBeams * 2) != cudaSuccess) {
         F.d_wmax = nullptr;
         return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");

@@ -77,12 +77,15 @@ __device__ __forceinline__ void deposit_one(const BeamArgs& B, double* __restric
     }
 }
 
-// The same m = 0 deposit as deposit_one, returned instead of applied: the 20 contributions of one
-// particle, v[(2 a + b) * 5 + c] for row k + a, node j + b, component c (B_RT0 .. B_RHO0), rows out of
-// the box carrying zero. Returns false when the particle deposits nothing (outside the wall or box).
-// jguess: a nearby radial cell (the gather's, before the push moved the particle), or < 0
+// The part of the m = 0 deposit that the m = 0 sweep reads, returned instead of applied: rho - J_z,
+// J_z and J_theta (B_RT0, B_JZ0, B_JP1I; the sweep never reads the beam's J_r and rho, and a field file
+// deposits its beam density again) of one particle, v[(2 a + b) * 3 + c] for row k + a, node j + b,
+// rows out of the box carrying zero. Returns false when the particle deposits nothing (outside the wall
+// or box). jguess: a nearby radial cell (the gather's, before the push moved the particle), or < 0
+constexpr int kDep0 = 3;                             // components of deposit_vals0
 __device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, double Y, double PX, double PY, double PZ,
-                                              double XI, double wi, int jguess, int& k, int& j, double (&v)[20]) {
+                                              double XI, double wi, int jguess, int& k, int& j,
+                                              double (&v)[4 * kDep0]) {
     const double R = B.R;
     const double r = sqrt(X * X + Y * Y);
     if (r > R) return false;
@@ -96,7 +99,7 @@ __device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, doubl
     const double gam = sqrt(1.0 + p2 + PZ * PZ);
     const double omvz = (1.0 + p2) / (gam * (gam + PZ));
     const double vz = PZ / gam, vx = PX / gam, vy = PY / gam;
-    const double vr = c * vx + s * vy, vt = c * vy - s * vx;
+    const double vt = c * vy - s * vx;
     // the cell of r (src/RadialGrid.hpp:35-50): a short walk from the guess, the search otherwise
     j = locate_near(B.r, B.N, R, r, jguess);
     double t = (r - B.r[j]) * B.inv_h[j];
@@ -111,20 +114,19 @@ __device__ __forceinline__ bool deposit_vals0(const BeamArgs& B, double X, doubl
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             const double d = row ? wi * q * Wk[a] * Wr[b] * B.inv_V[j + b] * B.idxi : 0.0;
-            double* o = v + (2 * a + b) * 5;
-            o[B_RT0] = d * omvz;
-            o[B_JZ0] = d * vz;
-            o[B_JP1R] = d * vr;
-            o[B_JP1I] = d * vt;
-            o[B_RHO0] = d;
+            double* o = v + (2 * a + b) * kDep0;
+            o[0] = d * omvz;
+            o[1] = d * vz;
+            o[2] = d * vt;
         }
     }
     return true;
 }
 
-// adds the 20 contributions of deposit_vals0 into bsrc (FP64 reductions into L2, or exact)
+// adds the contributions of deposit_vals0 into bsrc (FP64 reductions into L2, or exact)
 __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restrict__ bsrc, int k, int j,
-                                             const double (&v)[20]) {
+                                             const double (&v)[4 * kDep0]) {
+    constexpr int comp[kDep0] = {B_RT0, B_JZ0, B_JP1I};
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         const int kk = k + a;
@@ -135,11 +137,11 @@ __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restri
             if (B.fx_scale) {
                 const double sc = B.fx_scale[j + b];
 #pragma unroll
-                for (int c = 0; c < 5; ++c)
-                    beam_fx_add(o + c, B.fx_lo, v[(2 * a + b) * 5 + c], sc, B.fx_inv2s, B.fx_2s);
+                for (int c = 0; c < kDep0; ++c)
+                    beam_fx_add(o + comp[c], B.fx_lo, v[(2 * a + b) * kDep0 + c], sc, B.fx_inv2s, B.fx_2s);
             } else {
 #pragma unroll
-                for (int c = 0; c < 5; ++c) atomicAdd(o + c, v[(2 * a + b) * 5 + c]);
+                for (int c = 0; c < kDep0; ++c) atomicAdd(o + comp[c], v[(2 * a + b) * kDep0 + c]);
             }
         }
     }

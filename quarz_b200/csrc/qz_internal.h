@@ -111,9 +111,9 @@ struct BeamArgs {
     double xi_min, dxi, idxi;
     int K, ngp, modes;
     int pusher;                     // 0 vay, 1 boris, 2 hc, 3 imp (stand-alone push kernels only)
-    // exact deposits (m = 0 runs of qz_sim): when fx_scale is set, bsrc holds two 64-bit integer limbs
-    // per value, the high limb where the double would be and the low limb fx_lo doubles further; a
-    // contribution v to node j is t = v fx_scale[j] (a power of two), split at S bits (beam_fx_add)
+    // exact deposits (m = 0 runs of qz_sim): when fx_scale is set, bsrc holds two integer-valued
+    // limbs per value, the high limb where the double would be and the low limb fx_lo doubles further;
+    // a contribution v to node j is t = v fx_scale[j] (a power of two), split at S bits (beam_fx_add)
     const double* fx_scale;
     double fx_inv2s, fx_2s;         // 2^-S, 2^S
     long fx_lo;

@@ -375,7 +375,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 const long i = base + lane;
                 bool dep = false;
                 int dk = 0, dj = 0;
-                double v[20];
+                double v[4 * beam_detail::kDep0];
                 if (i < i1) {
                     PState7 p;
                     p.w = __ldcg(Bb.w + i);
@@ -406,9 +406,9 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 }
                 if (!dep)
 #pragma unroll
-                    for (int c = 0; c < 20; ++c) v[c] = 0.0;
+                    for (int c = 0; c < 4 * beam_detail::kDep0; ++c) v[c] = 0.0;
                 const int key = dep ? (dk + 1) * M + dj : -1 - lane;
-                if (warp_runs_sum<20>(key, v) && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
+                if (warp_runs_sum<4 * beam_detail::kDep0>(key, v) && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
             }
         } else
         for (long i = i0 + lane; i < i1; i += 32) {
