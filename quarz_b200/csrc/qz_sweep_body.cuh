@@ -262,6 +262,11 @@ __device__ __forceinline__ void scan_bwd_n(const double (&a)[NS], const double (
 template <int NS>
 __device__ __forceinline__ void scan_pivots(double (&m)[NS][4], double (&p)[NS], double (&q)[NS], double* tot) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // The thread's matrices must come renormalised (largest entry in [1, 2)); a product of at most 32 such
+    // matrices stays below 2^63 and the products of the 16 renormalised warp totals below 2^31, so the
+    // scan renormalises once per lane after the warp stage instead of at every level. Renormalising
+    // scales by powers of two, which is exact, and the pivots use only ratios of p and q: the results
+    // are the same bits either way.
 #pragma unroll
     for (int st = 1; st < 32; st <<= 1) {
 #pragma unroll
@@ -272,10 +277,11 @@ __device__ __forceinline__ void scan_pivots(double (&m)[NS][4], double (&p)[NS],
                 const double n00 = m[s][0] * p00 + m[s][1] * p10, n01 = m[s][0] * p01 + m[s][1] * p11;
                 const double n10 = m[s][2] * p00 + m[s][3] * p10, n11 = m[s][2] * p01 + m[s][3] * p11;
                 m[s][0] = n00; m[s][1] = n01; m[s][2] = n10; m[s][3] = n11;
-                renorm(m[s][0], m[s][1], m[s][2], m[s][3]);
             }
         }
     }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) renorm(m[s][0], m[s][1], m[s][2], m[s][3]);
     if (lane == 31)
 #pragma unroll
         for (int s = 0; s < NS; ++s)
@@ -302,7 +308,6 @@ __device__ __forceinline__ void scan_pivots(double (&m)[NS][4], double (&p)[NS],
                 const double n00 = t00 * p00 + t01 * p10, n01 = t00 * p01 + t01 * p11;
                 const double n10 = t10 * p00 + t11 * p10, n11 = t10 * p01 + t11 * p11;
                 t00 = n00; t01 = n01; t10 = n10; t11 = n11;
-                renorm(t00, t01, t10, t11);
             }
         }
         const int src = (warp + 31) & 31;

@@ -960,8 +960,9 @@ __device__ __forceinline__ bool sweep_m1_body(const SweepArgs& A, double* smem_r
 #pragma unroll
                 for (int sy = 0; sy < 4; ++sy) {
                     row_bp(C, T, N, sy, i, ra[sy], rbv[sy], rc[sy], rcm[sy], dir[sy]);
-                    // T_i = [[b_i, -a_i c_{i-1}], [1, 0]]
+                    // T_i = [[b_i, -a_i c_{i-1}], [1, 0]], renormalised as scan_pivots needs
                     m[sy][0] = rbv[sy]; m[sy][1] = -ra[sy] * rcm[sy]; m[sy][2] = 1.0; m[sy][3] = 0.0;
+                    renorm(m[sy][0], m[sy][1], m[sy][2], m[sy][3]);
                 }
             }
             double pp[4], qq[4];
