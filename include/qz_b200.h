@@ -366,6 +366,13 @@ qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const qz_sweep_p
 qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* moments_host, void* stream);
 /* instances, CTAs of the last run, its kernel time (ms), 0 */
 qz_status qz_batch_info(qz_batch* b, double* out4);
+/* Per-instance timeline of the next runs (enable = 1; 0 stops recording): qz_batch_trace then gives, for
+   each instance of the last run in qz_batch_add order, 5 values: the CTA that ran it, its start and end
+   (ms from the first start), ms in its sweeps, ms in its beam phases (moments, pushes, deposits). out
+   holds n >= the instance count rows. The autotuner of quarz_b200.scan fits its cost model to these
+   times. No counterpart in the reference (it runs a scan as separate processes). */
+qz_status qz_batch_set_trace(qz_batch* b, int enable);
+qz_status qz_batch_trace(qz_batch* b, double* out, int n);
 
 #ifdef __cplusplus
 }

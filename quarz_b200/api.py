@@ -562,6 +562,18 @@ class Batch:
         check(lib().qz_batch_info(self.h, _p(v)))
         return {"instances": int(v[0]), "ctas": int(v[1]), "kernel_ms": float(v[2])}
 
+    def set_trace(self, enable: bool = True) -> None:
+        """qz_batch_set_trace: record the per-instance timeline of the next runs."""
+        check(lib().qz_batch_set_trace(self.h, 1 if enable else 0))
+
+    def trace(self) -> np.ndarray:
+        """qz_batch_trace: (instances, 5) of the last traced run, in order of addition: CTA, start ms,
+        end ms, ms in sweeps, ms in beam phases."""
+        n = len(self.specs)
+        out = np.zeros((max(n, 1), 5))
+        check(lib().qz_batch_trace(self.h, _p(out), n))
+        return out[:n]
+
     def __del__(self):
         if getattr(self, "h", None):
             try:

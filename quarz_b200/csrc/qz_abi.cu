@@ -387,6 +387,16 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     s->np = (int)mob[0].size();
     s->npad = ((s->np + 31) / 32) * 32;
     if (s->npad == 0) s->npad = 32;
+    // plasma in global memory (more particles per slice than threads): keep a shared-memory copy of
+    // the particles when a layout leaves room for it (the fastest such layout)
+    A.pcache = 0;
+    if (p->modes == 0 && s->np > qzb::kSweepThreads)
+        for (int i = 0; i < 4; ++i)
+            if (qzb::sweep_m0_smem_bytes(M, kLayouts[i][0], kLayouts[i][1], filter, s->np) <= (size_t)optin) {
+                lay = i;
+                A.pcache = s->np;
+                break;
+            }
     s->nbg = (int)bg[0].size();
     std::vector<double> pinit((size_t)6 * s->npad, 0.0);
     for (int v = 0; v < 6; ++v) std::copy(mob[v].begin(), mob[v].end(), pinit.begin() + (size_t)v * s->npad);
@@ -2192,10 +2202,14 @@ struct qz_batch {
     size_t fld_alloc = 0, diag_alloc = 0, bsrc_alloc = 0, mom_alloc = 0;   // doubles
     float last_ms = 0;
     int last_grid = 0;
+    bool trace = false;                          // qz_batch_set_trace
+    unsigned long long* d_trace = nullptr;
+    size_t trace_n = 0;
+    std::vector<unsigned long long> h_trace;     // the last traced run, kBatchTrace words per instance
     ~qz_batch() {
         for (Inst* i : inst) delete i;
         for (void* q : {(void*)d_inst, (void*)d_order, (void*)d_next, (void*)d_fld, (void*)d_diag, (void*)d_bsrc,
-                        (void*)d_mom})
+                        (void*)d_mom, (void*)d_trace})
             if (q) cudaFree(q);
     }
 };
@@ -2241,13 +2255,21 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
             }
         } else {
             static const bool kLay[4][2] = {{true, true}, {false, true}, {true, false}, {false, false}};
-            int lay = -1;
+            const bool filt = p->smooth_length > 0;
+            int lay = -1, pc = 0;
+            // with plasma in global memory, the fastest layout that also holds the particle copy, if any
+            if (D.sw.np > qzb::kSweepThreads)
+                for (int l = 0; l < 4 && lay < 0; ++l)
+                    if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1], filt, D.sw.np) + reserve <= (size_t)optin) {
+                        lay = l;
+                        pc = D.sw.np;
+                    }
             for (int l = 0; l < 4 && lay < 0; ++l)
-                if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1], p->smooth_length > 0) + reserve <= (size_t)optin)
-                    lay = l;
+                if (qzb::sweep_m0_smem_bytes(M, kLay[l][0], kLay[l][1], filt) + reserve <= (size_t)optin) lay = l;
             if (lay < 0) { delete I; return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep"); }
             D.sw.dbuf = kLay[lay][0];
             D.sw.const_smem = kLay[lay][1];
+            D.sw.pcache = pc;
         }
     }
     D.modes = p->modes;
@@ -2302,7 +2324,7 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
         dmax = std::max(dmax, km * (m1 ? 9 : 3));            // diag (K, M, 9 / 3)
         bmax = std::max(bmax, km * (m1 ? 15 : 5));           // bsrc (K, M, 15 / 5)
         smem = std::max(smem, m1 ? qzb::sweep_m1_smem_bytes(A.M)
-                                 : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0));
+                                 : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0, A.pcache));
         mom_off[i] = mom_total;
         mom_total += (size_t)(nsteps + 1) * std::max(1, b->inst[i]->dev.nbeams) * 17;
     }
@@ -2364,6 +2386,19 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     B.fld = b->d_fld; B.diag = b->d_diag; B.bsrc = b->d_bsrc;
     B.fld_slot = fmax; B.diag_slot = dmax; B.bsrc_slot = bmax;
     B.next = b->d_next;
+    B.trace = nullptr;
+    if (b->trace) {
+        const size_t nt = (size_t)ni * qzb::kBatchTrace;
+        if (b->trace_n < nt) {
+            if (b->d_trace) cudaFree(b->d_trace);
+            b->d_trace = nullptr;
+            b->trace_n = 0;
+            QZ_CUDA(cudaMalloc((void**)&b->d_trace, sizeof(unsigned long long) * nt));
+            b->trace_n = nt;
+        }
+        QZ_CUDA(cudaMemsetAsync(b->d_trace, 0, sizeof(unsigned long long) * nt, st));
+        B.trace = b->d_trace;
+    }
     cudaEvent_t e0, e1;
     QZ_CUDA(cudaEventCreate(&e0));
     QZ_CUDA(cudaEventCreate(&e1));
@@ -2371,11 +2406,40 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     QZ_CUDA(qzb::launch_batch(B, grid, smem, st));
     QZ_CUDA(cudaEventRecord(e1, st));
     if (mom_host) QZ_CUDA(cudaMemcpyAsync(mom_host, b->d_mom, sizeof(double) * mom_total, cudaMemcpyDeviceToHost, st));
+    if (B.trace) {
+        b->h_trace.resize((size_t)ni * qzb::kBatchTrace);
+        QZ_CUDA(cudaMemcpyAsync(b->h_trace.data(), B.trace, sizeof(unsigned long long) * b->h_trace.size(),
+                                cudaMemcpyDeviceToHost, st));
+    }
     QZ_CUDA(cudaStreamSynchronize(st));
     QZ_CUDA(cudaEventElapsedTime(&b->last_ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->last_grid = grid;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_set_trace(qz_batch* b, int enable) {
+    if (!b) return fail(QZ_ERR_ARG, "qz_batch_set_trace: null pointer");
+    b->trace = enable != 0;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_trace(qz_batch* b, double* out, int n) {
+    if (!b || !out || n < 0) return fail(QZ_ERR_ARG, "qz_batch_trace: bad argument");
+    const size_t ni = b->h_trace.size() / qzb::kBatchTrace;
+    if ((size_t)n < ni) return fail(QZ_ERR_SIZE, "qz_batch_trace: out holds fewer instances than the last run");
+    unsigned long long t0 = ~0ull;
+    for (size_t i = 0; i < ni; ++i) t0 = std::min(t0, b->h_trace[i * qzb::kBatchTrace + 1]);
+    for (size_t i = 0; i < ni; ++i) {
+        const unsigned long long* t = b->h_trace.data() + i * qzb::kBatchTrace;
+        double* o = out + i * 5;
+        o[0] = (double)t[0];
+        o[1] = 1e-6 * (double)(t[1] - t0);
+        o[2] = 1e-6 * (double)(t[2] - t0);
+        o[3] = 1e-6 * (double)t[3];
+        o[4] = 1e-6 * (double)t[4];
+    }
     return QZ_OK;
 }
 

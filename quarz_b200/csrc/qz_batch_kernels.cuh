@@ -24,6 +24,12 @@ using beam_detail::sums_add;
 
 constexpr int kT = kSweepThreads;
 
+__device__ __forceinline__ unsigned long long batch_timer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
 // beam work of one instance by the whole CTA: moments (step n) of every beam, then, when push,
 // the push with the fields of step n and the deposit into bsrc (zeroed first)
 __device__ void beam_phase(const BatchInst& I, const SweepArgs& A, const BatchArgs& B, int n, bool push, bool startup,
@@ -129,8 +135,11 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
         __syncthreads();
         const SweepArgs& A = I.sw;
         const bool reg = A.np <= kSweepThreads;
+        unsigned long long t_start = 0, t_mark = 0, t_sweep = 0, t_beam = 0;
+        if (B.trace && tid == 0) t_start = t_mark = batch_timer();
         beam_deposit0(I, A);
         for (int n = 0; n <= B.nsteps; ++n) {
+            if (B.trace && tid == 0) { const unsigned long long t = batch_timer(); t_beam += t - t_mark; t_mark = t; }
             NoGate g;
             if (WITH_M1 && I.modes) {
                 if constexpr (WITH_M1) sweep_m1_body<ORD, NoGate, EXT>(A, smem_raw, g);
@@ -141,9 +150,15 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
                 sweep_body<ORD, false, 4, NoGate, EXT>(A, smem_raw, g);
             }
             __syncthreads();
+            if (B.trace && tid == 0) { const unsigned long long t = batch_timer(); t_sweep += t - t_mark; t_mark = t; }
             beam_phase(I, A, B, n, n < B.nsteps, n == 0, red);
         }
         __syncthreads();
+        if (B.trace && tid == 0) {
+            const unsigned long long t = batch_timer();
+            unsigned long long* o = B.trace + (size_t)B.order[qi] * kBatchTrace;
+            o[0] = blockIdx.x; o[1] = t_start; o[2] = t; o[3] = t_sweep; o[4] = t_beam + (t - t_mark);
+        }
     }
 }
 

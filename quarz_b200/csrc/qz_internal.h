@@ -47,6 +47,8 @@ struct SweepArgs {
     unsigned long long* timing;     // optional: clock cycles per phase [6]
     int dbuf;                       // double-buffered slice sources (push fused with the next deposit)
     int const_smem;                 // per-node constants copied into shared memory
+    int pcache;                     // > 0 (= np, plasma in global memory): a shared-memory copy of the
+                                    // particles' positions, momenta and cells (Smem::pc)
     // modes = 1 only
     int picard;                     // B+ iterations (src/Simulation.cpp:560)
     const double* consts1;          // 9 x M: L1D Thomas 1/u, -a/u, -c/u; L0 rows a b c; L2D rows a b c
@@ -83,7 +85,7 @@ struct SweepArgs {
     double* pout;
 };
 
-size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter = false);
+size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter = false, int pcache = 0);
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
 // the modes = 1 sweep: one CTA, one radial row per thread (M <= kSweepThreads), plasma in A.ps
 size_t sweep_m1_smem_bytes(int M);
@@ -210,7 +212,7 @@ struct PipeArgs {
 constexpr int kTraceStride = 22;
 constexpr int kWorkerTotals = 6;    // trace totals of the push workers after the steps
 
-size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter = false);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter = false, int pcache = 0);
 // resident CTAs of the pipeline kernel on this device (0 if it cannot run); *sms: the SM count
 int pipeline_max_grid(const PipeArgs& P, int* sms);
 // cooperative launch of grid CTAs (fails unless all of them can be resident at once)
@@ -312,7 +314,11 @@ struct BatchArgs {
     double *fld, *diag, *bsrc;      // per slot (= CTA)
     size_t fld_slot, diag_slot, bsrc_slot;
     int* next;                      // queue head (0)
+    // optional, kBatchTrace words per instance (by instance index): the CTA that ran it, %globaltimer at
+    // its start and end, ns in its sweeps, ns in its beam phases
+    unsigned long long* trace;
 };
+constexpr int kBatchTrace = 5;
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t stream);
 int batch_max_grid(int ord, bool with_m1, bool with_ext, size_t smem, int* sms);

@@ -147,8 +147,8 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
     return cudaGetLastError();
 }
 
-size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter) {
-    const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem, filter);
+size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter, int pcache) {
+    const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem, filter, pcache);
     const size_t worker = sizeof(double) * (3 * (size_t)M + (size_t)(kSweepThreads / 32) * 17 * 32) + 64;
     return sweep > worker ? sweep : worker;
 }
@@ -158,7 +158,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
     if (cudaGetDevice(&dev) != cudaSuccess) return 0;
     if (cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return 0;
     *sms = nsm;
-    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0, P.sw.pcache);
     int per = 0;
     switch (P.sw.ord) {
         case 1: per = pipeline_occupancy_ord<1>(P, smem); break;
@@ -174,7 +174,7 @@ int pipeline_max_grid(const PipeArgs& P, int* sms) {
 cudaError_t launch_pipeline(const PipeArgs& P, int grid, cudaStream_t stream) {
     if (P.sw.rows_per_thread < 1 || P.sw.rows_per_thread > 4) return cudaErrorInvalidValue;
     if (P.nsweep < 1 || grid <= P.nsweep || P.ring < 2 || P.nbeams > kMaxBeams) return cudaErrorInvalidValue;
-    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0);
+    const size_t smem = pipeline_smem_bytes(P.modes, P.sw.M, P.sw.dbuf, P.sw.const_smem, P.sw.filter != 0, P.sw.pcache);
     switch (P.sw.ord) {
         case 1: return pipeline_launch_ord<1>(P, grid, smem, stream);
         case 2: return pipeline_launch_ord<2>(P, grid, smem, stream);

@@ -12,11 +12,14 @@ __global__ void __launch_bounds__(kSweepThreads, 1) sweep_m0_kernel(const SweepA
     sweep_body<ORD, REG, kMaxR, NoGate, EXT>(A, smem_raw, g);
 }
 
-size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter) {
+size_t sweep_m0_smem_bytes(int M, bool dbuf, bool const_smem, bool filter, int pcache) {
     size_t d = (size_t)(3 + 2 + 6 + (dbuf ? 18 : 9)) * M + 2 * 8 * (kSweepThreads / 32);
     if (const_smem) d += 13 * (size_t)M;
     if (filter) d += 4 * (size_t)M + 2 * 14 * (kSweepThreads / 32);
-    return sizeof(double) * d + 16 + 4 * 16;       // + lost, flag, 14 exponent maxima and counters, the cells-crossed word
+    // + lost, flag, 14 exponent maxima and counters, the cells-crossed word (128 B with the particle copy
+    // behind them: 6 doubles and a cell index per particle)
+    if (pcache > 0) return sizeof(double) * d + 128 + (size_t)pcache * (6 * sizeof(double) + sizeof(int));
+    return sizeof(double) * d + 16 + 4 * 16;
 }
 
 namespace {
@@ -45,7 +48,7 @@ cudaError_t launch_o(const SweepArgs& A, size_t smem, cudaStream_t stream) {
 
 cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream) {
     if (A.rows_per_thread < 1 || A.rows_per_thread > 4) return cudaErrorInvalidValue;
-    const size_t smem = sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0);
+    const size_t smem = sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0, A.pcache);
     switch (A.ord) {
         case 1: return launch_o<1>(A, smem, stream);
         case 2: return launch_o<2>(A, smem, stream);

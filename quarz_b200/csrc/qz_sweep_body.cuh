@@ -427,6 +427,11 @@ struct Smem {
     // counters: [11] extra sub-slices, [12] particles removed as trapped, [13] non-finite deposits
     int* fx;
     unsigned long long* cmax;                             // most cells crossed (sub-slicing), as double bits
+    // A.pcache > 0 (plasma in global memory, np = A.pcache): a copy of every particle's x y px py Delta w
+    // (pc, 6 x np) and its radial cell (pj), written through with the global state whenever a particle
+    // moves; the passes that only read the particles take them from here, without a cell search
+    double* pc;
+    int* pj;
 };
 
 __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
@@ -451,6 +456,8 @@ __device__ __forceinline__ Smem carve(double* base, const SweepArgs& A) {
     S.flag = S.lost + 1;
     S.fx = S.lost + 2;
     S.cmax = reinterpret_cast<unsigned long long*>(S.lost + 16);
+    S.pc = A.pcache ? reinterpret_cast<double*>(reinterpret_cast<char*>(S.lost) + 128) : nullptr;
+    S.pj = A.pcache ? reinterpret_cast<int*>(S.pc + 6 * (size_t)A.pcache) : nullptr;
     return S;
 }
 
@@ -709,6 +716,41 @@ __device__ __forceinline__ void pstore(const PState<ORD>& P, double* __restrict_
     for (int m = 0; m < ORD; ++m)
 #pragma unroll
         for (int v = 0; v < 5; ++v) ps[(6 + (size_t)m * 5 + v) * npad + p] = P.h[m][v];
+}
+
+// x y px py Delta w of particle p: from the shared copy (A.pcache) or from the global state
+template <int ORD>
+__device__ __forceinline__ void pbase(PState<ORD>& P, const Smem& S, const SweepArgs& A, const double* __restrict__ ps,
+                                      int npad, int p) {
+    if (A.pcache) {
+        const size_t n = (size_t)A.pcache;
+        P.x = S.pc[p]; P.y = S.pc[n + p]; P.px = S.pc[2 * n + p]; P.py = S.pc[3 * n + p];
+        P.dl = S.pc[4 * n + p]; P.w = S.pc[5 * n + p];
+    } else {
+        P.x = ps[p]; P.y = ps[npad + p]; P.px = ps[2 * (size_t)npad + p]; P.py = ps[3 * (size_t)npad + p];
+        P.dl = ps[4 * (size_t)npad + p]; P.w = ps[5 * (size_t)npad + p];
+    }
+}
+template <int ORD>
+__device__ __forceinline__ void pbase_put(const PState<ORD>& P, const Smem& S, const SweepArgs& A, int p) {
+    if (!A.pcache) return;
+    const size_t n = (size_t)A.pcache;
+    S.pc[p] = P.x; S.pc[n + p] = P.y; S.pc[2 * n + p] = P.px; S.pc[3 * n + p] = P.py;
+    S.pc[4 * n + p] = P.dl; S.pc[5 * n + p] = P.w;
+}
+// AB history of particle p from the global state
+template <int ORD>
+__device__ __forceinline__ void phist(PState<ORD>& P, const double* __restrict__ ps, int npad, int p) {
+#pragma unroll
+    for (int m = 0; m < ORD; ++m)
+#pragma unroll
+        for (int v = 0; v < 5; ++v) P.h[m][v] = ps[(6 + (size_t)m * 5 + v) * npad + p];
+}
+
+// the geometry of particle p at (x, y): from its kept cell (A.pcache; the cell locate() would find) or by
+// the search
+__device__ __forceinline__ PGeo pgeo(const Smem& S, const SweepArgs& A, int N, double R, int p, double x, double y) {
+    return A.pcache ? geometry_in(S.r, S.ih, x, y, S.pj[p]) : geometry(S.r, S.ih, N, R, x, y);
 }
 
 __device__ __forceinline__ void species_params(const SweepArgs& A, int p, double& q, double& qm) {
@@ -1147,6 +1189,11 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                 for (int v = 0; v < 6; ++v) gate.ps(A)[(size_t)v * npad + p] = A.p_init[(size_t)v * npad + p];
                 for (int v = 0; v < 5 * ORD; ++v) gate.ps(A)[(size_t)(6 + v) * npad + p] = 0.0;
             }
+            if (A.pcache) {
+                const double* src = A.pin ? A.pin : A.p_init;
+#pragma unroll
+                for (int v = 0; v < 6; ++v) S.pc[(size_t)v * A.pcache + p] = src[(size_t)v * npad + p];
+            }
         }
     }
     __syncthreads();
@@ -1259,11 +1306,14 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                     int j = 0;
                     double v[12];
                     if (p < np) {
-                        pload(Q, gate.ps(A), npad, p);
+                        pbase(Q, S, A, gate.ps(A), npad, p);
                         species_params(A, p, Q.q, Q.qm);
                         act = Q.w != 0.0;
                         if (act) {
-                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                            // the first pass searches the cell and keeps it for the later passes
+                            const PGeo g = pass == 0 ? geometry(S.r, S.ih, N, R, Q.x, Q.y)
+                                                     : pgeo(S, A, N, R, p, Q.x, Q.y);
+                            if (pass == 0 && A.pcache) S.pj[p] = g.j;
                             j = g.j;
                             deposit_values(Q, g, S, v);
                         }
@@ -1469,11 +1519,11 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                     double v[4];
                     if (p < np) {
                         PState<ORD> Q;
-                        pload(Q, gate.ps(A), npad, p);
+                        pbase(Q, S, A, gate.ps(A), npad, p);
                         species_params(A, p, Q.q, Q.qm);
                         act = Q.w != 0.0;
                         if (act) {
-                            const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                            const PGeo g = pgeo(S, A, N, R, p, Q.x, Q.y);
                             j = g.j;
                             depositS_values(Q, g, S, N, v);
                         }
@@ -1697,14 +1747,22 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                         double v[12];
                         PState<ORD> Q;
                         if (p < np) {
-                            pload(Q, gate.ps(A), npad, p);
+                            pbase(Q, S, A, gate.ps(A), npad, p);
                             species_params(A, p, Q.q, Q.qm);
                             if (Q.w != 0.0) {
                                 if (pass == 0) {
-                                    const PGeo g = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                    phist(Q, gate.ps(A), npad, p);
+                                    const PGeo g = pgeo(S, A, N, R, p, Q.x, Q.y);
                                     const int pr = push_particle(Q, g, S, A, first, abc, hstep);
                                     if (pr > 0) {
-                                        const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                        PGeo g2;
+                                        if (A.pcache) {        // the new cell by a short walk from the old one
+                                            const int jn = locate_from(S.r, N, R, sqrt(Q.x * Q.x + Q.y * Q.y), g.j);
+                                            g2 = geometry_in(S.r, S.ih, Q.x, Q.y, jn);
+                                            S.pj[p] = jn;
+                                        } else {
+                                            g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                        }
                                         j = g2.j;
                                         deposit_values(Q, g2, S, v);
                                         act = true;
@@ -1713,8 +1771,9 @@ __device__ __forceinline__ bool sweep_body(const SweepArgs& A, double* smem_raw,
                                         if (pr < 0) atomicAdd(S.fx + 12, 1);
                                     }
                                     pstore(Q, gate.ps(A), npad, p);
+                                    pbase_put(Q, S, A, p);
                                 } else {
-                                    const PGeo g2 = geometry(S.r, S.ih, N, R, Q.x, Q.y);
+                                    const PGeo g2 = pgeo(S, A, N, R, p, Q.x, Q.y);
                                     j = g2.j;
                                     deposit_values(Q, g2, S, v);
                                     act = true;
