@@ -366,10 +366,19 @@ qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const qz_sweep_p
 qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* moments_host, void* stream);
 /* instances, CTAs of the last run, its kernel time (ms), 0 */
 qz_status qz_batch_info(qz_batch* b, double* out4);
+/* The tuning of instance `index` (from qz_batch_add): its shared-memory layout for modes = 0, a bit set
+   (1: double-buffered slice sources, 2: per-node constants in shared memory, 4: the copy of plasma kept in
+   global memory, np > 512), or -1 to keep the current one; and its cost, the key of the largest-first
+   queue, or <= 0 to keep it. qz_batch_add picks the fastest layout that fits and the estimate
+   K (M + 4 np) + 2 N_beam; the autotuner (quarz_b200.tune) measures both instead. Fails with QZ_ERR_SIZE
+   for a layout that does not fit the device's shared memory. qz_batch_tuning reads them back.
+   No counterpart in the reference. */
+qz_status qz_batch_set_tuning(qz_batch* b, int index, int layout, double cost);
+qz_status qz_batch_tuning(qz_batch* b, int index, int* layout, double* cost);
 /* Per-instance timeline of the next runs (enable = 1; 0 stops recording): qz_batch_trace then gives, for
    each instance of the last run in qz_batch_add order, 5 values: the CTA that ran it, its start and end
    (ms from the first start), ms in its sweeps, ms in its beam phases (moments, pushes, deposits). out
-   holds n >= the instance count rows. The autotuner of quarz_b200.scan fits its cost model to these
+   holds n >= the instance count rows. The autotuner (quarz_b200.tune) fits its cost model to these
    times. No counterpart in the reference (it runs a scan as separate processes). */
 qz_status qz_batch_set_trace(qz_batch* b, int enable);
 qz_status qz_batch_trace(qz_batch* b, double* out, int n);

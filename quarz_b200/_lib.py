@@ -121,6 +121,8 @@ SIGNATURES = {
     "qz_batch_run": [C.c_void_p, C.c_int, C.c_double, _dp, C.c_void_p],
     "qz_batch_info": [C.c_void_p, _dp],
     "qz_batch_set_trace": [C.c_void_p, C.c_int],
+    "qz_batch_set_tuning": [C.c_void_p, C.c_int, C.c_int, C.c_double],
+    "qz_batch_tuning": [C.c_void_p, C.c_int, C.POINTER(C.c_int), _dp],
     "qz_batch_trace": [C.c_void_p, _dp, C.c_int],
 }
 

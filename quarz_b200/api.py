@@ -562,6 +562,17 @@ class Batch:
         check(lib().qz_batch_info(self.h, _p(v)))
         return {"instances": int(v[0]), "ctas": int(v[1]), "kernel_ms": float(v[2])}
 
+    def set_tuning(self, index: int, layout: int = -1, cost: float = 0.0) -> None:
+        """qz_batch_set_tuning: instance `index`'s shared-memory layout (bits: 1 double-buffered sources,
+        2 constants in shared memory, 4 particle copy; -1 keeps it) and queue cost (<= 0 keeps it)."""
+        check(lib().qz_batch_set_tuning(self.h, int(index), int(layout), float(cost)))
+
+    def tuning(self, index: int) -> Tuple[int, float]:
+        """qz_batch_tuning: (layout bits or -1 for modes = 1, queue cost) of instance `index`."""
+        lay, cost = C.c_int(), np.zeros(1)
+        check(lib().qz_batch_tuning(self.h, int(index), C.byref(lay), _p(cost)))
+        return lay.value, float(cost[0])
+
     def set_trace(self, enable: bool = True) -> None:
         """qz_batch_set_trace: record the per-instance timeline of the next runs."""
         check(lib().qz_batch_set_trace(self.h, 1 if enable else 0))

@@ -1313,10 +1313,21 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     const int wmin = std::max(8, (2 * g1) / 5);             // measured best: ~2/5 of the SMs push
     int nsweep = P_.sweep_ctas > 0 ? P_.sweep_ctas : std::min(nsteps + 1, g1 - wmin);
     nsweep = std::max(1, std::min({nsweep, nsteps + 1, g1 - 1}));
-    const int ring = rec ? std::max(2, nsteps + 1) : std::max(2, std::min(nsteps + 1, nsweep + 2));
     // 3. buffers
     const size_t KM = (size_t)K * M;
     const size_t bslot = sim_bsrc_doubles(s);           // a beam-source slot: two limbs per value for m = 0
+    // ring slots: one per step in flight; one per step of the run when that fits in half the free memory,
+    // which lets the push workers read the field rows through L1 (PipeArgs::fld_l1)
+    int ring = rec ? std::max(2, nsteps + 1) : std::max(2, std::min(nsteps + 1, nsweep + 2));
+    if (ring < nsteps + 1 && P_.ring >= nsteps + 1) {
+        ring = nsteps + 1;                              // the rings already hold a slot per step
+    } else if (ring < nsteps + 1) {
+        size_t fr = 0, tot = 0;
+        const size_t per = sizeof(double) * (KM * (s->fnc + s->dnc) + bslot);
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess && (size_t)(nsteps + 1 - std::max(P_.ring, 0)) * per < fr / 2)
+            ring = nsteps + 1;
+        cudaGetLastError();
+    }
     if (P_.ring < ring) {
         for (double* q : {P_.fld, P_.diag, P_.bsrc})
             if (q) cudaFree(q);
@@ -1361,6 +1372,7 @@ qz_status run_pipelined(qz_sim* s, int nsteps, double dt, double* mom_host, cuda
     A.nsteps = nsteps;
     A.nsweep = nsweep;
     A.ring = ring;
+    A.fld_l1 = (ring >= nsteps + 1 && (M * s->fnc) % 16 == 0) ? 1 : 0;
     A.fld_slot = KM * s->fnc;
     A.diag_slot = KM * s->dnc;
     A.bsrc_slot = bslot;
@@ -2416,6 +2428,39 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     b->last_grid = grid;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_set_tuning(qz_batch* b, int index, int layout, double cost) {
+    if (!b || index < 0 || index >= (int)b->inst.size()) return fail(QZ_ERR_ARG, "qz_batch_set_tuning: bad index");
+    auto* I = b->inst[index];
+    if (cost > 0.0) I->cost = cost;
+    if (layout < 0) return QZ_OK;
+    qzb::SweepArgs& A = I->dev.sw;
+    if (I->dev.modes != 0 || layout > 7) return fail(QZ_ERR_ARG, "qz_batch_set_tuning: layouts are for modes = 0 (0..7)");
+    const bool dbuf = layout & 1, cs = (layout >> 1) & 1, pc = (layout >> 2) & 1;
+    if (pc && A.np <= qzb::kSweepThreads)
+        return fail(QZ_ERR_ARG, "qz_batch_set_tuning: the particle copy is for plasma in global memory (np > 512)");
+    int dev = 0, optin = 0;
+    QZ_CUDA(cudaGetDevice(&dev));
+    QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+    const size_t reserve = sizeof(qzb::BatchInst) + sizeof(double) * 17 * (qzb::kSweepThreads / 32) + 256;
+    if (qzb::sweep_m0_smem_bytes(A.M, dbuf, cs, A.filter != 0, pc ? A.np : 0) + reserve > (size_t)optin)
+        return fail(QZ_ERR_SIZE, "qz_batch_set_tuning: layout " + std::to_string(layout) + " does not fit M = " +
+                                     std::to_string(A.M));
+    A.dbuf = dbuf;
+    A.const_smem = cs;
+    A.pcache = pc ? A.np : 0;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_batch_tuning(qz_batch* b, int index, int* layout, double* cost) {
+    if (!b || index < 0 || index >= (int)b->inst.size() || !layout || !cost)
+        return fail(QZ_ERR_ARG, "qz_batch_tuning: bad argument");
+    const auto* I = b->inst[index];
+    const qzb::SweepArgs& A = I->dev.sw;
+    *layout = I->dev.modes ? -1 : (A.dbuf ? 1 : 0) | (A.const_smem ? 2 : 0) | (A.pcache ? 4 : 0);
+    *cost = I->cost;
     return QZ_OK;
 }
 

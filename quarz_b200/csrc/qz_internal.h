@@ -170,6 +170,10 @@ struct PipeArgs {
     int nsteps;                     // sweeps 0..nsteps, pushes 0..nsteps-1
     int nsweep;                     // CTAs running sweeps
     int ring;                       // slots of the field / diagnostics / beam-source rings
+    // the push workers gather the fields through L1: set when no field slot is reused within the run
+    // (ring > nsteps) and every field row starts on a 128-byte line, so no cached line can hold a row
+    // before the sweep published it (rows are only read once published, and kernels start with L1 clean)
+    int fld_l1;
     int modes, bnc;                 // azimuthal modes (0 / 1), beam-source components per node
     size_t fld_slot, diag_slot, bsrc_slot, ps_slot;   // doubles per slot (ps: per sweep CTA)
     double *fld, *diag, *bsrc, *ps;

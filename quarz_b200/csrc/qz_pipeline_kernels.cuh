@@ -388,7 +388,8 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                             bool alive = true;
                             int jg = 0;
                             if (!rigid) {
-                                alive = push_one<true>(Bb, fld, p, h, hs, P.dt_drift, &jg);
+                                alive = P.fld_l1 ? push_one<false>(Bb, fld, p, h, hs, P.dt_drift, &jg)
+                                                 : push_one<true>(Bb, fld, p, h, hs, P.dt_drift, &jg);
                                 __stcg(Bb.x + i, p.x); __stcg(Bb.y + i, p.y);
                                 __stcg(Bb.px + i, p.px); __stcg(Bb.py + i, p.py); __stcg(Bb.pz + i, p.pz);
                                 __stcg(Bb.xi + i, p.xi);
@@ -424,7 +425,8 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 cmax = max(cmax, xi_cell(Bb, p.xi));
                 continue;
             }
-            const bool alive = push_one<true>(Bb, fld, p, h, hs, P.dt_drift);
+            const bool alive = P.fld_l1 ? push_one<false>(Bb, fld, p, h, hs, P.dt_drift)
+                                        : push_one<true>(Bb, fld, p, h, hs, P.dt_drift);
             __stcg(Bb.x + i, p.x); __stcg(Bb.y + i, p.y);
             __stcg(Bb.px + i, p.px); __stcg(Bb.py + i, p.py); __stcg(Bb.pz + i, p.pz);
             __stcg(Bb.xi + i, p.xi);

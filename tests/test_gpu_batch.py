@@ -96,3 +96,34 @@ def test_batch_with_smoothing():
     for i in (0, 3):
         s, bm, mom = specs[i], beams[i], moms[i]
         _close(s, mom, O.OracleSim(s, beams=bm).run(2, s.dt), bm, 1e-8)
+
+
+def test_autotuned_batch_equals_default_batch():
+    # the autotuner (quarz_b200.tune) measures every candidate layout of each size class on representatives
+    # and reorders the queue by measured cost; the tuned batch computes the same runs: every layout gives
+    # the same moments to rounding (1e-10 of their natural scale), the queue order none at all
+    from quarz_b200 import tune
+
+    specs = workloads.scan_instances(12, seed=21, beam_particles=4000, steps=3)
+    assert min(s.M for s in specs) <= 513 < max(s.M for s in specs)
+    beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
+    base = Q.Batch()
+    for s, bm in zip(specs, beams):
+        base.add(s, bm)
+    ref = base.run(3, specs[0].dt)
+    tuned, t = tune.tuned_batch(specs, beams, 3, specs[0].dt, steps=1)
+    assert set(t.layouts) == {tune.size_class(s) for s in specs}
+    for i, s in enumerate(specs):
+        lay, cost = tuned.tuning(i)
+        assert lay == t.layout(s) and cost > 0
+        if tune.plasma_per_slice(s) <= tune.REG_PARTICLES:
+            assert not (lay & 4)
+    tuned.set_trace(True)
+    moms = tuned.run(3, specs[0].dt)
+    tr = tuned.trace()
+    assert np.all(tr[:, 2] >= tr[:, 1]) and np.all(tr[:, 3] > 0)
+    for s, bm, mom, r in zip(specs, beams, moms, ref):
+        _close(s, mom, r, bm, 1e-10)
+    # a saved tuning gives the same choices
+    again = tune.Tuning.from_json(t.to_json())
+    assert again.layouts == t.layouts and again.sweep_us == t.sweep_us
