@@ -158,6 +158,21 @@ typedef struct {
 /* adds the beam's sources to bsrc (dev, (K, M, B_NC)); bsrc is NOT cleared */
 qz_status qz_beam_deposit(const qz_grid* g, const qz_beam_view* b, const qz_box* box, double* bsrc_dev,
                           void* stream);
+/* Exact beam sources outside qz_sim (a staged run): the node quanta of the two-limb format qz_sim's m = 0
+   runs use (qz_sim_set_exact), for up to nparticles beam particles whose weights satisfy
+   sum over beams of max |w q| <= wq. qz_beam_deposit_fx adds a beam into bsrc2 (dev, 2 x K x M x B_NC0:
+   the high limbs, then the low limbs; zero it first) with them; qz_sweep_set_exact_sources(s, fx) makes
+   s read its bsrc, and a stage's guard row (2 x M x B_NC0), in that format (NULL: plain doubles again).
+   Sums of integer limbs do not depend on the order of the adds, so slabs that deposit their own particles
+   give the beam sources of the whole box bit for bit: a staged run then equals the single-GPU run in its
+   fields and particles, as the reference's pipelined MPI run does (README.md:1755-1758). modes = 0.
+   No counterpart in the reference (its deposits are atomic FP64 adds). */
+typedef struct qz_fx qz_fx;
+qz_status qz_fx_create(const qz_grid* g, double dxi, double wq, int64_t nparticles, qz_fx** out);
+qz_status qz_fx_destroy(qz_fx* fx);
+qz_status qz_beam_deposit_fx(const qz_grid* g, const qz_beam_view* b, const qz_box* box, const qz_fx* fx,
+                             double* bsrc2_dev, void* stream);
+qz_status qz_sweep_set_exact_sources(qz_sweep* s, const qz_fx* fx);
 /* advance by dt (move = 1) or the explicit start-up kick (move = 0) with the fields fld (dev) */
 qz_status qz_beam_advance(const qz_grid* g, qz_beam_view* b, const qz_box* box, const double* fld_dev,
                           double dt_kick, double dt_drift, int move, void* stream);

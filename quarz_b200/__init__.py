@@ -15,8 +15,8 @@ There is no CPU fallback: if the library cannot be loaded every entry point rais
 from __future__ import annotations
 
 from ._lib import QZError, lib, library_path  # noqa: F401
-from .api import (Batch, BeamOps, RadialGrid, Simulation, Sweep, analytic_beam, sample_beam,  # noqa: F401
+from .api import (Batch, BeamOps, ExactSources, RadialGrid, Simulation, Sweep, analytic_beam, sample_beam,  # noqa: F401
                   sample_gaussian, slice_table, sweep_params, write_fields)
 
-__all__ = ["QZError", "lib", "library_path", "RadialGrid", "Sweep", "BeamOps", "Simulation", "Batch",
+__all__ = ["QZError", "lib", "library_path", "RadialGrid", "Sweep", "BeamOps", "ExactSources", "Simulation", "Batch",
            "sample_gaussian", "sample_beam", "sweep_params", "slice_table", "analytic_beam", "write_fields"]

@@ -75,6 +75,10 @@ SIGNATURES = {
                            C.POINTER(PlasmaState), C.POINTER(Counters), C.c_void_p],
     "qz_sweep_timing": [C.c_void_p, C.c_int, C.POINTER(C.c_ulonglong)],
     "qz_beam_deposit": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_void_p],
+    "qz_fx_create": [C.c_void_p, C.c_double, C.c_double, C.c_int64, C.POINTER(C.c_void_p)],
+    "qz_fx_destroy": [C.c_void_p],
+    "qz_beam_deposit_fx": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_void_p, C.c_void_p],
+    "qz_sweep_set_exact_sources": [C.c_void_p, C.c_void_p],
     "qz_beam_advance": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,
                         C.c_int, C.c_void_p],
     "qz_beam_push": [C.c_void_p, C.POINTER(BeamView), C.POINTER(Box), C.c_void_p, C.c_double, C.c_double,

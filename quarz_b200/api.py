@@ -95,6 +95,36 @@ def sweep_params(spec: "_deck.RunSpec") -> SweepParams:
 
 
 # ---------------------------------------------------------------- sweep
+class ExactSources:
+    """The node quanta of exact (two-limb, order-independent) beam sources (qz_fx): for beams whose
+    sum over beams of max |w q| is at most wq and that hold at most nparticles particles in all."""
+
+    def __init__(self, grid: RadialGrid, dxi: float, wq: float, nparticles: int):
+        self.grid = grid
+        h = C.c_void_p()
+        check(lib().qz_fx_create(grid.h, float(dxi), float(wq), int(nparticles), C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def bound(beams, charges) -> Tuple[float, int]:
+        """(wq, particles) of beams given as (n, 7) rows (weight last) with their charges, in the order
+        qz_sim sums them."""
+        wq, n = 0.0, 0
+        for rows, q in zip(beams, charges):
+            if len(rows):
+                wq += float(np.max(np.abs(rows[:, 6]))) * abs(float(q))
+            n += len(rows)
+        return wq, n
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            try:
+                lib().qz_fx_destroy(self.h)
+            except Exception:
+                pass
+            self.h = None
+
+
 class Sweep:
     """One quasi-static sweep per call (qz_sweep)."""
 
@@ -111,6 +141,12 @@ class Sweep:
         self.last_counters = {"lost": int(cnt.lost), "nonfinite": int(cnt.nonfinite), "trapped": int(cnt.trapped),
                               "subslices": int(cnt.subslices)}
         return int(cnt.lost)
+
+    def set_exact_sources(self, fx: Optional["ExactSources"]) -> None:
+        """qz_sweep_set_exact_sources: read bsrc (2, K, M, 5) and the guard row (2, M, 5) as exact limbs
+        (None: plain doubles)."""
+        check(lib().qz_sweep_set_exact_sources(self.h, fx.h if fx is not None else None))
+        self._fx = fx
 
     def run_async(self, bsrc, fld, diag, stream=None) -> None:
         check(lib().qz_sweep_run(self.h, _dev(bsrc), _dev(fld), _dev(diag), None, _stream_ptr(stream)))
@@ -195,6 +231,12 @@ class BeamOps:
     def deposit(grid: RadialGrid, cols, q, m, box: Box, bsrc, stream=None):
         v = BeamOps.view(cols, q, m)
         check(lib().qz_beam_deposit(grid.h, C.byref(v), C.byref(box), _dev(bsrc), _stream_ptr(stream)))
+
+    @staticmethod
+    def deposit_fx(grid: RadialGrid, cols, q, m, box: Box, fx: ExactSources, bsrc2, stream=None):
+        """qz_beam_deposit_fx: adds the beam into exact two-limb sources bsrc2 (2, K, M, 5)."""
+        v = BeamOps.view(cols, q, m)
+        check(lib().qz_beam_deposit_fx(grid.h, C.byref(v), C.byref(box), fx.h, _dev(bsrc2), _stream_ptr(stream)))
 
     @staticmethod
     def advance(grid, cols, q, m, box, fld, dt_kick, dt_drift, move, stream=None, pusher: int = 0):

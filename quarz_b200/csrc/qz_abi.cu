@@ -233,8 +233,20 @@ extern "C" qz_status qz_grid_operator(const qz_grid* g, int op, double* a, doubl
 }
 
 // ===================================================================== sweep
+// node quanta of the exact beam deposits (qz_fx_create): 2^-qe_j (scales) then 2^qe_j (quanta), the split S
+struct qz_fx {
+    int M = 0;
+    int S = 0;
+    std::vector<int> qe;
+    double* d_q = nullptr;
+    ~qz_fx() {
+        if (d_q) cudaFree(d_q);
+    }
+};
+
 struct qz_sweep {
     const qz_grid* g = nullptr;
+    const qz_fx* fx = nullptr;            // qz_sweep_set_exact_sources: bsrc in the two-limb format
     qz_sweep_params p{};
     int np = 0, npad = 0, nbg = 0;
     double* d_pinit = nullptr;
@@ -500,6 +512,11 @@ qz_status sweep_launch(qz_sweep* s, const double* bsrc, double* fld, double* dia
     A.bq = x.bq;
     A.bfx_2s = x.bfx_2s;
     A.bfx_lo = x.bfx_lo;
+    if (!x.bq && s->fx && s->p.modes == 0) {          // the caller's sources in the two-limb format
+        A.bq = s->fx->d_q + s->g->M;
+        A.bfx_2s = std::ldexp(1.0, s->fx->S);
+        A.bfx_lo = (long)s->p.K * s->g->M * qzb::B_NC0;
+    }
     A.pin = x.pin;
     A.pin_pushed = x.pin_pushed;
     A.bguard = x.bguard;
@@ -1061,6 +1078,36 @@ namespace {
 // S = 53 - nbits and B = 2 S keep both limb sums integers below 2^53 (exact in FP64, beam_fx_add).
 // The run deposits exactly for m = 0 up to 2^25 particles (B >= 56: the quantum is at most 2^-56 of
 // the bound); m = 1 runs and larger beams keep FP64 reductions.
+// the node quanta for n contributions bounded by wq (sum over beams of max |w q|): every contribution to
+// node j is below bound_j = 2 wq / V_j / dxi < 2^(qe_j + B); S = 53 - nbits and B = 2 S with 2^nbits > n.
+// False beyond 2^25 contributions (the quantum would exceed 2^-56 of the bound).
+bool fx_quanta(const qz_grid* g, double dxi, double wq, long ntot, std::vector<int>& qe, int& S) {
+    int nbits = 1;
+    while (nbits < 62 && (1L << nbits) <= ntot) ++nbits;
+    if (nbits > 25) return false;
+    S = 53 - nbits;
+    const int B = 2 * S;
+    qe.assign(g->M, 0);
+    for (int j = 0; j < g->M; ++j) {
+        const double bound = 2.0 * wq * g->inv_V[j] / dxi;
+        int e = 0;
+        if (bound > 0.0 && std::isfinite(bound)) std::frexp(bound, &e);    // bound < 2^e
+        qe[j] = e - B;
+    }
+    return true;
+}
+
+qz_status fx_upload(const std::vector<int>& qe, double* d_q) {
+    const size_t M = qe.size();
+    std::vector<double> q(2 * M);
+    for (size_t j = 0; j < M; ++j) {
+        q[j] = std::ldexp(1.0, -qe[j]);
+        q[M + j] = std::ldexp(1.0, qe[j]);
+    }
+    QZ_CUDA(cudaMemcpy(d_q, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
+    return QZ_OK;
+}
+
 qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     auto& F = s->fx;
     const bool was = F.on;
@@ -1070,10 +1117,11 @@ qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     const int M = s->g->M;
     long ntot = 0;
     for (const auto& b : s->beams) ntot += (long)b.n;
-    int nbits = 1;
-    while (nbits < 62 && (1L << nbits) <= ntot) ++nbits;
-    if (nbits > 25) return QZ_OK;                   // beyond 2^25 particles: FP64 reductions
-    const int S = 53 - nbits, B = 2 * S;
+    {
+        std::vector<int> probe;
+        int Sp = 0;
+        if (!fx_quanta(s->g, s->p.dxi, 1.0, ntot, probe, Sp)) return QZ_OK;   // beyond 2^25: FP64 reductions
+    }
     if (!F.d_wmax && cudaMalloc((void**)&F.d_wmax, sizeof(double) * qzb::kMaxBeams * 2) != cudaSuccess) {
         F.d_wmax = nullptr;
         return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");
@@ -1091,24 +1139,15 @@ qz_status fx_prepare(qz_sim* s, cudaStream_t st) {
     QZ_CUDA(cudaStreamSynchronize(st));
     if ((int)s->beams.size() > nb) return QZ_OK;    // more beams than bounds: FP64 reductions
     for (int b = 0; b < nb; ++b) wq += wm[b] * std::fabs(s->beams[b].q);
-    std::vector<int> qe(M, 0);
-    for (int j = 0; j < M; ++j) {
-        const double bound = 2.0 * wq * s->g->inv_V[j] / s->p.dxi;
-        int e = 0;
-        if (bound > 0.0 && std::isfinite(bound)) std::frexp(bound, &e);    // bound < 2^e
-        qe[j] = e - B;
-    }
+    std::vector<int> qe;
+    int S = 0;
+    fx_quanta(s->g, s->p.dxi, wq, ntot, qe, S);
     if (!F.d_q && cudaMalloc((void**)&F.d_q, sizeof(double) * 2 * M) != cudaSuccess) {
         F.d_q = nullptr;
         return fail(QZ_ERR_NOMEM, "qz_sim_run: device allocation failed (deposit bounds)");
     }
     if (qe != F.qe || F.S != S) {
-        std::vector<double> q(2 * (size_t)M);
-        for (int j = 0; j < M; ++j) {
-            q[j] = std::ldexp(1.0, -qe[j]);
-            q[M + j] = std::ldexp(1.0, qe[j]);
-        }
-        QZ_CUDA(cudaMemcpy(F.d_q, q.data(), sizeof(double) * q.size(), cudaMemcpyHostToDevice));
+        if (qz_status e = fx_upload(qe, F.d_q)) return e;
         F.qe = qe;
         s->bsrc_valid = false;                      // sources kept from the last run used other quanta
     }
@@ -1178,7 +1217,15 @@ qz_status sim_push_deposit(qz_sim* s, qz_sim::Beam& b, double dt_kick, double dt
         QZ_CUDA(qzb::launch_beam_push(B, s->d_fld, -0.5 * dt_kick, -0.5 * dt_kick, 0, st));
         b.started = 1;
     }
-    QZ_CUDA(qzb::launch_beam_push_deposit(B, s->d_fld, dt_kick, dt_drift, bsrc_next, st));
+    if (B.fx_scale) {
+        // exact sources: deposit the stored particles with the deposit kernel, so that any path that
+        // deposits the same particles (a staged run's slabs, qz_beam_deposit_fx) gives the same limbs (the
+        // fused kernel shares subexpressions with the push and rounds the deposit values differently)
+        QZ_CUDA(qzb::launch_beam_push(B, s->d_fld, dt_kick, dt_drift, 1, st));
+        QZ_CUDA(qzb::launch_beam_deposit(B, bsrc_next, st));
+    } else {
+        QZ_CUDA(qzb::launch_beam_push_deposit(B, s->d_fld, dt_kick, dt_drift, bsrc_next, st));
+    }
     return QZ_OK;
 }
 
@@ -1922,6 +1969,53 @@ extern "C" qz_status qz_sim_restart(qz_sim* s) {
 extern "C" qz_status qz_sim_set_adjoint_checkpoint(qz_sim* s, int every) {
     if (!s || every < 0) return fail(QZ_ERR_ARG, "qz_sim_set_adjoint_checkpoint: bad argument");
     s->ckpt_every = every;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_fx_create(const qz_grid* g, double dxi, double wq, int64_t nparticles, qz_fx** out) {
+    if (!g || !out || !(dxi > 0.0) || !(wq >= 0.0) || nparticles < 0) return fail(QZ_ERR_ARG, "qz_fx_create: bad argument");
+    auto* f = new (std::nothrow) qz_fx;
+    if (!f) return fail(QZ_ERR_NOMEM, "qz_fx_create: out of host memory");
+    f->M = g->M;
+    if (!fx_quanta(g, dxi, wq, (long)nparticles, f->qe, f->S)) {
+        delete f;
+        return fail(QZ_ERR_UNSUPPORTED, "qz_fx_create: exact deposits take at most 2^25 beam particles");
+    }
+    if (cudaMalloc((void**)&f->d_q, sizeof(double) * 2 * g->M) != cudaSuccess) {
+        cudaGetLastError();
+        f->d_q = nullptr;
+        delete f;
+        return fail(QZ_ERR_NOMEM, "qz_fx_create: device allocation failed");
+    }
+    if (qz_status e = fx_upload(f->qe, f->d_q)) { delete f; return e; }
+    *out = f;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_fx_destroy(qz_fx* f) {
+    delete f;
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_beam_deposit_fx(const qz_grid* g, const qz_beam_view* b, const qz_box* box, const qz_fx* fx,
+                                        double* bsrc2, void* stream) {
+    if (qz_status st = check_beam(g, b, box)) return st;
+    if (!fx || !bsrc2) return fail(QZ_ERR_ARG, "qz_beam_deposit_fx: null pointer");
+    if (box->modes != 0 || fx->M != g->M) return fail(QZ_ERR_ARG, "qz_beam_deposit_fx: modes = 0 and the grid of fx");
+    qzb::BeamArgs B = beam_args(g, b, box);
+    B.fx_scale = fx->d_q;
+    B.fx_inv2s = std::ldexp(1.0, -fx->S);
+    B.fx_2s = std::ldexp(1.0, fx->S);
+    B.fx_lo = (long)box->K * g->M * qzb::B_NC0;
+    QZ_CUDA(qzb::launch_beam_deposit(B, bsrc2, (cudaStream_t)stream));
+    return QZ_OK;
+}
+
+extern "C" qz_status qz_sweep_set_exact_sources(qz_sweep* s, const qz_fx* fx) {
+    if (!s) return fail(QZ_ERR_ARG, "qz_sweep_set_exact_sources: null pointer");
+    if (fx && (s->p.modes != 0 || fx->M != s->g->M))
+        return fail(QZ_ERR_ARG, "qz_sweep_set_exact_sources: modes = 0 and the grid of fx");
+    s->fx = fx;
     return QZ_OK;
 }
 

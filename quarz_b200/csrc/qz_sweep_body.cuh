@@ -485,6 +485,14 @@ __device__ __forceinline__ double ldbs(const SweepArgs& A, const double* bsrc, c
     return v;
 }
 
+// component c of node j of the guard row (the slice ahead of a later slab's first one): doubles, or two
+// limbs (the high row, then the low row M B_NC0 values further) when bsrc has the exact format
+__device__ __forceinline__ double guard_at(const SweepArgs& A, int j, int c) {
+    if (!A.bguard) return 0.0;
+    const double* g = A.bguard + (size_t)j * B_NC0 + c;
+    return A.bq ? beam_fx_value(g[0], g[(size_t)A.M * B_NC0], A.bq[j], A.bfx_2s) : g[0];
+}
+
 template <bool kL2, bool kStat = false>
 __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bsrc, int k, int j) {
     const size_t st = (size_t)A.M * B_NC0;
@@ -505,7 +513,7 @@ __device__ __forceinline__ BeamRow beam_row(const SweepArgs& A, const double* bs
     r.jt = ld(bk + B_JP1I);
     const int K = A.K;
     // the slice ahead of slice 0: none at the box head, the guard row in a later slab of a staged run
-    const double guard = A.bguard ? A.bguard[(size_t)j * B_NC0 + B_RT0] : 0.0;
+    const double guard = guard_at(A, j, B_RT0);
     if (A.ngp) {
         const double prev = (k > 0) ? ld(bk + B_RT0 - (ptrdiff_t)st) : guard;
         r.drt = (r.rt - prev) * A.idxi;
@@ -1054,8 +1062,7 @@ __device__ __forceinline__ BeamRow beam_row_at(const SweepArgs& A, const double*
     auto row = [&](int kk) { return beam_row<kL2, kStat>(A, bsrc, kk, j); };
     double djz = 0.0, djt = 0.0;
     if (A.ngp) {
-        const BeamRow p = k > 0 ? row(k - 1) : BeamRow{0.0, 0.0, A.bguard ? A.bguard[(size_t)j * B_NC0 + B_JZ0] : 0.0,
-                                                      A.bguard ? A.bguard[(size_t)j * B_NC0 + B_JP1I] : 0.0};
+        const BeamRow p = k > 0 ? row(k - 1) : BeamRow{0.0, 0.0, guard_at(A, j, B_JZ0), guard_at(A, j, B_JP1I)};
         djz = (r.jz - p.jz) * A.idxi;
         djt = (r.jt - p.jt) * A.idxi;
     } else if (K > 1) {

@@ -17,8 +17,10 @@ A stage only ever waits for the stage ahead of it, so with one rank per stage co
 concurrently, staggered by one slab per rank. The xi shape must be ngp (src/Beam.cpp:746, :980-983):
 a particle then deposits into and gathers from its own slice only, so no slab needs another slab's
 beams within a step. Every sweep gives the fields of the whole-box sweep bit for bit (its plasma deposits
-are exact); the beam deposits of the granular calls used here are FP64 reductions, so a multi-step
-staged run agrees with the single-GPU run to rounding.
+are exact). With exact beam sources (the default; qz_beam_deposit_fx with the quanta qz_sim derives from
+the same beams) every slab's beam sources are the whole box's bit for bit too, so a staged run equals the
+single-GPU run in its fields and particles; its moment sums, added over the stages, agree to rounding.
+exact=False deposits with FP64 reductions (the whole run then agrees to rounding).
 
 Messages go over torch.distributed (send / recv of float64 tensors, NCCL between GPUs, gloo on CPU), or
 between stages run one after the other in one process (Stages.run with a local channel), which is how it
@@ -58,7 +60,8 @@ def slab_spec(spec, k0: int, kl: int):
 
 class Message:
     """What a stage hands on in one step: the plasma state (a (6 + 5 order, npad) tensor and whether it was
-    pushed), the guard row (M x 5) and the beam particles that entered the next slab, per beam (7, n)."""
+    pushed), the guard row (M x 5, or 2 x M x 5 exact limbs) and the beam particles that entered the next
+    slab, per beam (7, n)."""
 
     def __init__(self, state, pushed: bool, guard, beams):
         self.state, self.pushed, self.guard, self.beams = state, pushed, guard, beams
@@ -81,8 +84,9 @@ class DistChannel:
     """Messages between ranks over torch.distributed: a float64 header (pushed, beam counts) then the
     state, the guard row and each beam's particles, all on the rank's device."""
 
-    def __init__(self, device, nbeams: int, state_shape, M: int):
+    def __init__(self, device, nbeams: int, state_shape, M: int, exact: bool = True):
         self.device, self.nbeams, self.state_shape, self.M = device, nbeams, state_shape, M
+        self.guard_shape = (2, M, 5) if exact else (M, 5)
 
     def send(self, dst: int, step: int, msg: Message):
         import torch
@@ -105,7 +109,7 @@ class DistChannel:
         dist.recv(head, src)
         state = torch.empty(self.state_shape, dtype=torch.float64, device=self.device)
         dist.recv(state, src)
-        guard = torch.empty((self.M, 5), dtype=torch.float64, device=self.device)
+        guard = torch.empty(self.guard_shape, dtype=torch.float64, device=self.device)
         dist.recv(guard, src)
         beams = []
         for q in range(self.nbeams):
@@ -120,7 +124,9 @@ class DistChannel:
 class Stage:
     """One slab of the box on one device: its sweep, beam sources, fields and beam particles."""
 
-    def __init__(self, spec, rank: int, nstages: int, beams, device=None):
+    def __init__(self, spec, rank: int, nstages: int, beams, device=None, bound=None):
+        """bound: (wq, particles) of the whole run's beams for exact beam sources (ExactSources.bound), or
+        None for FP64 reductions."""
         import torch
 
         if not spec.ngp:
@@ -138,7 +144,9 @@ class Stage:
         self.box = Q.BeamOps.box(self.spec.xi_min, spec.dxi, self.kl, True, 0)
         M = spec.M
         f64 = dict(dtype=torch.float64, device=self.device)
-        self.bsrc = torch.zeros((self.kl, M, 5), **f64)
+        self.fx = Q.ExactSources(self.grid, spec.dxi, bound[0], bound[1]) if bound is not None else None
+        self.sweep.set_exact_sources(self.fx)
+        self.bsrc = torch.zeros((2, self.kl, M, 5) if self.fx else (self.kl, M, 5), **f64)
         self.fld = torch.zeros((self.kl, M, 6), **f64)
         self.diag = torch.zeros((self.kl, M, 3), **f64)
         self.state_out = None if self.last else self.sweep.new_state()
@@ -175,7 +183,10 @@ class Stage:
         self.bsrc.zero_()
         for b, c in zip(self.bspec, self.cols):
             if c.shape[1]:
-                Q.BeamOps.deposit(self.grid, c, b.q, b.m, self.box, self.bsrc)
+                if self.fx is not None:
+                    Q.BeamOps.deposit_fx(self.grid, c, b.q, b.m, self.box, self.fx, self.bsrc)
+                else:
+                    Q.BeamOps.deposit(self.grid, c, b.q, b.m, self.box, self.bsrc)
         state_in = None
         if msg is not None:
             state_in = msg.state
@@ -186,7 +197,8 @@ class Stage:
             self.counts[k] += cnt[k]
         out = None
         if not self.last:
-            out = Message(self.state_out, True, self.bsrc[self.kl - 1].clone(), self.outbox)
+            last = self.bsrc[:, self.kl - 1] if self.fx is not None else self.bsrc[self.kl - 1]
+            out = Message(self.state_out, True, last.contiguous().clone(), self.outbox)
             self.outbox = [torch.zeros((7, 0), dtype=torch.float64, device=self.device) for _ in self.cols]
         mom = torch.zeros((len(self.cols), 17), dtype=torch.float64, device=self.device)
         for q, c in enumerate(self.cols):
@@ -220,12 +232,15 @@ class Stages:
     LocalChannel one process holds all the stages and runs them in turn within every step."""
 
     def __init__(self, spec, nstages: int, beams, ranks: Optional[Sequence[int]] = None, channel=None,
-                 device=None):
+                 device=None, exact: bool = True):
         self.spec, self.nstages = spec, nstages
         self.local = channel is None or isinstance(channel, LocalChannel)
         self.channel = channel if channel is not None else LocalChannel()
         mine = list(range(nstages)) if ranks is None else list(ranks)
-        self.stages = [Stage(spec, r, nstages, beams, device) for r in mine]
+        bound = Q.ExactSources.bound([p for p, _, _ in beams], [b.q for b in spec.beams]) if exact else None
+        if bound is not None and bound[1] > 1 << 25:
+            bound = None                  # beyond 2^25 particles the run deposits with FP64 reductions
+        self.stages = [Stage(spec, r, nstages, beams, device, bound) for r in mine]
 
     def run(self, nsteps: int, dt: float) -> np.ndarray:
         """nsteps time steps (nsteps + 1 sweeps); returns the moment sums (nsteps + 1, nbeams, 17) summed over

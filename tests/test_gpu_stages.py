@@ -6,10 +6,12 @@ the other through qz_sweep_run_stage, each taking the plasma state and the guard
   its pipelined MPI run with the ngp xi shape (README.md:1755-1758); here it holds because the sweep's
   plasma deposits are exact sums. Checked on the pinched-witness deck with beams.xi_shape = ngp, cut box
   and full box.
-- A staged run of 5 time steps (quarz_b200.stages, stages run in turn in one process) equals the
-  single-GPU run of the same deck to rounding: the staged beam deposits are the granular FP64
-  reductions, the single-GPU run's the exact ones. Derived moments 1e-10 relative to their natural scale,
-  E_z / B_z and particles 1e-9.
+- A staged run of 5 time steps (quarz_b200.stages, stages run in turn in one process) with exact beam
+  sources (qz_beam_deposit_fx with the quanta the single-GPU run derives from the same beams) equals the
+  single-GPU step-by-step run bit for bit in the last fields and diagnostics and in every particle; the
+  moment sums, added over the stages, agree to rounding (1e-10 relative to their natural scale). With
+  exact=False (FP64 reductions) the whole run agrees to rounding: moments 1e-10, E_z / B_z and particles
+  1e-9.
 - The entry point refuses what a stage cannot do: a guard row with the linear xi shape, a plasma state of
   the wrong shape.
 """
@@ -75,17 +77,17 @@ def test_stage_sweeps_equal_the_whole_sweep_bit_for_bit(full):
         assert nlost == lost, (ns, nlost, lost)
 
 
-@pytest.mark.parametrize("ns", [2, 3])
-def test_staged_run_equals_the_single_gpu_run(ns):
+@pytest.mark.parametrize("ns,exact", [(2, True), (3, True), (2, False)])
+def test_staged_run_equals_the_single_gpu_run(ns, exact):
     spec = _ngp_spec(False, steps=5, n=50000)
     beams = [Q.sample_beam(b) for b in spec.beams]
     sim = Q.Simulation(spec, beams=beams)
     sim.set_schedule(False)
     mom = sim.run(spec.steps, spec.dt)
-    fld, _ = sim.fields()
-    run = stages.Stages(spec, ns, beams)
+    fld, diag = sim.fields()
+    run = stages.Stages(spec, ns, beams, exact=exact)
     smom = run.run(spec.steps, spec.dt)
-    sfld, _ = run.fields()
+    sfld, sdiag = run.fields()
     # particles per beam: the staged run keeps them grouped by slab; compare in the caller's order of ids
     single = [sim.beam(q) for q in range(len(beams))]
     staged = [run.beam(q) for q in range(len(beams))]
@@ -97,6 +99,10 @@ def test_staged_run_equals_the_single_gpu_run(ns):
         kb = np.lexsort(b.T[::-1])
         order.append((a[ka], b[kb]))
     _same(spec, beams, (smom, sfld, [b for _, b in order]), (mom, fld, [a for a, _ in order]))
+    if exact:
+        assert np.array_equal(sfld, fld) and np.array_equal(sdiag, diag)
+        for a, b in order:
+            assert np.array_equal(a, b)
 
 
 def test_stage_entry_point_refuses_what_a_stage_cannot_do():

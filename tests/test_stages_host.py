@@ -26,7 +26,7 @@ def _message(step, rng_seed):
 
     rng = np.random.default_rng(rng_seed + step)
     state = torch.from_numpy(rng.normal(size=(21, 512)))
-    guard = torch.from_numpy(rng.normal(size=(64, 5)))
+    guard = torch.from_numpy(rng.normal(size=(2, 64, 5)))          # exact limbs: high row, low row
     beams = [torch.from_numpy(rng.normal(size=(7, 3 + step))), torch.zeros((7, 0), dtype=torch.float64)]
     return stages.Message(state, step > 0, guard, beams)
 
