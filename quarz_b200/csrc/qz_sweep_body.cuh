@@ -352,9 +352,13 @@ __device__ __forceinline__ bool warp_runs_sum(int key, double (&v)[NV]) {
     const bool head = (lane == 0) || (kprev != key);
     const unsigned heads = __ballot_sync(FULL, head);
     if (heads == FULL) return true;                   // no shared cell in this warp
-    const int seg = __popc(heads & (0xffffffffu >> (31 - lane)));
-#pragma unroll
-    for (int st = 1; st < 32; st <<= 1) {
+    const unsigned le = heads & (0xffffffffu >> (31 - lane));     // run heads at or below this lane
+    const int seg = __popc(le);
+    // the scan levels the longest run of the warp needs: a level of stride st adds only within runs
+    // longer than st, so stopping after them leaves every sum as the full scan gives it, bit for bit
+    const int maxoff = (int)__reduce_max_sync(FULL, (unsigned)(lane - (31 - __clz(le))));
+#pragma unroll 1
+    for (int st = 1; st <= maxoff; st <<= 1) {
         const int sp = __shfl_up_sync(FULL, seg, st);
         double vp[NV];
 #pragma unroll
