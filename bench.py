@@ -573,9 +573,11 @@ def run_adjoint(args, rank, world, local_rank):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": _config(spec, nbt, T, {"objective": "witness mean energy gain",
                                              "parameters": "64 driver-profile bins + witness delay",
-                                             "adjoint": "pipelined forward recording the plasma trajectory and "
-                                                        "the beams of every step in HBM, then the pipelined "
-                                                        "reverse pass (reverse sweeps + beam adjoint tasks)"},
+                                             "adjoint": "pipelined forward recording the beams of every step, "
+                                                        "the plasma state at every ceil(sqrt(K))-th slice and the "
+                                                        "W+ field of every slice, then the pipelined reverse pass "
+                                                        "(reverse sweeps that push each segment again from its "
+                                                        "checkpoint, beam adjoint tasks)"},
                               "adjoint"),
             "forward_ms": f_ms, "adjoint_ms": a_ms,
             "adjoint_split_ms": {"forward_keeping_beams": float(np.median([m[0] for m in split])),
