@@ -174,9 +174,10 @@ def sweep_latency(spec, beams, dev, sim, steps_traced):
     sw = Q.Sweep(grid, Q.sweep_params(spec))
     K, M = spec.K, spec.M
     f64 = dict(dtype=torch.float64, device=dev)
-    bsrc = torch.zeros(K * M * 5, **f64)
-    fld = torch.zeros(K * M * 6, **f64)
-    diag = torch.zeros(K * M * 3, **f64)
+    m1 = spec.modes == 1                    # (B_NC, F_NC, D_NC) = (15, 18, 9) with mode 1, else (5, 6, 3)
+    bsrc = torch.zeros(K * M * (15 if m1 else 5), **f64)
+    fld = torch.zeros(K * M * (18 if m1 else 6), **f64)
+    diag = torch.zeros(K * M * (9 if m1 else 3), **f64)
     box = Q.BeamOps.box(spec.xi_min, spec.dxi, K, spec.ngp, spec.modes)
     for b, (parts, _, _) in zip(spec.beams, beams):
         cols = torch.from_numpy(np.ascontiguousarray(parts.T)).to(dev).contiguous()
@@ -794,7 +795,7 @@ def main():
                                 "sample": f"{args.cpu_steps} full time steps of the same workload (sweep + moment "
                                           f"sums + beam push), oracle on {oracle_rate.threads} host threads, "
                                           f"{el:.1f} s"}
-    if rank == 0 and world == 1 and not args.no_extras:
+    if rank == 0 and world == 1 and not args.no_extras and args.workload == WORKLOAD and not args.smooth:
         line.update(extras(args, r, line))
     if world > 1:
         import torch

@@ -147,6 +147,63 @@ __device__ __forceinline__ void deposit_add0(const BeamArgs& B, double* __restri
     }
 }
 
+// The part of the m = 1 deposit that the m = 1 sweep reads (rho - J_z, J_z and J_perp in modes 0 and 1,
+// J_perp also in mode 2; not the beam densities), per corner: deposit_setup1 takes the particle's cell,
+// weights and velocities once (deposit_one's m = 1 branch, src/Beam.cpp:725-785), deposit_corner1 the 12
+// values of corner (row k + a, node j + b), deposit_add1 adds them with FP64 reductions.
+constexpr int kDep1 = 12;
+struct Dep1 {
+    int k, j;
+    double d0, tk, t, c, s, omvz, vz, vx, vy, vr, vt;
+};
+__device__ __forceinline__ bool deposit_setup1(const BeamArgs& B, double X, double Y, double PX, double PY, double PZ,
+                                               double XI, double wi, int jguess, Dep1& D) {
+    const double R = B.R;
+    const double r = sqrt(X * X + Y * Y);
+    if (r > R) return false;
+    D.c = r > 0.0 ? X / r : 1.0;
+    D.s = r > 0.0 ? Y / r : 0.0;
+    const double sx = (XI - B.xi_min) * B.idxi;
+    D.k = B.ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
+    if (D.k < -1 || D.k >= B.K) return false;
+    D.tk = B.ngp ? 0.0 : sx - D.k;
+    const double p2 = PX * PX + PY * PY;
+    const double gam = sqrt(1.0 + p2 + PZ * PZ);
+    D.omvz = (1.0 + p2) / (gam * (gam + PZ));
+    D.vz = PZ / gam; D.vx = PX / gam; D.vy = PY / gam;
+    D.vr = D.c * D.vx + D.s * D.vy;
+    D.vt = D.c * D.vy - D.s * D.vx;
+    D.j = locate_near(B.r, B.N, R, r, jguess);
+    const double t = (r - B.r[D.j]) * B.inv_h[D.j];
+    D.t = t < 0.0 ? 0.0 : (t > 1.0 ? 1.0 : t);
+    D.d0 = wi * B.q;
+    return true;
+}
+// corner (a, b): v in the order B_RT0, B_RT1R, B_RT1I, B_JZ0, B_JZ1R, B_JZ1I, B_JP0R, B_JP0I, B_JP1R,
+// B_JP1I, B_JP2R, B_JP2I; zero for a row outside the box or the second row of the ngp shape
+__device__ __forceinline__ void deposit_corner1(const BeamArgs& B, const Dep1& D, int a, int b,
+                                                double (&v)[kDep1]) {
+    const int kk = D.k + a;
+    const bool row = (a == 0 || !B.ngp) && kk >= 0 && kk < B.K;
+    const double Wk = a ? D.tk : 1.0 - D.tk, Wr = b ? D.t : 1.0 - D.t;
+    const double d = row ? D.d0 * Wk * Wr * B.inv_V[D.j + b] * B.idxi : 0.0;
+    const double c2 = D.c * D.c - D.s * D.s, s2 = 2.0 * D.c * D.s;
+    v[0] = d * D.omvz; v[1] = d * D.omvz * D.c; v[2] = -d * D.omvz * D.s;
+    v[3] = d * D.vz; v[4] = d * D.vz * D.c; v[5] = -d * D.vz * D.s;
+    v[6] = d * D.vx; v[7] = d * D.vy;
+    v[8] = d * D.vr; v[9] = d * D.vt;
+    v[10] = d * (D.vx * c2 + D.vy * s2); v[11] = d * (D.vy * c2 - D.vx * s2);
+}
+__device__ __forceinline__ void deposit_add1(const BeamArgs& B, double* __restrict__ bsrc, int kk, int jj,
+                                             const double (&v)[kDep1]) {
+    if (kk < 0 || kk >= B.K) return;
+    constexpr int comp[kDep1] = {B_RT0, B_RT1R, B_RT1I, B_JZ0, B_JZ1R, B_JZ1I, B_JP0R, B_JP0I, B_JP1R, B_JP1I,
+                                 B_JP2R, B_JP2I};
+    double* o = bsrc + ((size_t)kk * B.M + jj) * B_NC1;
+#pragma unroll
+    for (int c = 0; c < kDep1; ++c) atomicAdd(o + comp[c], v[c]);
+}
+
 // bilinear (xi, r) gather and mode sums at the particle (src/Beam.cpp:972-1008)
 template <bool kL2>
 __device__ __forceinline__ void gather(const BeamArgs& B, const double* __restrict__ fld, double X, double Y,

@@ -411,6 +411,50 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
                 const int key = dep ? (dk + 1) * M + dj : -1 - lane;
                 if (warp_runs_sum<4 * beam_detail::kDep0>(key, v) && dep) beam_detail::deposit_add0(Bb, bnext, dk, dj, v);
             }
+        } else if (P.modes == 1) {
+            // m = 1: the same runs of equal cells across the warp, summed per corner (12 components each)
+            for (long base = i0; base < i1; base += 32) {
+                const long i = base + lane;
+                bool dep = false;
+                beam_detail::Dep1 D;
+                D.k = D.j = 0;
+                if (i < i1) {
+                    PState7 p;
+                    p.w = __ldcg(Bb.w + i);
+                    if (p.w != 0.0) {
+                        p.x = __ldcg(Bb.x + i); p.y = __ldcg(Bb.y + i);
+                        p.px = __ldcg(Bb.px + i); p.py = __ldcg(Bb.py + i); p.pz = __ldcg(Bb.pz + i);
+                        p.xi = __ldcg(Bb.xi + i);
+                        bool alive = true;
+                        int jg = -1;
+                        if (!rigid) {
+                            alive = P.fld_l1 ? push_one<false>(Bb, fld, p, h, hs, P.dt_drift, &jg)
+                                             : push_one<true>(Bb, fld, p, h, hs, P.dt_drift, &jg);
+                            __stcg(Bb.x + i, p.x); __stcg(Bb.y + i, p.y);
+                            __stcg(Bb.px + i, p.px); __stcg(Bb.py + i, p.py); __stcg(Bb.pz + i, p.pz);
+                            __stcg(Bb.xi + i, p.xi);
+                            if (!alive) __stcg(Bb.w + i, 0.0);
+                        }
+                        if (alive) {
+                            dep = beam_detail::deposit_setup1(Bb, p.x, p.y, p.px, p.py, p.pz, p.xi, p.w, jg, D);
+                            cmax = max(cmax, xi_cell(Bb, p.xi));
+                        }
+                    }
+                }
+                const int key = dep ? (D.k + 1) * M + D.j : -1 - lane;
+#pragma unroll 1
+                for (int cr = 0; cr < 4; ++cr) {
+                    const int a = cr >> 1, b = cr & 1;
+                    if (a == 1 && Bb.ngp) continue;                  // (uniform: the beam's shape)
+                    double v[beam_detail::kDep1];
+                    if (dep) beam_detail::deposit_corner1(Bb, D, a, b, v);
+                    else
+#pragma unroll
+                        for (int c = 0; c < beam_detail::kDep1; ++c) v[c] = 0.0;
+                    if (warp_runs_sum<beam_detail::kDep1>(key, v) && dep)
+                        beam_detail::deposit_add1(Bb, bnext, D.k + a, D.j + b, v);
+                }
+            }
         } else
         for (long i = i0 + lane; i < i1; i += 32) {
             PState7 p;
