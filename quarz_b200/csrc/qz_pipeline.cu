@@ -149,7 +149,7 @@ cudaError_t group_starts(const CellSortBuf& buf, long nlive, int width, int ngro
 
 size_t pipeline_smem_bytes(int modes, int M, bool dbuf, bool const_smem, bool filter, int pcache) {
     const size_t sweep = modes == 1 ? sweep_m1_smem_bytes(M) : sweep_m0_smem_bytes(M, dbuf, const_smem, filter, pcache);
-    const size_t worker = sizeof(double) * (3 * (size_t)M + (size_t)(kSweepThreads / 32) * 17 * 32) + 64;
+    const size_t worker = sizeof(double) * (4 * (size_t)M + (size_t)(kSweepThreads / 32) * 17 * 32) + 64;
     return sweep > worker ? sweep : worker;
 }
 

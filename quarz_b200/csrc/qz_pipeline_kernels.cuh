@@ -269,14 +269,20 @@ __device__ __forceinline__ bool claim_task(const PipeArgs& P, int last, int& n, 
 __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
     const int tid = threadIdx.x, lane = tid & 31;
     const int M = P.sw.M, N = P.sw.N, K = P.sw.K;
-    // grid arrays in shared memory: the binary search of every lookup stays on chip
+    // grid arrays in shared memory: the binary search of every lookup stays on chip; so do the node
+    // scales of the exact deposits (a global load of them before every quantisation stalled each warp
+    // on L2 latency: ~10k cycles per 32-particle iteration)
     double* r = smem;
     double* ih = r + M;
     double* iV = ih + M;
+    double* fxs = iV + M + (size_t)(kT / 32) * 17 * 32;        // behind the per-warp moment slots
+    const double* fx_src = nullptr;
+    for (int q = 0; q < P.nbeams && !fx_src; ++q) fx_src = P.beam[q].fx_scale;
     for (int j = tid; j < M; j += kT) {
         r[j] = P.sw.r[j];
         iV[j] = P.sw.inv_V[j];
         if (j < N) ih[j] = P.sw.inv_h[j];
+        if (fx_src) fxs[j] = fx_src[j];
     }
     __syncthreads();
     const int last = P.pmom ? P.nsteps : P.nsteps - 1;     // the last step with tasks
@@ -296,6 +302,7 @@ __device__ __forceinline__ void worker_role(const PipeArgs& P, double* smem) {
         Bb.r = r;
         Bb.inv_h = ih;
         Bb.inv_V = iV;
+        if (Bb.fx_scale) Bb.fx_scale = fxs;                      // (every beam of a run has the same scales)
         const double* fld = P.fld + (size_t)(n % P.ring) * P.fld_slot;
         double* bnext = P.bsrc + (size_t)((n + 1) % P.ring) * P.bsrc_slot;
         // bring the task's inputs towards L2 while it starts: the particle columns, the field rows it
