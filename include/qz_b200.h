@@ -329,7 +329,7 @@ qz_status qz_sim_counters(qz_sim* s, qz_counters* out);
 qz_status qz_sim_step_host(qz_sim* s, double* const* cols_host, double dt_kick, double dt_drift, int push,
                            double* moments_host, void* stream);
 
-/* The adjoint of a run (no reference counterpart; modes = 0, linear xi shape, one mobile plasma
+/* The adjoint of a run (no reference counterpart; modes = 0, linear or ngp xi shape, one mobile plasma
  * species with at most 512 particles per slice, M <= 512). Runs nsteps like qz_sim_run (step by step,
  * keeping the beams of every step on the device; the beams must not have been pushed yet), then the
  * reverse pass: the beam pushes, sweeps and beam deposits of every step in reverse order.

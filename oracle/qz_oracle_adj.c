@@ -20,9 +20,10 @@
  *   plasma deposit           src/PlasmaSpecies.cpp:409-478
  *   beam deposit             src/Beam.cpp:725-785
  *
- * Scope: modes = 0, linear beam shape in xi (ngp = 0), one mobile plasma species (immobile ones
- * only add a constant background), constant AB coefficients, constant dt. Particle removal, cell
- * changes and clamps are piecewise constant, so their derivative is taken as zero.
+ * Scope: modes = 0, linear or nearest-grid-point beam shape in xi, one mobile plasma species
+ * (immobile ones only add a constant background), constant AB coefficients, constant dt. Particle
+ * removal, cell changes, clamps and the nearest-slice choice are piecewise constant, so their
+ * derivative is taken as zero.
  *
  * Storage: the beams of every step are kept; the sweep of step n is recomputed in the reverse pass
  * from the beams of step n, recording the plasma state at the start of every slice.
@@ -523,6 +524,11 @@ static void sweep_back(qzo_sim* s, int isp, const double* lfld, double* lbsrc) {
             LB(k, j, B_JP1R) += A.l_jpr[j];
             LB(k, j, B_JP1I) += A.l_jpi[j];
             const double ld = A.l_drho[j] * idxi;
+            if (s->p.ngp) {      /* ngp: the backward difference of rho - J_z (no row ahead of the box head) */
+                LB(k, j, B_RT0) += ld;
+                if (k > 0) LB(k - 1, j, B_RT0) -= ld;
+                continue;
+            }
             if (K == 1) continue;
             if (k == 0) { LB(1, j, B_RT0) += ld; LB(0, j, B_RT0) -= ld; }
             else if (k == K - 1) { LB(K - 1, j, B_RT0) += ld; LB(K - 2, j, B_RT0) -= ld; }
@@ -629,11 +635,20 @@ static void beam_push_back(qzo_sim* s, const beam_t* B, long i, double dt_kick, 
     const double r = sqrt(X * X + Y * Y);
     const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
     double sl = (B->xi[i] - xmin) * idxi;
-    int k = (int)floor(sl), kclamp = 0;
-    if (k < 0) { k = 0; sl = 0; kclamp = 1; }
-    if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = 1; }
-    const double tk = sl - k;
-    const int k1 = k + 1;
+    int k, kclamp = 0;
+    double tk;
+    if (s->p.ngp) {          /* the slice nearest to the particle, no xi interpolation (src/Beam.cpp:980-983) */
+        k = (int)floor(sl + 0.5);
+        k = k < 0 ? 0 : (k > nloc - 1 ? nloc - 1 : k);
+        tk = 0.0;
+        kclamp = 1;          /* piecewise constant in xi: no xi derivative */
+    } else {
+        k = (int)floor(sl);
+        if (k < 0) { k = 0; sl = 0; kclamp = 1; }
+        if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = 1; }
+        tk = sl - k;
+    }
+    const int k1 = s->p.ngp ? k : k + 1;
     int j; double t;
     grid_weights(g, r, &j, &t);
 #define FL(kk, jj, comp) fld[((size_t)(kk) * M + (jj)) * 6 + (comp)]
@@ -731,9 +746,10 @@ static void beam_deposit_back(qzo_sim* s, const beam_t* B, long i, const double*
     if (r > R) return;
     const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
     const double sx = (B->xi[i] - xmin) * idxi;
-    const int k = (int)floor(sx);
+    const int ngp = s->p.ngp;
+    const int k = ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
     if (k < -1 || k >= nloc) return;
-    const double tk = sx - k;
+    const double tk = ngp ? 0.0 : sx - k;
     const double PX = B->px[i], PY = B->py[i], PZ = B->pz[i];
     const double p2 = PX * PX + PY * PY;
     const double gam = sqrt(1.0 + p2 + PZ * PZ);
@@ -745,7 +761,7 @@ static void beam_deposit_back(qzo_sim* s, const beam_t* B, long i, const double*
     const double Wr[2] = {1.0 - t, t};
     const double Wk[2] = {1.0 - tk, tk};
     double l_omvz = 0, l_vz = 0, l_vr = 0, l_vt = 0, l_w = 0, lWk[2] = {0, 0}, lWr[2] = {0, 0};
-    for (int a = 0; a < 2; ++a) {
+    for (int a = 0; a < (ngp ? 1 : 2); ++a) {
         const int kk = k + a;
         if (kk < 0 || kk >= nloc) continue;
         for (int b = 0; b < 2; ++b) {
@@ -764,7 +780,7 @@ static void beam_deposit_back(qzo_sim* s, const beam_t* B, long i, const double*
         }
     }
     lam7[6] += l_w;
-    lam7[5] += (lWk[1] - lWk[0]) * idxi;
+    if (!ngp) lam7[5] += (lWk[1] - lWk[0]) * idxi;
     const double tt = (r - g->r[j]) * g->inv_h[j];
     const double l_r = (tt > 0.0 && tt < 1.0) ? (lWr[1] - lWr[0]) * g->inv_h[j] : 0.0;
     const double l_vx = l_vr * c - l_vt * sn, l_vy = l_vr * sn + l_vt * c;
@@ -827,7 +843,7 @@ static void beams_load(qzo_sim* s, const double* in) {
    J = sum lamS * sums. mom (optional): the forward's moment sums ((nsteps + 1), nb, 17).
    Returns 0, or -2 when the deck is outside the adjoint's scope. The sim ends at the last step. */
 int qzo_sim_adjoint(qzo_sim* s, int nsteps, double dt, const double* lamS, double* lam_out, double* mom) {
-    if (s->m1 || s->p.ngp || nsteps < 1) return -2;
+    if (s->m1 || nsteps < 1) return -2;
     int isp = -1;
     for (int i = 0; i < s->nsp; ++i)
         if (s->sp[i].p.mobile) { if (isp >= 0) return -2; isp = i; }

@@ -1777,9 +1777,8 @@ qz_status sim_adjoint(qz_sim* s, int nsteps, double dt, const AdjSeed& seed, dou
     if (!s || nsteps < 1 || !(dt > 0.0) || (!seed.fixed && !seed.fn) || (!s->beams.empty() && !lam_host))
         return fail(QZ_ERR_ARG, "qz_sim_adjoint: bad argument");
     const qzb::SweepArgs& base = s->sw->base;
-    if (s->p.modes != 0 || s->p.ngp || s->p.K < 2 || base.max_cells > 0.0)
-        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0 with the linear xi shape, K >= 2, "
-                                        "without adaptive sub-slicing");
+    if (s->p.modes != 0 || s->p.K < 2 || base.max_cells > 0.0)
+        return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: built for modes = 0, K >= 2, without adaptive sub-slicing");
     if (base.M > qzb::kSweepThreads || base.np > qzb::kSweepThreads || base.nsp != 1)
         return fail(QZ_ERR_UNSUPPORTED, "qz_sim_adjoint: needs M <= 512, one mobile species, <= 512 plasma "
                                         "particles per slice");

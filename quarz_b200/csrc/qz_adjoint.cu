@@ -146,12 +146,20 @@ __device__ void push_back_one(const BeamArgs& B, const double* __restrict__ fld,
     const double r = sqrt(X * X + Y * Y);
     const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
     double sl = (XI - xmin) * B.idxi;
-    int k = (int)floor(sl);
+    int k;
     bool kclamp = false;
-    if (k < 0) { k = 0; sl = 0; kclamp = true; }
-    if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = true; }
-    const double tk = sl - k;
-    const int k1 = k + 1;
+    double tk;
+    if (B.ngp) {            // the nearest slice, piecewise constant in xi: no xi derivative
+        k = min(max((int)floor(sl + 0.5), 0), nloc - 1);
+        tk = 0.0;
+        kclamp = true;
+    } else {
+        k = (int)floor(sl);
+        if (k < 0) { k = 0; sl = 0; kclamp = true; }
+        if (k > nloc - 2) { k = nloc - 2; sl = nloc - 1; kclamp = true; }
+        tk = sl - k;
+    }
+    const int k1 = B.ngp ? k : k + 1;
     int j;
     double t;
     weights(B.r, B.inv_h, B.N, B.R, r, j, t);
@@ -232,8 +240,10 @@ __device__ void push_back_one(const BeamArgs& B, const double* __restrict__ fld,
             double* g10p = lfld + ((size_t)k1 * M + j) * F_NC0;
             atomicAdd(g00p + cm, l * (1.0 - tk) * (1.0 - t));
             atomicAdd(g00p + F_NC0 + cm, l * (1.0 - tk) * t);
-            atomicAdd(g10p + cm, l * tk * (1.0 - t));
-            atomicAdd(g10p + F_NC0 + cm, l * tk * t);
+            if (!B.ngp) {
+                atomicAdd(g10p + cm, l * tk * (1.0 - t));
+                atomicAdd(g10p + F_NC0 + cm, l * tk * t);
+            }
         }
         l_tk += l * (((1.0 - t) * f10[cm] + t * f11[cm]) - ((1.0 - t) * f00[cm] + t * f01[cm]));
         l_t += l * ((1.0 - tk) * (f01[cm] - f00[cm]) + tk * (f11[cm] - f10[cm]));
@@ -261,7 +271,7 @@ __global__ void push_back_kernel(BeamArgs B, const double* __restrict__ fld, dou
     }
 }
 
-// Beam::deposit of particle i in reverse (m = 0, linear xi shape): l7 += d(lbsrc . bsrc)/d(particle);
+// Beam::deposit of particle i in reverse (m = 0, linear or ngp xi shape): l7 += d(lbsrc . bsrc)/d(particle);
 // kL2: lbsrc was written by other SMs during the same launch
 template <bool kL2>
 __device__ void deposit_back_one(const BeamArgs& B, const double* __restrict__ lbsrc, long i, double (&l7)[7]) {
@@ -273,9 +283,10 @@ __device__ void deposit_back_one(const BeamArgs& B, const double* __restrict__ l
     if (r > B.R) return;
     const double c = r > 0.0 ? X / r : 1.0, sn = r > 0.0 ? Y / r : 0.0;
     const double sx = (B.xi[i] - B.xi_min) * B.idxi;
-    const int k = (int)floor(sx);
+    const int k = B.ngp ? (int)floor(sx + 0.5) : (int)floor(sx);
     if (k < -1 || k >= nloc) return;
-    const double tk = sx - k;
+    const double tk = B.ngp ? 0.0 : sx - k;
+    const int na = B.ngp ? 1 : 2;
     const double PX = B.px[i], PY = B.py[i], PZ = B.pz[i];
     const double p2 = PX * PX + PY * PY;
     const double gam = sqrt(1.0 + p2 + PZ * PZ);
@@ -291,7 +302,7 @@ __device__ void deposit_back_one(const BeamArgs& B, const double* __restrict__ l
 #pragma unroll
     for (int a = 0; a < 2; ++a) {
         const int kk = k + a;
-        if (kk < 0 || kk >= nloc) continue;
+        if (a >= na || kk < 0 || kk >= nloc) continue;
 #pragma unroll
         for (int b = 0; b < 2; ++b) {
             const int jj = j + b;
@@ -311,7 +322,7 @@ __device__ void deposit_back_one(const BeamArgs& B, const double* __restrict__ l
         }
     }
     l7[6] += l_w;
-    l7[5] += (lWk[1] - lWk[0]) * B.idxi;
+    if (!B.ngp) l7[5] += (lWk[1] - lWk[0]) * B.idxi;
     const double tt = (r - B.r[j]) * B.inv_h[j];
     const double l_r = (tt > 0.0 && tt < 1.0) ? (lWr[1] - lWr[0]) * B.inv_h[j] : 0.0;
     const double l_vx = l_vr * c - l_vt * sn, l_vy = l_vr * sn + l_vt * c;
@@ -1103,7 +1114,10 @@ __device__ bool sweep_back_body(const SweepArgs& A, const double* __restrict__ t
             Lk[B_JP1I] += v;
             const double ld = S.l_drho[i] * A.idxi;
             const size_t st = (size_t)M * B_NC0;
-            if (K > 1) {
+            if (A.ngp) {     // the backward difference (the row ahead of the box head is zero)
+                Lk[B_RT0] += ld;
+                if (k > 0) Lk[B_RT0 - (ptrdiff_t)st] -= ld;
+            } else if (K > 1) {
                 if (k == 0) { Lk[st + B_RT0] += ld; Lk[B_RT0] -= ld; }
                 else if (k == K - 1) { Lk[B_RT0] += ld; Lk[B_RT0 - (ptrdiff_t)st] -= ld; }
                 else { Lk[st + B_RT0] += 0.5 * ld; Lk[B_RT0 - (ptrdiff_t)st] -= 0.5 * ld; }
@@ -1373,8 +1387,10 @@ __device__ void adj_worker_role(const AdjPipeArgs& P, double* smem) {
                     for (int q = 0; q < 6; ++q) {
                         atomicAdd(g0 + comp[q], g[q * 4 + 0]);
                         atomicAdd(g0 + F_NC0 + comp[q], g[q * 4 + 1]);
-                        atomicAdd(g1 + comp[q], g[q * 4 + 2]);
-                        atomicAdd(g1 + F_NC0 + comp[q], g[q * 4 + 3]);
+                        if (!B0.ngp) {        // ngp: one row (k may be the last slice)
+                            atomicAdd(g1 + comp[q], g[q * 4 + 2]);
+                            atomicAdd(g1 + F_NC0 + comp[q], g[q * 4 + 3]);
+                        }
                     }
                 }
             }

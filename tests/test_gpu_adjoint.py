@@ -3,7 +3,8 @@ and the gradients of witness energy gain and spread against central differences 
 
 Deck: the one of tests/test_oracle_adjoint.py (24 uniform cells, 71 slices, AB3, driver and witness
 with 300 particles each, 2 steps) and a stretched-grid variant with 3 steps, each also with the smoothing
-filter (plasma.smooth_length 0.3 and 0.05: the adjoint then runs the filters in reverse). Tolerances: every
+filter (plasma.smooth_length 0.3 and 0.05: the adjoint then runs the filters in reverse), and both with
+the nearest-slice beam shape (beams.xi_shape = ngp; the stretched one with the filter). Tolerances: every
 component of the particle adjoint 1e-8 relative L2 against the oracle (the forwards differ in the
 order of their deposit sums, about 1e-13); the profile and delay gradients 1e-5 relative against
 central differences with h = 1e-6 (their error is that of the differences). Both schedules: the
@@ -27,11 +28,14 @@ def _specs():
     sm = deck.run_spec(deck.parse_deck(TEXT, ["plasma.smooth_length=0.3"]))
     sms = deck.run_spec(deck.parse_deck(TEXT, ["time.steps=3", "plasma.smooth_length=0.05"]))
     sms.nodes = workloads.scan_nodes(129, 2e-3)
-    return [spec, st, sm, sms]
+    ngp = deck.run_spec(deck.parse_deck(TEXT, ["beams.xi_shape=ngp"]))
+    ngps = deck.run_spec(deck.parse_deck(TEXT, ["beams.xi_shape=ngp", "time.steps=3", "plasma.smooth_length=0.05"]))
+    ngps.nodes = workloads.scan_nodes(129, 2e-3)
+    return [spec, st, sm, sms, ngp, ngps]
 
 
 @pytest.mark.parametrize("pipelined", [True, False])
-@pytest.mark.parametrize("which", [0, 1, 2, 3])
+@pytest.mark.parametrize("which", [0, 1, 2, 3, 4, 5])
 def test_adjoint_against_oracle(which, pipelined):
     spec = _specs()[which]
     beams = [Q.sample_beam(b) for b in spec.beams]
