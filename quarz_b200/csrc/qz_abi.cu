@@ -360,9 +360,12 @@ extern "C" qz_status qz_sweep_create(const qz_grid* g, const qz_sweep_params* p,
     if (p->max_cells_per_step > 0.0 && (p->modes != 0 || p->smooth_length > 0.0))
         return fail(QZ_ERR_UNSUPPORTED, "qz_sweep_create: adaptive sub-slicing (pusher.max_cells_per_step) runs with "
                                         "modes = 0 and without plasma.smooth_length");
-    if (p->modes == 1 && (M > qzb::kSweepThreads || qzb::sweep_m1_smem_bytes(M) > (size_t)optin))
+    // modes = 1: one radial node per thread, 512 threads or (513..1024 nodes) 1024
+    if (p->modes == 1 && (M > 2 * qzb::kSweepThreads ||
+                          (M <= qzb::kSweepThreads ? qzb::sweep_m1_smem_bytes(M) : qzb::sweep_m1w_smem_bytes(M)) >
+                              (size_t)optin))
         return fail(QZ_ERR_SIZE, "qz_sweep_create: the modes = 1 sweep holds one radial node per thread: M = " +
-                                     std::to_string(M) + " > " + std::to_string(qzb::kSweepThreads));
+                                     std::to_string(M) + " > " + std::to_string(2 * qzb::kSweepThreads));
     if (lay < 0 || rpt > 4)
         return fail(QZ_ERR_SIZE, "qz_sweep_create: M = " + std::to_string(M) + " is too large for one CTA (" +
                                      std::to_string(qzb::sweep_m0_smem_bytes(M, false, false, filter)) + " B of shared memory, "
@@ -1569,7 +1572,9 @@ extern "C" qz_status qz_sim_run(qz_sim* s, int nsteps, double dt, double* mom_ho
     cudaStream_t st = (cudaStream_t)stream;
     bool vay_only = true;                 // the pipeline's push workers use Vay
     for (const auto& b : s->beams) vay_only = vay_only && b.pusher == 0;
-    if (s->pipe.enabled && !s->beams.empty() && vay_only) return run_pipelined(s, nsteps, dt, mom_host, st);
+    // (the pipeline's sweep CTAs have 512 threads: m = 1 runs with more nodes go step by step)
+    const bool wide_m1 = s->p.modes == 1 && s->sw->base.M > qzb::kSweepThreads;
+    if (s->pipe.enabled && !s->beams.empty() && vay_only && !wide_m1) return run_pipelined(s, nsteps, dt, mom_host, st);
     return run_sequential(s, nsteps, dt, mom_host, st);
 }
 
@@ -2337,8 +2342,8 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         !m || !rigid || !gref || !xiref)))
         return fail(QZ_ERR_ARG, "qz_batch_add: bad argument (at most 2 beams per instance)");
     if (p->modes != 0 && p->modes != 1) return fail(QZ_ERR_ARG, "qz_batch_add: modes must be 0 or 1");
-    if (p->modes == 1 && M > qzb::kSweepThreads)
-        return fail(QZ_ERR_SIZE, "qz_batch_add: modes = 1 instances need M <= 512 (one radial row per thread)");
+    if (p->modes == 1 && M > 2 * qzb::kSweepThreads)
+        return fail(QZ_ERR_SIZE, "qz_batch_add: modes = 1 instances need M <= 1024 (one radial row per thread)");
     if (b->ord && p->ab_order != b->ord) return fail(QZ_ERR_ARG, "qz_batch_add: every instance needs the same AB order");
     auto* I = new (std::nothrow) qz_batch::Inst;
     if (!I) return fail(QZ_ERR_NOMEM, "qz_batch_add: out of host memory");
@@ -2354,7 +2359,9 @@ extern "C" qz_status qz_batch_add(qz_batch* b, const double* nodes, int M, const
         QZ_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
         const size_t reserve = sizeof(qzb::BatchInst) + sizeof(double) * 17 * (qzb::kSweepThreads / 32) + 256;
         if (p->modes == 1) {
-            if (qzb::sweep_m1_smem_bytes(M) + reserve > (size_t)optin) {
+            const bool wide = M > qzb::kSweepThreads;     // the 1024-thread batch kernel (qz_batch_m1w.cu)
+            if ((wide ? qzb::sweep_m1w_smem_bytes(M) + qzb::batch_m1w_static_bytes()
+                      : qzb::sweep_m1_smem_bytes(M) + reserve) > (size_t)optin) {
                 delete I;
                 return fail(QZ_ERR_SIZE, "qz_batch_add: M too large for the batched sweep");
             }
@@ -2415,42 +2422,71 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     const int ni = (int)b->inst.size();
     if (ni == 0) return QZ_OK;
     cudaStream_t st = (cudaStream_t)stream;
-    // slot sizes and shared memory: the largest instance
-    size_t fmax = 0, dmax = 0, bmax = 0, smem = 0, mom_total = 0;
-    bool with_m1 = false, with_ext = false;
+    // two groups: the 512-thread batch kernel takes every m = 0 instance and the m = 1 ones with up to 512
+    // nodes; m = 1 instances with more nodes (wide) run after it in the 1024-thread kernel (qz_batch_m1w.cu).
+    // Per group the slot sizes and shared memory of its largest instance; the two launches run one after
+    // the other on the stream and share the slot buffers.
+    struct Group {
+        size_t fmax = 0, dmax = 0, bmax = 0, smem = 0;
+        bool with_m1 = false, with_ext = false;
+        int n = 0, grid = 0;
+    } gr[2];
+    size_t mom_total = 0;
     std::vector<size_t> mom_off(ni);
+    std::vector<int> grp(ni);
     for (int i = 0; i < ni; ++i) {
         const auto& A = b->inst[i]->dev.sw;
         const bool m1 = b->inst[i]->dev.modes == 1;
-        with_m1 = with_m1 || m1;
-        with_ext = with_ext || A.filter;
+        grp[i] = (m1 && A.M > qzb::kSweepThreads) ? 1 : 0;
+        Group& G = gr[grp[i]];
+        ++G.n;
+        G.with_m1 = G.with_m1 || m1;
+        G.with_ext = G.with_ext || A.filter;
         const size_t km = (size_t)A.K * A.M;
-        fmax = std::max(fmax, km * (m1 ? 18 : 6));           // fld (K, M, 18 / 6)
-        dmax = std::max(dmax, km * (m1 ? 9 : 3));            // diag (K, M, 9 / 3)
-        bmax = std::max(bmax, km * (m1 ? 15 : 5));           // bsrc (K, M, 15 / 5)
-        smem = std::max(smem, m1 ? qzb::sweep_m1_smem_bytes(A.M)
-                                 : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0, A.pcache));
+        G.fmax = std::max(G.fmax, km * (m1 ? 18 : 6));        // fld (K, M, 18 / 6)
+        G.dmax = std::max(G.dmax, km * (m1 ? 9 : 3));         // diag (K, M, 9 / 3)
+        G.bmax = std::max(G.bmax, km * (m1 ? 15 : 5));        // bsrc (K, M, 15 / 5)
+        G.smem = std::max(G.smem, grp[i] ? qzb::sweep_m1w_smem_bytes(A.M)
+                                  : m1 ? qzb::sweep_m1_smem_bytes(A.M)
+                                       : qzb::sweep_m0_smem_bytes(A.M, A.dbuf, A.const_smem, A.filter != 0, A.pcache));
         mom_off[i] = mom_total;
         mom_total += (size_t)(nsteps + 1) * std::max(1, b->inst[i]->dev.nbeams) * 17;
     }
     int sms = 0;
-    const int grid = std::min(qzb::batch_max_grid(b->ord, with_m1, with_ext, smem, &sms), ni);
-    if (grid < 1) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the batch kernel cannot be resident here");
-    const size_t need = (size_t)grid;
-    if (b->fld_alloc < need * fmax || b->diag_alloc < need * dmax || b->bsrc_alloc < need * bmax) {
+    if (gr[0].n) {
+        gr[0].grid = std::min(qzb::batch_max_grid(b->ord, gr[0].with_m1, gr[0].with_ext, gr[0].smem, &sms), gr[0].n);
+        if (gr[0].grid < 1) return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the batch kernel cannot be resident here");
+    }
+    if (gr[1].n) {
+        int dev = 0, per = 0;
+        QZ_CUDA(cudaGetDevice(&dev));
+        QZ_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+        qzb::BatchArgs probe{};
+        probe.ord = b->ord;
+        probe.with_m1 = 1;
+        probe.with_ext = gr[1].with_ext ? 1 : 0;
+        QZ_CUDA(qzb::launch_batch_m1w(&probe, sizeof(probe), 0, gr[1].smem, st, &per));
+        gr[1].grid = std::min(per * sms, gr[1].n);
+        if (gr[1].grid < 1)
+            return fail(QZ_ERR_UNSUPPORTED, "qz_batch_run: the 1024-thread batch kernel cannot be resident here");
+    }
+    const size_t fneed = std::max((size_t)gr[0].grid * gr[0].fmax, (size_t)gr[1].grid * gr[1].fmax);
+    const size_t dneed = std::max((size_t)gr[0].grid * gr[0].dmax, (size_t)gr[1].grid * gr[1].dmax);
+    const size_t bneed = std::max((size_t)gr[0].grid * gr[0].bmax, (size_t)gr[1].grid * gr[1].bmax);
+    if (b->fld_alloc < fneed || b->diag_alloc < dneed || b->bsrc_alloc < bneed) {
         for (double* q : {b->d_fld, b->d_diag, b->d_bsrc})
             if (q) cudaFree(q);
         b->d_fld = b->d_diag = b->d_bsrc = nullptr;
         b->fld_alloc = b->diag_alloc = b->bsrc_alloc = 0;
-        if (cudaMalloc((void**)&b->d_fld, sizeof(double) * need * fmax) != cudaSuccess ||
-            cudaMalloc((void**)&b->d_diag, sizeof(double) * need * dmax) != cudaSuccess ||
-            cudaMalloc((void**)&b->d_bsrc, sizeof(double) * need * bmax) != cudaSuccess) {
+        if (cudaMalloc((void**)&b->d_fld, sizeof(double) * fneed) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_diag, sizeof(double) * dneed) != cudaSuccess ||
+            cudaMalloc((void**)&b->d_bsrc, sizeof(double) * bneed) != cudaSuccess) {
             cudaGetLastError();
             return fail(QZ_ERR_NOMEM, "qz_batch_run: device allocation failed (slot buffers)");
         }
-        b->fld_alloc = need * fmax;
-        b->diag_alloc = need * dmax;
-        b->bsrc_alloc = need * bmax;
+        b->fld_alloc = fneed;
+        b->diag_alloc = dneed;
+        b->bsrc_alloc = bneed;
     }
     if (b->mom_alloc < mom_total) {
         if (b->d_mom) cudaFree(b->d_mom);
@@ -2463,10 +2499,12 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
         hi[i] = b->inst[i]->dev;
         hi[i].mom = b->d_mom + mom_off[i];
     }
+    // the queue: the 512-thread group, then the wide group, each largest first
     std::vector<int> order(ni);
     for (int i = 0; i < ni; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int x, int y) { return b->inst[x]->cost > b->inst[y]->cost; });
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return grp[x] != grp[y] ? grp[x] < grp[y] : b->inst[x]->cost > b->inst[y]->cost;
+    });
     if (!b->d_inst) {
         QZ_CUDA(cudaMalloc((void**)&b->d_next, sizeof(int)));
     }
@@ -2478,18 +2516,17 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     QZ_CUDA(cudaMalloc((void**)&b->d_order, sizeof(int) * ni));
     QZ_CUDA(cudaMemcpyAsync(b->d_inst, hi.data(), sizeof(qzb::BatchInst) * ni, cudaMemcpyHostToDevice, st));
     QZ_CUDA(cudaMemcpyAsync(b->d_order, order.data(), sizeof(int) * ni, cudaMemcpyHostToDevice, st));
-    QZ_CUDA(cudaMemsetAsync(b->d_next, 0, sizeof(int), st));
     qzb::BatchArgs B{};
     B.inst = b->d_inst;
     B.order = b->d_order;
-    B.ninst = ni;
+    B.ninst = gr[0].n;
     B.nsteps = nsteps;
     B.dt = dt;
     B.ord = b->ord;
-    B.with_m1 = with_m1 ? 1 : 0;
-    B.with_ext = with_ext ? 1 : 0;
+    B.with_m1 = gr[0].with_m1 ? 1 : 0;
+    B.with_ext = gr[0].with_ext ? 1 : 0;
     B.fld = b->d_fld; B.diag = b->d_diag; B.bsrc = b->d_bsrc;
-    B.fld_slot = fmax; B.diag_slot = dmax; B.bsrc_slot = bmax;
+    B.fld_slot = gr[0].fmax; B.diag_slot = gr[0].dmax; B.bsrc_slot = gr[0].bmax;
     B.next = b->d_next;
     B.trace = nullptr;
     if (b->trace) {
@@ -2508,7 +2545,20 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     QZ_CUDA(cudaEventCreate(&e0));
     QZ_CUDA(cudaEventCreate(&e1));
     QZ_CUDA(cudaEventRecord(e0, st));
-    QZ_CUDA(qzb::launch_batch(B, grid, smem, st));
+    if (gr[0].n) {
+        QZ_CUDA(cudaMemsetAsync(b->d_next, 0, sizeof(int), st));
+        QZ_CUDA(qzb::launch_batch(B, gr[0].grid, gr[0].smem, st));
+    }
+    if (gr[1].n) {
+        qzb::BatchArgs W = B;
+        W.order = b->d_order + gr[0].n;
+        W.ninst = gr[1].n;
+        W.with_m1 = 1;
+        W.with_ext = gr[1].with_ext ? 1 : 0;
+        W.fld_slot = gr[1].fmax; W.diag_slot = gr[1].dmax; W.bsrc_slot = gr[1].bmax;
+        QZ_CUDA(cudaMemsetAsync(b->d_next, 0, sizeof(int), st));
+        QZ_CUDA(qzb::launch_batch_m1w(&W, sizeof(W), gr[1].grid, gr[1].smem, st, nullptr));
+    }
     QZ_CUDA(cudaEventRecord(e1, st));
     if (mom_host) QZ_CUDA(cudaMemcpyAsync(mom_host, b->d_mom, sizeof(double) * mom_total, cudaMemcpyDeviceToHost, st));
     if (B.trace) {
@@ -2520,7 +2570,7 @@ extern "C" qz_status qz_batch_run(qz_batch* b, int nsteps, double dt, double* mo
     QZ_CUDA(cudaEventElapsedTime(&b->last_ms, e0, e1));
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    b->last_grid = grid;
+    b->last_grid = gr[0].n ? gr[0].grid : gr[1].grid;
     return QZ_OK;
 }
 

@@ -135,6 +135,7 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
         __syncthreads();
         const SweepArgs& A = I.sw;
         const bool reg = A.np <= kSweepThreads;
+        (void)reg;
         unsigned long long t_start = 0, t_mark = 0, t_sweep = 0, t_beam = 0;
         if (B.trace && tid == 0) t_start = t_mark = batch_timer();
         beam_deposit0(I, A);
@@ -143,11 +144,13 @@ __global__ void __launch_bounds__(kSweepThreads, 1) batch_kernel(const __grid_co
             NoGate g;
             if (WITH_M1 && I.modes) {
                 if constexpr (WITH_M1) sweep_m1_body<ORD, NoGate, EXT>(A, smem_raw, g);
-            } else if (A.rows_per_thread == 1) {
-                if (reg) sweep_body<ORD, true, 1, NoGate, EXT>(A, smem_raw, g);
-                else sweep_body<ORD, false, 1, NoGate, EXT>(A, smem_raw, g);
-            } else {
-                sweep_body<ORD, false, 4, NoGate, EXT>(A, smem_raw, g);
+            } else if constexpr (kSweepThreads == 512) {     // (the 1024-thread build runs m = 1 only)
+                if (A.rows_per_thread == 1) {
+                    if (reg) sweep_body<ORD, true, 1, NoGate, EXT>(A, smem_raw, g);
+                    else sweep_body<ORD, false, 1, NoGate, EXT>(A, smem_raw, g);
+                } else {
+                    sweep_body<ORD, false, 4, NoGate, EXT>(A, smem_raw, g);
+                }
             }
             __syncthreads();
             if (B.trace && tid == 0) { const unsigned long long t = batch_timer(); t_sweep += t - t_mark; t_mark = t; }

@@ -6,7 +6,12 @@
 
 namespace qzb {
 
-constexpr int kSweepThreads = 512;
+// threads of a sweep CTA: 512, or 1024 in the translation units of the wide m = 1 sweep (modes = 1
+// with 513..1024 radial nodes, one node per thread), which compile these headers in namespace qzb_w
+#ifndef QZ_SWEEP_THREADS
+#define QZ_SWEEP_THREADS 512
+#endif
+constexpr int kSweepThreads = QZ_SWEEP_THREADS;
 constexpr int kMaxSpecies = 4;
 
 // Everything the m = 0 sweep kernel reads or writes. Pointers are device pointers.
@@ -90,6 +95,10 @@ cudaError_t launch_sweep_m0(const SweepArgs& A, cudaStream_t stream);
 // the modes = 1 sweep: one CTA, one radial row per thread (M <= kSweepThreads), plasma in A.ps
 size_t sweep_m1_smem_bytes(int M);
 cudaError_t launch_sweep_m1(const SweepArgs& A, cudaStream_t stream);
+// the modes = 1 sweep with 1024 threads (513..1024 nodes, qz_sweep_m1w.cu): args points to a SweepArgs of
+// args_size bytes
+size_t sweep_m1w_smem_bytes(int M);
+cudaError_t launch_sweep_m1w(const void* args, size_t args_size, cudaStream_t stream);
 
 // the adjoint of an m = 0 run (qz_adjoint.cu): one CTA runs the sweep of one step in reverse, from
 // the field-store adjoint lfld (K, M, 6) to the beam-source adjoint lbsrc (K, M, 5, accumulated),
@@ -326,5 +335,9 @@ constexpr int kBatchTrace = 5;
 
 cudaError_t launch_batch(const BatchArgs& B, int grid, size_t smem, cudaStream_t stream);
 int batch_max_grid(int ord, bool with_m1, bool with_ext, size_t smem, int* sms);
+// the batch kernel for modes = 1 instances with 513..1024 nodes (1024 threads, qz_batch_m1w.cu): args points
+// to a BatchArgs of args_size bytes; per_sm != nullptr asks only for the resident CTAs per SM
+size_t batch_m1w_static_bytes();
+cudaError_t launch_batch_m1w(const void* args, size_t args_size, int grid, size_t smem, cudaStream_t s, int* per_sm);
 
 }  // namespace qzb

@@ -33,6 +33,7 @@ cudaError_t launch_t(const SweepArgs& A, size_t smem, cudaStream_t stream) {
 }  // namespace
 
 cudaError_t launch_sweep_m1(const SweepArgs& A, cudaStream_t stream) {
+    if (A.M > kSweepThreads && A.M <= 2 * kSweepThreads) return launch_sweep_m1w(&A, sizeof(A), stream);
     if (A.M > kSweepThreads || A.M < 3) return cudaErrorInvalidValue;
     const size_t smem = sweep_m1_smem_bytes(A.M);
     switch (A.ord) {

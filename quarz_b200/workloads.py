@@ -18,8 +18,8 @@ All are synthetic: seeded gaussian beams from the reference's generator, uniform
                     log-uniform in [0.05, 0.3] (set through the witness n_b, pinched-witness shape),
                     5e4 + 5e4 beam particles, dt 5, 20 steps, m = 0
   scan, modes = 1   the same draws with azimuthal modes m = 0, 1 (Picard 3, 4 azimuths per plasma ring,
-                    driver offset 0.1 in x) and N_r uniform in 128..511 cells: the m = 1 sweep keeps one
-                    radial row per thread, so M <= 512
+                    driver offset 0.1 in x) and N_r uniform in 128..1023 cells: the m = 1 sweep keeps one
+                    radial row per thread of a CTA of 512 threads, or 1024 above 512 nodes, so M <= 1024
 """
 from __future__ import annotations
 
@@ -179,7 +179,7 @@ def scan_instances(count: int = 512, seed: int = 2024, beam_particles: int = 100
     logu = lambda a, b: float(np.exp(rng.uniform(np.log(a), np.log(b))))  # noqa: E731
     out = []
     for i in range(count):
-        ncell = int(rng.integers(128, 1025 if modes == 0 else 512))
+        ncell = int(rng.integers(128, 1025 if modes == 0 else 1024))
         h0 = logu(5e-4, 5e-3)
         L = float(rng.uniform(8.0, 16.0))
         n0d = logu(1.0, 10.0)

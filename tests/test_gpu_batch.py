@@ -5,7 +5,8 @@ Instances are drawn like the scan workload (quarz_b200.workloads.scan_instances:
 stretched grids, xi lengths 8-16) with 4000 beam particles and 3 steps. Tolerances: derived beam
 moments 1e-10 relative to their natural scale against the single runs (only the summation order of
 the beam deposits differs), 1e-8 against the oracle. The m = 1 case draws the same way with modes 0, 1
-(Picard 3, 4 azimuths per ring, 128-511 cells), mixed in one batch with m = 0 instances; and a batch of
+(Picard 3, 4 azimuths per ring, 128-1023 cells: two of the three above 512 nodes, run by the 1024-thread
+batch kernel after the 512-thread one), mixed in one batch with m = 0 instances; and a batch of
 m = 0 and m = 1 instances of which three smooth their plasma sources (plasma.smooth_length = 0.02), run by
 the kernel variant with the filter."""
 import numpy as np
@@ -52,7 +53,8 @@ def test_batch_equals_single_runs_and_oracle():
 
 
 def test_batch_m1_and_mixed_modes():
-    m1 = workloads.scan_instances(3, seed=11, beam_particles=2000, steps=2, modes=1)
+    m1 = workloads.scan_instances(3, seed=4, beam_particles=2000, steps=2, modes=1)
+    assert sorted(s.M > 512 for s in m1) == [False, True, True]
     m0 = workloads.scan_instances(2, seed=12, beam_particles=2000, steps=2)
     specs = m1 + m0
     beams = [[Q.sample_beam(b) for b in s.beams] for s in specs]
@@ -71,8 +73,8 @@ def test_batch_m1_and_mixed_modes():
 def test_batch_m1_refuses_wide_grids():
     spec = workloads.scan_instances(1, seed=3, beam_particles=1000, steps=1, modes=1)[0]
     spec.modes = 1
-    spec.nodes = workloads.scan_nodes(700, 1e-3)
-    with pytest.raises(Q.QZError, match="M <= 512"):
+    spec.nodes = workloads.scan_nodes(1100, 1e-3)
+    with pytest.raises(Q.QZError, match="M <= 1024"):
         Q.Batch().add(spec)
 
 

@@ -4,7 +4,8 @@ oracle on the same inputs.
 Workload: the pinched-witness grid (512 stretched nodes) with modes = 1, Picard 3, 8 azimuths per
 plasma ring (4088 particles per slice), the driver offset 0.1 in x and tilted 1e-3, the witness offset
 0.02; box cut to xi in [-9, 0] with dxi 0.01 (901 slices) and 2 x 20000 beam particles so that the
-oracle finishes in seconds.
+oracle finishes in seconds. The wide cases put the same deck on geometric grids of 700 and 1024 nodes
+(axis cell 1e-3, wall r = 6): the m = 1 sweep then runs in a CTA of 1024 threads, one node per thread.
 
 Tolerances (relative L2 per stored component): beam sources 1e-12; fields and diagnostics after one
 sweep max(1e-10, 4 x the reference algorithm's own round-off floor on this input, i.e. the difference
@@ -25,9 +26,12 @@ MOMENT_TOL = 1e-8
 KEYS = ("gamma_mean", "gamma_rms", "xi_mean", "xi_rms", "x_mean", "y_mean", "sigma_x", "emit_nx", "charge_w", "alive")
 
 
-def _spec(steps=3, n=20000):
+def _spec(steps=3, n=20000, M=None):
     text = workloads.hosing_deck(xi_min=-9.0, driver_np=n, witness_np=n, steps=steps)
-    return workloads.spec_from_text(text, ["xi.step=0.01"])
+    spec = workloads.spec_from_text(text, ["xi.step=0.01"])
+    if M is not None:
+        spec.nodes = workloads.scan_nodes(M, 1e-3)
+    return spec
 
 
 def _gpu_sweep(spec, beams):
@@ -49,8 +53,9 @@ def _gpu_sweep(spec, beams):
             diag.cpu().numpy().reshape(K, M, 9), lost)
 
 
-def test_sweep_m1_one_step_against_oracle():
-    spec = _spec()
+@pytest.mark.parametrize("M", [None, 700, 1024])
+def test_sweep_m1_one_step_against_oracle(M):
+    spec = _spec(M=M)
     beams = [Q.sample_beam(b) for b in spec.beams]
     a = O.OracleSim(spec, beams=beams, tridiag="thomas")
     a.step_fields(0.0)
@@ -76,17 +81,18 @@ def test_sweep_m1_one_step_against_oracle():
     assert lost == a.lost()
 
 
-@pytest.mark.parametrize("pipelined", [True, False])
-def test_run_m1_moments_against_oracle(pipelined):
-    # the whole run as one pipelined launch (sweeps of consecutive steps concurrent), and step by step
-    spec = _spec(steps=3)
+@pytest.mark.parametrize("pipelined,M", [(True, None), (False, None), (True, 700)])
+def test_run_m1_moments_against_oracle(pipelined, M):
+    # the whole run as one pipelined launch (sweeps of consecutive steps concurrent), and step by step;
+    # with more than 512 nodes the run goes step by step (the pipeline's sweep CTAs have 512 threads)
+    spec = _spec(steps=3, M=M)
     beams = [Q.sample_beam(b) for b in spec.beams]
     ref = O.OracleSim(spec, beams=beams)
     mom_ref = ref.run(spec.steps, spec.dt)
     sim = Q.Simulation(spec, beams=beams)
     sim.set_schedule(pipelined)
     mom = sim.run(spec.steps, spec.dt)
-    assert sim.schedule()["pipelined"] == (1 if pipelined else 0)
+    assert sim.schedule()["pipelined"] == (1 if pipelined and spec.M <= 512 else 0)
     L = spec.K * spec.dxi
     for q, (_, gref, xiref) in enumerate(beams):
         for n in range(spec.steps + 1):
