@@ -17,7 +17,8 @@ Other workloads (not the headline; their lines are recorded beside it):
                       offset / tilted driver, 2e6 + 2e6 particles, 200 steps
   --workload scan     512 independent runs of 20 steps (a parameter scan) in one launch: runs/s, with
                       the plain loop over single runs (step by step, and pipelined) timed on a sample
-  --workload scan_m1  the same scan with azimuthal modes 0 and 1 (M <= 512)
+  --workload scan_m1  the same scan with azimuthal modes 0 and 1 (128..1023 cells; above 512 nodes the
+                      m = 1 instances run in a second launch of 1024-thread CTAs)
   --workload adjoint  the gradient of witness energy gain and spread with respect to a 64-bin driver
                       profile and the witness delay, pinched witness over 50 steps: adjoint / forward time
   --workload stages   the xi-pipelined run over the ranks (one slab of the box per GPU, the reference's

@@ -364,9 +364,9 @@ qz_status qz_sim_timing(qz_sim* s, int enable, unsigned long long* cycles16);
 
 /* ------------------------------------------------------------------ batched independent runs
  * A parameter scan: many independent small runs (each its own grid, box, plasma and up to 2 beams,
- * modes 0 or 1 (M <= 512 for modes 1), one AB order for all) in ONE persistent launch, a CTA per
- * instance taken from a queue
- * (largest first). No counterpart in the reference, which runs one deck per process; each instance
+ * modes 0 or 1 (M <= 1024 for modes 1), one AB order for all) in ONE persistent launch, a CTA per
+ * instance taken from a queue (largest first); m = 1 instances with more than 512 nodes run after it in a
+ * second launch of 1024-thread CTAs. No counterpart in the reference, which runs one deck per process; each instance
  * is Simulation::run (src/Simulation.cpp:1370-1448) for constant dt. */
 typedef struct qz_batch qz_batch;
 qz_status qz_batch_create(qz_batch** out);
