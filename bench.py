@@ -511,7 +511,7 @@ def run_scan(args, rank, world, local_rank):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "modes": modes, "instances": len(all_specs),
                        "instances_with_results": done, "time_steps_per_run": T,
-                       "beam_particles_per_run": 100000, "radial_nodes": "129..1025" if modes == 0 else "129..512",
+                       "beam_particles_per_run": 100000, "radial_nodes": "129..1025" if modes == 0 else "129..1024",
                        "xi_slices": "801..1601",
                        "parallelism": "a CTA per instance, one launch per batch; instances split over GPUs by cost"},
             "loop_runs_per_s": loop, "speedup_vs_step_by_step_loop": value / world / loop["step_by_step"],
